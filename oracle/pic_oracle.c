@@ -1,0 +1,1390 @@
+/*
+ * pic_oracle.c — CPU restatement of PiCoPiC's per-timestep PIC loop.
+ *
+ * TEST INFRASTRUCTURE ONLY (see pic_oracle.h).  Every function cites the
+ * reference file:line it restates.  The operation order of every floating
+ * point expression follows the reference source exactly, including the
+ * reference's arithmetic defects, so that with -ffp-contract=off the
+ * results are bit-identical to the compiled reference (oracle/_ref).
+ *
+ * Constants are the reference's rounded SI values (constant.hpp:35-57).
+ */
+#include "pic_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define K_PI 3.1415926535897932
+#define K_EPSILON0 8.85E-12
+#define K_EL_MASS 9.1E-31
+#define K_EL_CHARGE 1.6E-19
+#define K_LIGHT_VEL 3.0E8
+#define K_LIGHT_VEL_POW_2 (K_LIGHT_VEL * K_LIGHT_VEL)
+#define K_MAGN_CONST 1.26E-6
+#define K_MNZL 1e-15
+#define K_REL_LIMIT 5e7
+#define K_REL_LIMIT_POW_2 (K_REL_LIMIT * K_REL_LIMIT)
+#define MAX_SPECIES 16
+
+/* Status codes shared with the product ABI. */
+#define ST_OK 0
+#define ST_ARG (-1)
+#define ST_FATAL (-10)
+
+typedef struct {
+  int id, is_beam;
+  char name[64];
+  double charge, mass; /* SI: SpecieP ctor specieP.cpp:37-38 */
+  size_t n, cap;
+  double *r, *phi, *z, *r_old, *phi_old, *z_old, *vr, *vphi, *vz, *w, *sn;
+  long long *cell_r, *cell_z;
+  /* BeamP state (beamP.cpp:22-69) */
+  unsigned macro_amount, bunches_amount, current_bunch;
+  double start_time, radius, density, bunch_length, bunches_distance, velocity;
+  double finish_time, domain_radius, bunch_macro_amount, macro_per_step;
+} species_t;
+
+typedef struct {
+  uint32_t mt[624];
+  int idx;
+} mt19937_t;
+
+struct orc_sim {
+  int nr, nz, ld;
+  double R, L, dr, dz, dt, t;
+  int pml[4];
+  double pml_sigma[2];
+  size_t gcr, gcz; /* Geometry::global_cell_amount (geometry.hpp:70-71) */
+  int pusher, current, quirks;
+  double *E[3], *H[3], *Hat[3], *J[3], *sigma;
+  int nsp;
+  species_t sp[MAX_SPECIES];
+  int rng_kind;
+  uint64_t seed, step_index;
+  mt19937_t mt;
+  long errors, removed;
+};
+
+/* ------------------------------------------------------------------ */
+/* Grid<T> indexing with the 2-cell halo (grid.hpp:46-58, 165-168).     */
+#define IDX(s, i, k) ((size_t)((i) + 2) * (size_t)(s)->ld + (size_t)((k) + 2))
+
+static void halo_set(orc_sim* s, double* a, double v) { /* Grid::overlay_set grid.hpp:87-97 */
+  int xr = s->nr + 4, yr = s->nz + 4;
+  for (int i = 0; i < xr; ++i)
+    for (int j = 0; j < yr; ++j)
+      if (i < 2 || j < 2 || i >= xr - 2 || j >= yr - 2) a[(size_t)i * yr + j] = v;
+}
+
+/* ------------------------------------------------------------------ */
+/* Random sources                                                       */
+
+static void mt_seed(mt19937_t* g, uint32_t s) {
+  g->mt[0] = s;
+  for (int i = 1; i < 624; ++i)
+    g->mt[i] = 1812433253u * (g->mt[i - 1] ^ (g->mt[i - 1] >> 30)) + (uint32_t)i;
+  g->idx = 624;
+}
+
+static uint32_t mt_next(mt19937_t* g) {
+  if (g->idx >= 624) {
+    for (int i = 0; i < 624; ++i) {
+      uint32_t x = (g->mt[i] & 0x80000000u) | (g->mt[(i + 1) % 624] & 0x7fffffffu);
+      uint32_t xa = x >> 1;
+      if (x & 1u) xa ^= 0x9908b0dfu;
+      g->mt[i] = g->mt[(i + 397) % 624] ^ xa;
+    }
+    g->idx = 0;
+  }
+  uint32_t y = g->mt[g->idx++];
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+/* std::uniform_real_distribution<double>(0, 1) over std::mt19937 as
+ * libstdc++ implements it: generate_canonical<double, 53> draws two 32-bit
+ * words, sum = w0 + w1 * 2^32 (rounded to double), result = sum / 2^64,
+ * clamped below 1. */
+static double mt_uniform(mt19937_t* g) {
+  double sum = 0.0, tmp = 1.0;
+  for (int k = 0; k < 2; ++k) {
+    sum += (double)mt_next(g) * tmp;
+    tmp *= 4294967296.0;
+  }
+  double r = sum / tmp;
+  if (r >= 1.0) r = nextafter(1.0, 0.0);
+  return r;
+}
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int round = 0; round < 10; ++round) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Two 53-bit uniforms in [0,1) per Philox block: which = 0 or 1. */
+double orc_philox_uniform(uint64_t seed, uint32_t stream, uint64_t step, uint32_t index,
+                          int which) {
+  uint32_t ctr[4] = {index, (uint32_t)step, (uint32_t)(step >> 32), stream};
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t o[4];
+  orc_philox4x32_10(ctr, key, o);
+  uint32_t a = which ? o[2] : o[0], b = which ? o[3] : o[1];
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+/* ------------------------------------------------------------------ */
+/* Relativity: phys::rel (rel.cpp:24-55)                                */
+
+static int lorenz_factor(double sq_velocity, double* gamma_out) {
+  double beta = sq_velocity / K_LIGHT_VEL_POW_2;
+  if (beta > 1) return ST_FATAL; /* LOG_S(FATAL) rel.cpp:33-34 */
+  double gamma = 1 / sqrt(1.0 - beta);
+  if (isinf(gamma)) gamma = 1e100; /* rel.cpp:38-42 */
+  *gamma_out = gamma;
+  return ST_OK;
+}
+
+static double lorenz_factor_inv(double sq_velocity) {
+  return pow(1.0 + sq_velocity / K_LIGHT_VEL_POW_2, -0.5);
+}
+
+/* ------------------------------------------------------------------ */
+/* Geometry macros (geometry.hpp:186-198), keeping the reference's        */
+/* unparenthesised macro argument: CELL_VOLUME(i+1) expands to            */
+/* PI*dz*dr*dr*(2.0*i + 1 + 1).                                           */
+
+static inline double cell_volume_expr(double two_i_plus_rest, double dr, double dz) {
+  return K_PI * dz * dr * dr * two_i_plus_rest;
+}
+#define CELL_NUMBER(pos, dx) ((int)floor((pos) / (dx)))
+
+/* ------------------------------------------------------------------ */
+/* PML: MaxwellSolverYee::set_pml (maxwellSolverYee.cpp:57-109)          */
+
+static void set_pml(orc_sim* s) {
+  double dr = s->dr, dz = s->dz;
+  double l_left = dz * (double)s->pml[1];
+  double l_right = dz * (double)s->pml[3];
+  double l_ext = dr * (double)s->pml[2];
+  double r_off = 0.0 * dr, z_off = 0.0 * dz;
+  double sys_r = s->R, sys_l = s->L;
+  double dsig = s->pml_sigma[1] - s->pml_sigma[0];
+  if (s->pml[2] != 0)
+    for (int i = 0; i < s->nr; i++)
+      for (int k = 0; k < s->nz; k++) {
+        double dist = (double)(s->gcr - 0 - (size_t)i) * dr; /* Geometry::dist_x_to_end */
+        if (dist < l_ext)
+          s->sigma[IDX(s, i, k)] += s->pml_sigma[0] + dsig / pow(l_ext, 2) *
+                                                          pow(dr * (i + 1) + r_off - sys_r + l_ext, 2);
+      }
+  if (s->pml[1] != 0)
+    for (int k = 0; k < s->nz; k++)
+      for (int i = 0; i < s->nr; i++)
+        if (dz * k + z_off < l_left)
+          s->sigma[IDX(s, i, k)] += s->pml_sigma[0] + dsig / pow(l_left, 2) *
+                                                          pow(l_left - dz * k - z_off, 2);
+  if (s->pml[3] != 0)
+    for (int k = 0; k < s->nz; k++)
+      for (int i = 0; i < s->nr; i++) {
+        double dist = (double)(s->gcz - 0 - (size_t)k) * dz; /* Geometry::dist_y_to_end */
+        if (dist < l_right)
+          s->sigma[IDX(s, i, k)] += s->pml_sigma[0] + dsig / pow(l_right, 2) *
+                                                          pow(dz * (k + 1) + z_off - sys_l + l_right, 2);
+      }
+}
+
+/* ------------------------------------------------------------------ */
+/* Yee solver                                                            */
+
+/* MaxwellSolverYee::calc_field_e (maxwellSolverYee.cpp:161-257); one
+ * domain: walls on, r_begin = z_begin = 1, r_end = nr-1, z_end = nz-1. */
+static int field_e(orc_sim* s) {
+  double *Er = s->E[0], *Ep = s->E[1], *Ez = s->E[2];
+  double *Jr = s->J[0], *Jp = s->J[1], *Jz = s->J[2];
+  double *Hr = s->Hat[0], *Hp = s->Hat[1], *Hz = s->Hat[2];
+  for (int c = 0; c < 3; ++c) halo_set(s, s->E[c], 0.0);
+  double dr = s->dr, dz = s->dz, dt = s->dt;
+  int r_begin = 1, z_begin = 1, r_end = s->nr - 1, z_end = s->nz - 1;
+
+  for (int k = z_begin; k < z_end; ++k) { /* axis r = 0, :170-194 */
+    int i = 0;
+    double epsx2 = 2 * K_EPSILON0;
+    double sigma_t = s->sigma[IDX(s, i, k)] * dt;
+    double koef_e = (epsx2 - sigma_t) / (epsx2 + sigma_t);
+    double koef_h = 2 * dt / (epsx2 + sigma_t);
+    size_t p = IDX(s, i, k);
+    Er[p] *= koef_e;
+    Er[p] -= (Jr[p] + (Hp[p] - Hp[IDX(s, i, k - 1)]) / dz) * koef_h;
+    Ez[p] *= koef_e;
+    Ez[p] -= (Jz[p] - Hp[p] * 4. / dr) * koef_h;
+  }
+  for (int i = r_begin; i < r_end; ++i) { /* z = 0 wall, :196-218 */
+    int k = 0;
+    double epsx2 = 2 * K_EPSILON0;
+    double sigma_t = s->sigma[IDX(s, i, k)] * dt;
+    double koef_e = (epsx2 - sigma_t) / (epsx2 + sigma_t);
+    double koef_h = 2 * dt / (epsx2 + sigma_t);
+    size_t p = IDX(s, i, k), pm = IDX(s, i - 1, k);
+    Ez[p] *= koef_e;
+    Ez[p] -= (Jz[p] - (Hp[p] - Hp[pm]) / dr - (Hp[p] + Hp[pm]) / (2. * dr * (double)i)) * koef_h;
+  }
+  for (int i = r_begin; i < r_end; i++) /* regular, :220-256 */
+    for (int k = z_begin; k < z_end; k++) {
+      double epsx2 = 2 * K_EPSILON0;
+      double sigma_t = s->sigma[IDX(s, i, k)] * dt;
+      double koef_e = (epsx2 - sigma_t) / (epsx2 + sigma_t);
+      double koef_h = 2 * dt / (epsx2 + sigma_t);
+      size_t p = IDX(s, i, k), pkm = IDX(s, i, k - 1), pim = IDX(s, i - 1, k);
+      Er[p] *= koef_e;
+      Er[p] -= (Jr[p] + (Hp[p] - Hp[pkm]) / dz) * koef_h;
+      Ep[p] *= koef_e;
+      Ep[p] -= (Jp[p] - (Hr[p] - Hr[pkm]) / dz + (Hz[p] - Hz[pim]) / dr) * koef_h;
+      Ez[p] *= koef_e;
+      Ez[p] -= (Jz[p] - (Hp[p] - Hp[pim]) / dr - (Hp[p] + Hp[pim]) / (2. * dr * (double)i)) * koef_h;
+      if (isnan(Er[p]) || isnan(Ep[p]) || isnan(Ez[p])) return ST_FATAL; /* :253-255 */
+    }
+  return ST_OK;
+}
+
+/* MaxwellSolverYee::calc_field_h (maxwellSolverYee.cpp:111-159). */
+static int field_h(orc_sim* s) {
+  double *Er = s->E[0], *Ep = s->E[1], *Ez = s->E[2];
+  for (int c = 0; c < 3; ++c) {
+    halo_set(s, s->H[c], 0.0);
+    halo_set(s, s->Hat[c], 0.0);
+  }
+  double dr = s->dr, dz = s->dz, dt = s->dt;
+  int fix = s->quirks == ORC_QUIRKS_FIXED;
+  if (!fix) /* outer-wall H_r loop :119-130, updated again by the regular loop */
+    for (int k = 0; k < s->nz; k++) {
+      int i = s->nr - 1;
+      size_t p = IDX(s, i, k);
+      double alpha_t = dt * (Ep[IDX(s, i, k + 1)] - Ep[p]) / (dz * K_MAGN_CONST);
+      s->H[0][p] = s->Hat[0][p] + alpha_t / 2;
+      s->Hat[0][p] += alpha_t;
+    }
+  for (int i = 0; i < s->nr; i++)
+    for (int k = 0; k < s->nz; k++) {
+      size_t p = IDX(s, i, k), pk = IDX(s, i, k + 1), pi = IDX(s, i + 1, k);
+      double a_r = dt * (Ep[pk] - Ep[p]) / (dz * K_MAGN_CONST);
+      s->H[0][p] = s->Hat[0][p] + a_r / 2;
+      s->Hat[0][p] += a_r;
+      double a_phi = dt * ((Ez[pi] - Ez[p]) / dr - (Er[pk] - Er[p]) / dz) / K_MAGN_CONST;
+      s->H[1][p] = s->Hat[1][p] + a_phi / 2;
+      s->Hat[1][p] += a_phi;
+      double a_z = dt * ((Ep[pi] + Ep[p]) / (2. * dr * (i + 0.5 + 0.0)) + (Ep[pi] - Ep[p]) / dr) / K_MAGN_CONST;
+      s->H[2][p] = s->Hat[2][p] - a_z / 2;
+      s->Hat[2][p] -= a_z;
+    }
+  return ST_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* Field gather: MaxwellSolver::get_field_h / get_field_e                */
+/* (maxwellSolver.hpp:101-209, 211-316).  Each term is                   */
+/*   field * PI * dz_ * (rb*rb - ra*ra) / vol                            */
+/* evaluated left to right, as the macro expansion of CYL_RNG_VOL gives.  */
+
+static inline double term(double f, double dzz, double ra, double rb, double vol) {
+  return f * K_PI * dzz * (rb * rb - ra * ra) / vol;
+}
+
+static void gather_h(const orc_sim* s, double radius, double longitude, double cmp[3]) {
+  const double dr = s->dr, dz = s->dz;
+  const double *Hr = s->H[0], *Hp = s->H[1], *Hz = s->H[2];
+  double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr, r2, dz1, dz2, v1, v2;
+  int i, k;
+  cmp[0] = cmp[1] = cmp[2] = 0;
+  /* H_z :120-147 */
+  i = CELL_NUMBER(radius - 0.5 * dr, dr);
+  k = CELL_NUMBER(longitude, dz);
+  v1 = cell_volume_expr(2.0 * i + 1 + 1, dr, dz);
+  v2 = cell_volume_expr(2.0 * i + 3 + 1, dr, dz);
+  dz1 = (k + 1) * dz - longitude;
+  dz2 = longitude - k * dz;
+  r2 = (i + 1) * dr;
+  cmp[2] += term(Hz[IDX(s, i, k)], dz1, r1, r2, v1);
+  cmp[2] += term(Hz[IDX(s, i + 1, k)], dz1, r2, r3, v2);
+  cmp[2] += term(Hz[IDX(s, i, k + 1)], dz2, r1, r2, v1);
+  cmp[2] += term(Hz[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+  /* H_r :149-177 */
+  i = CELL_NUMBER(radius, dr);
+  k = CELL_NUMBER(longitude - 0.5 * dz, dz);
+  v1 = cell_volume_expr(2.0 * i + 1, dr, dz);
+  v2 = cell_volume_expr(2.0 * i + 2 + 1, dr, dz);
+  r2 = (i + 0.5) * dr;
+  dz1 = (k + 1.5) * dz - longitude;
+  dz2 = longitude - (k + 0.5) * dz;
+  cmp[0] += term(Hr[IDX(s, i, k)], dz1, r1, r2, v1);
+  cmp[0] += term(Hr[IDX(s, i + 1, k)], dz1, r2, r3, v2);
+  cmp[0] += term(Hr[IDX(s, i, k + 1)], dz2, r1, r2, v1);
+  cmp[0] += term(Hr[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+  /* H_phi :179-206 */
+  i = CELL_NUMBER(radius - 0.5 * dr, dr);
+  k = CELL_NUMBER(longitude - 0.5 * dz, dz);
+  r2 = (i + 1) * dr;
+  v1 = cell_volume_expr(2.0 * i + 1 + 1, dr, dz);
+  v2 = cell_volume_expr(2.0 * i + 3 + 1, dr, dz);
+  dz1 = (k + 1.5) * dz - longitude;
+  dz2 = longitude - (k + 0.5) * dz;
+  cmp[1] += term(Hp[IDX(s, i, k)], dz1, r1, r2, v1);
+  cmp[1] += term(Hp[IDX(s, i + 1, k)], dz1, r2, r3, v2);
+  cmp[1] += term(Hp[IDX(s, i, k + 1)], dz2, r1, r2, v1);
+  cmp[1] += term(Hp[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+}
+
+static void gather_e(const orc_sim* s, double radius, double longitude, double cmp[3]) {
+  const double dr = s->dr, dz = s->dz;
+  const double *Er = s->E[0], *Ep = s->E[1], *Ez = s->E[2];
+  double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr, r2, dz1, dz2, v1, v2;
+  int i, k;
+  cmp[0] = cmp[1] = cmp[2] = 0;
+  /* E_r :231-257 */
+  i = CELL_NUMBER(radius - 0.5 * dr, dr);
+  k = CELL_NUMBER(longitude, dz);
+  v1 = cell_volume_expr(2.0 * i + 1 + 1, dr, dz);
+  v2 = cell_volume_expr(2.0 * i + 3 + 1, dr, dz);
+  dz1 = (k + 1) * dz - longitude;
+  dz2 = longitude - k * dz;
+  r2 = (i + 1) * dr;
+  cmp[0] += term(Er[IDX(s, i, k)], dz1, r1, r2, v1);
+  cmp[0] += term(Er[IDX(s, i + 1, k)], dz1, r2, r3, v2);
+  cmp[0] += term(Er[IDX(s, i, k + 1)], dz2, r1, r2, v1);
+  cmp[0] += term(Er[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+  /* E_z :259-283 */
+  i = CELL_NUMBER(radius, dr);
+  k = CELL_NUMBER(longitude - 0.5 * dz, dz);
+  v1 = cell_volume_expr(2.0 * i + 1, dr, dz);
+  v2 = cell_volume_expr(2.0 * i + 2 + 1, dr, dz);
+  r2 = (i + 0.5) * dr;
+  dz1 = (k + 1.5) * dz - longitude;
+  dz2 = longitude - (k + 0.5) * dz;
+  cmp[2] += term(Ez[IDX(s, i, k)], dz1, r1, r2, v1);
+  cmp[2] += term(Ez[IDX(s, i + 1, k)], dz1, r2, r3, v2);
+  cmp[2] += term(Ez[IDX(s, i, k + 1)], dz2, r1, r2, v1);
+  cmp[2] += term(Ez[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+  /* E_phi :285-313; the reference adds the [i+1][k+1] E_phi term to E_z */
+  i = CELL_NUMBER(radius, dr);
+  k = CELL_NUMBER(longitude, dz);
+  v1 = cell_volume_expr(2.0 * i + 1, dr, dz);
+  v2 = cell_volume_expr(2.0 * i + 2 + 1, dr, dz);
+  r2 = (i + 0.5) * dr;
+  dz1 = (k + 1) * dz - longitude;
+  dz2 = longitude - k * dz;
+  cmp[1] += term(Ep[IDX(s, i, k)], dz1, r1, r2, v1);
+  cmp[1] += term(Ep[IDX(s, i + 1, k)], dz1, r2, r3, v2);
+  cmp[1] += term(Ep[IDX(s, i, k + 1)], dz2, r1, r2, v1);
+  if (s->quirks == ORC_QUIRKS_FIXED)
+    cmp[1] += term(Ep[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+  else
+    cmp[2] += term(Ep[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
+}
+
+/* ------------------------------------------------------------------ */
+/* Pushers                                                               */
+
+static double len2(const double v[3]) { return v[0] * v[0] + v[1] * v[1] + v[2] * v[2]; }
+
+/* PusherBoris::operator() (pusherBoris.cpp:23-151) for one particle.
+ * ADAPTIVE uses v^2 > REL_LIMIT^2 as the (intended) switch; the reference
+ * leaves `use_rel` uninitialised otherwise (:38). */
+static int push_boris(int mode, double charge, double mass, double dt, const double e_in[3],
+                      const double b_in[3], double v[3]) {
+  double e[3] = {e_in[0], e_in[1], e_in[2]}, b[3] = {b_in[0], b_in[1], b_in[2]}, vt[3];
+  double c2m = charge * dt / (2 * mass);
+  double gamma = 1;
+  for (int c = 0; c < 3; ++c) e[c] *= c2m;
+  double bk = c2m * K_MAGN_CONST;
+  for (int c = 0; c < 3; ++c) b[c] *= bk;
+  int use_rel = (mode == ORC_PUSHER_BORIS_RELATIVISTIC) ||
+                (mode == ORC_PUSHER_BORIS_ADAPTIVE &&
+                 pow(v[0], 2) + pow(v[1], 2) + pow(v[2], 2) > K_REL_LIMIT_POW_2);
+  if (use_rel) {
+    if (lorenz_factor(len2(v), &gamma) != ST_OK) return ST_FATAL;
+    for (int c = 0; c < 3; ++c) v[c] *= gamma;
+  }
+  for (int c = 0; c < 3; ++c) v[c] += e[c];
+  if (use_rel) {
+    gamma = lorenz_factor_inv(len2(v));
+    for (int c = 0; c < 3; ++c) b[c] *= gamma;
+  }
+  double const2 = 2. / (1. + len2(b));
+  vt[0] = v[0]; vt[1] = v[1]; vt[2] = v[2];
+  v[0] = vt[0] + const2 * ((vt[1] - vt[0] * b[2] + vt[2] * b[0]) * b[2] -
+                           (vt[2] + vt[0] * b[1] - vt[1] * b[0]) * b[1]);
+  v[1] = vt[1] + const2 * (-(vt[0] + vt[1] * b[2] - vt[2] * b[1]) * b[2] +
+                           (vt[2] + vt[0] * b[1] - vt[1] * b[0]) * b[0]);
+  v[2] = vt[2] + const2 * ((vt[0] + vt[1] * b[2] - vt[2] * b[1]) * b[1] -
+                           (vt[1] - vt[0] * b[2] + vt[2] * b[0]) * b[0]);
+  for (int c = 0; c < 3; ++c) v[c] += e[c];
+  if (use_rel) {
+    gamma = lorenz_factor_inv(len2(v));
+    for (int c = 0; c < 3; ++c) v[c] *= gamma;
+  }
+  return ST_OK;
+}
+
+static double dot3(const double a[3], const double b[3]) {
+  double r = 0;
+  for (int c = 0; c < 3; ++c) r += a[c] * b[c];
+  return r;
+}
+
+/* PusherVay::operator() (pusherVay.cpp:22-114).  quirks=reference keeps
+ * the reference's use of u in m/s where the scheme expects u/c. */
+static int push_vay(int fixed, double charge, double mass, double dt, const double e_in[3],
+                    const double b_in[3], double v[3]) {
+  double e[3] = {e_in[0], e_in[1], e_in[2]}, b[3] = {b_in[0], b_in[1], b_in[2]};
+  double up[3], psm[3], gamma, s, us2, alpha, B2;
+  double c2m = charge * dt / (2 * mass);
+  if (lorenz_factor(len2(v), &gamma) != ST_OK) return ST_FATAL;
+  for (int c = 0; c < 3; ++c) v[c] *= gamma;
+  if (fixed) /* work in units of c */
+    for (int c = 0; c < 3; ++c) v[c] /= K_LIGHT_VEL;
+  up[0] = v[0]; up[1] = v[1]; up[2] = v[2];
+  double ek = 2. * c2m;
+  for (int c = 0; c < 3; ++c) e[c] *= ek;
+  if (fixed)
+    for (int c = 0; c < 3; ++c) e[c] /= K_LIGHT_VEL;
+  for (int c = 0; c < 3; ++c) up[c] += e[c];
+  double bk = c2m * K_MAGN_CONST;
+  for (int c = 0; c < 3; ++c) b[c] *= bk;
+  if (fixed) {
+    gamma = 1. / sqrt(1. + len2(v));
+  } else {
+    gamma = lorenz_factor_inv(len2(v));
+  }
+  up[0] += gamma * (v[1] * b[2] - v[2] * b[1]);
+  up[1] += gamma * (v[2] * b[0] - v[0] * b[2]);
+  up[2] += gamma * (v[0] * b[1] - v[1] * b[0]);
+  alpha = 1. + len2(up);
+  B2 = len2(b);
+  s = alpha - B2;
+  us2 = pow(dot3(up, b), 2);
+  alpha = 1. / sqrt(0.5 * (s + sqrt(s * s + 4. * (B2 + us2))));
+  for (int c = 0; c < 3; ++c) b[c] *= alpha;
+  s = 1. / (1. + len2(b));
+  alpha = dot3(up, b);
+  psm[0] = s * (up[0] + alpha * b[0] + b[2] * up[1] - b[1] * up[2]);
+  psm[1] = s * (up[1] + alpha * b[1] + b[0] * up[2] - b[2] * up[0]);
+  psm[2] = s * (up[2] + alpha * b[2] + b[1] * up[0] - b[0] * up[1]);
+  if (fixed) {
+    gamma = 1. / sqrt(1. + len2(psm));
+    for (int c = 0; c < 3; ++c) psm[c] *= gamma * K_LIGHT_VEL;
+  } else {
+    gamma = lorenz_factor_inv(len2(psm));
+    for (int c = 0; c < 3; ++c) psm[c] *= gamma;
+  }
+  v[0] = psm[0]; v[1] = psm[1]; v[2] = psm[2];
+  return ST_OK;
+}
+
+/* PusherHC::operator() (pusherHC.cpp:23-117).  quirks=reference keeps the
+ * m/s-as-normalised defect and inv_det_B = 1/(1+b2[0]+b2[1]+b2[0]) (:94). */
+static int push_hc(int fixed, double charge, double mass, double dt, const double e_in[3],
+                   const double b_in[3], double v[3]) {
+  double e[3] = {e_in[0], e_in[1], e_in[2]}, b[3] = {b_in[0], b_in[1], b_in[2]};
+  double psm[3], um[3], upv[3], b2[3], bx[3], gamma, B2;
+  double c2m = charge * dt / (2 * mass);
+  if (lorenz_factor(len2(v), &gamma) != ST_OK) return ST_FATAL;
+  for (int c = 0; c < 3; ++c) v[c] *= gamma;
+  if (fixed)
+    for (int c = 0; c < 3; ++c) v[c] /= K_LIGHT_VEL;
+  for (int c = 0; c < 3; ++c) e[c] *= c2m;
+  if (fixed)
+    for (int c = 0; c < 3; ++c) e[c] /= K_LIGHT_VEL;
+  psm[0] = e[0]; psm[1] = e[1]; psm[2] = e[2];
+  for (int c = 0; c < 3; ++c) um[c] = v[c] + psm[c];
+  double gfm2 = (1. + len2(um));
+  double bk = c2m * K_MAGN_CONST;
+  for (int c = 0; c < 3; ++c) b[c] *= bk;
+  B2 = len2(b);
+  gamma = 1. / sqrt(0.5 * (gfm2 - B2 +
+                           sqrt(pow(gfm2 - B2, 2) +
+                                4.0 * (B2 + pow(b[0] * um[0] + b[1] * um[1] + b[2] * um[2], 2)))));
+  for (int c = 0; c < 3; ++c) b[c] *= gamma;
+  for (int c = 0; c < 3; ++c) b2[c] = b[c] * b[c];
+  bx[0] = b[0] * b[1];
+  bx[1] = b[1] * b[2];
+  bx[2] = b[2] * b[0];
+  double inv_det_B = fixed ? 1.0 / (1.0 + b2[0] + b2[1] + b2[2]) : 1.0 / (1.0 + b2[0] + b2[1] + b2[0]);
+  /* the reference uses b[2] in the last term of up[0] (:97); Higuera-Cary has b[1] */
+  upv[0] = ((1.0 + b2[0] - b2[1] - b2[2]) * um[0] + 2. * (bx[0] + b[2]) * um[1] +
+            2. * (bx[2] - (fixed ? b[1] : b[2])) * um[2]) * inv_det_B;
+  upv[1] = (2. * (bx[0] - b[2]) * um[0] + (1. - b2[0] + b2[1] - b2[2]) * um[1] +
+            2. * (bx[1] + b[0]) * um[2]) * inv_det_B;
+  upv[2] = (2. * (bx[2] + b[1]) * um[0] + 2. * (bx[1] - b[0]) * um[1] +
+            (1. - b2[0] - b2[1] + b2[2]) * um[2]) * inv_det_B;
+  for (int c = 0; c < 3; ++c) psm[c] += upv[c];
+  if (fixed) {
+    gamma = 1. / sqrt(1. + len2(psm));
+    for (int c = 0; c < 3; ++c) psm[c] *= gamma * K_LIGHT_VEL;
+  } else {
+    gamma = lorenz_factor_inv(len2(psm));
+    for (int c = 0; c < 3; ++c) psm[c] *= gamma;
+  }
+  v[0] = psm[0]; v[1] = psm[1]; v[2] = psm[2];
+  return ST_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* Particle kinematics (specieP.cpp:482-663, beamP.cpp:159-177)          */
+
+static void stage_dump_old(species_t* p) { /* dump_position_to_old :642-650 */
+  for (size_t j = 0; j < p->n; ++j) {
+    p->r_old[j] = p->r[j];
+    p->phi_old[j] = p->phi[j];
+    p->z_old[j] = p->z[j];
+  }
+}
+
+static void stage_move(species_t* p, double dt) { /* mover_cylindrical :482-491 */
+  for (size_t j = 0; j < p->n; ++j) {
+    p->r[j] = p->r[j] + p->vr[j] * dt;
+    p->phi[j] = p->phi[j] + p->vphi[j] * dt;
+    p->z[j] = p->z[j] + p->vz[j] * dt;
+  }
+}
+
+static void stage_pos_rz(species_t* p) { /* back_position_to_rz :609-622 */
+  for (size_t j = 0; j < p->n; ++j) {
+    double pr = p->r[j], pp = p->phi[j];
+    double r = sqrt(pr * pr + pp * pp);
+    p->sn[j] = pp / r;
+    p->r[j] = r;
+    p->phi[j] = 0;
+  }
+}
+
+static void stage_vel_rz(species_t* p) { /* back_velocity_to_rz :624-640 */
+  for (size_t j = 0; j < p->n; ++j) {
+    double sn = p->sn[j];
+    double cs = sqrt(1 - sn * sn);
+    double vr = p->vr[j], vp = p->vphi[j];
+    double u2 = cs * vr - sn * vp;
+    double v2 = sn * vr + cs * vp;
+    p->vr[j] = u2;
+    p->vphi[j] = v2;
+  }
+}
+
+static void stage_bind(species_t* p, double dr, double dz) { /* bind_cell_numbers :652-663 */
+  for (size_t j = 0; j < p->n; ++j) {
+    p->cell_r[j] = CELL_NUMBER(p->r[j], dr);
+    p->cell_z[j] = CELL_NUMBER(p->z[j], dz);
+  }
+}
+
+/* SpecieP::reflect (specieP.cpp:493-607) for one domain at the origin. */
+static int reflect_one(const orc_sim* s, int fixed, double* r, double* z, double r_old,
+                       double z_old, double* vr, double* vz) {
+  double dr = s->dr, dz = s->dz;
+  double half_dr = dr / 2., half_dz = dz / 2.;
+  double radius_wall = s->R - dr / 2.;
+  double longitude_wall = s->L - dz / 2.;
+  double radius_wallX2 = radius_wall * 2.;
+  double longitude_wallX2 = longitude_wall * 2.;
+  double pos_r = *r - 0.0, pos_z = *z - 0.0;
+  double pos_old_r = r_old - 0.0, pos_old_z = z_old - 0.0;
+  double pdr = pos_r - pos_old_r, pdz = pos_z - pos_old_z;
+  int guard = 0;
+  while (isnormal(pos_r) && isnormal(pos_z) &&
+         (pos_r > radius_wall || pos_z > longitude_wall || pos_r < half_dr || pos_z < half_dz)) {
+    if (++guard > 1000) return ST_FATAL;
+    if (pos_r > radius_wall) {
+      *vr = -*vr;
+      double dr_small = radius_wall - pos_old_r;
+      double dz_small = dr_small * pdz / pdr;
+      pos_r = radius_wallX2 - pos_r;
+      pdr = pdr - dr_small;
+      pdz = pdz - dz_small;
+      pos_old_r = radius_wall;
+      pos_old_z = pos_old_z - dz_small;
+    }
+    if (pos_z > longitude_wall) {
+      *vz = -*vz;
+      double dz_small = longitude_wall - pos_old_z;
+      double dr_small = dz_small * pdr / pdz;
+      pos_z = longitude_wallX2 - pos_z;
+      pdr = pdr - dr_small;
+      pdz = pdz - dz_small;
+      pos_old_z = longitude_wall;
+      pos_old_r = pos_old_r - dr_small;
+    }
+    if (pos_r < half_dr) {
+      *vr = -*vr;
+      double dr_small = half_dr - pos_old_r;
+      double dz_small = dr_small * pdz / pdr;
+      pos_r = dr - pos_r;
+      pdr = pdr - dr_small;
+      pdz = pdz - dz_small;
+      pos_old_r = half_dr;
+      pos_old_z = pos_old_z - dz_small;
+      if (pos_r < half_dr) pos_r = half_dr;
+    }
+    if (pos_z < half_dz) {
+      *vz = -*vz;
+      double dz_small = half_dz - pos_old_z;
+      double dr_small = dz_small * pdr / pdz;
+      pos_z = dz - pos_z;
+      pdr = pdr - dr_small;
+      pdz = pdz - dz_small;
+      pos_old_z = fixed ? half_dz : dz; /* the reference resets to dz (:592) */
+      pos_old_r = pos_old_r - dr_small;
+      if (pos_z < half_dz) pos_z = half_dz;
+    }
+  }
+  *r = pos_r + 0.0;
+  *z = pos_z + 0.0;
+  return ST_OK;
+}
+
+static int stage_reflect(orc_sim* s, species_t* p) {
+  if (p->is_beam) { /* BeamP::reflect beamP.cpp:159-177: the axis only */
+    double half_dr = s->dr / 2.;
+    for (size_t j = 0; j < p->n; ++j) {
+      double pos_r = p->r[j] - 0.0;
+      if (pos_r < half_dr) {
+        p->r[j] = s->dr - pos_r + 0.0;
+        p->vr[j] = -p->vr[j];
+      }
+    }
+    return ST_OK;
+  }
+  int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  for (size_t j = 0; j < p->n; ++j)
+    if (reflect_one(s, fixed, &p->r[j], &p->z[j], p->r_old[j], p->z_old[j], &p->vr[j],
+                    &p->vz[j]) != ST_OK)
+      return ST_FATAL;
+  return ST_OK;
+}
+
+/* SMB::particles_runaway_collector for one domain (SMB.cpp:232-345):
+ * stable removal of particles bound outside [0,nr) x [0,nz). */
+static void stage_collect(orc_sim* s, species_t* p) {
+  size_t o = 0;
+  for (size_t j = 0; j < p->n; ++j) {
+    long long cr = p->cell_r[j], cz = p->cell_z[j];
+    int gone = cr < 0 || cz < 0 || cr >= s->nr || cz >= s->nz;
+    if (gone) {
+      ++s->removed;
+      continue;
+    }
+    if (o != j) {
+      p->r[o] = p->r[j]; p->phi[o] = p->phi[j]; p->z[o] = p->z[j];
+      p->r_old[o] = p->r_old[j]; p->phi_old[o] = p->phi_old[j]; p->z_old[o] = p->z_old[j];
+      p->vr[o] = p->vr[j]; p->vphi[o] = p->vphi[j]; p->vz[o] = p->vz[j];
+      p->w[o] = p->w[j]; p->sn[o] = p->sn[j];
+      p->cell_r[o] = p->cell_r[j]; p->cell_z[o] = p->cell_z[j];
+    }
+    ++o;
+  }
+  p->n = o;
+}
+
+/* ------------------------------------------------------------------ */
+/* Villasenor-Buneman current (currentVB.cpp:22-735)                     */
+
+static inline double ssd_r(double q, double r, double dr, double dz, double dt) {
+  return q / (2. * K_PI * r * dr * dz * dt * 2. * dr); /* SOME_SHIT_DENSITY_R */
+}
+static inline double ssd_z(double q, double r, double dr, double dz, double dt) {
+  return q / (2. * K_PI * r * dr * dz * dt * dz); /* SOME_SHIT_DENSITY_Z */
+}
+static inline double ssd_strict(double q, double r, double dr, double dz, double dt) {
+  return q / (K_PI * 4. * r * dz * dz * dr * dt); /* SOME_SHIT_DENSITY_STRICT */
+}
+
+/* simple_current_distribution :22-173 — a segment inside cell (i_n, k_n). */
+static void vb_simple(orc_sim* s, double rn, double zn, double ro, double zo, int i_n, int k_n,
+                      double q) {
+  double *Jr = s->J[0], *Jz = s->J[2];
+  double dr = s->dr, dz = s->dz, dt = s->dt, wj, k, b, r0, r1, sd;
+  double delta_r = rn - ro, delta_z = zn - zo;
+  if ((fabs(delta_r) < K_MNZL) || (fabs(delta_z) < K_MNZL)) return;
+  if (i_n >= 1) {
+    k = delta_r / delta_z;
+    b = ro;
+    sd = ssd_r(q, i_n * dr, dr, dz, dt);
+    wj = sd * (dr * delta_z - k * delta_z * delta_z / 2. - delta_z * b +
+               dr * dr / k * ((i_n + 0.5) * (i_n + 0.5) - 0.25) * log((k * delta_z + b) / b));
+    Jz[IDX(s, i_n, k_n)] += wj;
+    sd = ssd_r(q, (i_n + 1) * dr, dr, dz, dt);
+    wj = sd * (k * delta_z * delta_z / 2. + delta_z * b + delta_z * dr +
+               dr * dr / k * (0.25 - (i_n + 0.5) * (i_n + 0.5)) * log((k * delta_z + b) / b));
+    Jz[IDX(s, i_n + 1, k_n)] += wj;
+  } else {
+    k = delta_r / delta_z;
+    b = ro;
+    sd = q / (2. * K_PI * dr / 4. * dr * dz * dt * dr);
+    wj = sd * (dr * delta_z - k * delta_z * delta_z / 2. - delta_z * b);
+    Jz[IDX(s, i_n, k_n)] += wj;
+    sd = ssd_r(q, dr, dr, dz, dt);
+    wj = sd * (k * delta_z * delta_z / 2. + delta_z * dr + delta_z * b);
+    Jz[IDX(s, i_n + 1, k_n)] += wj;
+  }
+  /* J_r, identical in both branches :78-108 and :135-171 */
+  k = -delta_z / delta_r;
+  r0 = (i_n + 0.5) * dr;
+  r1 = ro;
+  b = (k_n + 1.) * dz - zo;
+  sd = ssd_z(q, r0, dr, dz, dt);
+  wj = sd * (r0 * k * delta_r + k / 2. * delta_r * (ro + delta_r / 2.) +
+             0.5 * delta_r * (b - k * (2 * r0 + r1)) +
+             delta_r * (b - k * r1) * (4 * r0 * r0 - dr * dr) / (8 * ro * (ro + delta_r)) +
+             (k * (r0 * r0 / 2. - dr * dr / 8.)) * log((ro + delta_r) / ro));
+  Jr[IDX(s, i_n, k_n)] += wj;
+  b = zo - k_n * dz;
+  wj = sd * (-r0 * k * delta_r - k / 2. * delta_r * (ro + delta_r / 2.) +
+             0.5 * delta_r * (b + k * (2 * r0 + r1)) +
+             delta_r * (b + k * r1) * (4 * r0 * r0 - dr * dr) / (8 * ro * (ro + delta_r)) -
+             (k * (r0 * r0 / 2. - dr * dr / 8.)) * log((ro + delta_r) / ro));
+  Jr[IDX(s, i_n, k_n + 1)] += wj;
+}
+
+/* strict_motion_distribution :500-729 — purely axial or radial motion. */
+static void vb_strict(orc_sim* s, double rn, double zn, double ro, double zo, double q) {
+  double *Jr = s->J[0], *Jz = s->J[2];
+  double dr = s->dr, dz = s->dz, dt = s->dt;
+  int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  int i_n = CELL_NUMBER(rn, dr), k_n = CELL_NUMBER(zn, dz);
+  int i_o = CELL_NUMBER(ro, dr), k_o = CELL_NUMBER(zo, dz);
+  if ((fabs(rn - ro) < K_MNZL) && (fabs(zn - zo) < K_MNZL)) return;
+  if (fabs(rn - ro) < K_MNZL) { /* axial :524-604 */
+    double delta_z = 0., wj, lo, up;
+    double value_part = 2. * K_PI * rn * dr * dz;
+    double r1 = rn - 0.5 * dr, r2 = (i_n + 0.5) * dr, r3 = rn + 0.5 * dr;
+    if (i_n == 0)
+      lo = q / (dt * K_PI * dr * dr / 4.) * K_PI * (r2 * r2 - r1 * r1) / value_part;
+    else
+      lo = q / (dt * 2. * K_PI * i_n * dr * dr) * K_PI * (r2 * r2 - r1 * r1) / value_part;
+    up = q / (dt * 2 * K_PI * (i_n + 1) * dr * dr) * K_PI * (r3 * r3 - r2 * r2) / value_part;
+    if (!fixed) { /* :545-546 overwrite J_r at two nodes */
+      Jr[IDX(s, i_n, k_n)] = 0.;
+      Jr[IDX(s, i_n, k_n + 1)] = 0.;
+    }
+    switch (k_n - k_o) {
+      case 0:
+        delta_z = zn - zo;
+        wj = lo * delta_z; Jz[IDX(s, i_n, k_n)] += wj;
+        wj = up * delta_z; Jz[IDX(s, i_n + 1, k_n)] += wj;
+        break;
+      case 1:
+        delta_z = k_n * dz - zo;
+        wj = lo * delta_z; Jz[IDX(s, i_n, k_n - 1)] += wj;
+        wj = up * delta_z; Jz[IDX(s, i_n + 1, k_n - 1)] += wj;
+        delta_z = zn - k_n * dz;
+        wj = lo * delta_z; Jz[IDX(s, i_n, k_n)] += wj;
+        wj = up * delta_z; Jz[IDX(s, i_n + 1, k_n)] += wj;
+        break;
+      case -1:
+        delta_z = (k_n + 1) * dz - zo;
+        wj = lo * delta_z; Jz[IDX(s, i_n, k_n + 1)] += wj;
+        wj = up * delta_z; Jz[IDX(s, i_n + 1, k_n + 1)] += wj;
+        delta_z = zn - (k_n + 1) * dz;
+        wj = lo * delta_z; Jz[IDX(s, i_n, k_n)] += wj;
+        wj = up * delta_z; Jz[IDX(s, i_n + 1, k_n)] += wj;
+        break;
+      default: break;
+    }
+  } else if (fabs(zn - zo) < K_MNZL) { /* radial :607-728 */
+    double wj, delta_r, ldz, rdz, r0, sd;
+    switch (i_n - i_o) {
+      case 0:
+        delta_r = rn - ro;
+        ldz = (k_n + 1) * dz - zn;
+        rdz = zn - k_n * dz;
+        r0 = (i_n + 0.5) * dr;
+        sd = ssd_strict(q, r0, dr, dz, dt);
+        wj = sd * (delta_r - r0 * r0 / (ro + delta_r) + r0 * r0 / ro +
+                   dr * dr / (4. * (ro + delta_r)) - dr * dr / (4. * ro));
+        Jr[IDX(s, i_n, k_n)] += wj * ldz;
+        Jr[IDX(s, i_n, k_n + 1)] += wj * rdz;
+        break;
+      case 1:
+        delta_r = (i_n) * dr - ro;
+        ldz = (k_n + 1) * dz - zn;
+        rdz = zn - k_n * dz;
+        r0 = (i_n - 0.5) * dr;
+        sd = ssd_strict(q, r0, dr, dz, dt);
+        wj = sd * (delta_r - r0 * r0 / (ro + delta_r) + r0 * r0 / ro +
+                   dr * dr / (4. * (ro + delta_r)) - dr * dr / (4. * ro));
+        Jr[IDX(s, i_n - 1, k_n)] += wj * ldz;
+        Jr[IDX(s, i_n - 1, k_n + 1)] += wj * rdz;
+        delta_r = rn - i_n * dr;
+        r0 = (i_n + 0.5) * dr;
+        sd = ssd_strict(q, r0, dr, dz, dt);
+        if (fixed) /* (r0*r0)/(i_n*dr), where the reference has r0*r0/i_n*dr (:673) */
+          wj = sd * (delta_r - r0 * r0 / (i_n * dr + delta_r) + r0 * r0 / (i_n * dr) +
+                     dr * dr / (4. * (i_n * dr + delta_r)) - dr * dr / (4. * i_n * dr));
+        else
+          wj = sd * (delta_r - r0 * r0 / (i_n * dr + delta_r) + r0 * r0 / i_n * dr +
+                     dr * dr / (4. * (i_n * dr + delta_r)) - dr * dr / (4. * i_n * dr));
+        Jr[IDX(s, i_n, k_n)] += wj * ldz;
+        Jr[IDX(s, i_n, k_n + 1)] += wj * rdz;
+        break;
+      case -1:
+        delta_r = (i_n + 1) * dr - ro;
+        ldz = (k_n + 1) * dz - zn;
+        rdz = zn - k_n * dz;
+        r0 = (i_n + 1.5) * dr;
+        sd = ssd_strict(q, r0, dr, dz, dt);
+        wj = sd * (delta_r - r0 * r0 / (ro + delta_r) + r0 * r0 / ro +
+                   dr * dr / (4. * (ro + delta_r)) - dr * dr / (4. * ro));
+        Jr[IDX(s, i_n + 1, k_n)] += wj * ldz;
+        Jr[IDX(s, i_n + 1, k_n + 1)] += wj * rdz;
+        delta_r = rn - (i_n + 1) * dr;
+        r0 = (i_n + 0.5) * dr;
+        sd = ssd_strict(q, r0, dr, dz, dt);
+        if (fixed)
+          wj = sd * (delta_r - r0 * r0 / ((i_n + 1) * dr + delta_r) + r0 * r0 / ((i_n + 1) * dr) +
+                     dr * dr / (4. * ((i_n + 1) * dr + delta_r)) - dr * dr / (4. * (i_n + 1) * dr));
+        else
+          wj = sd * (delta_r - r0 * r0 / ((i_n + 1) * dr + delta_r) + r0 * r0 / (i_n + 1) * dr +
+                     dr * dr / (4. * ((i_n + 1) * dr + delta_r)) - dr * dr / (4. * (i_n + 1) * dr));
+        Jr[IDX(s, i_n, k_n)] += wj * ldz;
+        Jr[IDX(s, i_n, k_n + 1)] += wj * rdz;
+        break;
+      default: break;
+    }
+  }
+}
+
+/* azimuthal_current_distribution :398-498 for one particle. */
+static void vb_azimuthal_one(orc_sim* s, double q, double r, double z, double ro, double zo,
+                             double vphi, int r_i, int z_k) {
+  double *Jp = s->J[1];
+  double dr = s->dr, dz = s->dz;
+  double v_1 = cell_volume_expr(2.0 * r_i + 1, dr, dz);
+  double v_2 = cell_volume_expr(2.0 * r_i + 1 + 1, dr, dz);
+  double pos_r = (r + ro) / 2;
+  double pos_z = (z + zo) / 2;
+  /* both branches of :418-496 evaluate the same expressions */
+  double r1 = pos_r - 0.5 * dr, r2 = (r_i + 0.5) * dr, r3 = pos_r + 0.5 * dr;
+  double ro_v = q / (2. * K_PI * dz * dr * pos_r);
+  double dz1 = (z_k + 0.5) * dz - (pos_z - 0.5 * dz);
+  double dz2 = (pos_z + 0.5 * dz) - (z_k + 0.5) * dz;
+  double rho, wj;
+  rho = ro_v * K_PI * dz1 * (r2 * r2 - r1 * r1) / v_1; wj = rho * vphi; Jp[IDX(s, r_i, z_k)] += wj;
+  rho = ro_v * K_PI * dz1 * (r3 * r3 - r2 * r2) / v_2; wj = rho * vphi; Jp[IDX(s, r_i + 1, z_k)] += wj;
+  rho = ro_v * K_PI * dz2 * (r2 * r2 - r1 * r1) / v_1; wj = rho * vphi; Jp[IDX(s, r_i, z_k + 1)] += wj;
+  rho = ro_v * K_PI * dz2 * (r3 * r3 - r2 * r2) / v_2; wj = rho * vphi; Jp[IDX(s, r_i + 1, z_k + 1)] += wj;
+}
+
+/* rz_current_distribution :175-396 for one particle. */
+static void vb_rz_one(orc_sim* s, double q, double R, double Z, double RO, double ZO,
+                      long long cell_r, long long cell_z) {
+  double dr = s->dr, dz = s->dz;
+  int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  int i_n = (int)cell_r, k_n = (int)cell_z;
+  int i_o = CELL_NUMBER(RO, dr), k_o = CELL_NUMBER(ZO, dz);
+  if (RO == (i_o + 1) * dr) i_o = i_n;
+  if (ZO == (k_o + 1) * dz) k_o = k_n;
+  if (R == (i_n + 1) * dr) i_n = i_o;
+  if (Z == (k_n + 1) * dz) k_n = k_o;
+  int res_cell = abs(i_n - i_o) + abs(k_n - k_o);
+  int too_far = fixed ? (abs(i_n - i_o) > 1 || abs(k_n - k_o) > 1) : (abs(i_n - i_o) > 1);
+  if (too_far) {
+    ++s->errors; /* LOG_S(ERROR) :199-204 */
+    return;
+  }
+  if ((fabs(R - RO) < K_MNZL) || (fabs(Z - ZO) < K_MNZL)) {
+    vb_strict(s, R, Z, RO, ZO, q);
+    return;
+  }
+  if (res_cell == 0) {
+    vb_simple(s, R, Z, RO, ZO, i_n, k_n, q);
+  } else if (res_cell == 1) {
+    if ((i_n != i_o) && (k_n == k_o)) {
+      if (RO > (i_n + 1) * dr) {
+        double a = (RO - R) / (ZO - Z);
+        double r_b = (i_n + 1) * dr;
+        double delta_r = r_b - R;
+        double z_b = Z + delta_r / a;
+        vb_simple(s, r_b, z_b, RO, ZO, i_n + 1, k_n, q);
+        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+      } else {
+        double a = (R - RO) / (Z - ZO);
+        double r_b = (i_n) * dr;
+        double delta_r = r_b - RO;
+        double z_b = ZO + delta_r / a;
+        vb_simple(s, r_b, z_b, RO, ZO, i_n - 1, k_n, q);
+        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+      }
+    } else if ((i_n == i_o) && (k_n != k_o)) {
+      if (ZO < k_n * dz) {
+        double z_b = k_n * dz;
+        double delta_z = z_b - ZO;
+        double a = (R - RO) / (Z - ZO);
+        double r_b = RO + a * delta_z;
+        vb_simple(s, r_b, z_b, RO, ZO, i_n, k_n - 1, q);
+        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+      } else {
+        double z_b = (k_n + 1) * dz;
+        double delta_z = z_b - Z;
+        double a = (RO - R) / (ZO - Z);
+        double r_b = R + a * delta_z;
+        vb_simple(s, r_b, z_b, RO, ZO, i_n, k_n + 1, q);
+        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+      }
+    }
+  } else if (res_cell == 2) {
+    if (i_o < i_n) {
+      if (k_o < k_n) {
+        double a = (R - RO) / (Z - ZO);
+        double r1 = i_n * dr;
+        double delta_z1 = (r1 - RO) / a;
+        double z1 = ZO + delta_z1;
+        double z2 = k_n * dz;
+        double delta_r2 = (z2 - ZO) * a;
+        double r2 = RO + delta_r2;
+        if (z1 < k_n * dz) {
+          vb_simple(s, r1, z1, RO, ZO, i_n - 1, k_n - 1, q);
+          vb_simple(s, r2, z2, r1, z1, i_n, k_n - 1, q);
+          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+        } else if (z1 > k_n * dz) {
+          vb_simple(s, r2, z2, RO, ZO, i_n - 1, k_n - 1, q);
+          vb_simple(s, r1, z1, r2, z2, i_n - 1, k_n, q);
+          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+        }
+      } else {
+        double a = (R - RO) / (Z - ZO);
+        double r1 = i_n * dr;
+        double delta_z1 = (r1 - RO) / a;
+        double z1 = ZO + delta_z1;
+        double z2 = (k_n + 1) * dz;
+        double delta_r2 = -(ZO - z2) * a;
+        double r2 = RO + delta_r2;
+        if (z1 > (k_n + 1) * dz) {
+          vb_simple(s, r1, z1, RO, ZO, i_n - 1, k_n + 1, q);
+          vb_simple(s, r2, z2, r1, z1, i_n, k_n + 1, q);
+          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+        } else if (z1 < (k_n + 1) * dz) {
+          vb_simple(s, r2, z2, RO, ZO, i_n - 1, k_n + 1, q);
+          vb_simple(s, r1, z1, r2, z2, i_n - 1, k_n, q);
+          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+        }
+      }
+    } else if (i_o > i_n) {
+      if (k_o < k_n) {
+        double a = (R - RO) / (Z - ZO);
+        double r1 = (i_n + 1) * dr;
+        double delta_z1 = -(RO - r1) / a;
+        double z1 = ZO + delta_z1;
+        double z2 = k_n * dz;
+        double delta_r2 = -(z2 - ZO) * a;
+        double r2 = RO - delta_r2;
+        if (z1 < (k_n) * dz) {
+          vb_simple(s, r1, z1, RO, ZO, i_n + 1, k_n - 1, q);
+          vb_simple(s, r2, z2, r1, z1, i_n, k_n - 1, q);
+          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+        } else if (z1 > (k_n) * dz) {
+          vb_simple(s, r2, z2, RO, ZO, i_n + 1, k_n - 1, q);
+          vb_simple(s, r1, z1, r2, z2, i_n + 1, k_n, q);
+          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+        }
+      } else if (k_o > k_n) {
+        double a = (RO - R) / (ZO - Z);
+        double r1 = (i_n + 1) * dr;
+        double delta_z1 = (r1 - R) / a;
+        double z1 = Z + delta_z1;
+        double z2 = (k_n + 1) * dz;
+        double delta_r2 = (z2 - Z) * a;
+        double r2 = R + delta_r2;
+        if (z1 > (k_n + 1) * dz) {
+          vb_simple(s, r1, z1, RO, ZO, i_n + 1, k_n + 1, q);
+          vb_simple(s, r2, z2, r1, z1, i_n, k_n + 1, q);
+          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+        } else if (z1 < (k_n + 1) * dz) {
+          vb_simple(s, r2, z2, RO, ZO, i_n + 1, k_n + 1, q);
+          vb_simple(s, r1, z1, r2, z2, i_n + 1, k_n, q);
+          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+        }
+      }
+    }
+  }
+}
+
+static void current_vb(orc_sim* s) { /* current_distribution :731-735 */
+  for (int c = 0; c < 3; ++c) halo_set(s, s->J[c], 0.0);
+  for (int t = 0; t < s->nsp; ++t) {
+    species_t* p = &s->sp[t];
+    for (size_t j = 0; j < p->n; ++j)
+      vb_azimuthal_one(s, p->charge * p->w[j], p->r[j], p->z[j], p->r_old[j], p->z_old[j],
+                       p->vphi[j], (int)p->cell_r[j], (int)p->cell_z[j]);
+  }
+  for (int c = 0; c < 3; ++c) halo_set(s, s->J[c], 0.0);
+  for (int t = 0; t < s->nsp; ++t) {
+    species_t* p = &s->sp[t];
+    for (size_t j = 0; j < p->n; ++j)
+      vb_rz_one(s, p->charge * p->w[j], p->r[j], p->z[j], p->r_old[j], p->z_old[j],
+                p->cell_r[j], p->cell_z[j]);
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* ZigZag current (currentZigZag.cpp:22-136, RELAY_POINT currentZigZag.hpp:28-30) */
+
+static inline double dmin(double a, double b) { return (b < a) ? b : a; } /* std::min */
+static inline double dmax(double a, double b) { return (a < b) ? b : a; } /* std::max */
+static inline double relay(int i1, int i2, double x1, double x2, double dx) {
+  return dmin(dmin(i1 * dx, i2 * dx) + dx, dmax(dmax(i1 * dx, i2 * dx), (x1 + x2) / 2.));
+}
+
+static void current_zigzag(orc_sim* s) {
+  for (int c = 0; c < 3; ++c) halo_set(s, s->J[c], 0.0);
+  double *Jr = s->J[0], *Jp = s->J[1], *Jz = s->J[2];
+  double dr = s->dr, dz = s->dz, dt = s->dt;
+  for (int t = 0; t < s->nsp; ++t) {
+    species_t* p = &s->sp[t];
+    for (size_t j = 0; j < p->n; ++j) {
+      double ro = p->r_old[j], zo = p->z_old[j], rn = p->r[j], zn = p->z[j];
+      double cod = p->charge * p->w[j] / dt;
+      int i_n = CELL_NUMBER(rn, dr), i_o = CELL_NUMBER(ro, dr);
+      int k_n = CELL_NUMBER(zn, dz), k_o = CELL_NUMBER(zo, dz);
+      int i_mid = CELL_NUMBER((rn + ro) / 2., dr);
+      double oov = 1 / (cell_volume_expr(2.0 * i_mid + 1, dr, dz));
+      double F_phi = p->charge * p->w[j] * p->vphi[j];
+      double W_phi = p->vphi[j] * dt / (2. * K_PI * (ro + rn));
+      double rr = relay(i_o, i_n, ro, rn, dr), zr = relay(k_o, k_n, zo, zn, dz);
+      double F_r1 = cod * (rr - ro), F_r2 = cod * (rn - rr);
+      double F_z1 = cod * (zr - zo), F_z2 = cod * (zn - zr);
+      double W_r1 = (ro + rr) / 2 - i_o * dr, W_r2 = (rn + rr) / 2 - i_n * dr;
+      double W_z1 = (zo + zr) / 2 - k_o * dz, W_z2 = (zn + zr) / 2 - k_n * dz;
+      double mWr1 = 1 - W_r1, mWr2 = 1 - W_r2, mWz1 = 1 - W_z1, mWz2 = 1 - W_z2, mWp = 1 - W_phi;
+      double Jr_a = oov * F_r1 * mWp * mWz1, Jr_b = oov * F_r2 * mWp * mWz2;
+      double Jr_c = oov * F_r1 * W_phi * mWz1, Jr_d = oov * F_r2 * W_phi * mWz2;
+      double Jr_e = oov * F_r1 * mWp * W_z1, Jr_f = oov * F_r2 * mWp * W_z2;
+      double Jr_g = oov * F_r1 * W_phi * W_z1, Jr_h = oov * F_r2 * W_phi * W_z2;
+      double Jp_a = oov * F_phi * mWr2 * mWz2, Jp_b = oov * F_phi * mWr2 * W_z1;
+      double Jp_c = oov * F_phi * W_r2 * mWz2, Jp_d = oov * F_phi * W_r2 * W_z2;
+      double Jz_a = oov * F_z1 * mWr1 * mWp, Jz_b = oov * F_z2 * mWr2 * mWp;
+      double Jz_c = oov * F_z1 * mWr1 * W_phi, Jz_d = oov * F_z2 * mWr2 * W_phi;
+      double Jz_e = oov * F_z1 * W_r1 * mWp, Jz_f = oov * F_z2 * W_r2 * mWp;
+      double Jz_g = oov * F_z1 * W_r1 * W_phi, Jz_h = oov * F_z2 * W_r2 * W_phi;
+      Jr[IDX(s, i_o, k_o)] += Jr_a + Jr_c;
+      Jr[IDX(s, i_o, k_o + 1)] += Jr_e + Jr_g;
+      Jr[IDX(s, i_n, k_n)] += Jr_b + Jr_d;
+      Jr[IDX(s, i_n, k_n + 1)] += Jr_f + Jr_h;
+      Jp[IDX(s, i_n, k_n)] += Jp_a;
+      Jp[IDX(s, i_n, k_n + 1)] += Jp_b;
+      Jp[IDX(s, i_n + 1, k_n)] += Jp_c;
+      Jp[IDX(s, i_n + 1, k_n + 1)] += Jp_d;
+      Jz[IDX(s, i_o, k_o)] += Jz_a + Jz_c;
+      Jz[IDX(s, i_o + 1, k_o)] += Jz_e + Jz_g;
+      Jz[IDX(s, i_n, k_n)] += Jz_b + Jz_d;
+      Jz[IDX(s, i_n + 1, k_n)] += Jz_f + Jz_h;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Beam injection: BeamP::inject (beamP.cpp:71-157)                      */
+
+static int grow(species_t* p, size_t need) {
+  if (need <= p->cap) return ST_OK;
+  size_t cap = p->cap ? p->cap : 64;
+  while (cap < need) cap *= 2;
+  double** arrs[] = {&p->r, &p->phi, &p->z, &p->r_old, &p->phi_old, &p->z_old,
+                     &p->vr, &p->vphi, &p->vz, &p->w, &p->sn};
+  for (size_t a = 0; a < sizeof(arrs) / sizeof(arrs[0]); ++a) {
+    double* q = (double*)realloc(*arrs[a], cap * sizeof(double));
+    if (!q) return ST_ARG;
+    memset(q + p->cap, 0, (cap - p->cap) * sizeof(double));
+    *arrs[a] = q;
+  }
+  long long* cr = (long long*)realloc(p->cell_r, cap * sizeof(long long));
+  if (!cr) return ST_ARG;
+  p->cell_r = cr;
+  long long* cz = (long long*)realloc(p->cell_z, cap * sizeof(long long));
+  if (!cz) return ST_ARG;
+  p->cell_z = cz;
+  p->cap = cap;
+  return ST_OK;
+}
+
+static double draw(orc_sim* s, int slot, uint32_t idx, int which) {
+  if (s->rng_kind == ORC_RNG_PHILOX)
+    return orc_philox_uniform(s->seed, 0x6265616du + (uint32_t)slot, s->step_index, idx, which);
+  return mt_uniform(&s->mt);
+}
+
+static int stage_inject(orc_sim* s, int slot) {
+  species_t* p = &s->sp[slot];
+  if (!p->is_beam) return ST_OK; /* SpecieP::inject is empty (specieP.cpp:480) */
+  double t = s->t;
+  if (p->current_bunch < p->bunches_amount) {
+    double bunch_start = p->start_time + (p->bunch_length + p->bunches_distance) / p->velocity * p->current_bunch;
+    double bunch_finish = bunch_start + p->bunch_length / p->velocity;
+    if (0.0 * s->dr < p->radius && t >= bunch_start && t < bunch_finish) {
+      double dr = s->dr, dz = s->dz;
+      double dl = p->velocity * s->dt;
+      double half_z = dz / 2.;
+      double v_macro_avg = K_PI * p->radius * dr * dz;
+      double N_total = K_PI * p->radius * p->radius * p->bunch_length * p->bunches_amount * p->density;
+      double n_per_macro_avg = N_total / p->macro_amount;
+      for (unsigned i = 0; i < p->macro_per_step; ++i) {
+        double rand_r = draw(s, slot, i, 0);
+        double rand_z = draw(s, slot, i, 1);
+        double pos_r = p->domain_radius * rand_r + dr / 2 + 0.0 * dr;
+        if (grow(p, p->n + 1) != ST_OK) return ST_ARG;
+        size_t j = p->n++;
+        p->r[j] = pos_r; p->phi[j] = 0; p->z[j] = dl * rand_z + half_z;
+        p->vr[j] = 0; p->vphi[j] = 0; p->vz[j] = p->velocity;
+        p->r_old[j] = p->phi_old[j] = p->z_old[j] = 0; p->sn[j] = 0;
+        double norm;
+        if (pos_r > dr / 2)
+          norm = 2 * K_PI * pos_r * dr * dz / v_macro_avg;
+        else
+          norm = K_PI * (pos_r * pos_r + pos_r * dr + dr * dr / 4.) * dz / v_macro_avg;
+        p->w[j] = n_per_macro_avg * norm;
+        p->cell_r[j] = CELL_NUMBER(p->r[j], dr);
+        p->cell_z[j] = CELL_NUMBER(p->r[j], dz); /* :137 binds z from pos_r */
+      }
+    }
+    if (t > bunch_finish) ++p->current_bunch;
+  }
+  return ST_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* API                                                                   */
+
+orc_sim* orc_create(int nr, int nz, double radius, double longitude, double dt, double t_start,
+                    const int* pml_size, const double* pml_sigma, int pusher, int current,
+                    int quirks) {
+  if (nr < 2 || nz < 2) return NULL;
+  orc_sim* s = (orc_sim*)calloc(1, sizeof(orc_sim));
+  s->nr = nr; s->nz = nz; s->ld = nz + 4;
+  s->R = radius; s->L = longitude;
+  s->dr = radius / nr; s->dz = longitude / nz; /* Geometry ctor geometry.hpp:67-68 */
+  s->gcr = (size_t)(radius / s->dr);          /* geometry.hpp:70-71 */
+  s->gcz = (size_t)(longitude / s->dz);
+  s->dt = dt; s->t = t_start;
+  for (int i = 0; i < 4; ++i) s->pml[i] = pml_size ? pml_size[i] : 0;
+  s->pml_sigma[0] = pml_sigma ? pml_sigma[0] : 0; s->pml_sigma[1] = pml_sigma ? pml_sigma[1] : 0;
+  s->pusher = pusher; s->current = current; s->quirks = quirks;
+  size_t ng = (size_t)(nr + 4) * (size_t)(nz + 4);
+  for (int c = 0; c < 3; ++c) {
+    s->E[c] = (double*)calloc(ng, sizeof(double));
+    s->H[c] = (double*)calloc(ng, sizeof(double));
+    s->Hat[c] = (double*)calloc(ng, sizeof(double));
+    s->J[c] = (double*)calloc(ng, sizeof(double));
+  }
+  s->sigma = (double*)calloc(ng, sizeof(double));
+  set_pml(s);
+  mt_seed(&s->mt, 5489u);
+  s->rng_kind = ORC_RNG_MT19937;
+  return s;
+}
+
+static int add_common(orc_sim* s, int id, const char* name, double charge_e, double mass_e) {
+  if (s->nsp >= MAX_SPECIES) return ST_ARG;
+  species_t* p = &s->sp[s->nsp];
+  memset(p, 0, sizeof(*p));
+  p->id = id;
+  strncpy(p->name, name ? name : "", sizeof(p->name) - 1);
+  p->charge = charge_e * K_EL_CHARGE;
+  p->mass = mass_e * K_EL_MASS;
+  return s->nsp++;
+}
+
+int orc_add_species(orc_sim* s, int id, const char* name, double charge_e, double mass_e) {
+  return add_common(s, id, name, charge_e, mass_e);
+}
+
+int orc_add_beam(orc_sim* s, int id, const char* name, double charge_e, double mass_e,
+                 unsigned macro_amount, double start_time, double b_radius, double density,
+                 double amount, double length, double distance, double velocity) {
+  int slot = add_common(s, id, name, charge_e, mass_e);
+  if (slot < 0) return slot;
+  species_t* p = &s->sp[slot];
+  p->is_beam = 1;
+  p->macro_amount = macro_amount; /* BeamP ctor beamP.cpp:22-69 */
+  p->radius = b_radius; p->density = density; p->velocity = velocity;
+  p->start_time = start_time; p->bunches_amount = (unsigned)amount;
+  p->bunch_length = length; p->bunches_distance = distance;
+  p->finish_time = p->start_time + p->bunch_length / p->velocity * p->bunches_amount +
+                   p->bunches_distance / p->velocity * (p->bunches_amount - 1);
+  if (b_radius > (double)s->nr * s->dr) p->domain_radius = s->R;
+  else if (b_radius > 0.0 * s->dr) p->domain_radius = b_radius - 0.0 * s->dr;
+  else p->domain_radius = 0;
+  double macro_normalizer = p->domain_radius / p->radius;
+  p->bunch_macro_amount = (double)(p->macro_amount / p->bunches_amount) * macro_normalizer;
+  p->macro_per_step = p->bunch_macro_amount * p->velocity * s->dt / p->bunch_length;
+  return slot;
+}
+
+void orc_set_rng(orc_sim* s, int kind, uint64_t seed) {
+  s->rng_kind = kind;
+  s->seed = seed;
+  if (kind == ORC_RNG_MT19937) mt_seed(&s->mt, (uint32_t)seed);
+}
+
+int orc_set_particles(orc_sim* s, int sid, size_t n, const double* r, const double* z,
+                      const double* vr, const double* vphi, const double* vz, const double* w) {
+  if (sid < 0 || sid >= s->nsp) return ST_ARG;
+  species_t* p = &s->sp[sid];
+  if (grow(p, n) != ST_OK) return ST_ARG;
+  p->n = n;
+  for (size_t j = 0; j < n; ++j) {
+    p->r[j] = r[j]; p->z[j] = z[j]; p->phi[j] = 0;
+    p->vr[j] = vr[j]; p->vphi[j] = vphi[j]; p->vz[j] = vz[j]; p->w[j] = w[j];
+    p->r_old[j] = p->phi_old[j] = p->z_old[j] = 0; p->sn[j] = 0;
+    p->cell_r[j] = CELL_NUMBER(r[j], s->dr);
+    p->cell_z[j] = CELL_NUMBER(z[j], s->dz);
+  }
+  return ST_OK;
+}
+
+long orc_count(orc_sim* s, int sid) {
+  if (sid < 0 || sid >= s->nsp) return -1;
+  return (long)s->sp[sid].n;
+}
+
+int orc_get_particles(orc_sim* s, int sid, size_t cap, double* r, double* z, double* vr,
+                      double* vphi, double* vz, double* w, double* r_old, double* z_old,
+                      long long* cell_r, long long* cell_z) {
+  if (sid < 0 || sid >= s->nsp) return ST_ARG;
+  species_t* p = &s->sp[sid];
+  if (cap < p->n) return -4;
+  for (size_t j = 0; j < p->n; ++j) {
+    r[j] = p->r[j]; z[j] = p->z[j]; vr[j] = p->vr[j]; vphi[j] = p->vphi[j]; vz[j] = p->vz[j];
+    w[j] = p->w[j];
+    if (r_old) r_old[j] = p->r_old[j];
+    if (z_old) z_old[j] = p->z_old[j];
+    if (cell_r) cell_r[j] = p->cell_r[j];
+    if (cell_z) cell_z[j] = p->cell_z[j];
+  }
+  return ST_OK;
+}
+
+static double* field_ptr(orc_sim* s, int which) {
+  if (which >= 0 && which < 3) return s->E[which];
+  if (which >= 3 && which < 6) return s->H[which - 3];
+  if (which >= 6 && which < 9) return s->Hat[which - 6];
+  if (which >= 9 && which < 12) return s->J[which - 9];
+  if (which == 12) return s->sigma;
+  return NULL;
+}
+
+int orc_set_field(orc_sim* s, int which, const double* src) {
+  double* a = field_ptr(s, which);
+  if (!a || which == 12) return ST_ARG;
+  memcpy(a, src, sizeof(double) * (size_t)(s->nr + 4) * (size_t)(s->nz + 4));
+  return ST_OK;
+}
+
+int orc_get_field(orc_sim* s, int which, double* dst) {
+  double* a = field_ptr(s, which);
+  if (!a) return ST_ARG;
+  memcpy(dst, a, sizeof(double) * (size_t)(s->nr + 4) * (size_t)(s->nz + 4));
+  return ST_OK;
+}
+
+int orc_stage(orc_sim* s, int stage) {
+  int st = ST_OK;
+  switch (stage) {
+    case ORC_STAGE_INJECT:
+      for (int t = 0; t < s->nsp && st == ST_OK; ++t) st = stage_inject(s, t);
+      return st;
+    case ORC_STAGE_FIELD_E: return field_e(s);
+    case ORC_STAGE_FIELD_H: return field_h(s);
+    case ORC_STAGE_PUSH:
+      for (int t = 0; t < s->nsp; ++t) {
+        species_t* p = &s->sp[t];
+        for (size_t j = 0; j < p->n; ++j) {
+          double pr = p->r[j], pz = p->z[j], e[3], b[3];
+          double v[3] = {p->vr[j], p->vphi[j], p->vz[j]};
+          if (isnan(pr) || isinf(pr) || isnan(pz) || isinf(pz)) return ST_FATAL; /* :51-57 */
+          gather_e(s, pr, pz, e);
+          gather_h(s, pr, pz, b);
+          int fixed = s->quirks == ORC_QUIRKS_FIXED;
+          if (s->pusher == ORC_PUSHER_VAY) st = push_vay(fixed, p->charge, p->mass, s->dt, e, b, v);
+          else if (s->pusher == ORC_PUSHER_HC) st = push_hc(fixed, p->charge, p->mass, s->dt, e, b, v);
+          else st = push_boris(s->pusher, p->charge, p->mass, s->dt, e, b, v);
+          if (st != ST_OK) return st;
+          p->vr[j] = v[0]; p->vphi[j] = v[1]; p->vz[j] = v[2];
+        }
+      }
+      return ST_OK;
+    case ORC_STAGE_DUMP_OLD:
+      for (int t = 0; t < s->nsp; ++t) stage_dump_old(&s->sp[t]);
+      return ST_OK;
+    case ORC_STAGE_MOVE:
+      for (int t = 0; t < s->nsp; ++t) stage_move(&s->sp[t], s->dt);
+      return ST_OK;
+    case ORC_STAGE_POS_RZ:
+      for (int t = 0; t < s->nsp; ++t) stage_pos_rz(&s->sp[t]);
+      return ST_OK;
+    case ORC_STAGE_REFLECT:
+      for (int t = 0; t < s->nsp && st == ST_OK; ++t) st = stage_reflect(s, &s->sp[t]);
+      return st;
+    case ORC_STAGE_VEL_RZ:
+      for (int t = 0; t < s->nsp; ++t) stage_vel_rz(&s->sp[t]);
+      return ST_OK;
+    case ORC_STAGE_BIND:
+      for (int t = 0; t < s->nsp; ++t) stage_bind(&s->sp[t], s->dr, s->dz);
+      return ST_OK;
+    case ORC_STAGE_COLLECT:
+      for (int t = 0; t < s->nsp; ++t) stage_collect(s, &s->sp[t]);
+      return ST_OK;
+    case ORC_STAGE_RESET_CURRENT: { /* Domain::reset_current domain.cpp:135-139 */
+      size_t ng = (size_t)(s->nr + 4) * (size_t)(s->nz + 4);
+      for (int c = 0; c < 3; ++c) memset(s->J[c], 0, ng * sizeof(double));
+      return ST_OK;
+    }
+    case ORC_STAGE_CURRENT:
+      if (s->current == ORC_CURRENT_ZIGZAG) current_zigzag(s);
+      else current_vb(s);
+      return ST_OK;
+    case ORC_STAGE_ADVANCE_TIME:
+      s->t += s->dt;
+      s->step_index += 1;
+      return ST_OK;
+    default: return ST_ARG;
+  }
+}
+
+int orc_step(orc_sim* s, int nsteps) {
+  for (int n = 0; n < nsteps; ++n)
+    for (int st = 0; st < ORC_STAGE_COUNT; ++st) {
+      int rc = orc_stage(s, st);
+      if (rc != ST_OK) return rc;
+    }
+  return ST_OK;
+}
+
+double orc_time(orc_sim* s) { return s->t; }
+long orc_removed(orc_sim* s) { return s->removed; }
+long orc_error_count(orc_sim* s) { return s->errors; }
+
+void orc_destroy(orc_sim* s) {
+  if (!s) return;
+  for (int c = 0; c < 3; ++c) {
+    free(s->E[c]); free(s->H[c]); free(s->Hat[c]); free(s->J[c]);
+  }
+  free(s->sigma);
+  for (int t = 0; t < s->nsp; ++t) {
+    species_t* p = &s->sp[t];
+    free(p->r); free(p->phi); free(p->z); free(p->r_old); free(p->phi_old); free(p->z_old);
+    free(p->vr); free(p->vphi); free(p->vz); free(p->w); free(p->sn);
+    free(p->cell_r); free(p->cell_z);
+  }
+  free(s);
+}

@@ -1,0 +1,71 @@
+"""The CPU oracle against the reference's own sources, stage by stage.
+
+oracle/Makefile.ref compiles the unmodified reference hot path into
+oracle/_ref/; these tests run the same seeded inputs through both and demand
+bit-identical fields, particles, cell indices and status codes after every
+stage of the reference step order (PiCoPiC.cpp:326-347, SMB.cpp:1231-1306).
+"""
+import numpy as np
+import pytest
+
+from oracle.harness import FIELDS, STAGES, OracleSim, RefSim, reference_available
+from tests.cases import ELECTRONS, IONS, beam_spec, load, small_grid
+
+COMBOS = [(p, c) for p in ("borisrel", "boris", "vay", "hc") for c in ("vb", "zigzag")]
+
+
+def _assert_same(o, r, nsp, where):
+    fo, fr = o.fields(), r.fields()
+    for k in FIELDS:
+        np.testing.assert_array_equal(fo[k], fr[k], err_msg=f"{where}: field {k}")
+    for sid in range(nsp):
+        po, pr = o.get_particles(sid), r.get_particles(sid)
+        for k in po:
+            np.testing.assert_array_equal(po[k], pr[k], err_msg=f"{where}: species {sid} {k}")
+
+
+@pytest.mark.parametrize("pusher,current", COMBOS)
+def test_stagewise_bit_exact(pusher, current):
+    if not reference_available(pusher, current):
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    grid = small_grid()
+    species = [ELECTRONS, IONS, beam_spec(grid)]
+    o, r = OracleSim(grid, pusher, current), RefSim(grid, pusher, current)
+    load(o, grid, species, 2000, seed=11)
+    load(r, grid, species, 2000, seed=11)
+    o.set_rng("mt19937", 42)
+    r.seed(42)
+    for step in range(3):
+        for st in STAGES:
+            assert o.stage(st) == r.stage(st) == 0, st
+            if step == 0:
+                _assert_same(o, r, len(species), f"step {step} after {st}")
+        _assert_same(o, r, len(species), f"after step {step}")
+    assert o.count(2) > 0, "beam was injected"
+    assert o.errors == r.errors
+
+
+def test_fatal_nan_position():
+    """A NaN position is FATAL in the pusher (pusherBoris.cpp:51-57).
+
+    The reference aborts there (and reads out of bounds if it went on), so
+    only the oracle's error status is checked.
+    """
+    grid = small_grid(pml=False)
+    o = OracleSim(grid)
+    o.add(ELECTRONS)
+    o.set_particles(0, [np.nan, 5e-4], [5e-4, 5e-4], [0, 0], [0, 0], [0, 0], [1, 1])
+    assert o.stage("push") == -10
+
+
+def test_long_run_removal_and_reflection():
+    """20 full steps with fast particles: reflections and removals agree."""
+    if not reference_available():
+        pytest.skip("compiled reference not built")
+    grid = small_grid(nr=16, nz=32)
+    species = [ELECTRONS, IONS]
+    o, r = OracleSim(grid), RefSim(grid)
+    load(o, grid, species, 3000, seed=5)
+    load(r, grid, species, 3000, seed=5)
+    assert o.step(20) == r.step(20) == 0
+    _assert_same(o, r, 2, "after 20 steps")
