@@ -1,0 +1,195 @@
+/*
+ * pcg.h — C ABI of the B200-native PiCoPiC per-timestep PIC loop.
+ *
+ * One handle = one simulation domain (the whole r-z grid on one GPU) with
+ * its particle species and beams, owning its device memory and one CUDA
+ * stream.  A handle is not thread-safe; use one host thread per handle.
+ *
+ * The entry points replace the per-domain façade that the reference's
+ * scheduler (SMB) drives every step.  Reference interfaces (file:line in
+ * the PiCoPiC sources):
+ *
+ *   pcg_create            Domain::Domain                 src/domain.cpp:26-84
+ *                         (Geometry from Cfg::init_geometry src/cfg.cpp:379-429,
+ *                          TimeSim from Cfg::init_time     src/cfg.cpp:430-440)
+ *   pcg_add_species       SpecieP::SpecieP               src/specieP.cpp:23-70
+ *   pcg_add_beam          BeamP::BeamP                   src/beamP.cpp:22-69
+ *   pcg_import_species    SpecieP::particles (vector<Particle*>)
+ *                                                        include/specieP.hpp:74-163
+ *   pcg_export_species    same, read back
+ *   pcg_set_field /       MaxwellSolver::field_e, field_h include/maxwellSolver.hpp:39-40,
+ *   pcg_export_field      MaxwellSolverYee::field_h_at_et include/maxwellSolver/maxwellSolverYee.hpp:29,
+ *                         Current::current                include/current.hpp:41
+ *                         (Grid<double> with a 2-cell halo include/algo/grid.hpp:25-58)
+ *   pcg_stage             one Domain method:
+ *                           PCG_STAGE_INJECT        Domain::manage_beam        src/domain.cpp:180-186
+ *                           PCG_STAGE_FIELD_E       Domain::weight_field_e     src/domain.cpp:123-126
+ *                           PCG_STAGE_FIELD_H       Domain::weight_field_h     src/domain.cpp:118-121
+ *                           PCG_STAGE_PUSH          Domain::push_particles     src/domain.cpp:141-144
+ *                           PCG_STAGE_DUMP_OLD      Domain::dump_particle_positions_to_old src/domain.cpp:193-197
+ *                           PCG_STAGE_MOVE          Domain::update_particles_coords src/domain.cpp:146-151
+ *                           PCG_STAGE_POS_RZ        Domain::particles_back_position_to_rz src/domain.cpp:168-172
+ *                           PCG_STAGE_REFLECT       Domain::reflect            src/domain.cpp:160-165
+ *                           PCG_STAGE_VEL_RZ        Domain::particles_back_velocity_to_rz src/domain.cpp:174-178
+ *                           PCG_STAGE_BIND          Domain::bind_cell_numbers  src/domain.cpp:153-158
+ *                           PCG_STAGE_COLLECT       SMB::particles_runaway_collector src/SMB.cpp:194-349
+ *                           PCG_STAGE_RESET_CURRENT Domain::reset_current      src/domain.cpp:135-139
+ *                           PCG_STAGE_CURRENT       Domain::weight_current     src/domain.cpp:188-191
+ *                           PCG_STAGE_ADVANCE_TIME  main loop time += step     src/PiCoPiC.cpp:347
+ *   pcg_step              one full step in the order of src/PiCoPiC.cpp:326-347 and
+ *                         SMB::inject_beam/solve_maxvell/advance_particles/solve_current
+ *                         src/SMB.cpp:1231-1322, as fused device kernels.
+ *
+ * Errors: every call returns a status (PCG_OK = 0, negative on error).  The
+ * reference aborts on LOG_S(FATAL) (NaN positions pusherBoris.cpp:51-57,
+ * NaN fields maxwellSolverYee.cpp:253-255, v > c rel.cpp:33-34); here the
+ * device raises an error word and the call returns PCG_ERR_NAN or
+ * PCG_ERR_SUPERLUMINAL.  The reference's LOG_S(ERROR) on a particle moving
+ * more than one cell (currentVB.cpp:199-204) skips that particle's current,
+ * as in the reference, and is counted in pcg_diagnostics.move_errors.
+ *
+ * Layout conventions of the host arrays: fields are (nr+4) x (nz+4) doubles,
+ * row i (radius) major, z contiguous, node (i, k) at [(i+2)*(nz+4) + k+2],
+ * as Grid<double> stores them.  Particle arrays are structure-of-arrays of
+ * doubles in SI units (m, m/s, real particles per macroparticle).
+ */
+#ifndef PCG_H
+#define PCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCG_ABI_VERSION 1
+
+/* status codes */
+#define PCG_OK 0
+#define PCG_ERR_ARG (-1)
+#define PCG_ERR_CUDA (-2)
+#define PCG_ERR_NOMEM (-3)
+#define PCG_ERR_STATE (-4)
+#define PCG_ERR_CAPACITY (-5)
+#define PCG_ERR_NAN (-10)
+#define PCG_ERR_SUPERLUMINAL (-11)
+#define PCG_ERR_TIMEOUT (-12)
+#define PCG_ERR_UNSUPPORTED (-13)
+
+/* pusher switch (configure.ac:96-98, 226-239) */
+#define PCG_PUSHER_BORIS 0
+#define PCG_PUSHER_BORIS_ADAPTIVE 1
+#define PCG_PUSHER_BORIS_RELATIVISTIC 2
+#define PCG_PUSHER_VAY 3
+#define PCG_PUSHER_HC 4
+
+/* charge-conserving current scheme (configure.ac:108-110, 268-275) */
+#define PCG_CURRENT_VB 0
+#define PCG_CURRENT_ZIGZAG 1
+
+/* arithmetic of the particle path */
+#define PCG_PRECISION_F64 0 /* positions in double, the reference arithmetic */
+#define PCG_PRECISION_F32 1 /* int32 cell + float offset, float fields */
+
+/* PCG_QUIRKS_REFERENCE reproduces the reference's arithmetic defects;
+ * PCG_QUIRKS_FIXED corrects them where a correction is defined. */
+#define PCG_QUIRKS_REFERENCE 0
+#define PCG_QUIRKS_FIXED 1
+
+/* stages, numbered as the oracle's */
+#define PCG_STAGE_INJECT 0
+#define PCG_STAGE_FIELD_E 1
+#define PCG_STAGE_FIELD_H 2
+#define PCG_STAGE_PUSH 3
+#define PCG_STAGE_DUMP_OLD 4
+#define PCG_STAGE_MOVE 5
+#define PCG_STAGE_POS_RZ 6
+#define PCG_STAGE_REFLECT 7
+#define PCG_STAGE_VEL_RZ 8
+#define PCG_STAGE_BIND 9
+#define PCG_STAGE_COLLECT 10
+#define PCG_STAGE_RESET_CURRENT 11
+#define PCG_STAGE_CURRENT 12
+#define PCG_STAGE_ADVANCE_TIME 13
+
+/* field slots */
+#define PCG_FIELD_E_R 0
+#define PCG_FIELD_E_PHI 1
+#define PCG_FIELD_E_Z 2
+#define PCG_FIELD_H_R 3
+#define PCG_FIELD_H_PHI 4
+#define PCG_FIELD_H_Z 5
+#define PCG_FIELD_HAT_R 6 /* field_h_at_et */
+#define PCG_FIELD_HAT_PHI 7
+#define PCG_FIELD_HAT_Z 8
+#define PCG_FIELD_J_R 9
+#define PCG_FIELD_J_PHI 10
+#define PCG_FIELD_J_Z 11
+
+typedef struct pcg_handle pcg_handle;
+
+typedef struct pcg_config {
+  int nr, nz;                /* grid cells in r and z */
+  double radius, longitude;  /* domain size, m (dr = radius/nr, dz = longitude/nz) */
+  double dt, t_start;        /* time step and start time, s */
+  int pml_size[4];           /* PML cells on the walls r=0 (unused), z=0, r=R, z=L */
+  double pml_sigma[2];       /* PML sigma_1, sigma_2 */
+  int pusher, current, precision, quirks;
+  int device;                /* CUDA device ordinal */
+  uint64_t seed;             /* beam-injection random stream (Philox4x32-10) */
+} pcg_config;
+
+typedef struct pcg_diagnostics {
+  double time;                  /* simulation time, s */
+  uint64_t steps;               /* steps taken by pcg_step / PCG_STAGE_ADVANCE_TIME */
+  uint64_t particles;           /* live macroparticles, all species */
+  uint64_t removed;             /* removed by the runaway collector */
+  uint64_t move_errors;         /* >1-cell moves whose current was skipped */
+  uint64_t particle_steps;      /* sum over steps of live particles pushed */
+  double field_energy_e;        /* sum over interior nodes of eps0/2 E^2 * cell volume, J */
+  double field_energy_h;        /* sum of mu0/2 H^2 * cell volume, J */
+  double kinetic_energy;        /* sum of (gamma-1) m c^2 * weight, J */
+} pcg_diagnostics;
+
+int pcg_abi_version(void);
+int pcg_create(const pcg_config* cfg, pcg_handle** out);
+int pcg_destroy(pcg_handle* h);
+const char* pcg_last_error(const pcg_handle* h);
+
+/* Species are added before the first particle import; `slot` returns the
+ * index used by the calls below (species are processed in slot order, as
+ * the reference processes its species vector). */
+int pcg_add_species(pcg_handle* h, int id, const char* name, double charge_e, double mass_e,
+                    size_t capacity, int* slot);
+int pcg_add_beam(pcg_handle* h, int id, const char* name, double charge_e, double mass_e,
+                 size_t capacity, unsigned macro_amount, double start_time, double bunch_radius,
+                 double density, double bunches_amount, double bunch_length,
+                 double bunches_distance, double velocity, int* slot);
+
+/* Replace (import) or extend (append) a species' particles from host SoA. */
+int pcg_import_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
+                       const double* vr, const double* vphi, const double* vz, const double* w);
+int pcg_append_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
+                       const double* vr, const double* vphi, const double* vz, const double* w);
+int pcg_count(pcg_handle* h, int slot, size_t* n);
+/* Copy a species back (live particles in reference order).  cell_r/cell_z
+ * may be NULL.  Fails with PCG_ERR_CAPACITY if cap < count. */
+int pcg_export_species(pcg_handle* h, int slot, size_t cap, double* r, double* z, double* vr,
+                       double* vphi, double* vz, double* w, int32_t* cell_r, int32_t* cell_z,
+                       size_t* n);
+
+int pcg_set_field(pcg_handle* h, int which, const double* src);
+int pcg_export_field(pcg_handle* h, int which, double* dst);
+
+int pcg_stage(pcg_handle* h, int stage);
+int pcg_step(pcg_handle* h, int nsteps);
+int pcg_synchronize(pcg_handle* h);
+int pcg_diag(pcg_handle* h, pcg_diagnostics* out);
+/* The handle's cudaStream_t, for callers that time or order work on it. */
+int pcg_get_stream(pcg_handle* h, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

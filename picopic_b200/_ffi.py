@@ -1,0 +1,92 @@
+"""ctypes binding of libpcg.so (the C ABI in include/pcg.h).
+
+The library is loaded from this package directory only; when it is missing
+the import fails loudly, there is no other implementation to fall back to.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libpcg.so")
+
+PCG_OK = 0
+STATUS = {0: "PCG_OK", -1: "PCG_ERR_ARG", -2: "PCG_ERR_CUDA", -3: "PCG_ERR_NOMEM",
+          -4: "PCG_ERR_STATE", -5: "PCG_ERR_CAPACITY", -10: "PCG_ERR_NAN",
+          -11: "PCG_ERR_SUPERLUMINAL", -12: "PCG_ERR_TIMEOUT", -13: "PCG_ERR_UNSUPPORTED"}
+
+
+class PcgError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("nr", ctypes.c_int), ("nz", ctypes.c_int),
+                ("radius", ctypes.c_double), ("longitude", ctypes.c_double),
+                ("dt", ctypes.c_double), ("t_start", ctypes.c_double),
+                ("pml_size", ctypes.c_int * 4), ("pml_sigma", ctypes.c_double * 2),
+                ("pusher", ctypes.c_int), ("current", ctypes.c_int),
+                ("precision", ctypes.c_int), ("quirks", ctypes.c_int),
+                ("device", ctypes.c_int), ("seed", ctypes.c_uint64)]
+
+
+class Diagnostics(ctypes.Structure):
+    _fields_ = [("time", ctypes.c_double), ("steps", ctypes.c_uint64),
+                ("particles", ctypes.c_uint64), ("removed", ctypes.c_uint64),
+                ("move_errors", ctypes.c_uint64), ("particle_steps", ctypes.c_uint64),
+                ("field_energy_e", ctypes.c_double), ("field_energy_h", ctypes.c_double),
+                ("kinetic_energy", ctypes.c_double)]
+
+
+_D = ctypes.c_double
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI32 = ctypes.POINTER(ctypes.c_int32)
+_H = ctypes.c_void_p
+
+# name -> (restype, argtypes); every export of include/pcg.h
+SIGNATURES = {
+    "pcg_abi_version": (ctypes.c_int, []),
+    "pcg_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),
+    "pcg_destroy": (ctypes.c_int, [_H]),
+    "pcg_last_error": (ctypes.c_char_p, [_H]),
+    "pcg_add_species": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_char_p, _D, _D, ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_int)]),
+    "pcg_add_beam": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_char_p, _D, _D, ctypes.c_size_t,
+                                    ctypes.c_uint, _D, _D, _D, _D, _D, _D, _D,
+                                    ctypes.POINTER(ctypes.c_int)]),
+    "pcg_import_species": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_size_t] + [_PD] * 6),
+    "pcg_append_species": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_size_t] + [_PD] * 6),
+    "pcg_count": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "pcg_export_species": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_size_t] + [_PD] * 6 +
+                           [_PI32, _PI32, ctypes.POINTER(ctypes.c_size_t)]),
+    "pcg_set_field": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
+    "pcg_export_field": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
+    "pcg_stage": (ctypes.c_int, [_H, ctypes.c_int]),
+    "pcg_step": (ctypes.c_int, [_H, ctypes.c_int]),
+    "pcg_synchronize": (ctypes.c_int, [_H]),
+    "pcg_diag": (ctypes.c_int, [_H, ctypes.POINTER(Diagnostics)]),
+    "pcg_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libpcg.so and declare every exported function."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m picopic_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.pcg_abi_version() != 1:
+        raise ImportError("libpcg.so ABI version mismatch")
+    _lib = lib
+    return lib

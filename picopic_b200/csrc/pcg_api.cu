@@ -1,0 +1,724 @@
+// pcg_api.cu — host implementation of the C ABI declared in include/pcg.h.
+//
+// A handle owns one domain: the field grids (Grid<double> layout with the
+// 2-cell halo), the PML profile, the species buffers, one CUDA stream and a
+// device status block.  Work is queued on the stream; calls that return
+// data (export, diag, synchronize) wait for it and turn the device error
+// word into a status code.
+#include <cuda_runtime.h>
+#include <cub/device/device_select.cuh>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pcg.h"
+#include "pcg_f32.h"
+#include "pcg_kernels.h"
+#include "pcg_yee.cuh"
+
+using namespace pcg;
+
+namespace {
+
+struct Species {
+  int id = 0;
+  std::string name;
+  double charge_e = 0, mass_e = 0, charge = 0, mass = 0;
+  bool beam = false;
+  size_t cap = 0, n = 0;
+  unsigned long long order_base = 0;  // unused slots are never reused before compaction
+  // BeamP state (beamP.cpp:22-69)
+  unsigned macro_amount = 0, bunches_amount = 0, current_bunch = 0;
+  double start_time = 0, radius = 0, density = 0, bunch_length = 0, bunches_distance = 0,
+         velocity = 0, finish_time = 0, domain_radius = 0, bunch_macro_amount = 0,
+         macro_per_step = 0;
+  // double layout
+  double *r = nullptr, *z = nullptr, *vr = nullptr, *vphi = nullptr, *vz = nullptr,
+         *w = nullptr, *r_old = nullptr, *z_old = nullptr;
+  double *phi = nullptr, *phi_old = nullptr, *sn = nullptr;
+  int *cell_r = nullptr, *cell_z = nullptr;
+  // float layout
+  SpeciesF32Buffers f32;
+};
+
+const char* kFieldNames[12] = {"E_r", "E_phi", "E_z", "H_r", "H_phi", "H_z",
+                               "Hat_r", "Hat_phi", "Hat_z", "J_r", "J_phi", "J_z"};
+
+}  // namespace
+
+struct pcg_handle {
+  pcg_config cfg{};
+  GridGeom g{};
+  cudaStream_t stream = nullptr;
+  DevStatus* d_status = nullptr;
+  DevStatus* h_status = nullptr;  // pinned mirror
+  size_t nodes = 0;               // (nr+4)*(nz+4)
+  double* f64[12] = {};
+  float* f32[12] = {};
+  double* sig64[3] = {};          // r, z0, zl profiles
+  float* sig32[3] = {};
+  unsigned long long* reset = nullptr;
+  std::vector<Species> sp;
+  double t = 0;
+  uint64_t steps = 0, particle_steps = 0;
+  bool staged = false;   // stage-by-stage buffers allocated
+  bool started = false;  // particles imported or stepped: species list frozen
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  std::string err;
+};
+
+namespace {
+
+int fail(pcg_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(h, expr)                                                        \
+  do {                                                                           \
+    cudaError_t e_ = (expr);                                                     \
+    if (e_ != cudaSuccess)                                                       \
+      return fail((h), PCG_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int dalloc(pcg_handle* h, T** p, size_t count) {
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) return fail(h, PCG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return PCG_OK;
+}
+
+bool is_f64(const pcg_handle* h) { return h->cfg.precision == PCG_PRECISION_F64; }
+
+// PML profiles of MaxwellSolverYee::set_pml (maxwellSolverYee.cpp:57-109):
+// each wall adds a quadratic ramp that depends on i alone (r=R) or k alone
+// (z=0, z=L), so sigma(i,k) = sig_r[i] + sig_z0[k] + sig_zl[k].
+void pml_profiles(const pcg_config& c, const GridGeom& g, std::vector<double>& sr,
+                  std::vector<double>& s0, std::vector<double>& sl) {
+  sr.assign(g.nr, 0.0);
+  s0.assign(g.nz, 0.0);
+  sl.assign(g.nz, 0.0);
+  const double dr = g.dr, dz = g.dz;
+  const double l_left = dz * (double)c.pml_size[1];
+  const double l_right = dz * (double)c.pml_size[3];
+  const double l_ext = dr * (double)c.pml_size[2];
+  const double dsig = c.pml_sigma[1] - c.pml_sigma[0];
+  const size_t gcr = (size_t)(g.R / dr), gcz = (size_t)(g.L / dz);  // geometry.hpp:70-71
+  if (c.pml_size[2] != 0)
+    for (int i = 0; i < g.nr; i++) {
+      double dist = (double)(gcr - 0 - (size_t)i) * dr;
+      if (dist < l_ext)
+        sr[i] = c.pml_sigma[0] + dsig / pow(l_ext, 2) * pow(dr * (i + 1) + 0.0 * dr - g.R + l_ext, 2);
+    }
+  if (c.pml_size[1] != 0)
+    for (int k = 0; k < g.nz; k++)
+      if (dz * k + 0.0 * dz < l_left)
+        s0[k] = c.pml_sigma[0] + dsig / pow(l_left, 2) * pow(l_left - dz * k - 0.0 * dz, 2);
+  if (c.pml_size[3] != 0)
+    for (int k = 0; k < g.nz; k++) {
+      double dist = (double)(gcz - 0 - (size_t)k) * dz;
+      if (dist < l_right)
+        sl[k] = c.pml_sigma[0] + dsig / pow(l_right, 2) * pow(dz * (k + 1) + 0.0 * dz - g.L + l_right, 2);
+    }
+}
+
+FieldsF64 fields64(pcg_handle* h) {
+  FieldsF64 f;
+  for (int c = 0; c < 3; ++c) {
+    f.E[c] = h->f64[c]; f.H[c] = h->f64[3 + c]; f.Hat[c] = h->f64[6 + c]; f.J[c] = h->f64[9 + c];
+  }
+  f.sig_r = h->sig64[0]; f.sig_z0 = h->sig64[1]; f.sig_zl = h->sig64[2];
+  return f;
+}
+
+template <typename Real>
+YeeArgs<Real> yee_args(pcg_handle* h, Real* const* fld, Real* const* sig, int zero_j) {
+  YeeArgs<Real> a;
+  a.g = h->g;
+  for (int c = 0; c < 3; ++c) {
+    a.E[c] = fld[c]; a.H[c] = fld[3 + c]; a.Hat[c] = fld[6 + c]; a.J[c] = fld[9 + c];
+  }
+  a.sig_r = sig[0]; a.sig_z0 = sig[1]; a.sig_zl = sig[2];
+  a.zero_j = zero_j;
+  a.st = h->d_status;
+  return a;
+}
+
+SpeciesF64 view64(pcg_handle* h, Species& s) {
+  SpeciesF64 v;
+  v.n = s.n;
+  v.r = s.r; v.z = s.z; v.vr = s.vr; v.vphi = s.vphi; v.vz = s.vz; v.w = s.w;
+  v.r_old = s.r_old; v.z_old = s.z_old;
+  v.phi = s.phi; v.phi_old = s.phi_old; v.sn = s.sn;
+  v.cell_r = s.cell_r; v.cell_z = s.cell_z;
+  v.charge = s.charge; v.mass = s.mass;
+  v.c2m = s.charge * h->cfg.dt / (2 * s.mass);
+  v.is_beam = s.beam ? 1 : 0;
+  return v;
+}
+
+int alloc_species(pcg_handle* h, Species& s) {
+  int rc;
+  if (is_f64(h)) {
+    double** arrs[] = {&s.r, &s.z, &s.vr, &s.vphi, &s.vz, &s.w, &s.r_old, &s.z_old};
+    for (double** a : arrs)
+      if ((rc = dalloc(h, a, s.cap)) != PCG_OK) return rc;
+  } else {
+    if ((rc = f32_alloc_species(s.f32, s.cap)) != 0)
+      return fail(h, PCG_ERR_NOMEM, "cudaMalloc of a float species failed");
+  }
+  return PCG_OK;
+}
+
+int ensure_staged(pcg_handle* h) {
+  if (h->staged) return PCG_OK;
+  if (!is_f64(h)) return fail(h, PCG_ERR_UNSUPPORTED, "stage-by-stage calls need PCG_PRECISION_F64");
+  for (Species& s : h->sp) {
+    int rc;
+    double** arrs[] = {&s.phi, &s.phi_old, &s.sn};
+    for (double** a : arrs) {
+      if ((rc = dalloc(h, a, s.cap)) != PCG_OK) return rc;
+      CUDA_TRY(h, cudaMemsetAsync(*a, 0, sizeof(double) * s.cap, h->stream));
+    }
+    if ((rc = dalloc(h, &s.cell_r, s.cap)) != PCG_OK) return rc;
+    if ((rc = dalloc(h, &s.cell_z, s.cap)) != PCG_OK) return rc;
+    // bind the current positions, as after SpecieP::bind_cell_numbers
+    SpeciesF64 v = view64(h, s);
+    launch_stage_f64(PCG_STAGE_BIND, h->g, fields64(h), v, 0, 0, 0, h->d_status, h->stream);
+  }
+  h->staged = true;
+  return PCG_OK;
+}
+
+int check_status(pcg_handle* h) {
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                              h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  CUDA_TRY(h, cudaGetLastError());
+  unsigned e = h->h_status->error;
+  if (e & kErrNanPosition) return fail(h, PCG_ERR_NAN, "particle position is not a finite number");
+  if (e & kErrNanField) return fail(h, PCG_ERR_NAN, "electric field became NaN");
+  if (e & kErrSuperluminal) return fail(h, PCG_ERR_SUPERLUMINAL, "particle speed above c");
+  if (e & kErrReflectLoop) return fail(h, PCG_ERR_STATE, "wall reflection did not converge");
+  if (e & kErrOutOfGrid) return fail(h, PCG_ERR_STATE, "particle outside the grid");
+  if (e & kErrCapacity) return fail(h, PCG_ERR_CAPACITY, "species capacity exceeded");
+  if (e & kErrUnsupported) return fail(h, PCG_ERR_UNSUPPORTED, "switch combination not implemented");
+  return PCG_OK;
+}
+
+// BeamP::inject timing (beamP.cpp:73-156), evaluated on the host in the
+// reference's double arithmetic: returns how many particles to add now.
+unsigned beam_count(pcg_handle* h, Species& s, BeamInject* b, int slot) {
+  unsigned count = 0;
+  if (s.current_bunch < s.bunches_amount) {
+    double bunch_start = s.start_time + (s.bunch_length + s.bunches_distance) / s.velocity * s.current_bunch;
+    double bunch_finish = bunch_start + s.bunch_length / s.velocity;
+    if (0.0 * h->g.dr < s.radius && h->t >= bunch_start && h->t < bunch_finish) {
+      const double dr = h->g.dr, dz = h->g.dz;
+      b->seed = h->cfg.seed;
+      b->stream = 0x6265616du + (uint32_t)slot;
+      b->step = h->steps;
+      b->domain_radius = s.domain_radius;
+      b->dl = s.velocity * h->cfg.dt;
+      b->half_z = dz / 2.;
+      b->velocity = s.velocity;
+      b->v_macro_avg = kPi * s.radius * dr * dz;
+      double N_total = kPi * s.radius * s.radius * s.bunch_length * s.bunches_amount * s.density;
+      b->n_per_macro_avg = N_total / s.macro_amount;
+      for (unsigned i = 0; i < s.macro_per_step; ++i) ++count;
+    }
+    if (h->t > bunch_finish) ++s.current_bunch;
+  }
+  return count;
+}
+
+int stage_inject(pcg_handle* h) {
+  for (size_t t = 0; t < h->sp.size(); ++t) {
+    Species& s = h->sp[t];
+    if (!s.beam) continue;
+    BeamInject b{};
+    unsigned count = beam_count(h, s, &b, (int)t);
+    if (count == 0) continue;
+    if (s.n + count > s.cap) return fail(h, PCG_ERR_CAPACITY, "beam '" + s.name + "' capacity exceeded");
+    if (is_f64(h)) {
+      launch_inject_f64(h->g, view64(h, s), s.n, count, b, h->stream);
+    } else {
+      f32_launch_inject(h->g, s.f32, s.n, count, b, h->stream);
+    }
+    s.n += count;
+  }
+  return PCG_OK;
+}
+
+// Stable removal of dead slots (the erase of std::remove_if, SMB.cpp:216-345).
+int compact(pcg_handle* h) {
+  for (Species& s : h->sp) {
+    if (s.n == 0) continue;
+    size_t n = s.n;
+    unsigned* idx = nullptr;
+    unsigned* nsel = nullptr;
+    unsigned char* flags = nullptr;
+    int rc;
+    if ((rc = dalloc(h, &idx, 2 * n + 1)) != PCG_OK) return rc;
+    nsel = idx + 2 * n;
+    if ((rc = dalloc(h, &flags, n)) != PCG_OK) return rc;
+    if (is_f64(h)) f64_alive_flags(s.r, flags, n, h->stream);
+    else f32_alive_flags(s.f32, flags, n, h->stream);
+    iota_u32(idx + n, n, h->stream);
+    size_t tmp = 0;
+    cub::DeviceSelect::Flagged(nullptr, tmp, idx + n, flags, idx, nsel, (int)n, h->stream);
+    if (tmp > h->scratch_bytes) {
+      cudaFree(h->scratch);
+      h->scratch = nullptr;
+      if ((rc = dalloc(h, (unsigned char**)&h->scratch, tmp)) != PCG_OK) return rc;
+      h->scratch_bytes = tmp;
+    }
+    cub::DeviceSelect::Flagged(h->scratch, tmp, idx + n, flags, idx, nsel, (int)n, h->stream);
+    unsigned kept = 0;
+    CUDA_TRY(h, cudaMemcpyAsync(&kept, nsel, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    if (kept != n) {
+      if (is_f64(h)) {
+        double* tmpd = nullptr;
+        if ((rc = dalloc(h, &tmpd, kept)) != PCG_OK) return rc;
+        double* arrs[] = {s.r, s.z, s.vr, s.vphi, s.vz, s.w, s.r_old, s.z_old, s.phi, s.phi_old, s.sn};
+        for (double* a : arrs) {
+          if (!a) continue;
+          launch_gather_f64(a, tmpd, idx, kept, h->stream);
+          CUDA_TRY(h, cudaMemcpyAsync(a, tmpd, sizeof(double) * kept, cudaMemcpyDeviceToDevice, h->stream));
+        }
+        int* arri[] = {s.cell_r, s.cell_z};
+        for (int* a : arri) {
+          if (!a) continue;
+          launch_gather_i32(a, (int*)tmpd, idx, kept, h->stream);
+          CUDA_TRY(h, cudaMemcpyAsync(a, tmpd, sizeof(int) * kept, cudaMemcpyDeviceToDevice, h->stream));
+        }
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        cudaFree(tmpd);
+      } else {
+        if (f32_compact(s.f32, idx, kept, h->stream) != 0) return fail(h, PCG_ERR_NOMEM, "compaction");
+      }
+      s.n = kept;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    cudaFree(idx);
+    cudaFree(flags);
+  }
+  CUDA_TRY(h, cudaMemsetAsync(&h->d_status->dead_slots, 0, sizeof(unsigned long long), h->stream));
+  return PCG_OK;
+}
+
+int run_stage(pcg_handle* h, int stage) {
+  int rc;
+  const int fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
+  // Stage-by-stage mode keeps every Particle field of the reference on the
+  // device (phi, old phi, sin, bound cells), from the first stage on.
+  if (is_f64(h) && (rc = ensure_staged(h)) != PCG_OK) return rc;
+  if (stage == PCG_STAGE_INJECT) return stage_inject(h);
+  if (stage == PCG_STAGE_ADVANCE_TIME) {
+    h->t += h->cfg.dt;
+    h->steps += 1;
+    return PCG_OK;
+  }
+  if (stage == PCG_STAGE_FIELD_E || stage == PCG_STAGE_FIELD_H) {
+    if (is_f64(h)) {
+      YeeArgs<double> a = yee_args<double>(h, h->f64, h->sig64, 0);
+      if (stage == PCG_STAGE_FIELD_E) launch_yee_e_f64(a, h->stream);
+      else launch_yee_h_f64(a, fixed, h->stream);
+    } else {
+      YeeArgs<float> a = yee_args<float>(h, h->f32, h->sig32, 0);
+      if (stage == PCG_STAGE_FIELD_E) f32_launch_yee_e(a, h->stream);
+      else f32_launch_yee_h(a, fixed, h->stream);
+    }
+    return PCG_OK;
+  }
+  if (stage == PCG_STAGE_RESET_CURRENT) {  // Domain::reset_current domain.cpp:135-139
+    for (int c = 9; c < 12; ++c) {
+      if (is_f64(h)) CUDA_TRY(h, cudaMemsetAsync(h->f64[c], 0, sizeof(double) * h->nodes, h->stream));
+      else CUDA_TRY(h, cudaMemsetAsync(h->f32[c], 0, sizeof(float) * h->nodes, h->stream));
+    }
+    return PCG_OK;
+  }
+  if ((rc = ensure_staged(h)) != PCG_OK) return rc;
+  FieldsF64 f = fields64(h);
+  if (stage == PCG_STAGE_CURRENT) {
+    std::vector<SpeciesF64> v;
+    for (Species& s : h->sp) v.push_back(view64(h, s));
+    launch_current_stage_f64(h->g, f, v.data(), (int)v.size(), fixed, h->cfg.current, h->reset,
+                             h->d_status, h->stream);
+    return PCG_OK;
+  }
+  if (stage < PCG_STAGE_PUSH || stage > PCG_STAGE_COLLECT) return fail(h, PCG_ERR_ARG, "unknown stage");
+  for (size_t t = 0; t < h->sp.size(); ++t)
+    launch_stage_f64(stage, h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
+                     h->d_status, h->stream);
+  return PCG_OK;
+}
+
+// One fused step (PiCoPiC.cpp:326-347).
+int fused_step(pcg_handle* h) {
+  int rc;
+  const int fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
+  if ((rc = stage_inject(h)) != PCG_OK) return rc;
+  uint64_t live = 0;
+  for (Species& s : h->sp) live += s.n;
+  if (is_f64(h)) {
+    // E consumes J of the previous step, then clears it for this step's deposit.
+    launch_yee_e_f64(yee_args<double>(h, h->f64, h->sig64, 1), h->stream);
+    launch_yee_h_f64(yee_args<double>(h, h->f64, h->sig64, 0), fixed, h->stream);
+    FieldsF64 f = fields64(h);
+    if (h->cfg.current == PCG_CURRENT_VB)
+      CUDA_TRY(h, cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream));
+    for (size_t t = 0; t < h->sp.size(); ++t)
+      launch_advance_f64(h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
+                         h->cfg.current, h->reset, h->d_status, h->stream);
+    for (size_t t = 0; t < h->sp.size(); ++t)
+      launch_deposit_f64(h->g, f, view64(h, h->sp[t]), (int)t, fixed, h->cfg.current, h->reset,
+                         h->d_status, h->stream);
+  } else {
+    f32_launch_yee_e(yee_args<float>(h, h->f32, h->sig32, 1), h->stream);
+    f32_launch_yee_h(yee_args<float>(h, h->f32, h->sig32, 0), fixed, h->stream);
+    F32Step st;
+    st.g = h->g;
+    for (int c = 0; c < 12; ++c) st.fld[c] = h->f32[c];
+    st.pusher = h->cfg.pusher;
+    st.current = h->cfg.current;
+    st.fixed = fixed;
+    st.status = h->d_status;
+    for (size_t t = 0; t < h->sp.size(); ++t) {
+      Species& s = h->sp[t];
+      f32_launch_step(st, s.f32, s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream);
+    }
+  }
+  h->t += h->cfg.dt;
+  h->steps += 1;
+  h->particle_steps += live;
+  return PCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pcg_abi_version(void) { return PCG_ABI_VERSION; }
+
+int pcg_create(const pcg_config* cfg, pcg_handle** out) {
+  if (!cfg || !out) return PCG_ERR_ARG;
+  *out = nullptr;
+  if (cfg->nr < 2 || cfg->nz < 2 || cfg->nr > 32000 || cfg->nz > 32000 || !(cfg->radius > 0) ||
+      !(cfg->longitude > 0) || !(cfg->dt > 0))
+    return PCG_ERR_ARG;
+  if (cfg->pusher < 0 || cfg->pusher > 4 || cfg->current < 0 || cfg->current > 1 ||
+      cfg->precision < 0 || cfg->precision > 1 || cfg->quirks < 0 || cfg->quirks > 1)
+    return PCG_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PCG_ERR_CUDA;
+  if (cfg->device < 0 || cfg->device >= ndev) return PCG_ERR_ARG;
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return PCG_ERR_CUDA;
+  pcg_handle* h = new pcg_handle();
+  h->cfg = *cfg;
+  GridGeom& g = h->g;
+  g.nr = cfg->nr; g.nz = cfg->nz; g.ld = cfg->nz + 4;
+  g.R = cfg->radius; g.L = cfg->longitude;
+  g.dr = cfg->radius / cfg->nr;  // Geometry ctor geometry.hpp:67-68
+  g.dz = cfg->longitude / cfg->nz;
+  g.dt = cfg->dt;
+  g.pml_r = cfg->pml_size[2] != 0; g.pml_z0 = cfg->pml_size[1] != 0; g.pml_zl = cfg->pml_size[3] != 0;
+  h->t = cfg->t_start;
+  h->nodes = (size_t)(g.nr + 4) * (size_t)g.ld;
+  int rc = PCG_OK;
+  auto bail = [&](int code) { pcg_destroy(h); return code; };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PCG_ERR_CUDA);
+  if ((rc = dalloc(h, &h->d_status, 1)) != PCG_OK) return bail(rc);
+  if (cudaMallocHost((void**)&h->h_status, sizeof(DevStatus)) != cudaSuccess) return bail(PCG_ERR_NOMEM);
+  cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), h->stream);
+  std::vector<double> sr, s0, sl;
+  pml_profiles(*cfg, g, sr, s0, sl);
+  if (is_f64(h)) {
+    for (int c = 0; c < 12; ++c) {
+      if ((rc = dalloc(h, &h->f64[c], h->nodes)) != PCG_OK) return bail(rc);
+      cudaMemsetAsync(h->f64[c], 0, sizeof(double) * h->nodes, h->stream);
+    }
+    const std::vector<double>* prof[3] = {&sr, &s0, &sl};
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = dalloc(h, &h->sig64[c], prof[c]->size())) != PCG_OK) return bail(rc);
+      cudaMemcpyAsync(h->sig64[c], prof[c]->data(), sizeof(double) * prof[c]->size(),
+                      cudaMemcpyHostToDevice, h->stream);
+    }
+    if ((rc = dalloc(h, &h->reset, h->nodes)) != PCG_OK) return bail(rc);
+    cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream);
+  } else {
+    for (int c = 0; c < 12; ++c) {
+      if ((rc = dalloc(h, &h->f32[c], h->nodes)) != PCG_OK) return bail(rc);
+      cudaMemsetAsync(h->f32[c], 0, sizeof(float) * h->nodes, h->stream);
+    }
+    std::vector<float> prof[3];
+    const std::vector<double>* src[3] = {&sr, &s0, &sl};
+    for (int c = 0; c < 3; ++c) {
+      prof[c].assign(src[c]->begin(), src[c]->end());
+      if ((rc = dalloc(h, &h->sig32[c], prof[c].size())) != PCG_OK) return bail(rc);
+      cudaMemcpyAsync(h->sig32[c], prof[c].data(), sizeof(float) * prof[c].size(),
+                      cudaMemcpyHostToDevice, h->stream);
+    }
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(PCG_ERR_CUDA);
+  *out = h;
+  return PCG_OK;
+}
+
+int pcg_destroy(pcg_handle* h) {
+  if (!h) return PCG_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int c = 0; c < 12; ++c) { cudaFree(h->f64[c]); cudaFree(h->f32[c]); }
+  for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
+  cudaFree(h->reset);
+  cudaFree(h->scratch);
+  for (Species& s : h->sp) {
+    void* arrs[] = {s.r, s.z, s.vr, s.vphi, s.vz, s.w, s.r_old, s.z_old, s.phi, s.phi_old, s.sn,
+                    s.cell_r, s.cell_z};
+    for (void* a : arrs) cudaFree(a);
+    f32_free_species(s.f32);
+  }
+  cudaFree(h->d_status);
+  if (h->h_status) cudaFreeHost(h->h_status);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return PCG_OK;
+}
+
+const char* pcg_last_error(const pcg_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+static int add_common(pcg_handle* h, int id, const char* name, double charge_e, double mass_e,
+                      size_t capacity, int* slot, Species** out) {
+  if (!h || !slot) return PCG_ERR_ARG;
+  if (h->started) return fail(h, PCG_ERR_STATE, "species must be added before particles are imported");
+  if (!(mass_e > 0) || capacity == 0) return fail(h, PCG_ERR_ARG, "mass must be positive and capacity non-zero");
+  if (h->sp.size() >= 255) return fail(h, PCG_ERR_ARG, "too many species");
+  h->sp.emplace_back();
+  Species& s = h->sp.back();
+  s.id = id;
+  s.name = name ? name : "";
+  s.charge_e = charge_e; s.mass_e = mass_e;
+  s.charge = charge_e * kElCharge;  // SpecieP ctor specieP.cpp:37-38
+  s.mass = mass_e * kElMass;
+  s.cap = capacity;
+  int rc = alloc_species(h, s);
+  if (rc != PCG_OK) { h->sp.pop_back(); return rc; }
+  *slot = (int)h->sp.size() - 1;
+  *out = &s;
+  return PCG_OK;
+}
+
+int pcg_add_species(pcg_handle* h, int id, const char* name, double charge_e, double mass_e,
+                    size_t capacity, int* slot) {
+  Species* s = nullptr;
+  return add_common(h, id, name, charge_e, mass_e, capacity, slot, &s);
+}
+
+int pcg_add_beam(pcg_handle* h, int id, const char* name, double charge_e, double mass_e,
+                 size_t capacity, unsigned macro_amount, double start_time, double bunch_radius,
+                 double density, double bunches_amount, double bunch_length,
+                 double bunches_distance, double velocity, int* slot) {
+  if (!(velocity > 0) || !(bunch_length > 0) || !(bunch_radius > 0) || bunches_amount < 1)
+    return fail(h, PCG_ERR_ARG, "beam velocity, length, radius and bunch count must be positive");
+  Species* s = nullptr;
+  int rc = add_common(h, id, name, charge_e, mass_e, capacity, slot, &s);
+  if (rc != PCG_OK) return rc;
+  // BeamP ctor (beamP.cpp:22-69) for a domain at the origin
+  s->beam = true;
+  s->macro_amount = macro_amount;
+  s->radius = bunch_radius; s->density = density; s->velocity = velocity;
+  s->start_time = start_time; s->bunches_amount = (unsigned)bunches_amount;
+  s->bunch_length = bunch_length; s->bunches_distance = bunches_distance;
+  s->finish_time = s->start_time + s->bunch_length / s->velocity * s->bunches_amount +
+                   s->bunches_distance / s->velocity * (s->bunches_amount - 1);
+  if (bunch_radius > (double)h->g.nr * h->g.dr) s->domain_radius = h->g.R;
+  else if (bunch_radius > 0.0 * h->g.dr) s->domain_radius = bunch_radius - 0.0 * h->g.dr;
+  else s->domain_radius = 0;
+  double macro_normalizer = s->domain_radius / s->radius;
+  s->bunch_macro_amount = (double)(s->macro_amount / s->bunches_amount) * macro_normalizer;
+  s->macro_per_step = s->bunch_macro_amount * s->velocity * h->cfg.dt / s->bunch_length;
+  return PCG_OK;
+}
+
+static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
+                         const double* vr, const double* vphi, const double* vz, const double* w,
+                         bool append) {
+  if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  if (n && !(r && z && vr && vphi && vz && w)) return fail(h, PCG_ERR_ARG, "null particle array");
+  Species& s = h->sp[slot];
+  size_t n0 = append ? s.n : 0;
+  if (n0 + n > s.cap) return fail(h, PCG_ERR_CAPACITY, "species '" + s.name + "' capacity exceeded");
+  h->started = true;
+  if (n) {
+    double* stage = nullptr;
+    int rc = dalloc(h, &stage, 6 * n);
+    if (rc != PCG_OK) return rc;
+    const double* src[6] = {r, z, vr, vphi, vz, w};
+    for (int a = 0; a < 6; ++a)
+      CUDA_TRY(h, cudaMemcpyAsync(stage + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    if (is_f64(h)) launch_import_f64(h->g, view64(h, s), n0, n, stage, h->stream);
+    else f32_launch_import(h->g, s.f32, n0, n, stage, h->stream);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    cudaFree(stage);
+  }
+  s.n = n0 + n;
+  return PCG_OK;
+}
+
+int pcg_import_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
+                       const double* vr, const double* vphi, const double* vz, const double* w) {
+  return put_particles(h, slot, n, r, z, vr, vphi, vz, w, false);
+}
+
+int pcg_append_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
+                       const double* vr, const double* vphi, const double* vz, const double* w) {
+  return put_particles(h, slot, n, r, z, vr, vphi, vz, w, true);
+}
+
+int pcg_count(pcg_handle* h, int slot, size_t* n) {
+  if (!h || !n || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  if (h->h_status->dead_slots && (rc = compact(h)) != PCG_OK) return rc;
+  *n = h->sp[slot].n;
+  return PCG_OK;
+}
+
+int pcg_export_species(pcg_handle* h, int slot, size_t cap, double* r, double* z, double* vr,
+                       double* vphi, double* vz, double* w, int32_t* cell_r, int32_t* cell_z,
+                       size_t* n) {
+  size_t cnt = 0;
+  int rc = pcg_count(h, slot, &cnt);
+  if (rc != PCG_OK) return rc;
+  if (n) *n = cnt;
+  if (cap < cnt) return fail(h, PCG_ERR_CAPACITY, "export buffer too small");
+  if (cnt == 0) return PCG_OK;
+  Species& s = h->sp[slot];
+  if (is_f64(h)) {
+    double* dst[6] = {r, z, vr, vphi, vz, w};
+    double* src[6] = {s.r, s.z, s.vr, s.vphi, s.vz, s.w};
+    for (int a = 0; a < 6; ++a)
+      if (dst[a]) CUDA_TRY(h, cudaMemcpyAsync(dst[a], src[a], sizeof(double) * cnt, cudaMemcpyDeviceToHost, h->stream));
+    if (s.cell_r) {  // stage-by-stage mode keeps the bound cells (they may lag the positions)
+      if (cell_r) CUDA_TRY(h, cudaMemcpyAsync(cell_r, s.cell_r, sizeof(int) * cnt, cudaMemcpyDeviceToHost, h->stream));
+      if (cell_z) CUDA_TRY(h, cudaMemcpyAsync(cell_z, s.cell_z, sizeof(int) * cnt, cudaMemcpyDeviceToHost, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    } else {
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+      if ((cell_r || cell_z) && !(r && z)) return fail(h, PCG_ERR_ARG, "cells need r and z");
+      for (size_t j = 0; cell_r && j < cnt; ++j) cell_r[j] = (int32_t)floor(r[j] / h->g.dr);
+      for (size_t j = 0; cell_z && j < cnt; ++j) cell_z[j] = (int32_t)floor(z[j] / h->g.dz);
+    }
+  } else {
+    if (f32_export(h->g, s.f32, cnt, r, z, vr, vphi, vz, w, cell_r, cell_z, h->stream) != 0)
+      return fail(h, PCG_ERR_CUDA, "float export failed");
+  }
+  return PCG_OK;
+}
+
+int pcg_set_field(pcg_handle* h, int which, const double* src) {
+  if (!h || !src || which < 0 || which >= 12) return PCG_ERR_ARG;
+  if (is_f64(h)) {
+    CUDA_TRY(h, cudaMemcpyAsync(h->f64[which], src, sizeof(double) * h->nodes, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    std::vector<float> tmp(src, src + h->nodes);
+    CUDA_TRY(h, cudaMemcpyAsync(h->f32[which], tmp.data(), sizeof(float) * h->nodes, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  return PCG_OK;
+}
+
+int pcg_export_field(pcg_handle* h, int which, double* dst) {
+  if (!h || !dst || which < 0 || which >= 12) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  if (is_f64(h)) {
+    CUDA_TRY(h, cudaMemcpyAsync(dst, h->f64[which], sizeof(double) * h->nodes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  } else {
+    std::vector<float> tmp(h->nodes);
+    CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->f32[which], sizeof(float) * h->nodes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (size_t p = 0; p < h->nodes; ++p) dst[p] = tmp[p];
+  }
+  (void)kFieldNames;
+  return PCG_OK;
+}
+
+int pcg_stage(pcg_handle* h, int stage) {
+  if (!h) return PCG_ERR_ARG;
+  if (stage < 0 || stage > PCG_STAGE_ADVANCE_TIME) return fail(h, PCG_ERR_ARG, "unknown stage");
+  h->started = true;
+  int rc = run_stage(h, stage);
+  if (rc != PCG_OK) return rc;
+  if (stage == PCG_STAGE_COLLECT) return pcg_synchronize(h);
+  return PCG_OK;
+}
+
+int pcg_step(pcg_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return PCG_ERR_ARG;
+  h->started = true;
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = fused_step(h);
+    if (rc != PCG_OK) return rc;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(h, PCG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return PCG_OK;
+}
+
+int pcg_synchronize(pcg_handle* h) {
+  if (!h) return PCG_ERR_ARG;
+  return check_status(h);
+}
+
+int pcg_get_stream(pcg_handle* h, void** stream) {
+  if (!h || !stream) return PCG_ERR_ARG;
+  *stream = (void*)h->stream;
+  return PCG_OK;
+}
+
+int pcg_diag(pcg_handle* h, pcg_diagnostics* out) {
+  if (!h || !out) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  std::memset(out, 0, sizeof(*out));
+  out->time = h->t;
+  out->steps = h->steps;
+  out->removed = h->h_status->removed;
+  out->move_errors = h->h_status->move_errors;
+  out->particle_steps = h->particle_steps;
+  uint64_t slots = 0;
+  for (Species& s : h->sp) slots += s.n;
+  out->particles = slots - h->h_status->dead_slots;
+  double ee = 0, eh = 0, ek = 0;
+  if (is_f64(h)) {
+    if ((rc = f64_energies(h->g, fields64(h), &ee, &eh, h->stream)) != 0) return fail(h, PCG_ERR_CUDA, "energy reduction");
+    for (Species& s : h->sp) {
+      double e = 0;
+      if ((rc = f64_kinetic(s.vr, s.vphi, s.vz, s.w, s.r, s.n, s.mass, &e, h->stream)) != 0) return fail(h, PCG_ERR_CUDA, "kinetic");
+      ek += e;
+    }
+  } else {
+    float* fl[12];
+    for (int c = 0; c < 12; ++c) fl[c] = h->f32[c];
+    if (f32_energies(h->g, fl, &ee, &eh, h->stream) != 0) return fail(h, PCG_ERR_CUDA, "energy reduction");
+    for (Species& s : h->sp) {
+      double e = 0;
+      if (f32_kinetic(s.f32, s.n, s.mass, &e, h->stream) != 0) return fail(h, PCG_ERR_CUDA, "kinetic");
+      ek += e;
+    }
+  }
+  out->field_energy_e = ee;
+  out->field_energy_h = eh;
+  out->kinetic_energy = ek;
+  return PCG_OK;
+}
+
+}  // extern "C"

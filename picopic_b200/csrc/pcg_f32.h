@@ -1,0 +1,60 @@
+// pcg_f32.h — the single-precision production particle path: positions as a
+// packed int16 (cell_r, cell_z) pair plus float in-cell offsets, velocities
+// and weights in float, float field grids.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "pcg_common.cuh"
+#include "pcg_kernels.h"
+
+namespace pcg {
+
+template <typename Real>
+struct YeeArgs;
+
+// cell = (uint16)cell_r | cell_z << 16; a dead slot has cell < 0.
+struct SpeciesF32Buffers {
+  int* cell = nullptr;
+  float *off_r = nullptr, *off_z = nullptr;  // in-cell offsets in [0, 1), units of dr and dz
+  float *vr = nullptr, *vphi = nullptr, *vz = nullptr;  // m/s
+  float* w = nullptr;                                    // real particles per macroparticle
+  size_t cap = 0;
+};
+
+struct F32Step {
+  GridGeom g;
+  float* fld[12];
+  int pusher, current, fixed;
+  DevStatus* status;
+};
+
+__host__ __device__ __forceinline__ int pack_cell(int ci, int ck) {
+  return (int)(((unsigned)ci & 0xffffu) | ((unsigned)ck << 16));
+}
+__host__ __device__ __forceinline__ int cell_r_of(int cell) { return (int)(short)(cell & 0xffff); }
+__host__ __device__ __forceinline__ int cell_z_of(int cell) { return cell >> 16; }
+constexpr int kDeadCell = (int)0x80000000u;
+
+int f32_alloc_species(SpeciesF32Buffers& b, size_t cap);
+void f32_free_species(SpeciesF32Buffers& b);
+void f32_launch_yee_e(const YeeArgs<float>& a, cudaStream_t s);
+void f32_launch_yee_h(const YeeArgs<float>& a, int fixed, cudaStream_t s);
+void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsigned count,
+                       const BeamInject& bi, cudaStream_t s);
+void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_t n,
+                       const double* src, cudaStream_t s);
+void f32_launch_step(const F32Step& st, SpeciesF32Buffers& b, size_t n, double charge,
+                     double mass, int is_beam, cudaStream_t s);
+void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s);
+int f32_compact(SpeciesF32Buffers& b, const unsigned* idx, size_t kept, cudaStream_t s);
+int f32_export(const GridGeom& g, SpeciesF32Buffers& b, size_t n, double* r, double* z,
+               double* vr, double* vphi, double* vz, double* w, int32_t* cell_r, int32_t* cell_z,
+               cudaStream_t s);
+int f32_energies(const GridGeom& g, float* const fld[12], double* ee, double* eh, cudaStream_t s);
+int f32_kinetic(const SpeciesF32Buffers& b, size_t n, double mass, double* out, cudaStream_t s);
+
+}  // namespace pcg

@@ -1,0 +1,597 @@
+// pcg_f32_step.cuh — the fused single-precision particle step.
+//
+// One thread per macroparticle does, in registers: field gather, push,
+// move in the local Cartesian frame, rotation back to r-z, wall reflection,
+// velocity rotation, cell binding, the runaway test and the particle's
+// charge-conserving current.  Positions are kept as an integer cell and a
+// float offset in [0, 1) (units of dr, dz), so that per-step displacements
+// of 1e-4..1e-1 cells keep ~1e-7 relative precision far from the axis.
+//
+// Every formula is the reference's, rewritten in these normalised
+// coordinates (citations at each function); where the reference's form
+// cancels (the logarithms of the Villasenor-Buneman weights), the same
+// quantity is evaluated by a series in t = dx/x.  Arithmetic quirks of the
+// reference are kept (PCG_QUIRKS_REFERENCE) except the order-dependent J_r
+// overwrite of strict axial motion (currentVB.cpp:545-546), which has no
+// order-free meaning for a parallel deposit; the double-precision path
+// reproduces that one.
+#pragma once
+
+#include "pcg_f32.h"
+
+namespace pcg {
+namespace f32 {
+
+constexpr int kThreads = 256;
+
+struct StepArgs {
+  GridGeom g;
+  float *Er, *Ep, *Ez, *Hr, *Hp, *Hz;  // fields; H is field_h (time-centred)
+  float *Jr, *Jp, *Jz;
+  int nr, nz, ld;
+  float dt_dr, dt_dz;          // dt/dr, dt/dz
+  float c2m;                   // charge*dt/(2*mass), pusherBoris.cpp:67
+  float bk;                    // c2m * MAGN_CONST
+  float qz, qr, qp;            // per unit weight: q/(4 pi dr^2 dt), q/(2 pi dr dz dt), q/(2 pi dz dr^2)
+  float mnzl_r, mnzl_z;        // MNZL/dr, MNZL/dz
+  float dr_m, dz_m, dt_s;      // dr, dz, dt in SI (ZigZag keeps metre-valued weights)
+  float zz_vol;                // 1/(PI dz dr^2)
+  int pusher, current, fixed, is_beam;
+  DevStatus* st;
+};
+
+__device__ __forceinline__ long long node(const StepArgs& a, int i, int k) {
+  return (long long)(i + 2) * a.ld + (k + 2);
+}
+
+// ---------------------------------------------------------------------------
+// Gather (maxwellSolver.hpp:101-316) in normalised coordinates.  With
+// x = r/dr, a component staggered by s_r in r has i = floor(x - s_r),
+// u = x - s_r - i, and the ring-volume weights reduce to
+//   s_r = 1/2: (1-u)(2i+1+u)/(2i+2),  u(2i+2+u)/(2i+4)
+//   s_r = 0  : (1-u)(2i+u)/(2i+1),    u(2i+1+u)/(2i+3)
+// (the denominators are the reference's CELL_VOLUME arguments after macro
+// expansion); along z the weights are 1-v and v.
+
+struct Stagger {
+  int i;
+  float u;
+};
+
+__device__ __forceinline__ Stagger half_shift(int c, float f) {  // floor(x - 1/2)
+  Stagger s;
+  if (f >= 0.5f) { s.i = c; s.u = f - 0.5f; } else { s.i = c - 1; s.u = f + 0.5f; }
+  return s;
+}
+
+__device__ __forceinline__ void radial_w_half(int i, float u, float* w0, float* w1) {
+  const float fi = (float)i;
+  *w0 = (1.f - u) * (2.f * fi + 1.f + u) / (2.f * fi + 2.f);
+  *w1 = u * (2.f * fi + 2.f + u) / (2.f * fi + 4.f);
+}
+
+__device__ __forceinline__ void radial_w_int(int i, float u, float* w0, float* w1) {
+  const float fi = (float)i;
+  *w0 = (1.f - u) * (2.f * fi + u) / (2.f * fi + 1.f);
+  *w1 = u * (2.f * fi + 1.f + u) / (2.f * fi + 3.f);
+}
+
+__device__ __forceinline__ float interp4(const float* F, const StepArgs& a, int i, int k, float w0,
+                                         float w1, float v) {
+  const long long p = node(a, i, k);
+  const float f00 = __ldg(F + p), f10 = __ldg(F + p + a.ld);
+  const float f01 = __ldg(F + p + 1), f11 = __ldg(F + p + a.ld + 1);
+  return (f00 * w0 + f10 * w1) * (1.f - v) + (f01 * w0 + f11 * w1) * v;
+}
+
+__device__ __forceinline__ void gather(const StepArgs& a, int ci, float fr, int ck, float fz,
+                                       float e[3], float b[3]) {
+  const Stagger rh = half_shift(ci, fr), zh = half_shift(ck, fz);
+  float h0, h1, n0, n1;
+  radial_w_half(rh.i, rh.u, &h0, &h1);
+  radial_w_int(ci, fr, &n0, &n1);
+  // E_r: (1/2, 0); E_z: (0, 1/2); E_phi: (0, 0)
+  e[0] = interp4(a.Er, a, rh.i, ck, h0, h1, fz);
+  e[2] = interp4(a.Ez, a, ci, zh.i, n0, n1, zh.u);
+  {
+    const long long p = node(a, ci, ck);
+    const float f00 = __ldg(a.Ep + p), f10 = __ldg(a.Ep + p + a.ld);
+    const float f01 = __ldg(a.Ep + p + 1), f11 = __ldg(a.Ep + p + a.ld + 1);
+    const float t11 = f11 * n1 * fz;
+    e[1] = (f00 * n0 + f10 * n1) * (1.f - fz) + f01 * n0 * fz;
+    if (a.fixed) e[1] += t11; else e[2] += t11;  // maxwellSolver.hpp:313
+  }
+  // H_z: (1/2, 0); H_r: (0, 1/2); H_phi: (1/2, 1/2)
+  b[2] = interp4(a.Hz, a, rh.i, ck, h0, h1, fz);
+  b[0] = interp4(a.Hr, a, ci, zh.i, n0, n1, zh.u);
+  b[1] = interp4(a.Hp, a, rh.i, zh.i, h0, h1, zh.u);
+}
+
+// ---------------------------------------------------------------------------
+// Pushers (pusherBoris.cpp:23-151, pusherVay.cpp:22-114, pusherHC.cpp:23-117)
+
+constexpr float kC2 = 9.0e16f;  // LIGHT_VEL^2
+
+__device__ __forceinline__ float len2(const float v[3]) { return v[0] * v[0] + v[1] * v[1] + v[2] * v[2]; }
+
+__device__ __forceinline__ bool gamma_of_v(float v2, float* g, DevStatus* st) {  // rel.cpp:24-45
+  const float beta = v2 / kC2;
+  if (beta > 1.f) { raise_error(st, kErrSuperluminal); return false; }
+  *g = rsqrtf(1.f - beta);
+  return true;
+}
+
+__device__ __forceinline__ float gamma_inv_of_u(float u2) { return rsqrtf(1.f + u2 / kC2); }  // rel.cpp:47-55
+
+__device__ __forceinline__ bool push(const StepArgs& a, const float ein[3], const float bin[3],
+                                     float v[3]) {
+  float e[3], b[3];
+  for (int c = 0; c < 3; ++c) b[c] = bin[c] * a.bk;
+  if (a.pusher <= 2) {  // Boris: classic, adaptive, relativistic
+    for (int c = 0; c < 3; ++c) e[c] = ein[c] * a.c2m;
+    const bool rel = a.pusher == 2 || (a.pusher == 1 && len2(v) > (float)kRelLimit2);
+    float gm = 1.f;
+    if (rel) {
+      if (!gamma_of_v(len2(v), &gm, a.st)) return false;
+      for (int c = 0; c < 3; ++c) v[c] *= gm;
+    }
+    for (int c = 0; c < 3; ++c) v[c] += e[c];
+    if (rel) {
+      gm = gamma_inv_of_u(len2(v));
+      for (int c = 0; c < 3; ++c) b[c] *= gm;
+    }
+    const float k2 = 2.f / (1.f + len2(b));
+    const float t0 = v[0], t1 = v[1], t2 = v[2];
+    v[0] = t0 + k2 * ((t1 - t0 * b[2] + t2 * b[0]) * b[2] - (t2 + t0 * b[1] - t1 * b[0]) * b[1]);
+    v[1] = t1 + k2 * (-(t0 + t1 * b[2] - t2 * b[1]) * b[2] + (t2 + t0 * b[1] - t1 * b[0]) * b[0]);
+    v[2] = t2 + k2 * ((t0 + t1 * b[2] - t2 * b[1]) * b[1] - (t1 - t0 * b[2] + t2 * b[0]) * b[0]);
+    for (int c = 0; c < 3; ++c) v[c] += e[c];
+    if (rel) {
+      gm = gamma_inv_of_u(len2(v));
+      for (int c = 0; c < 3; ++c) v[c] *= gm;
+    }
+    return true;
+  }
+  // Vay and Higuera-Cary work on u = gamma v; `fixed` measures u in units of c.
+  const float cn = a.fixed ? 1.f / 3.0e8f : 1.f;
+  float gm;
+  if (!gamma_of_v(len2(v), &gm, a.st)) return false;
+  float u[3] = {v[0] * gm * cn, v[1] * gm * cn, v[2] * gm * cn};
+  float psm[3];
+  if (a.pusher == 3) {
+    const float ek = 2.f * a.c2m * cn;
+    float up[3] = {u[0] + ein[0] * ek, u[1] + ein[1] * ek, u[2] + ein[2] * ek};
+    const float gi = a.fixed ? rsqrtf(1.f + len2(u)) : gamma_inv_of_u(len2(u));
+    up[0] += gi * (u[1] * b[2] - u[2] * b[1]);
+    up[1] += gi * (u[2] * b[0] - u[0] * b[2]);
+    up[2] += gi * (u[0] * b[1] - u[1] * b[0]);
+    const float alpha0 = 1.f + len2(up), B2 = len2(b);
+    const float s0 = alpha0 - B2;
+    const float ub = up[0] * b[0] + up[1] * b[1] + up[2] * b[2];
+    const float al = rsqrtf(0.5f * (s0 + sqrtf(s0 * s0 + 4.f * (B2 + ub * ub))));
+    for (int c = 0; c < 3; ++c) b[c] *= al;
+    const float s = 1.f / (1.f + len2(b));
+    const float ab = up[0] * b[0] + up[1] * b[1] + up[2] * b[2];
+    psm[0] = s * (up[0] + ab * b[0] + b[2] * up[1] - b[1] * up[2]);
+    psm[1] = s * (up[1] + ab * b[1] + b[0] * up[2] - b[2] * up[0]);
+    psm[2] = s * (up[2] + ab * b[2] + b[1] * up[0] - b[0] * up[1]);
+  } else {
+    const float ek = a.c2m * cn;
+    for (int c = 0; c < 3; ++c) psm[c] = ein[c] * ek;
+    float um[3] = {u[0] + psm[0], u[1] + psm[1], u[2] + psm[2]};
+    const float gfm2 = 1.f + len2(um), B2 = len2(b);
+    const float bu = b[0] * um[0] + b[1] * um[1] + b[2] * um[2];
+    const float gi = rsqrtf(0.5f * (gfm2 - B2 + sqrtf((gfm2 - B2) * (gfm2 - B2) + 4.f * (B2 + bu * bu))));
+    for (int c = 0; c < 3; ++c) b[c] *= gi;
+    const float b2x = b[0] * b[0], b2y = b[1] * b[1], b2z = b[2] * b[2];
+    const float bxy = b[0] * b[1], byz = b[1] * b[2], bzx = b[2] * b[0];
+    const float idet = a.fixed ? 1.f / (1.f + b2x + b2y + b2z) : 1.f / (1.f + b2x + b2y + b2x);
+    const float upx = ((1.f + b2x - b2y - b2z) * um[0] + 2.f * (bxy + b[2]) * um[1] +
+                       2.f * (bzx - (a.fixed ? b[1] : b[2])) * um[2]) * idet;
+    const float upy = (2.f * (bxy - b[2]) * um[0] + (1.f - b2x + b2y - b2z) * um[1] +
+                       2.f * (byz + b[0]) * um[2]) * idet;
+    const float upz = (2.f * (bzx + b[1]) * um[0] + 2.f * (byz - b[0]) * um[1] +
+                       (1.f - b2x - b2y + b2z) * um[2]) * idet;
+    psm[0] += upx; psm[1] += upy; psm[2] += upz;
+  }
+  if (a.fixed) {
+    const float gi = rsqrtf(1.f + len2(psm)) * 3.0e8f;
+    for (int c = 0; c < 3; ++c) v[c] = psm[c] * gi;
+  } else {
+    const float gi = gamma_inv_of_u(len2(psm));
+    for (int c = 0; c < 3; ++c) v[c] = psm[c] * gi;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Positions
+
+__device__ __forceinline__ void renorm(int* c, float* f) {
+  const float fl = floorf(*f);
+  *c += (int)fl;
+  *f -= fl;
+  if (*f >= 1.f) { *f -= 1.f; *c += 1; }  // f just below an integer rounded up
+}
+
+// Mirror (c, f) about the wall at cell cw, offset 1/2: x' = 2 w - x.
+__device__ __forceinline__ void mirror(int* c, float* f, int cw) {
+  const float d = (float)(*c - cw) + (*f - 0.5f);
+  float t = 0.5f - d;
+  int nc = cw;
+  renorm(&nc, &t);
+  *c = nc;
+  *f = t;
+}
+
+// SpecieP::reflect (specieP.cpp:493-607): the walls sit half a cell inside
+// the domain; the reference's old-position bookkeeping inside the loop does
+// not reach its outputs and is omitted.
+__device__ __forceinline__ bool reflect(const StepArgs& a, int* ci, float* fr, int* ck, float* fz,
+                                        float* vr, float* vz) {
+  for (int guard = 0; guard < 64; ++guard) {
+    const bool out_r = *ci > a.nr - 1 || (*ci == a.nr - 1 && *fr > 0.5f);
+    const bool out_z = *ck > a.nz - 1 || (*ck == a.nz - 1 && *fz > 0.5f);
+    const bool in_r = *ci < 0 || (*ci == 0 && *fr < 0.5f);
+    const bool in_z = *ck < 0 || (*ck == 0 && *fz < 0.5f);
+    if (!(out_r || out_z || in_r || in_z)) return true;
+    if (out_r) { *vr = -*vr; mirror(ci, fr, a.nr - 1); }
+    if (*ck > a.nz - 1 || (*ck == a.nz - 1 && *fz > 0.5f)) { *vz = -*vz; mirror(ck, fz, a.nz - 1); }
+    if (*ci < 0 || (*ci == 0 && *fr < 0.5f)) {
+      *vr = -*vr;
+      mirror(ci, fr, 0);
+      if (*ci == 0 && *fr < 0.5f) *fr = 0.5f;
+    }
+    if (*ck < 0 || (*ck == 0 && *fz < 0.5f)) {
+      *vz = -*vz;
+      mirror(ck, fz, 0);
+      if (*ck == 0 && *fz < 0.5f) *fz = 0.5f;
+    }
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Villasenor-Buneman current (currentVB.cpp:22-735) in normalised form.
+//
+// For a segment inside cell (i, k) from (i+ao, k+bo) to (i+an, k+bn), with
+// dx = an-ao, dy = bn-bo, xo = i+ao, xn = i+an, t = dx/xo,
+//   g(t) = ln(1+t)/t, h(t) = g - 1 + t/2, m(t) = 1/(1+t) - g,
+// the reference's J_z and J_r increments (:46-108, :110-172) become
+//   Jz[i]   += Qz dy A/i,      A = (1-ao)(2i+ao)/xo - dx/2 (1 + i(i+1)/xo^2) + i(i+1) h/xo
+//   Jz[i+1] += Qz dy B/(i+1),  B = ao(2i+1+ao)/xo + dx/2 (1 + i(i+1)/xo^2) - i(i+1) h/xo
+//   (i = 0: Jz[0] += 8 Qz dy (1 - ao - dx/2), Jz[1] += Qz dy (1 + ao + dx/2))
+//   Jr[k]   += Qr/(i+1/2) [dx (b/2 - dy/4) + c/xo (dx b/xn + dy m)],      b = 1 - bo
+//   Jr[k+1] += Qr/(i+1/2) [dx (bo/2 + dy/4) + c/xo (dx bo/xn - dy m)],   c = i(i+1)/2
+// with Qz = q/(4 pi dr^2 dt) and Qr = q/(2 pi dr dz dt).
+
+__device__ __forceinline__ void g_terms(float t, float* h, float* m) {
+  if (fabsf(t) < 0.1f) {
+    const float t2 = t * t;
+    *h = t2 * (1.f / 3.f + t * (-0.25f + t * (0.2f + t * (-1.f / 6.f + t * (1.f / 7.f + t * (-0.125f))))));
+    *m = t * (-0.5f + t * (2.f / 3.f + t * (-0.75f + t * (0.8f + t * (-5.f / 6.f + t * (6.f / 7.f + t * (-0.875f)))))));
+  } else {
+    const float g = log1pf(t) / t;
+    *h = g - 1.f + 0.5f * t;
+    *m = 1.f / (1.f + t) - g;
+  }
+}
+
+struct Dep {
+  float* Jr;
+  float* Jp;
+  float* Jz;
+  int ld;
+  __device__ __forceinline__ void add(float* J, int i, int k, float v) const {
+    atomicAdd(J + (long long)(i + 2) * ld + (k + 2), v);
+  }
+};
+
+// simple_current_distribution for cell (i, k); points relative to that cell.
+__device__ __forceinline__ void vb_simple(const StepArgs& a, const Dep& d, float q, int i, int k,
+                                          float ao, float bo, float an, float bn) {
+  const float dx = an - ao, dy = bn - bo;
+  if (fabsf(dx) < a.mnzl_r || fabsf(dy) < a.mnzl_z) return;  // currentVB.cpp:45-46
+  const float fi = (float)i;
+  const float xo = fi + ao, xn = fi + an;
+  float h, m;
+  g_terms(dx / xo, &h, &m);
+  const float qz = q * a.qz * dy;
+  if (i >= 1) {
+    const float cc = fi * (fi + 1.f);
+    const float lin = 0.5f * dx * (1.f + cc / (xo * xo));
+    const float hh = cc * h / xo;
+    const float A = (1.f - ao) * (2.f * fi + ao) / xo - lin + hh;
+    const float B = ao * (2.f * fi + 1.f + ao) / xo + lin - hh;
+    d.add(d.Jz, i, k, qz * A / fi);
+    d.add(d.Jz, i + 1, k, qz * B / (fi + 1.f));
+  } else {
+    d.add(d.Jz, i, k, 8.f * qz * (1.f - ao - 0.5f * dx));
+    d.add(d.Jz, i + 1, k, qz * (1.f + ao + 0.5f * dx));
+  }
+  const float c = 0.5f * fi * (fi + 1.f);
+  const float qr = q * a.qr / (fi + 0.5f);
+  const float bb = 1.f - bo;
+  const float cx = c / xo;
+  d.add(d.Jr, i, k, qr * (dx * (0.5f * bb - 0.25f * dy) + cx * (dx * bb / xn + dy * m)));
+  d.add(d.Jr, i, k + 1, qr * (dx * (0.5f * bo + 0.25f * dy) + cx * (dx * bo / xn - dy * m)));
+}
+
+// strict_motion_distribution (:500-729); X*, Y* relative to the new cell.
+__device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float q, int in, int kn,
+                                          float Xo, float Yo, float Xn, float Yn) {
+  const float dX = Xn - Xo, dY = Yn - Yo;
+  const bool sr = fabsf(dX) < a.mnzl_r, sz = fabsf(dY) < a.mnzl_z;
+  if (sr && sz) return;
+  const float fi = (float)in;
+  const float xn = fi + Xn;
+  const int ko = kn + (int)floorf(Yo), io = in + (int)floorf(Xo);
+  if (sr) {  // axial motion :524-604 (the J_r overwrite is not reproduced here)
+    const float qz = q * a.qz;
+    const float lo = (in == 0) ? 8.f * qz * Xn * (1.f - Xn) / xn
+                               : qz * (1.f - Xn) * (2.f * fi + Xn) / (fi * xn);
+    const float up = qz * Xn * (2.f * fi + 1.f + Xn) / ((fi + 1.f) * xn);
+    switch (kn - ko) {
+      case 0:
+        d.add(d.Jz, in, kn, lo * dY);
+        d.add(d.Jz, in + 1, kn, up * dY);
+        break;
+      case 1:
+        d.add(d.Jz, in, kn - 1, lo * (0.f - Yo));
+        d.add(d.Jz, in + 1, kn - 1, up * (0.f - Yo));
+        d.add(d.Jz, in, kn, lo * Yn);
+        d.add(d.Jz, in + 1, kn, up * Yn);
+        break;
+      case -1:
+        d.add(d.Jz, in, kn + 1, lo * (1.f - Yo));
+        d.add(d.Jz, in + 1, kn + 1, up * (1.f - Yo));
+        d.add(d.Jz, in, kn, lo * (Yn - 1.f));
+        d.add(d.Jz, in + 1, kn, up * (Yn - 1.f));
+        break;
+      default: break;
+    }
+    return;
+  }
+  if (!sz) return;
+  // radial motion :607-728; bracket/dr in normalised units, wj = q Qr/(2(i+1/2)) * bracket
+  const float xo = fi + Xo;
+  const float ldz = 1.f - Yn, rdz = Yn;
+  auto put = [&](int i, float br) {
+    const float wj = q * a.qr * 0.5f / ((float)i + 0.5f) * br;
+    d.add(d.Jr, i, kn, wj * ldz);
+    d.add(d.Jr, i, kn + 1, wj * rdz);
+  };
+  const float dr2 = a.dr_m * a.dr_m;
+  switch (in - io) {
+    case 0:
+      put(in, dX * (1.f + fi * (fi + 1.f) / (xo * xn)));
+      break;
+    case 1: {
+      const float d1 = 0.f - Xo;  // to the boundary at x = in
+      put(in - 1, d1 * (1.f + (fi - 1.f) / xo));
+      const float d2 = Xn;
+      const float r0 = fi + 0.5f;
+      const float br = a.fixed ? d2 * (1.f + (fi + 1.f) / xn)
+                               : d2 - r0 * r0 / xn + r0 * r0 * dr2 / fi + 0.25f / xn - 0.25f / fi;  // :673
+      put(in, br);
+      break;
+    }
+    case -1: {
+      const float d1 = 1.f - Xo;
+      put(in + 1, d1 * (1.f + (fi + 2.f) / xo));
+      const float d2 = Xn - 1.f;
+      const float r0 = fi + 0.5f;
+      const float br = a.fixed ? d2 * (1.f + fi / xn)
+                               : d2 - r0 * r0 / xn + r0 * r0 * dr2 / (fi + 1.f) + 0.25f / xn - 0.25f / (fi + 1.f);  // :714
+      put(in, br);
+      break;
+    }
+    default: break;
+  }
+}
+
+// azimuthal_current_distribution (:398-498): J_phi from the mid-point, in
+// the cell of the new position (a, b may lie outside [0, 1)).
+__device__ __forceinline__ void vb_azimuthal(const StepArgs& a, const Dep& d, float q, float vphi,
+                                             int in, int kn, float Xm, float Ym) {
+  const float fi = (float)in;
+  const float xm = fi + Xm;
+  const float qp = q * a.qp * vphi / xm;
+  const float w0 = (1.f - Xm) * (2.f * fi + Xm) / (2.f * fi + 1.f);
+  const float w1 = Xm * (2.f * fi + 1.f + Xm) / (2.f * fi + 2.f);
+  const bool i0 = in >= 0 && in < a.nr, i1 = in + 1 < a.nr;
+  const bool k0 = kn >= 0 && kn < a.nz, k1 = kn + 1 < a.nz;
+  // the halo of J_phi is cleared before the rz deposit (currentVB.cpp:177)
+  if (i0 && k0) d.add(d.Jp, in, kn, qp * w0 * (1.f - Ym));
+  if (i1 && k0) d.add(d.Jp, in + 1, kn, qp * w1 * (1.f - Ym));
+  if (i0 && k1) d.add(d.Jp, in, kn + 1, qp * w0 * Ym);
+  if (i1 && k1) d.add(d.Jp, in + 1, kn + 1, qp * w1 * Ym);
+}
+
+// rz_current_distribution (:175-396); old point (Xo, Yo) relative to the
+// new cell (in, kn), new point (Xn, Yn) in [0, 1)^2.
+__device__ __forceinline__ bool vb_rz(const StepArgs& a, const Dep& d, float q, int in, int kn,
+                                      float Xo, float Yo, float Xn, float Yn) {
+  const int di = (int)floorf(Xo), dk = (int)floorf(Yo);  // old cell - new cell
+  if (abs(di) > 1 || (a.fixed && abs(dk) > 1)) return false;
+  if (fabsf(Xn - Xo) < a.mnzl_r || fabsf(Yn - Yo) < a.mnzl_z) {
+    vb_strict(a, d, q, in, kn, Xo, Yo, Xn, Yn);
+    return true;
+  }
+  const int res = abs(di) + abs(dk);
+  // Segment helper: points relative to (in, kn), deposited in cell (in+ci, kn+ck).
+  auto seg = [&](float x0, float y0, float x1, float y1, int ci, int ck) {
+    vb_simple(a, d, q, in + ci, kn + ck, x0 - ci, y0 - ck, x1 - ci, y1 - ck);
+  };
+  const float sl = (Yn - Yo) / (Xn - Xo);  // dz/dr in cells
+  if (res == 0) {
+    seg(Xo, Yo, Xn, Yn, 0, 0);
+  } else if (res == 1) {
+    if (di != 0) {
+      const float xb = di > 0 ? 1.f : 0.f;  // boundary x = in+1 (from outside) or x = in
+      const float yb = Yo + (xb - Xo) * sl;
+      seg(Xo, Yo, xb, yb, di, 0);
+      seg(xb, yb, Xn, Yn, 0, 0);
+    } else {
+      const float yb = dk > 0 ? 1.f : 0.f;
+      const float xb = Xo + (yb - Yo) / sl;
+      seg(Xo, Yo, xb, yb, 0, dk);
+      seg(xb, yb, Xn, Yn, 0, 0);
+    }
+  } else if (res == 2 && di != 0) {
+    // boundary lines crossed: x = xb (between old and new column), y = yb
+    const float xb = di > 0 ? 1.f : 0.f;
+    const float yb = dk > 0 ? 1.f : 0.f;
+    const float y1 = Yo + (xb - Xo) * sl;  // where the path meets x = xb
+    const float x2 = Xo + (yb - Yo) / sl;  // where it meets y = yb
+    // The path meets the radial boundary first when, at x = xb, it is still
+    // on the old side of y = yb (:271-381); a crossing exactly through the
+    // corner deposits nothing, as in the reference.
+    if (y1 == yb) return true;
+    const bool r_first = (dk < 0) ? (y1 < yb) : (y1 > yb);
+    if (r_first) {  // old cell -> (0, dk) cell -> new cell
+      seg(Xo, Yo, xb, y1, di, dk);
+      seg(xb, y1, x2, yb, 0, dk);
+      seg(x2, yb, Xn, Yn, 0, 0);
+    } else {        // old cell -> (di, 0) cell -> new cell
+      seg(Xo, Yo, x2, yb, di, dk);
+      seg(x2, yb, xb, y1, di, 0);
+      seg(xb, y1, Xn, Yn, 0, 0);
+    }
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// ZigZag current (currentZigZag.cpp:22-136) with the reference's metre-valued
+// weights W = (mean position - cell edge) in metres.
+
+__device__ __forceinline__ void zigzag(const StepArgs& a, const Dep& d, float qw, float vphi,
+                                       int in, int kn, float Xo, float Yo, float Xn, float Yn) {
+  const int io = (int)floorf(Xo), ko = (int)floorf(Yo);  // relative to the new cell
+  const int imid = in + (int)floorf(0.5f * (Xo + Xn));
+  const float oov = a.zz_vol / (2.f * (float)imid + 1.f);
+  const float ro = ((float)in + Xo) * a.dr_m, rn = ((float)in + Xn) * a.dr_m;
+  const float F_phi = qw * vphi;
+  const float W_phi = vphi * a.dt_s / (2.f * 3.14159265f * (ro + rn));
+  const float xr = fminf((float)min(io, 0) + 1.f, fmaxf((float)max(io, 0), 0.5f * (Xo + Xn)));
+  const float yr = fminf((float)min(ko, 0) + 1.f, fmaxf((float)max(ko, 0), 0.5f * (Yo + Yn)));
+  const float cod = qw / a.dt_s;
+  const float F_r1 = cod * a.dr_m * (xr - Xo), F_r2 = cod * a.dr_m * (Xn - xr);
+  const float F_z1 = cod * a.dz_m * (yr - Yo), F_z2 = cod * a.dz_m * (Yn - yr);
+  const float W_r1 = a.dr_m * (0.5f * (Xo + xr) - (float)io), W_r2 = a.dr_m * (0.5f * (Xn + xr));
+  const float W_z1 = a.dz_m * (0.5f * (Yo + yr) - (float)ko), W_z2 = a.dz_m * (0.5f * (Yn + yr));
+  const float mWr1 = 1.f - W_r1, mWr2 = 1.f - W_r2, mWz1 = 1.f - W_z1, mWz2 = 1.f - W_z2, mWp = 1.f - W_phi;
+  const int ia = in + io, ka = kn + ko;
+  d.add(d.Jr, ia, ka, oov * F_r1 * mWp * mWz1 + oov * F_r1 * W_phi * mWz1);
+  d.add(d.Jr, ia, ka + 1, oov * F_r1 * mWp * W_z1 + oov * F_r1 * W_phi * W_z1);
+  d.add(d.Jr, in, kn, oov * F_r2 * mWp * mWz2 + oov * F_r2 * W_phi * mWz2);
+  d.add(d.Jr, in, kn + 1, oov * F_r2 * mWp * W_z2 + oov * F_r2 * W_phi * W_z2);
+  d.add(d.Jp, in, kn, oov * F_phi * mWr2 * mWz2);
+  d.add(d.Jp, in, kn + 1, oov * F_phi * mWr2 * W_z1);
+  d.add(d.Jp, in + 1, kn, oov * F_phi * W_r2 * mWz2);
+  d.add(d.Jp, in + 1, kn + 1, oov * F_phi * W_r2 * W_z2);
+  d.add(d.Jz, ia, ka, oov * F_z1 * mWr1 * mWp + oov * F_z1 * mWr1 * W_phi);
+  d.add(d.Jz, ia + 1, ka, oov * F_z1 * W_r1 * mWp + oov * F_z1 * W_r1 * W_phi);
+  d.add(d.Jz, in, kn, oov * F_z2 * mWr2 * mWp + oov * F_z2 * mWr2 * W_phi);
+  d.add(d.Jz, in + 1, kn, oov * F_z2 * W_r2 * mWp + oov * F_z2 * W_r2 * W_phi);
+}
+
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) step_kernel(StepArgs a, SpeciesF32Buffers b, size_t n) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int cell = b.cell[j];
+  if (cell < 0) return;
+  const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
+  const float fr0 = b.off_r[j], fz0 = b.off_z[j];
+  if (ci0 < -1 || ci0 > a.nr || ck0 < -1 || ck0 > a.nz) {  // gather would leave the halo
+    raise_error(a.st, kErrOutOfGrid);
+    return;
+  }
+  float v[3] = {b.vr[j], b.vphi[j], b.vz[j]};
+  const float w = b.w[j];
+  float e[3], bb[3];
+  gather(a, ci0, fr0, ck0, fz0, e, bb);
+  if (!push(a, e, bb, v)) return;
+  // mover_cylindrical + back_position_to_rz (specieP.cpp:482-491, 609-622):
+  // x' = sqrt((x+dx)^2 + dy^2), taken as dx + dy^2/(X + x') to keep the
+  // displacement's precision.
+  const float dx = v[0] * a.dt_dr, dyp = v[1] * a.dt_dr, dzz = v[2] * a.dt_dz;
+  const float X = (float)ci0 + fr0 + dx;
+  const float xn = sqrtf(X * X + dyp * dyp);
+  const float sn = dyp / xn;
+  int ci = ci0, ck = ck0;
+  // far from the axis x' - x = dx + dy^2/(X + x'); near it (or across it,
+  // X < 0) x' itself is small and exact enough
+  float fr = (X > 0.5f) ? fr0 + dx + dyp * dyp / (X + xn) : xn - (float)ci0;
+  float fz = fz0 + dzz;
+  renorm(&ci, &fr);
+  renorm(&ck, &fz);
+  if (a.is_beam) {  // BeamP::reflect beamP.cpp:159-177
+    if (ci < 0 || (ci == 0 && fr < 0.5f)) { mirror(&ci, &fr, 0); v[0] = -v[0]; }
+  } else if (!reflect(a, &ci, &fr, &ck, &fz, &v[0], &v[2])) {
+    raise_error(a.st, kErrReflectLoop);
+  }
+  const float cs = sqrtf(1.f - sn * sn);  // back_velocity_to_rz :624-640
+  const float vr2 = cs * v[0] - sn * v[1];
+  const float vp2 = sn * v[0] + cs * v[1];
+  v[0] = vr2;
+  v[1] = vp2;
+  b.vr[j] = v[0];
+  b.vphi[j] = v[1];
+  b.vz[j] = v[2];
+  if (ci < 0 || ck < 0 || ci >= a.nr || ck >= a.nz) {  // runaway collector SMB.cpp:252-337
+    b.cell[j] = kDeadCell;
+    atomicAdd(&a.st->removed, 1ull);
+    atomicAdd(&a.st->dead_slots, 1ull);
+    return;
+  }
+  b.cell[j] = pack_cell(ci, ck);
+  b.off_r[j] = fr;
+  b.off_z[j] = fz;
+  // the old point relative to the new cell
+  const float Xo = (float)(ci0 - ci) + fr0, Yo = (float)(ck0 - ck) + fz0;
+  const Dep d{a.Jr, a.Jp, a.Jz, a.ld};
+  if (a.current == 1) {
+    zigzag(a, d, w * 1.0f, v[1], ci, ck, Xo, Yo, fr, fz);
+    return;
+  }
+  const float q = w;  // Qz, Qr, Qp carry the species charge
+  vb_azimuthal(a, d, q, v[1], ci, ck, 0.5f * (Xo + fr), 0.5f * (Yo + fz));
+  if (!vb_rz(a, d, q, ci, ck, Xo, Yo, fr, fz)) atomicAdd(&a.st->move_errors, 1ull);
+}
+
+}  // namespace f32
+
+inline void launch_f32_particle_step(const F32Step& st, SpeciesF32Buffers& b, size_t n,
+                                     double charge, double mass, int is_beam, cudaStream_t s) {
+  if (n == 0) return;
+  const GridGeom& g = st.g;
+  f32::StepArgs a;
+  a.g = g;
+  a.Er = st.fld[0]; a.Ep = st.fld[1]; a.Ez = st.fld[2];
+  a.Hr = st.fld[3]; a.Hp = st.fld[4]; a.Hz = st.fld[5];
+  a.Jr = st.fld[9]; a.Jp = st.fld[10]; a.Jz = st.fld[11];
+  a.nr = g.nr; a.nz = g.nz; a.ld = g.ld;
+  a.dt_dr = (float)(g.dt / g.dr);
+  a.dt_dz = (float)(g.dt / g.dz);
+  const double c2m = charge * g.dt / (2 * mass);
+  a.c2m = (float)c2m;
+  a.bk = (float)(c2m * kMagnConst);
+  a.qz = (float)(charge / (4.0 * kPi * g.dr * g.dr * g.dt));
+  a.qr = (float)(charge / (2.0 * kPi * g.dr * g.dz * g.dt));
+  a.qp = (float)(charge / (2.0 * kPi * g.dz * g.dr * g.dr));
+  a.mnzl_r = (float)(kMnzl / g.dr);
+  a.mnzl_z = (float)(kMnzl / g.dz);
+  a.dr_m = (float)g.dr; a.dz_m = (float)g.dz; a.dt_s = (float)g.dt;
+  a.zz_vol = (float)(1.0 / (kPi * g.dz * g.dr * g.dr));
+  a.pusher = st.pusher; a.current = st.current; a.fixed = st.fixed; a.is_beam = is_beam;
+  a.st = st.status;
+  if (st.current == 1) a.zz_vol *= (float)charge;  // ZigZag: fold q into 1/V
+  const unsigned blocks = (unsigned)((n + f32::kThreads - 1) / f32::kThreads);
+  f32::step_kernel<<<blocks, f32::kThreads, 0, s>>>(a, b, n);
+}
+
+}  // namespace pcg

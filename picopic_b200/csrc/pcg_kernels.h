@@ -1,0 +1,81 @@
+// pcg_kernels.h — device data views and kernel launchers shared by the host
+// API (pcg_api.cu) and the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "pcg_common.cuh"
+
+namespace pcg {
+
+template <typename Real>
+struct YeeArgs;
+
+struct FieldsF64 {
+  double* E[3];
+  double* H[3];
+  double* Hat[3];
+  double* J[3];
+  const double* sig_r;
+  const double* sig_z0;
+  const double* sig_zl;
+};
+
+// One species in the double-precision layout (structure of arrays).
+struct SpeciesF64 {
+  size_t n;  // slots in use (dead slots have r < 0)
+  double *r, *z, *vr, *vphi, *vz, *w, *r_old, *z_old;
+  double *phi, *phi_old, *sn;  // stage-by-stage mode only, else null
+  int *cell_r, *cell_z;        // stage-by-stage mode only, else null
+  double charge, mass;         // SI
+  double c2m;                  // charge * dt / (2 * mass), pusherBoris.cpp:67
+  int is_beam;
+};
+
+// Per-step parameters of BeamP::inject (beamP.cpp:71-157).
+struct BeamInject {
+  uint64_t seed;
+  uint32_t stream;
+  uint64_t step;
+  double domain_radius, dl, half_z, velocity, v_macro_avg, n_per_macro_avg;
+};
+
+void launch_yee_e_f64(const YeeArgs<double>& a, cudaStream_t s);
+void launch_yee_h_f64(const YeeArgs<double>& a, int fixed, cudaStream_t s);
+void launch_stage_f64(int stage, const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp,
+                      int slot, int pusher, int fixed, DevStatus* st, cudaStream_t s);
+void launch_current_stage_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64* sp,
+                              int nsp, int fixed, int current, unsigned long long* reset,
+                              DevStatus* st, cudaStream_t s);
+void launch_advance_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp, int slot,
+                        int pusher, int fixed, int current, unsigned long long* reset,
+                        DevStatus* st, cudaStream_t s);
+void launch_deposit_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp, int slot,
+                        int fixed, int current, const unsigned long long* reset, DevStatus* st,
+                        cudaStream_t s);
+void launch_halo_zero_f64(const GridGeom& g, double* a0, double* a1, double* a2, cudaStream_t s);
+void launch_inject_f64(const GridGeom& g, const SpeciesF64& sp, size_t n0, unsigned count,
+                       const BeamInject& b, cudaStream_t s);
+void launch_import_f64(const GridGeom& g, const SpeciesF64& sp, size_t n0, size_t n,
+                       const double* src, cudaStream_t s);
+void launch_gather_f64(const double* src, double* dst, const unsigned* idx, size_t n, cudaStream_t s);
+void launch_gather_i32(const int* src, int* dst, const unsigned* idx, size_t n, cudaStream_t s);
+
+}  // namespace pcg
+
+namespace pcg {
+
+// Utilities (pcg_util.cu)
+void f64_alive_flags(const double* r, unsigned char* flags, size_t n, cudaStream_t s);
+void iota_u32(unsigned* a, size_t n, cudaStream_t s);
+// Field energies over interior nodes: sum of eps0/2 |E|^2 V_i and mu0/2 |H|^2 V_i
+// with V_i = PI dz dr^2 (2i+1), H taken at the centred time (field_h).
+int f64_energies(const GridGeom& g, const FieldsF64& f, double* ee, double* eh, cudaStream_t s);
+// Kinetic energy sum w m v^2 gamma^2/(gamma+1) of live particles (r >= 0).
+int f64_kinetic(const double* vr, const double* vphi, const double* vz, const double* w,
+                const double* r, size_t n, double mass, double* out, cudaStream_t s);
+
+}  // namespace pcg

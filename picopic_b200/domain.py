@@ -1,0 +1,218 @@
+"""Host-side mirror of the reference's per-domain façade, on the GPU.
+
+:class:`Domain` exposes the methods that the reference scheduler (``SMB``)
+calls on ``Domain`` (src/domain.cpp:86-204) — ``weight_field_e``,
+``weight_field_h``, ``push_particles``, ``dump_particle_positions_to_old``,
+``update_particles_coords``, ``particles_back_position_to_rz``, ``reflect``,
+``particles_back_velocity_to_rz``, ``bind_cell_numbers``,
+``reset_current``, ``weight_current``, ``manage_beam`` — each one a CUDA
+kernel behind the C ABI, plus :meth:`step`, the fused step of
+src/PiCoPiC.cpp:326-347.  Field and particle access follows the reference
+layouts (``Grid<double>`` with a 2-cell halo; ``SpecieP::particles``).
+
+Errors surface as :class:`PcgError`, the counterpart of the reference's
+``LOG_S(FATAL)`` aborts.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._ffi import Config, Diagnostics, PcgError, load
+
+PUSHERS = {"boris": 0, "borisadaptive": 1, "borisrel": 2, "vay": 3, "hc": 4}
+CURRENTS = {"vb": 0, "zigzag": 1}
+PRECISIONS = {"f64": 0, "f32": 1}
+QUIRKS = {"reference": 0, "fixed": 1}
+STAGES = ["inject", "field_e", "field_h", "push", "dump_old", "move", "pos_rz", "reflect",
+          "vel_rz", "bind", "collect", "reset_current", "current", "advance_time"]
+STAGE = {n: i for i, n in enumerate(STAGES)}
+FIELDS = ["e_r", "e_phi", "e_z", "h_r", "h_phi", "h_z", "hat_r", "hat_phi", "hat_z",
+          "j_r", "j_phi", "j_z"]
+FIELD = {n: i for i, n in enumerate(FIELDS)}
+
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI32 = ctypes.POINTER(ctypes.c_int32)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_PD)
+
+
+@dataclass
+class Geometry:
+    """One domain at the origin with all four walls (src/cfg.cpp:379-429)."""
+    nr: int
+    nz: int
+    radius: float
+    longitude: float
+    dt: float
+    t_start: float = 0.0
+    pml_size: tuple = (0, 0, 0, 0)
+    pml_sigma: tuple = (0.0, 0.0)
+
+    @property
+    def dr(self):
+        return self.radius / self.nr
+
+    @property
+    def dz(self):
+        return self.longitude / self.nz
+
+    @property
+    def shape(self):
+        return (self.nr + 4, self.nz + 4)
+
+
+class Domain:
+    """A simulation domain on one GPU, driven like the reference ``Domain``."""
+
+    def __init__(self, geometry, pusher="borisrel", current="vb", precision="f64",
+                 quirks="reference", device=0, seed=0):
+        self.lib = load()
+        self.grid = geometry
+        c = Config()
+        c.nr, c.nz = int(geometry.nr), int(geometry.nz)
+        c.radius, c.longitude = float(geometry.radius), float(geometry.longitude)
+        c.dt, c.t_start = float(geometry.dt), float(geometry.t_start)
+        for i in range(4):
+            c.pml_size[i] = int(geometry.pml_size[i])
+        c.pml_sigma[0], c.pml_sigma[1] = float(geometry.pml_sigma[0]), float(geometry.pml_sigma[1])
+        c.pusher, c.current = PUSHERS[pusher], CURRENTS[current]
+        c.precision, c.quirks = PRECISIONS[precision], QUIRKS[quirks]
+        c.device, c.seed = int(device), int(seed)
+        h = ctypes.c_void_p()
+        rc = self.lib.pcg_create(ctypes.byref(c), ctypes.byref(h))
+        if rc != 0:
+            raise PcgError(rc, "pcg_create", "invalid configuration or no CUDA device")
+        self.h = h
+        self.precision = precision
+        self.species = []
+
+    # -- error handling ------------------------------------------------------
+    def _check(self, rc, where):
+        if rc != 0:
+            msg = self.lib.pcg_last_error(self.h)
+            raise PcgError(rc, where, msg.decode() if msg else "")
+        return rc
+
+    # -- species (SpecieP / BeamP) ----------------------------------------------
+    def add(self, spec, capacity=None) -> int:
+        """Add a species or beam described like ``SpecieP``/``BeamP``."""
+        cap = int(capacity or getattr(spec, "capacity", 0) or 1 << 16)
+        slot = ctypes.c_int()
+        if getattr(spec, "beam", None) is None:
+            self._check(self.lib.pcg_add_species(self.h, int(spec.id), spec.name.encode(),
+                                                 float(spec.charge), float(spec.mass), cap,
+                                                 ctypes.byref(slot)), "pcg_add_species")
+        else:
+            b = spec.beam
+            self._check(self.lib.pcg_add_beam(self.h, int(spec.id), spec.name.encode(),
+                                              float(spec.charge), float(spec.mass), cap,
+                                              int(b["macro_amount"]), b["start_time"],
+                                              b["radius"], b["density"], b["amount"], b["length"],
+                                              b["distance"], b["velocity"], ctypes.byref(slot)),
+                        "pcg_add_beam")
+        self.species.append(spec)
+        return slot.value
+
+    def set_particles(self, slot, r, z, vr, vphi, vz, w, append=False):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (r, z, vr, vphi, vz, w)]
+        fn = self.lib.pcg_append_species if append else self.lib.pcg_import_species
+        self._check(fn(self.h, slot, arrs[0].size, *[_dp(a) for a in arrs]), "pcg_import_species")
+
+    def count(self, slot) -> int:
+        n = ctypes.c_size_t()
+        self._check(self.lib.pcg_count(self.h, slot, ctypes.byref(n)), "pcg_count")
+        return n.value
+
+    def get_particles(self, slot) -> dict:
+        n = self.count(slot)
+        m = max(n, 1)
+        out = {k: np.zeros(m) for k in ("r", "z", "vr", "vphi", "vz", "w")}
+        cr = np.zeros(m, dtype=np.int32)
+        cz = np.zeros(m, dtype=np.int32)
+        got = ctypes.c_size_t()
+        self._check(self.lib.pcg_export_species(self.h, slot, m, *[_dp(out[k]) for k in
+                                                ("r", "z", "vr", "vphi", "vz", "w")],
+                                                cr.ctypes.data_as(_PI32), cz.ctypes.data_as(_PI32),
+                                                ctypes.byref(got)), "pcg_export_species")
+        out = {k: v[:n] for k, v in out.items()}
+        out["cell_r"] = cr[:n].astype(np.int64)
+        out["cell_z"] = cz[:n].astype(np.int64)
+        return out
+
+    # -- fields (Grid<double> with halo) -------------------------------------------
+    def set_field(self, which, arr):
+        idx = FIELD[which] if isinstance(which, str) else int(which)
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.shape == tuple(self.grid.shape)
+        self._check(self.lib.pcg_set_field(self.h, idx, _dp(a)), "pcg_set_field")
+
+    def get_field(self, which) -> np.ndarray:
+        idx = FIELD[which] if isinstance(which, str) else int(which)
+        a = np.zeros(self.grid.shape)
+        self._check(self.lib.pcg_export_field(self.h, idx, _dp(a)), "pcg_export_field")
+        return a
+
+    def fields(self) -> dict:
+        return {n: self.get_field(n) for n in FIELDS}
+
+    # -- the Domain façade (src/domain.cpp:86-204) -----------------------------------
+    def stage(self, name) -> int:
+        idx = STAGE[name] if isinstance(name, str) else int(name)
+        return self._check(self.lib.pcg_stage(self.h, idx), "pcg_stage")
+
+    def manage_beam(self): return self.stage("inject")
+    def weight_field_e(self): return self.stage("field_e")
+    def weight_field_h(self): return self.stage("field_h")
+    def push_particles(self): return self.stage("push")
+    def dump_particle_positions_to_old(self): return self.stage("dump_old")
+    def update_particles_coords(self): return self.stage("move")
+    def particles_back_position_to_rz(self): return self.stage("pos_rz")
+    def reflect(self): return self.stage("reflect")
+    def particles_back_velocity_to_rz(self): return self.stage("vel_rz")
+    def bind_cell_numbers(self): return self.stage("bind")
+    def particles_runaway_collector(self): return self.stage("collect")
+    def reset_current(self): return self.stage("reset_current")
+    def weight_current(self): return self.stage("current")
+
+    def step(self, n: int = 1) -> int:
+        """``n`` full steps (inject, E, H, advance particles, current) on the device."""
+        self._check(self.lib.pcg_step(self.h, int(n)), "pcg_step")
+        return 0
+
+    def synchronize(self):
+        self._check(self.lib.pcg_synchronize(self.h), "pcg_synchronize")
+
+    def diag(self) -> Diagnostics:
+        d = Diagnostics()
+        self._check(self.lib.pcg_diag(self.h, ctypes.byref(d)), "pcg_diag")
+        return d
+
+    @property
+    def time(self) -> float:
+        return self.diag().time
+
+    @property
+    def removed(self) -> int:
+        return int(self.diag().removed)
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.pcg_get_stream(self.h, ctypes.byref(s)), "pcg_get_stream")
+        return s.value or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

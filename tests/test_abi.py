@@ -1,0 +1,44 @@
+"""The C-ABI library loads and exports every entry point include/pcg.h declares.
+
+No compute call is made here (this runs on machines without a GPU).
+"""
+import ctypes
+import os
+import re
+
+from picopic_b200 import _ffi
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    text = open(os.path.join(REPO, "include", header)).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pcg_\w+)\s*\(", text, re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = ctypes.CDLL(_ffi.LIB_PATH)
+    names = _declared("pcg.h")
+    assert len(names) >= 17
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_header():
+    assert set(_declared("pcg.h")) <= set(_ffi.SIGNATURES)
+
+
+def test_abi_version_without_device():
+    lib = _ffi.load()
+    assert lib.pcg_abi_version() == 1
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    import pytest
+    saved = _ffi._lib
+    _ffi._lib = None
+    try:
+        with pytest.raises(ImportError):
+            _ffi.load(str(tmp_path / "libpcg.so"))
+    finally:
+        _ffi._lib = saved

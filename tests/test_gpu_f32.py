@@ -1,0 +1,79 @@
+"""The single-precision production path against the double-precision oracle.
+
+The float path keeps positions as (cell, offset) and rewrites the
+reference formulas in those coordinates; it is compared with the oracle on
+the same seeded inputs.  Tolerances (stated relative to the array maximum):
+fields after one step within RTOL_FIELD_1 = 2e-4 (float rounding in the
+deposit of ~1e4 particles), particle positions within 1e-6 and velocities
+within 1e-5; per-cell particle counts may differ only for particles within
+float rounding of a cell boundary.
+"""
+import numpy as np
+import pytest
+
+from oracle.harness import FIELDS, OracleSim
+from tests.cases import ELECTRONS, IONS, beam_spec, particles, random_fields, small_grid
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FIELD_1 = 2e-4
+RTOL_POS = 1e-6
+RTOL_VEL = 1e-5
+COMBOS = [(p, c) for p in ("borisrel", "boris", "vay", "hc") for c in ("vb", "zigzag")]
+
+
+def _pair(grid, pusher, current, species, n, seed):
+    from picopic_b200 import Domain
+    gpu = Domain(grid, pusher=pusher, current=current, precision="f32", seed=7)
+    orc = OracleSim(grid, pusher, current)
+    for sp in species:
+        gpu.add(sp, capacity=20000)
+        orc.add(sp)
+    for i, sp in enumerate(species):
+        if sp.beam is None:
+            p = particles(grid, n, seed + i, mass=sp.mass, boost=30.0 if sp.mass == 1 else 150.0)
+            gpu.set_particles(i, *p)
+            orc.set_particles(i, *p)
+    for name, a in random_fields(grid, seed).items():
+        gpu.set_field(name, a)
+        orc.set_field(name, a)
+    orc.set_rng("philox", 7)
+    return gpu, orc
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300) if a.size else 0.0
+
+
+@pytest.mark.parametrize("pusher,current", COMBOS)
+def test_f32_one_step(pusher, current):
+    grid = small_grid()
+    species = [ELECTRONS, IONS, beam_spec(grid)]
+    gpu, orc = _pair(grid, pusher, current, species, 3000, seed=3)
+    gpu.step(1)
+    assert orc.step(1) == 0
+    for k in FIELDS:
+        assert _rel(gpu.get_field(k), orc.get_field(k)) <= RTOL_FIELD_1, k
+    for sid in range(len(species)):
+        pg, po = gpu.get_particles(sid), orc.get_particles(sid)
+        assert pg["r"].size == po["r"].size
+        assert _rel(pg["r"], po["r"]) <= RTOL_POS and _rel(pg["z"], po["z"]) <= RTOL_POS
+        for k in ("vr", "vphi", "vz"):
+            assert _rel(pg[k], po[k]) <= RTOL_VEL, (sid, k)
+        assert np.mean(pg["cell_r"] != po["cell_r"]) < 1e-3
+        assert np.mean(pg["cell_z"] != po["cell_z"]) < 1e-3
+
+
+def test_f32_ten_steps_field_energy():
+    """Ten steps of the float path keep the field energy within 1e-3 of the
+    double oracle on a small noisy case."""
+    grid = small_grid()
+    species = [ELECTRONS, IONS]
+    gpu, orc = _pair(grid, "borisrel", "vb", species, 3000, seed=5)
+    gpu.step(10)
+    assert orc.step(10) == 0
+    def energy(fields):
+        return sum(float(np.sum(fields[k][2:-2, 2:-2] ** 2)) for k in ("e_r", "e_phi", "e_z"))
+    eg = energy({k: gpu.get_field(k) for k in ("e_r", "e_phi", "e_z")})
+    eo = energy({k: orc.get_field(k) for k in ("e_r", "e_phi", "e_z")})
+    assert abs(eg - eo) / eo < 1e-3
