@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Throughput of the PIC step: particle-steps/s on one B200.
+
+Workload (default): the beam-plasma wakefield configuration — a 256 x 4096
+cell r-z grid (dr = dz = 1e-4 m), electron and proton plasma at 1e17 m^-3
+with 50 macroparticles per cell per species (Te = 1 eV, Ti = 0.1 eV),
+a 5 MeV electron bunch (1e16 m^-3, radius 2 mm, Gaussian sigma_z = 1 mm,
+100 macroparticles per cell of the bunch) injected at z = 0, relativistic
+Boris pusher, Villasenor-Buneman current, Yee fields, dt = 0.5 Courant.
+The plasma is seeded on the device (Philox); nothing is read from disk.
+
+Timed: exactly K steps after W warm-up steps, CUDA events on the library's
+stream, a barrier and device synchronisation on both sides, the maximum over
+ranks.  The particle arrays (2.9 GB) exceed L2 (126 MB), so no flush is
+needed between steps.  One JSON line is printed by rank 0.
+
+`--impl reference` times the reference's own hot-path sources (compiled by
+oracle/Makefile.ref with its release flags) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "particle-steps/s on 1 B200 (FP32 vs FP64 oracle); learned vs binary collision speedup"
+UNIT = "particle-steps/s"
+BYTES_PER_PARTICLE_F32 = 52   # read cell, 2 offsets, 3 velocities, weight (28 B); write all but weight (24 B)
+BYTES_PER_PARTICLE_F64 = 88   # read r, z, 3 velocities, weight (48 B); write r, z, 3 velocities (40 B)
+
+C = 3.0e8
+DR = 1e-4
+WORKLOAD = dict(
+    name="beam-plasma wakefield 256x4096, 50 ppc/species e+p, 5 MeV Gaussian bunch",
+    nr=256, nz=4096, dr=DR, dz=DR, density=1e17, ppc=50, te=1.0, ti=0.1,
+    beam_energy_mev=5.0, beam_density=1e16, beam_radius=2e-3, beam_sigma_z=1e-3,
+    beam_ppc=100, pusher="borisrel", current="vb")
+
+
+def dt_courant(dr):
+    return 0.5 * dr / (C * np.sqrt(2.0))
+
+
+def beam_velocity(mev):
+    gamma = 1.0 + mev * 1e6 * 1.6e-19 / (9.1e-31 * C * C)
+    return C * np.sqrt(1.0 - 1.0 / gamma ** 2)
+
+
+def scaled(w, nz=None, ppc=None):
+    w = dict(w)
+    if nz:
+        w["nz"] = nz
+    if ppc:
+        w["ppc"] = ppc
+    return w
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+
+def make_domain(w, precision, seed=1234, host_beam=False, device=0):
+    from picopic_b200 import Domain, Geometry
+    g = Geometry(w["nr"], w["nz"], w["nr"] * w["dr"], w["nz"] * w["dz"], dt_courant(w["dr"]))
+    d = Domain(g, pusher=w["pusher"], current=w["current"], precision=precision, seed=seed,
+               device=device)
+    n = w["nr"] * w["nz"] * w["ppc"]
+    vb = beam_velocity(w["beam_energy_mev"])
+    cells_b = (w["beam_radius"] / w["dr"]) * (6 * w["beam_sigma_z"] / w["dz"])
+    nb = int(w["beam_ppc"] * cells_b * 1.05) + 4096
+    e = d.add(_spec("electrons", -1, 1, 1), capacity=n)
+    i = d.add(_spec("ions", 1, 1836, 2), capacity=n)
+    if host_beam:
+        b = d.add(_spec("beam_electrons", -1, 1, 1000), capacity=nb)
+    else:
+        b = d.add(_spec("beam_electrons", -1, 1, 1000, beam=dict(
+            macro_amount=max(1, int(w["beam_ppc"] * cells_b)), start_time=0.0,
+            radius=w["beam_radius"], density=w["beam_density"], amount=1,
+            length=6 * w["beam_sigma_z"], distance=0.0, velocity=vb)), capacity=nb)
+        d.set_beam_profile(b, "gaussian", w["beam_sigma_z"], w["beam_ppc"])
+    d.seed_plasma(e, n, w["density"], w["te"], seed)
+    d.seed_plasma(i, n, w["density"], w["ti"], seed + 1)
+    return d, (e, i, b), g, vb
+
+
+class _spec:
+    def __init__(self, name, charge, mass, id, beam=None):
+        self.name, self.charge, self.mass, self.id, self.beam = name, charge, mass, id, beam
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    p = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def timed_steps(d, K, stream_ptr):
+    import torch
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    d.step(K)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_gpu(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
+    d, slots, g, vb = make_domain(w, "f32", seed=1234 + 7919 * rank, device=local)
+    d.step(args.warmup)
+    d.synchronize()
+    p0 = d.diag().particle_steps
+    d.kernel_times()
+    d.enable_timers(True)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = timed_steps(d, args.steps, d.stream)
+    clocks = sampler.stop()
+    barrier()
+    ms_max = allmax(ms)
+    kt = d.kernel_times()
+    d.enable_timers(False)
+    diag = d.diag()
+    psteps = allsum(float(diag.particle_steps - p0))
+    value = psteps / (ms_max * 1e-3)
+    live = diag.particles
+    # roofline of the dominant kernel: algorithmic bytes of one step's particle
+    # launches over their measured duration
+    part_ms, part_n = kt["particles"]
+    per_launch_ms = part_ms / max(part_n, 1)
+    particles_per_step = (diag.particle_steps - p0) / args.steps
+    alg_bytes = BYTES_PER_PARTICLE_F32 * particles_per_step
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tr = ncu_traffic().get("f32_particle_step")
+    if tr:
+        traffic = tr["bytes_per_particle"] * particles_per_step
+    f64 = None
+    e2e = None
+    cpu = None
+    if not args.no_f64:
+        del d
+        torch.cuda.empty_cache()
+        d64, _, _, _ = make_domain(w, "f64", seed=1234 + 7919 * rank, device=local)
+        d64.step(max(2, args.warmup // 2))
+        d64.synchronize()
+        q0 = d64.diag().particle_steps
+        k64 = max(3, args.steps // 5)
+        barrier()
+        ms64 = allmax(timed_steps(d64, k64, d64.stream))
+        q1 = d64.diag().particle_steps
+        f64 = {"value": allsum(float(q1 - q0)) / (ms64 * 1e-3), "unit": UNIT,
+               "ms_per_step": ms64 / k64, "steps": k64,
+               "bytes_per_particle_step": BYTES_PER_PARTICLE_F64}
+        del d64
+        torch.cuda.empty_cache()
+    if not args.no_e2e:
+        e2e = run_e2e(w, args, rank, local, barrier, allmax, allsum)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(w)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["name"], "grid": [w["nr"], w["nz"]], "particles": int(live),
+                       "pusher": w["pusher"], "current": w["current"], "precision": "f32",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (particle arrays 2.9 GB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "f32 fused particle step",
+                         "algorithmic_bytes_per_particle": BYTES_PER_PARTICLE_F32,
+                         "kernel_ms_per_step": per_launch_ms},
+            "kernel_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in kt.items() if v[1]},
+            "clocks": clocks,
+            "f64": f64,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(sum(v[1] for v in kt.values()) * 1 + args.steps * 2),
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_e2e(w, args, rank, local, barrier, allmax, allsum):
+    """Same metric through the C ABI with host buffers: every step appends
+    that step's bunch slice from pinned host memory and reads the device
+    status block back (pcg_synchronize)."""
+    import torch
+    d, slots, g, vb = make_domain(w, "f32", seed=4321 + 7919 * rank, host_beam=True, device=local)
+    K = args.steps
+    rng = np.random.default_rng(99 + rank)
+    dl = vb * g.dt
+    mps = w["beam_ppc"] * (w["beam_radius"] / w["dr"]) * (dl / w["dz"])
+    slab = np.pi * (w["beam_radius"] ** 2 - (0.5 * w["dr"]) ** 2) * dl
+    w0 = w["beam_density"] * slab / mps
+    steps_total = args.warmup + K
+    slices = []
+    for m in range(steps_total):
+        cnt = int(np.floor((m + 1) * mps) - np.floor(m * mps))
+        u0, u1 = rng.random(cnt), rng.random(cnt)
+        r = np.sqrt((0.5 * w["dr"]) ** 2 + u0 * (w["beam_radius"] ** 2 - (0.5 * w["dr"]) ** 2))
+        z = dl * u1 + 0.5 * w["dz"]
+        s = (m + 1) * dl - dl * u1 - 3 * w["beam_sigma_z"]
+        wt = w0 * np.exp(-s * s / (2 * w["beam_sigma_z"] ** 2))
+        buf = torch.empty((6, cnt), dtype=torch.float64, pin_memory=True).numpy()
+        buf[0], buf[1], buf[2], buf[3], buf[4], buf[5] = r, z, 0.0, 0.0, vb, wt
+        slices.append(buf)
+    beam = slots[2]
+
+    def one(m):
+        b = slices[m]
+        if b.shape[1]:
+            d.set_particles(beam, *b, append=True)
+        d.step(1)
+        d.synchronize()
+
+    for m in range(args.warmup):
+        one(m)
+    p0 = d.diag().particle_steps
+    h2d = sum(slices[m].nbytes for m in range(args.warmup, steps_total))
+    barrier()
+    t0 = time.perf_counter()
+    for m in range(args.warmup, steps_total):
+        one(m)
+    t1 = time.perf_counter()
+    barrier()
+    el = allmax(t1 - t0)
+    p1 = d.diag().particle_steps
+    del d
+    torch.cuda.empty_cache()
+    return {"value": allsum(float(p1 - p0)) / el, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+            "d2h_bytes_per_step": 32, "ms_per_step": el * 1e3 / K,
+            "path": "pcg_append_species (pinned host, bunch slice) + pcg_step(1) + pcg_synchronize"}
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (the reference's own sources, compiled by oracle/Makefile.ref)
+
+def _plasma_sample(w, nz, seed):
+    """Host-generated plasma of the same distribution on a z-slab."""
+    rng = np.random.default_rng(seed)
+    R, L, dr, dz = w["nr"] * w["dr"], nz * w["dz"], w["dr"], w["dz"]
+    n = w["nr"] * nz * w["ppc"]
+    out = []
+    for mass, T in ((1.0, w["te"]), (1836.0, w["ti"])):
+        r0, r1 = 0.5 * dr, R - 0.5 * dr
+        r = np.sqrt(r0 ** 2 + rng.random(n) * (r1 ** 2 - r0 ** 2))
+        z = 0.5 * dz + rng.random(n) * (L - dz)
+        s = np.sqrt(T * 1.6e-19 / (mass * 9.1e-31))
+        v = rng.normal(size=(3, n)) * s
+        wt = np.full(n, w["density"] * np.pi * (r1 ** 2 - r0 ** 2) * (L - dz) / n)
+        out.append((r, z, v[0], v[1], v[2], wt))
+    return out
+
+
+def _ref_domain(w, nz, seed):
+    from oracle.harness import GridSpec, RefSim, SpeciesSpec, reference_available, OracleSim
+    grid = GridSpec(w["nr"], nz, w["nr"] * w["dr"], nz * w["dz"], dt_courant(w["dr"]))
+    if reference_available("borisrel", "vb", perf=True):
+        sim, kind = RefSim(grid, "borisrel", "vb", perf=True), "reference"
+    else:
+        sim, kind = OracleSim(grid, "borisrel", "vb"), "port"
+    sim.add(SpeciesSpec("electrons", -1, 1, id=1))
+    sim.add(SpeciesSpec("ions", 1, 1836, id=2))
+    n = 0
+    for sid, p in enumerate(_plasma_sample(w, nz, seed)):
+        sim.set_particles(sid, *p)
+        n += p[0].size
+    return sim, kind, n
+
+
+def cpu_baseline(w, nz=256, steps=2):
+    """One core, one domain: a 256 x 256 z-slab of the workload (6.6e6
+    particles), 2 full steps of the reference step order."""
+    sim, kind, n = _ref_domain(w, nz, 7)
+    sim.step(1)
+    t0 = time.perf_counter()
+    sim.step(steps)
+    el = time.perf_counter() - t0
+    return {"value": n * steps / el, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{w['nr']}x{nz} z-slab of the workload, {n} particles, {steps} steps, "
+                      "reference hot path compiled with its release flags"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
+    threads = os.cpu_count() or 1
+    nz = 64 if not args.small else 32
+    sims = []
+    kind = None
+    for t in range(threads):
+        s, kind, n = _ref_domain(w, nz, 100 + t)
+        sims.append((s, n))
+    for s, _ in sims:  # one warm-up step per domain
+        s.step(1)
+    steps = max(1, args.steps // 25)
+
+    def work(s):
+        s.step(steps)
+
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=work, args=(s,)) for s, _ in sims]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    el = time.perf_counter() - t0
+    total = sum(n for _, n in sims) * steps
+    value = total / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": steps, "warmup": 1, "ms_per_step": el * 1e3 / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["name"], "sample": f"{threads} domains of {w['nr']}x{nz} cells, "
+                                                        f"one per host thread"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{threads} independent {w['nr']}x{nz} z-slab domains "
+                                       f"({sum(n for _, n in sims)} particles), {steps} steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="a reduced grid for quick checks")
+    ap.add_argument("--no-f64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

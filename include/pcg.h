@@ -179,6 +179,39 @@ int pcg_export_species(pcg_handle* h, int slot, size_t cap, double* r, double* z
                        double* vphi, double* vz, double* w, int32_t* cell_r, int32_t* cell_z,
                        size_t* n);
 
+/* Seed a species on the device with `n` macroparticles of a uniform
+ * plasma filling the region between the reflecting walls: r^2 uniform in
+ * [(dr/2)^2, (R-dr/2)^2], z uniform in [dz/2, L-dz/2], Maxwellian velocity
+ * components of variance T*e/m, equal weights density*volume/n.  The
+ * random numbers are Philox4x32-10 keyed by `seed` and the species slot.
+ * Replaces SpecieP::fullyfill_spatial_distribution + velocity_distribution
+ * (specieP.cpp:79-478) as the source of synthetic initial conditions. */
+int pcg_seed_plasma(pcg_handle* h, int slot, size_t n, double density, double temperature_ev,
+                    uint64_t seed);
+
+/* Longitudinal bunch profile of a beam.  PCG_PROFILE_RECTANGLE is BeamP
+ * (beamP.cpp:71-157).  PCG_PROFILE_GAUSSIAN injects a bunch of density
+ * density*exp(-(s-3 sigma_z)^2/(2 sigma_z^2)) over 6 sigma_z behind its
+ * head s = 0, with macro_per_cell macroparticles per cell of the bunch
+ * cylinder; the reference parses a `profile` key but only injects
+ * rectangles (cfg.cpp:366-367). */
+#define PCG_PROFILE_RECTANGLE 0
+#define PCG_PROFILE_GAUSSIAN 1
+int pcg_set_beam_profile(pcg_handle* h, int slot, int profile, double sigma_z,
+                         double macro_per_cell);
+
+/* Device time per kernel class, measured with CUDA events on the handle's
+ * stream while enabled; pcg_kernel_times returns milliseconds and launch
+ * counts accumulated since the last call and resets them. */
+#define PCG_TIMER_FIELD_E 0
+#define PCG_TIMER_FIELD_H 1
+#define PCG_TIMER_INJECT 2
+#define PCG_TIMER_PARTICLES 3 /* fused push/move/reflect/bind(/deposit) */
+#define PCG_TIMER_DEPOSIT 4   /* separate deposit kernel of the double path */
+#define PCG_TIMER_COUNT 5
+int pcg_enable_timers(pcg_handle* h, int on);
+int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n);
+
 int pcg_set_field(pcg_handle* h, int which, const double* src);
 int pcg_export_field(pcg_handle* h, int which, double* dst);
 

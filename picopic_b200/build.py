@@ -30,6 +30,7 @@ UNITS = {
     "pcg_util.cu": [],
     "pcg_kernels_f64.cu": ["--fmad=false"],
     "pcg_kernels_f32.cu": [],
+    "pcg_init.cu": [],
 }
 
 

@@ -16,6 +16,7 @@
 
 #include "pcg.h"
 #include "pcg_f32.h"
+#include "pcg_init.h"
 #include "pcg_kernels.h"
 #include "pcg_yee.cuh"
 
@@ -35,6 +36,9 @@ struct Species {
   double start_time = 0, radius = 0, density = 0, bunch_length = 0, bunches_distance = 0,
          velocity = 0, finish_time = 0, domain_radius = 0, bunch_macro_amount = 0,
          macro_per_step = 0;
+  // PCG_PROFILE_GAUSSIAN
+  int profile = PCG_PROFILE_RECTANGLE;
+  double sigma_z = 0, gauss_mps = 0;
   // double layout
   double *r = nullptr, *z = nullptr, *vr = nullptr, *vphi = nullptr, *vz = nullptr,
          *w = nullptr, *r_old = nullptr, *z_old = nullptr;
@@ -68,6 +72,14 @@ struct pcg_handle {
   bool started = false;  // particles imported or stepped: species list frozen
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  double* staging = nullptr;  // host-to-device particle staging, reused
+  size_t staging_n = 0;
+  // kernel timers: event pairs per class, recycled after each query
+  TileGrid tiles{};       // float path: tile sort geometry
+  int sort_interval = 16;  // float path: steps between tile sorts
+  bool timers = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
   std::string err;
 };
 
@@ -169,7 +181,7 @@ int alloc_species(pcg_handle* h, Species& s) {
     for (double** a : arrs)
       if ((rc = dalloc(h, a, s.cap)) != PCG_OK) return rc;
   } else {
-    if ((rc = f32_alloc_species(s.f32, s.cap)) != 0)
+    if ((rc = f32_alloc_species(s.f32, s.cap, h->tiles)) != 0)
       return fail(h, PCG_ERR_NOMEM, "cudaMalloc of a float species failed");
   }
   return PCG_OK;
@@ -215,6 +227,31 @@ int check_status(pcg_handle* h) {
 // reference's double arithmetic: returns how many particles to add now.
 unsigned beam_count(pcg_handle* h, Species& s, BeamInject* b, int slot) {
   unsigned count = 0;
+  if (s.profile == PCG_PROFILE_GAUSSIAN) {
+    // 6 sigma_z of bunch pass z = 0 starting at start_time; the number of
+    // macroparticles entering during step m is floor((m+1) a) - floor(m a).
+    const double since = h->t - s.start_time;
+    const double window = 6.0 * s.sigma_z / s.velocity;
+    if (since < 0 || since >= window) return 0;
+    const double m = floor(since / h->cfg.dt + 0.5);
+    count = (unsigned)(floor((m + 1) * s.gauss_mps) - floor(m * s.gauss_mps));
+    const double dr = h->g.dr, dz = h->g.dz;
+    b->seed = h->cfg.seed;
+    b->stream = 0x6265616du + (uint32_t)slot;
+    b->step = h->steps;
+    b->dl = s.velocity * h->cfg.dt;
+    b->half_z = dz / 2.;
+    b->velocity = s.velocity;
+    b->profile = 1;
+    b->r_min = 0.5 * dr;
+    b->radius = s.radius;
+    b->sigma = s.sigma_z;
+    b->head_dist = (m + 1) * b->dl;
+    // equal-volume macroparticles: the slab volume of one step over its count
+    const double slab = kPi * (s.radius * s.radius - b->r_min * b->r_min) * b->dl;
+    b->w0 = s.density * slab / s.gauss_mps;
+    return count;
+  }
   if (s.current_bunch < s.bunches_amount) {
     double bunch_start = s.start_time + (s.bunch_length + s.bunches_distance) / s.velocity * s.current_bunch;
     double bunch_finish = bunch_start + s.bunch_length / s.velocity;
@@ -237,7 +274,37 @@ unsigned beam_count(pcg_handle* h, Species& s, BeamInject* b, int slot) {
   return count;
 }
 
+// Kernel timers: an event pair around each timed launch group.
+cudaEvent_t timer_event(pcg_handle* h) {
+  if (!h->ev_pool.empty()) {
+    cudaEvent_t e = h->ev_pool.back();
+    h->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct TimerScope {
+  pcg_handle* h;
+  int cls;
+  cudaEvent_t a = nullptr, b = nullptr;
+  TimerScope(pcg_handle* hh, int c) : h(hh), cls(c) {
+    if (!h->timers) return;
+    a = timer_event(h);
+    b = timer_event(h);
+    cudaEventRecord(a, h->stream);
+  }
+  ~TimerScope() {
+    if (!h->timers) return;
+    cudaEventRecord(b, h->stream);
+    h->ev_used.push_back({cls, {a, b}});
+  }
+};
+
 int stage_inject(pcg_handle* h) {
+  TimerScope ts(h, PCG_TIMER_INJECT);
   for (size_t t = 0; t < h->sp.size(); ++t) {
     Species& s = h->sp[t];
     if (!s.beam) continue;
@@ -369,20 +436,27 @@ int fused_step(pcg_handle* h) {
   for (Species& s : h->sp) live += s.n;
   if (is_f64(h)) {
     // E consumes J of the previous step, then clears it for this step's deposit.
-    launch_yee_e_f64(yee_args<double>(h, h->f64, h->sig64, 1), h->stream);
-    launch_yee_h_f64(yee_args<double>(h, h->f64, h->sig64, 0), fixed, h->stream);
+    { TimerScope ts(h, PCG_TIMER_FIELD_E); launch_yee_e_f64(yee_args<double>(h, h->f64, h->sig64, 1), h->stream); }
+    { TimerScope ts(h, PCG_TIMER_FIELD_H); launch_yee_h_f64(yee_args<double>(h, h->f64, h->sig64, 0), fixed, h->stream); }
     FieldsF64 f = fields64(h);
-    if (h->cfg.current == PCG_CURRENT_VB)
-      CUDA_TRY(h, cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream));
-    for (size_t t = 0; t < h->sp.size(); ++t)
-      launch_advance_f64(h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
-                         h->cfg.current, h->reset, h->d_status, h->stream);
-    for (size_t t = 0; t < h->sp.size(); ++t)
-      launch_deposit_f64(h->g, f, view64(h, h->sp[t]), (int)t, fixed, h->cfg.current, h->reset,
-                         h->d_status, h->stream);
+    {
+      TimerScope ts(h, PCG_TIMER_PARTICLES);
+      if (h->cfg.current == PCG_CURRENT_VB)
+        CUDA_TRY(h, cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream));
+      for (size_t t = 0; t < h->sp.size(); ++t)
+        launch_advance_f64(h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
+                           h->cfg.current, h->reset, h->d_status, h->stream);
+    }
+    {
+      TimerScope ts(h, PCG_TIMER_DEPOSIT);
+      for (size_t t = 0; t < h->sp.size(); ++t)
+        launch_deposit_f64(h->g, f, view64(h, h->sp[t]), (int)t, fixed, h->cfg.current, h->reset,
+                           h->d_status, h->stream);
+    }
   } else {
-    f32_launch_yee_e(yee_args<float>(h, h->f32, h->sig32, 1), h->stream);
-    f32_launch_yee_h(yee_args<float>(h, h->f32, h->sig32, 0), fixed, h->stream);
+    { TimerScope ts(h, PCG_TIMER_FIELD_E); f32_launch_yee_e(yee_args<float>(h, h->f32, h->sig32, 1), h->stream); }
+    { TimerScope ts(h, PCG_TIMER_FIELD_H); f32_launch_yee_h(yee_args<float>(h, h->f32, h->sig32, 0), fixed, h->stream); }
+    TimerScope ts(h, PCG_TIMER_PARTICLES);
     F32Step st;
     st.g = h->g;
     for (int c = 0; c < 12; ++c) st.fld[c] = h->f32[c];
@@ -390,9 +464,12 @@ int fused_step(pcg_handle* h) {
     st.current = h->cfg.current;
     st.fixed = fixed;
     st.status = h->d_status;
+    st.tiles = h->tiles;
+    st.sort_interval = h->sort_interval;
     for (size_t t = 0; t < h->sp.size(); ++t) {
       Species& s = h->sp[t];
-      f32_launch_step(st, s.f32, s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream);
+      if (f32_step_species(st, s.f32, &s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream) != 0)
+        return fail(h, PCG_ERR_CUDA, "tile sort of species '" + s.name + "' failed");
     }
   }
   h->t += h->cfg.dt;
@@ -431,6 +508,7 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
   g.pml_r = cfg->pml_size[2] != 0; g.pml_z0 = cfg->pml_size[1] != 0; g.pml_zl = cfg->pml_size[3] != 0;
   h->t = cfg->t_start;
   h->nodes = (size_t)(g.nr + 4) * (size_t)g.ld;
+  h->tiles = f32_tile_grid(g);
   int rc = PCG_OK;
   auto bail = [&](int code) { pcg_destroy(h); return code; };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PCG_ERR_CUDA);
@@ -478,6 +556,9 @@ int pcg_destroy(pcg_handle* h) {
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
   cudaFree(h->reset);
   cudaFree(h->scratch);
+  cudaFree(h->staging);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  for (auto& u : h->ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
   for (Species& s : h->sp) {
     void* arrs[] = {s.r, s.z, s.vr, s.vphi, s.vz, s.w, s.r_old, s.z_old, s.phi, s.phi_old, s.sn,
                     s.cell_r, s.cell_z};
@@ -556,16 +637,23 @@ static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, con
   if (n0 + n > s.cap) return fail(h, PCG_ERR_CAPACITY, "species '" + s.name + "' capacity exceeded");
   h->started = true;
   if (n) {
-    double* stage = nullptr;
-    int rc = dalloc(h, &stage, 6 * n);
-    if (rc != PCG_OK) return rc;
+    if (h->staging_n < n) {  // grow the reusable staging buffer
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+      cudaFree(h->staging);
+      h->staging = nullptr;
+      h->staging_n = 0;
+      int rc = dalloc(h, &h->staging, 6 * n);
+      if (rc != PCG_OK) return rc;
+      h->staging_n = n;
+    }
+    double* stage = h->staging;
     const double* src[6] = {r, z, vr, vphi, vz, w};
     for (int a = 0; a < 6; ++a)
       CUDA_TRY(h, cudaMemcpyAsync(stage + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
     if (is_f64(h)) launch_import_f64(h->g, view64(h, s), n0, n, stage, h->stream);
     else f32_launch_import(h->g, s.f32, n0, n, stage, h->stream);
+    // the caller may reuse its host arrays once this call returns
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    cudaFree(stage);
   }
   s.n = n0 + n;
   return PCG_OK;
@@ -676,6 +764,75 @@ int pcg_step(pcg_handle* h, int nsteps) {
 int pcg_synchronize(pcg_handle* h) {
   if (!h) return PCG_ERR_ARG;
   return check_status(h);
+}
+
+int pcg_seed_plasma(pcg_handle* h, int slot, size_t n, double density, double temperature_ev,
+                    uint64_t seed) {
+  if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  if (!(density >= 0) || !(temperature_ev >= 0)) return fail(h, PCG_ERR_ARG, "negative density or temperature");
+  Species& s = h->sp[slot];
+  if (s.n + n > s.cap) return fail(h, PCG_ERR_CAPACITY, "species '" + s.name + "' capacity exceeded");
+  h->started = true;
+  const GridGeom& g = h->g;
+  const double r0 = 0.5 * g.dr, r1 = g.R - 0.5 * g.dr;
+  const double volume = kPi * (r1 * r1 - r0 * r0) * (g.L - g.dz);
+  PlasmaSeed p;
+  p.seed = seed;
+  p.stream = 0x706c6100u + (uint32_t)slot;
+  p.sigma_v = sqrt(temperature_ev * kElCharge / s.mass);
+  p.weight = n ? density * volume / (double)n : 0.0;
+  if (is_f64(h)) launch_seed_f64(g, p, view64(h, s), s.n, n, h->stream);
+  else {
+    if (s.n == 0) { s.f32.next_id = 0; s.f32.sorted_n = 0; }
+    launch_seed_f32(g, p, s.f32, s.n, n, h->stream);
+    s.f32.next_id += (unsigned)n;
+  }
+  s.n += n;
+  CUDA_TRY(h, cudaGetLastError());
+  return PCG_OK;
+}
+
+int pcg_set_beam_profile(pcg_handle* h, int slot, int profile, double sigma_z,
+                         double macro_per_cell) {
+  if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  Species& s = h->sp[slot];
+  if (!s.beam) return fail(h, PCG_ERR_ARG, "not a beam");
+  if (profile == PCG_PROFILE_RECTANGLE) {
+    s.profile = profile;
+    return PCG_OK;
+  }
+  if (profile != PCG_PROFILE_GAUSSIAN || !(sigma_z > 0) || !(macro_per_cell > 0))
+    return fail(h, PCG_ERR_ARG, "unknown profile or non-positive sigma/macro count");
+  s.profile = profile;
+  s.sigma_z = sigma_z;
+  // macroparticles per step: per cell of the bunch cylinder times the cells
+  // its cross-section covers times the cells it advances per step
+  s.gauss_mps = macro_per_cell * (s.radius / h->g.dr) * (s.velocity * h->cfg.dt / h->g.dz);
+  return PCG_OK;
+}
+
+int pcg_enable_timers(pcg_handle* h, int on) {
+  if (!h) return PCG_ERR_ARG;
+  h->timers = on != 0;
+  return PCG_OK;
+}
+
+int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n) {
+  if (!h || !ms || n < 0) return PCG_ERR_ARG;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < n; ++c) { ms[c] = 0; if (launches) launches[c] = 0; }
+  for (auto& u : h->ev_used) {
+    float t = 0;
+    CUDA_TRY(h, cudaEventElapsedTime(&t, u.second.first, u.second.second));
+    if (u.first < n) {
+      ms[u.first] += t;
+      if (launches) launches[u.first] += 1;
+    }
+    h->ev_pool.push_back(u.second.first);
+    h->ev_pool.push_back(u.second.second);
+  }
+  h->ev_used.clear();
+  return PCG_OK;
 }
 
 int pcg_get_stream(pcg_handle* h, void** stream) {

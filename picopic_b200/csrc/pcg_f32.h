@@ -1,6 +1,8 @@
 // pcg_f32.h — the single-precision production particle path: positions as a
 // packed int16 (cell_r, cell_z) pair plus float in-cell offsets, velocities
-// and weights in float, float field grids.
+// and weights in float, float field grids.  Particles are kept grouped by
+// tile (a rectangle of cells) so that one thread block deposits a tile's
+// current in shared memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,13 +18,29 @@ namespace pcg {
 template <typename Real>
 struct YeeArgs;
 
+// Tiles of tr x tz cells; a block's shared window adds `halo` cells per side.
+struct TileGrid {
+  int tr, tz, ntr, ntz, ntiles, halo;
+};
+
 // cell = (uint16)cell_r | cell_z << 16; a dead slot has cell < 0.
 struct SpeciesF32Buffers {
   int* cell = nullptr;
   float *off_r = nullptr, *off_z = nullptr;  // in-cell offsets in [0, 1), units of dr and dz
   float *vr = nullptr, *vphi = nullptr, *vz = nullptr;  // m/s
   float* w = nullptr;                                    // real particles per macroparticle
+  unsigned* id = nullptr;  // insertion order, to export in the reference's particle order
+  // second buffer set, the target of the tile sort
+  int* cell2 = nullptr;
+  float *off_r2 = nullptr, *off_z2 = nullptr, *vr2 = nullptr, *vphi2 = nullptr, *vz2 = nullptr,
+        *w2 = nullptr;
+  unsigned* id2 = nullptr;
+  unsigned* tile_start = nullptr;   // ntiles + 1: particles of tile t are [start[t], start[t+1])
+  unsigned* tile_cursor = nullptr;  // ntiles, scatter cursors
   size_t cap = 0;
+  size_t sorted_n = 0;       // [0, sorted_n) are grouped by tile; later slots were appended
+  int steps_since_sort = 1 << 30;
+  unsigned next_id = 0;
 };
 
 struct F32Step {
@@ -30,6 +48,8 @@ struct F32Step {
   float* fld[12];
   int pusher, current, fixed;
   DevStatus* status;
+  TileGrid tiles;
+  int sort_interval;  // steps between tile sorts
 };
 
 __host__ __device__ __forceinline__ int pack_cell(int ci, int ck) {
@@ -39,7 +59,8 @@ __host__ __device__ __forceinline__ int cell_r_of(int cell) { return (int)(short
 __host__ __device__ __forceinline__ int cell_z_of(int cell) { return cell >> 16; }
 constexpr int kDeadCell = (int)0x80000000u;
 
-int f32_alloc_species(SpeciesF32Buffers& b, size_t cap);
+TileGrid f32_tile_grid(const GridGeom& g);
+int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg);
 void f32_free_species(SpeciesF32Buffers& b);
 void f32_launch_yee_e(const YeeArgs<float>& a, cudaStream_t s);
 void f32_launch_yee_h(const YeeArgs<float>& a, int fixed, cudaStream_t s);
@@ -47,7 +68,10 @@ void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsig
                        const BeamInject& bi, cudaStream_t s);
 void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_t n,
                        const double* src, cudaStream_t s);
-void f32_launch_step(const F32Step& st, SpeciesF32Buffers& b, size_t n, double charge,
+// One step of a species; returns the new slot count (a tile sort drops dead
+// particles).  Sorts when the species was appended to without a sort or
+// `sort_interval` steps have passed.
+int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
                      double mass, int is_beam, cudaStream_t s);
 void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s);
 int f32_compact(SpeciesF32Buffers& b, const unsigned* idx, size_t kept, cudaStream_t s);

@@ -277,23 +277,33 @@ __device__ __forceinline__ void g_terms(float t, float* h, float* m) {
   }
 }
 
+// Where the current goes: a shared-memory window of the tile a block works
+// on (nodes [i0, i0+wr) x [k0, k0+wz)), and the global grid for anything
+// outside it.  comp: 0 J_r, 1 J_phi, 2 J_z.
 struct Dep {
-  float* Jr;
-  float* Jp;
-  float* Jz;
+  float* J[3];
   int ld;
-  __device__ __forceinline__ void add(float* J, int i, int k, float v) const {
-    atomicAdd(J + (long long)(i + 2) * ld + (k + 2), v);
+  float* sJ;  // 3 planes of wr x wz floats, or null
+  int i0, k0, wr, wz;
+  __device__ __forceinline__ void add(int comp, int i, int k, float v) const {
+    const int li = i - i0, lk = k - k0;
+    if (sJ && (unsigned)li < (unsigned)wr && (unsigned)lk < (unsigned)wz)
+      atomicAdd(sJ + (comp * wr + li) * wz + lk, v);
+    else
+      atomicAdd(J[comp] + (long long)(i + 2) * ld + (k + 2), v);
   }
 };
 
-// simple_current_distribution for cell (i, k); points relative to that cell.
+// simple_current_distribution for cell (i, k): start point (ao, bo) relative
+// to that cell and the displacement (dx, dy).  Displacements are carried
+// exactly (from the velocity, split by path fractions), never differenced
+// from rounded offsets, so the MNZL test below means what it means in the
+// reference's double arithmetic.
 __device__ __forceinline__ void vb_simple(const StepArgs& a, const Dep& d, float q, int i, int k,
-                                          float ao, float bo, float an, float bn) {
-  const float dx = an - ao, dy = bn - bo;
+                                          float ao, float bo, float dx, float dy) {
   if (fabsf(dx) < a.mnzl_r || fabsf(dy) < a.mnzl_z) return;  // currentVB.cpp:45-46
   const float fi = (float)i;
-  const float xo = fi + ao, xn = fi + an;
+  const float xo = fi + ao, xn = xo + dx;
   float h, m;
   g_terms(dx / xo, &h, &m);
   const float qz = q * a.qz * dy;
@@ -303,24 +313,25 @@ __device__ __forceinline__ void vb_simple(const StepArgs& a, const Dep& d, float
     const float hh = cc * h / xo;
     const float A = (1.f - ao) * (2.f * fi + ao) / xo - lin + hh;
     const float B = ao * (2.f * fi + 1.f + ao) / xo + lin - hh;
-    d.add(d.Jz, i, k, qz * A / fi);
-    d.add(d.Jz, i + 1, k, qz * B / (fi + 1.f));
+    d.add(2,i, k, qz * A / fi);
+    d.add(2,i + 1, k, qz * B / (fi + 1.f));
   } else {
-    d.add(d.Jz, i, k, 8.f * qz * (1.f - ao - 0.5f * dx));
-    d.add(d.Jz, i + 1, k, qz * (1.f + ao + 0.5f * dx));
+    d.add(2,i, k, 8.f * qz * (1.f - ao - 0.5f * dx));
+    d.add(2,i + 1, k, qz * (1.f + ao + 0.5f * dx));
   }
   const float c = 0.5f * fi * (fi + 1.f);
   const float qr = q * a.qr / (fi + 0.5f);
   const float bb = 1.f - bo;
   const float cx = c / xo;
-  d.add(d.Jr, i, k, qr * (dx * (0.5f * bb - 0.25f * dy) + cx * (dx * bb / xn + dy * m)));
-  d.add(d.Jr, i, k + 1, qr * (dx * (0.5f * bo + 0.25f * dy) + cx * (dx * bo / xn - dy * m)));
+  d.add(0,i, k, qr * (dx * (0.5f * bb - 0.25f * dy) + cx * (dx * bb / xn + dy * m)));
+  d.add(0,i, k + 1, qr * (dx * (0.5f * bo + 0.25f * dy) + cx * (dx * bo / xn - dy * m)));
 }
 
-// strict_motion_distribution (:500-729); X*, Y* relative to the new cell.
+// strict_motion_distribution (:500-729).  (Xo, Yo) is the old point relative
+// to the new cell, (dX, dY) the exact displacement, (Xn, Yn) the new offsets.
 __device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float q, int in, int kn,
-                                          float Xo, float Yo, float Xn, float Yn) {
-  const float dX = Xn - Xo, dY = Yn - Yo;
+                                          float Xo, float Yo, float dX, float dY, float Xn,
+                                          float Yn) {
   const bool sr = fabsf(dX) < a.mnzl_r, sz = fabsf(dY) < a.mnzl_z;
   if (sr && sz) return;
   const float fi = (float)in;
@@ -333,21 +344,25 @@ __device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float
     const float up = qz * Xn * (2.f * fi + 1.f + Xn) / ((fi + 1.f) * xn);
     switch (kn - ko) {
       case 0:
-        d.add(d.Jz, in, kn, lo * dY);
-        d.add(d.Jz, in + 1, kn, up * dY);
+        d.add(2,in, kn, lo * dY);
+        d.add(2,in + 1, kn, up * dY);
         break;
-      case 1:
-        d.add(d.Jz, in, kn - 1, lo * (0.f - Yo));
-        d.add(d.Jz, in + 1, kn - 1, up * (0.f - Yo));
-        d.add(d.Jz, in, kn, lo * Yn);
-        d.add(d.Jz, in + 1, kn, up * Yn);
+      case 1: {  // crossed y = kn: first part in row kn-1
+        const float d1 = 0.f - Yo, d2 = dY - d1;
+        d.add(2,in, kn - 1, lo * d1);
+        d.add(2,in + 1, kn - 1, up * d1);
+        d.add(2,in, kn, lo * d2);
+        d.add(2,in + 1, kn, up * d2);
         break;
-      case -1:
-        d.add(d.Jz, in, kn + 1, lo * (1.f - Yo));
-        d.add(d.Jz, in + 1, kn + 1, up * (1.f - Yo));
-        d.add(d.Jz, in, kn, lo * (Yn - 1.f));
-        d.add(d.Jz, in + 1, kn, up * (Yn - 1.f));
+      }
+      case -1: {  // crossed y = kn+1: first part in row kn+1
+        const float d1 = 1.f - Yo, d2 = dY - d1;
+        d.add(2,in, kn + 1, lo * d1);
+        d.add(2,in + 1, kn + 1, up * d1);
+        d.add(2,in, kn, lo * d2);
+        d.add(2,in + 1, kn, up * d2);
         break;
+      }
       default: break;
     }
     return;
@@ -358,8 +373,8 @@ __device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float
   const float ldz = 1.f - Yn, rdz = Yn;
   auto put = [&](int i, float br) {
     const float wj = q * a.qr * 0.5f / ((float)i + 0.5f) * br;
-    d.add(d.Jr, i, kn, wj * ldz);
-    d.add(d.Jr, i, kn + 1, wj * rdz);
+    d.add(0,i, kn, wj * ldz);
+    d.add(0,i, kn + 1, wj * rdz);
   };
   const float dr2 = a.dr_m * a.dr_m;
   switch (in - io) {
@@ -367,9 +382,8 @@ __device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float
       put(in, dX * (1.f + fi * (fi + 1.f) / (xo * xn)));
       break;
     case 1: {
-      const float d1 = 0.f - Xo;  // to the boundary at x = in
+      const float d1 = 0.f - Xo, d2 = dX - d1;  // to and from the boundary x = in
       put(in - 1, d1 * (1.f + (fi - 1.f) / xo));
-      const float d2 = Xn;
       const float r0 = fi + 0.5f;
       const float br = a.fixed ? d2 * (1.f + (fi + 1.f) / xn)
                                : d2 - r0 * r0 / xn + r0 * r0 * dr2 / fi + 0.25f / xn - 0.25f / fi;  // :673
@@ -377,9 +391,8 @@ __device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float
       break;
     }
     case -1: {
-      const float d1 = 1.f - Xo;
+      const float d1 = 1.f - Xo, d2 = dX - d1;  // to and from the boundary x = in+1
       put(in + 1, d1 * (1.f + (fi + 2.f) / xo));
-      const float d2 = Xn - 1.f;
       const float r0 = fi + 0.5f;
       const float br = a.fixed ? d2 * (1.f + fi / xn)
                                : d2 - r0 * r0 / xn + r0 * r0 * dr2 / (fi + 1.f) + 0.25f / xn - 0.25f / (fi + 1.f);  // :714
@@ -402,65 +415,54 @@ __device__ __forceinline__ void vb_azimuthal(const StepArgs& a, const Dep& d, fl
   const bool i0 = in >= 0 && in < a.nr, i1 = in + 1 < a.nr;
   const bool k0 = kn >= 0 && kn < a.nz, k1 = kn + 1 < a.nz;
   // the halo of J_phi is cleared before the rz deposit (currentVB.cpp:177)
-  if (i0 && k0) d.add(d.Jp, in, kn, qp * w0 * (1.f - Ym));
-  if (i1 && k0) d.add(d.Jp, in + 1, kn, qp * w1 * (1.f - Ym));
-  if (i0 && k1) d.add(d.Jp, in, kn + 1, qp * w0 * Ym);
-  if (i1 && k1) d.add(d.Jp, in + 1, kn + 1, qp * w1 * Ym);
+  if (i0 && k0) d.add(1,in, kn, qp * w0 * (1.f - Ym));
+  if (i1 && k0) d.add(1,in + 1, kn, qp * w1 * (1.f - Ym));
+  if (i0 && k1) d.add(1,in, kn + 1, qp * w0 * Ym);
+  if (i1 && k1) d.add(1,in + 1, kn + 1, qp * w1 * Ym);
 }
 
-// rz_current_distribution (:175-396); old point (Xo, Yo) relative to the
-// new cell (in, kn), new point (Xn, Yn) in [0, 1)^2.
+// rz_current_distribution (:175-396).  (Xo, Yo): old point relative to the
+// new cell (in, kn); (dX, dY): the exact displacement; (Xn, Yn): the new
+// offsets.  Crossings split the displacement by path fractions.
 __device__ __forceinline__ bool vb_rz(const StepArgs& a, const Dep& d, float q, int in, int kn,
-                                      float Xo, float Yo, float Xn, float Yn) {
+                                      float Xo, float Yo, float dX, float dY, float Xn, float Yn) {
   const int di = (int)floorf(Xo), dk = (int)floorf(Yo);  // old cell - new cell
   if (abs(di) > 1 || (a.fixed && abs(dk) > 1)) return false;
-  if (fabsf(Xn - Xo) < a.mnzl_r || fabsf(Yn - Yo) < a.mnzl_z) {
-    vb_strict(a, d, q, in, kn, Xo, Yo, Xn, Yn);
+  if (fabsf(dX) < a.mnzl_r || fabsf(dY) < a.mnzl_z) {
+    vb_strict(a, d, q, in, kn, Xo, Yo, dX, dY, Xn, Yn);
     return true;
   }
   const int res = abs(di) + abs(dk);
-  // Segment helper: points relative to (in, kn), deposited in cell (in+ci, kn+ck).
-  auto seg = [&](float x0, float y0, float x1, float y1, int ci, int ck) {
-    vb_simple(a, d, q, in + ci, kn + ck, x0 - ci, y0 - ck, x1 - ci, y1 - ck);
+  // part of the path from fraction f0 to f1 (0..1), deposited in cell (in+ci, kn+ck)
+  auto seg = [&](float f0, float f1, int ci, int ck) {
+    vb_simple(a, d, q, in + ci, kn + ck, Xo + f0 * dX - ci, Yo + f0 * dY - ck, (f1 - f0) * dX,
+              (f1 - f0) * dY);
   };
-  const float sl = (Yn - Yo) / (Xn - Xo);  // dz/dr in cells
   if (res == 0) {
-    seg(Xo, Yo, Xn, Yn, 0, 0);
+    seg(0.f, 1.f, 0, 0);
   } else if (res == 1) {
-    if (di != 0) {
-      const float xb = di > 0 ? 1.f : 0.f;  // boundary x = in+1 (from outside) or x = in
-      const float yb = Yo + (xb - Xo) * sl;
-      seg(Xo, Yo, xb, yb, di, 0);
-      seg(xb, yb, Xn, Yn, 0, 0);
-    } else {
-      const float yb = dk > 0 ? 1.f : 0.f;
-      const float xb = Xo + (yb - Yo) / sl;
-      seg(Xo, Yo, xb, yb, 0, dk);
-      seg(xb, yb, Xn, Yn, 0, 0);
-    }
+    // radial crossing at x = in+1 (from outside) or x = in; axial likewise
+    const float f = (di != 0) ? ((di > 0 ? 1.f : 0.f) - Xo) / dX : ((dk > 0 ? 1.f : 0.f) - Yo) / dY;
+    seg(0.f, f, di, dk);
+    seg(f, 1.f, 0, 0);
   } else if (res == 2 && di != 0) {
-    // boundary lines crossed: x = xb (between old and new column), y = yb
-    const float xb = di > 0 ? 1.f : 0.f;
-    const float yb = dk > 0 ? 1.f : 0.f;
-    const float y1 = Yo + (xb - Xo) * sl;  // where the path meets x = xb
-    const float x2 = Xo + (yb - Yo) / sl;  // where it meets y = yb
-    // The path meets the radial boundary first when, at x = xb, it is still
-    // on the old side of y = yb (:271-381); a crossing exactly through the
-    // corner deposits nothing, as in the reference.
-    if (y1 == yb) return true;
-    const bool r_first = (dk < 0) ? (y1 < yb) : (y1 > yb);
-    if (r_first) {  // old cell -> (0, dk) cell -> new cell
-      seg(Xo, Yo, xb, y1, di, dk);
-      seg(xb, y1, x2, yb, 0, dk);
-      seg(x2, yb, Xn, Yn, 0, 0);
-    } else {        // old cell -> (di, 0) cell -> new cell
-      seg(Xo, Yo, x2, yb, di, dk);
-      seg(x2, yb, xb, y1, di, 0);
-      seg(xb, y1, Xn, Yn, 0, 0);
+    const float xb = di > 0 ? 1.f : 0.f, yb = dk > 0 ? 1.f : 0.f;
+    const float fx = (xb - Xo) / dX, fy = (yb - Yo) / dY;  // path fractions of the two crossings
+    if (fx == fy) return true;  // through the corner: the reference deposits nothing (:278-300)
+    if (fx < fy) {  // radial boundary first: old cell -> (0, dk) -> new
+      seg(0.f, fx, di, dk);
+      seg(fx, fy, 0, dk);
+      seg(fy, 1.f, 0, 0);
+    } else {        // axial boundary first: old cell -> (di, 0) -> new
+      seg(0.f, fy, di, dk);
+      seg(fy, fx, di, 0);
+      seg(fx, 1.f, 0, 0);
     }
   }
   return true;
 }
+
+// ---------------------------------------------------------------------------
 
 // ---------------------------------------------------------------------------
 // ZigZag current (currentZigZag.cpp:22-136) with the reference's metre-valued
@@ -483,25 +485,26 @@ __device__ __forceinline__ void zigzag(const StepArgs& a, const Dep& d, float qw
   const float W_z1 = a.dz_m * (0.5f * (Yo + yr) - (float)ko), W_z2 = a.dz_m * (0.5f * (Yn + yr));
   const float mWr1 = 1.f - W_r1, mWr2 = 1.f - W_r2, mWz1 = 1.f - W_z1, mWz2 = 1.f - W_z2, mWp = 1.f - W_phi;
   const int ia = in + io, ka = kn + ko;
-  d.add(d.Jr, ia, ka, oov * F_r1 * mWp * mWz1 + oov * F_r1 * W_phi * mWz1);
-  d.add(d.Jr, ia, ka + 1, oov * F_r1 * mWp * W_z1 + oov * F_r1 * W_phi * W_z1);
-  d.add(d.Jr, in, kn, oov * F_r2 * mWp * mWz2 + oov * F_r2 * W_phi * mWz2);
-  d.add(d.Jr, in, kn + 1, oov * F_r2 * mWp * W_z2 + oov * F_r2 * W_phi * W_z2);
-  d.add(d.Jp, in, kn, oov * F_phi * mWr2 * mWz2);
-  d.add(d.Jp, in, kn + 1, oov * F_phi * mWr2 * W_z1);
-  d.add(d.Jp, in + 1, kn, oov * F_phi * W_r2 * mWz2);
-  d.add(d.Jp, in + 1, kn + 1, oov * F_phi * W_r2 * W_z2);
-  d.add(d.Jz, ia, ka, oov * F_z1 * mWr1 * mWp + oov * F_z1 * mWr1 * W_phi);
-  d.add(d.Jz, ia + 1, ka, oov * F_z1 * W_r1 * mWp + oov * F_z1 * W_r1 * W_phi);
-  d.add(d.Jz, in, kn, oov * F_z2 * mWr2 * mWp + oov * F_z2 * mWr2 * W_phi);
-  d.add(d.Jz, in + 1, kn, oov * F_z2 * W_r2 * mWp + oov * F_z2 * W_r2 * W_phi);
+  d.add(0,ia, ka, oov * F_r1 * mWp * mWz1 + oov * F_r1 * W_phi * mWz1);
+  d.add(0,ia, ka + 1, oov * F_r1 * mWp * W_z1 + oov * F_r1 * W_phi * W_z1);
+  d.add(0,in, kn, oov * F_r2 * mWp * mWz2 + oov * F_r2 * W_phi * mWz2);
+  d.add(0,in, kn + 1, oov * F_r2 * mWp * W_z2 + oov * F_r2 * W_phi * W_z2);
+  d.add(1,in, kn, oov * F_phi * mWr2 * mWz2);
+  d.add(1,in, kn + 1, oov * F_phi * mWr2 * W_z1);
+  d.add(1,in + 1, kn, oov * F_phi * W_r2 * mWz2);
+  d.add(1,in + 1, kn + 1, oov * F_phi * W_r2 * W_z2);
+  d.add(2,ia, ka, oov * F_z1 * mWr1 * mWp + oov * F_z1 * mWr1 * W_phi);
+  d.add(2,ia + 1, ka, oov * F_z1 * W_r1 * mWp + oov * F_z1 * W_r1 * W_phi);
+  d.add(2,in, kn, oov * F_z2 * mWr2 * mWp + oov * F_z2 * mWr2 * W_phi);
+  d.add(2,in + 1, kn, oov * F_z2 * W_r2 * mWp + oov * F_z2 * W_r2 * W_phi);
 }
 
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads) step_kernel(StepArgs a, SpeciesF32Buffers b, size_t n) {
-  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (j >= n) return;
+// One macroparticle: gather, push, move, reflect, bind, runaway test and
+// current.  Returns without touching the particle if it is dead.
+__device__ __forceinline__ void advance_one(const StepArgs& a, const SpeciesF32Buffers& b,
+                                            size_t j, const Dep& d) {
   const int cell = b.cell[j];
   if (cell < 0) return;
   const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
@@ -525,14 +528,24 @@ __global__ void __launch_bounds__(kThreads) step_kernel(StepArgs a, SpeciesF32Bu
   int ci = ci0, ck = ck0;
   // far from the axis x' - x = dx + dy^2/(X + x'); near it (or across it,
   // X < 0) x' itself is small and exact enough
-  float fr = (X > 0.5f) ? fr0 + dx + dyp * dyp / (X + xn) : xn - (float)ci0;
-  float fz = fz0 + dzz;
+  float dX = (X > 0.5f) ? dx + dyp * dyp / (X + xn) : xn - ((float)ci0 + fr0);  // exact displacement
+  float dY = dzz;
+  float fr = fr0 + dX;
+  float fz = fz0 + dY;
   renorm(&ci, &fr);
   renorm(&ck, &fz);
+  bool reflected = false;
   if (a.is_beam) {  // BeamP::reflect beamP.cpp:159-177
-    if (ci < 0 || (ci == 0 && fr < 0.5f)) { mirror(&ci, &fr, 0); v[0] = -v[0]; }
-  } else if (!reflect(a, &ci, &fr, &ck, &fz, &v[0], &v[2])) {
-    raise_error(a.st, kErrReflectLoop);
+    if (ci < 0 || (ci == 0 && fr < 0.5f)) { mirror(&ci, &fr, 0); v[0] = -v[0]; reflected = true; }
+  } else {
+    const int c0 = ci, k0 = ck;
+    const float f0 = fr, g0 = fz;
+    if (!reflect(a, &ci, &fr, &ck, &fz, &v[0], &v[2])) raise_error(a.st, kErrReflectLoop);
+    reflected = ci != c0 || ck != k0 || fr != f0 || fz != g0;
+  }
+  if (reflected) {  // the deposit follows the straight line to the mirrored point
+    dX = (float)(ci - ci0) + (fr - fr0);
+    dY = (float)(ck - ck0) + (fz - fz0);
   }
   const float cs = sqrtf(1.f - sn * sn);  // back_velocity_to_rz :624-640
   const float vr2 = cs * v[0] - sn * v[1];
@@ -553,21 +566,52 @@ __global__ void __launch_bounds__(kThreads) step_kernel(StepArgs a, SpeciesF32Bu
   b.off_z[j] = fz;
   // the old point relative to the new cell
   const float Xo = (float)(ci0 - ci) + fr0, Yo = (float)(ck0 - ck) + fz0;
-  const Dep d{a.Jr, a.Jp, a.Jz, a.ld};
   if (a.current == 1) {
-    zigzag(a, d, w * 1.0f, v[1], ci, ck, Xo, Yo, fr, fz);
+    zigzag(a, d, w, v[1], ci, ck, Xo, Yo, fr, fz);
     return;
   }
-  const float q = w;  // Qz, Qr, Qp carry the species charge
-  vb_azimuthal(a, d, q, v[1], ci, ck, 0.5f * (Xo + fr), 0.5f * (Yo + fz));
-  if (!vb_rz(a, d, q, ci, ck, Xo, Yo, fr, fz)) atomicAdd(&a.st->move_errors, 1ull);
+  vb_azimuthal(a, d, w, v[1], ci, ck, Xo + 0.5f * dX, Yo + 0.5f * dY);
+  if (!vb_rz(a, d, w, ci, ck, Xo, Yo, dX, dY, fr, fz)) atomicAdd(&a.st->move_errors, 1ull);
+}
+
+// Particles [j0, j1), one per thread, current straight to the global grid
+// (particles appended since the last tile sort).
+__global__ void __launch_bounds__(kThreads) step_flat_kernel(StepArgs a, SpeciesF32Buffers b,
+                                                             size_t j0, size_t j1) {
+  const size_t j = j0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= j1) return;
+  const Dep d{{a.Jr, a.Jp, a.Jz}, a.ld, nullptr, 0, 0, 0, 0};
+  advance_one(a, b, j, d);
+}
+
+// One block per tile of TileGrid: the tile's particles (grouped by the last
+// sort) deposit into a shared-memory window of the tile plus `halo` cells,
+// which is added to the global grid once at the end.
+__global__ void __launch_bounds__(kThreads) step_tiled_kernel(StepArgs a, SpeciesF32Buffers b,
+                                                              TileGrid tg) {
+  extern __shared__ float sJ[];
+  const int t = blockIdx.x;
+  const int tr = t / tg.ntz, tz = t - tr * tg.ntz;
+  const int wr = tg.tr + 2 * tg.halo, wz = tg.tz + 2 * tg.halo;
+  const Dep d{{a.Jr, a.Jp, a.Jz}, a.ld, sJ, tr * tg.tr - tg.halo, tz * tg.tz - tg.halo, wr, wz};
+  const int nw = 3 * wr * wz;
+  for (int e = threadIdx.x; e < nw; e += blockDim.x) sJ[e] = 0.f;
+  __syncthreads();
+  const unsigned s = b.tile_start[t], e = b.tile_start[t + 1];
+  for (unsigned j = s + threadIdx.x; j < e; j += blockDim.x) advance_one(a, b, j, d);
+  __syncthreads();
+  for (int q = threadIdx.x; q < nw; q += blockDim.x) {
+    const float v = sJ[q];
+    if (v == 0.f) continue;
+    const int comp = q / (wr * wz), rem = q - comp * wr * wz;
+    const int i = d.i0 + rem / wz, k = d.k0 + rem % wz;
+    atomicAdd(d.J[comp] + (long long)(i + 2) * a.ld + (k + 2), v);
+  }
 }
 
 }  // namespace f32
 
-inline void launch_f32_particle_step(const F32Step& st, SpeciesF32Buffers& b, size_t n,
-                                     double charge, double mass, int is_beam, cudaStream_t s) {
-  if (n == 0) return;
+inline f32::StepArgs f32_step_args(const F32Step& st, double charge, double mass, int is_beam) {
   const GridGeom& g = st.g;
   f32::StepArgs a;
   a.g = g;
@@ -586,12 +630,11 @@ inline void launch_f32_particle_step(const F32Step& st, SpeciesF32Buffers& b, si
   a.mnzl_r = (float)(kMnzl / g.dr);
   a.mnzl_z = (float)(kMnzl / g.dz);
   a.dr_m = (float)g.dr; a.dz_m = (float)g.dz; a.dt_s = (float)g.dt;
-  a.zz_vol = (float)(1.0 / (kPi * g.dz * g.dr * g.dr));
+  // ZigZag: 1/(PI dz dr^2) with the species charge folded in
+  a.zz_vol = (float)(charge / (kPi * g.dz * g.dr * g.dr));
   a.pusher = st.pusher; a.current = st.current; a.fixed = st.fixed; a.is_beam = is_beam;
   a.st = st.status;
-  if (st.current == 1) a.zz_vol *= (float)charge;  // ZigZag: fold q into 1/V
-  const unsigned blocks = (unsigned)((n + f32::kThreads - 1) / f32::kThreads);
-  f32::step_kernel<<<blocks, f32::kThreads, 0, s>>>(a, b, n);
+  return a;
 }
 
 }  // namespace pcg

@@ -41,7 +41,35 @@ struct BeamInject {
   uint32_t stream;
   uint64_t step;
   double domain_radius, dl, half_z, velocity, v_macro_avg, n_per_macro_avg;
+  // Gaussian longitudinal profile (profile == 1): r^2 uniform in
+  // [r_min^2, radius^2], weight w0 * exp(-(s - 3 sigma)^2 / (2 sigma^2)) with
+  // s = head_dist - dl * u_z the particle's distance behind the bunch head.
+  int profile;
+  double r_min, radius, sigma, head_dist, w0;
 };
+
+// The shared particle placement of both layouts (beamP.cpp:100-145 for
+// profile 0).  u[0], u[1] are the two Philox uniforms of the particle.
+__host__ __device__ inline void beam_particle(const BeamInject& b, double dr, double dz,
+                                              const double u[2], double* r, double* z,
+                                              double* w) {
+  if (b.profile == 1) {
+    *r = sqrt(b.r_min * b.r_min + u[0] * (b.radius * b.radius - b.r_min * b.r_min));
+    *z = b.dl * u[1] + b.half_z;
+    const double s = b.head_dist - b.dl * u[1] - 3.0 * b.sigma;
+    *w = b.w0 * exp(-s * s / (2.0 * b.sigma * b.sigma));
+    return;
+  }
+  const double pos_r = b.domain_radius * u[0] + dr / 2 + 0.0 * dr;
+  *r = pos_r;
+  *z = b.dl * u[1] + b.half_z;
+  double norm;
+  if (pos_r > dr / 2)
+    norm = 2 * 3.1415926535897932 * pos_r * dr * dz / b.v_macro_avg;
+  else
+    norm = 3.1415926535897932 * (pos_r * pos_r + pos_r * dr + dr * dr / 4.) * dz / b.v_macro_avg;
+  *w = b.n_per_macro_avg * norm;
+}
 
 void launch_yee_e_f64(const YeeArgs<double>& a, cudaStream_t s);
 void launch_yee_h_f64(const YeeArgs<double>& a, int fixed, cudaStream_t s);

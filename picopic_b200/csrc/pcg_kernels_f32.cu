@@ -1,8 +1,11 @@
 // pcg_kernels_f32.cu — the single-precision production path: float Yee
 // update, species buffers in (cell, offset) form, import/export, beam
-// injection and the fused particle step.
+// injection, the tile sort and the fused particle step.
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -16,6 +19,7 @@ namespace pcg {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kTileR = 8, kTileZ = 64, kHalo = 3;
 
 inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
@@ -45,10 +49,11 @@ __global__ void import_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, size_t
   b.vphi[j] = (float)src[3 * n + i];
   b.vz[j] = (float)src[4 * n + i];
   b.w[j] = (float)src[5 * n + i];
+  b.id[j] = b.next_id + (unsigned)i;
 }
 
-// BeamP::inject (beamP.cpp:100-145) with the same Philox stream as the
-// double path; positions are computed in double and then split.
+// BeamP::inject (beamP.cpp:100-145), or the Gaussian bunch, with the same
+// Philox stream as the double path; positions are computed in double.
 __global__ void inject_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, unsigned count,
                               BeamInject bi) {
   unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -56,13 +61,8 @@ __global__ void inject_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, unsign
   const double dr = g.dr, dz = g.dz;
   double u[2];
   philox_uniform2(bi.seed, bi.stream, bi.step, i, u);
-  const double pos_r = bi.domain_radius * u[0] + dr / 2 + 0.0 * dr;
-  const double pos_z = bi.dl * u[1] + bi.half_z;
-  double norm;
-  if (pos_r > dr / 2)
-    norm = 2 * kPi * pos_r * dr * dz / bi.v_macro_avg;
-  else
-    norm = kPi * (pos_r * pos_r + pos_r * dr + dr * dr / 4.) * dz / bi.v_macro_avg;
+  double pos_r, pos_z, wgt;
+  beam_particle(bi, dr, dz, u, &pos_r, &pos_z, &wgt);
   const size_t j = n0 + i;
   int ci, ck;
   float fr, fz;
@@ -74,7 +74,8 @@ __global__ void inject_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, unsign
   b.vr[j] = 0.f;
   b.vphi[j] = 0.f;
   b.vz[j] = (float)bi.velocity;
-  b.w[j] = (float)(bi.n_per_macro_avg * norm);
+  b.w[j] = (float)wgt;
+  b.id[j] = b.next_id + i;
 }
 
 __global__ void alive_kernel(const int* cell, unsigned char* flags, size_t n) {
@@ -88,20 +89,97 @@ __global__ void gather_kernel(const T* src, T* dst, const unsigned* idx, size_t 
   if (i < n) dst[i] = src[idx[i]];
 }
 
-__global__ void export_kernel(GridGeom g, SpeciesF32Buffers b, size_t n, double* out,
-                              int* cells) {
+__global__ void iota_kernel(unsigned* a, size_t n) {
   size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (j >= n) return;
+  if (j < n) a[j] = (unsigned)j;
+}
+
+// Export in insertion order: perm[m] is the slot of the m-th smallest id.
+__global__ void export_kernel(GridGeom g, SpeciesF32Buffers b, size_t n, const unsigned* perm,
+                              double* out, int* cells) {
+  size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const size_t j = perm[m];
   const int c = b.cell[j];
   const int ci = cell_r_of(c), ck = cell_z_of(c);
-  out[j] = ((double)ci + (double)b.off_r[j]) * g.dr;
-  out[n + j] = ((double)ck + (double)b.off_z[j]) * g.dz;
-  out[2 * n + j] = b.vr[j];
-  out[3 * n + j] = b.vphi[j];
-  out[4 * n + j] = b.vz[j];
-  out[5 * n + j] = b.w[j];
-  cells[j] = ci;
-  cells[n + j] = ck;
+  out[m] = ((double)ci + (double)b.off_r[j]) * g.dr;
+  out[n + m] = ((double)ck + (double)b.off_z[j]) * g.dz;
+  out[2 * n + m] = b.vr[j];
+  out[3 * n + m] = b.vphi[j];
+  out[4 * n + m] = b.vz[j];
+  out[5 * n + m] = b.w[j];
+  cells[m] = ci;
+  cells[n + m] = ck;
+}
+
+// ---------------------------------------------------------------------------
+// Tile sort: counting sort of live particles by tile, into the second buffer.
+
+__device__ __forceinline__ int tile_key(int cell, const TileGrid& tg) {
+  if (cell < 0) return -1;
+  return (cell_r_of(cell) / tg.tr) * tg.ntz + cell_z_of(cell) / tg.tz;
+}
+
+__global__ void tile_hist_kernel(const int* cell, size_t n, TileGrid tg, unsigned* counts) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int key = j < n ? tile_key(cell[j], tg) : -1;
+  const unsigned mask = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(mask) - 1;
+  if ((int)(threadIdx.x & 31) == leader && key >= 0) atomicAdd(counts + key, (unsigned)__popc(mask));
+}
+
+__global__ void tile_scatter_kernel(SpeciesF32Buffers b, size_t n, TileGrid tg, unsigned* cursor) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int key = j < n ? tile_key(b.cell[j], tg) : -1;
+  const unsigned mask = __match_any_sync(0xffffffffu, key);
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (lane == leader && key >= 0) base = atomicAdd(cursor + key, (unsigned)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (key < 0) return;
+  const unsigned pos = base + __popc(mask & ((1u << lane) - 1u));
+  b.cell2[pos] = b.cell[j];
+  b.off_r2[pos] = b.off_r[j];
+  b.off_z2[pos] = b.off_z[j];
+  b.vr2[pos] = b.vr[j];
+  b.vphi2[pos] = b.vphi[j];
+  b.vz2[pos] = b.vz[j];
+  b.w2[pos] = b.w[j];
+  b.id2[pos] = b.id[j];
+}
+
+void swap_buffers(SpeciesF32Buffers& b) {
+  std::swap(b.cell, b.cell2);
+  std::swap(b.off_r, b.off_r2);
+  std::swap(b.off_z, b.off_z2);
+  std::swap(b.vr, b.vr2);
+  std::swap(b.vphi, b.vphi2);
+  std::swap(b.vz, b.vz2);
+  std::swap(b.w, b.w2);
+  std::swap(b.id, b.id2);
+}
+
+int tile_sort(const TileGrid& tg, SpeciesF32Buffers& b, size_t* n, cudaStream_t s) {
+  const size_t nt = (size_t)tg.ntiles;
+  unsigned* counts = b.tile_cursor;  // reused: counts, then cursors
+  cudaMemsetAsync(counts, 0, (nt + 1) * sizeof(unsigned), s);
+  if (*n) tile_hist_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b.cell, *n, tg, counts);
+  size_t tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp, counts, b.tile_start, (int)(nt + 1), s);
+  void* tmpbuf = nullptr;
+  if (cudaMallocAsync(&tmpbuf, tmp, s) != cudaSuccess) return -1;
+  cub::DeviceScan::ExclusiveSum(tmpbuf, tmp, counts, b.tile_start, (int)(nt + 1), s);
+  cudaFreeAsync(tmpbuf, s);
+  cudaMemcpyAsync(b.tile_cursor, b.tile_start, nt * sizeof(unsigned), cudaMemcpyDeviceToDevice, s);
+  if (*n) tile_scatter_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b, *n, tg, b.tile_cursor);
+  unsigned kept = 0;
+  cudaMemcpyAsync(&kept, b.tile_start + nt, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+  swap_buffers(b);
+  *n = kept;
+  b.sorted_n = kept;
+  b.steps_since_sort = 0;
+  return 0;
 }
 
 __device__ __forceinline__ double block_sum(double v) {
@@ -162,18 +240,38 @@ __global__ void kinetic_kernel(SpeciesF32Buffers b, size_t n, double mass, doubl
 
 }  // namespace
 
-int f32_alloc_species(SpeciesF32Buffers& b, size_t cap) {
+TileGrid f32_tile_grid(const GridGeom& g) {
+  TileGrid t;
+  t.tr = std::min(kTileR, g.nr);
+  t.tz = std::min(kTileZ, g.nz);
+  t.ntr = (g.nr + t.tr - 1) / t.tr;
+  t.ntz = (g.nz + t.tz - 1) / t.tz;
+  t.ntiles = t.ntr * t.ntz;
+  t.halo = kHalo;
+  return t;
+}
+
+int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg) {
   if (cap == 0) cap = 1;
   b.cap = cap;
-  if (cudaMalloc((void**)&b.cell, cap * sizeof(int)) != cudaSuccess) return -1;
-  float** arrs[] = {&b.off_r, &b.off_z, &b.vr, &b.vphi, &b.vz, &b.w};
+  int** ints[] = {&b.cell, &b.cell2};
+  for (int** a : ints)
+    if (cudaMalloc((void**)a, cap * sizeof(int)) != cudaSuccess) return -1;
+  float** arrs[] = {&b.off_r, &b.off_z, &b.vr, &b.vphi, &b.vz, &b.w,
+                    &b.off_r2, &b.off_z2, &b.vr2, &b.vphi2, &b.vz2, &b.w2};
   for (float** a : arrs)
     if (cudaMalloc((void**)a, cap * sizeof(float)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.id, cap * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.id2, cap * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.tile_start, (tg.ntiles + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.tile_cursor, (tg.ntiles + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
   return 0;
 }
 
 void f32_free_species(SpeciesF32Buffers& b) {
-  void* arrs[] = {b.cell, b.off_r, b.off_z, b.vr, b.vphi, b.vz, b.w};
+  void* arrs[] = {b.cell, b.off_r, b.off_z, b.vr, b.vphi, b.vz, b.w, b.id,
+                  b.cell2, b.off_r2, b.off_z2, b.vr2, b.vphi2, b.vz2, b.w2, b.id2,
+                  b.tile_start, b.tile_cursor};
   for (void* a : arrs) cudaFree(a);
   b = SpeciesF32Buffers();
 }
@@ -190,12 +288,37 @@ void f32_launch_yee_h(const YeeArgs<float>& a, int fixed, cudaStream_t s) {
 
 void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsigned count,
                        const BeamInject& bi, cudaStream_t s) {
-  if (count) inject_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, b, n0, count, bi);
+  if (!count) return;
+  inject_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, b, n0, count, bi);
+  b.next_id += count;
 }
 
 void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_t n,
                        const double* src, cudaStream_t s) {
+  if (n0 == 0) {  // a replacement: ids restart, no tile grouping yet
+    b.next_id = 0;
+    b.sorted_n = 0;
+    b.steps_since_sort = 1 << 30;
+  }
   if (n) import_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b, n0, n, src);
+  b.next_id += (unsigned)n;
+}
+
+int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
+                     double mass, int is_beam, cudaStream_t s) {
+  if (*n == 0) return 0;
+  if (b.sorted_n == 0 || b.steps_since_sort >= st.sort_interval)
+    if (tile_sort(st.tiles, b, n, s) != 0) return -1;
+  const f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
+  const TileGrid& tg = st.tiles;
+  if (b.sorted_n) {
+    const size_t smem = 3 * (size_t)(tg.tr + 2 * tg.halo) * (tg.tz + 2 * tg.halo) * sizeof(float);
+    f32::step_tiled_kernel<<<tg.ntiles, f32::kThreads, smem, s>>>(a, b, tg);
+  }
+  if (*n > b.sorted_n)
+    f32::step_flat_kernel<<<blocks_for(*n - b.sorted_n), f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
+  b.steps_since_sort += 1;
+  return 0;
 }
 
 void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s) {
@@ -203,19 +326,20 @@ void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n,
 }
 
 int f32_compact(SpeciesF32Buffers& b, const unsigned* idx, size_t kept, cudaStream_t s) {
-  if (kept == 0) return 0;
-  void* tmp = nullptr;
-  if (cudaMalloc(&tmp, kept * sizeof(float)) != cudaSuccess) return -1;
-  gather_kernel<int><<<blocks_for(kept), kThreads, 0, s>>>(b.cell, (int*)tmp, idx, kept);
-  cudaMemcpyAsync(b.cell, tmp, kept * sizeof(int), cudaMemcpyDeviceToDevice, s);
-  float* arrs[] = {b.off_r, b.off_z, b.vr, b.vphi, b.vz, b.w};
-  for (float* a : arrs) {
-    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(a, (float*)tmp, idx, kept);
-    cudaMemcpyAsync(a, tmp, kept * sizeof(float), cudaMemcpyDeviceToDevice, s);
+  if (kept) {
+    gather_kernel<int><<<blocks_for(kept), kThreads, 0, s>>>(b.cell, b.cell2, idx, kept);
+    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(b.off_r, b.off_r2, idx, kept);
+    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(b.off_z, b.off_z2, idx, kept);
+    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(b.vr, b.vr2, idx, kept);
+    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(b.vphi, b.vphi2, idx, kept);
+    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(b.vz, b.vz2, idx, kept);
+    gather_kernel<float><<<blocks_for(kept), kThreads, 0, s>>>(b.w, b.w2, idx, kept);
+    gather_kernel<unsigned><<<blocks_for(kept), kThreads, 0, s>>>(b.id, b.id2, idx, kept);
+    swap_buffers(b);
   }
-  cudaError_t e = cudaStreamSynchronize(s);
-  cudaFree(tmp);
-  return e == cudaSuccess ? 0 : -1;
+  b.sorted_n = 0;  // the grouping by tile no longer holds
+  b.steps_since_sort = 1 << 30;
+  return cudaStreamSynchronize(s) == cudaSuccess ? 0 : -1;
 }
 
 int f32_export(const GridGeom& g, SpeciesF32Buffers& b, size_t n, double* r, double* z,
@@ -223,18 +347,37 @@ int f32_export(const GridGeom& g, SpeciesF32Buffers& b, size_t n, double* r, dou
                cudaStream_t s) {
   double* d = nullptr;
   int* c = nullptr;
-  if (cudaMalloc((void**)&d, 6 * n * sizeof(double)) != cudaSuccess) return -1;
-  if (cudaMalloc((void**)&c, 2 * n * sizeof(int)) != cudaSuccess) { cudaFree(d); return -1; }
-  export_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b, n, d, c);
-  double* dst[6] = {r, z, vr, vphi, vz, w};
-  for (int a = 0; a < 6; ++a)
-    if (dst[a]) cudaMemcpyAsync(dst[a], d + a * n, n * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (cell_r) cudaMemcpyAsync(cell_r, c, n * sizeof(int), cudaMemcpyDeviceToHost, s);
-  if (cell_z) cudaMemcpyAsync(cell_z, c + n, n * sizeof(int), cudaMemcpyDeviceToHost, s);
-  cudaError_t e = cudaStreamSynchronize(s);
+  unsigned *keys = nullptr, *perm = nullptr;
+  void* tmp = nullptr;
+  size_t tmpb = 0;
+  int rc = 0;
+  if (cudaMalloc((void**)&d, 6 * n * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&c, 2 * n * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&keys, 2 * n * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc((void**)&perm, 2 * n * sizeof(unsigned)) != cudaSuccess) {
+    rc = -1;
+  } else {
+    iota_kernel<<<blocks_for(n), kThreads, 0, s>>>(perm, n);
+    cub::DeviceRadixSort::SortPairs(nullptr, tmpb, b.id, keys, perm, perm + n, (int)n, 0, 32, s);
+    if (cudaMalloc(&tmp, tmpb) != cudaSuccess) {
+      rc = -1;
+    } else {
+      cub::DeviceRadixSort::SortPairs(tmp, tmpb, b.id, keys, perm, perm + n, (int)n, 0, 32, s);
+      export_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b, n, perm + n, d, c);
+      double* dst[6] = {r, z, vr, vphi, vz, w};
+      for (int a = 0; a < 6; ++a)
+        if (dst[a]) cudaMemcpyAsync(dst[a], d + a * n, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+      if (cell_r) cudaMemcpyAsync(cell_r, c, n * sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (cell_z) cudaMemcpyAsync(cell_z, c + n, n * sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) rc = -1;
+    }
+  }
+  cudaFree(tmp);
   cudaFree(d);
   cudaFree(c);
-  return e == cudaSuccess ? 0 : -1;
+  cudaFree(keys);
+  cudaFree(perm);
+  return rc;
 }
 
 int f32_energies(const GridGeom& g, float* const fld[12], double* ee, double* eh, cudaStream_t s) {
@@ -264,11 +407,6 @@ int f32_kinetic(const SpeciesF32Buffers& b, size_t n, double mass, double* out, 
   cudaError_t e = cudaStreamSynchronize(s);
   cudaFree(d);
   return e == cudaSuccess ? 0 : -1;
-}
-
-void f32_launch_step(const F32Step& st, SpeciesF32Buffers& b, size_t n, double charge,
-                     double mass, int is_beam, cudaStream_t s) {
-  launch_f32_particle_step(st, b, n, charge, mass, is_beam, s);
 }
 
 }  // namespace pcg

@@ -246,18 +246,13 @@ __global__ void inject_kernel(GridGeom g, SpeciesF64 sp, size_t n0, unsigned cou
   const double dr = g.dr, dz = g.dz;
   double u[2];
   philox_uniform2(b.seed, b.stream, b.step, i, u);
-  const double rand_r = u[0], rand_z = u[1];
-  const double pos_r = b.domain_radius * rand_r + dr / 2 + 0.0 * dr;
+  double pos_r, pos_z, w;
+  beam_particle(b, dr, dz, u, &pos_r, &pos_z, &w);
   size_t j = n0 + i;
   sp.r[j] = pos_r;
-  sp.z[j] = b.dl * rand_z + b.half_z;
+  sp.z[j] = pos_z;
   sp.vr[j] = 0; sp.vphi[j] = 0; sp.vz[j] = b.velocity;
-  double norm;
-  if (pos_r > dr / 2)
-    norm = 2 * kPi * pos_r * dr * dz / b.v_macro_avg;
-  else
-    norm = kPi * (pos_r * pos_r + pos_r * dr + dr * dr / 4.) * dz / b.v_macro_avg;
-  sp.w[j] = b.n_per_macro_avg * norm;
+  sp.w[j] = w;
   sp.r_old[j] = 0; sp.z_old[j] = 0;
   if (sp.phi) { sp.phi[j] = 0; sp.phi_old[j] = 0; sp.sn[j] = 0; }
   if (sp.cell_r) { sp.cell_r[j] = cell_number(pos_r, dr); sp.cell_z[j] = cell_number(pos_r, dz); }

@@ -123,6 +123,29 @@ class Domain:
         fn = self.lib.pcg_append_species if append else self.lib.pcg_import_species
         self._check(fn(self.h, slot, arrs[0].size, *[_dp(a) for a in arrs]), "pcg_import_species")
 
+    def seed_plasma(self, slot, n, density, temperature_ev, seed=0):
+        """Fill a species on the device with a uniform Maxwellian plasma."""
+        self._check(self.lib.pcg_seed_plasma(self.h, slot, int(n), float(density),
+                                             float(temperature_ev), int(seed)), "pcg_seed_plasma")
+
+    def set_beam_profile(self, slot, profile="gaussian", sigma_z=0.0, macro_per_cell=0.0):
+        code = {"rectangle": 0, "gaussian": 1}[profile]
+        self._check(self.lib.pcg_set_beam_profile(self.h, slot, code, float(sigma_z),
+                                                  float(macro_per_cell)), "pcg_set_beam_profile")
+
+    def enable_timers(self, on=True):
+        self._check(self.lib.pcg_enable_timers(self.h, 1 if on else 0), "pcg_enable_timers")
+
+    TIMERS = ["field_e", "field_h", "inject", "particles", "deposit"]
+
+    def kernel_times(self) -> dict:
+        """Milliseconds and launches per kernel class since the last call."""
+        n = len(self.TIMERS)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int * n)()
+        self._check(self.lib.pcg_kernel_times(self.h, ms, cnt, n), "pcg_kernel_times")
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(self.TIMERS)}
+
     def count(self, slot) -> int:
         n = ctypes.c_size_t()
         self._check(self.lib.pcg_count(self.h, slot, ctypes.byref(n)), "pcg_count")
