@@ -210,6 +210,7 @@ def run_gpu(args):
         return float(t.item())
 
     w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
+    w = scaled(w, nz=args.nz, ppc=args.ppc)
     d, slots, g, vb = make_domain(w, "f32", seed=1234 + 7919 * rank, device=local)
     d.step(args.warmup)
     d.synchronize()
@@ -438,6 +439,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="a reduced grid for quick checks")
+    ap.add_argument("--ppc", type=int, default=None, help="override plasma macroparticles per cell")
+    ap.add_argument("--nz", type=int, default=None, help="override the axial cell count")
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
