@@ -212,6 +212,32 @@ int pcg_set_beam_profile(pcg_handle* h, int slot, int profile, double sigma_z,
 int pcg_enable_timers(pcg_handle* h, int on);
 int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n);
 
+/* Villasenor-Buneman current of one species, double precision, that
+ * allocates no device memory.  No counterpart in the reference: it exists
+ * for callers that may not call cudaMalloc (a host code that owns and
+ * pre-partitions the device memory, or one that cannot afford cudaMalloc's
+ * device synchronisation inside its step loop).  All arrays are the
+ * caller's device memory: positions r, z (new) and r_old, z_old (before the
+ * move), v_phi and weights of n particles, and the three J grids of
+ * (nr+4) x (nz+4) doubles with the 2-cell halo, which receive the deposit
+ * exactly as PCG_STAGE_CURRENT does for a single species (the halo is
+ * cleared, the interior accumulates).  Work is queued on `stream`
+ * (cudaStream_t, 0 for the default stream); when move_errors is not NULL
+ * the call waits for the stream and stores the number of particles whose
+ * current was skipped for moving more than one cell.
+ * Scratch lives in a fixed device array shared by every call on a device:
+ * grids with (nr+4)*(nz+4) > PCG_NOALLOC_MAX_NODES return PCG_ERR_CAPACITY;
+ * each call clears the scratch first, so calls that overlap on the GPU
+ * (different streams, no ordering) race.  The first call on each device
+ * looks up the scratch address; make that first call before any stream
+ * capture on that device. */
+#define PCG_NOALLOC_MAX_NODES 262144
+int pcg_current_vb_f64_noalloc(int nr, int nz, double radius, double longitude, double dt,
+                               size_t n, double charge_e, const double* r, const double* z,
+                               const double* r_old, const double* z_old, const double* vphi,
+                               const double* w, double* j_r, double* j_phi, double* j_z,
+                               int quirks, void* stream, unsigned long long* move_errors);
+
 int pcg_set_field(pcg_handle* h, int which, const double* src);
 int pcg_export_field(pcg_handle* h, int which, double* dst);
 

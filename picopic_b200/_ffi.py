@@ -73,6 +73,10 @@ SIGNATURES = {
     "pcg_set_beam_profile": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _D, _D]),
     "pcg_enable_timers": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_kernel_times": (ctypes.c_int, [_H, _PD, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "pcg_current_vb_f64_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _D, _D, _D,
+                                                  ctypes.c_size_t, _D] + [ctypes.c_void_p] * 9 +
+                                   [ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 _lib = None

@@ -31,6 +31,7 @@ UNITS = {
     "pcg_kernels_f64.cu": ["--fmad=false"],
     "pcg_kernels_f32.cu": [],
     "pcg_init.cu": [],
+    "pcg_noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -434,7 +434,7 @@ __device__ __forceinline__ double ssd_strict(double q, double r, double dr, doub
 }
 
 // simple_current_distribution :22-173
-__device__ void vb_simple(const Sink& s, double rn, double zn, double ro, double zo, int i_n,
+__device__ inline void vb_simple(const Sink& s, double rn, double zn, double ro, double zo, int i_n,
                           int k_n, double q) {
   const GridGeom& g = *s.g;
   const double dr = g.dr, dz = g.dz, dt = g.dt;
@@ -482,7 +482,7 @@ __device__ void vb_simple(const Sink& s, double rn, double zn, double ro, double
 
 // strict_motion_distribution :500-729.  The J_r overwrite of the axial
 // branch is applied by the caller through Sink::reset.
-__device__ void vb_strict(const Sink& s, bool fixed, double rn, double zn, double ro, double zo,
+__device__ inline void vb_strict(const Sink& s, bool fixed, double rn, double zn, double ro, double zo,
                           double q) {
   const GridGeom& g = *s.g;
   const double dr = g.dr, dz = g.dz, dt = g.dt;
@@ -627,7 +627,7 @@ __device__ __forceinline__ bool vb_strict_axial_nodes(const GridGeom& g, bool fi
 
 // rz_current_distribution :175-396 for one particle.  Returns false when
 // the particle moved more than one cell (logged as ERROR, no current).
-__device__ bool vb_rz(const Sink& s, bool fixed, double q, double R, double Z, double RO,
+__device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, double Z, double RO,
                       double ZO, int cell_r, int cell_z) {
   const GridGeom& g = *s.g;
   const double dr = g.dr, dz = g.dz;
