@@ -29,7 +29,8 @@ UNITS = {
     "pcg_api.cu": [],
     "pcg_util.cu": [],
     "pcg_kernels_f64.cu": ["--fmad=false"],
-    "pcg_kernels_f32.cu": [],
+    # the float production path: approximate division/sqrt (2 ulp) and FTZ
+    "pcg_kernels_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "pcg_init.cu": [],
     "pcg_noalloc.cu": ["--fmad=false"],
 }

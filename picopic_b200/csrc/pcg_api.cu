@@ -61,7 +61,8 @@ struct pcg_handle {
   DevStatus* h_status = nullptr;  // pinned mirror
   size_t nodes = 0;               // (nr+4)*(nz+4)
   double* f64[12] = {};
-  float* f32[12] = {};
+  float* f32[12] = {};            // planes of one allocation, f32_plane floats apart
+  size_t f32_plane = 0;
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -460,6 +461,7 @@ int fused_step(pcg_handle* h) {
     F32Step st;
     st.g = h->g;
     for (int c = 0; c < 12; ++c) st.fld[c] = h->f32[c];
+    st.plane = (int)h->f32_plane;
     st.pusher = h->cfg.pusher;
     st.current = h->cfg.current;
     st.fixed = fixed;
@@ -531,10 +533,11 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
     if ((rc = dalloc(h, &h->reset, h->nodes)) != PCG_OK) return bail(rc);
     cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream);
   } else {
-    for (int c = 0; c < 12; ++c) {
-      if ((rc = dalloc(h, &h->f32[c], h->nodes)) != PCG_OK) return bail(rc);
-      cudaMemsetAsync(h->f32[c], 0, sizeof(float) * h->nodes, h->stream);
-    }
+    // one allocation: a particle kernel reaches component c at base + c * plane
+    h->f32_plane = (h->nodes + 63) / 64 * 64;
+    if ((rc = dalloc(h, &h->f32[0], 12 * h->f32_plane)) != PCG_OK) return bail(rc);
+    cudaMemsetAsync(h->f32[0], 0, sizeof(float) * 12 * h->f32_plane, h->stream);
+    for (int c = 1; c < 12; ++c) h->f32[c] = h->f32[0] + c * h->f32_plane;
     std::vector<float> prof[3];
     const std::vector<double>* src[3] = {&sr, &s0, &sl};
     for (int c = 0; c < 3; ++c) {
@@ -552,7 +555,8 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
 int pcg_destroy(pcg_handle* h) {
   if (!h) return PCG_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (int c = 0; c < 12; ++c) { cudaFree(h->f64[c]); cudaFree(h->f32[c]); }
+  for (int c = 0; c < 12; ++c) cudaFree(h->f64[c]);
+  cudaFree(h->f32[0]);
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
   cudaFree(h->reset);
   cudaFree(h->scratch);

@@ -19,6 +19,9 @@ template <typename Real>
 struct YeeArgs;
 
 // Tiles of tr x tz cells; a block's shared window adds `halo` cells per side.
+constexpr int kTileCells = 512;             // tr * tz at most
+constexpr int kTileWords = kTileCells / 32;  // 32-cell words of a tile's layer mask
+constexpr int kLayerCap = 128;              // layers kept in order; deeper ranks go to an overflow run
 struct TileGrid {
   int tr, tz, ntr, ntz, ntiles, halo;
 };
@@ -36,7 +39,20 @@ struct SpeciesF32Buffers {
         *w2 = nullptr;
   unsigned* id2 = nullptr;
   unsigned* tile_start = nullptr;   // ntiles + 1: particles of tile t are [start[t], start[t+1])
-  unsigned* tile_cursor = nullptr;  // ntiles, scatter cursors
+  unsigned* tile_cursor = nullptr;  // ntiles + 1, per-tile counts before the scan
+  // layered order inside a tile (see tile_sort): per particle its rank in its
+  // cell, per tile cell counts and, per layer q, which cells hold more than q
+  unsigned* rank = nullptr;            // cap
+  unsigned* cell_count = nullptr;      // ntiles * kTileCells
+  unsigned* layer_mask = nullptr;      // ntiles * kLayerCap * kTileWords
+  unsigned short* layer_prefix = nullptr;  // same shape: set bits in the words before
+  unsigned* layer_start = nullptr;     // ntiles * (kLayerCap + 1); entry kLayerCap: overflow run
+  unsigned* overflow = nullptr;        // ntiles, cursors of the overflow runs
+  unsigned* sort_info = nullptr;       // device: largest tile, occupied tiles
+  unsigned* host_info = nullptr;       // pinned: live count, largest tile, occupied tiles
+  void* scan_tmp = nullptr;            // the tile-count scan's workspace
+  size_t scan_tmp_bytes = 0;
+  int splits = 1;                      // blocks per tile in the step (the largest tile's share)
   size_t cap = 0;
   size_t sorted_n = 0;       // [0, sorted_n) are grouped by tile; later slots were appended
   int steps_since_sort = 1 << 30;
@@ -45,7 +61,8 @@ struct SpeciesF32Buffers {
 
 struct F32Step {
   GridGeom g;
-  float* fld[12];
+  float* fld[12];  // planes of one allocation: fld[c] = fld[0] + c * plane
+  int plane;
   int pusher, current, fixed;
   DevStatus* status;
   TileGrid tiles;

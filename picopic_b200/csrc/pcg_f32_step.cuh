@@ -29,6 +29,7 @@ struct StepArgs {
   float *Er, *Ep, *Ez, *Hr, *Hp, *Hz;  // fields; H is field_h (time-centred)
   float *Jr, *Jp, *Jz;
   int nr, nz, ld;
+  int plane;                   // Ep = Er + plane, ..., Hz = Er + 5 * plane
   float dt_dr, dt_dz;          // dt/dr, dt/dz
   float c2m;                   // charge*dt/(2*mass), pusherBoris.cpp:67
   float bk;                    // c2m * MAGN_CONST
@@ -40,8 +41,9 @@ struct StepArgs {
   DevStatus* st;
 };
 
-__device__ __forceinline__ long long node(const StepArgs& a, int i, int k) {
-  return (long long)(i + 2) * a.ld + (k + 2);
+// Grids are far below 2^31 nodes, so node indices are 32-bit.
+__device__ __forceinline__ int node(const StepArgs& a, int i, int k) {
+  return (i + 2) * a.ld + (k + 2);
 }
 
 // ---------------------------------------------------------------------------
@@ -76,35 +78,45 @@ __device__ __forceinline__ void radial_w_int(int i, float u, float* w0, float* w
   *w1 = u * (2.f * fi + 1.f + u) / (2.f * fi + 3.f);
 }
 
-__device__ __forceinline__ float interp4(const float* F, const StepArgs& a, int i, int k, float w0,
-                                         float w1, float v) {
-  const long long p = node(a, i, k);
-  const float f00 = __ldg(F + p), f10 = __ldg(F + p + a.ld);
-  const float f01 = __ldg(F + p + 1), f11 = __ldg(F + p + a.ld + 1);
+// Six field components (E_r, E_phi, E_z, H_r, H_phi, H_z) seen through a
+// window: component c at node (i, k) is base[c * plane + (i - i0) * ld + (k - k0)].
+// The global grid is the window with i0 = k0 = -2, ld = nz + 4 and the
+// allocation's plane stride; a block's shared-memory copy of its tile is a
+// smaller one.  Five scalars, so a thread picks either with selects.
+struct FieldView {
+  const float* base;
+  int plane, ld, i0, k0;
+};
+
+__device__ __forceinline__ float interp4(const FieldView& fv, int c, int i, int k,
+                                         float w0, float w1, float v) {
+  const float* F = fv.base + c * fv.plane + (i - fv.i0) * fv.ld + (k - fv.k0);
+  const float f00 = F[0], f10 = F[fv.ld];
+  const float f01 = F[1], f11 = F[fv.ld + 1];
   return (f00 * w0 + f10 * w1) * (1.f - v) + (f01 * w0 + f11 * w1) * v;
 }
 
-__device__ __forceinline__ void gather(const StepArgs& a, int ci, float fr, int ck, float fz,
-                                       float e[3], float b[3]) {
+__device__ __forceinline__ void gather(const FieldView& fv, int fixed, int ci, float fr, int ck,
+                                       float fz, float e[3], float b[3]) {
   const Stagger rh = half_shift(ci, fr), zh = half_shift(ck, fz);
   float h0, h1, n0, n1;
   radial_w_half(rh.i, rh.u, &h0, &h1);
   radial_w_int(ci, fr, &n0, &n1);
   // E_r: (1/2, 0); E_z: (0, 1/2); E_phi: (0, 0)
-  e[0] = interp4(a.Er, a, rh.i, ck, h0, h1, fz);
-  e[2] = interp4(a.Ez, a, ci, zh.i, n0, n1, zh.u);
+  e[0] = interp4(fv, 0, rh.i, ck, h0, h1, fz);
+  e[2] = interp4(fv, 2, ci, zh.i, n0, n1, zh.u);
   {
-    const long long p = node(a, ci, ck);
-    const float f00 = __ldg(a.Ep + p), f10 = __ldg(a.Ep + p + a.ld);
-    const float f01 = __ldg(a.Ep + p + 1), f11 = __ldg(a.Ep + p + a.ld + 1);
+    const float* F = fv.base + fv.plane + (ci - fv.i0) * fv.ld + (ck - fv.k0);
+    const float f00 = F[0], f10 = F[fv.ld];
+    const float f01 = F[1], f11 = F[fv.ld + 1];
     const float t11 = f11 * n1 * fz;
     e[1] = (f00 * n0 + f10 * n1) * (1.f - fz) + f01 * n0 * fz;
-    if (a.fixed) e[1] += t11; else e[2] += t11;  // maxwellSolver.hpp:313
+    if (fixed) e[1] += t11; else e[2] += t11;  // maxwellSolver.hpp:313
   }
   // H_z: (1/2, 0); H_r: (0, 1/2); H_phi: (1/2, 1/2)
-  b[2] = interp4(a.Hz, a, rh.i, ck, h0, h1, fz);
-  b[0] = interp4(a.Hr, a, ci, zh.i, n0, n1, zh.u);
-  b[1] = interp4(a.Hp, a, rh.i, zh.i, h0, h1, zh.u);
+  b[2] = interp4(fv, 5, rh.i, ck, h0, h1, fz);
+  b[0] = interp4(fv, 3, ci, zh.i, n0, n1, zh.u);
+  b[1] = interp4(fv, 4, rh.i, zh.i, h0, h1, zh.u);
 }
 
 // ---------------------------------------------------------------------------
@@ -277,20 +289,27 @@ __device__ __forceinline__ void g_terms(float t, float* h, float* m) {
   }
 }
 
-// Where the current goes: a shared-memory window of the tile a block works
-// on (nodes [i0, i0+wr) x [k0, k0+wz)), and the global grid for anything
-// outside it.  comp: 0 J_r, 1 J_phi, 2 J_z.
-struct Dep {
-  float* J[3];
-  int ld;
-  float* sJ;  // 3 planes of wr x wz floats, or null
-  int i0, k0, wr, wz;
+// Where the current goes.  comp: 0 J_r, 1 J_phi, 2 J_z.
+//
+// SharedDep: the block's shared-memory window over nodes [i0, i0+wr) x
+// [k0, k0+wz); the caller has checked that every node the particle's
+// deposit touches lies in it.
+struct SharedDep {
+  float* s;  // 3 planes of wr x wz floats
+  int wr, wz, i0, k0;
   __device__ __forceinline__ void add(int comp, int i, int k, float v) const {
-    const int li = i - i0, lk = k - k0;
-    if (sJ && (unsigned)li < (unsigned)wr && (unsigned)lk < (unsigned)wz)
-      atomicAdd(sJ + (comp * wr + li) * wz + lk, v);
-    else
-      atomicAdd(J[comp] + (long long)(i + 2) * ld + (k + 2), v);
+    // a native shared-memory reduction (the pointer alone would make it generic)
+    const unsigned p = (unsigned)__cvta_generic_to_shared(s + (comp * wr + (i - i0)) * wz + (k - k0));
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(p), "f"(v) : "memory");
+  }
+};
+
+// GlobalDep: the grids themselves (J_r, J_phi, J_z are consecutive planes).
+struct GlobalDep {
+  float* J;
+  int plane, ld;
+  __device__ __forceinline__ void add(int comp, int i, int k, float v) const {
+    atomicAdd(J + comp * plane + (i + 2) * ld + (k + 2), v);
   }
 };
 
@@ -299,37 +318,39 @@ struct Dep {
 // exactly (from the velocity, split by path fractions), never differenced
 // from rounded offsets, so the MNZL test below means what it means in the
 // reference's double arithmetic.
-__device__ __forceinline__ void vb_simple(const StepArgs& a, const Dep& d, float q, int i, int k,
+template <class D>
+__device__ __forceinline__ void vb_simple(const StepArgs& a, const D& d, float q, int i, int k,
                                           float ao, float bo, float dx, float dy) {
   if (fabsf(dx) < a.mnzl_r || fabsf(dy) < a.mnzl_z) return;  // currentVB.cpp:45-46
   const float fi = (float)i;
   const float xo = fi + ao, xn = xo + dx;
+  const float ixo = 1.f / xo, ixn = 1.f / xn;
   float h, m;
-  g_terms(dx / xo, &h, &m);
+  g_terms(dx * ixo, &h, &m);
   const float qz = q * a.qz * dy;
+  const float cc = fi * (fi + 1.f);
   if (i >= 1) {
-    const float cc = fi * (fi + 1.f);
-    const float lin = 0.5f * dx * (1.f + cc / (xo * xo));
-    const float hh = cc * h / xo;
-    const float A = (1.f - ao) * (2.f * fi + ao) / xo - lin + hh;
-    const float B = ao * (2.f * fi + 1.f + ao) / xo + lin - hh;
-    d.add(2,i, k, qz * A / fi);
-    d.add(2,i + 1, k, qz * B / (fi + 1.f));
+    const float lin = 0.5f * dx * (1.f + cc * ixo * ixo);
+    const float hh = cc * h * ixo;
+    const float A = (1.f - ao) * (2.f * fi + ao) * ixo - lin + hh;
+    const float B = ao * (2.f * fi + 1.f + ao) * ixo + lin - hh;
+    d.add(2, i, k, qz * A / fi);
+    d.add(2, i + 1, k, qz * B / (fi + 1.f));
   } else {
-    d.add(2,i, k, 8.f * qz * (1.f - ao - 0.5f * dx));
-    d.add(2,i + 1, k, qz * (1.f + ao + 0.5f * dx));
+    d.add(2, i, k, 8.f * qz * (1.f - ao - 0.5f * dx));
+    d.add(2, i + 1, k, qz * (1.f + ao + 0.5f * dx));
   }
-  const float c = 0.5f * fi * (fi + 1.f);
   const float qr = q * a.qr / (fi + 0.5f);
   const float bb = 1.f - bo;
-  const float cx = c / xo;
-  d.add(0,i, k, qr * (dx * (0.5f * bb - 0.25f * dy) + cx * (dx * bb / xn + dy * m)));
-  d.add(0,i, k + 1, qr * (dx * (0.5f * bo + 0.25f * dy) + cx * (dx * bo / xn - dy * m)));
+  const float cx = 0.5f * cc * ixo;
+  d.add(0, i, k, qr * (dx * (0.5f * bb - 0.25f * dy) + cx * (dx * bb * ixn + dy * m)));
+  d.add(0, i, k + 1, qr * (dx * (0.5f * bo + 0.25f * dy) + cx * (dx * bo * ixn - dy * m)));
 }
 
 // strict_motion_distribution (:500-729).  (Xo, Yo) is the old point relative
 // to the new cell, (dX, dY) the exact displacement, (Xn, Yn) the new offsets.
-__device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float q, int in, int kn,
+template <class D>
+__device__ __forceinline__ void vb_strict(const StepArgs& a, const D& d, float q, int in, int kn,
                                           float Xo, float Yo, float dX, float dY, float Xn,
                                           float Yn) {
   const bool sr = fabsf(dX) < a.mnzl_r, sz = fabsf(dY) < a.mnzl_z;
@@ -405,7 +426,8 @@ __device__ __forceinline__ void vb_strict(const StepArgs& a, const Dep& d, float
 
 // azimuthal_current_distribution (:398-498): J_phi from the mid-point, in
 // the cell of the new position (a, b may lie outside [0, 1)).
-__device__ __forceinline__ void vb_azimuthal(const StepArgs& a, const Dep& d, float q, float vphi,
+template <class D>
+__device__ __forceinline__ void vb_azimuthal(const StepArgs& a, const D& d, float q, float vphi,
                                              int in, int kn, float Xm, float Ym) {
   const float fi = (float)in;
   const float xm = fi + Xm;
@@ -424,7 +446,8 @@ __device__ __forceinline__ void vb_azimuthal(const StepArgs& a, const Dep& d, fl
 // rz_current_distribution (:175-396).  (Xo, Yo): old point relative to the
 // new cell (in, kn); (dX, dY): the exact displacement; (Xn, Yn): the new
 // offsets.  Crossings split the displacement by path fractions.
-__device__ __forceinline__ bool vb_rz(const StepArgs& a, const Dep& d, float q, int in, int kn,
+template <class D>
+__device__ __forceinline__ bool vb_rz(const StepArgs& a, const D& d, float q, int in, int kn,
                                       float Xo, float Yo, float dX, float dY, float Xn, float Yn) {
   const int di = (int)floorf(Xo), dk = (int)floorf(Yo);  // old cell - new cell
   if (abs(di) > 1 || (a.fixed && abs(dk) > 1)) return false;
@@ -433,31 +456,30 @@ __device__ __forceinline__ bool vb_rz(const StepArgs& a, const Dep& d, float q, 
     return true;
   }
   const int res = abs(di) + abs(dk);
-  // part of the path from fraction f0 to f1 (0..1), deposited in cell (in+ci, kn+ck)
-  auto seg = [&](float f0, float f1, int ci, int ck) {
-    vb_simple(a, d, q, in + ci, kn + ck, Xo + f0 * dX - ci, Yo + f0 * dY - ck, (f1 - f0) * dX,
-              (f1 - f0) * dY);
-  };
-  if (res == 0) {
-    seg(0.f, 1.f, 0, 0);
-  } else if (res == 1) {
+  if (res > 2 || (res == 2 && di == 0)) return true;  // the reference deposits nothing
+  // The path is cut at its cell-boundary crossings into nseg <= 3 parts, part
+  // s running over path fractions [f[s], f[s+1]] inside cell (in+ci[s], kn+ck[s]).
+  float f[4] = {0.f, 1.f, 1.f, 1.f};
+  int ci[3] = {0, 0, 0}, ck[3] = {0, 0, 0};
+  int nseg = 1;
+  if (res == 1) {
     // radial crossing at x = in+1 (from outside) or x = in; axial likewise
-    const float f = (di != 0) ? ((di > 0 ? 1.f : 0.f) - Xo) / dX : ((dk > 0 ? 1.f : 0.f) - Yo) / dY;
-    seg(0.f, f, di, dk);
-    seg(f, 1.f, 0, 0);
-  } else if (res == 2 && di != 0) {
+    f[1] = (di != 0) ? ((di > 0 ? 1.f : 0.f) - Xo) / dX : ((dk > 0 ? 1.f : 0.f) - Yo) / dY;
+    ci[0] = di; ck[0] = dk;
+    nseg = 2;
+  } else if (res == 2) {
     const float xb = di > 0 ? 1.f : 0.f, yb = dk > 0 ? 1.f : 0.f;
     const float fx = (xb - Xo) / dX, fy = (yb - Yo) / dY;  // path fractions of the two crossings
     if (fx == fy) return true;  // through the corner: the reference deposits nothing (:278-300)
-    if (fx < fy) {  // radial boundary first: old cell -> (0, dk) -> new
-      seg(0.f, fx, di, dk);
-      seg(fx, fy, 0, dk);
-      seg(fy, 1.f, 0, 0);
-    } else {        // axial boundary first: old cell -> (di, 0) -> new
-      seg(0.f, fy, di, dk);
-      seg(fy, fx, di, 0);
-      seg(fx, 1.f, 0, 0);
-    }
+    ci[0] = di; ck[0] = dk;
+    if (fx < fy) { f[1] = fx; f[2] = fy; ci[1] = 0; ck[1] = dk; }   // radial boundary first
+    else         { f[1] = fy; f[2] = fx; ci[1] = di; ck[1] = 0; }   // axial boundary first
+    nseg = 3;
+  }
+  for (int s = 0; s < nseg; ++s) {
+    const float f0 = f[s], f1 = f[s + 1];
+    vb_simple(a, d, q, in + ci[s], kn + ck[s], Xo + f0 * dX - ci[s], Yo + f0 * dY - ck[s],
+              (f1 - f0) * dX, (f1 - f0) * dY);
   }
   return true;
 }
@@ -468,7 +490,8 @@ __device__ __forceinline__ bool vb_rz(const StepArgs& a, const Dep& d, float q, 
 // ZigZag current (currentZigZag.cpp:22-136) with the reference's metre-valued
 // weights W = (mean position - cell edge) in metres.
 
-__device__ __forceinline__ void zigzag(const StepArgs& a, const Dep& d, float qw, float vphi,
+template <class D>
+__device__ __forceinline__ void zigzag(const StepArgs& a, const D& d, float qw, float vphi,
                                        int in, int kn, float Xo, float Yo, float Xn, float Yn) {
   const int io = (int)floorf(Xo), ko = (int)floorf(Yo);  // relative to the new cell
   const int imid = in + (int)floorf(0.5f * (Xo + Xn));
@@ -501,26 +524,28 @@ __device__ __forceinline__ void zigzag(const StepArgs& a, const Dep& d, float qw
 
 // ---------------------------------------------------------------------------
 
-// One macroparticle: gather, push, move, reflect, bind, runaway test and
-// current.  Returns without touching the particle if it is dead.
-__device__ __forceinline__ void advance_one(const StepArgs& a, const SpeciesF32Buffers& b,
-                                            size_t j, const Dep& d) {
-  const int cell = b.cell[j];
-  if (cell < 0) return;
-  const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
-  const float fr0 = b.off_r[j], fz0 = b.off_z[j];
-  if (ci0 < -1 || ci0 > a.nr || ck0 < -1 || ck0 > a.nz) {  // gather would leave the halo
-    raise_error(a.st, kErrOutOfGrid);
-    return;
-  }
+// What the current deposit of one moved particle needs: the new cell and
+// offsets, the old point relative to the new cell, the exact displacement.
+struct Moved {
+  int ci, ck;      // new cell
+  int ci0, ck0;    // old cell
+  float fr, fz;    // new offsets
+  float Xo, Yo;    // old point relative to the new cell
+  float dX, dY;    // displacement (straight line to the mirrored point after a reflection)
+  float w, vphi;
+};
+
+// One macroparticle after its gather: push, move, reflect, bind and the
+// runaway test (pusher*.cpp, specieP.cpp:482-491, 609-640, beamP.cpp:159-177,
+// SMB.cpp:252-337).  Writes the particle back; returns false if it left the
+// domain (no current) and fills `m` otherwise.
+__device__ __forceinline__ bool advance_one(const StepArgs& a, const SpeciesF32Buffers& b,
+                                            size_t j, int ci0, int ck0, float fr0, float fz0,
+                                            const float e[3], const float bb[3], Moved* m) {
   float v[3] = {b.vr[j], b.vphi[j], b.vz[j]};
-  const float w = b.w[j];
-  float e[3], bb[3];
-  gather(a, ci0, fr0, ck0, fz0, e, bb);
-  if (!push(a, e, bb, v)) return;
-  // mover_cylindrical + back_position_to_rz (specieP.cpp:482-491, 609-622):
-  // x' = sqrt((x+dx)^2 + dy^2), taken as dx + dy^2/(X + x') to keep the
-  // displacement's precision.
+  if (!push(a, e, bb, v)) return false;
+  // mover_cylindrical + back_position_to_rz: x' = sqrt((x+dx)^2 + dy^2),
+  // taken as dx + dy^2/(X + x') to keep the displacement's precision.
   const float dx = v[0] * a.dt_dr, dyp = v[1] * a.dt_dr, dzz = v[2] * a.dt_dz;
   const float X = (float)ci0 + fr0 + dx;
   const float xn = sqrtf(X * X + dyp * dyp);
@@ -537,7 +562,8 @@ __device__ __forceinline__ void advance_one(const StepArgs& a, const SpeciesF32B
   bool reflected = false;
   if (a.is_beam) {  // BeamP::reflect beamP.cpp:159-177
     if (ci < 0 || (ci == 0 && fr < 0.5f)) { mirror(&ci, &fr, 0); v[0] = -v[0]; reflected = true; }
-  } else {
+  } else if (ci < 1 || ci > a.nr - 2 || ck < 1 || ck > a.nz - 2) {
+    // only cells next to a wall can cross one (walls at x = 1/2 and nr - 1/2)
     const int c0 = ci, k0 = ck;
     const float f0 = fr, g0 = fz;
     if (!reflect(a, &ci, &fr, &ck, &fz, &v[0], &v[2])) raise_error(a.st, kErrReflectLoop);
@@ -550,62 +576,146 @@ __device__ __forceinline__ void advance_one(const StepArgs& a, const SpeciesF32B
   const float cs = sqrtf(1.f - sn * sn);  // back_velocity_to_rz :624-640
   const float vr2 = cs * v[0] - sn * v[1];
   const float vp2 = sn * v[0] + cs * v[1];
-  v[0] = vr2;
-  v[1] = vp2;
-  b.vr[j] = v[0];
-  b.vphi[j] = v[1];
+  b.vr[j] = vr2;
+  b.vphi[j] = vp2;
   b.vz[j] = v[2];
   if (ci < 0 || ck < 0 || ci >= a.nr || ck >= a.nz) {  // runaway collector SMB.cpp:252-337
     b.cell[j] = kDeadCell;
     atomicAdd(&a.st->removed, 1ull);
     atomicAdd(&a.st->dead_slots, 1ull);
-    return;
+    return false;
   }
   b.cell[j] = pack_cell(ci, ck);
   b.off_r[j] = fr;
   b.off_z[j] = fz;
-  // the old point relative to the new cell
-  const float Xo = (float)(ci0 - ci) + fr0, Yo = (float)(ck0 - ck) + fz0;
-  if (a.current == 1) {
-    zigzag(a, d, w, v[1], ci, ck, Xo, Yo, fr, fz);
-    return;
-  }
-  vb_azimuthal(a, d, w, v[1], ci, ck, Xo + 0.5f * dX, Yo + 0.5f * dY);
-  if (!vb_rz(a, d, w, ci, ck, Xo, Yo, dX, dY, fr, fz)) atomicAdd(&a.st->move_errors, 1ull);
+  m->ci = ci; m->ck = ck; m->ci0 = ci0; m->ck0 = ck0;
+  m->fr = fr; m->fz = fz;
+  m->Xo = (float)(ci0 - ci) + fr0;
+  m->Yo = (float)(ck0 - ck) + fz0;
+  m->dX = dX; m->dY = dY;
+  m->w = b.w[j];
+  m->vphi = vp2;
+  return true;
 }
 
-// Particles [j0, j1), one per thread, current straight to the global grid
+// The current of one moved particle (CUR: 0 Villasenor-Buneman, 1 ZigZag).
+template <int CUR, class D>
+__device__ __forceinline__ void deposit(const StepArgs& a, const D& d, const Moved& m) {
+  if (CUR == 1) {
+    zigzag(a, d, m.w, m.vphi, m.ci, m.ck, m.Xo, m.Yo, m.fr, m.fz);
+  } else {
+    vb_azimuthal(a, d, m.w, m.vphi, m.ci, m.ck, m.Xo + 0.5f * m.dX, m.Yo + 0.5f * m.dY);
+    if (!vb_rz(a, d, m.w, m.ci, m.ck, m.Xo, m.Yo, m.dX, m.dY, m.fr, m.fz))
+      atomicAdd(&a.st->move_errors, 1ull);
+  }
+}
+
+__device__ __forceinline__ bool cell_in_halo(const StepArgs& a, int cell) {
+  const int ci = cell_r_of(cell), ck = cell_z_of(cell);
+  if (ci < -1 || ci > a.nr || ck < -1 || ck > a.nz) {  // the gather would leave the halo
+    raise_error(a.st, kErrOutOfGrid);
+    return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ FieldView global_view(const StepArgs& a) {
+  return FieldView{a.Er, a.plane, a.ld, -2, -2};
+}
+
+__device__ __forceinline__ GlobalDep global_dep(const StepArgs& a) {
+  return GlobalDep{a.Jr, a.plane, a.ld};
+}
+
+// Particles [j0, j1), one per thread, fields and current on the global grid
 // (particles appended since the last tile sort).
+template <int CUR>
 __global__ void __launch_bounds__(kThreads) step_flat_kernel(StepArgs a, SpeciesF32Buffers b,
                                                              size_t j0, size_t j1) {
   const size_t j = j0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (j >= j1) return;
-  const Dep d{{a.Jr, a.Jp, a.Jz}, a.ld, nullptr, 0, 0, 0, 0};
-  advance_one(a, b, j, d);
+  const int cell = b.cell[j];
+  if (cell < 0 || !cell_in_halo(a, cell)) return;
+  const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
+  const float fr0 = b.off_r[j], fz0 = b.off_z[j];
+  float e[3], bb[3];
+  gather(global_view(a), a.fixed, ci0, fr0, ck0, fz0, e, bb);
+  Moved m;
+  if (advance_one(a, b, j, ci0, ck0, fr0, fz0, e, bb, &m)) deposit<CUR>(a, global_dep(a), m);
 }
 
-// One block per tile of TileGrid: the tile's particles (grouped by the last
-// sort) deposit into a shared-memory window of the tile plus `halo` cells,
-// which is added to the global grid once at the end.
-__global__ void __launch_bounds__(kThreads) step_tiled_kernel(StepArgs a, SpeciesF32Buffers b,
+// Shared memory of a tile block: the six field components over the tile
+// plus `halo` + 1 nodes per side, then the three current components over
+// the tile plus `halo` nodes per side.
+__host__ __device__ inline int field_window_r(const TileGrid& tg) { return tg.tr + 2 * tg.halo + 2; }
+__host__ __device__ inline int field_window_z(const TileGrid& tg) { return tg.tz + 2 * tg.halo + 2; }
+__host__ __device__ inline size_t tile_smem_bytes(const TileGrid& tg) {
+  return sizeof(float) * (6 * (size_t)field_window_r(tg) * field_window_z(tg) +
+                          3 * (size_t)(tg.tr + 2 * tg.halo) * (tg.tz + 2 * tg.halo));
+}
+
+// One block per tile: the tile's particles (grouped by the last sort) gather
+// from a shared copy of the fields around the tile and deposit into a shared
+// current window that is added to the global grid once at the end.
+// Particles that drifted beyond the halo use the global grid.
+template <int CUR>
+__global__ void __launch_bounds__(kThreads, 5) step_tiled_kernel(StepArgs a, SpeciesF32Buffers b,
                                                               TileGrid tg) {
-  extern __shared__ float sJ[];
+  extern __shared__ float smem[];
   const int t = blockIdx.x;
+  // blockIdx.y of gridDim.y blocks sharing the tile takes every gridDim.y-th run of blockDim.x
+  const unsigned s = b.tile_start[t] + blockIdx.y * blockDim.x, e = b.tile_start[t + 1];
+  if (s >= e) return;
   const int tr = t / tg.ntz, tz = t - tr * tg.ntz;
+  const int r0 = tr * tg.tr, z0 = tz * tg.tz;  // first cell of the tile
+  const int fwr = field_window_r(tg), fwz = field_window_z(tg);
+  const int fi0 = r0 - tg.halo - 1, fk0 = z0 - tg.halo - 1;  // field window origin (node)
+  float* sF = smem;
+  float* sJ = smem + 6 * fwr * fwz;
   const int wr = tg.tr + 2 * tg.halo, wz = tg.tz + 2 * tg.halo;
-  const Dep d{{a.Jr, a.Jp, a.Jz}, a.ld, sJ, tr * tg.tr - tg.halo, tz * tg.tz - tg.halo, wr, wz};
-  const int nw = 3 * wr * wz;
-  for (int e = threadIdx.x; e < nw; e += blockDim.x) sJ[e] = 0.f;
+  const int ji0 = r0 - tg.halo, jk0 = z0 - tg.halo;  // current window origin (node)
+  // load the field window (nodes outside the halo-padded grid read as 0)
+  const int nf = fwr * fwz;
+  for (int q = threadIdx.x; q < 6 * nf; q += blockDim.x) {
+    const int c = q / nf, rem = q - c * nf;
+    const int i = fi0 + rem / fwz, k = fk0 + rem % fwz;
+    float val = 0.f;
+    if (i >= -2 && i < a.nr + 2 && k >= -2 && k < a.nz + 2)
+      val = __ldg(a.Er + c * a.plane + (i + 2) * a.ld + (k + 2));
+    sF[q] = val;
+  }
+  for (int q = threadIdx.x; q < 3 * wr * wz; q += blockDim.x) sJ[q] = 0.f;
   __syncthreads();
-  const unsigned s = b.tile_start[t], e = b.tile_start[t + 1];
-  for (unsigned j = s + threadIdx.x; j < e; j += blockDim.x) advance_one(a, b, j, d);
+  const FieldView sv{sF, nf, fwz, fi0, fk0};
+  const SharedDep sd{sJ, wr, wz, ji0, jk0};
+  for (unsigned j = s + threadIdx.x; j < e; j += gridDim.y * blockDim.x) {
+    const int cell = b.cell[j];
+    if (cell < 0) continue;
+    const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
+    // the gather reads nodes ci-1 .. ci+1, ck-1 .. ck+1
+    const bool inside = ci0 - 1 >= fi0 && ci0 + 2 < fi0 + fwr && ck0 - 1 >= fk0 && ck0 + 2 < fk0 + fwz;
+    if (!inside && !cell_in_halo(a, cell)) continue;
+    const float fr0 = b.off_r[j], fz0 = b.off_z[j];
+    float ef[3], bf[3];
+    if (inside) gather(sv, a.fixed, ci0, fr0, ck0, fz0, ef, bf);
+    else gather(global_view(a), a.fixed, ci0, fr0, ck0, fz0, ef, bf);
+    Moved m;
+    if (!advance_one(a, b, j, ci0, ck0, fr0, fz0, ef, bf, &m)) continue;
+    // every node a deposit touches lies in [min(old, new) cell, max + 1] per axis
+    const int lo_r = min(m.ci0, m.ci), hi_r = max(m.ci0, m.ci) + 1;
+    const int lo_z = min(m.ck0, m.ck), hi_z = max(m.ck0, m.ck) + 1;
+    if (lo_r >= ji0 && hi_r < ji0 + wr && lo_z >= jk0 && hi_z < jk0 + wz)
+      deposit<CUR>(a, sd, m);
+    else
+      deposit<CUR>(a, global_dep(a), m);
+  }
   __syncthreads();
-  for (int q = threadIdx.x; q < nw; q += blockDim.x) {
+  for (int q = threadIdx.x; q < 3 * wr * wz; q += blockDim.x) {
     const float v = sJ[q];
     if (v == 0.f) continue;
     const int comp = q / (wr * wz), rem = q - comp * wr * wz;
-    const int i = d.i0 + rem / wz, k = d.k0 + rem % wz;
-    atomicAdd(d.J[comp] + (long long)(i + 2) * a.ld + (k + 2), v);
+    const int i = ji0 + rem / wz, k = jk0 + rem % wz;
+    atomicAdd(a.Jr + comp * a.plane + (i + 2) * a.ld + (k + 2), v);  // J_r, J_phi, J_z are consecutive planes
   }
 }
 
@@ -619,6 +729,7 @@ inline f32::StepArgs f32_step_args(const F32Step& st, double charge, double mass
   a.Hr = st.fld[3]; a.Hp = st.fld[4]; a.Hz = st.fld[5];
   a.Jr = st.fld[9]; a.Jp = st.fld[10]; a.Jz = st.fld[11];
   a.nr = g.nr; a.nz = g.nz; a.ld = g.ld;
+  a.plane = st.plane;
   a.dt_dr = (float)(g.dt / g.dr);
   a.dt_dz = (float)(g.dt / g.dz);
   const double c2m = charge * g.dt / (2 * mass);

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <vector>
 
+#include "pcg.h"
 #include "pcg_f32.h"
 #include "pcg_f32_step.cuh"
 #include "pcg_philox.cuh"
@@ -113,31 +114,125 @@ __global__ void export_kernel(GridGeom g, SpeciesF32Buffers b, size_t n, const u
 }
 
 // ---------------------------------------------------------------------------
-// Tile sort: counting sort of live particles by tile, into the second buffer.
+// Tile sort: live particles grouped by tile, and inside a tile in layered
+// order: layer q holds the particles of rank q in their cell (the q-th to
+// arrive there), one per occupied cell, in cell order (z fastest).  A warp
+// then takes 32 particles of 32 neighbouring cells, so its gathers from and
+// deposits to the block's shared windows hit distinct addresses and banks.
 
-__device__ __forceinline__ int tile_key(int cell, const TileGrid& tg) {
+static_assert(kTileR * kTileZ <= kTileCells, "tile larger than the layer masks");
+
+// tile of a packed cell and the cell's index inside the tile (z fastest)
+__device__ __forceinline__ int tile_key(int cell, const TileGrid& tg, int* lc) {
   if (cell < 0) return -1;
-  return (cell_r_of(cell) / tg.tr) * tg.ntz + cell_z_of(cell) / tg.tz;
+  const int ci = cell_r_of(cell), ck = cell_z_of(cell);
+  const int tr = ci / tg.tr, tz = ck / tg.tz;
+  *lc = (ci - tr * tg.tr) * tg.tz + (ck - tz * tg.tz);
+  return tr * tg.ntz + tz;
 }
 
-__global__ void tile_hist_kernel(const int* cell, size_t n, TileGrid tg, unsigned* counts) {
+// rank of each particle in its cell (warp-aggregated counter increments)
+__global__ void cell_rank_kernel(const int* cell, size_t n, TileGrid tg, unsigned* cell_count,
+                                 unsigned* rank) {
   const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const int key = j < n ? tile_key(cell[j], tg) : -1;
-  const unsigned mask = __match_any_sync(0xffffffffu, key);
-  const int leader = __ffs(mask) - 1;
-  if ((int)(threadIdx.x & 31) == leader && key >= 0) atomicAdd(counts + key, (unsigned)__popc(mask));
-}
-
-__global__ void tile_scatter_kernel(SpeciesF32Buffers b, size_t n, TileGrid tg, unsigned* cursor) {
-  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const int key = j < n ? tile_key(b.cell[j], tg) : -1;
+  int lc = 0;
+  const int t = j < n ? tile_key(cell[j], tg, &lc) : -1;
+  const int key = t < 0 ? -1 : t * kTileCells + lc;
   const unsigned mask = __match_any_sync(0xffffffffu, key);
   const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
   unsigned base = 0;
-  if (lane == leader && key >= 0) base = atomicAdd(cursor + key, (unsigned)__popc(mask));
+  if (lane == leader && key >= 0) base = atomicAdd(cell_count + key, (unsigned)__popc(mask));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (key < 0) return;
-  const unsigned pos = base + __popc(mask & ((1u << lane) - 1u));
+  if (j < n) rank[j] = key < 0 ? ~0u : base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// One block per tile: the tile's particle count and its layer tables.
+__global__ void __launch_bounds__(kThreads) tile_layers_kernel(TileGrid tg, SpeciesF32Buffers b,
+                                                               unsigned* tile_count) {
+  __shared__ unsigned cnt[kTileCells];
+  __shared__ unsigned layer_size[kLayerCap];
+  __shared__ unsigned red_max[kThreads / 32], red_sum[kThreads / 32];
+  const int t = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned mx = 0, sum = 0;
+  for (int c = threadIdx.x; c < kTileCells; c += blockDim.x) {
+    const unsigned v = b.cell_count[(size_t)t * kTileCells + c];
+    cnt[c] = v;
+    mx = max(mx, v);
+    sum += v;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  }
+  if (lane == 0) { red_max[wid] = mx; red_sum[wid] = sum; }
+  __syncthreads();
+  mx = 0; sum = 0;
+  for (int w = 0; w < kThreads / 32; ++w) { mx = max(mx, red_max[w]); sum += red_sum[w]; }
+  if (threadIdx.x == 0) {
+    tile_count[t] = sum;
+    b.overflow[t] = 0;
+    if (sum) { atomicMax(b.sort_info, sum); atomicAdd(b.sort_info + 1, 1u); }
+  }
+  const int nq = (int)min(mx, (unsigned)kLayerCap);
+  // layer q: word w of the mask has bit l set when cell 32 w + l holds more than q
+  for (int q = wid; q < nq; q += kThreads / 32) {
+    unsigned mine = 0;
+    for (int w = 0; w < kTileWords; ++w) {
+      const unsigned m = __ballot_sync(0xffffffffu, cnt[w * 32 + lane] > (unsigned)q);
+      if (lane == w) mine = m;
+    }
+    // exclusive prefix of the set bits over the words (lanes 0..15)
+    const unsigned pc = lane < kTileWords ? __popc(mine) : 0u;
+    unsigned incl = pc;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const size_t at = ((size_t)t * kLayerCap + q) * kTileWords + lane;
+    if (lane < kTileWords) {
+      b.layer_mask[at] = mine;
+      b.layer_prefix[at] = (unsigned short)(incl - pc);
+    }
+    if (lane == 31) layer_size[q] = incl;
+  }
+  __syncthreads();
+  if (wid == 0) {  // layer starts: exclusive scan of the layer sizes, 4 per lane
+    unsigned v[kLayerCap / 32], tot = 0;
+    for (int r = 0; r < kLayerCap / 32; ++r) {
+      const int q = lane * (kLayerCap / 32) + r;
+      v[r] = q < nq ? layer_size[q] : 0u;
+      tot += v[r];
+    }
+    unsigned incl = tot;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
+    }
+    unsigned run = incl - tot;
+    unsigned* ls = b.layer_start + (size_t)t * (kLayerCap + 1);
+    for (int r = 0; r < kLayerCap / 32; ++r) {
+      ls[lane * (kLayerCap / 32) + r] = run;
+      run += v[r];
+    }
+    if (lane == 31) ls[kLayerCap] = run;  // the overflow run starts after all kept layers
+  }
+}
+
+__global__ void tile_scatter_kernel(SpeciesF32Buffers b, size_t n, TileGrid tg) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int lc = 0;
+  const int t = tile_key(b.cell[j], tg, &lc);
+  if (t < 0) return;
+  const unsigned q = b.rank[j];
+  unsigned pos = b.tile_start[t];
+  if (q < (unsigned)kLayerCap) {
+    const size_t at = ((size_t)t * kLayerCap + q) * kTileWords + (lc >> 5);
+    pos += b.layer_start[(size_t)t * (kLayerCap + 1) + q] + b.layer_prefix[at] +
+           __popc(b.layer_mask[at] & ((1u << (lc & 31)) - 1u));
+  } else {
+    pos += b.layer_start[(size_t)t * (kLayerCap + 1) + kLayerCap] + atomicAdd(b.overflow + t, 1u);
+  }
   b.cell2[pos] = b.cell[j];
   b.off_r2[pos] = b.off_r[j];
   b.off_z2[pos] = b.off_z[j];
@@ -159,23 +254,33 @@ void swap_buffers(SpeciesF32Buffers& b) {
   std::swap(b.id, b.id2);
 }
 
+// Blocks per tile for the step: enough to fill the GPU when few tiles are
+// occupied (a narrow beam), each with at least kMinSplitParticles particles.
+constexpr unsigned kTargetBlocks = 148 * 8, kMinSplitParticles = 4 * kThreads;
+
 int tile_sort(const TileGrid& tg, SpeciesF32Buffers& b, size_t* n, cudaStream_t s) {
   const size_t nt = (size_t)tg.ntiles;
-  unsigned* counts = b.tile_cursor;  // reused: counts, then cursors
-  cudaMemsetAsync(counts, 0, (nt + 1) * sizeof(unsigned), s);
-  if (*n) tile_hist_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b.cell, *n, tg, counts);
-  size_t tmp = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmp, counts, b.tile_start, (int)(nt + 1), s);
-  void* tmpbuf = nullptr;
-  if (cudaMallocAsync(&tmpbuf, tmp, s) != cudaSuccess) return -1;
-  cub::DeviceScan::ExclusiveSum(tmpbuf, tmp, counts, b.tile_start, (int)(nt + 1), s);
-  cudaFreeAsync(tmpbuf, s);
-  cudaMemcpyAsync(b.tile_cursor, b.tile_start, nt * sizeof(unsigned), cudaMemcpyDeviceToDevice, s);
-  if (*n) tile_scatter_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b, *n, tg, b.tile_cursor);
-  unsigned kept = 0;
-  cudaMemcpyAsync(&kept, b.tile_start + nt, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  unsigned* counts = b.tile_cursor;
+  cudaMemsetAsync(b.cell_count, 0, nt * kTileCells * sizeof(unsigned), s);
+  cudaMemsetAsync(counts + nt, 0, sizeof(unsigned), s);
+  cudaMemsetAsync(b.sort_info, 0, 2 * sizeof(unsigned), s);
+  if (*n) cell_rank_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b.cell, *n, tg, b.cell_count, b.rank);
+  tile_layers_kernel<<<(unsigned)nt, kThreads, 0, s>>>(tg, b, counts);
+  size_t tmp = b.scan_tmp_bytes;
+  cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp, counts, b.tile_start, (int)(nt + 1), s);
+  if (*n) tile_scatter_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b, *n, tg);
+  cudaMemcpyAsync(b.host_info, b.tile_start + nt, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(b.host_info + 1, b.sort_info, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
   swap_buffers(b);
+  const unsigned kept = b.host_info[0], largest = b.host_info[1], occupied = b.host_info[2];
+  unsigned splits = 1;
+  if (occupied) {
+    splits = std::max(1u, std::min((kTargetBlocks + occupied - 1) / occupied,
+                                   (largest + kMinSplitParticles - 1) / kMinSplitParticles));
+    splits = std::min(splits, 65535u);
+  }
+  b.splits = (int)splits;
   *n = kept;
   b.sorted_n = kept;
   b.steps_since_sort = 0;
@@ -265,14 +370,28 @@ int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg) {
   if (cudaMalloc((void**)&b.id2, cap * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.tile_start, (tg.ntiles + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.tile_cursor, (tg.ntiles + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
+  const size_t nt = (size_t)tg.ntiles;
+  if (cudaMalloc((void**)&b.rank, cap * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.cell_count, nt * kTileCells * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.layer_mask, nt * kLayerCap * kTileWords * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.layer_prefix, nt * kLayerCap * kTileWords * sizeof(unsigned short)) != cudaSuccess)
+    return -1;
+  if (cudaMalloc((void**)&b.layer_start, nt * (kLayerCap + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.overflow, nt * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.sort_info, 2 * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMallocHost((void**)&b.host_info, 3 * sizeof(unsigned)) != cudaSuccess) return -1;
+  cub::DeviceScan::ExclusiveSum(nullptr, b.scan_tmp_bytes, b.tile_cursor, b.tile_start, (int)(nt + 1));
+  if (cudaMalloc(&b.scan_tmp, std::max<size_t>(b.scan_tmp_bytes, 16)) != cudaSuccess) return -1;
   return 0;
 }
 
 void f32_free_species(SpeciesF32Buffers& b) {
   void* arrs[] = {b.cell, b.off_r, b.off_z, b.vr, b.vphi, b.vz, b.w, b.id,
                   b.cell2, b.off_r2, b.off_z2, b.vr2, b.vphi2, b.vz2, b.w2, b.id2,
-                  b.tile_start, b.tile_cursor};
+                  b.tile_start, b.tile_cursor, b.rank, b.cell_count, b.layer_mask, b.layer_prefix,
+                  b.layer_start, b.overflow, b.sort_info, b.scan_tmp};
   for (void* a : arrs) cudaFree(a);
+  cudaFreeHost(b.host_info);
   b = SpeciesF32Buffers();
 }
 
@@ -312,11 +431,19 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   const f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
   const TileGrid& tg = st.tiles;
   if (b.sorted_n) {
-    const size_t smem = 3 * (size_t)(tg.tr + 2 * tg.halo) * (tg.tz + 2 * tg.halo) * sizeof(float);
-    f32::step_tiled_kernel<<<tg.ntiles, f32::kThreads, smem, s>>>(a, b, tg);
+    const size_t smem = f32::tile_smem_bytes(tg);
+    if (st.current == PCG_CURRENT_ZIGZAG)
+      f32::step_tiled_kernel<1><<<dim3(tg.ntiles, b.splits), f32::kThreads, smem, s>>>(a, b, tg);
+    else
+      f32::step_tiled_kernel<0><<<dim3(tg.ntiles, b.splits), f32::kThreads, smem, s>>>(a, b, tg);
   }
-  if (*n > b.sorted_n)
-    f32::step_flat_kernel<<<blocks_for(*n - b.sorted_n), f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
+  if (*n > b.sorted_n) {
+    const unsigned nb = blocks_for(*n - b.sorted_n);
+    if (st.current == PCG_CURRENT_ZIGZAG)
+      f32::step_flat_kernel<1><<<nb, f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
+    else
+      f32::step_flat_kernel<0><<<nb, f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
+  }
   b.steps_since_sort += 1;
   return 0;
 }
