@@ -63,6 +63,7 @@ struct pcg_handle {
   double* f64[12] = {};
   float* f32[12] = {};            // planes of one allocation, f32_plane floats apart
   size_t f32_plane = 0;
+  float4* recip32 = nullptr;      // radial reciprocal table of the float step
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -462,6 +463,7 @@ int fused_step(pcg_handle* h) {
     st.g = h->g;
     for (int c = 0; c < 12; ++c) st.fld[c] = h->f32[c];
     st.plane = (int)h->f32_plane;
+    st.recip = h->recip32;
     st.pusher = h->cfg.pusher;
     st.current = h->cfg.current;
     st.fixed = fixed;
@@ -538,6 +540,18 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
     if ((rc = dalloc(h, &h->f32[0], 12 * h->f32_plane)) != PCG_OK) return bail(rc);
     cudaMemsetAsync(h->f32[0], 0, sizeof(float) * 12 * h->f32_plane, h->stream);
     for (int c = 1; c < 12; ++c) h->f32[c] = h->f32[0] + c * h->f32_plane;
+    // rows i = -2 .. nr+2: {1/(2i+1), 1/(2i+2), 1/(2i+3), 1/(2i+4)}, {1/i, 1/(i+1), 1/(i+1/2), 0},
+    // each correctly rounded from double, 0 where the denominator is 0
+    const int rows = h->g.nr + 5;
+    std::vector<float4> rt(2 * (size_t)rows);
+    auto inv = [](double d) { return d == 0.0 ? 0.f : (float)(1.0 / d); };
+    for (int r = 0; r < rows; ++r) {
+      const double i = r - 2;
+      rt[2 * r] = make_float4(inv(2 * i + 1), inv(2 * i + 2), inv(2 * i + 3), inv(2 * i + 4));
+      rt[2 * r + 1] = make_float4(inv(i), inv(i + 1), inv(i + 0.5), 0.f);
+    }
+    if ((rc = dalloc(h, &h->recip32, rt.size())) != PCG_OK) return bail(rc);
+    cudaMemcpyAsync(h->recip32, rt.data(), sizeof(float4) * rt.size(), cudaMemcpyHostToDevice, h->stream);
     std::vector<float> prof[3];
     const std::vector<double>* src[3] = {&sr, &s0, &sl};
     for (int c = 0; c < 3; ++c) {
@@ -557,6 +571,7 @@ int pcg_destroy(pcg_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (int c = 0; c < 12; ++c) cudaFree(h->f64[c]);
   cudaFree(h->f32[0]);
+  cudaFree(h->recip32);
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
   cudaFree(h->reset);
   cudaFree(h->scratch);

@@ -19,7 +19,8 @@ template <typename Real>
 struct YeeArgs;
 
 // Tiles of tr x tz cells; a block's shared window adds `halo` cells per side.
-constexpr int kTileCells = 512;             // tr * tz at most
+constexpr int kTileR = 8, kTileZ = 64, kHalo = 3;  // every tile is kTileR x kTileZ cells
+constexpr int kTileCells = kTileR * kTileZ;
 constexpr int kTileWords = kTileCells / 32;  // 32-cell words of a tile's layer mask
 constexpr int kLayerCap = 128;              // layers kept in order; deeper ranks go to an overflow run
 struct TileGrid {
@@ -63,6 +64,7 @@ struct F32Step {
   GridGeom g;
   float* fld[12];  // planes of one allocation: fld[c] = fld[0] + c * plane
   int plane;
+  const float4* recip;  // radial reciprocal table, 2 float4 per node row from i = -2
   int pusher, current, fixed;
   DevStatus* status;
   TileGrid tiles;

@@ -38,8 +38,18 @@ struct StepArgs {
   float dr_m, dz_m, dt_s;      // dr, dz, dt in SI (ZigZag keeps metre-valued weights)
   float zz_vol;                // 1/(PI dz dr^2)
   int pusher, current, fixed, is_beam;
+  // per radial node i (row i + 2): {1/(2i+1), 1/(2i+2), 1/(2i+3), 1/(2i+4)},
+  // {1/i, 1/(i+1), 1/(i+1/2), 0}; a zero where the denominator is zero
+  const float4* rt;
   DevStatus* st;
 };
+
+
+// Shared-memory windows of a tile block, fixed by the tile geometry: the
+// fields over the tile plus kHalo + 1 nodes per side, the current over the
+// tile plus kHalo nodes per side.
+constexpr int kFWR = kTileR + 2 * kHalo + 2, kFWZ = kTileZ + 2 * kHalo + 2;
+constexpr int kJWR = kTileR + 2 * kHalo, kJWZ = kTileZ + 2 * kHalo;
 
 // Grids are far below 2^31 nodes, so node indices are 32-bit.
 __device__ __forceinline__ int node(const StepArgs& a, int i, int k) {
@@ -66,52 +76,66 @@ __device__ __forceinline__ Stagger half_shift(int c, float f) {  // floor(x - 1/
   return s;
 }
 
-__device__ __forceinline__ void radial_w_half(int i, float u, float* w0, float* w1) {
-  const float fi = (float)i;
-  *w0 = (1.f - u) * (2.f * fi + 1.f + u) / (2.f * fi + 2.f);
-  *w1 = u * (2.f * fi + 2.f + u) / (2.f * fi + 4.f);
-}
-
-__device__ __forceinline__ void radial_w_int(int i, float u, float* w0, float* w1) {
-  const float fi = (float)i;
-  *w0 = (1.f - u) * (2.f * fi + u) / (2.f * fi + 1.f);
-  *w1 = u * (2.f * fi + 1.f + u) / (2.f * fi + 3.f);
-}
-
 // Six field components (E_r, E_phi, E_z, H_r, H_phi, H_z) seen through a
-// window: component c at node (i, k) is base[c * plane + (i - i0) * ld + (k - k0)].
-// The global grid is the window with i0 = k0 = -2, ld = nz + 4 and the
-// allocation's plane stride; a block's shared-memory copy of its tile is a
-// smaller one.  Five scalars, so a thread picks either with selects.
-struct FieldView {
+// window: component c at node (i, k) is at(c, i, k).  GlobalFields is the
+// grid itself (i0 = k0 = -2, ld = nz + 4, the allocation's plane stride);
+// SharedFields a block's copy around its tile, whose strides are constants.
+// Each also serves the radial reciprocal rows (recip_row / recip_int).
+struct GlobalFields {
   const float* base;
   int plane, ld, i0, k0;
+  const float4* rt;  // the global table, row i at rt[2 * (i + 2)]
+  __device__ __forceinline__ const float* at(int c, int i, int k) const {
+    return base + c * plane + (i - i0) * ld + (k - k0);
+  }
+  __device__ __forceinline__ int stride() const { return ld; }
+  __device__ __forceinline__ float4 row(int i) const { return __ldg(rt + 2 * (i + 2)); }
+  __device__ __forceinline__ float4 row_int(int i) const { return __ldg(rt + 2 * (i + 2) + 1); }
 };
 
-__device__ __forceinline__ float interp4(const FieldView& fv, int c, int i, int k,
-                                         float w0, float w1, float v) {
-  const float* F = fv.base + c * fv.plane + (i - fv.i0) * fv.ld + (k - fv.k0);
-  const float f00 = F[0], f10 = F[fv.ld];
-  const float f01 = F[1], f11 = F[fv.ld + 1];
+struct SharedFields {
+  static constexpr int kLd = kFWZ, kPlane = kFWR * kFWZ;
+  const float* base;
+  int i0, k0;
+  const float4* rt;  // the window's rows of the table, row i at rt[2 * (i - i0)]
+  __device__ __forceinline__ const float* at(int c, int i, int k) const {
+    return base + c * kPlane + (i - i0) * kLd + (k - k0);
+  }
+  __device__ __forceinline__ int stride() const { return kLd; }
+  __device__ __forceinline__ float4 row(int i) const { return rt[2 * (i - i0)]; }
+  __device__ __forceinline__ float4 row_int(int i) const { return rt[2 * (i - i0) + 1]; }
+};
+
+template <class V>
+__device__ __forceinline__ float interp4(const V& fv, int c, int i, int k, float w0, float w1, float v) {
+  const float* F = fv.at(c, i, k);
+  const int ld = fv.stride();
+  const float f00 = F[0], f10 = F[ld];
+  const float f01 = F[1], f11 = F[ld + 1];
   return (f00 * w0 + f10 * w1) * (1.f - v) + (f01 * w0 + f11 * w1) * v;
 }
 
-__device__ __forceinline__ void gather(const FieldView& fv, int fixed, int ci, float fr, int ck,
+template <class V>
+__device__ __forceinline__ void gather(const StepArgs& a, const V& fv, int ci, float fr, int ck,
                                        float fz, float e[3], float b[3]) {
   const Stagger rh = half_shift(ci, fr), zh = half_shift(ck, fz);
-  float h0, h1, n0, n1;
-  radial_w_half(rh.i, rh.u, &h0, &h1);
-  radial_w_int(ci, fr, &n0, &n1);
+  // ring-volume weights; the reciprocals of their denominators come from
+  // the table (row ci: 1/(2ci+1), 1/(2ci+3); row rh.i: 1/(2i+2), 1/(2i+4))
+  const float4 tn = fv.row(ci), th = fv.row(rh.i);
+  const float fi = (float)ci, fh = (float)rh.i, u = rh.u;
+  const float n0 = (1.f - fr) * (2.f * fi + fr) * tn.x, n1 = fr * (2.f * fi + 1.f + fr) * tn.z;
+  const float h0 = (1.f - u) * (2.f * fh + 1.f + u) * th.y, h1 = u * (2.f * fh + 2.f + u) * th.w;
   // E_r: (1/2, 0); E_z: (0, 1/2); E_phi: (0, 0)
   e[0] = interp4(fv, 0, rh.i, ck, h0, h1, fz);
   e[2] = interp4(fv, 2, ci, zh.i, n0, n1, zh.u);
   {
-    const float* F = fv.base + fv.plane + (ci - fv.i0) * fv.ld + (ck - fv.k0);
-    const float f00 = F[0], f10 = F[fv.ld];
-    const float f01 = F[1], f11 = F[fv.ld + 1];
+    const float* F = fv.at(1, ci, ck);
+    const int ld = fv.stride();
+    const float f00 = F[0], f10 = F[ld];
+    const float f01 = F[1], f11 = F[ld + 1];
     const float t11 = f11 * n1 * fz;
     e[1] = (f00 * n0 + f10 * n1) * (1.f - fz) + f01 * n0 * fz;
-    if (fixed) e[1] += t11; else e[2] += t11;  // maxwellSolver.hpp:313
+    if (a.fixed) e[1] += t11; else e[2] += t11;  // maxwellSolver.hpp:313
   }
   // H_z: (1/2, 0); H_r: (0, 1/2); H_phi: (1/2, 1/2)
   b[2] = interp4(fv, 5, rh.i, ck, h0, h1, fz);
@@ -291,15 +315,29 @@ __device__ __forceinline__ void g_terms(float t, float* h, float* m) {
 
 // Where the current goes.  comp: 0 J_r, 1 J_phi, 2 J_z.
 //
-// SharedDep: the block's shared-memory window over nodes [i0, i0+wr) x
-// [k0, k0+wz); the caller has checked that every node the particle's
+// SharedDep: the block's shared-memory window over nodes [i0, i0+kJWR) x
+// [k0, k0+kJWZ); the caller has checked that every node the particle's
 // deposit touches lies in it.
 struct SharedDep {
-  float* s;  // 3 planes of wr x wz floats
-  int wr, wz, i0, k0;
+  static constexpr int kPlane = kJWR * kJWZ;
+  float* s;  // 3 planes of kJWR x kJWZ floats
+  int i0, k0;
+  // shared-window address of J_r at node (i, k)
+  __device__ __forceinline__ unsigned addr(int i, int k) const {
+    return (unsigned)__cvta_generic_to_shared(s + (i - i0) * kJWZ + (k - k0));
+  }
+  // a native shared-memory reduction at addr + OFF bytes
+  template <int OFF>
+  __device__ __forceinline__ static void red(unsigned addr, float v) {
+    asm volatile("red.shared.add.f32 [%0+%1], %2;" ::"r"(addr), "n"(OFF), "f"(v) : "memory");
+  }
+  // byte offset of component comp at node (i + di, k + dk) from addr(i, k)
+  template <int COMP, int DI, int DK>
+  __device__ __forceinline__ static void red_at(unsigned addr, float v) {
+    red<4 * (COMP * kPlane + DI * kJWZ + DK)>(addr, v);
+  }
   __device__ __forceinline__ void add(int comp, int i, int k, float v) const {
-    // a native shared-memory reduction (the pointer alone would make it generic)
-    const unsigned p = (unsigned)__cvta_generic_to_shared(s + (comp * wr + (i - i0)) * wz + (k - k0));
+    const unsigned p = (unsigned)__cvta_generic_to_shared(s + comp * kPlane + (i - i0) * kJWZ + (k - k0));
     asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(p), "f"(v) : "memory");
   }
 };
@@ -539,10 +577,22 @@ struct Moved {
 // runaway test (pusher*.cpp, specieP.cpp:482-491, 609-640, beamP.cpp:159-177,
 // SMB.cpp:252-337).  Writes the particle back; returns false if it left the
 // domain (no current) and fills `m` otherwise.
+// One particle's slot contents, loaded ahead of its turn.
+struct Slot {
+  int cell;
+  float fr, fz, vr, vphi, vz, w;
+};
+
+__device__ __forceinline__ Slot load_slot(const SpeciesF32Buffers& b, size_t j) {
+  return Slot{b.cell[j], b.off_r[j], b.off_z[j], b.vr[j], b.vphi[j], b.vz[j], b.w[j]};
+}
+
 __device__ __forceinline__ bool advance_one(const StepArgs& a, const SpeciesF32Buffers& b,
-                                            size_t j, int ci0, int ck0, float fr0, float fz0,
-                                            const float e[3], const float bb[3], Moved* m) {
-  float v[3] = {b.vr[j], b.vphi[j], b.vz[j]};
+                                            size_t j, const Slot& p, const float e[3],
+                                            const float bb[3], Moved* m) {
+  const int ci0 = cell_r_of(p.cell), ck0 = cell_z_of(p.cell);
+  const float fr0 = p.fr, fz0 = p.fz;
+  float v[3] = {p.vr, p.vphi, p.vz};
   if (!push(a, e, bb, v)) return false;
   // mover_cylindrical + back_position_to_rz: x' = sqrt((x+dx)^2 + dy^2),
   // taken as dx + dy^2/(X + x') to keep the displacement's precision.
@@ -593,7 +643,7 @@ __device__ __forceinline__ bool advance_one(const StepArgs& a, const SpeciesF32B
   m->Xo = (float)(ci0 - ci) + fr0;
   m->Yo = (float)(ck0 - ck) + fz0;
   m->dX = dX; m->dY = dY;
-  m->w = b.w[j];
+  m->w = p.w;
   m->vphi = vp2;
   return true;
 }
@@ -610,6 +660,44 @@ __device__ __forceinline__ void deposit(const StepArgs& a, const D& d, const Mov
   }
 }
 
+// The Villasenor-Buneman deposit of the common case: the particle stayed in
+// an interior cell (1 <= i <= nr-2, k <= nz-2) and moved more than MNZL both
+// ways.  It is vb_azimuthal + vb_rz (one segment, vb_simple) with the row
+// reciprocals from the table and every address an offset from one base.
+__device__ __forceinline__ void vb_fast(const StepArgs& a, const SharedFields& sv, const SharedDep& d,
+                                        float q, float vphi, int in, int kn, float Xo, float Yo,
+                                        float dX, float dY) {
+  const float fi = (float)in;
+  const float4 tr = sv.row(in), ti = sv.row_int(in);
+  const unsigned p = d.addr(in, kn);
+  // J_phi from the mid-point (currentVB.cpp:398-498)
+  const float Xm = Xo + 0.5f * dX, Ym = Yo + 0.5f * dY;
+  const float qp = q * a.qp * vphi / (fi + Xm);
+  const float w0 = (1.f - Xm) * (2.f * fi + Xm) * tr.x;
+  const float w1 = Xm * (2.f * fi + 1.f + Xm) * tr.y;
+  SharedDep::red_at<1, 0, 0>(p, qp * w0 * (1.f - Ym));
+  SharedDep::red_at<1, 1, 0>(p, qp * w1 * (1.f - Ym));
+  SharedDep::red_at<1, 0, 1>(p, qp * w0 * Ym);
+  SharedDep::red_at<1, 1, 1>(p, qp * w1 * Ym);
+  // J_z and J_r of the segment (currentVB.cpp:22-173)
+  const float xo = fi + Xo, xn = xo + dX;
+  const float ixo = 1.f / xo, ixn = 1.f / xn;
+  float h, m;
+  g_terms(dX * ixo, &h, &m);
+  const float qz = q * a.qz * dY;
+  const float cc = fi * (fi + 1.f);
+  const float lin = 0.5f * dX * (1.f + cc * ixo * ixo);
+  const float hh = cc * h * ixo;
+  const float A = (1.f - Xo) * (2.f * fi + Xo) * ixo - lin + hh;
+  const float B = Xo * (2.f * fi + 1.f + Xo) * ixo + lin - hh;
+  SharedDep::red_at<2, 0, 0>(p, qz * A * ti.x);
+  SharedDep::red_at<2, 1, 0>(p, qz * B * ti.y);
+  const float qr = q * a.qr * ti.z;
+  const float bb = 1.f - Yo, cx = 0.5f * cc * ixo;
+  SharedDep::red_at<0, 0, 0>(p, qr * (dX * (0.5f * bb - 0.25f * dY) + cx * (dX * bb * ixn + dY * m)));
+  SharedDep::red_at<0, 0, 1>(p, qr * (dX * (0.5f * Yo + 0.25f * dY) + cx * (dX * Yo * ixn - dY * m)));
+}
+
 __device__ __forceinline__ bool cell_in_halo(const StepArgs& a, int cell) {
   const int ci = cell_r_of(cell), ck = cell_z_of(cell);
   if (ci < -1 || ci > a.nr || ck < -1 || ck > a.nz) {  // the gather would leave the halo
@@ -619,8 +707,8 @@ __device__ __forceinline__ bool cell_in_halo(const StepArgs& a, int cell) {
   return true;
 }
 
-__device__ __forceinline__ FieldView global_view(const StepArgs& a) {
-  return FieldView{a.Er, a.plane, a.ld, -2, -2};
+__device__ __forceinline__ GlobalFields global_fields(const StepArgs& a) {
+  return GlobalFields{a.Er, a.plane, a.ld, -2, -2, a.rt};
 }
 
 __device__ __forceinline__ GlobalDep global_dep(const StepArgs& a) {
@@ -634,88 +722,114 @@ __global__ void __launch_bounds__(kThreads) step_flat_kernel(StepArgs a, Species
                                                              size_t j0, size_t j1) {
   const size_t j = j0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (j >= j1) return;
-  const int cell = b.cell[j];
-  if (cell < 0 || !cell_in_halo(a, cell)) return;
-  const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
-  const float fr0 = b.off_r[j], fz0 = b.off_z[j];
+  const Slot p = load_slot(b, j);
+  if (p.cell < 0 || !cell_in_halo(a, p.cell)) return;
   float e[3], bb[3];
-  gather(global_view(a), a.fixed, ci0, fr0, ck0, fz0, e, bb);
+  gather(a, global_fields(a), cell_r_of(p.cell), p.fr, cell_z_of(p.cell), p.fz, e, bb);
   Moved m;
-  if (advance_one(a, b, j, ci0, ck0, fr0, fz0, e, bb, &m)) deposit<CUR>(a, global_dep(a), m);
+  if (advance_one(a, b, j, p, e, bb, &m)) deposit<CUR>(a, global_dep(a), m);
 }
 
-// Shared memory of a tile block: the six field components over the tile
-// plus `halo` + 1 nodes per side, then the three current components over
-// the tile plus `halo` nodes per side.
-__host__ __device__ inline int field_window_r(const TileGrid& tg) { return tg.tr + 2 * tg.halo + 2; }
-__host__ __device__ inline int field_window_z(const TileGrid& tg) { return tg.tz + 2 * tg.halo + 2; }
-__host__ __device__ inline size_t tile_smem_bytes(const TileGrid& tg) {
-  return sizeof(float) * (6 * (size_t)field_window_r(tg) * field_window_z(tg) +
-                          3 * (size_t)(tg.tr + 2 * tg.halo) * (tg.tz + 2 * tg.halo));
-}
-
-// One block per tile: the tile's particles (grouped by the last sort) gather
-// from a shared copy of the fields around the tile and deposit into a shared
-// current window that is added to the global grid once at the end.
-// Particles that drifted beyond the halo use the global grid.
+// One particle of a tile block: gather from the shared window (or the grid
+// when it drifted out), push and move, deposit into the shared current
+// window (or the grid when a node it touches lies outside).
 template <int CUR>
-__global__ void __launch_bounds__(kThreads, 5) step_tiled_kernel(StepArgs a, SpeciesF32Buffers b,
-                                                              TileGrid tg) {
+__device__ __forceinline__ void tile_particle(const StepArgs& a, const SpeciesF32Buffers& b,
+                                              unsigned j, const Slot& p, const SharedFields& sv,
+                                              const SharedDep& sd) {
+  if (p.cell < 0) return;
+  const int ci0 = cell_r_of(p.cell), ck0 = cell_z_of(p.cell);
+  // the gather reads nodes ci-1 .. ci+1, ck-1 .. ck+1
+  const bool inside = ci0 - 1 >= sv.i0 && ci0 + 2 < sv.i0 + kFWR && ck0 - 1 >= sv.k0 &&
+                      ck0 + 2 < sv.k0 + kFWZ;
+  if (!inside && !cell_in_halo(a, p.cell)) return;
+  float ef[3], bf[3];
+  if (inside) gather(a, sv, ci0, p.fr, ck0, p.fz, ef, bf);
+  else gather(a, global_fields(a), ci0, p.fr, ck0, p.fz, ef, bf);
+  Moved m;
+  if (!advance_one(a, b, j, p, ef, bf, &m)) return;
+  // every node a deposit touches lies in [min(old, new) cell, max + 1] per axis
+  const int lo_r = min(m.ci0, m.ci), hi_r = max(m.ci0, m.ci) + 1;
+  const int lo_z = min(m.ck0, m.ck), hi_z = max(m.ck0, m.ck) + 1;
+  if (lo_r >= sd.i0 && hi_r < sd.i0 + kJWR && lo_z >= sd.k0 && hi_z < sd.k0 + kJWZ) {
+    if (CUR == 0 && m.ci == m.ci0 && m.ck == m.ck0 && m.ci >= 1 && m.ci <= a.nr - 2 &&
+        m.ck <= a.nz - 2 && fabsf(m.dX) >= a.mnzl_r && fabsf(m.dY) >= a.mnzl_z)
+      vb_fast(a, sv, sd, m.w, m.vphi, m.ci, m.ck, m.Xo, m.Yo, m.dX, m.dY);
+    else
+      deposit<CUR>(a, sd, m);
+  } else {
+    deposit<CUR>(a, global_dep(a), m);
+  }
+}
+
+// Shared memory of a tile block: the field window, then the current window.
+constexpr size_t kTileSmemBytes = sizeof(float) * (6 * kFWR * kFWZ + 3 * kJWR * kJWZ) + sizeof(float4) * 2 * kFWR;
+static_assert((6 * kFWR * kFWZ + 3 * kJWR * kJWZ) % 4 == 0, "the table rows need 16-byte alignment");
+
+// One block per tile (or gridDim.y blocks sharing a crowded tile): the
+// tile's particles (grouped by the last sort) gather from a shared copy of
+// the fields around the tile and deposit into a shared current window that
+// is added to the global grid once at the end.  Particles that drifted
+// beyond the windows use the global grid.
+template <int CUR>
+__global__ void __launch_bounds__(kThreads, 4) step_tiled_kernel(StepArgs a, SpeciesF32Buffers b,
+                                                                 TileGrid tg) {
   extern __shared__ float smem[];
   const int t = blockIdx.x;
   // blockIdx.y of gridDim.y blocks sharing the tile takes every gridDim.y-th run of blockDim.x
   const unsigned s = b.tile_start[t] + blockIdx.y * blockDim.x, e = b.tile_start[t + 1];
   if (s >= e) return;
   const int tr = t / tg.ntz, tz = t - tr * tg.ntz;
-  const int r0 = tr * tg.tr, z0 = tz * tg.tz;  // first cell of the tile
-  const int fwr = field_window_r(tg), fwz = field_window_z(tg);
-  const int fi0 = r0 - tg.halo - 1, fk0 = z0 - tg.halo - 1;  // field window origin (node)
+  const int r0 = tr * kTileR, z0 = tz * kTileZ;  // first cell of the tile
+  const int fi0 = r0 - kHalo - 1, fk0 = z0 - kHalo - 1;  // field window origin (node)
+  const int ji0 = r0 - kHalo, jk0 = z0 - kHalo;          // current window origin (node)
   float* sF = smem;
-  float* sJ = smem + 6 * fwr * fwz;
-  const int wr = tg.tr + 2 * tg.halo, wz = tg.tz + 2 * tg.halo;
-  const int ji0 = r0 - tg.halo, jk0 = z0 - tg.halo;  // current window origin (node)
-  // load the field window (nodes outside the halo-padded grid read as 0)
-  const int nf = fwr * fwz;
-  for (int q = threadIdx.x; q < 6 * nf; q += blockDim.x) {
-    const int c = q / nf, rem = q - c * nf;
-    const int i = fi0 + rem / fwz, k = fk0 + rem % fwz;
-    float val = 0.f;
-    if (i >= -2 && i < a.nr + 2 && k >= -2 && k < a.nz + 2)
-      val = __ldg(a.Er + c * a.plane + (i + 2) * a.ld + (k + 2));
-    sF[q] = val;
+  float* sJ = smem + 6 * kFWR * kFWZ;
+  // load the field window, one row of one component per warp pass (nodes
+  // outside the halo-padded grid read as 0)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int row = warp; row < 6 * kFWR; row += kThreads / 32) {
+    const int c = row / kFWR, i = fi0 + (row - c * kFWR);
+    const bool row_ok = i >= -2 && i < a.nr + 2;
+    const float* src = a.Er + c * a.plane + (i + 2) * a.ld + 2;
+    for (int q = lane; q < kFWZ; q += 32) {
+      const int k = fk0 + q;
+      sF[row * kFWZ + q] = (row_ok && k >= -2 && k < a.nz + 2) ? __ldg(src + k) : 0.f;
+    }
   }
-  for (int q = threadIdx.x; q < 3 * wr * wz; q += blockDim.x) sJ[q] = 0.f;
-  __syncthreads();
-  const FieldView sv{sF, nf, fwz, fi0, fk0};
-  const SharedDep sd{sJ, wr, wz, ji0, jk0};
-  for (unsigned j = s + threadIdx.x; j < e; j += gridDim.y * blockDim.x) {
-    const int cell = b.cell[j];
-    if (cell < 0) continue;
-    const int ci0 = cell_r_of(cell), ck0 = cell_z_of(cell);
-    // the gather reads nodes ci-1 .. ci+1, ck-1 .. ck+1
-    const bool inside = ci0 - 1 >= fi0 && ci0 + 2 < fi0 + fwr && ck0 - 1 >= fk0 && ck0 + 2 < fk0 + fwz;
-    if (!inside && !cell_in_halo(a, cell)) continue;
-    const float fr0 = b.off_r[j], fz0 = b.off_z[j];
-    float ef[3], bf[3];
-    if (inside) gather(sv, a.fixed, ci0, fr0, ck0, fz0, ef, bf);
-    else gather(global_view(a), a.fixed, ci0, fr0, ck0, fz0, ef, bf);
-    Moved m;
-    if (!advance_one(a, b, j, ci0, ck0, fr0, fz0, ef, bf, &m)) continue;
-    // every node a deposit touches lies in [min(old, new) cell, max + 1] per axis
-    const int lo_r = min(m.ci0, m.ci), hi_r = max(m.ci0, m.ci) + 1;
-    const int lo_z = min(m.ck0, m.ck), hi_z = max(m.ck0, m.ck) + 1;
-    if (lo_r >= ji0 && hi_r < ji0 + wr && lo_z >= jk0 && hi_z < jk0 + wz)
-      deposit<CUR>(a, sd, m);
-    else
-      deposit<CUR>(a, global_dep(a), m);
+  for (int q = threadIdx.x; q < 3 * kJWR * kJWZ; q += kThreads) sJ[q] = 0.f;
+  // the window's rows of the radial reciprocal table (rows -2 .. nr+2 exist)
+  float4* sR = reinterpret_cast<float4*>(sJ + 3 * kJWR * kJWZ);
+  if (threadIdx.x < 2 * kFWR) {
+    const int i = fi0 + (int)(threadIdx.x >> 1);
+    sR[threadIdx.x] = (i >= -2 && i <= a.nr + 2) ? __ldg(a.rt + 2 * (i + 2) + (threadIdx.x & 1))
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < 3 * wr * wz; q += blockDim.x) {
-    const float v = sJ[q];
-    if (v == 0.f) continue;
-    const int comp = q / (wr * wz), rem = q - comp * wr * wz;
-    const int i = ji0 + rem / wz, k = jk0 + rem % wz;
-    atomicAdd(a.Jr + comp * a.plane + (i + 2) * a.ld + (k + 2), v);  // J_r, J_phi, J_z are consecutive planes
+  const SharedFields sv{sF, fi0, fk0, sR};
+  const SharedDep sd{sJ, ji0, jk0};
+  // each thread walks its slots with the next slot's loads in flight
+  const unsigned stride = gridDim.y * blockDim.x;
+  unsigned j = s + threadIdx.x;
+  Slot cur{};
+  if (j < e) cur = load_slot(b, j);
+  while (j < e) {
+    const unsigned jn = j + stride;
+    Slot nxt{};
+    if (jn < e) nxt = load_slot(b, jn);
+    tile_particle<CUR>(a, b, j, cur, sv, sd);
+    cur = nxt;
+    j = jn;
+  }
+  __syncthreads();
+  // add the window to the grid, one row of one component per warp pass
+  for (int row = warp; row < 3 * kJWR; row += kThreads / 32) {
+    const int c = row / kJWR, i = ji0 + (row - c * kJWR);
+    float* dst = a.Jr + c * a.plane + (i + 2) * a.ld + 2;  // J_r, J_phi, J_z are consecutive planes
+    for (int q = lane; q < kJWZ; q += 32) {
+      const float v = sJ[row * kJWZ + q];
+      if (v != 0.f) atomicAdd(dst + jk0 + q, v);
+    }
   }
 }
 
@@ -744,6 +858,7 @@ inline f32::StepArgs f32_step_args(const F32Step& st, double charge, double mass
   // ZigZag: 1/(PI dz dr^2) with the species charge folded in
   a.zz_vol = (float)(charge / (kPi * g.dz * g.dr * g.dr));
   a.pusher = st.pusher; a.current = st.current; a.fixed = st.fixed; a.is_beam = is_beam;
+  a.rt = st.recip;
   a.st = st.status;
   return a;
 }

@@ -20,7 +20,6 @@ namespace pcg {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTileR = 8, kTileZ = 64, kHalo = 3;
 
 inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
@@ -120,7 +119,7 @@ __global__ void export_kernel(GridGeom g, SpeciesF32Buffers b, size_t n, const u
 // then takes 32 particles of 32 neighbouring cells, so its gathers from and
 // deposits to the block's shared windows hit distinct addresses and banks.
 
-static_assert(kTileR * kTileZ <= kTileCells, "tile larger than the layer masks");
+static_assert(kTileCells % 32 == 0, "layer masks hold whole 32-cell words");
 
 // tile of a packed cell and the cell's index inside the tile (z fastest)
 __device__ __forceinline__ int tile_key(int cell, const TileGrid& tg, int* lc) {
@@ -347,8 +346,8 @@ __global__ void kinetic_kernel(SpeciesF32Buffers b, size_t n, double mass, doubl
 
 TileGrid f32_tile_grid(const GridGeom& g) {
   TileGrid t;
-  t.tr = std::min(kTileR, g.nr);
-  t.tz = std::min(kTileZ, g.nz);
+  t.tr = kTileR;  // grids smaller than a tile get one partly empty tile
+  t.tz = kTileZ;
   t.ntr = (g.nr + t.tr - 1) / t.tr;
   t.ntz = (g.nz + t.tz - 1) / t.tz;
   t.ntiles = t.ntr * t.ntz;
@@ -431,7 +430,7 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   const f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
   const TileGrid& tg = st.tiles;
   if (b.sorted_n) {
-    const size_t smem = f32::tile_smem_bytes(tg);
+    const size_t smem = f32::kTileSmemBytes;
     if (st.current == PCG_CURRENT_ZIGZAG)
       f32::step_tiled_kernel<1><<<dim3(tg.ntiles, b.splits), f32::kThreads, smem, s>>>(a, b, tg);
     else
