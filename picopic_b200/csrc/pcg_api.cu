@@ -78,7 +78,7 @@ struct pcg_handle {
   size_t staging_n = 0;
   // kernel timers: event pairs per class, recycled after each query
   TileGrid tiles{};       // float path: tile sort geometry
-  int sort_interval = 16;  // float path: steps between tile sorts
+  int sort_interval = 64;  // float path: most steps between tile sorts
   bool timers = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;

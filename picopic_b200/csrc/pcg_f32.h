@@ -54,6 +54,11 @@ struct SpeciesF32Buffers {
   void* scan_tmp = nullptr;            // the tile-count scan's workspace
   size_t scan_tmp_bytes = 0;
   int splits = 1;                      // blocks per tile in the step (the largest tile's share)
+  // particles of a step that left their tile's shared windows (and took the
+  // slow global path): counted on the device, copied to pinned memory after
+  // every step and read by the host, possibly a step late, to decide a sort
+  unsigned* drift = nullptr;
+  unsigned* drift_host = nullptr;
   size_t cap = 0;
   size_t sorted_n = 0;       // [0, sorted_n) are grouped by tile; later slots were appended
   int steps_since_sort = 1 << 30;
@@ -68,7 +73,7 @@ struct F32Step {
   int pusher, current, fixed;
   DevStatus* status;
   TileGrid tiles;
-  int sort_interval;  // steps between tile sorts
+  int sort_interval;  // most steps between tile sorts
 };
 
 __host__ __device__ __forceinline__ int pack_cell(int ci, int ck) {
@@ -88,8 +93,9 @@ void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsig
 void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_t n,
                        const double* src, cudaStream_t s);
 // One step of a species; returns the new slot count (a tile sort drops dead
-// particles).  Sorts when the species was appended to without a sort or
-// `sort_interval` steps have passed.
+// particles).  Sorts when the species has no tile grouping, when appended
+// particles exceed 1/4 of the slots, when more than 1 % of the particles
+// left their tile's windows in a recent step, or after `sort_interval` steps.
 int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
                      double mass, int is_beam, cudaStream_t s);
 void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s);

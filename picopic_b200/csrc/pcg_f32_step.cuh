@@ -743,11 +743,15 @@ __device__ __forceinline__ void tile_particle(const StepArgs& a, const SpeciesF3
   const bool inside = ci0 - 1 >= sv.i0 && ci0 + 2 < sv.i0 + kFWR && ck0 - 1 >= sv.k0 &&
                       ck0 + 2 < sv.k0 + kFWZ;
   if (!inside && !cell_in_halo(a, p.cell)) return;
+  bool slow = !inside;
   float ef[3], bf[3];
   if (inside) gather(a, sv, ci0, p.fr, ck0, p.fz, ef, bf);
   else gather(a, global_fields(a), ci0, p.fr, ck0, p.fz, ef, bf);
   Moved m;
-  if (!advance_one(a, b, j, p, ef, bf, &m)) return;
+  if (!advance_one(a, b, j, p, ef, bf, &m)) {
+    if (slow) atomicAdd(b.drift, 1u);
+    return;
+  }
   // every node a deposit touches lies in [min(old, new) cell, max + 1] per axis
   const int lo_r = min(m.ci0, m.ci), hi_r = max(m.ci0, m.ci) + 1;
   const int lo_z = min(m.ck0, m.ck), hi_z = max(m.ck0, m.ck) + 1;
@@ -759,7 +763,9 @@ __device__ __forceinline__ void tile_particle(const StepArgs& a, const SpeciesF3
       deposit<CUR>(a, sd, m);
   } else {
     deposit<CUR>(a, global_dep(a), m);
+    slow = true;
   }
+  if (slow) atomicAdd(b.drift, 1u);
 }
 
 // Shared memory of a tile block: the field window, then the current window.

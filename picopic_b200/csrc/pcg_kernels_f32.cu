@@ -379,6 +379,9 @@ int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg) {
   if (cudaMalloc((void**)&b.overflow, nt * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.sort_info, 2 * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMallocHost((void**)&b.host_info, 3 * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMalloc((void**)&b.drift, sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMallocHost((void**)&b.drift_host, sizeof(unsigned)) != cudaSuccess) return -1;
+  *b.drift_host = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, b.scan_tmp_bytes, b.tile_cursor, b.tile_start, (int)(nt + 1));
   if (cudaMalloc(&b.scan_tmp, std::max<size_t>(b.scan_tmp_bytes, 16)) != cudaSuccess) return -1;
   return 0;
@@ -388,9 +391,10 @@ void f32_free_species(SpeciesF32Buffers& b) {
   void* arrs[] = {b.cell, b.off_r, b.off_z, b.vr, b.vphi, b.vz, b.w, b.id,
                   b.cell2, b.off_r2, b.off_z2, b.vr2, b.vphi2, b.vz2, b.w2, b.id2,
                   b.tile_start, b.tile_cursor, b.rank, b.cell_count, b.layer_mask, b.layer_prefix,
-                  b.layer_start, b.overflow, b.sort_info, b.scan_tmp};
+                  b.layer_start, b.overflow, b.sort_info, b.scan_tmp, b.drift};
   for (void* a : arrs) cudaFree(a);
   cudaFreeHost(b.host_info);
+  cudaFreeHost(b.drift_host);
   b = SpeciesF32Buffers();
 }
 
@@ -425,8 +429,13 @@ void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_
 int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
                      double mass, int is_beam, cudaStream_t s) {
   if (*n == 0) return 0;
-  if (b.sorted_n == 0 || b.steps_since_sort >= st.sort_interval)
-    if (tile_sort(st.tiles, b, n, s) != 0) return -1;
+  const size_t drifted = *(volatile unsigned*)b.drift_host;  // a recent step's count (a hint)
+  if (b.sorted_n == 0 || b.steps_since_sort >= st.sort_interval || (*n - b.sorted_n) * 4 > *n ||
+      drifted * 100 > b.sorted_n) {
+    if (tile_sort(st.tiles, b, n, s) != 0) return -1;  // synchronises: no copy of drift is pending
+    *b.drift_host = 0;
+  }
+  cudaMemsetAsync(b.drift, 0, sizeof(unsigned), s);
   const f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
   const TileGrid& tg = st.tiles;
   if (b.sorted_n) {
@@ -443,6 +452,7 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
     else
       f32::step_flat_kernel<0><<<nb, f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
   }
+  cudaMemcpyAsync(b.drift_host, b.drift, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   b.steps_since_sort += 1;
   return 0;
 }
