@@ -69,7 +69,7 @@ def scaled(w, nz=None, ppc=None):
 # ---------------------------------------------------------------------------
 # GPU arm
 
-def make_domain(w, precision, seed=1234, host_beam=False, device=0):
+def make_domain(w, precision, seed=1234, host_beam=False, device=0, beam_capacity=0):
     from picopic_b200 import Domain, Geometry
     g = Geometry(w["nr"], w["nz"], w["nr"] * w["dr"], w["nz"] * w["dz"], dt_courant(w["dr"]))
     d = Domain(g, pusher=w["pusher"], current=w["current"], precision=precision, seed=seed,
@@ -77,7 +77,7 @@ def make_domain(w, precision, seed=1234, host_beam=False, device=0):
     n = w["nr"] * w["nz"] * w["ppc"]
     vb = beam_velocity(w["beam_energy_mev"])
     cells_b = (w["beam_radius"] / w["dr"]) * (6 * w["beam_sigma_z"] / w["dz"])
-    nb = int(w["beam_ppc"] * cells_b * 1.05) + 4096
+    nb = max(int(w["beam_ppc"] * cells_b * 1.05) + 4096, beam_capacity)
     e = d.add(_spec("electrons", -1, 1, 1), capacity=n)
     i = d.add(_spec("ions", 1, 1836, 2), capacity=n)
     if host_beam:
@@ -112,7 +112,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.index), "-lms", "200"],
+                                          "-i", str(self.index), "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -214,7 +214,8 @@ def run_gpu(args):
     d, slots, g, vb = make_domain(w, "f32", seed=1234 + 7919 * rank, device=local)
     d.step(args.warmup)
     d.synchronize()
-    p0 = d.diag().particle_steps
+    diag0 = d.diag()
+    p0 = diag0.particle_steps
     d.kernel_times()
     d.enable_timers(True)
     barrier()
@@ -284,7 +285,7 @@ def run_gpu(args):
             "f64": f64,
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "gpu_launches": int(sum(v[1] for v in kt.values()) * 1 + args.steps * 2),
+            "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
         }
         print(json.dumps(line))
     if dist:
@@ -296,11 +297,13 @@ def run_e2e(w, args, rank, local, barrier, allmax, allsum):
     that step's bunch slice from pinned host memory and reads the device
     status block back (pcg_synchronize)."""
     import torch
-    d, slots, g, vb = make_domain(w, "f32", seed=4321 + 7919 * rank, host_beam=True, device=local)
     K = args.steps
-    rng = np.random.default_rng(99 + rank)
-    dl = vb * g.dt
+    vb = beam_velocity(w["beam_energy_mev"])
+    dl = vb * dt_courant(w["dr"])
     mps = w["beam_ppc"] * (w["beam_radius"] / w["dr"]) * (dl / w["dz"])
+    d, slots, g, vb = make_domain(w, "f32", seed=4321 + 7919 * rank, host_beam=True, device=local,
+                                  beam_capacity=int(mps * (args.warmup + K)) + 4096)
+    rng = np.random.default_rng(99 + rank)
     slab = np.pi * (w["beam_radius"] ** 2 - (0.5 * w["dr"]) ** 2) * dl
     w0 = w["beam_density"] * slab / mps
     steps_total = args.warmup + K
@@ -435,7 +438,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="a reduced grid for quick checks")

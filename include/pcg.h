@@ -150,6 +150,7 @@ typedef struct pcg_diagnostics {
   double field_energy_e;        /* sum over interior nodes of eps0/2 E^2 * cell volume, J */
   double field_energy_h;        /* sum of mu0/2 H^2 * cell volume, J */
   double kinetic_energy;        /* sum of (gamma-1) m c^2 * weight, J */
+  uint64_t kernel_launches;     /* kernels launched by pcg_step and pcg_stage so far */
 } pcg_diagnostics;
 
 int pcg_abi_version(void);

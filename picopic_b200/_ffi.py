@@ -38,7 +38,7 @@ class Diagnostics(ctypes.Structure):
                 ("particles", ctypes.c_uint64), ("removed", ctypes.c_uint64),
                 ("move_errors", ctypes.c_uint64), ("particle_steps", ctypes.c_uint64),
                 ("field_energy_e", ctypes.c_double), ("field_energy_h", ctypes.c_double),
-                ("kinetic_energy", ctypes.c_double)]
+                ("kinetic_energy", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
 
 
 _D = ctypes.c_double

@@ -64,6 +64,8 @@ struct pcg_handle {
   float* f32[12] = {};            // planes of one allocation, f32_plane floats apart
   size_t f32_plane = 0;
   float4* recip32 = nullptr;      // radial reciprocal table of the float step
+  uint64_t dead_dropped = 0;      // dead slots the float tile sorts dropped since the last compaction
+  uint64_t launches = 0;          // kernels launched by steps and stages
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -320,6 +322,7 @@ int stage_inject(pcg_handle* h) {
       f32_launch_inject(h->g, s.f32, s.n, count, b, h->stream);
     }
     s.n += count;
+    h->launches += 1;
   }
   return PCG_OK;
 }
@@ -379,6 +382,7 @@ int compact(pcg_handle* h) {
     cudaFree(flags);
   }
   CUDA_TRY(h, cudaMemsetAsync(&h->d_status->dead_slots, 0, sizeof(unsigned long long), h->stream));
+  h->dead_dropped = 0;
   return PCG_OK;
 }
 
@@ -440,24 +444,30 @@ int fused_step(pcg_handle* h) {
     // E consumes J of the previous step, then clears it for this step's deposit.
     { TimerScope ts(h, PCG_TIMER_FIELD_E); launch_yee_e_f64(yee_args<double>(h, h->f64, h->sig64, 1), h->stream); }
     { TimerScope ts(h, PCG_TIMER_FIELD_H); launch_yee_h_f64(yee_args<double>(h, h->f64, h->sig64, 0), fixed, h->stream); }
+    h->launches += 2;
     FieldsF64 f = fields64(h);
     {
       TimerScope ts(h, PCG_TIMER_PARTICLES);
       if (h->cfg.current == PCG_CURRENT_VB)
         CUDA_TRY(h, cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream));
-      for (size_t t = 0; t < h->sp.size(); ++t)
+      for (size_t t = 0; t < h->sp.size(); ++t) {
         launch_advance_f64(h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
                            h->cfg.current, h->reset, h->d_status, h->stream);
+        h->launches += h->sp[t].n ? 1 : 0;
+      }
     }
     {
       TimerScope ts(h, PCG_TIMER_DEPOSIT);
-      for (size_t t = 0; t < h->sp.size(); ++t)
+      for (size_t t = 0; t < h->sp.size(); ++t) {
         launch_deposit_f64(h->g, f, view64(h, h->sp[t]), (int)t, fixed, h->cfg.current, h->reset,
                            h->d_status, h->stream);
+        h->launches += h->sp[t].n ? 1 : 0;
+      }
     }
   } else {
     { TimerScope ts(h, PCG_TIMER_FIELD_E); f32_launch_yee_e(yee_args<float>(h, h->f32, h->sig32, 1), h->stream); }
     { TimerScope ts(h, PCG_TIMER_FIELD_H); f32_launch_yee_h(yee_args<float>(h, h->f32, h->sig32, 0), fixed, h->stream); }
+    h->launches += 2;
     TimerScope ts(h, PCG_TIMER_PARTICLES);
     F32Step st;
     st.g = h->g;
@@ -472,8 +482,12 @@ int fused_step(pcg_handle* h) {
     st.sort_interval = h->sort_interval;
     for (size_t t = 0; t < h->sp.size(); ++t) {
       Species& s = h->sp[t];
+      const size_t n0 = s.n;
+      const uint64_t k0 = s.f32.launches;
       if (f32_step_species(st, s.f32, &s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream) != 0)
         return fail(h, PCG_ERR_CUDA, "tile sort of species '" + s.name + "' failed");
+      h->dead_dropped += n0 - s.n;  // a sort drops the species' dead slots
+      h->launches += s.f32.launches - k0;
     }
   }
   h->t += h->cfg.dt;
@@ -692,7 +706,7 @@ int pcg_count(pcg_handle* h, int slot, size_t* n) {
   if (!h || !n || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
-  if (h->h_status->dead_slots && (rc = compact(h)) != PCG_OK) return rc;
+  if (h->h_status->dead_slots > h->dead_dropped && (rc = compact(h)) != PCG_OK) return rc;
   *n = h->sp[slot].n;
   return PCG_OK;
 }
@@ -872,7 +886,9 @@ int pcg_diag(pcg_handle* h, pcg_diagnostics* out) {
   out->particle_steps = h->particle_steps;
   uint64_t slots = 0;
   for (Species& s : h->sp) slots += s.n;
-  out->particles = slots - h->h_status->dead_slots;
+  const uint64_t dead = h->h_status->dead_slots;
+  out->particles = slots - (dead > h->dead_dropped ? dead - h->dead_dropped : 0);
+  out->kernel_launches = h->launches;
   double ee = 0, eh = 0, ek = 0;
   if (is_f64(h)) {
     if ((rc = f64_energies(h->g, fields64(h), &ee, &eh, h->stream)) != 0) return fail(h, PCG_ERR_CUDA, "energy reduction");

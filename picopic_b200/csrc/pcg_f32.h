@@ -59,6 +59,7 @@ struct SpeciesF32Buffers {
   // every step and read by the host, possibly a step late, to decide a sort
   unsigned* drift = nullptr;
   unsigned* drift_host = nullptr;
+  uint64_t launches = 0;  // kernels launched for this species (sorts and steps)
   size_t cap = 0;
   size_t sorted_n = 0;       // [0, sorted_n) are grouped by tile; later slots were appended
   int steps_since_sort = 1 << 30;

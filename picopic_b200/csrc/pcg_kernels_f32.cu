@@ -268,6 +268,7 @@ int tile_sort(const TileGrid& tg, SpeciesF32Buffers& b, size_t* n, cudaStream_t 
   size_t tmp = b.scan_tmp_bytes;
   cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp, counts, b.tile_start, (int)(nt + 1), s);
   if (*n) tile_scatter_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b, *n, tg);
+  b.launches += (*n ? 2 : 0) + 1 + 2;  // rank, scatter; layers; the scan's two kernels
   cudaMemcpyAsync(b.host_info, b.tile_start + nt, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(b.host_info + 1, b.sort_info, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
@@ -452,6 +453,7 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
     else
       f32::step_flat_kernel<0><<<nb, f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
   }
+  b.launches += (b.sorted_n ? 1 : 0) + (*n > b.sorted_n ? 1 : 0);
   cudaMemcpyAsync(b.drift_host, b.drift, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   b.steps_since_sort += 1;
   return 0;
