@@ -213,6 +213,21 @@ int pcg_set_beam_profile(pcg_handle* h, int slot, int profile, double sigma_z,
 int pcg_enable_timers(pcg_handle* h, int on);
 int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n);
 
+/* Acceptance diagnostics of the deposit, double precision; no counterpart
+ * in the reference.  pcg_node_charge fills q ((nr+4) x (nz+4), C) with the
+ * particles' node charges in the shape the Villasenor-Buneman deposit
+ * conserves: a particle at x = r/dr in cell i gives node i the radial share
+ * 1/2 + i(i+1)/(2x) - x/2, node i+1 the rest, times linear axial shares.
+ * pcg_divergence fills out with the flux divergence of J (which =
+ * PCG_FIELD_J_R) or E (PCG_FIELD_E_R):
+ *   F_r(i,k) A(i) - F_r(i-1,k) A(i-1) + (F_z(i,k) - F_z(i,k-1)) S(i),
+ * A(i) = 2 pi (i+1/2) dr dz, S(i) = 2 pi i dr^2 (pi dr^2 / 4 on the axis),
+ * the face areas of the reference's Yee update.  Charge continuity over one
+ * step is then Q(n+1) - Q(n) + dt div J = 0, and the Gauss residual is
+ * eps0 div E - Q. */
+int pcg_node_charge(pcg_handle* h, double* q);
+int pcg_divergence(pcg_handle* h, int which, double* out);
+
 /* Villasenor-Buneman current of one species, double precision, that
  * allocates no device memory.  No counterpart in the reference: it exists
  * for callers that may not call cudaMalloc (a host code that owns and

@@ -77,6 +77,8 @@ SIGNATURES = {
                                                   ctypes.c_size_t, _D] + [ctypes.c_void_p] * 9 +
                                    [ctypes.c_int, ctypes.c_void_p,
                                     ctypes.POINTER(ctypes.c_ulonglong)]),
+    "pcg_node_charge": (ctypes.c_int, [_H, _PD]),
+    "pcg_divergence": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
 }
 
 _lib = None

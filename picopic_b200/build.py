@@ -33,6 +33,7 @@ UNITS = {
     "pcg_kernels_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "pcg_init.cu": [],
     "pcg_noalloc.cu": ["--fmad=false"],
+    "pcg_diag.cu": ["--fmad=false"],
 }
 
 

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pcg.h"
+#include "pcg_diag.h"
 #include "pcg_f32.h"
 #include "pcg_init.h"
 #include "pcg_kernels.h"
@@ -66,6 +67,7 @@ struct pcg_handle {
   float4* recip32 = nullptr;      // radial reciprocal table of the float step
   uint64_t dead_dropped = 0;      // dead slots the float tile sorts dropped since the last compaction
   uint64_t launches = 0;          // kernels launched by steps and stages
+  double* diag = nullptr;         // node-value scratch of the diagnostics
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -586,6 +588,7 @@ int pcg_destroy(pcg_handle* h) {
   for (int c = 0; c < 12; ++c) cudaFree(h->f64[c]);
   cudaFree(h->f32[0]);
   cudaFree(h->recip32);
+  cudaFree(h->diag);
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
   cudaFree(h->reset);
   cudaFree(h->scratch);
@@ -769,6 +772,50 @@ int pcg_export_field(pcg_handle* h, int which, double* dst) {
     for (size_t p = 0; p < h->nodes; ++p) dst[p] = tmp[p];
   }
   (void)kFieldNames;
+  return PCG_OK;
+}
+
+namespace {
+// A device array of node values for the diagnostics, allocated on first use.
+int diag_buffer(pcg_handle* h, double** out) {
+  if (!h->diag) {
+    int rc = dalloc(h, &h->diag, h->nodes);
+    if (rc != PCG_OK) return rc;
+  }
+  *out = h->diag;
+  return PCG_OK;
+}
+}  // namespace
+
+int pcg_node_charge(pcg_handle* h, double* q) {
+  if (!h || !q) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  double* d = nullptr;
+  if ((rc = diag_buffer(h, &d)) != PCG_OK) return rc;
+  CUDA_TRY(h, cudaMemsetAsync(d, 0, sizeof(double) * h->nodes, h->stream));
+  for (Species& s : h->sp) {
+    const int e = is_f64(h) ? diag_node_charge_f64(h->g, s.r, s.z, s.w, s.n, s.charge, d, h->stream)
+                            : diag_node_charge_f32(h->g, s.f32, s.n, s.charge, d, h->stream);
+    if (e != 0) return fail(h, PCG_ERR_CUDA, "node charge");
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(q, d, sizeof(double) * h->nodes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return PCG_OK;
+}
+
+int pcg_divergence(pcg_handle* h, int which, double* out) {
+  if (!h || !out || (which != PCG_FIELD_E_R && which != PCG_FIELD_J_R)) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  double* d = nullptr;
+  if ((rc = diag_buffer(h, &d)) != PCG_OK) return rc;
+  const int zc = which + 2;  // the z component of the same field
+  const int e = is_f64(h) ? diag_divergence(h->g, h->f64[which], h->f64[zc], 1, d, h->stream)
+                          : diag_divergence(h->g, h->f32[which], h->f32[zc], 0, d, h->stream);
+  if (e != 0) return fail(h, PCG_ERR_CUDA, "divergence");
+  CUDA_TRY(h, cudaMemcpyAsync(out, d, sizeof(double) * h->nodes, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return PCG_OK;
 }
 

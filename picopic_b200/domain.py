@@ -183,6 +183,31 @@ class Domain:
     def fields(self) -> dict:
         return {n: self.get_field(n) for n in FIELDS}
 
+    # -- acceptance diagnostics of the deposit (no reference counterpart) ------------
+    def node_charge(self) -> np.ndarray:
+        """Node charges (C) in the shape the Villasenor-Buneman deposit conserves."""
+        a = np.zeros(self.grid.shape)
+        self._check(self.lib.pcg_node_charge(self.h, _dp(a)), "pcg_node_charge")
+        return a
+
+    def divergence(self, which: str) -> np.ndarray:
+        """Flux divergence of J ("j") or E ("e") over the Yee face areas (A m^2 or V m)."""
+        a = np.zeros(self.grid.shape)
+        self._check(self.lib.pcg_divergence(self.h, FIELD["j_r" if which == "j" else "e_r"], _dp(a)),
+                    "pcg_divergence")
+        return a
+
+    def continuity_step(self) -> np.ndarray:
+        """Take one step and return the charge continuity residual of every
+        node, Q(n+1) - Q(n) + dt div J, relative to the largest |Q(n+1)|
+        (real nodes only; beam injection and runaway removal add or drop
+        charge without a current and show up here)."""
+        q0 = self.node_charge()
+        self.step(1)
+        q1 = self.node_charge()
+        r = q1 - q0 + self.grid.dt * self.divergence("j")
+        return r[2:-2, 2:-2] / max(np.abs(q1).max(), 1e-300)
+
     # -- the Domain façade (src/domain.cpp:86-204) -----------------------------------
     def stage(self, name) -> int:
         idx = STAGE[name] if isinstance(name, str) else int(name)
