@@ -256,6 +256,8 @@ class OracleSim(_Sim):
                                                ctypes.c_uint32, ctypes.c_int]
             lib.orc_philox_uniform.restype = _D
             lib.orc_philox4x32_10.argtypes = [ctypes.POINTER(ctypes.c_uint32)] * 3
+            lib.orc_collide.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.orc_collide.restype = ctypes.c_long
             self._bind(lib)
             OracleSim._lib = lib
         self.lib = OracleSim._lib
@@ -269,6 +271,10 @@ class OracleSim(_Sim):
 
     def set_rng(self, kind: str, seed: int):
         self.lib.orc_set_rng(self.h, {"mt19937": 0, "philox": 1}[kind], seed)
+
+    def collide(self, shuffle: bool = False) -> int:
+        """One binary-collision pass (Perez 2012); returns the pair calls."""
+        return int(self.lib.orc_collide(self.h, int(shuffle)))
 
     @property
     def errors(self) -> int:
@@ -288,6 +294,8 @@ class RefSim(_Sim):
             lib.ref_create.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _PI, _PD]
             lib.ref_seed.argtypes = [ctypes.c_uint]
             lib.ref_error_count.restype = ctypes.c_long
+            lib.ref_collide.argtypes = [ctypes.c_void_p]
+            lib.ref_collide.restype = ctypes.c_long
             self._bind(lib)
             RefSim._libs[path] = lib
         self.lib = RefSim._libs[path]
@@ -301,6 +309,10 @@ class RefSim(_Sim):
     def seed(self, s: int):
         """Seed the reference's global std::mt19937 (rand.cpp:25)."""
         self.lib.ref_seed(s)
+
+    def collide(self) -> int:
+        """One CollisionsP12 pass without its time-seeded shuffle; returns ncol."""
+        return int(self.lib.ref_collide(self.h))
 
     @property
     def errors(self) -> int:

@@ -62,6 +62,7 @@ struct orc_sim {
   species_t sp[MAX_SPECIES];
   int rng_kind;
   uint64_t seed, step_index;
+  uint32_t coll_pass; /* collision passes so far: the Philox counter of their draws */
   mt19937_t mt;
   long errors, removed;
 };
@@ -1387,4 +1388,421 @@ void orc_destroy(orc_sim* s) {
     free(p->cell_r); free(p->cell_z);
   }
   free(s);
+}
+
+/* ------------------------------------------------------------------ */
+/* Binary Coulomb collisions, Perez et al. 2012 (the reference's default */
+/* scheme): Collisions::operator() (collisions.cpp:230-236) over         */
+/* CollisionsP12::collide (collisionsP12.cpp:330-548) and ::collide_single */
+/* (:29-328).                                                            */
+/*                                                                       */
+/* quirks=reference keeps: the relative speed as the difference of the   */
+/* CM speeds (:139-140; equal masses then give a round-off speed), the    */
+/* deflection test U < w against the macroparticle weight (:255, :268),   */
+/* and `break` out of the cell row on a non-normal temperature or density */
+/* (:351-354).  quirks=fixed uses the sum of the CM speeds, deflects the  */
+/* lighter-weight particle always and the other with probability w_a/w_b, */
+/* and skips only the cell.                                              */
+/*                                                                       */
+/* Random numbers: with ORC_RNG_MT19937 the reference's sequence (U, phi, */
+/* U_defl per collision that passes the early returns) and no shuffle of  */
+/* the cell lists (the reference shuffles with std::srand(time(0)), which */
+/* no run can repeat); with ORC_RNG_PHILOX the GPU's counter scheme:      */
+/* collision m of cell c draws from blocks (c, 2m) and (c, 2m+1), and the */
+/* cell lists are shuffled by Fisher-Yates with draws (c, i); the third  */
+/* counter word is the pass number (one pass per collision call).        */
+
+#define K_PLANK_BAR (6.6261e-34 / (2. * K_PI))
+#define COLL_TAG 0x636f6c6cu
+#define SHUF_TAG 0x73687566u
+
+typedef struct {
+  orc_sim* s;
+  uint32_t cell, m; /* Philox counters of the current collision */
+} coll_rng;
+
+static double coll_draw(coll_rng* g, int q) {
+  orc_sim* s = g->s;
+  if (s->rng_kind != ORC_RNG_PHILOX) return mt_uniform(&s->mt);
+  uint32_t ctr[4] = {g->cell, 2u * g->m + (uint32_t)(q >> 1), s->coll_pass, COLL_TAG};
+  uint32_t key[2] = {(uint32_t)s->seed, (uint32_t)(s->seed >> 32)};
+  uint32_t o[4];
+  orc_philox4x32_10(ctr, key, o);
+  uint32_t a = (q & 1) ? o[2] : o[0], b = (q & 1) ? o[3] : o[1];
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+static double shuffle_draw(orc_sim* s, uint32_t cell, uint32_t i, uint32_t list) {
+  uint32_t ctr[4] = {cell, i, s->coll_pass, SHUF_TAG + list};
+  uint32_t key[2] = {(uint32_t)s->seed, (uint32_t)(s->seed >> 32)};
+  uint32_t o[4];
+  orc_philox4x32_10(ctr, key, o);
+  return ((double)(o[0] >> 5) * 67108864.0 + (double)(o[1] >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+typedef struct {
+  species_t* sp;
+  size_t j;
+} pref; /* a particle: species and index */
+
+static int lorenz_or_flag(orc_sim* s, double v2, double* g) {
+  if (lorenz_factor(v2, g) != ST_OK) { s->errors++; return 0; }
+  return 1;
+}
+
+/* CollisionsP12::collide_single (collisionsP12.cpp:29-328). */
+static void p12_single(orc_sim* s, coll_rng* g, double m_real_a, double m_real_b, double q_real_a,
+                       double q_real_b, pref pa, pref pb, double density_a_in,
+                       double density_b_in, double debye_in) {
+  const int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  double charge_a, mass_a, charge_b, mass_b, w_a, w_b, density_a, density_b;
+  double v_a[3], v_b[3];
+  int swap = 0;
+  double w_ratio = pa.sp->w[pa.j] / pb.sp->w[pb.j];
+  pref A = pa, B = pb;
+  if (w_ratio <= 1) {
+    charge_a = q_real_a; mass_a = m_real_a; density_a = density_a_in;
+    charge_b = q_real_b; mass_b = m_real_b; density_b = density_b_in;
+  } else {
+    A = pb; B = pa;
+    charge_a = q_real_b; mass_a = m_real_b; density_a = density_b_in;
+    charge_b = q_real_a; mass_b = m_real_a; density_b = density_a_in;
+    swap = 1;
+  }
+  v_a[0] = A.sp->vr[A.j]; v_a[1] = A.sp->vphi[A.j]; v_a[2] = A.sp->vz[A.j];
+  v_b[0] = B.sp->vr[B.j]; v_b[1] = B.sp->vphi[B.j]; v_b[2] = B.sp->vz[B.j];
+  w_a = A.sp->w[A.j];
+  w_b = B.sp->w[B.j];
+
+  if (v_a[0] == v_b[0] && v_a[1] == v_b[1] && v_a[2] == v_b[2]) return;
+
+  double gamma_a, gamma_b;
+  if (!lorenz_or_flag(s, len2(v_a), &gamma_a) || !lorenz_or_flag(s, len2(v_b), &gamma_b)) return;
+  const double ga0 = gamma_a, gb0 = gamma_b; /* momentum_0 / momentum recompute the same gamma */
+  const double p0_a = ga0 * mass_a * K_LIGHT_VEL, p0_b = gb0 * mass_b * K_LIGHT_VEL; /* rel.cpp:57-64 */
+  double p_a[3], p_b[3], beta_cm[3];
+  for (int c = 0; c < 3; ++c) { p_a[c] = v_a[c] * ga0; p_a[c] *= mass_a; } /* rel.cpp:66-72 */
+  for (int c = 0; c < 3; ++c) { p_b[c] = v_b[c] * gb0; p_b[c] *= mass_b; }
+  for (int c = 0; c < 3; ++c) beta_cm[c] = p_a[c] + p_b[c];
+  const double p0_sum = p0_a + p0_b;
+  for (int c = 0; c < 3; ++c) beta_cm[c] /= p0_sum;
+
+  double gamma_cm;
+  const double v_cm_2 = len2(beta_cm) * K_LIGHT_VEL_POW_2;
+  if (!lorenz_or_flag(s, v_cm_2, &gamma_cm)) return;
+
+  const double p0_a_cm = gamma_cm * (p0_a - dot3(beta_cm, p_a));
+  const double p0_b_cm = gamma_cm * (p0_b - dot3(beta_cm, p_b));
+
+  double p_a_cm[3], p_b_cm[3], t[3];
+  for (int c = 0; c < 3; ++c) p_a_cm[c] = p_a[c];
+  {
+    const double d = dot3(beta_cm, p_a), l2 = len2(beta_cm);
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2; }
+    for (int c = 0; c < 3; ++c) p_a_cm[c] += t[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0_a; }
+    for (int c = 0; c < 3; ++c) p_a_cm[c] -= t[c];
+  }
+  for (int c = 0; c < 3; ++c) p_b_cm[c] = -p_a_cm[c];
+
+  double v_cm[3];
+  for (int c = 0; c < 3; ++c) v_cm[c] = beta_cm[c] * K_LIGHT_VEL;
+  const double gamma_a_cm = (1 - dot3(v_a, v_cm) / K_LIGHT_VEL_POW_2) * gamma_a * gamma_cm;
+  const double gamma_b_cm = (1 - dot3(v_b, v_cm) / K_LIGHT_VEL_POW_2) * gamma_b * gamma_cm;
+
+  double v_a_cm[3], v_b_cm[3];
+  const double da = mass_a * gamma_a_cm, db = mass_b * gamma_b_cm;
+  for (int c = 0; c < 3; ++c) { v_a_cm[c] = p_a_cm[c] / da; v_b_cm[c] = p_b_cm[c] / db; }
+
+  const double la = sqrt(len2(v_a_cm)), lb = sqrt(len2(v_b_cm));
+  const double v_rel_abs = (fixed ? la + lb : la - lb) / (1 - dot3(v_a_cm, v_b_cm) / K_LIGHT_VEL_POW_2);
+
+  double gamma_rel;
+  if (!lorenz_or_flag(s, v_rel_abs * v_rel_abs, &gamma_rel)) return;
+  const double p_rel_abs = gamma_rel * mass_b * v_rel_abs;
+
+  if (p_rel_abs == 0) return;
+  if (v_rel_abs < K_MNZL) return;
+  if (!isnormal(density_a)) return;
+  if (!isnormal(density_b)) return;
+
+  const int rel = len2(v_a) > K_REL_LIMIT_POW_2 || len2(v_b) > K_REL_LIMIT_POW_2;
+  const double debye = rel ? debye_in * gamma_rel : debye_in;
+
+  /* phys::plasma::coulomb_logarithm (plasma.cpp:42-52) */
+  const double m_red = mass_a * mass_b / (mass_a + mass_b);
+  const double cl = log(debye * m_red * v_rel_abs / K_PLANK_BAR);
+  const double L_coulomb = 2. < cl ? cl : 2.; /* std::max(2., cl) */
+
+  const double density_w = density_a * density_b / (density_a < density_b ? density_a : density_b);
+  const double mass_ab = mass_a * mass_b / (mass_a + mass_b);
+
+  double s12;
+  if (rel) {
+    const double qq = charge_a * charge_b;
+    const double ec = K_EPSILON0 * K_LIGHT_VEL_POW_2;
+    const double f = mass_a * gamma_a_cm * mass_b * gamma_b_cm * K_LIGHT_VEL_POW_2 / len2(p_a_cm) + 1;
+    s12 = density_w * s->dt * L_coulomb * (qq * qq)
+          / (4 * K_PI * (ec * ec) * mass_a * gamma_a * mass_b * gamma_b)
+          * gamma_cm * sqrt(len2(p_a)) / (mass_a * gamma_a + mass_b * gamma_b)
+          * (f * f);
+  } else {
+    const double qq = charge_a * charge_b;
+    const double em = K_EPSILON0 * mass_ab;
+    s12 = density_w * s->dt * L_coulomb * (qq * qq)
+          / (4 * K_PI * (em * em) * pow(v_rel_abs, 3));
+  }
+
+  if (v_rel_abs < 1e6 && density_w > 7e13) { /* low-temperature cap :203-213 */
+    const double na = mass_a * pow(density_a, 2. / 3.), nb = mass_b * pow(density_b, 2. / 3.);
+    const double s12max = pow(4. / 3. * K_PI, 1. / 3.) * density_w * s->dt * (mass_a + mass_b)
+                          / (na > nb ? na : nb) * v_rel_abs;
+    if (s12max < s12) s12 = s12max;
+  }
+
+  const double U = coll_draw(g, 0);
+  double cos_xi_cm;
+  if (s12 < 0.1) {
+    cos_xi_cm = 1 + s12 * log(U);
+  } else if (s12 < 3) {
+    const double A_inv = 0.00569578 + 0.9560202 * s12 - 0.508139 * pow(s12, 2)
+                         + 0.47913906 * pow(s12, 3) - 0.12788975 * pow(s12, 4)
+                         + 0.02389567 * pow(s12, 5);
+    const double A = 1. / A_inv;
+    cos_xi_cm = A_inv * log(exp(-A) + 2. * U * sinh(A));
+  } else if (s12 < 6.) {
+    const double A = 3. * exp(-s12);
+    const double A_inv = 1. / A;
+    cos_xi_cm = A_inv * log(exp(-A) + 2. * U * sinh(A));
+  } else {
+    cos_xi_cm = 2 * U - 1;
+  }
+  const double sin_xi_cm = sqrt(1 - pow(cos_xi_cm, 2));
+
+  const double phi_cm = (2 * K_PI) * coll_draw(g, 1); /* uniform_distribution_angle rand.cpp:45-49 */
+  const double sin_phi_cm = sin(phi_cm), cos_phi_cm = cos(phi_cm);
+
+  double p_a_prime_cm[3];
+  const double p_a_cm_abs = sqrt(len2(p_a_cm));
+  const double p_cm_prp = sqrt(p_a_cm[0] * p_a_cm[0] + p_a_cm[1] * p_a_cm[1]);
+  p_a_prime_cm[0] = p_a_cm[0] * p_a_cm[2] / p_cm_prp * sin_xi_cm * cos_phi_cm
+                    - p_a_cm[1] * p_a_cm_abs / p_cm_prp * sin_xi_cm * sin_phi_cm
+                    + p_a_cm[0] * cos_xi_cm;
+  p_a_prime_cm[1] = p_a_cm[1] * p_a_cm[2] / p_cm_prp * sin_xi_cm * cos_phi_cm
+                    + p_a_cm[0] * p_a_cm_abs / p_cm_prp * sin_xi_cm * sin_phi_cm
+                    + p_a_cm[1] * cos_xi_cm;
+  p_a_prime_cm[2] = -p_cm_prp * sin_xi_cm * cos_phi_cm + p_a_cm[2] * cos_xi_cm;
+
+  const double U_defl = coll_draw(g, 2);
+  /* which of v_a', v_b' are computed (the others stay zero, vector3d()) */
+  const int defl_a = fixed ? 1 : U_defl < w_a;
+  const int defl_b = fixed ? U_defl < w_a / w_b : U_defl < w_b;
+
+  double v_a_prime[3] = {0, 0, 0}, v_b_prime[3] = {0, 0, 0};
+  const double l2b = len2(beta_cm);
+  if (defl_a) {
+    double pp[3];
+    for (int c = 0; c < 3; ++c) pp[c] = p_a_prime_cm[c];
+    const double d = dot3(beta_cm, p_a_prime_cm);
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2b; }
+    for (int c = 0; c < 3; ++c) pp[c] += t[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0_a_cm; }
+    for (int c = 0; c < 3; ++c) pp[c] += t[c];
+    for (int c = 0; c < 3; ++c) v_a_prime[c] = pp[c] / mass_a;
+    const double gi = pow(1.0 + len2(v_a_prime) / K_LIGHT_VEL_POW_2, -0.5); /* rel.cpp:47-55 */
+    for (int c = 0; c < 3; ++c) v_a_prime[c] *= gi;
+  }
+  if (defl_b) {
+    double pbp[3], pp[3];
+    for (int c = 0; c < 3; ++c) pbp[c] = -p_a_prime_cm[c];
+    for (int c = 0; c < 3; ++c) pp[c] = pbp[c];
+    const double d = dot3(beta_cm, pbp);
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2b; }
+    for (int c = 0; c < 3; ++c) pp[c] += t[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0_b_cm; }
+    for (int c = 0; c < 3; ++c) pp[c] += t[c];
+    for (int c = 0; c < 3; ++c) v_b_prime[c] = pp[c] / mass_b;
+    const double gi = pow(1.0 + len2(v_b_prime) / K_LIGHT_VEL_POW_2, -0.5);
+    for (int c = 0; c < 3; ++c) v_b_prime[c] *= gi;
+  }
+  /* write back (:279-310).  A is the lighter-weight particle (pa unless
+   * swapped); the reference tests U < w_a for pa and U < w_b for pb in
+   * both orders, so a swapped pair can receive a zero vector when a
+   * weight is below 1. */
+  const double* to_pa = swap ? v_b_prime : v_a_prime;
+  const double* to_pb = swap ? v_a_prime : v_b_prime;
+  int set_pa, set_pb;
+  if (fixed) {
+    set_pa = swap ? defl_b : defl_a;
+    set_pb = swap ? defl_a : defl_b;
+  } else {
+    set_pa = U_defl < w_a;
+    set_pb = U_defl < w_b;
+  }
+  if (set_pa) { pa.sp->vr[pa.j] = to_pa[0]; pa.sp->vphi[pa.j] = to_pa[1]; pa.sp->vz[pa.j] = to_pa[2]; }
+  if (set_pb) { pb.sp->vr[pb.j] = to_pb[0]; pb.sp->vphi[pb.j] = to_pb[1]; pb.sp->vz[pb.j] = to_pb[2]; }
+}
+
+static int name_is(const char* n, const char* lower, const char* cap) {
+  return strcmp(n, lower) == 0 || strcmp(n, cap) == 0;
+}
+
+/* One collision pass over all cells.  shuffle: Philox Fisher-Yates of the
+ * cell lists (ORC_RNG_PHILOX only).  Returns the number of collide_single
+ * calls, or a negative status. */
+long orc_collide(orc_sim* s, int shuffle) {
+  int el = -1, ion = -1;
+  for (int t = 0; t < s->nsp; ++t) { /* collisions.cpp:28-48: the last match wins */
+    if (name_is(s->sp[t].name, "electrons", "Electrons")) el = t;
+    if (name_is(s->sp[t].name, "ions", "Ions")) ion = t;
+  }
+  if (el < 0 || ion < 0) return ST_ARG;
+  const int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  const size_t ncell = (size_t)s->nr * s->nz;
+  /* sort_to_cells (collisions.cpp:87-108): counting sort, stable in species
+   * then particle order; ions to the ion lists, every other species to the
+   * electron lists */
+  size_t *cnt_e = calloc(ncell + 1, sizeof(size_t)), *cnt_i = calloc(ncell + 1, sizeof(size_t));
+  size_t tot_e = 0, tot_i = 0;
+  for (int t = 0; t < s->nsp; ++t) {
+    species_t* p = &s->sp[t];
+    const int is_ion = name_is(p->name, "ions", "Ions");
+    for (size_t j = 0; j < p->n; ++j) {
+      long long ci = p->cell_r[j], ck = p->cell_z[j];
+      if (ci < 0 || ck < 0 || ci >= s->nr || ck >= s->nz) continue;
+      size_t c = (size_t)ci * s->nz + (size_t)ck;
+      if (is_ion) { cnt_i[c + 1]++; tot_i++; } else { cnt_e[c + 1]++; tot_e++; }
+    }
+  }
+  for (size_t c = 0; c < ncell; ++c) { cnt_e[c + 1] += cnt_e[c]; cnt_i[c + 1] += cnt_i[c]; }
+  pref *le = malloc((tot_e + 1) * sizeof(pref)), *li = malloc((tot_i + 1) * sizeof(pref));
+  size_t *fe = malloc((ncell + 1) * sizeof(size_t)), *fi = malloc((ncell + 1) * sizeof(size_t));
+  memcpy(fe, cnt_e, (ncell + 1) * sizeof(size_t));
+  memcpy(fi, cnt_i, (ncell + 1) * sizeof(size_t));
+  for (int t = 0; t < s->nsp; ++t) {
+    species_t* p = &s->sp[t];
+    const int is_ion = name_is(p->name, "ions", "Ions");
+    for (size_t j = 0; j < p->n; ++j) {
+      long long ci = p->cell_r[j], ck = p->cell_z[j];
+      if (ci < 0 || ck < 0 || ci >= s->nr || ck >= s->nz) continue;
+      size_t c = (size_t)ci * s->nz + (size_t)ck;
+      pref r = {p, j};
+      if (is_ion) li[fi[c]++] = r; else le[fe[c]++] = r;
+    }
+  }
+  free(fe); free(fi);
+  if (shuffle && s->rng_kind == ORC_RNG_PHILOX) {
+    for (size_t c = 0; c < ncell; ++c) {
+      pref* L[2] = {le + cnt_e[c], li + cnt_i[c]};
+      size_t n[2] = {cnt_e[c + 1] - cnt_e[c], cnt_i[c + 1] - cnt_i[c]};
+      for (int l = 0; l < 2; ++l)
+        for (size_t i = 1; i < n[l]; ++i) {
+          size_t j = (size_t)(shuffle_draw(s, (uint32_t)c, (uint32_t)i, (uint32_t)l) * (double)(i + 1));
+          if (j > i) j = i;
+          pref tmp = L[l][i]; L[l][i] = L[l][j]; L[l][j] = tmp;
+        }
+    }
+  }
+  const double m_el = s->sp[el].mass, m_ion = s->sp[ion].mass;
+  const double q_el = s->sp[el].charge, q_ion = s->sp[ion].charge;
+  long calls = 0;
+  for (int i = 0; i < s->nr; ++i) {
+    for (int j = 0; j < s->nz; ++j) {
+      const size_t c = (size_t)i * s->nz + j;
+      pref* E = le + cnt_e[c];
+      pref* I = li + cnt_i[c];
+      const unsigned ne = (unsigned)(cnt_e[c + 1] - cnt_e[c]), ni = (unsigned)(cnt_i[c + 1] - cnt_i[c]);
+      /* collect_weighted_params_tot_grid (collisions.cpp:169-221) */
+      double e_tot_e = 0, amount_e = 0, e_tot_i = 0, amount_i = 0;
+      for (unsigned k = 0; k < ni; ++k) {
+        const species_t* p = I[k].sp; size_t q = I[k].j;
+        double v_sq = p->vr[q] * p->vr[q] + p->vphi[q] * p->vphi[q] + p->vz[q] * p->vz[q];
+        double wm = p->w[q] * m_ion;
+        amount_i += p->w[q];
+        e_tot_i += wm * v_sq / 2;
+      }
+      for (unsigned k = 0; k < ne; ++k) {
+        const species_t* p = E[k].sp; size_t q = E[k].j;
+        double v_sq = p->vr[q] * p->vr[q] + p->vphi[q] * p->vphi[q] + p->vz[q] * p->vz[q];
+        double wm = p->w[q] * m_el;
+        amount_e += p->w[q];
+        e_tot_e += wm * v_sq / 2;
+      }
+      const double vol = K_PI * s->dz * s->dr * s->dr * (2.0 * i + 1); /* CELL_VOLUME(i) */
+      const double T_el = e_tot_e / amount_e * (1. / K_EL_CHARGE);
+      const double T_ion = e_tot_i / amount_i * (1. / K_EL_CHARGE);
+      double n_el = 0, n_ion = 0;
+      for (unsigned k = 0; k < ne; ++k) n_el += E[k].sp->w[E[k].j];
+      for (unsigned k = 0; k < ni; ++k) n_ion += I[k].sp->w[I[k].j];
+      n_el /= vol;
+      n_ion /= vol;
+      if (!isnormal(T_ion) || !isnormal(T_el) || !isnormal(n_ion) || !isnormal(n_el)) {
+        if (fixed) continue;
+        break; /* collisionsP12.cpp:351-354 */
+      }
+      /* phys::plasma::debye_length (plasma.cpp:24-33) */
+      const double debye = 7433.944 / sqrt(n_el / T_el + n_ion / T_ion);
+      coll_rng g = {s, (uint32_t)c, 0};
+#define COLL(MA, MB, QA, QB, PA, PB, NA, NB) \
+      do { p12_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye); g.m++; calls++; } while (0)
+      if (ni % 2 == 0)
+        for (unsigned k = 0; k < ni; k += 2) COLL(m_ion, m_ion, q_ion, q_ion, I[k], I[k + 1], n_ion, n_ion);
+      if (ne % 2 == 0)
+        for (unsigned k = 0; k < ne; k += 2) COLL(m_el, m_el, q_el, q_el, E[k], E[k + 1], n_el, n_el);
+      if (ni % 2 != 0) {
+        if (ni >= 3) {
+          COLL(m_ion, m_ion, q_ion, q_ion, I[0], I[1], n_ion, n_ion);
+          COLL(m_ion, m_ion, q_ion, q_ion, I[1], I[2], n_ion, n_ion);
+          COLL(m_ion, m_ion, q_ion, q_ion, I[2], I[0], n_ion, n_ion);
+        }
+        if (ni >= 5)
+          for (unsigned k = 3; k < ni; k += 2) COLL(m_ion, m_ion, q_ion, q_ion, I[k], I[k + 1], n_ion, n_ion);
+      }
+      if (ne % 2 != 0) {
+        if (ne >= 3) {
+          COLL(m_el, m_el, q_el, q_el, E[0], E[1], n_el, n_el);
+          COLL(m_el, m_el, q_el, q_el, E[1], E[2], n_el, n_el);
+          COLL(m_el, m_el, q_el, q_el, E[2], E[0], n_el, n_el);
+        }
+        if (ne >= 5)
+          for (unsigned k = 3; k < ne; k += 2) COLL(m_el, m_el, q_el, q_el, E[k], E[k + 1], n_el, n_el);
+      }
+      if (ni == ne)
+        for (unsigned k = 0; k < ne; ++k) COLL(m_el, m_ion, q_el, q_ion, E[k], I[k], n_el, n_ion);
+      if (ni > ne && ne > 0 && ni > 0) {
+        const unsigned c_i = (unsigned)floor((float)ni / (float)ne);
+        const double c_r = (double)((float)ni / (float)ne - (float)c_i);
+        const unsigned ions_1st = (unsigned)((double)(c_i + 1) * c_r * ne);
+        const unsigned els_1st = (unsigned)(c_r * ne);
+        const unsigned ions_2nd = (unsigned)((double)c_i * (1 - c_r) * ne);
+        for (unsigned fgi = 0; fgi < ions_1st; ++fgi) {
+          int fge = (int)floor((float)fgi / (float)(c_i + 1));
+          COLL(m_el, m_ion, q_el, q_ion, E[fge], I[fgi], n_el, n_ion);
+        }
+        for (unsigned fgi = 0; fgi < ions_2nd; ++fgi) {
+          int fge = (int)floor((float)fgi / (float)c_i);
+          COLL(m_el, m_ion, q_el, q_ion, E[fge + els_1st], I[fgi + ions_1st], n_el, n_ion);
+        }
+      }
+      if (ni < ne && ne > 0 && ni > 0) {
+        const double c_i = floor((float)ne / (float)ni);
+        const double c_r = (double)((float)ne / (float)ni) - c_i;
+        const unsigned els_1st = (unsigned)((c_i + 1) * c_r * ni);
+        const unsigned ions_1st = (unsigned)(c_r * ni);
+        const unsigned els_2nd = (unsigned)(c_i * (1 - c_r) * ni);
+        for (unsigned fge = 0; fge < els_1st; ++fge) {
+          int fgi = (int)floor((float)fge / (float)(c_i + 1));
+          COLL(m_el, m_ion, q_el, q_ion, E[fge], I[fgi], n_el, n_ion);
+        }
+        for (unsigned fge = 0; fge < els_2nd; ++fge) {
+          int fgi = (int)floor((float)fge / (float)c_i);
+          COLL(m_el, m_ion, q_el, q_ion, E[fge + els_1st], I[fgi + ions_1st], n_el, n_ion);
+        }
+      }
+#undef COLL
+    }
+  }
+  free(cnt_e); free(cnt_i); free(le); free(li);
+  s->coll_pass++;
+  return calls;
 }

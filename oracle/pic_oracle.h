@@ -67,6 +67,12 @@ long orc_removed(orc_sim* s);
 long orc_error_count(orc_sim* s);
 void orc_destroy(orc_sim* s);
 
+/* One pass of the binary Coulomb collisions (Perez 2012 scheme,
+ * collisions.cpp:230-236 + collisionsP12.cpp) on the current velocities,
+ * cells from the last binding.  shuffle: Philox shuffle of the cell lists
+ * (ORC_RNG_PHILOX).  Returns the number of pair calls or a negative status. */
+long orc_collide(orc_sim* s, int shuffle);
+
 /* Building blocks exported for known-answer tests. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 double orc_philox_uniform(uint64_t seed, uint32_t stream, uint64_t step, uint32_t index,

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "domain.hpp"
+#include "collisions/collisionsP12.hpp"
 
 namespace math::random {
 extern std::mt19937 gen;  // rand.cpp:25, a non-static global
@@ -52,6 +53,21 @@ struct RefSim {
   std::vector<SpecieP*> species;
   Domain* domain = nullptr;
   size_t removed = 0;
+};
+
+// CollisionsP12 with its protected steps reachable: the pass without
+// Collisions::random_sort (which reseeds std::rand from time(0) and so can
+// never be repeated) is clear, sort_to_cells, collect, collide
+// (collisions.cpp:230-236 minus the shuffle).
+class P12Pass : public CollisionsP12 {
+ public:
+  P12Pass(Geometry* g, TimeSim* t, std::vector<SpecieP*> sp) : CollisionsP12(g, t, sp) {}
+  void run_unshuffled() {
+    clear();
+    sort_to_cells();
+    collect_weighted_params_tot_grid();
+    collide();
+  }
 };
 
 Domain* domain_of(RefSim* s) {
@@ -243,6 +259,16 @@ int ref_step(void* h, int nsteps) {
       if (rc != 0) return rc;
     }
   return 0;
+}
+
+// One P12 collision pass over the current particles (cells from the last
+// binding), without the time-seeded shuffle; returns the pair count.
+long ref_collide(void* h) {
+  RefSim* s = (RefSim*)h;
+  pcg_ref_log::g_fatal = false;
+  P12Pass c(s->geometry, &s->time, s->species);
+  c.run_unshuffled();
+  return pcg_ref_log::g_fatal ? -10 : (long)c.ncol;
 }
 
 double ref_time(void* h) { return ((RefSim*)h)->time.current; }

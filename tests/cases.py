@@ -54,3 +54,17 @@ def load(sim, grid, species, n, seed, fields=True):
     if fields:
         for name, a in random_fields(grid, seed).items():
             sim.set_field(name, a)
+
+
+def thermal_plasma(grid, n, seed, mass=1.0, temperature_ev=1.0, density=1e20, t_par_ratio=1.0):
+    """Uniform plasma of n macroparticles of equal weight (density in m^-3),
+    Maxwellian at temperature_ev, the z temperature scaled by t_par_ratio:
+    the collisional cases."""
+    rng = np.random.default_rng(seed)
+    r = grid.dr / 2 + rng.random(n) * (grid.radius - grid.dr)
+    z = grid.dz / 2 + rng.random(n) * (grid.longitude - grid.dz)
+    s = np.sqrt(temperature_ev * 1.6e-19 / (mass * 9.1e-31))
+    v = rng.normal(size=(3, n)) * s
+    v[2] *= np.sqrt(t_par_ratio)
+    w = np.full(n, density * np.pi * grid.radius ** 2 * grid.longitude / n)
+    return (r, z, v[0], v[1], v[2], w)

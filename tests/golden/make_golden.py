@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle.harness import FIELDS, RefSim  # noqa: E402
-from tests.cases import ELECTRONS, IONS, beam_spec, load, small_grid  # noqa: E402
+from tests.cases import ELECTRONS, IONS, beam_spec, load, small_grid, thermal_plasma  # noqa: E402
 
 CASES = [
     ("borisrel_vb_beam", "borisrel", "vb", True, True),
@@ -60,5 +60,30 @@ def main():
         print("wrote", name)
 
 
+def collisions_fixture():
+    """One Perez-2012 collision pass of the reference (no shuffle, mt19937)."""
+    grid = small_grid(nr=8, nz=16, pml=False)
+    n = grid.nr * grid.nz * 10
+    sim = RefSim(grid)
+    sim.add(ELECTRONS)
+    sim.add(IONS)
+    sim.set_particles(0, *thermal_plasma(grid, n, 1, 1.0, 1.0, 1e20, t_par_ratio=2.0))
+    sim.set_particles(1, *thermal_plasma(grid, n + 7, 2, 1836.0, 0.5, 1e20))
+    sim.seed(SEED)
+    out = {"grid": np.array([grid.nr, grid.nz, grid.radius, grid.longitude, grid.dt,
+                             grid.t_start, 0, 0, 0, 0, 0.0, 0.0]),
+           "seed": np.array(SEED), "n": np.array(n)}
+    for sid in (0, 1):
+        for k, v in sim.get_particles(sid).items():
+            out[f"in/p{sid}/{k}"] = v
+    out["ncol"] = np.array(sim.collide())
+    for sid in (0, 1):
+        for k, v in sim.get_particles(sid).items():
+            out[f"out/p{sid}/{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "collisions", "p12_pass.npz"), **out)
+    print("wrote collisions/p12_pass")
+
+
 if __name__ == "__main__":
     main()
+    collisions_fixture()

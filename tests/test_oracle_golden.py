@@ -50,3 +50,21 @@ def test_oracle_matches_reference_fixture(path):
 
 def test_golden_fixtures_present():
     assert len(GOLDEN) >= 5
+
+
+def test_oracle_collisions_match_reference_fixture():
+    """tests/golden/collisions/p12_pass.npz: one Perez-2012 pass of the
+    reference (no shuffle, mt19937 seeded) reproduced bit for bit."""
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "collisions", "p12_pass.npz"))
+    grid = _grid(d["grid"])
+    o = OracleSim(grid, quirks="reference")
+    o.add(ELECTRONS)
+    o.add(IONS)
+    for sid in (0, 1):
+        o.set_particles(sid, *[d[f"in/p{sid}/{k}"] for k in ("r", "z", "vr", "vphi", "vz", "w")])
+    o.set_rng("mt19937", int(d["seed"]))
+    assert o.collide() > 0
+    for sid in (0, 1):
+        p = o.get_particles(sid)
+        for k in ("vr", "vphi", "vz"):
+            np.testing.assert_array_equal(p[k], d[f"out/p{sid}/{k}"], err_msg=f"species {sid} {k}")

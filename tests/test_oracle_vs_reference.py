@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle.harness import FIELDS, STAGES, OracleSim, RefSim, reference_available
-from tests.cases import ELECTRONS, IONS, beam_spec, load, small_grid
+from tests.cases import ELECTRONS, IONS, beam_spec, load, small_grid, thermal_plasma
 
 COMBOS = [(p, c) for p in ("borisrel", "boris", "vay", "hc") for c in ("vb", "zigzag")]
 
@@ -69,3 +69,27 @@ def test_long_run_removal_and_reflection():
     load(r, grid, species, 3000, seed=5)
     assert o.step(20) == r.step(20) == 0
     _assert_same(o, r, 2, "after 20 steps")
+
+
+@pytest.mark.parametrize("ppc", [3, 10])
+def test_p12_collisions_bit_exact(ppc):
+    """One Perez-2012 collision pass (cells from the binding, no shuffle,
+    the reference's mt19937 draws): velocities bit-identical."""
+    if not reference_available():
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    grid = small_grid(nr=8, nz=16, pml=False)
+    n = grid.nr * grid.nz * ppc
+    o, r = OracleSim(grid, quirks="reference"), RefSim(grid)
+    for sim in (o, r):
+        sim.add(ELECTRONS)
+        sim.add(IONS)
+        sim.set_particles(0, *thermal_plasma(grid, n, 1, 1.0, 1.0, 1e20, t_par_ratio=2.0))
+        sim.set_particles(1, *thermal_plasma(grid, n + 7, 2, 1836.0, 0.5, 1e20))
+    o.set_rng("mt19937", 123)
+    r.seed(123)
+    assert o.collide() > 0
+    assert r.collide() > 0
+    for sid in (0, 1):
+        po, pr = o.get_particles(sid), r.get_particles(sid)
+        for k in ("vr", "vphi", "vz"):
+            np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
