@@ -228,6 +228,23 @@ int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n);
 int pcg_node_charge(pcg_handle* h, double* q);
 int pcg_divergence(pcg_handle* h, int which, double* out);
 
+/* One pass of binary Coulomb collisions, the Perez et al. 2012 scheme of
+ * CollisionsP12::operator() (collisions.cpp:230-236, collisionsP12.cpp:29-569),
+ * in double precision on the current velocities, with the cells of the last
+ * binding: the reference calls it between the push and the move
+ * (SMB.cpp:1289-1293, Domain::collide domain.cpp:199-204).  Electron lists
+ * take every species except those named "ions"/"Ions"; masses and charges
+ * come from the species named "electrons"/"Electrons" and "ions"/"Ions".
+ * Cell lists are shuffled and collisions draw from Philox keyed by the
+ * handle seed and a pass counter (the reference shuffles with
+ * std::srand(time(0)) and draws from its global mt19937).
+ * PCG_QUIRKS_REFERENCE keeps the reference's relative speed (difference of
+ * the centre-of-mass speeds), its deflection test against the macroparticle
+ * weight and its `break` out of a cell row at a non-normal temperature or
+ * density; PCG_QUIRKS_FIXED corrects them.  *pair_calls (may be NULL)
+ * receives the number of pair collisions attempted. */
+int pcg_collide(pcg_handle* h, unsigned long long* pair_calls);
+
 /* Villasenor-Buneman current of one species, double precision, that
  * allocates no device memory.  No counterpart in the reference: it exists
  * for callers that may not call cudaMalloc (a host code that owns and

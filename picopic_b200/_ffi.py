@@ -79,6 +79,7 @@ SIGNATURES = {
                                     ctypes.POINTER(ctypes.c_ulonglong)]),
     "pcg_node_charge": (ctypes.c_int, [_H, _PD]),
     "pcg_divergence": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
+    "pcg_collide": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 _lib = None

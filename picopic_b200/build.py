@@ -34,6 +34,7 @@ UNITS = {
     "pcg_init.cu": [],
     "pcg_noalloc.cu": ["--fmad=false"],
     "pcg_diag.cu": ["--fmad=false"],
+    "pcg_collide.cu": ["--fmad=false"],
 }
 
 

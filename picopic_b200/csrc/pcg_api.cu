@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pcg.h"
+#include "pcg_collide.h"
 #include "pcg_diag.h"
 #include "pcg_f32.h"
 #include "pcg_init.h"
@@ -68,6 +69,8 @@ struct pcg_handle {
   uint64_t dead_dropped = 0;      // dead slots the float tile sorts dropped since the last compaction
   uint64_t launches = 0;          // kernels launched by steps and stages
   double* diag = nullptr;         // node-value scratch of the diagnostics
+  CollWork coll;                  // scratch of the collision passes
+  uint32_t coll_pass = 0;         // collision passes so far (their Philox counter)
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -589,6 +592,7 @@ int pcg_destroy(pcg_handle* h) {
   cudaFree(h->f32[0]);
   cudaFree(h->recip32);
   cudaFree(h->diag);
+  collide_free(h->coll);
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
   cudaFree(h->reset);
   cudaFree(h->scratch);
@@ -817,6 +821,45 @@ int pcg_divergence(pcg_handle* h, int which, double* out) {
   CUDA_TRY(h, cudaMemcpyAsync(out, d, sizeof(double) * h->nodes, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return PCG_OK;
+}
+
+int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
+  if (!h) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
+  CollParams p{};
+  int el = -1, ion = -1;
+  std::vector<CollSpecies> v(h->sp.size());
+  for (size_t t = 0; t < h->sp.size(); ++t) {  // collisions.cpp:28-48: the last match wins
+    Species& s = h->sp[t];
+    if (s.name == "electrons" || s.name == "Electrons") el = (int)t;
+    if (s.name == "ions" || s.name == "Ions") ion = (int)t;
+    CollSpecies& c = v[t];
+    c.n = s.n;
+    c.is_ion = s.name == "ions" || s.name == "Ions";
+    if (is_f64(h)) {
+      c.r = s.r; c.z = s.z; c.vr64 = s.vr; c.vphi64 = s.vphi; c.vz64 = s.vz; c.w64 = s.w;
+    } else {
+      c.cell = s.f32.cell; c.id = s.f32.id;
+      c.vr32 = s.f32.vr; c.vphi32 = s.f32.vphi; c.vz32 = s.f32.vz; c.w32 = s.f32.w;
+    }
+  }
+  if (el < 0 || ion < 0) return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  p.m_el = h->sp[el].mass; p.q_el = h->sp[el].charge;
+  p.m_ion = h->sp[ion].mass; p.q_ion = h->sp[ion].charge;
+  p.dt = h->cfg.dt;
+  p.fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
+  p.shuffle = 1;
+  p.seed = h->cfg.seed;
+  p.pass = h->coll_pass++;
+  p.status = h->d_status;
+  unsigned long long calls = 0;
+  if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
+    return fail(h, PCG_ERR_CUDA, "collision pass");
+  h->launches += 8;
+  if (pair_calls) *pair_calls = calls;
+  return check_status(h);
 }
 
 int pcg_stage(pcg_handle* h, int stage) {

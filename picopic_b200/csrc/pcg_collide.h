@@ -1,0 +1,62 @@
+// pcg_collide.h — binary Coulomb collisions (Perez et al. 2012, the
+// reference's default scheme) on the GPU, in double precision for either
+// particle layout.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "pcg_common.cuh"
+
+namespace pcg {
+
+constexpr int kCollMaxSpecies = 8;
+
+// One species as the collision pass sees it.  Exactly one of the two
+// layouts is set: double (r, z: cells from floor(r/dr), floor(z/dz); ids are
+// slot indices) or float (packed cell, insertion ids).
+struct CollSpecies {
+  size_t n = 0;
+  int is_ion = 0;  // ion lists take "ions"/"Ions", electron lists every other species
+  const double* r = nullptr;
+  const double* z = nullptr;
+  double *vr64 = nullptr, *vphi64 = nullptr, *vz64 = nullptr;
+  const double* w64 = nullptr;
+  const int* cell = nullptr;
+  const unsigned* id = nullptr;
+  float *vr32 = nullptr, *vphi32 = nullptr, *vz32 = nullptr;
+  const float* w32 = nullptr;
+};
+
+struct CollParams {
+  double m_el, q_el, m_ion, q_ion;  // SI, of the species named electrons / ions
+  double dt;
+  int fixed;         // PCG_QUIRKS_FIXED
+  int shuffle;       // Fisher-Yates of the cell lists with Philox draws
+  uint64_t seed;
+  uint32_t pass;     // counter of collision passes: the Philox stream of this one
+  DevStatus* status; // superluminal pairs raise the error word (rel.cpp:33-34 is fatal)
+};
+
+// Scratch of a collision pass, grown on demand and kept by the handle.
+struct CollWork {
+  size_t cap = 0;  // entries per list
+  unsigned long long *keys[2] = {}, *keys2[2] = {}, *vals[2] = {}, *vals2[2] = {};
+  unsigned *count[2] = {}, *start[2] = {};  // per cell
+  double* moments = nullptr;                // per cell: T_el, T_ion, n_el, n_ion
+  int* row_stop = nullptr;                  // per row: first cell that stops the row
+  unsigned long long* calls = nullptr;      // device counter of pair calls
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+  size_t cells = 0;
+};
+
+// One collision pass over all cells; returns 0 or -1 (allocation/launch).
+// *pair_calls receives the number of collide_single calls.
+int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollParams& p,
+                CollWork& w, unsigned long long* pair_calls, cudaStream_t s);
+void collide_free(CollWork& w);
+
+}  // namespace pcg

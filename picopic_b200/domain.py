@@ -183,6 +183,13 @@ class Domain:
     def fields(self) -> dict:
         return {n: self.get_field(n) for n in FIELDS}
 
+    def collide(self) -> int:
+        """One binary-collision pass (Perez 2012, CollisionsP12::operator());
+        returns the number of pair collisions attempted."""
+        n = ctypes.c_ulonglong(0)
+        self._check(self.lib.pcg_collide(self.h, ctypes.byref(n)), "pcg_collide")
+        return int(n.value)
+
     # -- acceptance diagnostics of the deposit (no reference counterpart) ------------
     def node_charge(self) -> np.ndarray:
         """Node charges (C) in the shape the Villasenor-Buneman deposit conserves."""

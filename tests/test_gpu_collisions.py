@@ -1,0 +1,112 @@
+"""Binary Coulomb collisions (Perez 2012) on the GPU against the oracle.
+
+Both run the same pairing sequence per cell with the same Philox draws
+(shuffled cell lists, collision m of cell c drawing from blocks (c, 2m) and
+(c, 2m+1) of the pass), so velocities agree to the ulp-level differences of
+CUDA's and glibc's log/exp/pow/sin/cos: RTOL_F64 = 1e-11 of the largest
+speed.  The float layout collides in double and stores float:
+RTOL_F32 = 3e-7.  The fixed operator conserves momentum and energy of equal-
+weight pairs to rounding (RTOL_CONS_PASS = 2e-11 per pass).
+"""
+import numpy as np
+import pytest
+
+from oracle.harness import OracleSim
+from tests.cases import ELECTRONS, IONS, small_grid, thermal_plasma
+
+pytestmark = pytest.mark.gpu
+
+RTOL_F64 = 1e-11
+RTOL_F32 = 3e-7
+RTOL_CONS_PASS = 2e-11
+ME = 9.1e-31
+
+
+def _pair(precision, quirks, ppc=20, passes=1, extra_ions=13):
+    from picopic_b200 import Domain
+    grid = small_grid(nr=8, nz=16, pml=False)
+    n = grid.nr * grid.nz * ppc
+    inputs = [thermal_plasma(grid, n, 1, 1.0, 1.0, 1e20, t_par_ratio=2.0),
+              thermal_plasma(grid, n + extra_ions, 2, 1836.0, 0.5, 1e20)]
+    gpu = Domain(grid, precision=precision, quirks=quirks, seed=77)
+    orc = OracleSim(grid, quirks=quirks)
+    for sim in (gpu, orc):
+        sim.add(ELECTRONS)
+        sim.add(IONS)
+    for sid, p in enumerate(inputs):
+        gpu.set_particles(sid, *p)
+        if precision == "f32":  # the oracle starts from the stored floats
+            p = tuple(np.asarray(a, dtype=np.float32).astype(np.float64) if k >= 2 else a
+                      for k, a in enumerate(p))
+        orc.set_particles(sid, *p)
+    orc.set_rng("philox", 77)
+    calls = []
+    for _ in range(passes):
+        calls.append((gpu.collide(), orc.collide(shuffle=True)))
+    return gpu, orc, calls
+
+
+@pytest.mark.parametrize("quirks", ["reference", "fixed"])
+def test_p12_f64_matches_oracle(quirks):
+    gpu, orc, calls = _pair("f64", quirks, passes=2)
+    for g, o in calls:
+        assert g == o > 0
+    for sid in (0, 1):
+        pg, po = gpu.get_particles(sid), orc.get_particles(sid)
+        scale = max(np.abs(po[k]).max() for k in ("vr", "vphi", "vz"))
+        for k in ("vr", "vphi", "vz"):
+            assert np.abs(pg[k] - po[k]).max() <= RTOL_F64 * scale, (sid, k)
+
+
+def test_p12_f32_matches_oracle():
+    gpu, orc, calls = _pair("f32", "fixed")
+    assert calls[0][0] == calls[0][1] > 0
+    for sid in (0, 1):
+        pg, po = gpu.get_particles(sid), orc.get_particles(sid)
+        scale = max(np.abs(po[k]).max() for k in ("vr", "vphi", "vz"))
+        for k in ("vr", "vphi", "vz"):
+            assert np.abs(pg[k] - po[k]).max() <= RTOL_F32 * scale, (sid, k)
+
+
+def test_p12_fixed_conserves_momentum_and_energy():
+    """Equal weights everywhere (no rejection): every pair conserves the
+    relativistic momentum gamma m v and kinetic energy (gamma - 1) m c^2;
+    the sums drift only by rounding of the centre-of-mass transforms
+    (RTOL_CONS_PASS = 2e-11 of the momentum scale per pass, measured
+    ~1.3e-11)."""
+    gpu, _, _ = _pair("f64", "fixed", ppc=30, extra_ions=0)
+    c2 = 9e16
+
+    def totals():
+        out = np.zeros(4)
+        for sid, m in ((0, ME), (1, 1836 * ME)):
+            p = gpu.get_particles(sid)
+            v2 = p["vr"] ** 2 + p["vphi"] ** 2 + p["vz"] ** 2
+            g = 1 / np.sqrt(1 - v2 / c2)
+            mw = m * p["w"]
+            out += [np.sum(mw * g * p["vr"]), np.sum(mw * g * p["vphi"]), np.sum(mw * g * p["vz"]),
+                    np.sum(mw * v2 * g * g / (g + 1))]
+        return out
+
+    t0 = totals()
+    for _ in range(3):
+        gpu.collide()
+    t1 = totals()
+    p0 = gpu.get_particles(0)
+    pscale = np.sum(ME * p0["w"] * np.sqrt(p0["vr"] ** 2 + p0["vphi"] ** 2 + p0["vz"] ** 2))
+    assert np.abs(t1[:3] - t0[:3]).max() <= 3 * RTOL_CONS_PASS * pscale
+    assert abs(t1[3] - t0[3]) <= 3 * RTOL_CONS_PASS * t0[3]
+
+
+def test_p12_relaxes_anisotropy():
+    """Electrons with T_par = 2 T_perp isotropise: T_par/T_perp falls."""
+    gpu, _, _ = _pair("f64", "fixed", ppc=50)
+
+    def ratio():
+        p = gpu.get_particles(0)
+        return np.mean(p["vz"] ** 2) / np.mean(0.5 * (p["vr"] ** 2 + p["vphi"] ** 2))
+
+    r0 = ratio()
+    for _ in range(40):
+        gpu.collide()
+    assert ratio() < r0 - 0.01
