@@ -245,6 +245,30 @@ int pcg_divergence(pcg_handle* h, int which, double* out);
  * receives the number of pair collisions attempted. */
 int pcg_collide(pcg_handle* h, unsigned long long* pair_calls);
 
+/* The per-cell collision MLP of the learned collision step (no counterpart
+ * in the reference): 13 inputs -> 128 -> 128 -> 6 outputs, ReLU, BF16
+ * operands on the tensor cores with FP32 accumulation.  Parameters are FP32,
+ * row-major [in][out] per layer in the order W1, b1, W2, b2, W3, b3.
+ * pcg_mlp_create draws He-uniform weights from Philox(seed) on `device`;
+ * pcg_mlp_forward runs rows x 13 host inputs to rows x 6 host outputs;
+ * pcg_mlp_gradient returns the full-batch gradient (and value) of the loss
+ * mean((y - t)^2) over rows and outputs; pcg_mlp_set_data makes a training
+ * set resident and pcg_mlp_train takes Adam steps (beta 0.9, 0.999, eps
+ * 1e-8) on minibatches of `batch` rows drawn with Philox. */
+typedef struct pcg_mlp pcg_mlp;
+#define PCG_MLP_INPUTS 13
+#define PCG_MLP_HIDDEN 128
+#define PCG_MLP_OUTPUTS 6
+#define PCG_MLP_PARAMS 19078
+int pcg_mlp_create(int device, uint64_t seed, pcg_mlp** out);
+int pcg_mlp_destroy(pcg_mlp* m);
+int pcg_mlp_get_params(pcg_mlp* m, float* params);
+int pcg_mlp_set_params(pcg_mlp* m, const float* params);
+int pcg_mlp_forward(pcg_mlp* m, const float* x, size_t rows, float* y);
+int pcg_mlp_gradient(pcg_mlp* m, const float* x, const float* t, size_t rows, float* grad, float* loss);
+int pcg_mlp_set_data(pcg_mlp* m, const float* x, const float* t, size_t rows);
+int pcg_mlp_train(pcg_mlp* m, int steps, int batch, float lr, float* last_loss);
+
 /* Villasenor-Buneman current of one species, double precision, that
  * allocates no device memory.  No counterpart in the reference: it exists
  * for callers that may not call cudaMalloc (a host code that owns and

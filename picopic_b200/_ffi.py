@@ -43,6 +43,7 @@ class Diagnostics(ctypes.Structure):
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
+_PF = ctypes.POINTER(ctypes.c_float)
 _PI32 = ctypes.POINTER(ctypes.c_int32)
 _H = ctypes.c_void_p
 
@@ -80,6 +81,14 @@ SIGNATURES = {
     "pcg_node_charge": (ctypes.c_int, [_H, _PD]),
     "pcg_divergence": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
     "pcg_collide": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_ulonglong)]),
+    "pcg_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    "pcg_mlp_destroy": (ctypes.c_int, [_H]),
+    "pcg_mlp_get_params": (ctypes.c_int, [_H, _PF]),
+    "pcg_mlp_set_params": (ctypes.c_int, [_H, _PF]),
+    "pcg_mlp_forward": (ctypes.c_int, [_H, _PF, ctypes.c_size_t, _PF]),
+    "pcg_mlp_gradient": (ctypes.c_int, [_H, _PF, _PF, ctypes.c_size_t, _PF, _PF]),
+    "pcg_mlp_set_data": (ctypes.c_int, [_H, _PF, _PF, ctypes.c_size_t]),
+    "pcg_mlp_train": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_float, _PF]),
 }
 
 _lib = None
