@@ -269,6 +269,39 @@ int pcg_mlp_gradient(pcg_mlp* m, const float* x, const float* t, size_t rows, fl
 int pcg_mlp_set_data(pcg_mlp* m, const float* x, const float* t, size_t rows);
 int pcg_mlp_train(pcg_mlp* m, int steps, int batch, float lr, float* last_loss);
 
+/* The learned collision step (no counterpart in the reference).  Per cell,
+ * the moment sums of the electron list (every species not named ions) and
+ * the ion list give 13 features; the collision MLP (pcg_mlp_*) maps them to
+ * the change of the six axis temperatures over one step, and every particle
+ * of the cell moves to v' = u + (v - u) sqrt(T'/T) per axis in FP64, so each
+ * species keeps its momentum, the cell its thermal energy, and the new
+ * second moments hold exactly.  Cells whose features leave the model's
+ * training box (widened by 25 % of each feature's span) take the binary
+ * operator (pcg_collide) instead.
+ * pcg_set_collision_model loads PCG_MLP_PARAMS parameters and
+ * PCG_LEARNED_NORM floats: feature mean[13], std[13], target mean[6],
+ * std[6], feature low[13], high[13].  pcg_collide_learned reports the cells
+ * that took the learned and the binary path (either pointer may be NULL).
+ * pcg_cell_moments fills nr*nz x 16 doubles (per cell, electron list then
+ * ion list: N, sum w, sum w v_r, v_phi, v_z, sum w v_r^2, v_phi^2, v_z^2);
+ * pcg_cell_features fills nr*nz x 13 raw features (NaN where a cell has
+ * fewer than two particles in a list) and the per-cell collision scale
+ * S = s_ee + s_ei + s_ii that the targets are measured in. */
+#define PCG_LEARNED_NORM 64
+/* One binary collision pass (as pcg_collide) that also returns, per cell,
+ * the sum over its collisions of each collision's mean change over its
+ * scattering-angle draw given the velocities that collision meets
+ * (non-relativistic kinematics of the mean): an unbiased estimate of the
+ * pass's expected moment change with far less Monte Carlo noise than the
+ * change itself.  nr*nz x 12 doubles: the change of sum w v (3) and sum w
+ * v^2 (3) of the electron list, then of the ion list.  The training
+ * targets of the collision MLP. */
+int pcg_collide_expectation(pcg_handle* h, double* out);
+int pcg_set_collision_model(pcg_handle* h, const float* params, const float* norm);
+int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells);
+int pcg_cell_moments(pcg_handle* h, double* moments);
+int pcg_cell_features(pcg_handle* h, float* features, double* scale);
+
 /* Villasenor-Buneman current of one species, double precision, that
  * allocates no device memory.  No counterpart in the reference: it exists
  * for callers that may not call cudaMalloc (a host code that owns and

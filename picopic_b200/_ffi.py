@@ -81,6 +81,12 @@ SIGNATURES = {
     "pcg_node_charge": (ctypes.c_int, [_H, _PD]),
     "pcg_divergence": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
     "pcg_collide": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_ulonglong)]),
+    "pcg_set_collision_model": (ctypes.c_int, [_H, _PF, _PF]),
+    "pcg_collide_learned": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_ulonglong),
+                                           ctypes.POINTER(ctypes.c_ulonglong)]),
+    "pcg_cell_moments": (ctypes.c_int, [_H, _PD]),
+    "pcg_collide_expectation": (ctypes.c_int, [_H, _PD]),
+    "pcg_cell_features": (ctypes.c_int, [_H, _PF, _PD]),
     "pcg_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     "pcg_mlp_destroy": (ctypes.c_int, [_H]),
     "pcg_mlp_get_params": (ctypes.c_int, [_H, _PF]),

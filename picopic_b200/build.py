@@ -36,6 +36,7 @@ UNITS = {
     "pcg_diag.cu": ["--fmad=false"],
     "pcg_collide.cu": ["--fmad=false"],
     "pcg_mlp.cu": [],
+    "pcg_learned.cu": ["--fmad=false"],
 }
 
 

@@ -19,6 +19,7 @@
 #include "pcg_diag.h"
 #include "pcg_f32.h"
 #include "pcg_init.h"
+#include "pcg_learned.h"
 #include "pcg_kernels.h"
 #include "pcg_yee.cuh"
 
@@ -70,6 +71,7 @@ struct pcg_handle {
   uint64_t launches = 0;          // kernels launched by steps and stages
   double* diag = nullptr;         // node-value scratch of the diagnostics
   CollWork coll;                  // scratch of the collision passes
+  LearnedWork learned;            // the learned collision step: model and scratch
   uint32_t coll_pass = 0;         // collision passes so far (their Philox counter)
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
@@ -593,6 +595,7 @@ int pcg_destroy(pcg_handle* h) {
   cudaFree(h->recip32);
   cudaFree(h->diag);
   collide_free(h->coll);
+  learned_free(h->learned);
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
   cudaFree(h->reset);
   cudaFree(h->scratch);
@@ -823,15 +826,14 @@ int pcg_divergence(pcg_handle* h, int which, double* out) {
   return PCG_OK;
 }
 
-int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
-  if (!h) return PCG_ERR_ARG;
-  int rc = check_status(h);
-  if (rc != PCG_OK) return rc;
-  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
-  CollParams p{};
+namespace {
+// The species as the collision passes see them, and the masses and charges
+// of the species named electrons and ions (collisions.cpp:28-48: the last
+// match wins).  False when either is missing.
+bool collision_species(pcg_handle* h, std::vector<CollSpecies>& v, CollParams& p) {
   int el = -1, ion = -1;
-  std::vector<CollSpecies> v(h->sp.size());
-  for (size_t t = 0; t < h->sp.size(); ++t) {  // collisions.cpp:28-48: the last match wins
+  v.assign(h->sp.size(), CollSpecies());
+  for (size_t t = 0; t < h->sp.size(); ++t) {
     Species& s = h->sp[t];
     if (s.name == "electrons" || s.name == "Electrons") el = (int)t;
     if (s.name == "ions" || s.name == "Ions") ion = (int)t;
@@ -845,21 +847,139 @@ int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
       c.vr32 = s.f32.vr; c.vphi32 = s.f32.vphi; c.vz32 = s.f32.vz; c.w32 = s.f32.w;
     }
   }
-  if (el < 0 || ion < 0) return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  if (el < 0 || ion < 0) return false;
   p.m_el = h->sp[el].mass; p.q_el = h->sp[el].charge;
   p.m_ion = h->sp[ion].mass; p.q_ion = h->sp[ion].charge;
   p.dt = h->cfg.dt;
   p.fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
   p.shuffle = 1;
   p.seed = h->cfg.seed;
-  p.pass = h->coll_pass++;
   p.status = h->d_status;
+  return true;
+}
+
+LearnedPhys learned_phys(const CollParams& p) {
+  return LearnedPhys{p.m_el, p.q_el, p.m_ion, p.q_ion, p.dt};
+}
+}  // namespace
+
+int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
+  if (!h) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  if (!collision_species(h, v, p))
+    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  p.pass = h->coll_pass++;
   unsigned long long calls = 0;
   if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
     return fail(h, PCG_ERR_CUDA, "collision pass");
   h->launches += 8;
   if (pair_calls) *pair_calls = calls;
   return check_status(h);
+}
+
+int pcg_collide_expectation(pcg_handle* h, double* out) {
+  if (!h || !out) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  if (!collision_species(h, v, p))
+    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  const size_t cells = (size_t)h->g.nr * h->g.nz;
+  double* d = nullptr;
+  if (cudaMalloc((void**)&d, cells * 12 * sizeof(double)) != cudaSuccess) return fail(h, PCG_ERR_NOMEM, "expectation");
+  cudaMemsetAsync(d, 0, cells * 12 * sizeof(double), h->stream);
+  p.pass = h->coll_pass++;
+  p.expect = d;
+  unsigned long long calls = 0;
+  int e = collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream);
+  if (e == 0 && (cudaMemcpyAsync(out, d, cells * 12 * sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+                 cudaStreamSynchronize(h->stream) != cudaSuccess))
+    e = -1;
+  cudaFree(d);
+  return e == 0 ? check_status(h) : fail(h, PCG_ERR_CUDA, "expectation pass");
+}
+
+int pcg_set_collision_model(pcg_handle* h, const float* params, const float* norm) {
+  if (!h || !params || !norm) return PCG_ERR_ARG;
+  if (learned_set_model(h->learned, params, norm, h->stream) != 0) return fail(h, PCG_ERR_NOMEM, "collision model");
+  return PCG_OK;
+}
+
+int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells) {
+  if (!h) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  if (!h->learned.model) return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
+  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  if (!collision_species(h, v, p))
+    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  unsigned long long counts[2] = {0, 0};
+  if (learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream) != 0)
+    return fail(h, PCG_ERR_CUDA, "learned collision step");
+  h->launches += 1 + 2 * v.size();
+  if (counts[1]) {  // the binary operator on the cells outside the training box
+    p.pass = h->coll_pass++;
+    p.only = h->learned.flag;
+    p.only_value = 2;
+    unsigned long long calls = 0;
+    if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
+      return fail(h, PCG_ERR_CUDA, "collision fallback");
+    h->launches += 8;
+  }
+  if (learned_cells) *learned_cells = counts[0];
+  if (fallback_cells) *fallback_cells = counts[1];
+  return check_status(h);
+}
+
+int pcg_cell_moments(pcg_handle* h, double* out) {
+  if (!h || !out) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  collision_species(h, v, p);
+  if (learned_moments(h->g, v.data(), (int)v.size(), h->learned, h->stream) != 0)
+    return fail(h, PCG_ERR_CUDA, "cell moments");
+  CUDA_TRY(h, cudaMemcpyAsync(out, h->learned.mom, h->learned.cells * kMomWords * sizeof(double),
+                              cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return PCG_OK;
+}
+
+int pcg_cell_features(pcg_handle* h, float* x, double* scale) {
+  if (!h || !x || !scale) return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  if (!collision_species(h, v, p))
+    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  const size_t cells = (size_t)h->g.nr * h->g.nz;
+  float* dx = nullptr;
+  double* ds = nullptr;
+  if (cudaMalloc((void**)&dx, cells * kFeatures * sizeof(float)) != cudaSuccess ||
+      cudaMalloc((void**)&ds, cells * sizeof(double)) != cudaSuccess) {
+    cudaFree(dx);
+    return fail(h, PCG_ERR_NOMEM, "feature export");
+  }
+  int e = learned_features(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, dx, ds, h->stream);
+  if (e == 0 && (cudaMemcpyAsync(x, dx, cells * kFeatures * sizeof(float), cudaMemcpyDeviceToHost, h->stream) !=
+                     cudaSuccess ||
+                 cudaMemcpyAsync(scale, ds, cells * sizeof(double), cudaMemcpyDeviceToHost, h->stream) !=
+                     cudaSuccess ||
+                 cudaStreamSynchronize(h->stream) != cudaSuccess))
+    e = -1;
+  cudaFree(dx);
+  cudaFree(ds);
+  return e == 0 ? PCG_OK : fail(h, PCG_ERR_CUDA, "feature export");
 }
 
 int pcg_stage(pcg_handle* h, int stage) {

@@ -3,10 +3,10 @@
 // collisions.cpp:87-236), in double precision on the GPU.
 //
 // Steps, each a kernel:
-//  1. keys: every live particle in the grid gets a 64-bit key (cell, species,
-//     insertion id) in the electron or ion list (ions: species named
-//     "ions"/"Ions"; every other species goes to the electron list, as
-//     sort_to_cells does), and counts per cell;
+//  1. keys: every live particle in the grid (in the selected cells) gets a
+//     64-bit key (cell, species, insertion id), appended to the electron or
+//     ion list (ions: species named "ions"/"Ions"; every other species goes
+//     to the electron list, as sort_to_cells does), and counts per cell;
 //  2. a radix sort of each list by key gives the reference's cell lists
 //     (species order, then particle order) and an exclusive scan the starts;
 //  3. optionally a Fisher-Yates shuffle of every cell list (Philox draws
@@ -43,7 +43,6 @@ constexpr double kEps0 = 8.85e-12, kElCharge = 1.6e-19, kMnzl = 1e-15;
 constexpr double kRelLimit2 = 5e7 * 5e7;
 constexpr double kPlankBar = 6.6261e-34 / (2. * kPi);
 constexpr uint32_t kCollTag = 0x636f6c6cu, kShufTag = 0x73687566u;
-constexpr unsigned long long kNoKey = ~0ull;
 
 inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
@@ -65,32 +64,40 @@ __device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
 // ---------------------------------------------------------------------------
 // 1. keys
 
-__global__ void key_kernel(GridGeom g, SpeciesTable tab, int t, size_t base, unsigned long long* keys,
-                           unsigned long long* vals, unsigned* count) {
+__global__ void key_kernel(GridGeom g, SpeciesTable tab, int t, unsigned long long* keys,
+                           unsigned long long* vals, unsigned* count, unsigned* n_valid,
+                           const unsigned char* only, unsigned char only_value) {
   const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const CollSpecies& sp = tab.s[t];
-  if (j >= sp.n) return;
-  int ci, ck;
-  unsigned id;
-  if (sp.cell) {
-    const int c = sp.cell[j];
-    ci = c < 0 ? -1 : cell_r_of(c);
-    ck = c < 0 ? -1 : cell_z_of(c);
-    id = sp.id[j];
-  } else {
-    const double r = sp.r[j];
-    ci = r >= 0.0 ? (int)floor(r / g.dr) : -1;  // CELL_NUMBER geometry.hpp:198; dead slots have r < 0
-    ck = (int)floor(sp.z[j] / g.dz);
-    id = (unsigned)j;
+  int ci = -1, ck = -1;
+  unsigned id = 0;
+  if (j < sp.n) {
+    if (sp.cell) {
+      const int c = sp.cell[j];
+      ci = c < 0 ? -1 : cell_r_of(c);
+      ck = c < 0 ? -1 : cell_z_of(c);
+      id = sp.id[j];
+    } else {
+      const double r = sp.r[j];
+      ci = r >= 0.0 ? (int)floor(r / g.dr) : -1;  // CELL_NUMBER geometry.hpp:198; dead slots have r < 0
+      ck = (int)floor(sp.z[j] / g.dz);
+      id = (unsigned)j;
+    }
   }
-  unsigned long long key = kNoKey;
-  if (ci >= 0 && ck >= 0 && ci < g.nr && ck < g.nz) {
-    const unsigned long long c = (unsigned long long)ci * g.nz + ck;
-    key = (c << 36) | ((unsigned long long)t << 32) | id;
-    atomicAdd(count + c, 1u);
-  }
-  keys[base + j] = key;
-  vals[base + j] = ((unsigned long long)t << 40) | j;
+  bool valid = ci >= 0 && ck >= 0 && ci < g.nr && ck < g.nz;
+  const unsigned long long c = valid ? (unsigned long long)ci * g.nz + ck : 0ull;
+  if (valid && only && only[c] != only_value) valid = false;
+  // valid entries are appended (keys are unique, so the sort fixes the order)
+  const unsigned mask = __ballot_sync(0xffffffffu, valid);
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (mask && lane == leader) base = atomicAdd(n_valid, (unsigned)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
+  if (!valid) return;
+  const unsigned pos = base + __popc(mask & ((1u << lane) - 1u));
+  keys[pos] = (c << 36) | ((unsigned long long)t << 32) | id;
+  vals[pos] = ((unsigned long long)t << 40) | j;
+  atomicAdd(count + c, 1u);
 }
 
 // ---------------------------------------------------------------------------
@@ -210,8 +217,54 @@ struct PairCtx {
   const SpeciesTable* tab;
   const CollParams* p;
   uint32_t cell;
-  uint32_t m;  // collision number in the cell
+  uint32_t m;      // collision number in the cell
+  double* expect;  // the cell's 12 expected moment changes (expectation mode)
 };
+
+// Mean of cos(chi) and cos(chi)^2 over the P12 scattering-angle draw for
+// s12 (collisionsP12.cpp:215-240): 1 + s ln U for s < 0.1 (E ln U = -1,
+// E ln^2 U = 2); the density exp(A cos) / (2 sinh(A) / A) for s < 6
+// (E cos = coth A - 1/A, E cos^2 = 1 - 2 E[cos] / A); isotropic beyond.
+__device__ __forceinline__ void angle_moments(double s12, double* ec, double* ec2) {
+  double A;
+  if (s12 < 0.1) {
+    *ec = 1 - s12;
+    *ec2 = 1 - 2 * s12 + 2 * s12 * s12;
+    return;
+  } else if (s12 < 3) {
+    const double A_inv = 0.00569578 + 0.9560202 * s12 - 0.508139 * (s12 * s12) +
+                         0.47913906 * pow(s12, 3) - 0.12788975 * pow(s12, 4) + 0.02389567 * pow(s12, 5);
+    A = 1. / A_inv;
+  } else if (s12 < 6.) {
+    A = 3. * exp(-s12);
+  } else {
+    *ec = 0;
+    *ec2 = 1. / 3.;
+    return;
+  }
+  if (A < 1e-4) {  // near isotropic: coth A - 1/A = A/3 - A^3/45
+    *ec = A / 3 - A * A * A / 45;
+  } else {
+    *ec = 1 / tanh(A) - 1 / A;
+  }
+  *ec2 = A < 1e-4 ? 1. / 3. + 2 * A * A / 45 : 1 - 2 * *ec / A;
+}
+
+// Expected change of sum w v and sum w v^2 of a particle of weight w and
+// mass m whose CM momentum sign * p is rotated by the drawn angle (lab
+// velocity vcm + p'/m, deflected with probability prob).  The change is
+// formed directly, (Ec - 1) p / m and (1 - Ec2)(p^2 - 3 p_k^2) / (2 m^2),
+// so that it vanishes exactly without scattering.
+__device__ __forceinline__ void expect_add(double* acc, const double vcm[3], const double p[3], double sign,
+                                           double m, double w, double prob, double ec, double ec2) {
+  const double p2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+  for (int k = 0; k < 3; ++k) {
+    const double d1 = sign * (ec - 1) * p[k] / m;
+    const double d2 = 2 * vcm[k] * d1 + (1 - ec2) * (p2 - 3 * p[k] * p[k]) / (2 * m * m);
+    acc[k] += prob * w * d1;
+    acc[3 + k] += prob * w * d2;
+  }
+}
 
 __device__ void p12_single(PairCtx& x, double m_real_a, double m_real_b, double q_real_a,
                            double q_real_b, unsigned long long ra, unsigned long long rb,
@@ -303,6 +356,14 @@ __device__ void p12_single(PairCtx& x, double m_real_a, double m_real_b, double 
                           (na > nb ? na : nb) * v_rel_abs;
     if (s12max < s12) s12 = s12max;
   }
+  if (x.expect) {  // record this collision's mean change given the velocities it meets
+    double ec, ec2;
+    angle_moments(s12, &ec, &ec2);
+    const double pb_prob = fixed ? w_a / w_b : 1.0;
+    const int la = x.tab->s[(swap ? rb : ra) >> 40].is_ion, lb = x.tab->s[(swap ? ra : rb) >> 40].is_ion;
+    expect_add(x.expect + 6 * la, v_cm, p_a_cm, 1.0, mass_a, w_a, 1.0, ec, ec2);
+    expect_add(x.expect + 6 * lb, v_cm, p_a_cm, -1.0, mass_b, w_b, pb_prob, ec, ec2);
+  }
 
   uint32_t o[4], o2[4];
   philox4x32_10(x.cell, 2u * x.m, P.pass, kCollTag, (uint32_t)P.seed, (uint32_t)(P.seed >> 32), o);
@@ -386,6 +447,7 @@ __global__ void collide_kernel(GridGeom g, SpeciesTable tab, CollParams p, const
                                const int* row_stop, unsigned long long* calls) {
   const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (c >= (size_t)g.nr * g.nz) return;
+  if (p.only && p.only[c] != p.only_value) return;
   const int i = (int)(c / g.nz), k = (int)(c - (size_t)i * g.nz);
   const double T_el = mom[4 * c], T_ion = mom[4 * c + 1], n_el = mom[4 * c + 2], n_ion = mom[4 * c + 3];
   if (p.fixed) {
@@ -398,7 +460,8 @@ __global__ void collide_kernel(GridGeom g, SpeciesTable tab, CollParams p, const
   const unsigned long long* I = li + st_i[c];
   const unsigned ne = n_e[c], ni = n_i[c];
   const double me = p.m_el, mi = p.m_ion, qe = p.q_el, qi = p.q_ion;
-  PairCtx x{&tab, &p, (uint32_t)c, 0u};
+  double expect[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  PairCtx x{&tab, &p, (uint32_t)c, 0u, p.expect ? expect : nullptr};
 #define COLL(MA, MB, QA, QB, A, B, NA, NB) \
   do { p12_single(x, MA, MB, QA, QB, A, B, NA, NB, debye); ++x.m; } while (0)
   if (ni % 2 == 0)
@@ -457,6 +520,8 @@ __global__ void collide_kernel(GridGeom g, SpeciesTable tab, CollParams p, const
   }
 #undef COLL
   if (x.m) atomicAdd(calls, (unsigned long long)x.m);
+  if (p.expect)
+    for (int q = 0; q < 12; ++q) p.expect[c * 12 + q] = expect[q];
 }
 
 template <typename T>
@@ -473,7 +538,7 @@ void collide_free(CollWork& w) {
     cudaFree(w.keys[l]); cudaFree(w.keys2[l]); cudaFree(w.vals[l]); cudaFree(w.vals2[l]);
     cudaFree(w.count[l]); cudaFree(w.start[l]);
   }
-  cudaFree(w.moments); cudaFree(w.row_stop); cudaFree(w.calls); cudaFree(w.tmp);
+  cudaFree(w.moments); cudaFree(w.row_stop); cudaFree(w.calls); cudaFree(w.valid); cudaFree(w.tmp);
   w = CollWork();
 }
 
@@ -495,7 +560,9 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
           grow(&w.vals2[l], need) || grow(&w.count[l], cells + 1) || grow(&w.start[l], cells + 1))
         return -1;
     }
-    if (grow(&w.moments, 4 * cells) || grow(&w.row_stop, (size_t)g.nr) || grow(&w.calls, 1)) return -1;
+    if (grow(&w.moments, 4 * cells) || grow(&w.row_stop, (size_t)g.nr) || grow(&w.calls, 1) ||
+        grow(&w.valid, 2))
+      return -1;
     size_t b1 = 0, b2 = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b1, w.keys[0], w.keys2[0], w.vals[0], w.vals2[0], (int)need);
     cub::DeviceScan::ExclusiveSum(nullptr, b2, w.count[0], w.start[0], (int)(cells + 1));
@@ -505,26 +572,30 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
     w.cells = cells;
   }
   cudaMemsetAsync(w.calls, 0, sizeof(unsigned long long), s);
+  cudaMemsetAsync(w.valid, 0, 2 * sizeof(unsigned), s);
   for (int l = 0; l < 2; ++l) {
     cudaMemsetAsync(w.count[l], 0, (cells + 1) * sizeof(unsigned), s);
-    size_t base = 0;
     for (int t = 0; t < nsp; ++t) {
-      if ((sp[t].is_ion ? 1 : 0) != l) continue;
-      if (sp[t].n)
-        key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, tab, t, base, w.keys[l], w.vals[l], w.count[l]);
-      base += sp[t].n;
+      if ((sp[t].is_ion ? 1 : 0) != l || !sp[t].n) continue;
+      key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, tab, t, w.keys[l], w.vals[l], w.count[l],
+                                                          w.valid + l, p.only, p.only_value);
     }
-    if (total[l]) {
+  }
+  unsigned valid[2] = {0, 0};
+  if (cudaMemcpyAsync(valid, w.valid, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  for (int l = 0; l < 2; ++l) {
+    if (valid[l]) {
       size_t b = w.tmp_bytes;
-      // keys: cell < 2^28 (36 + 28 bits), species and id below
-      int bits = 36;  // the key is cell << 36 | species << 32 | id
+      int bits = 36;  // the key is cell << 36 | species << 32 | id, cell < 2^28
       while (bits < 64 && (1ull << (bits - 36)) < cells) ++bits;
       cub::DeviceRadixSort::SortPairs(w.tmp, b, w.keys[l], w.keys2[l], w.vals[l], w.vals2[l],
-                                      (int)total[l], 0, std::min(bits + 1, 64), s);
+                                      (int)valid[l], 0, std::min(bits + 1, 64), s);
     }
     size_t b = w.tmp_bytes;
     cub::DeviceScan::ExclusiveSum(w.tmp, b, w.count[l], w.start[l], (int)(cells + 1), s);
-    if (p.shuffle && total[l])
+    if (p.shuffle && valid[l])
       shuffle_kernel<<<blocks_for(cells), kThreads, 0, s>>>(cells, w.start[l], w.count[l], w.vals2[l],
                                                              p.seed, p.pass, (uint32_t)l);
   }

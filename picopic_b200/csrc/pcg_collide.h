@@ -38,6 +38,14 @@ struct CollParams {
   uint64_t seed;
   uint32_t pass;     // counter of collision passes: the Philox stream of this one
   DevStatus* status; // superluminal pairs raise the error word (rel.cpp:33-34 is fatal)
+  const unsigned char* only = nullptr;  // when set, collide only cells c with only[c] == only_value
+  unsigned char only_value = 1;
+  // when set, per cell the sum over the pass's collisions of each
+  // collision's mean change over its scattering draw, given the velocities
+  // it meets (the pass itself runs as usual): 12 doubles, sum w v (3) then
+  // sum w v^2 (3) of the electron list, then of the ion list
+  // (non-relativistic kinematics of the mean)
+  double* expect = nullptr;
 };
 
 // Scratch of a collision pass, grown on demand and kept by the handle.
@@ -48,6 +56,7 @@ struct CollWork {
   double* moments = nullptr;                // per cell: T_el, T_ion, n_el, n_ion
   int* row_stop = nullptr;                  // per row: first cell that stops the row
   unsigned long long* calls = nullptr;      // device counter of pair calls
+  unsigned* valid = nullptr;                // device: entries appended to each list
   void* tmp = nullptr;
   size_t tmp_bytes = 0;
   size_t cells = 0;

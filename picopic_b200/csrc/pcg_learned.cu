@@ -1,0 +1,349 @@
+// pcg_learned.cu — the learned collision step.
+//
+// Per cell and per list (electrons: every species not named ions; ions),
+// the moment sums N, W = sum w, W u = sum w v, sum w v^2 (per axis r, phi,
+// z) give the mean velocity u and the axis temperatures
+// T_a = m (sum w v_a^2 / W - u_a^2) / e (eV).  The 13 features are
+//   0-2   T_e,a / T_e - 1            (electron anisotropy, T_e the axis mean)
+//   3-5   T_i,a / T_i - 1            (ion anisotropy)
+//   6     ln(T_i / T_e)
+//   7-9   log10 of s_ee, s_ei, s_ii  (collision numbers of the step)
+//   10    |u_e - u_i| / sqrt(3 e T_e / m_e)
+//   11    ln(n_i / n_e)
+//   12    1 / sqrt(N_e + N_i)        (macroparticle noise)
+// with s_ab = max(n_a, n_b) dt L (q_a q_b)^2 / (4 pi eps0^2 m_ab^2 v_ab^3),
+// v_ab^2 = 3 e (T_a/m_a + T_b/m_b), L = 10: the P12 scattering parameter
+// (collisionsP12.cpp:193-201) at the thermal relative speed.  The network
+// predicts y, the change of the axis temperatures over one step in units of
+// T_s S, S = s_ee + s_ei + s_ii:
+//   T'_s,a = T_s,a + T_s S y_s,a.
+// The new temperatures are scaled by one factor per cell so that the
+// cell's thermal energy sum_s W_s sum_a T_s,a is unchanged, and every
+// particle of the cell moves to v_a' = u_a + (v_a - u_a) sqrt(T'_a / T_a):
+// the species' momentum and the new second moments hold exactly in FP64.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "pcg_f32.h"
+#include "pcg_learned.h"
+#include "pcg_mlp.cuh"
+
+namespace pcg {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr double kPi = 3.1415926535897932, kEps0 = 8.85e-12, kE = 1.6e-19, kLogL = 10.0;
+constexpr int kStateWords = 17;  // T_e[3], T_i[3], Tm_e, Tm_i, W_e, W_i, u_e[3], u_i[3], S
+// the training box is widened by this fraction of each feature's span
+constexpr float kBoxMargin = 0.25f;
+
+inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+// cell and velocity of slot j of a species; false for dead slots or cells off the grid
+__device__ __forceinline__ bool slot_of(const GridGeom& g, const CollSpecies& sp, size_t j, size_t* c,
+                                        double v[3]) {
+  int ci, ck;
+  if (sp.cell) {
+    const int p = sp.cell[j];
+    if (p < 0) return false;
+    ci = cell_r_of(p);
+    ck = cell_z_of(p);
+    v[0] = sp.vr32[j]; v[1] = sp.vphi32[j]; v[2] = sp.vz32[j];
+  } else {
+    const double r = sp.r[j];
+    if (!(r >= 0.0)) return false;
+    ci = (int)floor(r / g.dr);
+    ck = (int)floor(sp.z[j] / g.dz);
+    v[0] = sp.vr64[j]; v[1] = sp.vphi64[j]; v[2] = sp.vz64[j];
+  }
+  if (ci < 0 || ck < 0 || ci >= g.nr || ck >= g.nz) return false;
+  *c = (size_t)ci * g.nz + ck;
+  return true;
+}
+
+// Per-cell moment sums.  Lanes of a warp that share a cell and list add
+// their values with a warp reduction first (whole-warp groups, the usual
+// case for particles stored cell by cell) or one after another through the
+// group's leader, so that one atomic per word and group reaches memory.
+__global__ void moments_kernel(GridGeom g, CollSpecies sp, double* mom) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t c = 0;
+  double v[3] = {0, 0, 0}, w = 0;
+  const bool valid = j < sp.n && slot_of(g, sp, j, &c, v);
+  if (valid) w = sp.w64 ? sp.w64[j] : (double)sp.w32[j];
+  double val[8] = {valid ? 1.0 : 0.0, w, w * v[0], w * v[1], w * v[2], w * v[0] * v[0], w * v[1] * v[1],
+                   w * v[2] * v[2]};
+  const long long key = valid ? (long long)c : -1;
+  const unsigned group = __match_any_sync(0xffffffffu, key);
+  const int lane = threadIdx.x & 31, leader = __ffs(group) - 1;
+  if (group == 0xffffffffu) {
+    for (int q = 0; q < 8; ++q)
+      for (int o = 16; o > 0; o >>= 1) val[q] += __shfl_xor_sync(0xffffffffu, val[q], o);
+  } else {
+    // the leader gathers its group's values lane by lane
+    unsigned rest = group & ~(1u << leader);
+    while (__any_sync(0xffffffffu, rest != 0)) {
+      const int src = rest ? __ffs(rest) - 1 : lane;
+      for (int q = 0; q < 8; ++q) {
+        const double x = __shfl_sync(0xffffffffu, val[q], src);
+        if (lane == leader && rest) val[q] += x;
+      }
+      if (rest) rest &= rest - 1;
+    }
+  }
+  if (!valid || lane != leader) return;
+  double* m = mom + c * kMomWords + (sp.is_ion ? 8 : 0);
+  for (int q = 0; q < 8; ++q) atomicAdd(m + q, val[q]);
+}
+
+// The state and raw features of cell c (row i); false when the cell has
+// fewer than two particles in a list or no positive temperature.
+__device__ bool cell_features(const GridGeom& g, const LearnedPhys& ph, const double* m, int i,
+                              double st[kStateWords], float x[kFeatures]) {
+  const double mass[2] = {ph.m_el, ph.m_ion}, q[2] = {ph.q_el, ph.q_ion};
+  const double vol = kPi * g.dz * g.dr * g.dr * (2.0 * i + 1);
+  double n[2], N[2];
+  for (int l = 0; l < 2; ++l) {
+    const double* ml = m + 8 * l;
+    N[l] = ml[0];
+    const double W = ml[1];
+    if (N[l] < 2.0 || !(W > 0.0)) return false;
+    double tm = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const double u = ml[2 + a] / W;
+      const double T = mass[l] * (ml[5 + a] / W - u * u) / kE;
+      st[3 * l + a] = T;
+      st[10 + 3 * l + a] = u;
+      tm += T;
+    }
+    tm /= 3.0;
+    if (!(tm > 0.0)) return false;
+    st[6 + l] = tm;
+    st[8 + l] = W;
+    n[l] = W / vol;
+  }
+  auto s_of = [&](int a, int b) {
+    const double mab = mass[a] * mass[b] / (mass[a] + mass[b]);
+    const double v2 = 3.0 * kE * (st[6 + a] / mass[a] + st[6 + b] / mass[b]);
+    const double qq = q[a] * q[b];
+    const double em = kEps0 * mab;
+    return fmax(n[a], n[b]) * ph.dt * kLogL * (qq * qq) / (4.0 * kPi * em * em * v2 * sqrt(v2));
+  };
+  const double see = s_of(0, 0), sei = s_of(0, 1), sii = s_of(1, 1);
+  st[16] = see + sei + sii;
+  for (int a = 0; a < 3; ++a) {
+    x[a] = (float)(st[a] / st[6] - 1.0);
+    x[3 + a] = (float)(st[3 + a] / st[7] - 1.0);
+  }
+  x[6] = (float)log(st[7] / st[6]);
+  x[7] = (float)log10(see);
+  x[8] = (float)log10(sei);
+  x[9] = (float)log10(sii);
+  double du2 = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double d = st[10 + a] - st[13 + a];
+    du2 += d * d;
+  }
+  x[10] = (float)sqrt(du2 / (3.0 * kE * st[6] / mass[0]));
+  x[11] = (float)log(n[1] / n[0]);
+  x[12] = (float)(1.0 / sqrt(N[0] + N[1]));
+  return true;
+}
+
+__global__ void features_kernel(GridGeom g, LearnedPhys ph, const double* mom, float* x, double* scale) {
+  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= (size_t)g.nr * g.nz) return;
+  double st[kStateWords];
+  float f[kFeatures];
+  const bool ok = cell_features(g, ph, mom + c * kMomWords, (int)(c / g.nz), st, f);
+  for (int k = 0; k < kFeatures; ++k) x[c * kFeatures + k] = ok ? f[k] : __int_as_float(0x7fc00000);
+  scale[c] = ok ? st[16] : 0.0;
+}
+
+struct LearnSmem {
+  double st[mlp::kRowsPerBlock][kStateWords];
+  float y[mlp::kRowsPerBlock][mlp::kOutPad];
+  mlp::FwdSmem f;
+  unsigned char state[mlp::kRowsPerBlock];  // 0 none, 1 learned, 2 fallback
+  unsigned long long n_learned, n_fallback;
+};
+
+// Blocks take tiles of 64 cells in turn (the weights are staged in shared
+// memory once per block): features (one thread per cell), the MLP on the
+// tensor cores (a warp per 16 cells), then the new temperatures and the
+// transform of each cell.
+__global__ void __launch_bounds__(mlp::kMlpThreads) learned_cells_kernel(GridGeom g, LearnedPhys ph,
+                                                                         const double* mom, const float* P,
+                                                                         LearnedNorm nm, double* xform,
+                                                                         unsigned char* flag,
+                                                                         unsigned long long* count) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  LearnSmem& sm = *reinterpret_cast<LearnSmem*>(raw);
+  const size_t cells = (size_t)g.nr * g.nz;
+  const size_t tiles = (cells + mlp::kRowsPerBlock - 1) / mlp::kRowsPerBlock;
+  mlp::load_forward_weights(sm.f.W1t, sm.f.W2t, sm.f.W3t, P);
+  mlp::load_biases(sm.f, P);
+  if (threadIdx.x == 0) { sm.n_learned = 0; sm.n_fallback = 0; }
+  for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const size_t c0 = tile * mlp::kRowsPerBlock;
+    __syncthreads();  // the previous tile is done with X, y and the state
+    if (threadIdx.x < mlp::kRowsPerBlock) {
+      const int r = threadIdx.x;
+      const size_t c = c0 + r;
+      float x[kFeatures];
+      unsigned char stt = 0;
+      if (c < cells && cell_features(g, ph, mom + c * kMomWords, (int)(c / g.nz), sm.st[r], x)) {
+        stt = 1;
+        for (int k = 0; k < kFeatures; ++k) {
+          const float span = nm.x_hi[k] - nm.x_lo[k];
+          if (!(x[k] >= nm.x_lo[k] - kBoxMargin * span && x[k] <= nm.x_hi[k] + kBoxMargin * span)) stt = 2;
+        }
+      }
+      sm.state[r] = stt;
+      for (int k = 0; k < mlp::kInPad; ++k)
+        sm.f.X[r * mlp::kInPad + k] =
+            __float2bfloat16_rn(stt == 1 && k < kFeatures ? (x[k] - nm.x_mean[k]) / nm.x_std[k] : 0.f);
+    }
+    __syncthreads();
+    {
+      const int lane = threadIdx.x & 31, wr = (threadIdx.x >> 5) * 16, gq = lane >> 2, t = lane & 3;
+      float out[1][4];
+      mlp::forward_rows(sm.f, wr, lane, out);
+      for (int h = 0; h < 2; ++h)
+        for (int q = 0; q < 2; ++q) sm.y[wr + gq + 8 * h][2 * t + q] = out[0][2 * h + q];
+    }
+    __syncthreads();
+    if (threadIdx.x < mlp::kRowsPerBlock) {
+      const int r = threadIdx.x;
+      const size_t c = c0 + r;
+      if (c < cells) {
+        const unsigned char stt = sm.state[r];
+        double xf[12] = {0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1};
+        if (stt == 1) {
+          const double* st = sm.st[r];
+          double Tn[2][3], e0 = 0.0, e1 = 0.0;
+          for (int l = 0; l < 2; ++l)
+            for (int a = 0; a < 3; ++a) {
+              const double y = (double)sm.y[r][3 * l + a] * nm.y_std[3 * l + a] + nm.y_mean[3 * l + a];
+              Tn[l][a] = st[3 * l + a] + st[6 + l] * st[16] * y;
+              e0 += st[8 + l] * st[3 * l + a];
+              e1 += st[8 + l] * Tn[l][a];
+            }
+          const double f = e1 > 0.0 ? e0 / e1 : 1.0;  // the cell's thermal energy is kept
+          for (int l = 0; l < 2; ++l)
+            for (int a = 0; a < 3; ++a) {
+              const double T = st[3 * l + a], T1 = fmax(Tn[l][a] * f, 1e-6 * st[6 + l]);
+              xf[6 * l + a] = st[10 + 3 * l + a];
+              xf[6 * l + 3 + a] = T > 0.0 ? sqrt(T1 / T) : 1.0;
+            }
+          atomicAdd(&sm.n_learned, 1ull);
+        } else if (stt == 2) {
+          atomicAdd(&sm.n_fallback, 1ull);
+        }
+        for (int q = 0; q < 12; ++q) xform[c * 12 + q] = xf[q];
+        flag[c] = stt;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (sm.n_learned) atomicAdd(count, sm.n_learned);
+    if (sm.n_fallback) atomicAdd(count + 1, sm.n_fallback);
+  }
+}
+
+__global__ void transform_kernel(GridGeom g, CollSpecies sp, const double* xform, const unsigned char* flag) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= sp.n) return;
+  size_t c;
+  double v[3];
+  if (!slot_of(g, sp, j, &c, v) || flag[c] != 1) return;
+  const double* t = xform + c * 12 + (sp.is_ion ? 6 : 0);
+  for (int a = 0; a < 3; ++a) v[a] = t[a] + (v[a] - t[a]) * t[3 + a];
+  if (sp.cell) {
+    sp.vr32[j] = (float)v[0]; sp.vphi32[j] = (float)v[1]; sp.vz32[j] = (float)v[2];
+  } else {
+    sp.vr64[j] = v[0]; sp.vphi64[j] = v[1]; sp.vz64[j] = v[2];
+  }
+}
+
+template <typename T>
+int grow(T** p, size_t n) {
+  cudaFree(*p);
+  *p = nullptr;
+  return cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess ? 0 : -1;
+}
+
+int ensure(const GridGeom& g, LearnedWork& w) {
+  const size_t cells = (size_t)g.nr * g.nz;
+  if (w.cells == cells && w.mom) return 0;
+  if (grow(&w.mom, cells * kMomWords) || grow(&w.xform, cells * 12) || grow(&w.flag, cells) ||
+      grow(&w.count, 2))
+    return -1;
+  w.cells = cells;
+  return 0;
+}
+
+}  // namespace
+
+int learned_moments(const GridGeom& g, const CollSpecies* sp, int nsp, LearnedWork& w, cudaStream_t s) {
+  if (ensure(g, w)) return -1;
+  cudaMemsetAsync(w.mom, 0, w.cells * kMomWords * sizeof(double), s);
+  for (int t = 0; t < nsp; ++t)
+    if (sp[t].n) moments_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.mom);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int learned_features(const GridGeom& g, const CollSpecies* sp, int nsp, const LearnedPhys& ph, LearnedWork& w,
+                     float* x, double* scale, cudaStream_t s) {
+  if (learned_moments(g, sp, nsp, w, s)) return -1;
+  features_kernel<<<blocks_for(w.cells), kThreads, 0, s>>>(g, ph, w.mom, x, scale);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const LearnedPhys& ph, LearnedWork& w,
+                 unsigned long long counts[2], cudaStream_t s) {
+  if (!w.model) return -1;
+  if (learned_moments(g, sp, nsp, w, s)) return -1;
+  static const bool attr = cudaFuncSetAttribute(learned_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)sizeof(LearnSmem)) == cudaSuccess;
+  if (!attr) return -1;
+  cudaMemsetAsync(w.count, 0, 2 * sizeof(unsigned long long), s);
+  const size_t tiles = (w.cells + mlp::kRowsPerBlock - 1) / mlp::kRowsPerBlock;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned blocks = (unsigned)std::min<size_t>(tiles, (size_t)sms * 2);
+  learned_cells_kernel<<<blocks, mlp::kMlpThreads, sizeof(LearnSmem), s>>>(g, ph, w.mom, w.params, w.norm,
+                                                                           w.xform, w.flag, w.count);
+  for (int t = 0; t < nsp; ++t)
+    if (sp[t].n) transform_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.xform, w.flag);
+  if (cudaMemcpyAsync(counts, w.count, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int learned_set_model(LearnedWork& w, const float* params_host, const float* norm_host, cudaStream_t s) {
+  if (!w.params && grow(&w.params, (size_t)mlp::kParams)) return -1;
+  if (cudaMemcpyAsync(w.params, params_host, mlp::kParams * sizeof(float), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return -1;
+  static_assert(sizeof(LearnedNorm) == kNormFloats * sizeof(float), "normalisation block");
+  std::memcpy(&w.norm, norm_host, sizeof(LearnedNorm));
+  w.model = true;
+  return 0;
+}
+
+void learned_free(LearnedWork& w) {
+  cudaFree(w.mom); cudaFree(w.xform); cudaFree(w.flag); cudaFree(w.count); cudaFree(w.params);
+  w = LearnedWork();
+}
+
+}  // namespace pcg

@@ -39,7 +39,7 @@ namespace pcg {
 namespace mlp {
 namespace {
 
-constexpr int kRowsPerBlock = 64, kThreads = 128;
+constexpr int kThreads = 128;
 
 struct TrainSmem {
   __nv_bfloat16 W1t[kW1tElems], W2t[kW2tElems], W3t[kW3tElems];
@@ -51,13 +51,6 @@ struct TrainSmem {
   __nv_bfloat16 dH2[kRowsPerBlock * kHid], dH1[kRowsPerBlock * kHid];
   float b1[kHid], b2[kHid], b3[kOutPad];
   float db[kHid + kHid + kOutPad];
-};
-
-struct FwdSmem {
-  __nv_bfloat16 W1t[kW1tElems], W2t[kW2tElems], W3t[kW3tElems];
-  __nv_bfloat16 X[kRowsPerBlock * kInPad];
-  __nv_bfloat16 H1[kRowsPerBlock * kHid], H2[kRowsPerBlock * kHid];
-  float b1[kHid], b2[kHid], b3[kOutPad];
 };
 
 // rows of this block: data index of block row r (a minibatch draw, or r itself)
@@ -80,36 +73,6 @@ __device__ __forceinline__ void load_rows(S& sm, const float* x, size_t r0, size
     if (r0 + r < nrows && k < kIn) v = x[data_row(r0 + r, rows, sample, seed, step) * kIn + k];
     sm.X[q] = __float2bfloat16_rn(v);
   }
-}
-
-template <class S>
-__device__ __forceinline__ void load_biases(S& sm, const float* P) {
-  for (int q = threadIdx.x; q < kHid; q += blockDim.x) {
-    sm.b1[q] = P[kOffB1 + q];
-    sm.b2[q] = P[kOffB2 + q];
-  }
-  if (threadIdx.x < kOutPad) sm.b3[threadIdx.x] = threadIdx.x < kOut ? P[kOffB3 + threadIdx.x] : 0.f;
-}
-
-// forward of this warp's 16 rows; returns the output accumulators
-template <class S>
-__device__ __forceinline__ void forward_rows(S& sm, int r0, int lane, float out[1][4]) {
-  float acc[kHid / 8][4];
-  for (int i = 0; i < kHid / 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-  warp_gemm<kInPad, kHid>(acc, sm.X, kInPad, r0, sm.W1t, kInPad, lane);
-  bias_relu_store<kHid>(acc, sm.b1, true, sm.H1, kHid, r0, lane);
-  __syncwarp();
-  for (int i = 0; i < kHid / 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
-  warp_gemm<kHid, kHid>(acc, sm.H1, kHid, r0, sm.W2t, kHid, lane);
-  bias_relu_store<kHid>(acc, sm.b2, true, sm.H2, kHid, r0, lane);
-  __syncwarp();
-  out[0][0] = out[0][1] = out[0][2] = out[0][3] = 0.f;
-  warp_gemm<kHid, kOutPad>(out, sm.H2, kHid, r0, sm.W3t, kHid, lane);
-  const int t = lane & 3;
-  out[0][0] += sm.b3[2 * t];
-  out[0][1] += sm.b3[2 * t + 1];
-  out[0][2] += sm.b3[2 * t];
-  out[0][3] += sm.b3[2 * t + 1];
 }
 
 __global__ void __launch_bounds__(kThreads) forward_kernel(const float* P, const float* x, size_t rows, float* y) {

@@ -138,5 +138,47 @@ __device__ __forceinline__ void load_forward_weights(__nv_bfloat16* W1t, __nv_bf
   }
 }
 
+// A block of kMlpThreads threads (4 warps) runs the forward pass of 64 rows.
+constexpr int kRowsPerBlock = 64, kMlpThreads = 128;
+
+struct FwdSmem {
+  __nv_bfloat16 W1t[kW1tElems], W2t[kW2tElems], W3t[kW3tElems];
+  __nv_bfloat16 X[kRowsPerBlock * kInPad];
+  __nv_bfloat16 H1[kRowsPerBlock * kHid], H2[kRowsPerBlock * kHid];
+  float b1[kHid], b2[kHid], b3[kOutPad];
+};
+
+template <class S>
+__device__ __forceinline__ void load_biases(S& sm, const float* P) {
+  for (int q = threadIdx.x; q < kHid; q += blockDim.x) {
+    sm.b1[q] = P[kOffB1 + q];
+    sm.b2[q] = P[kOffB2 + q];
+  }
+  if (threadIdx.x < kOutPad) sm.b3[threadIdx.x] = threadIdx.x < kOut ? P[kOffB3 + threadIdx.x] : 0.f;
+}
+
+// Forward pass of one warp's 16 rows of sm.X (BF16, [64][16]); the hidden
+// activations go to sm.H1 / sm.H2 and the outputs stay in out (C layout:
+// out[0][2h+q] is row g + 8h, column 2t + q).
+template <class S>
+__device__ __forceinline__ void forward_rows(S& sm, int r0, int lane, float out[1][4]) {
+  float acc[kHid / 8][4];
+  for (int i = 0; i < kHid / 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+  warp_gemm<kInPad, kHid>(acc, sm.X, kInPad, r0, sm.W1t, kInPad, lane);
+  bias_relu_store<kHid>(acc, sm.b1, true, sm.H1, kHid, r0, lane);
+  __syncwarp();
+  for (int i = 0; i < kHid / 8; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+  warp_gemm<kHid, kHid>(acc, sm.H1, kHid, r0, sm.W2t, kHid, lane);
+  bias_relu_store<kHid>(acc, sm.b2, true, sm.H2, kHid, r0, lane);
+  __syncwarp();
+  out[0][0] = out[0][1] = out[0][2] = out[0][3] = 0.f;
+  warp_gemm<kHid, kOutPad>(out, sm.H2, kHid, r0, sm.W3t, kHid, lane);
+  const int t = lane & 3;
+  out[0][0] += sm.b3[2 * t];
+  out[0][1] += sm.b3[2 * t + 1];
+  out[0][2] += sm.b3[2 * t];
+  out[0][3] += sm.b3[2 * t + 1];
+}
+
 }  // namespace mlp
 }  // namespace pcg

@@ -190,6 +190,44 @@ class Domain:
         self._check(self.lib.pcg_collide(self.h, ctypes.byref(n)), "pcg_collide")
         return int(n.value)
 
+    # -- learned collisions (no reference counterpart) ---------------------------------
+    def set_collision_model(self, params, norm):
+        """Load the collision MLP's parameters (PCG_MLP_PARAMS floats) and its
+        normalisation / training box (PCG_LEARNED_NORM floats)."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        n = np.ascontiguousarray(norm, dtype=np.float32)
+        pf = ctypes.POINTER(ctypes.c_float)
+        self._check(self.lib.pcg_set_collision_model(self.h, p.ctypes.data_as(pf), n.ctypes.data_as(pf)),
+                    "pcg_set_collision_model")
+
+    def collide_learned(self):
+        """One learned collision step; returns (learned cells, binary fallback cells)."""
+        a, b = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)
+        self._check(self.lib.pcg_collide_learned(self.h, ctypes.byref(a), ctypes.byref(b)), "pcg_collide_learned")
+        return int(a.value), int(b.value)
+
+    def collide_expectation(self) -> np.ndarray:
+        """One binary pass; returns (nr*nz, 12): per cell and list the sum over its
+        collisions of each collision's mean change of sum w v (3), sum w v^2 (3)."""
+        m = np.zeros((self.grid.nr * self.grid.nz, 12))
+        self._check(self.lib.pcg_collide_expectation(self.h, _dp(m)), "pcg_collide_expectation")
+        return m
+
+    def cell_moments(self) -> np.ndarray:
+        """(nr*nz, 16): per cell, electron list then ion list: N, sum w, sum w v (3), sum w v^2 (3)."""
+        m = np.zeros((self.grid.nr * self.grid.nz, 16))
+        self._check(self.lib.pcg_cell_moments(self.h, _dp(m)), "pcg_cell_moments")
+        return m
+
+    def cell_features(self):
+        """Raw features (nr*nz, 13; NaN where a cell takes no collisions) and the scale S."""
+        cells = self.grid.nr * self.grid.nz
+        x = np.zeros((cells, 13), dtype=np.float32)
+        s = np.zeros(cells)
+        self._check(self.lib.pcg_cell_features(self.h, x.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _dp(s)),
+                    "pcg_cell_features")
+        return x, s
+
     # -- acceptance diagnostics of the deposit (no reference counterpart) ------------
     def node_charge(self) -> np.ndarray:
         """Node charges (C) in the shape the Villasenor-Buneman deposit conserves."""
