@@ -264,6 +264,9 @@ def run_gpu(args):
         torch.cuda.empty_cache()
     if not args.no_e2e:
         e2e = run_e2e(w, args, rank, local, barrier, allmax, allsum)
+    coll = None
+    if not args.no_collisions:
+        coll = run_collisions(args, local, barrier, allmax)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w)
     if rank == 0:
@@ -284,12 +287,70 @@ def run_gpu(args):
             "clocks": clocks,
             "f64": f64,
             "e2e": e2e,
+            "collisions": coll,
             "cpu_baseline": cpu,
             "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
         }
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+# Collisional anisotropy relaxation: 512 x 2048 cells of dr = dz = 1e-5 m
+# (the cell size is not given for this workload; 1e-5 m is ~14 Debye
+# lengths at 1 eV and 1e20 m^-3), 100 macroparticles per cell per species,
+# electrons T_par = 2 eV, T_perp = 1 eV, ions 0.5 eV, dt = 0.5 Courant.
+COLLISIONS = dict(name="collisional anisotropy relaxation 512x2048, 100 ppc/species e+p, n 1e20",
+                  nr=512, nz=2048, dr=1e-5, density=1e20, ppc=100, te_par=2.0, te_perp=1.0, ti=0.5)
+
+
+def run_collisions(args, local, barrier, allmax):
+    """One collision step on the collisional workload, binary (Perez 2012,
+    FP64 per pair) against learned (BF16 tensor-core MLP + FP64 transform):
+    device time per step, and the electron anisotropy relaxation time of
+    both operators at the same start on a 64 x 128-cell slab (the binary
+    one averaged over independent passes)."""
+    import torch
+    from picopic_b200 import Domain, Geometry
+    from picopic_b200 import learned as L
+    c = COLLISIONS
+    if args.small:
+        c = dict(c, nr=128, nz=256)
+    g = Geometry(c["nr"], c["nz"], c["nr"] * c["dr"], c["nz"] * c["dr"], dt_courant(c["dr"]))
+    n = c["nr"] * c["nz"] * c["ppc"]
+    d = Domain(g, precision="f32", quirks="fixed", seed=11, device=local)
+    d.add(L.ELECTRONS, capacity=n)
+    d.add(L.IONS, capacity=n)
+    d.seed_plasma_cells(0, c["ppc"], c["density"], c["te_par"], c["te_perp"], seed=1)
+    d.seed_plasma_cells(1, c["ppc"], c["density"], c["ti"], seed=2)
+    d.set_collision_model(*L.load_model())
+    d.collide()
+    d.collide_learned()
+    d.synchronize()
+    stream = torch.cuda.ExternalStream(d.stream)
+
+    def timed(fn, k):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = [fn() for _ in range(k)]
+        e1.record(stream)
+        e1.synchronize()
+        return allmax(e0.elapsed_time(e1)) / k, out
+
+    bin_ms, _ = timed(d.collide, 3)
+    lrn_ms, counts = timed(d.collide_learned, 10)
+    del d
+    torch.cuda.empty_cache()
+    gs = Geometry(64, 128, 64 * c["dr"], 128 * c["dr"], 1e-13)
+    tb, eb, _ = L.initial_relaxation_time(gs, "binary", passes=60, density=3e20, device=local)
+    tl, _, _ = L.initial_relaxation_time(gs, "learned", passes=1, density=3e20, device=local)
+    cells = c["nr"] * c["nz"]
+    return {"workload": c["name"], "particles": 2 * n, "precision": "f32 particles, FP64 collision arithmetic",
+            "binary_ms_per_step": bin_ms, "learned_ms_per_step": lrn_ms, "speedup": bin_ms / lrn_ms,
+            "learned_cell_fraction": counts[-1][0] / cells, "fallback_cell_fraction": counts[-1][1] / cells,
+            "relaxation_time_steps": {"slab": "64x128 cells, 100 ppc, n 3e20, dt 1e-13, Te 2/1 eV, Ti 0.5 eV",
+                                      "binary": tb, "binary_stderr": eb, "learned": tl, "ratio": tl / tb}}
 
 
 def run_e2e(w, args, rank, local, barrier, allmax, allsum):
@@ -447,6 +508,7 @@ def main():
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-collisions", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

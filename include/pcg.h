@@ -189,6 +189,13 @@ int pcg_export_species(pcg_handle* h, int slot, size_t cap, double* r, double* z
  * (specieP.cpp:79-478) as the source of synthetic initial conditions. */
 int pcg_seed_plasma(pcg_handle* h, int slot, size_t n, double density, double temperature_ev,
                     uint64_t seed);
+/* The same with `per_cell` macroparticles in every cell (nr*nz*per_cell
+ * in all), uniform in the cell's ring volume, weights density*V_cell/
+ * per_cell (the reference's equal-count cell filling, specieP.cpp:127-189),
+ * and a bi-Maxwellian: temperature t_par_ev along z, t_perp_ev along r and
+ * phi. */
+int pcg_seed_plasma_cells(pcg_handle* h, int slot, unsigned per_cell, double density, double t_par_ev,
+                          double t_perp_ev, uint64_t seed);
 
 /* Longitudinal bunch profile of a beam.  PCG_PROFILE_RECTANGLE is BeamP
  * (beamP.cpp:71-157).  PCG_PROFILE_GAUSSIAN injects a bunch of density

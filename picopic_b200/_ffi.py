@@ -71,6 +71,7 @@ SIGNATURES = {
     "pcg_diag": (ctypes.c_int, [_H, ctypes.POINTER(Diagnostics)]),
     "pcg_get_stream": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "pcg_seed_plasma": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_size_t, _D, _D, ctypes.c_uint64]),
+    "pcg_seed_plasma_cells": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_uint, _D, _D, _D, ctypes.c_uint64]),
     "pcg_set_beam_profile": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _D, _D]),
     "pcg_enable_timers": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_kernel_times": (ctypes.c_int, [_H, _PD, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),

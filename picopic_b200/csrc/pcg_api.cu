@@ -1009,6 +1009,34 @@ int pcg_synchronize(pcg_handle* h) {
   return check_status(h);
 }
 
+int pcg_seed_plasma_cells(pcg_handle* h, int slot, unsigned per_cell, double density, double t_par_ev,
+                          double t_perp_ev, uint64_t seed) {
+  if (!h || slot < 0 || slot >= (int)h->sp.size() || per_cell == 0) return PCG_ERR_ARG;
+  if (!(density >= 0) || !(t_par_ev >= 0) || !(t_perp_ev >= 0))
+    return fail(h, PCG_ERR_ARG, "negative density or temperature");
+  Species& s = h->sp[slot];
+  const size_t n = (size_t)h->g.nr * h->g.nz * per_cell;
+  if (s.n + n > s.cap) return fail(h, PCG_ERR_CAPACITY, "species '" + s.name + "' capacity exceeded");
+  h->started = true;
+  PlasmaSeed p;
+  p.seed = seed;
+  p.stream = 0x706c6300u + (uint32_t)slot;
+  p.sigma_v = sqrt(t_par_ev * kElCharge / s.mass);
+  p.sigma_v_perp = sqrt(t_perp_ev * kElCharge / s.mass);
+  p.weight = 0.0;
+  p.per_cell = per_cell;
+  p.density = density;
+  if (is_f64(h)) launch_seed_f64(h->g, p, view64(h, s), s.n, n, h->stream);
+  else {
+    if (s.n == 0) { s.f32.next_id = 0; s.f32.sorted_n = 0; }
+    launch_seed_f32(h->g, p, s.f32, s.n, n, h->stream);
+    s.f32.next_id += (unsigned)n;
+  }
+  s.n += n;
+  CUDA_TRY(h, cudaGetLastError());
+  return PCG_OK;
+}
+
 int pcg_seed_plasma(pcg_handle* h, int slot, size_t n, double density, double temperature_ev,
                     uint64_t seed) {
   if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;

@@ -13,7 +13,7 @@ namespace {
 constexpr int kThreads = 256;
 
 struct Draw {
-  double r, z, v[3];
+  double r, z, v[3], w;
 };
 
 // Particle j of a plasma: two Philox blocks give r, z and two normals, a
@@ -26,10 +26,22 @@ __device__ __forceinline__ Draw draw(const GridGeom& g, const PlasmaSeed& p, siz
   philox_uniform2(p.seed, p.stream, ((uint64_t)hi << 32) | 2u, idx, n2);
   Draw d;
   const double r0 = 0.5 * g.dr, r1 = g.R - 0.5 * g.dr;
-  d.r = sqrt(r0 * r0 + u[0] * (r1 * r1 - r0 * r0));
-  d.z = 0.5 * g.dz + u[1] * (g.L - g.dz);
   const double two_pi = 6.283185307179586;
   const double a1 = sqrt(-2.0 * log(1.0 - n1[0])), a2 = sqrt(-2.0 * log(1.0 - n2[0]));
+  if (p.per_cell) {  // cell j / per_cell, uniform in its ring volume
+    const size_t c = j / p.per_cell;
+    const double ci = (double)(c / g.nz), ck = (double)(c % g.nz);
+    d.r = g.dr * sqrt(ci * ci + u[0] * (2.0 * ci + 1.0));
+    d.z = g.dz * (ck + u[1]);
+    d.w = p.density * 3.1415926535897932 * g.dz * g.dr * g.dr * (2.0 * ci + 1.0) / p.per_cell;
+    d.v[0] = p.sigma_v_perp * a1 * cos(two_pi * n1[1]);
+    d.v[1] = p.sigma_v_perp * a1 * sin(two_pi * n1[1]);
+    d.v[2] = p.sigma_v * a2 * cos(two_pi * n2[1]);
+    return d;
+  }
+  d.r = sqrt(r0 * r0 + u[0] * (r1 * r1 - r0 * r0));
+  d.z = 0.5 * g.dz + u[1] * (g.L - g.dz);
+  d.w = p.weight;
   d.v[0] = p.sigma_v * a1 * cos(two_pi * n1[1]);
   d.v[1] = p.sigma_v * a1 * sin(two_pi * n1[1]);
   d.v[2] = p.sigma_v * a2 * cos(two_pi * n2[1]);
@@ -46,7 +58,7 @@ __global__ void seed_f64_kernel(GridGeom g, PlasmaSeed p, SpeciesF64 sp, size_t 
   const size_t j = n0 + i;
   sp.r[j] = d.r; sp.z[j] = d.z;
   sp.vr[j] = d.v[0]; sp.vphi[j] = d.v[1]; sp.vz[j] = d.v[2];
-  sp.w[j] = p.weight;
+  sp.w[j] = d.w;
   sp.r_old[j] = 0; sp.z_old[j] = 0;
   if (sp.phi) { sp.phi[j] = 0; sp.phi_old[j] = 0; sp.sn[j] = 0; }
   if (sp.cell_r) { sp.cell_r[j] = (int)floor(d.r / g.dr); sp.cell_z[j] = (int)floor(d.z / g.dz); }
@@ -68,7 +80,7 @@ __global__ void seed_f32_kernel(GridGeom g, PlasmaSeed p, SpeciesF32Buffers b, s
   b.vr[j] = (float)d.v[0];
   b.vphi[j] = (float)d.v[1];
   b.vz[j] = (float)d.v[2];
-  b.w[j] = (float)p.weight;
+  b.w[j] = (float)d.w;
   b.id[j] = b.next_id + (unsigned)i;
 }
 

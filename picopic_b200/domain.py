@@ -128,6 +128,13 @@ class Domain:
         self._check(self.lib.pcg_seed_plasma(self.h, slot, int(n), float(density),
                                              float(temperature_ev), int(seed)), "pcg_seed_plasma")
 
+    def seed_plasma_cells(self, slot, per_cell, density, t_par_ev, t_perp_ev=None, seed=0):
+        """Fill a species on the device with per_cell particles in every cell,
+        bi-Maxwellian (t_par along z, t_perp along r and phi)."""
+        t_perp_ev = t_par_ev if t_perp_ev is None else t_perp_ev
+        self._check(self.lib.pcg_seed_plasma_cells(self.h, slot, int(per_cell), float(density), float(t_par_ev),
+                                                   float(t_perp_ev), int(seed)), "pcg_seed_plasma_cells")
+
     def set_beam_profile(self, slot, profile="gaussian", sigma_z=0.0, macro_per_cell=0.0):
         code = {"rectangle": 0, "gaussian": 1}[profile]
         self._check(self.lib.pcg_set_beam_profile(self.h, slot, code, float(sigma_z),
