@@ -309,6 +309,16 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
 int pcg_cell_moments(pcg_handle* h, double* moments);
 int pcg_cell_features(pcg_handle* h, float* features, double* scale);
 
+/* Collisions inside pcg_step: every step then opens with one pass of the
+ * chosen operator on the velocities the previous step left.  The reference
+ * collides between the push and the move (SMB.cpp:1289-1293); a caller
+ * that needs exactly that order drives the step with pcg_stage and calls
+ * pcg_collide or pcg_collide_learned after PCG_STAGE_PUSH. */
+#define PCG_COLLISIONS_NONE 0
+#define PCG_COLLISIONS_BINARY 1
+#define PCG_COLLISIONS_LEARNED 2
+int pcg_set_collisions(pcg_handle* h, int mode);
+
 /* Villasenor-Buneman current of one species, double precision, that
  * allocates no device memory.  No counterpart in the reference: it exists
  * for callers that may not call cudaMalloc (a host code that owns and

@@ -73,6 +73,7 @@ struct pcg_handle {
   CollWork coll;                  // scratch of the collision passes
   LearnedWork learned;            // the learned collision step: model and scratch
   uint32_t coll_pass = 0;         // collision passes so far (their Philox counter)
+  int collisions = PCG_COLLISIONS_NONE;  // collision operator of every pcg_step
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -441,9 +442,90 @@ int run_stage(pcg_handle* h, int stage) {
 }
 
 // One fused step (PiCoPiC.cpp:326-347).
+// The species as the collision passes see them, and the masses and charges
+// of the species named electrons and ions (collisions.cpp:28-48: the last
+// match wins).  False when either is missing.
+bool collision_species(pcg_handle* h, std::vector<CollSpecies>& v, CollParams& p) {
+  int el = -1, ion = -1;
+  v.assign(h->sp.size(), CollSpecies());
+  for (size_t t = 0; t < h->sp.size(); ++t) {
+    Species& s = h->sp[t];
+    if (s.name == "electrons" || s.name == "Electrons") el = (int)t;
+    if (s.name == "ions" || s.name == "Ions") ion = (int)t;
+    CollSpecies& c = v[t];
+    c.n = s.n;
+    c.is_ion = s.name == "ions" || s.name == "Ions";
+    if (is_f64(h)) {
+      c.r = s.r; c.z = s.z; c.vr64 = s.vr; c.vphi64 = s.vphi; c.vz64 = s.vz; c.w64 = s.w;
+    } else {
+      c.cell = s.f32.cell; c.id = s.f32.id;
+      c.vr32 = s.f32.vr; c.vphi32 = s.f32.vphi; c.vz32 = s.f32.vz; c.w32 = s.f32.w;
+    }
+  }
+  if (el < 0 || ion < 0) return false;
+  p.m_el = h->sp[el].mass; p.q_el = h->sp[el].charge;
+  p.m_ion = h->sp[ion].mass; p.q_ion = h->sp[ion].charge;
+  p.dt = h->cfg.dt;
+  p.fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
+  p.shuffle = 1;
+  p.seed = h->cfg.seed;
+  p.status = h->d_status;
+  return true;
+}
+
+LearnedPhys learned_phys(const CollParams& p) {
+  return LearnedPhys{p.m_el, p.q_el, p.m_ion, p.q_ion, p.dt};
+}
+
+// One binary collision pass (no status check).
+int run_collide(pcg_handle* h, unsigned long long* pair_calls) {
+  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  if (!collision_species(h, v, p))
+    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  p.pass = h->coll_pass++;
+  unsigned long long calls = 0;
+  if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
+    return fail(h, PCG_ERR_CUDA, "collision pass");
+  h->launches += 8;
+  if (pair_calls) *pair_calls = calls;
+  return PCG_OK;
+}
+
+// One learned collision step with the binary fallback (no status check).
+int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells) {
+  if (!h->learned.model) return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
+  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
+  CollParams p{};
+  std::vector<CollSpecies> v;
+  if (!collision_species(h, v, p))
+    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
+  unsigned long long counts[2] = {0, 0};
+  if (learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream) != 0)
+    return fail(h, PCG_ERR_CUDA, "learned collision step");
+  h->launches += 1 + 2 * v.size();
+  if (counts[1]) {  // the binary operator on the cells outside the training box
+    p.pass = h->coll_pass++;
+    p.only = h->learned.flag;
+    p.only_value = 2;
+    unsigned long long calls = 0;
+    if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
+      return fail(h, PCG_ERR_CUDA, "collision fallback");
+    h->launches += 8;
+  }
+  if (learned_cells) *learned_cells = counts[0];
+  if (fallback_cells) *fallback_cells = counts[1];
+  return PCG_OK;
+}
+
 int fused_step(pcg_handle* h) {
   int rc;
   const int fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
+  // collisions open the step (on the velocities the last step left)
+  if (h->collisions == PCG_COLLISIONS_BINARY && (rc = run_collide(h, nullptr)) != PCG_OK) return rc;
+  if (h->collisions == PCG_COLLISIONS_LEARNED && (rc = run_collide_learned(h, nullptr, nullptr)) != PCG_OK)
+    return rc;
   if ((rc = stage_inject(h)) != PCG_OK) return rc;
   uint64_t live = 0;
   for (Species& s : h->sp) live += s.n;
@@ -826,58 +908,12 @@ int pcg_divergence(pcg_handle* h, int which, double* out) {
   return PCG_OK;
 }
 
-namespace {
-// The species as the collision passes see them, and the masses and charges
-// of the species named electrons and ions (collisions.cpp:28-48: the last
-// match wins).  False when either is missing.
-bool collision_species(pcg_handle* h, std::vector<CollSpecies>& v, CollParams& p) {
-  int el = -1, ion = -1;
-  v.assign(h->sp.size(), CollSpecies());
-  for (size_t t = 0; t < h->sp.size(); ++t) {
-    Species& s = h->sp[t];
-    if (s.name == "electrons" || s.name == "Electrons") el = (int)t;
-    if (s.name == "ions" || s.name == "Ions") ion = (int)t;
-    CollSpecies& c = v[t];
-    c.n = s.n;
-    c.is_ion = s.name == "ions" || s.name == "Ions";
-    if (is_f64(h)) {
-      c.r = s.r; c.z = s.z; c.vr64 = s.vr; c.vphi64 = s.vphi; c.vz64 = s.vz; c.w64 = s.w;
-    } else {
-      c.cell = s.f32.cell; c.id = s.f32.id;
-      c.vr32 = s.f32.vr; c.vphi32 = s.f32.vphi; c.vz32 = s.f32.vz; c.w32 = s.f32.w;
-    }
-  }
-  if (el < 0 || ion < 0) return false;
-  p.m_el = h->sp[el].mass; p.q_el = h->sp[el].charge;
-  p.m_ion = h->sp[ion].mass; p.q_ion = h->sp[ion].charge;
-  p.dt = h->cfg.dt;
-  p.fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
-  p.shuffle = 1;
-  p.seed = h->cfg.seed;
-  p.status = h->d_status;
-  return true;
-}
-
-LearnedPhys learned_phys(const CollParams& p) {
-  return LearnedPhys{p.m_el, p.q_el, p.m_ion, p.q_ion, p.dt};
-}
-}  // namespace
 
 int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
   if (!h) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
-  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
-  CollParams p{};
-  std::vector<CollSpecies> v;
-  if (!collision_species(h, v, p))
-    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
-  p.pass = h->coll_pass++;
-  unsigned long long calls = 0;
-  if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
-    return fail(h, PCG_ERR_CUDA, "collision pass");
-  h->launches += 8;
-  if (pair_calls) *pair_calls = calls;
+  if ((rc = run_collide(h, pair_calls)) != PCG_OK) return rc;
   return check_status(h);
 }
 
@@ -915,28 +951,16 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (!h) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
-  if (!h->learned.model) return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
-  if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
-  CollParams p{};
-  std::vector<CollSpecies> v;
-  if (!collision_species(h, v, p))
-    return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
-  unsigned long long counts[2] = {0, 0};
-  if (learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream) != 0)
-    return fail(h, PCG_ERR_CUDA, "learned collision step");
-  h->launches += 1 + 2 * v.size();
-  if (counts[1]) {  // the binary operator on the cells outside the training box
-    p.pass = h->coll_pass++;
-    p.only = h->learned.flag;
-    p.only_value = 2;
-    unsigned long long calls = 0;
-    if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
-      return fail(h, PCG_ERR_CUDA, "collision fallback");
-    h->launches += 8;
-  }
-  if (learned_cells) *learned_cells = counts[0];
-  if (fallback_cells) *fallback_cells = counts[1];
+  if ((rc = run_collide_learned(h, learned_cells, fallback_cells)) != PCG_OK) return rc;
   return check_status(h);
+}
+
+int pcg_set_collisions(pcg_handle* h, int mode) {
+  if (!h || mode < PCG_COLLISIONS_NONE || mode > PCG_COLLISIONS_LEARNED) return PCG_ERR_ARG;
+  if (mode == PCG_COLLISIONS_LEARNED && !h->learned.model)
+    return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
+  h->collisions = mode;
+  return PCG_OK;
 }
 
 int pcg_cell_moments(pcg_handle* h, double* out) {

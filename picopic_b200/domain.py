@@ -207,6 +207,11 @@ class Domain:
         self._check(self.lib.pcg_set_collision_model(self.h, p.ctypes.data_as(pf), n.ctypes.data_as(pf)),
                     "pcg_set_collision_model")
 
+    def set_collisions(self, mode):
+        """Collisions inside step(): "none", "binary" or "learned" (one pass opens every step)."""
+        code = {"none": 0, "binary": 1, "learned": 2}[mode]
+        self._check(self.lib.pcg_set_collisions(self.h, code), "pcg_set_collisions")
+
     def collide_learned(self):
         """One learned collision step; returns (learned cells, binary fallback cells)."""
         a, b = ctypes.c_ulonglong(0), ctypes.c_ulonglong(0)

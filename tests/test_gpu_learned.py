@@ -126,3 +126,33 @@ def test_out_of_box_cells_take_the_binary_operator():
     d.set_collision_model(*L.load_model())
     learned, fallback = d.collide_learned()
     assert learned == 0 and fallback == cells
+
+
+@pytest.mark.parametrize("mode", ["binary", "learned"])
+def test_pcg_step_with_collisions(mode):
+    """pcg_step with collisions: the electron anisotropy of a bi-Maxwellian
+    plasma falls over the steps, several times more than the collisionless
+    run's drift."""
+    from picopic_b200 import Domain
+    from picopic_b200 import learned as L
+    g = _grid(32, 64, dt=1e-14)  # 0.42 of the Courant limit
+
+    def run(collisions):
+        d = Domain(g, precision="f32", quirks="fixed", seed=3)
+        d.add(L.ELECTRONS, capacity=g.nr * g.nz * 100)
+        d.add(L.IONS, capacity=g.nr * g.nz * 100)
+        d.seed_plasma_cells(0, 100, 1e22, 2.0, 1.0, seed=1)
+        d.seed_plasma_cells(1, 100, 1e22, 0.5, seed=2)
+        if collisions != "none":
+            d.set_collision_model(*L.load_model())
+            d.set_collisions(collisions)
+        m = d.cell_moments().sum(0)
+        a0 = m[7] / (0.5 * (m[5] + m[6])) - 1
+        d.step(30)
+        m = d.cell_moments().sum(0)
+        return a0, m[7] / (0.5 * (m[5] + m[6])) - 1
+
+    a0, a1 = run(mode)
+    b0, b1 = run("none")
+    assert a1 < a0 - 0.03
+    assert a0 - a1 > 3 * abs(b1 - b0)  # well beyond the collisionless drift of the PIC noise
