@@ -69,11 +69,11 @@ def scaled(w, nz=None, ppc=None):
 # ---------------------------------------------------------------------------
 # GPU arm
 
-def make_domain(w, precision, seed=1234, host_beam=False, device=0, beam_capacity=0):
+def make_domain(w, precision, seed=1234, host_beam=False, device=0, beam_capacity=0, quirks="reference"):
     from picopic_b200 import Domain, Geometry
     g = Geometry(w["nr"], w["nz"], w["nr"] * w["dr"], w["nz"] * w["dz"], dt_courant(w["dr"]))
     d = Domain(g, pusher=w["pusher"], current=w["current"], precision=precision, seed=seed,
-               device=device)
+               device=device, quirks=quirks)
     n = w["nr"] * w["nz"] * w["ppc"]
     vb = beam_velocity(w["beam_energy_mev"])
     cells_b = (w["beam_radius"] / w["dr"]) * (6 * w["beam_sigma_z"] / w["dz"])
@@ -264,6 +264,9 @@ def run_gpu(args):
         torch.cuda.empty_cache()
     if not args.no_e2e:
         e2e = run_e2e(w, args, rank, local, barrier, allmax, allsum)
+    acc = None
+    if not args.no_accuracy and world == 1:
+        acc = run_accuracy(w, args, local)
     coll = None
     if not args.no_collisions:
         coll = run_collisions(args, local, barrier, allmax)
@@ -288,12 +291,44 @@ def run_gpu(args):
             "f64": f64,
             "e2e": e2e,
             "collisions": coll,
+            "accuracy": acc,
             "cpu_baseline": cpu,
             "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
         }
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def run_accuracy(w, args, local):
+    """The float path against the FP64 path on the wakefield workload from
+    the same seeded start (the same Philox plasma and bunch): relative field
+    energy difference after `n` steps, and the charge continuity residual
+    of one step, max |Q(n+1) - Q(n) + dt div J| over the nodes behind the
+    injection plane (k >= 2) relative to max |Q|, in both precisions.  Both
+    runs use PCG_QUIRKS_FIXED: the reference's strict-axial J_r overwrite
+    (currentVB.cpp:545-546), which the injected beam's purely axial motion
+    triggers, breaks charge conservation by design."""
+    import torch
+    n = 200 if args.small else 1000
+    out = {"steps": n}
+    energies = {}
+    for prec in ("f32", "f64"):
+        d, _, _, _ = make_domain(w, prec, seed=1234, device=local, quirks="fixed")
+        d.step(n)
+        dg = d.diag()
+        energies[prec] = (dg.field_energy_e, dg.field_energy_h, dg.kinetic_energy)
+        r = d.continuity_step()
+        q = np.abs(r[:, 2:]).max()
+        out[f"continuity_{prec}"] = float(q)
+        del d
+        torch.cuda.empty_cache()
+    e32, e64 = energies["f32"], energies["f64"]
+    out["field_energy_e_rel_diff"] = abs(e32[0] - e64[0]) / abs(e64[0])
+    out["field_energy_h_rel_diff"] = abs(e32[1] - e64[1]) / abs(e64[1])
+    out["kinetic_energy_rel_diff"] = abs(e32[2] - e64[2]) / abs(e64[2])
+    out["field_energy_f64_J"] = e64[0] + e64[1]
+    return out
 
 
 # Collisional anisotropy relaxation: 512 x 2048 cells of dr = dz = 1e-5 m
@@ -509,6 +544,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-collisions", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -711,10 +711,57 @@ static inline double ssd_strict(double q, double r, double dr, double dz, double
   return q / (K_PI * 4. * r * dz * dz * dr * dt); /* SOME_SHIT_DENSITY_STRICT */
 }
 
+static inline double log1p_ratio(double e) { return e == 0.0 ? 1.0 : log1p(e) / e; }
+
+/* The fixed mode's form of simple_current_distribution: the same integrals
+ * with k dz = dr and k log((r_o + dr) / r_o) = -(dz / r_o) log1p(e) / e
+ * substituted (e = dr / r_o), so that no term divides by dr or dz; the
+ * reference's form loses a nearly axial or nearly radial segment's digits
+ * and drops every segment with |dr| or |dz| below MNZL (:45-46).  On the
+ * axis row the factor 4 r0^2 - dr^2 is exactly 0 and its 1/r_o terms are
+ * left out. */
+static void vb_simple_fixed(orc_sim* s, double rn, double zn, double ro, double zo, int i_n,
+                            int k_n, double q) {
+  double *Jr = s->J[0], *Jz = s->J[2];
+  double dr = s->dr, dz = s->dz, dt = s->dt, sd, wj, b;
+  double delta_r = rn - ro, delta_z = zn - zo;
+  if (delta_r == 0.0 && delta_z == 0.0) return;
+  double lr = i_n >= 1 ? log1p_ratio(delta_r / ro) : 0.0;
+  if (i_n >= 1) {
+    double t = dr * dr * ((i_n + 0.5) * (i_n + 0.5) - 0.25) * (delta_z / ro) * lr;
+    sd = ssd_r(q, i_n * dr, dr, dz, dt);
+    Jz[IDX(s, i_n, k_n)] += sd * (dr * delta_z - delta_r * delta_z / 2. - delta_z * ro + t);
+    sd = ssd_r(q, (i_n + 1) * dr, dr, dz, dt);
+    Jz[IDX(s, i_n + 1, k_n)] += sd * (delta_r * delta_z / 2. + delta_z * ro + delta_z * dr - t);
+  } else {
+    sd = q / (2. * K_PI * dr / 4. * dr * dz * dt * dr);
+    Jz[IDX(s, i_n, k_n)] += sd * (dr * delta_z - delta_r * delta_z / 2. - delta_z * ro);
+    sd = ssd_r(q, dr, dr, dz, dt);
+    Jz[IDX(s, i_n + 1, k_n)] += sd * (delta_r * delta_z / 2. + delta_z * dr + delta_z * ro);
+  }
+  double r0 = (i_n + 0.5) * dr, r1 = ro;
+  double p8 = 4 * r0 * r0 - dr * dr;
+  sd = ssd_z(q, r0, dr, dz, dt);
+  b = (k_n + 1.) * dz - zo;
+  wj = -r0 * delta_z - delta_z / 2. * (ro + delta_r / 2.) + 0.5 * (delta_r * b + delta_z * (2 * r0 + r1));
+  if (p8 != 0.0)
+    wj += (delta_r * b + delta_z * r1) * p8 / (8 * ro * (ro + delta_r)) - delta_z / ro * (p8 / 8.) * lr;
+  Jr[IDX(s, i_n, k_n)] += sd * wj;
+  b = zo - k_n * dz;
+  wj = r0 * delta_z + delta_z / 2. * (ro + delta_r / 2.) + 0.5 * (delta_r * b - delta_z * (2 * r0 + r1));
+  if (p8 != 0.0)
+    wj += (delta_r * b - delta_z * r1) * p8 / (8 * ro * (ro + delta_r)) + delta_z / ro * (p8 / 8.) * lr;
+  Jr[IDX(s, i_n, k_n + 1)] += sd * wj;
+}
+
 /* simple_current_distribution :22-173 — a segment inside cell (i_n, k_n). */
 static void vb_simple(orc_sim* s, double rn, double zn, double ro, double zo, int i_n, int k_n,
                       double q) {
   double *Jr = s->J[0], *Jz = s->J[2];
+  if (s->quirks == ORC_QUIRKS_FIXED) {
+    vb_simple_fixed(s, rn, zn, ro, zo, i_n, k_n, q);
+    return;
+  }
   double dr = s->dr, dz = s->dz, dt = s->dt, wj, k, b, r0, r1, sd;
   double delta_r = rn - ro, delta_z = zn - zo;
   if ((fabs(delta_r) < K_MNZL) || (fabs(delta_z) < K_MNZL)) return;

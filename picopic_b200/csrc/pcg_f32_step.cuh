@@ -355,11 +355,13 @@ struct GlobalDep {
 // to that cell and the displacement (dx, dy).  Displacements are carried
 // exactly (from the velocity, split by path fractions), never differenced
 // from rounded offsets, so the MNZL test below means what it means in the
-// reference's double arithmetic.
+// reference's double arithmetic.  The terms below have no 1/dx or 1/dy
+// (g_terms carries the logarithm as a series near 0), so the fixed mode
+// deposits the segments the reference drops.
 template <class D>
 __device__ __forceinline__ void vb_simple(const StepArgs& a, const D& d, float q, int i, int k,
                                           float ao, float bo, float dx, float dy) {
-  if (fabsf(dx) < a.mnzl_r || fabsf(dy) < a.mnzl_z) return;  // currentVB.cpp:45-46
+  if (!a.fixed && (fabsf(dx) < a.mnzl_r || fabsf(dy) < a.mnzl_z)) return;  // currentVB.cpp:45-46
   const float fi = (float)i;
   const float xo = fi + ao, xn = xo + dx;
   const float ixo = 1.f / xo, ixn = 1.f / xn;

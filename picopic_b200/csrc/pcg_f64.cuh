@@ -433,9 +433,63 @@ __device__ __forceinline__ double ssd_strict(double q, double r, double dr, doub
   return q / (kPi * 4. * r * dz * dz * dr * dt);
 }
 
+// log1p(e) / e, 1 at e = 0.
+__device__ __forceinline__ double log1p_ratio(double e) { return e == 0.0 ? 1.0 : log1p(e) / e; }
+
+// The fixed mode's form of simple_current_distribution: the same integrals
+// with k dz = dr and k log((r_o + dr) / r_o) = -(dz / r_o) log1p(e) / e
+// substituted (e = dr / r_o), so that no term divides by dr or dz.  The
+// reference's form loses a nearly axial or nearly radial segment's digits
+// in 1/k and k, and drops every segment with |dr| or |dz| below 1e-15 m
+// (:45-46) -- its whole J_z with it when a nearly axial particle crosses a
+// cell face.  On the axis row (i_n = 0) the factor 4 r0^2 - dr^2 is
+// exactly 0 and its 1/r_o terms are left out.
+__device__ inline void vb_simple_fixed(const Sink& s, double rn, double zn, double ro, double zo, int i_n,
+                                       int k_n, double q) {
+  const GridGeom& g = *s.g;
+  const double dr = g.dr, dz = g.dz, dt = g.dt;
+  const double delta_r = rn - ro, delta_z = zn - zo;
+  if (delta_r == 0.0 && delta_z == 0.0) return;
+  const double lr = i_n >= 1 ? log1p_ratio(delta_r / ro) : 0.0;
+  double sd, wj;
+  if (i_n >= 1) {
+    const double t = dr * dr * ((i_n + 0.5) * (i_n + 0.5) - 0.25) * (delta_z / ro) * lr;
+    sd = ssd_r(q, i_n * dr, dr, dz, dt);
+    wj = sd * (dr * delta_z - delta_r * delta_z / 2. - delta_z * ro + t);
+    s.add_z(i_n, k_n, wj);
+    sd = ssd_r(q, (i_n + 1) * dr, dr, dz, dt);
+    wj = sd * (delta_r * delta_z / 2. + delta_z * ro + delta_z * dr - t);
+    s.add_z(i_n + 1, k_n, wj);
+  } else {
+    sd = q / (2. * kPi * dr / 4. * dr * dz * dt * dr);
+    wj = sd * (dr * delta_z - delta_r * delta_z / 2. - delta_z * ro);
+    s.add_z(i_n, k_n, wj);
+    sd = ssd_r(q, dr, dr, dz, dt);
+    wj = sd * (delta_r * delta_z / 2. + delta_z * dr + delta_z * ro);
+    s.add_z(i_n + 1, k_n, wj);
+  }
+  const double r0 = (i_n + 0.5) * dr, r1 = ro;
+  const double p8 = 4 * r0 * r0 - dr * dr;  // 8 (r0^2 / 2 - dr^2 / 8)
+  sd = ssd_z(q, r0, dr, dz, dt);
+  double b = (k_n + 1.) * dz - zo;
+  wj = -r0 * delta_z - delta_z / 2. * (ro + delta_r / 2.) + 0.5 * (delta_r * b + delta_z * (2 * r0 + r1));
+  if (p8 != 0.0)
+    wj += (delta_r * b + delta_z * r1) * p8 / (8 * ro * (ro + delta_r)) - delta_z / ro * (p8 / 8.) * lr;
+  s.add_r(i_n, k_n, sd * wj);
+  b = zo - k_n * dz;
+  wj = r0 * delta_z + delta_z / 2. * (ro + delta_r / 2.) + 0.5 * (delta_r * b - delta_z * (2 * r0 + r1));
+  if (p8 != 0.0)
+    wj += (delta_r * b - delta_z * r1) * p8 / (8 * ro * (ro + delta_r)) + delta_z / ro * (p8 / 8.) * lr;
+  s.add_r(i_n, k_n + 1, sd * wj);
+}
+
 // simple_current_distribution :22-173
-__device__ inline void vb_simple(const Sink& s, double rn, double zn, double ro, double zo, int i_n,
-                          int k_n, double q) {
+__device__ inline void vb_simple(const Sink& s, bool fixed, double rn, double zn, double ro, double zo,
+                                 int i_n, int k_n, double q) {
+  if (fixed) {
+    vb_simple_fixed(s, rn, zn, ro, zo, i_n, k_n, q);
+    return;
+  }
   const GridGeom& g = *s.g;
   const double dr = g.dr, dz = g.dz, dt = g.dt;
   double wj, k, b, r0, r1, sd;
@@ -645,7 +699,7 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
     return true;
   }
   if (res_cell == 0) {
-    vb_simple(s, R, Z, RO, ZO, i_n, k_n, q);
+    vb_simple(s, fixed, R, Z, RO, ZO, i_n, k_n, q);
   } else if (res_cell == 1) {
     if ((i_n != i_o) && (k_n == k_o)) {
       if (RO > (i_n + 1) * dr) {
@@ -653,15 +707,15 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
         const double r_b = (i_n + 1) * dr;
         const double delta_r = r_b - R;
         const double z_b = Z + delta_r / a;
-        vb_simple(s, r_b, z_b, RO, ZO, i_n + 1, k_n, q);
-        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+        vb_simple(s, fixed, r_b, z_b, RO, ZO, i_n + 1, k_n, q);
+        vb_simple(s, fixed, R, Z, r_b, z_b, i_n, k_n, q);
       } else {
         const double a = (R - RO) / (Z - ZO);
         const double r_b = (i_n) * dr;
         const double delta_r = r_b - RO;
         const double z_b = ZO + delta_r / a;
-        vb_simple(s, r_b, z_b, RO, ZO, i_n - 1, k_n, q);
-        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+        vb_simple(s, fixed, r_b, z_b, RO, ZO, i_n - 1, k_n, q);
+        vb_simple(s, fixed, R, Z, r_b, z_b, i_n, k_n, q);
       }
     } else if ((i_n == i_o) && (k_n != k_o)) {
       if (ZO < k_n * dz) {
@@ -669,15 +723,15 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
         const double delta_z = z_b - ZO;
         const double a = (R - RO) / (Z - ZO);
         const double r_b = RO + a * delta_z;
-        vb_simple(s, r_b, z_b, RO, ZO, i_n, k_n - 1, q);
-        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+        vb_simple(s, fixed, r_b, z_b, RO, ZO, i_n, k_n - 1, q);
+        vb_simple(s, fixed, R, Z, r_b, z_b, i_n, k_n, q);
       } else {
         const double z_b = (k_n + 1) * dz;
         const double delta_z = z_b - Z;
         const double a = (RO - R) / (ZO - Z);
         const double r_b = R + a * delta_z;
-        vb_simple(s, r_b, z_b, RO, ZO, i_n, k_n + 1, q);
-        vb_simple(s, R, Z, r_b, z_b, i_n, k_n, q);
+        vb_simple(s, fixed, r_b, z_b, RO, ZO, i_n, k_n + 1, q);
+        vb_simple(s, fixed, R, Z, r_b, z_b, i_n, k_n, q);
       }
     }
   } else if (res_cell == 2) {
@@ -691,13 +745,13 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
         const double delta_r2 = (z2 - ZO) * a;
         const double r2 = RO + delta_r2;
         if (z1 < k_n * dz) {
-          vb_simple(s, r1, z1, RO, ZO, i_n - 1, k_n - 1, q);
-          vb_simple(s, r2, z2, r1, z1, i_n, k_n - 1, q);
-          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+          vb_simple(s, fixed, r1, z1, RO, ZO, i_n - 1, k_n - 1, q);
+          vb_simple(s, fixed, r2, z2, r1, z1, i_n, k_n - 1, q);
+          vb_simple(s, fixed, R, Z, r2, z2, i_n, k_n, q);
         } else if (z1 > k_n * dz) {
-          vb_simple(s, r2, z2, RO, ZO, i_n - 1, k_n - 1, q);
-          vb_simple(s, r1, z1, r2, z2, i_n - 1, k_n, q);
-          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+          vb_simple(s, fixed, r2, z2, RO, ZO, i_n - 1, k_n - 1, q);
+          vb_simple(s, fixed, r1, z1, r2, z2, i_n - 1, k_n, q);
+          vb_simple(s, fixed, R, Z, r1, z1, i_n, k_n, q);
         }
       } else {
         const double a = (R - RO) / (Z - ZO);
@@ -708,13 +762,13 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
         const double delta_r2 = -(ZO - z2) * a;
         const double r2 = RO + delta_r2;
         if (z1 > (k_n + 1) * dz) {
-          vb_simple(s, r1, z1, RO, ZO, i_n - 1, k_n + 1, q);
-          vb_simple(s, r2, z2, r1, z1, i_n, k_n + 1, q);
-          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+          vb_simple(s, fixed, r1, z1, RO, ZO, i_n - 1, k_n + 1, q);
+          vb_simple(s, fixed, r2, z2, r1, z1, i_n, k_n + 1, q);
+          vb_simple(s, fixed, R, Z, r2, z2, i_n, k_n, q);
         } else if (z1 < (k_n + 1) * dz) {
-          vb_simple(s, r2, z2, RO, ZO, i_n - 1, k_n + 1, q);
-          vb_simple(s, r1, z1, r2, z2, i_n - 1, k_n, q);
-          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+          vb_simple(s, fixed, r2, z2, RO, ZO, i_n - 1, k_n + 1, q);
+          vb_simple(s, fixed, r1, z1, r2, z2, i_n - 1, k_n, q);
+          vb_simple(s, fixed, R, Z, r1, z1, i_n, k_n, q);
         }
       }
     } else if (i_o > i_n) {
@@ -727,13 +781,13 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
         const double delta_r2 = -(z2 - ZO) * a;
         const double r2 = RO - delta_r2;
         if (z1 < (k_n) * dz) {
-          vb_simple(s, r1, z1, RO, ZO, i_n + 1, k_n - 1, q);
-          vb_simple(s, r2, z2, r1, z1, i_n, k_n - 1, q);
-          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+          vb_simple(s, fixed, r1, z1, RO, ZO, i_n + 1, k_n - 1, q);
+          vb_simple(s, fixed, r2, z2, r1, z1, i_n, k_n - 1, q);
+          vb_simple(s, fixed, R, Z, r2, z2, i_n, k_n, q);
         } else if (z1 > (k_n) * dz) {
-          vb_simple(s, r2, z2, RO, ZO, i_n + 1, k_n - 1, q);
-          vb_simple(s, r1, z1, r2, z2, i_n + 1, k_n, q);
-          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+          vb_simple(s, fixed, r2, z2, RO, ZO, i_n + 1, k_n - 1, q);
+          vb_simple(s, fixed, r1, z1, r2, z2, i_n + 1, k_n, q);
+          vb_simple(s, fixed, R, Z, r1, z1, i_n, k_n, q);
         }
       } else if (k_o > k_n) {
         const double a = (RO - R) / (ZO - Z);
@@ -744,13 +798,13 @@ __device__ inline bool vb_rz(const Sink& s, bool fixed, double q, double R, doub
         const double delta_r2 = (z2 - Z) * a;
         const double r2 = R + delta_r2;
         if (z1 > (k_n + 1) * dz) {
-          vb_simple(s, r1, z1, RO, ZO, i_n + 1, k_n + 1, q);
-          vb_simple(s, r2, z2, r1, z1, i_n, k_n + 1, q);
-          vb_simple(s, R, Z, r2, z2, i_n, k_n, q);
+          vb_simple(s, fixed, r1, z1, RO, ZO, i_n + 1, k_n + 1, q);
+          vb_simple(s, fixed, r2, z2, r1, z1, i_n, k_n + 1, q);
+          vb_simple(s, fixed, R, Z, r2, z2, i_n, k_n, q);
         } else if (z1 < (k_n + 1) * dz) {
-          vb_simple(s, r2, z2, RO, ZO, i_n + 1, k_n + 1, q);
-          vb_simple(s, r1, z1, r2, z2, i_n + 1, k_n, q);
-          vb_simple(s, R, Z, r1, z1, i_n, k_n, q);
+          vb_simple(s, fixed, r2, z2, RO, ZO, i_n + 1, k_n + 1, q);
+          vb_simple(s, fixed, r1, z1, r2, z2, i_n + 1, k_n, q);
+          vb_simple(s, fixed, R, Z, r1, z1, i_n, k_n, q);
         }
       }
     }

@@ -39,6 +39,22 @@ def particles(grid, n, seed, mass=1.0, boost=30.0):
     return (r, z, v[0], v[1], v[2], w)
 
 
+def near_axial(grid, n, seed, dt=None):
+    """Particles that cross a z cell face in one step while moving radially
+    by only 1.2e-15 to 5e-15 m, so that the part of the step behind the face
+    moves less than the reference's 1e-15 m segment threshold radially."""
+    rng = np.random.default_rng(seed)
+    dt = grid.dt if dt is None else dt
+    vz = 2.0e8
+    step = vz * dt / grid.dz
+    r = (1.5 + rng.random(n) * (grid.nr / 2)) * grid.dr
+    k = rng.integers(2, grid.nz - 4, size=n)
+    z = (k + 1.0 - step * (0.05 + 0.9 * rng.random(n))) * grid.dz
+    dr = (1.2e-15 + rng.random(n) * 3.8e-15) * rng.choice([-1.0, 1.0], size=n)
+    w = rng.random(n) * 1e6 + 1e5
+    return (r, z, dr / dt, np.zeros(n), np.full(n, vz), w)
+
+
 def random_fields(grid, seed, scale=1e3):
     rng = np.random.default_rng(seed + 7919)
     return {f: rng.normal(size=grid.shape) * scale for f in FIELDS}

@@ -12,7 +12,7 @@ against a numpy restatement on the same particles.
 import numpy as np
 import pytest
 
-from tests.cases import ELECTRONS, IONS, particles, small_grid
+from tests.cases import ELECTRONS, IONS, near_axial, particles, small_grid
 
 pytestmark = pytest.mark.gpu
 
@@ -65,6 +65,20 @@ def test_continuity_f64(quirks):
     for _ in range(3):
         r = d.continuity_step()
         assert np.abs(r).max() <= RTOL_CONT_F64
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_continuity_near_axial_face_crossing(precision):
+    """Radial steps of 1.2e-15 to 5e-15 m across a z face: the fixed mode's
+    segment integrals (and the float path's shares) keep continuity where
+    the reference's 1e-15 m segment threshold drops charge."""
+    from picopic_b200 import Domain
+    grid = small_grid(pml=False)
+    d = Domain(grid, pusher="borisrel", current="vb", precision=precision, quirks="fixed", seed=7)
+    d.add(ELECTRONS, capacity=4000)
+    d.set_particles(0, *near_axial(grid, 2000, 5))
+    r = d.continuity_step()
+    assert np.abs(r).max() <= (RTOL_CONT_F64 if precision == "f64" else RTOL_CONT_F32)
 
 
 def test_continuity_f32():
