@@ -305,10 +305,20 @@ static inline double term(double f, double dzz, double ra, double rb, double vol
   return f * K_PI * dzz * (rb * rb - ra * ra) / vol;
 }
 
+/* The fixed mode divides each ring term by the volume of the particle's
+ * cloud, pi dz (r3^2 - r1^2), so that the weights of a component sum to 1;
+ * the reference divides by cell volumes, which weights a uniform field by
+ * about 1 - 1/(2i) at row i (a density-deposit formula used to interpolate). */
+#define GATHER_VOLUMES(s, a, b)                                            \
+  do {                                                                     \
+    if ((s)->quirks == ORC_QUIRKS_FIXED) (a) = (b) = cloud;                \
+  } while (0)
+
 static void gather_h(const orc_sim* s, double radius, double longitude, double cmp[3]) {
   const double dr = s->dr, dz = s->dz;
   const double *Hr = s->H[0], *Hp = s->H[1], *Hz = s->H[2];
   double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr, r2, dz1, dz2, v1, v2;
+  const double cloud = K_PI * dz * (r3 * r3 - r1 * r1);
   int i, k;
   cmp[0] = cmp[1] = cmp[2] = 0;
   /* H_z :120-147 */
@@ -316,6 +326,7 @@ static void gather_h(const orc_sim* s, double radius, double longitude, double c
   k = CELL_NUMBER(longitude, dz);
   v1 = cell_volume_expr(2.0 * i + 1 + 1, dr, dz);
   v2 = cell_volume_expr(2.0 * i + 3 + 1, dr, dz);
+  GATHER_VOLUMES(s, v1, v2);
   dz1 = (k + 1) * dz - longitude;
   dz2 = longitude - k * dz;
   r2 = (i + 1) * dr;
@@ -328,6 +339,7 @@ static void gather_h(const orc_sim* s, double radius, double longitude, double c
   k = CELL_NUMBER(longitude - 0.5 * dz, dz);
   v1 = cell_volume_expr(2.0 * i + 1, dr, dz);
   v2 = cell_volume_expr(2.0 * i + 2 + 1, dr, dz);
+  GATHER_VOLUMES(s, v1, v2);
   r2 = (i + 0.5) * dr;
   dz1 = (k + 1.5) * dz - longitude;
   dz2 = longitude - (k + 0.5) * dz;
@@ -341,6 +353,7 @@ static void gather_h(const orc_sim* s, double radius, double longitude, double c
   r2 = (i + 1) * dr;
   v1 = cell_volume_expr(2.0 * i + 1 + 1, dr, dz);
   v2 = cell_volume_expr(2.0 * i + 3 + 1, dr, dz);
+  GATHER_VOLUMES(s, v1, v2);
   dz1 = (k + 1.5) * dz - longitude;
   dz2 = longitude - (k + 0.5) * dz;
   cmp[1] += term(Hp[IDX(s, i, k)], dz1, r1, r2, v1);
@@ -353,6 +366,7 @@ static void gather_e(const orc_sim* s, double radius, double longitude, double c
   const double dr = s->dr, dz = s->dz;
   const double *Er = s->E[0], *Ep = s->E[1], *Ez = s->E[2];
   double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr, r2, dz1, dz2, v1, v2;
+  const double cloud = K_PI * dz * (r3 * r3 - r1 * r1);
   int i, k;
   cmp[0] = cmp[1] = cmp[2] = 0;
   /* E_r :231-257 */
@@ -360,6 +374,7 @@ static void gather_e(const orc_sim* s, double radius, double longitude, double c
   k = CELL_NUMBER(longitude, dz);
   v1 = cell_volume_expr(2.0 * i + 1 + 1, dr, dz);
   v2 = cell_volume_expr(2.0 * i + 3 + 1, dr, dz);
+  GATHER_VOLUMES(s, v1, v2);
   dz1 = (k + 1) * dz - longitude;
   dz2 = longitude - k * dz;
   r2 = (i + 1) * dr;
@@ -372,6 +387,7 @@ static void gather_e(const orc_sim* s, double radius, double longitude, double c
   k = CELL_NUMBER(longitude - 0.5 * dz, dz);
   v1 = cell_volume_expr(2.0 * i + 1, dr, dz);
   v2 = cell_volume_expr(2.0 * i + 2 + 1, dr, dz);
+  GATHER_VOLUMES(s, v1, v2);
   r2 = (i + 0.5) * dr;
   dz1 = (k + 1.5) * dz - longitude;
   dz2 = longitude - (k + 0.5) * dz;
@@ -384,6 +400,7 @@ static void gather_e(const orc_sim* s, double radius, double longitude, double c
   k = CELL_NUMBER(longitude, dz);
   v1 = cell_volume_expr(2.0 * i + 1, dr, dz);
   v2 = cell_volume_expr(2.0 * i + 2 + 1, dr, dz);
+  GATHER_VOLUMES(s, v1, v2);
   r2 = (i + 0.5) * dr;
   dz1 = (k + 1) * dz - longitude;
   dz2 = longitude - k * dz;

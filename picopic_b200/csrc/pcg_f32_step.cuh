@@ -120,11 +120,19 @@ __device__ __forceinline__ void gather(const StepArgs& a, const V& fv, int ci, f
                                        float fz, float e[3], float b[3]) {
   const Stagger rh = half_shift(ci, fr), zh = half_shift(ck, fz);
   // ring-volume weights; the reciprocals of their denominators come from
-  // the table (row ci: 1/(2ci+1), 1/(2ci+3); row rh.i: 1/(2i+2), 1/(2i+4))
-  const float4 tn = fv.row(ci), th = fv.row(rh.i);
+  // the table (row ci: 1/(2ci+1), 1/(2ci+3); row rh.i: 1/(2i+2), 1/(2i+4)),
+  // or in the fixed mode all are 1/(2x), the particle's cloud volume, so
+  // that each component's weights sum to 1
   const float fi = (float)ci, fh = (float)rh.i, u = rh.u;
-  const float n0 = (1.f - fr) * (2.f * fi + fr) * tn.x, n1 = fr * (2.f * fi + 1.f + fr) * tn.z;
-  const float h0 = (1.f - u) * (2.f * fh + 1.f + u) * th.y, h1 = u * (2.f * fh + 2.f + u) * th.w;
+  float sn0, sn1, sh0, sh1;
+  if (a.fixed) {
+    sn0 = sn1 = sh0 = sh1 = 0.5f / (fi + fr);
+  } else {
+    const float4 tn = fv.row(ci), th = fv.row(rh.i);
+    sn0 = tn.x; sn1 = tn.z; sh0 = th.y; sh1 = th.w;
+  }
+  const float n0 = (1.f - fr) * (2.f * fi + fr) * sn0, n1 = fr * (2.f * fi + 1.f + fr) * sn1;
+  const float h0 = (1.f - u) * (2.f * fh + 1.f + u) * sh0, h1 = u * (2.f * fh + 2.f + u) * sh1;
   // E_r: (1/2, 0); E_z: (0, 1/2); E_phi: (0, 0)
   e[0] = interp4(fv, 0, rh.i, ck, h0, h1, fz);
   e[2] = interp4(fv, 2, ci, zh.i, n0, n1, zh.u);

@@ -49,11 +49,16 @@ __device__ __forceinline__ double pml_sigma(const Fields& f, int i, int k) {
 // ---------------------------------------------------------------------------
 // Gather: MaxwellSolver::get_field_h / get_field_e (maxwellSolver.hpp:101-316)
 
-__device__ __forceinline__ void gather_h(const GridGeom& g, const Fields& f, double radius,
+// The fixed mode divides each ring term by the volume of the particle's
+// cloud, pi dz (r3^2 - r1^2), so that a component's weights sum to 1; the
+// reference divides by cell volumes, which weights a uniform field by about
+// 1 - 1/(2i) at row i and lowers the plasma frequency by half that.
+__device__ __forceinline__ void gather_h(const GridGeom& g, const Fields& f, bool fixed, double radius,
                                          double longitude, double cmp[3]) {
   const double dr = g.dr, dz = g.dz;
   const double *Hr = f.H[0], *Hp = f.H[1], *Hz = f.H[2];
   const double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr;
+  const double cloud = kPi * dz * (r3 * r3 - r1 * r1);
   double r2, dz1, dz2, v1, v2;
   int i, k;
   cmp[0] = cmp[1] = cmp[2] = 0;
@@ -61,6 +66,7 @@ __device__ __forceinline__ void gather_h(const GridGeom& g, const Fields& f, dou
   k = cell_number(longitude, dz);
   v1 = cell_volume(2.0 * i + 1 + 1, dr, dz);
   v2 = cell_volume(2.0 * i + 3 + 1, dr, dz);
+  if (fixed) v1 = v2 = cloud;
   dz1 = (k + 1) * dz - longitude;
   dz2 = longitude - k * dz;
   r2 = (i + 1) * dr;
@@ -72,6 +78,7 @@ __device__ __forceinline__ void gather_h(const GridGeom& g, const Fields& f, dou
   k = cell_number(longitude - 0.5 * dz, dz);
   v1 = cell_volume(2.0 * i + 1, dr, dz);
   v2 = cell_volume(2.0 * i + 2 + 1, dr, dz);
+  if (fixed) v1 = v2 = cloud;
   r2 = (i + 0.5) * dr;
   dz1 = (k + 1.5) * dz - longitude;
   dz2 = longitude - (k + 0.5) * dz;
@@ -84,6 +91,7 @@ __device__ __forceinline__ void gather_h(const GridGeom& g, const Fields& f, dou
   r2 = (i + 1) * dr;
   v1 = cell_volume(2.0 * i + 1 + 1, dr, dz);
   v2 = cell_volume(2.0 * i + 3 + 1, dr, dz);
+  if (fixed) v1 = v2 = cloud;
   dz1 = (k + 1.5) * dz - longitude;
   dz2 = longitude - (k + 0.5) * dz;
   cmp[1] += ring_term(Hp[gidx(g, i, k)], dz1, r1, r2, v1);
@@ -97,6 +105,7 @@ __device__ __forceinline__ void gather_e(const GridGeom& g, const Fields& f, boo
   const double dr = g.dr, dz = g.dz;
   const double *Er = f.E[0], *Ep = f.E[1], *Ez = f.E[2];
   const double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr;
+  const double cloud = kPi * dz * (r3 * r3 - r1 * r1);
   double r2, dz1, dz2, v1, v2;
   int i, k;
   cmp[0] = cmp[1] = cmp[2] = 0;
@@ -104,6 +113,7 @@ __device__ __forceinline__ void gather_e(const GridGeom& g, const Fields& f, boo
   k = cell_number(longitude, dz);
   v1 = cell_volume(2.0 * i + 1 + 1, dr, dz);
   v2 = cell_volume(2.0 * i + 3 + 1, dr, dz);
+  if (fixed) v1 = v2 = cloud;
   dz1 = (k + 1) * dz - longitude;
   dz2 = longitude - k * dz;
   r2 = (i + 1) * dr;
@@ -115,6 +125,7 @@ __device__ __forceinline__ void gather_e(const GridGeom& g, const Fields& f, boo
   k = cell_number(longitude - 0.5 * dz, dz);
   v1 = cell_volume(2.0 * i + 1, dr, dz);
   v2 = cell_volume(2.0 * i + 2 + 1, dr, dz);
+  if (fixed) v1 = v2 = cloud;
   r2 = (i + 0.5) * dr;
   dz1 = (k + 1.5) * dz - longitude;
   dz2 = longitude - (k + 0.5) * dz;
@@ -126,6 +137,7 @@ __device__ __forceinline__ void gather_e(const GridGeom& g, const Fields& f, boo
   k = cell_number(longitude, dz);
   v1 = cell_volume(2.0 * i + 1, dr, dz);
   v2 = cell_volume(2.0 * i + 2 + 1, dr, dz);
+  if (fixed) v1 = v2 = cloud;
   r2 = (i + 0.5) * dr;
   dz1 = (k + 1) * dz - longitude;
   dz2 = longitude - k * dz;
@@ -305,7 +317,7 @@ __device__ __forceinline__ bool gather_push(const GridGeom& g, const Fields& f, 
   }
   double e[3], b[3];
   gather_e(g, f, fixed, r, z, e);
-  gather_h(g, f, r, z, b);
+  gather_h(g, f, fixed, r, z, b);
   if (pusher == 3) return push_vay(fixed, c2m, e, b, v, st);
   if (pusher == 4) return push_hc(fixed, c2m, e, b, v, st);
   return push_boris(pusher, c2m, e, b, v, st);

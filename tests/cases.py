@@ -55,6 +55,41 @@ def near_axial(grid, n, seed, dt=None):
     return (r, z, dr / dt, np.zeros(n), np.full(n, vz), w)
 
 
+def quiet_plasma(grid, density, per_cell=4, v0=0.0):
+    """Cold, exactly neutral plasma for the Langmuir test: a regular lattice of
+    per_cell x per_cell points per cell over the region between the
+    reflecting walls (r in [dr/2, R - dr/2], z in [dz/2, L - dz/2]), each
+    point's weight its ring volume times `density`.  Electrons and ions share
+    the lattice; the electrons get v_z = v0 sin(2 pi z / L).  Returns the
+    electron and ion arrays (r, z, vr, vphi, vz, w)."""
+    nr_p, nz_p = per_cell * (grid.nr - 1), per_cell * (grid.nz - 1)
+    hr, hz = (grid.radius - grid.dr) / nr_p, (grid.longitude - grid.dz) / nz_p
+    r1 = grid.dr / 2 + (np.arange(nr_p) + 0.5) * hr
+    z1 = grid.dz / 2 + (np.arange(nz_p) + 0.5) * hz
+    r, z = (a.ravel() for a in np.meshgrid(r1, z1, indexing="ij"))
+    w = density * 2 * np.pi * r * hr * hz
+    zero = np.zeros_like(r)
+    vz = v0 * np.sin(2 * np.pi * z / grid.longitude)
+    return (r, z, zero, zero, vz, w), (r.copy(), z.copy(), zero, zero, zero, w.copy())
+
+
+def dominant_frequency(x, dt, lo, hi):
+    """Angular frequency in [lo, hi] at which |sum (x - mean) e^{-i w t}| peaks
+    (a fine scan refined by a parabola through the peak)."""
+    x = np.asarray(x, dtype=float) - np.mean(x)
+    t = np.arange(len(x)) * dt
+    w = np.linspace(lo, hi, 4001)
+    p = np.abs(np.exp(-1j * np.outer(w, t)) @ x)
+    m = int(np.clip(np.argmax(p), 1, len(w) - 2))
+    a, b, c = p[m - 1], p[m], p[m + 1]
+    return w[m] + 0.5 * (a - c) / (a - 2 * b + c) * (w[1] - w[0])
+
+
+def plasma_frequency(density, mass=1.0):
+    """sqrt(n e^2 / (eps0 m)) with the reference's constants (constant.hpp)."""
+    return np.sqrt(density * 1.6e-19 ** 2 / (8.85e-12 * 9.1e-31 * mass))
+
+
 def random_fields(grid, seed, scale=1e3):
     rng = np.random.default_rng(seed + 7919)
     return {f: rng.normal(size=grid.shape) * scale for f in FIELDS}
