@@ -270,6 +270,9 @@ def run_gpu(args):
     coll = None
     if not args.no_collisions:
         coll = run_collisions(args, local, barrier, allmax)
+    large = None
+    if not args.no_large:
+        large = run_large(args, local, barrier, allmax, allsum)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w)
     if rank == 0:
@@ -291,6 +294,7 @@ def run_gpu(args):
             "f64": f64,
             "e2e": e2e,
             "collisions": coll,
+            "large": large,
             "accuracy": acc,
             "cpu_baseline": cpu,
             "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
@@ -328,6 +332,54 @@ def run_accuracy(w, args, local):
     out["field_energy_h_rel_diff"] = abs(e32[1] - e64[1]) / abs(e64[1])
     out["kinetic_energy_rel_diff"] = abs(e32[2] - e64[2]) / abs(e64[2])
     out["field_energy_f64_J"] = e64[0] + e64[1]
+    return out
+
+
+# The large configuration: 1024 x 16384 cells of 5e-5 m, n = 1e18 m^-3, 12
+# macroparticles per cell per species (4.0e8 plasma particles), a 20 MeV
+# Gaussian bunch (R = 1 mm, sigma_z = 0.5 mm; its density is not given for
+# this configuration, 1e17 m^-3 here), Vay pusher, ZigZag current.
+LARGE = dict(
+    name="large beam-plasma 1024x16384, 12 ppc/species e+p, 20 MeV Gaussian bunch, Vay + ZigZag",
+    nr=1024, nz=16384, dr=5e-5, dz=5e-5, density=1e18, ppc=12, te=1.0, ti=0.1,
+    beam_energy_mev=20.0, beam_density=1e17, beam_radius=1e-3, beam_sigma_z=5e-4,
+    beam_ppc=100, pusher="vay", current="zigzag")
+
+
+def run_large(args, local, barrier, allmax, allsum):
+    """The large configuration in the float path: particle-steps/s of the
+    collisionless step, then the step with the learned collision operator
+    (the wide model; binary fallback for cells outside its training box,
+    the bunch's among them) opening it."""
+    import torch
+    from picopic_b200 import learned as L
+    w = LARGE if not args.small else scaled(LARGE, nz=2048)
+    d, _, _, _ = make_domain(w, "f32", seed=4321, device=local)
+    d.step(3)
+    d.synchronize()
+    p0 = d.diag().particle_steps
+    k = 10 if args.small else 20
+    barrier()
+    ms = allmax(timed_steps(d, k, d.stream))
+    dg = d.diag()
+    out = {"workload": w["name"], "grid": [w["nr"], w["nz"]], "particles": int(dg.particles),
+           "pusher": w["pusher"], "current": w["current"], "precision": "f32",
+           "value": allsum(float(dg.particle_steps - p0)) / (ms * 1e-3), "unit": UNIT,
+           "ms_per_step": ms / k, "steps": k}
+    d.set_collision_model(*L.load_model(L.WIDE_MODEL_PATH))  # 12 ppc, n 1e18: the wide model's states
+    learned, fallback = d.collide_learned()
+    d.set_collisions("learned")
+    d.step(1)
+    d.synchronize()
+    kc = 3
+    barrier()
+    ms_c = allmax(timed_steps(d, kc, d.stream))
+    cells = w["nr"] * w["nz"]
+    out["with_learned_collisions"] = {"ms_per_step": ms_c / kc, "steps": kc,
+                                      "learned_cell_fraction": learned / cells,
+                                      "fallback_cell_fraction": fallback / cells}
+    del d
+    torch.cuda.empty_cache()
     return out
 
 
@@ -545,6 +597,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-collisions", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -488,7 +488,7 @@ int run_collide(pcg_handle* h, unsigned long long* pair_calls) {
   unsigned long long calls = 0;
   if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
     return fail(h, PCG_ERR_CUDA, "collision pass");
-  h->launches += 8;
+  h->launches += h->coll.launches;
   if (pair_calls) *pair_calls = calls;
   return PCG_OK;
 }
@@ -512,7 +512,7 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
     unsigned long long calls = 0;
     if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
       return fail(h, PCG_ERR_CUDA, "collision fallback");
-    h->launches += 8;
+    h->launches += h->coll.launches;
   }
   if (learned_cells) *learned_cells = counts[0];
   if (fallback_cells) *fallback_cells = counts[1];

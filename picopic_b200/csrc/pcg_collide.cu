@@ -11,6 +11,10 @@
 //     (species order, then particle order) and an exclusive scan the starts;
 //  3. optionally a Fisher-Yates shuffle of every cell list (Philox draws
 //     (cell, i) of this pass);
+//  3b. the lists' velocities and weights are copied, in list order, into
+//     contiguous FP64 staging (the particle arrays are in the step's tile
+//     order, so a cell's particles lie far apart); steps 4-5 read and write
+//     the copy and a last kernel writes the velocities back;
 //  4. per cell: weight, energy and density sums in list order (the
 //     reference's collect pass), the temperatures and the row stop of the
 //     reference's `break` on a non-normal value (:351-354);
@@ -49,7 +53,11 @@ inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kT
 struct SpeciesTable {
   CollSpecies s[kCollMaxSpecies];
   int n;
+  double4* stage[2];  // the staged lists (entries referenced as kStaged | list << 40 | position)
 };
+
+constexpr unsigned long long kStaged = 1ull << 63;
+constexpr unsigned long long kRefMask = (1ull << 40) - 1;
 
 // std::isnormal: neither zero, subnormal, infinite nor NaN
 __device__ __forceinline__ bool normal(double x) {
@@ -125,6 +133,12 @@ __global__ void shuffle_kernel(size_t cells, const unsigned* start, const unsign
 
 __device__ __forceinline__ void load_v(const SpeciesTable& tab, unsigned long long ref, double v[3],
                                        double* w) {
+  if (ref & kStaged) {
+    const double4 e = tab.stage[(ref >> 40) & 1][ref & kRefMask];
+    v[0] = e.x; v[1] = e.y; v[2] = e.z;
+    *w = e.w;
+    return;
+  }
   const CollSpecies& sp = tab.s[ref >> 40];
   const size_t j = ref & ((1ull << 40) - 1);
   if (sp.vr64) {
@@ -136,13 +150,24 @@ __device__ __forceinline__ void load_v(const SpeciesTable& tab, unsigned long lo
   }
 }
 
+// 0 for the electron list, 1 for the ion list
+__device__ __forceinline__ int list_of(const SpeciesTable& tab, unsigned long long ref) {
+  return (ref & kStaged) ? (int)((ref >> 40) & 1) : tab.s[ref >> 40].is_ion;
+}
+
 __device__ __forceinline__ double load_w(const SpeciesTable& tab, unsigned long long ref) {
+  if (ref & kStaged) return tab.stage[(ref >> 40) & 1][ref & kRefMask].w;
   const CollSpecies& sp = tab.s[ref >> 40];
   const size_t j = ref & ((1ull << 40) - 1);
   return sp.w64 ? sp.w64[j] : (double)sp.w32[j];
 }
 
 __device__ __forceinline__ void store_v(const SpeciesTable& tab, unsigned long long ref, const double v[3]) {
+  if (ref & kStaged) {
+    double4* e = tab.stage[(ref >> 40) & 1] + (ref & kRefMask);
+    e->x = v[0]; e->y = v[1]; e->z = v[2];
+    return;
+  }
   const CollSpecies& sp = tab.s[ref >> 40];
   const size_t j = ref & ((1ull << 40) - 1);
   if (sp.vr64) {
@@ -150,6 +175,29 @@ __device__ __forceinline__ void store_v(const SpeciesTable& tab, unsigned long l
   } else {
     sp.vr32[j] = (float)v[0]; sp.vphi32[j] = (float)v[1]; sp.vz32[j] = (float)v[2];
   }
+}
+
+// 3b. staging: entry q of list `list` is copied to stage[q] and referenced
+// by staged[q]; the write-back stores the (possibly scattered) velocities
+// through the original reference.  A float velocity that no collision
+// touched returns unchanged, (float)(double)x == x.
+__global__ void stage_kernel(SpeciesTable tab, const unsigned long long* refs, unsigned n, int list,
+                             double4* stage, unsigned long long* staged) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  double v[3], w;
+  load_v(tab, refs[q], v, &w);
+  stage[q] = make_double4(v[0], v[1], v[2], w);
+  staged[q] = kStaged | ((unsigned long long)list << 40) | q;
+}
+
+__global__ void unstage_kernel(SpeciesTable tab, const unsigned long long* refs, unsigned n,
+                               const double4* stage) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const double4 e = stage[q];
+  const double v[3] = {e.x, e.y, e.z};
+  store_v(tab, refs[q], v);
 }
 
 // ---------------------------------------------------------------------------
@@ -360,7 +408,7 @@ __device__ void p12_single(PairCtx& x, double m_real_a, double m_real_b, double 
     double ec, ec2;
     angle_moments(s12, &ec, &ec2);
     const double pb_prob = fixed ? w_a / w_b : 1.0;
-    const int la = x.tab->s[(swap ? rb : ra) >> 40].is_ion, lb = x.tab->s[(swap ? ra : rb) >> 40].is_ion;
+    const int la = list_of(*x.tab, swap ? rb : ra), lb = list_of(*x.tab, swap ? ra : rb);
     expect_add(x.expect + 6 * la, v_cm, p_a_cm, 1.0, mass_a, w_a, 1.0, ec, ec2);
     expect_add(x.expect + 6 * lb, v_cm, p_a_cm, -1.0, mass_b, w_b, pb_prob, ec, ec2);
   }
@@ -536,7 +584,7 @@ int grow(T** p, size_t n) {
 void collide_free(CollWork& w) {
   for (int l = 0; l < 2; ++l) {
     cudaFree(w.keys[l]); cudaFree(w.keys2[l]); cudaFree(w.vals[l]); cudaFree(w.vals2[l]);
-    cudaFree(w.count[l]); cudaFree(w.start[l]);
+    cudaFree(w.count[l]); cudaFree(w.start[l]); cudaFree(w.stage[l]);
   }
   cudaFree(w.moments); cudaFree(w.row_stop); cudaFree(w.calls); cudaFree(w.valid); cudaFree(w.tmp);
   w = CollWork();
@@ -557,7 +605,8 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   if (w.cap < need || w.cells != cells) {
     for (int l = 0; l < 2; ++l) {
       if (grow(&w.keys[l], need) || grow(&w.keys2[l], need) || grow(&w.vals[l], need) ||
-          grow(&w.vals2[l], need) || grow(&w.count[l], cells + 1) || grow(&w.start[l], cells + 1))
+          grow(&w.vals2[l], need) || grow(&w.count[l], cells + 1) || grow(&w.start[l], cells + 1) ||
+          grow(&w.stage[l], need))
         return -1;
     }
     if (grow(&w.moments, 4 * cells) || grow(&w.row_stop, (size_t)g.nr) || grow(&w.calls, 1) ||
@@ -573,12 +622,14 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   }
   cudaMemsetAsync(w.calls, 0, sizeof(unsigned long long), s);
   cudaMemsetAsync(w.valid, 0, 2 * sizeof(unsigned), s);
+  w.launches = 2;  // moments and the pairs
   for (int l = 0; l < 2; ++l) {
     cudaMemsetAsync(w.count[l], 0, (cells + 1) * sizeof(unsigned), s);
     for (int t = 0; t < nsp; ++t) {
       if ((sp[t].is_ion ? 1 : 0) != l || !sp[t].n) continue;
       key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, tab, t, w.keys[l], w.vals[l], w.count[l],
                                                           w.valid + l, p.only, p.only_value);
+      ++w.launches;
     }
   }
   unsigned valid[2] = {0, 0};
@@ -595,18 +646,31 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
     }
     size_t b = w.tmp_bytes;
     cub::DeviceScan::ExclusiveSum(w.tmp, b, w.count[l], w.start[l], (int)(cells + 1), s);
-    if (p.shuffle && valid[l])
+    if (p.shuffle && valid[l]) {
       shuffle_kernel<<<blocks_for(cells), kThreads, 0, s>>>(cells, w.start[l], w.count[l], w.vals2[l],
                                                              p.seed, p.pass, (uint32_t)l);
+      ++w.launches;
+    }
+    // the sorted keys are spent: keys2 now holds the staged references
+    if (valid[l]) {
+      stage_kernel<<<blocks_for(valid[l]), kThreads, 0, s>>>(tab, w.vals2[l], valid[l], l, w.stage[l],
+                                                             w.keys2[l]);
+      w.launches += 2;  // and its write-back
+    }
   }
+  tab.stage[0] = w.stage[0];
+  tab.stage[1] = w.stage[1];
   // 0x7f7f7f7f in every row: no stop unless a non-normal cell sets one
   cudaMemsetAsync(w.row_stop, 0x7f, (size_t)g.nr * sizeof(int), s);
-  moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.vals2[0],
-                                                        w.start[1], w.count[1], w.vals2[1], w.moments,
+  moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
+                                                        w.start[1], w.count[1], w.keys2[1], w.moments,
                                                         w.row_stop);
-  collide_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.vals2[0],
-                                                        w.start[1], w.count[1], w.vals2[1], w.moments,
+  collide_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
+                                                        w.start[1], w.count[1], w.keys2[1], w.moments,
                                                         w.row_stop, w.calls);
+  for (int l = 0; l < 2; ++l)
+    if (valid[l])
+      unstage_kernel<<<blocks_for(valid[l]), kThreads, 0, s>>>(tab, w.vals2[l], valid[l], w.stage[l]);
   if (cudaMemcpyAsync(pair_calls, w.calls, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return -1;
   if (cudaStreamSynchronize(s) != cudaSuccess) return -1;

@@ -53,6 +53,7 @@ struct CollWork {
   size_t cap = 0;  // entries per list
   unsigned long long *keys[2] = {}, *keys2[2] = {}, *vals[2] = {}, *vals2[2] = {};
   unsigned *count[2] = {}, *start[2] = {};  // per cell
+  double4* stage[2] = {};                   // per list entry: v (3), w, in list order
   double* moments = nullptr;                // per cell: T_el, T_ion, n_el, n_ion
   int* row_stop = nullptr;                  // per row: first cell that stops the row
   unsigned long long* calls = nullptr;      // device counter of pair calls
@@ -60,6 +61,7 @@ struct CollWork {
   void* tmp = nullptr;
   size_t tmp_bytes = 0;
   size_t cells = 0;
+  unsigned launches = 0;                    // this library's kernels launched by the last pass
 };
 
 // One collision pass over all cells; returns 0 or -1 (allocation/launch).

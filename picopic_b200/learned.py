@@ -17,8 +17,10 @@ give the training pairs:
 relaxation time of an anisotropic plasma under both operators is what
 ``relaxation_time`` measures.
 
-Command line (one GPU):
+Command lines (one GPU) of the two committed models:
     python -m picopic_b200.learned train --out picopic_b200/models/collision_p12.npz
+    python -m picopic_b200.learned train --wide --batches 96 --steps 1000000 \
+        --out picopic_b200/models/collision_p12_wide.npz
 """
 from __future__ import annotations
 
@@ -35,6 +37,9 @@ ME, E_CHARGE = 9.1e-31, 1.6e-19
 MASS_ION = 1836.0
 FEATURES, TARGETS = 13, 6
 MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "collision_p12.npz")
+# trained on Sampling.wide() with inverse-noise weighting: for few macroparticles
+# per cell or weakly collisional plasmas, where the default model's box ends
+WIDE_MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "collision_p12_wide.npz")
 
 
 @dataclasses.dataclass
@@ -48,6 +53,15 @@ class Sampling:
     drift: float = 0.1                # electron drift per axis, in thermal speeds
     ppc: tuple = (60, 140)            # macroparticles per cell per species (log-uniform)
     ion_density: float = 0.2          # ion density n_e exp(U(-a, a))
+
+    @classmethod
+    def wide(cls):
+        """The states of the wide model: down to 8 macroparticles per cell
+        and 1e16 m^-3 (collision numbers down to ~1e-7 per step), with the
+        drift, anisotropy and density-ratio spread that few particles per
+        cell show."""
+        return cls(ti=(0.05, 2.0), density=(1e16, 1e21), e_aniso=0.8, i_aniso=0.6, drift=0.6,
+                   ppc=(8, 200), ion_density=1.0)
 
 
 class _Spec:
@@ -175,6 +189,17 @@ def normalisation(x, y):
     ym, ysd = y.mean(0), np.maximum(y.std(0), 1e-12)
     lo, hi = np.percentile(x, 0.05, axis=0), np.percentile(x, 99.95, axis=0)
     return np.concatenate([xm, xsd, ym, ysd, lo, hi]).astype(np.float32)
+
+
+def inverse_noise_resample(x, y, seed=0):
+    """Pairs resampled with probability proportional to the macroparticle
+    count N of their cell (feature 12 is 1/sqrt(N)): the variance of a
+    target given its features falls as 1/N, so this is the inverse-variance
+    weighting of the squared loss, which keeps the many noisy low-count
+    cells from swamping the fit where the targets are sharp."""
+    wgt = 1.0 / np.square(x[:, 12].astype(np.float64))
+    idx = np.random.default_rng(seed).choice(len(x), size=len(x), p=wgt / wgt.sum())
+    return x[idx], y[idx]
 
 
 def fit(x, y, steps=20000, batch=8192, lr=2e-3, seed=3, device=0, log=print):
@@ -314,6 +339,30 @@ def relaxation_time(steps, values, lo=0.95):
     return -1.0 / p[0]
 
 
+RELAX_STATES = (  # density m^-3, electron (T_par, T_perp) eV, ion T eV, macroparticles per cell
+    (5e19, (2.0, 1.0), 0.5, 100), (1e20, (2.0, 1.0), 0.5, 100), (3e20, (2.0, 1.0), 0.5, 100),
+    (1e21, (3.0, 1.5), 1.0, 100), (3e20, (1.0, 0.5), 0.25, 100), (3e20, (2.0, 1.0), 0.5, 12))
+
+
+def relax_table(paths, passes=200, device=0, log=print):
+    """Initial electron-anisotropy relaxation time of each model against the
+    binary operator (mean of `passes` passes, with its standard error) on a
+    64 x 128 slab of cells of 1e-5 m, dt 1e-13 s, for RELAX_STATES."""
+    from .domain import Geometry
+    g = Geometry(64, 128, 64e-5, 128e-5, 1e-13)
+    models = [load_model(p) for p in paths]
+    rows = []
+    for n, te, ti, ppc in RELAX_STATES:
+        tb, eb, _ = initial_relaxation_time(g, "binary", passes=passes, density=n, te=te, ti=ti, ppc=ppc,
+                                            device=device)
+        ratios = [initial_relaxation_time(g, "learned", passes=1, density=n, te=te, ti=ti, ppc=ppc,
+                                          model=m, device=device)[0] / tb for m in models]
+        rows.append((n, te, ti, ppc, tb, eb, ratios))
+        log(f"n {n:.0e} Te {te} Ti {ti} ppc {ppc}: binary {tb:.1f} +- {eb:.1f} steps; " +
+            ", ".join(f"{os.path.basename(p)} {x:.4f}" for p, x in zip(paths, ratios)))
+    return rows
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -325,17 +374,27 @@ def main(argv=None):
     t.add_argument("--dt", type=float, default=1e-13)
     t.add_argument("--steps", type=int, default=200000)
     t.add_argument("--seed", type=int, default=1)
+    t.add_argument("--wide", action="store_true",
+                   help="the wide model: Sampling.wide() states, inverse-noise weighting")
+    r = sub.add_parser("relax", help="relaxation-time ratio learned / binary on six plasma states")
+    r.add_argument("--model", action="append", default=None, help="model file (repeatable)")
+    r.add_argument("--passes", type=int, default=200)
     a = ap.parse_args(argv)
     from .domain import Geometry
+    if a.cmd == "relax":
+        relax_table(a.model or [MODEL_PATH, WIDE_MODEL_PATH], a.passes)
+        return
     dr = 1e-5
     grid = Geometry(a.nr, a.nz, a.nr * dr, a.nz * dr, a.dt)
     t0 = time.time()
-    x, y = generate(grid, a.batches, seed=a.seed)
+    sampling = Sampling.wide() if a.wide else Sampling()
+    x, y = generate(grid, a.batches, seed=a.seed, sampling=sampling)
     t1 = time.time()
-    params, norm, loss = fit(x, y, steps=a.steps, seed=a.seed + 2)
+    xf, yf = inverse_noise_resample(x, y, seed=a.seed + 5) if a.wide else (x, y)
+    params, norm, loss = fit(xf, yf, steps=a.steps, seed=a.seed + 2)
     meta = {"pairs": int(x.shape[0]), "grid": [a.nr, a.nz], "dr": dr, "dt": a.dt,
-            "sampling": dataclasses.asdict(Sampling()), "final_minibatch_loss": loss,
-            "generate_s": round(t1 - t0, 1), "train_s": round(time.time() - t1, 1)}
+            "sampling": dataclasses.asdict(sampling), "weighting": "inverse noise" if a.wide else "uniform",
+            "final_minibatch_loss": loss, "generate_s": round(t1 - t0, 1), "train_s": round(time.time() - t1, 1)}
     save_model(a.out, params, norm, meta)
     print("saved", a.out, meta)
 

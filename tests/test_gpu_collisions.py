@@ -110,3 +110,19 @@ def test_p12_relaxes_anisotropy():
     for _ in range(40):
         gpu.collide()
     assert ratio() < r0 - 0.01
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_expectation_pass_conserves_mean_momentum(precision):
+    """The expectation pass (training targets of the learned operator): per
+    cell, each collision's mean momentum change cancels between its two
+    particles in the fixed mode (a is deflected always, b with probability
+    w_a/w_b), so m_e sum w dv (electron list) + m_i sum w dv (ion list)
+    vanishes to rounding, here with unequal electron and ion weights."""
+    gpu, _, _ = _pair(precision, "fixed", ppc=20)
+    e = gpu.collide_expectation()
+    assert np.isfinite(e).all()
+    pe, pi = ME * e[:, 0:3], 1836 * ME * e[:, 6:9]
+    scale = np.abs(pe).max()
+    assert scale > 0
+    assert np.abs(pe + pi).max() <= 1e-9 * scale

@@ -15,6 +15,9 @@ operator (the committed model picopic_b200/models/collision_p12.npz).
 * What the network gains: the learned step is at least 5x faster than the
   binary pass at the same relaxation time.
 * Cells outside the training box (widened by 25 %) take the binary operator.
+* The wide model (8-200 macroparticles per cell, n down to 1e16 m^-3) takes
+  cells of 12 macroparticles per species on the learned path and matches
+  the binary relaxation time there to 1 % plus three standard errors.
 """
 import numpy as np
 import pytest
@@ -109,7 +112,7 @@ def test_learned_step_is_faster_than_binary():
 
 
 def test_out_of_box_cells_take_the_binary_operator():
-    """Electrons streaming at twice their thermal speed through the ions are
+    """Electrons streaming at four times sqrt(T_e/m_e) through the ions are
     far outside the training states (drift up to 0.1 thermal speeds)."""
     from picopic_b200 import learned as L
     g = _grid(16, 32)
@@ -117,7 +120,7 @@ def test_out_of_box_cells_take_the_binary_operator():
     cells = g.nr * g.nz
     te = np.full((cells, 3), 1.0)
     drift = np.zeros((cells, 3))
-    drift[:, 2] = 2 * np.sqrt(1.6e-19 / ME)
+    drift[:, 2] = 4 * np.sqrt(1.6e-19 / ME)
     d = L._domain(g, 0, 1, capacity=cells * 100 + 16)
     pp = np.full(cells, 100)
     d.set_particles(0, *L.cell_particles(g, rng, te, np.full(cells, 1e20), drift, pp, 1.0))
@@ -156,3 +159,24 @@ def test_pcg_step_with_collisions(mode):
     b0, b1 = run("none")
     assert a1 < a0 - 0.03
     assert a0 - a1 > 3 * abs(b1 - b0)  # well beyond the collisionless drift of the PIC noise
+
+
+def test_wide_model_covers_few_particles_per_cell():
+    from picopic_b200 import learned as L
+    g = _grid(64, 128)
+    model = L.load_model(L.WIDE_MODEL_PATH)
+    tb, eb, _ = L.initial_relaxation_time(g, "binary", passes=120, density=3e20, ppc=12)
+    tl, _, _ = L.initial_relaxation_time(g, "learned", passes=1, density=3e20, ppc=12, model=model)
+    assert abs(tl / tb - 1) <= 0.01 + 3 * eb / tb
+    # a weakly collisional plasma of 12 per cell (collision numbers ~1e-6 per step)
+    cells = g.nr * g.nz
+    rng = np.random.default_rng(3)
+    d = L._domain(g, 0, 3, capacity=cells * 12 + 16)
+    pp = np.full(cells, 12)
+    te = np.full((cells, 3), 1.0)
+    d.set_particles(0, *L.cell_particles(g, rng, te, np.full(cells, 1e18), np.zeros((cells, 3)), pp, 1.0))
+    d.set_particles(1, *L.cell_particles(g, rng, te / 10, np.full(cells, 1e18), np.zeros((cells, 3)), pp,
+                                         L.MASS_ION))
+    d.set_collision_model(*model)
+    learned, fallback = d.collide_learned()
+    assert learned >= 0.9 * cells
