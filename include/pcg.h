@@ -252,6 +252,21 @@ int pcg_divergence(pcg_handle* h, int which, double* out);
  * receives the number of pair collisions attempted. */
 int pcg_collide(pcg_handle* h, unsigned long long* pair_calls);
 
+/* The binary operator of pcg_collide and of PCG_COLLISIONS_BINARY steps;
+ * replaces the compile-time choice of collisions scheme
+ * (Domain::Domain domain.cpp:55-60, CollisionsP12 or CollisionsTA77S).
+ * PCG_COLLIDE_TA77S is collisionsTA77S.cpp: Takizuka-Abe pairs with the
+ * weighted second angle (:33-208) in the same pairing sequence, then
+ * correct_velocities (:419-566), which gives each species of each cell back
+ * its momentum and kinetic energy from before the pass.
+ * PCG_QUIRKS_REFERENCE keeps its sign of b's velocity change (+m_ab/m_b du2,
+ * :191-193) and its |alpha| for a negative correction factor; the fixed mode
+ * subtracts and leaves such a species uncorrected.  The learned step's
+ * fallback is always P12, the operator its model was trained on. */
+#define PCG_COLLIDE_P12 0
+#define PCG_COLLIDE_TA77S 1
+int pcg_set_collision_scheme(pcg_handle* h, int scheme);
+
 /* The per-cell collision MLP of the learned collision step (no counterpart
  * in the reference): 13 inputs -> 128 -> 128 -> 6 outputs, ReLU, BF16
  * operands on the tensor cores with FP32 accumulation.  Parameters are FP32,

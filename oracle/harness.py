@@ -258,6 +258,8 @@ class OracleSim(_Sim):
             lib.orc_philox4x32_10.argtypes = [ctypes.POINTER(ctypes.c_uint32)] * 3
             lib.orc_collide.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.orc_collide.restype = ctypes.c_long
+            lib.orc_collide_ta77s.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.orc_collide_ta77s.restype = ctypes.c_long
             self._bind(lib)
             OracleSim._lib = lib
         self.lib = OracleSim._lib
@@ -272,9 +274,11 @@ class OracleSim(_Sim):
     def set_rng(self, kind: str, seed: int):
         self.lib.orc_set_rng(self.h, {"mt19937": 0, "philox": 1}[kind], seed)
 
-    def collide(self, shuffle: bool = False) -> int:
-        """One binary-collision pass (Perez 2012); returns the pair calls."""
-        return int(self.lib.orc_collide(self.h, int(shuffle)))
+    def collide(self, shuffle: bool = False, scheme: str = "p12") -> int:
+        """One binary-collision pass (scheme "p12": Perez 2012, "ta77s":
+        Takizuka-Abe with the weighted correction); returns the pair calls."""
+        f = self.lib.orc_collide_ta77s if scheme == "ta77s" else self.lib.orc_collide
+        return int(f(self.h, int(shuffle)))
 
     @property
     def errors(self) -> int:
@@ -296,6 +300,8 @@ class RefSim(_Sim):
             lib.ref_error_count.restype = ctypes.c_long
             lib.ref_collide.argtypes = [ctypes.c_void_p]
             lib.ref_collide.restype = ctypes.c_long
+            lib.ref_collide_ta77s.argtypes = [ctypes.c_void_p]
+            lib.ref_collide_ta77s.restype = ctypes.c_long
             self._bind(lib)
             RefSim._libs[path] = lib
         self.lib = RefSim._libs[path]
@@ -310,8 +316,11 @@ class RefSim(_Sim):
         """Seed the reference's global std::mt19937 (rand.cpp:25)."""
         self.lib.ref_seed(s)
 
-    def collide(self) -> int:
-        """One CollisionsP12 pass without its time-seeded shuffle; returns ncol."""
+    def collide(self, scheme: str = "p12") -> int:
+        """One CollisionsP12 pass without its time-seeded shuffle (returns ncol),
+        or one CollisionsTA77S pass likewise (returns 0: it keeps no count)."""
+        if scheme == "ta77s":
+            return int(self.lib.ref_collide_ta77s(self.h))
         return int(self.lib.ref_collide(self.h))
 
     @property

@@ -1707,14 +1707,116 @@ static void p12_single(orc_sim* s, coll_rng* g, double m_real_a, double m_real_b
   if (set_pb) { pb.sp->vr[pb.j] = to_pb[0]; pb.sp->vphi[pb.j] = to_pb[1]; pb.sp->vz[pb.j] = to_pb[2]; }
 }
 
+/* std::normal_distribution<double>(0, stddev) as libstdc++ implements it
+ * (Marsaglia's polar method; a fresh distribution object per call, as
+ * math::random::normal makes one, so the second value of each accepted
+ * pair is discarded).  Philox mode: Box-Muller on draws 0 and 1. */
+static double coll_normal(coll_rng* g, double stddev) {
+  orc_sim* s = g->s;
+  double y, mult;
+  if (s->rng_kind == ORC_RNG_PHILOX) {
+    const double u0 = coll_draw(g, 0), u1 = coll_draw(g, 1);
+    y = sqrt(-2.0 * log(1.0 - u0)) * cos(2.0 * K_PI * u1);
+    return y * stddev;
+  }
+  double x, r2;
+  do {
+    x = 2.0 * mt_uniform(&s->mt) - 1.0;
+    y = 2.0 * mt_uniform(&s->mt) - 1.0;
+    r2 = x * x + y * y;
+  } while (r2 > 1.0 || r2 == 0.0);
+  mult = sqrt(-2 * log(r2) / r2);
+  return y * mult * stddev + 0.0;
+}
+
+/* phys::plasma::coulomb_logarithm (plasma.cpp:42-52) */
+static double coulomb_log(double m_a, double m_b, double debye, double v_rel) {
+  const double m_ab = m_a * m_b / (m_a + m_b);
+  const double cl = log(debye * m_ab * v_rel / K_PLANK_BAR);
+  return cl > 2. ? cl : 2.;
+}
+
+/* CollisionsTA77S::collide_single (collisionsTA77S.cpp:33-208): Takizuka-Abe
+ * scattering by a normal delta of variance q_a^2 q_b^2 n L dt /
+ * (8 pi eps0^2 m_ab^2 u^3), with the weighted second angle for the heavier-
+ * weight particle.  Draws: delta (normal), Phi (uniform angle), dzeta.
+ * The reference adds m_ab/m_b du2 to b (:191-193), where the scheme
+ * subtracts it; the fixed mode subtracts. */
+static void ta77s_single(orc_sim* s, coll_rng* g, double m_real_a, double m_real_b, double q_real_a,
+                         double q_real_b, pref pa, pref pb, double density_a_in, double density_b_in,
+                         double debye) {
+  const int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  double w_ratio = pa.sp->w[pa.j] / pb.sp->w[pb.j];
+  pref A = pa, B = pb;
+  double charge_a, mass_a, density_a, charge_b, mass_b, density_b;
+  if (w_ratio <= 1) {
+    charge_a = q_real_a; mass_a = m_real_a; density_a = density_a_in;
+    charge_b = q_real_b; mass_b = m_real_b; density_b = density_b_in;
+  } else {
+    A = pb; B = pa;
+    charge_a = q_real_b; mass_a = m_real_b; density_a = density_b_in;
+    charge_b = q_real_a; mass_b = m_real_a; density_b = density_a_in;
+    w_ratio = 1 / w_ratio;
+  }
+  const double vr_a = A.sp->vr[A.j], vphi_a = A.sp->vphi[A.j], vz_a = A.sp->vz[A.j];
+  const double vr_b = B.sp->vr[B.j], vphi_b = B.sp->vphi[B.j], vz_b = B.sp->vz[B.j];
+  const double density_lowest = density_a < density_b ? density_a : density_b;
+  const double m_ab = mass_a * mass_b / (mass_a + mass_b);
+  const double ux = vr_a - vr_b, uy = vphi_a - vphi_b, uz = vz_a - vz_b;
+  const double u = sqrt(ux * ux + uy * uy + uz * uz);
+  if (u == 0) return;
+  const double lambda = coulomb_log(mass_a, mass_b, debye, u);
+  const double u_p = sqrt(ux * ux + uy * uy);
+  const double variance_d = charge_a * charge_a * (charge_b * charge_b) * density_lowest * lambda /
+                            (8 * K_PI * (K_EPSILON0 * K_EPSILON0) * (m_ab * m_ab) * pow(u, 3)) * s->dt;
+  const double delta = coll_normal(g, sqrt(variance_d));
+  const double sin_T = 2 * delta / (1 + delta * delta);
+  const double cos_T = 1 - 2 * (delta * delta) / (1 + delta * delta);
+  double sin_T2 = sqrt(w_ratio * (sin_T * sin_T) + w_ratio * (1 - w_ratio) * ((1 - cos_T) * (1 - cos_T)));
+  const double cos_T2 = 1 - w_ratio * (1 - cos_T);
+  if (sin_T2 * sin_T < 0) sin_T2 = -sin_T2;
+  const double phi = (s->rng_kind == ORC_RNG_PHILOX ? coll_draw(g, 2) : mt_uniform(&s->mt)) * (2 * K_PI) + 0.0;
+  const double dzeta = s->rng_kind == ORC_RNG_PHILOX ? coll_draw(g, 3) : mt_uniform(&s->mt);
+  const double phi2 = phi + 2 * K_PI * (1 - sqrt(w_ratio)) * (1 - dzeta);
+  const double sin_P = sin(phi), cos_P = cos(phi), sin_P2 = sin(phi2), cos_P2 = cos(phi2);
+  double du[3], du2[3];
+  if (u_p == 0) {
+    du[0] = u * sin_T * cos_P; du[1] = u * sin_T * sin_P; du[2] = -u * (1 - cos_T);
+    du2[0] = u * sin_T2 * cos_P2; du2[1] = u * sin_T2 * sin_P2; du2[2] = -u * (1 - cos_T2);
+  } else {
+    du[0] = (ux / u_p) * uz * sin_T * cos_P - (uy / u_p) * u * sin_T * sin_P - ux * (1 - cos_T);
+    du[1] = (uy / u_p) * uz * sin_T * cos_P + (ux / u_p) * u * sin_T * sin_P - uy * (1 - cos_T);
+    du[2] = u_p * sin_T * cos_P - uz * (1 - cos_T);
+    du2[0] = (ux / u_p) * uz * sin_T2 * cos_P2 - (uy / u_p) * u * sin_T2 * sin_P2 - ux * (1 - cos_T2);
+    du2[1] = (uy / u_p) * uz * sin_T2 * cos_P2 + (ux / u_p) * u * sin_T2 * sin_P2 - uy * (1 - cos_T2);
+    du2[2] = u_p * sin_T2 * cos_P2 - uz * (1 - cos_T2);
+  }
+  const double kb = fixed ? -(m_ab / mass_b) : m_ab / mass_b;
+  A.sp->vr[A.j] = vr_a + m_ab / mass_a * du[0];
+  A.sp->vphi[A.j] = vphi_a + m_ab / mass_a * du[1];
+  A.sp->vz[A.j] = vz_a + m_ab / mass_a * du[2];
+  B.sp->vr[B.j] = vr_b + kb * du2[0];
+  B.sp->vphi[B.j] = vphi_b + kb * du2[1];
+  B.sp->vz[B.j] = vz_b + kb * du2[2];
+}
+
 static int name_is(const char* n, const char* lower, const char* cap) {
   return strcmp(n, lower) == 0 || strcmp(n, cap) == 0;
 }
 
-/* One collision pass over all cells.  shuffle: Philox Fisher-Yates of the
- * cell lists (ORC_RNG_PHILOX only).  Returns the number of collide_single
- * calls, or a negative status. */
-long orc_collide(orc_sim* s, int shuffle) {
+/* Per cell and list (0 electrons, 1 ions): the sums of
+ * collect_weighted_params_tot_grid (collisions.cpp:172-221). */
+typedef struct {
+  double amount, mom[3], energy;
+} coll_tot;
+
+static void ta77s_correct(orc_sim* s, pref* L, unsigned n, double mass, const coll_tot* t);
+
+/* One collision pass over all cells (scheme 0: CollisionsP12, 1:
+ * CollisionsTA77S with its correct_velocities).  shuffle: Philox
+ * Fisher-Yates of the cell lists (ORC_RNG_PHILOX only).  Returns the number
+ * of collide_single calls, or a negative status. */
+static long collide_pass(orc_sim* s, int shuffle, int scheme) {
   int el = -1, ion = -1;
   for (int t = 0; t < s->nsp; ++t) { /* collisions.cpp:28-48: the last match wins */
     if (name_is(s->sp[t].name, "electrons", "Electrons")) el = t;
@@ -1769,6 +1871,28 @@ long orc_collide(orc_sim* s, int shuffle) {
   }
   const double m_el = s->sp[el].mass, m_ion = s->sp[ion].mass;
   const double q_el = s->sp[el].charge, q_ion = s->sp[ion].charge;
+  /* collect_weighted_params_tot_grid (collisions.cpp:172-221), every cell
+   * before any collision: ions, then electrons, in list order */
+  coll_tot* tot = calloc(2 * ncell, sizeof(coll_tot));
+  for (size_t c = 0; c < ncell; ++c) {
+    for (int l = 1; l >= 0; --l) {
+      pref* L = l ? li + cnt_i[c] : le + cnt_e[c];
+      const size_t n = l ? cnt_i[c + 1] - cnt_i[c] : cnt_e[c + 1] - cnt_e[c];
+      const double mass = l ? m_ion : m_el;
+      coll_tot* t = &tot[2 * c + l];
+      for (size_t k = 0; k < n; ++k) {
+        const species_t* p = L[k].sp; size_t q = L[k].j;
+        double vr = p->vr[q], vphi = p->vphi[q], vz = p->vz[q];
+        double v_sq = vr * vr + vphi * vphi + vz * vz;
+        double wm = p->w[q] * mass;
+        t->mom[0] += wm * vr;
+        t->mom[1] += wm * vphi;
+        t->mom[2] += wm * vz;
+        t->amount += p->w[q];
+        t->energy += wm * v_sq / 2;
+      }
+    }
+  }
   long calls = 0;
   for (int i = 0; i < s->nr; ++i) {
     for (int j = 0; j < s->nz; ++j) {
@@ -1776,25 +1900,9 @@ long orc_collide(orc_sim* s, int shuffle) {
       pref* E = le + cnt_e[c];
       pref* I = li + cnt_i[c];
       const unsigned ne = (unsigned)(cnt_e[c + 1] - cnt_e[c]), ni = (unsigned)(cnt_i[c + 1] - cnt_i[c]);
-      /* collect_weighted_params_tot_grid (collisions.cpp:169-221) */
-      double e_tot_e = 0, amount_e = 0, e_tot_i = 0, amount_i = 0;
-      for (unsigned k = 0; k < ni; ++k) {
-        const species_t* p = I[k].sp; size_t q = I[k].j;
-        double v_sq = p->vr[q] * p->vr[q] + p->vphi[q] * p->vphi[q] + p->vz[q] * p->vz[q];
-        double wm = p->w[q] * m_ion;
-        amount_i += p->w[q];
-        e_tot_i += wm * v_sq / 2;
-      }
-      for (unsigned k = 0; k < ne; ++k) {
-        const species_t* p = E[k].sp; size_t q = E[k].j;
-        double v_sq = p->vr[q] * p->vr[q] + p->vphi[q] * p->vphi[q] + p->vz[q] * p->vz[q];
-        double wm = p->w[q] * m_el;
-        amount_e += p->w[q];
-        e_tot_e += wm * v_sq / 2;
-      }
       const double vol = K_PI * s->dz * s->dr * s->dr * (2.0 * i + 1); /* CELL_VOLUME(i) */
-      const double T_el = e_tot_e / amount_e * (1. / K_EL_CHARGE);
-      const double T_ion = e_tot_i / amount_i * (1. / K_EL_CHARGE);
+      const double T_el = tot[2 * c].energy / tot[2 * c].amount * (1. / K_EL_CHARGE);
+      const double T_ion = tot[2 * c + 1].energy / tot[2 * c + 1].amount * (1. / K_EL_CHARGE);
       double n_el = 0, n_ion = 0;
       for (unsigned k = 0; k < ne; ++k) n_el += E[k].sp->w[E[k].j];
       for (unsigned k = 0; k < ni; ++k) n_ion += I[k].sp->w[I[k].j];
@@ -1808,7 +1916,12 @@ long orc_collide(orc_sim* s, int shuffle) {
       const double debye = 7433.944 / sqrt(n_el / T_el + n_ion / T_ion);
       coll_rng g = {s, (uint32_t)c, 0};
 #define COLL(MA, MB, QA, QB, PA, PB, NA, NB) \
-      do { p12_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye); g.m++; calls++; } while (0)
+      do {                                                                          \
+        if (scheme == 1) ta77s_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye);    \
+        else p12_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye);                  \
+        g.m++;                                                                      \
+        calls++;                                                                    \
+      } while (0)
       if (ni % 2 == 0)
         for (unsigned k = 0; k < ni; k += 2) COLL(m_ion, m_ion, q_ion, q_ion, I[k], I[k + 1], n_ion, n_ion);
       if (ne % 2 == 0)
@@ -1866,7 +1979,60 @@ long orc_collide(orc_sim* s, int shuffle) {
 #undef COLL
     }
   }
+  if (scheme == 1) /* correct_velocities (collisionsTA77S.cpp:419-566), every cell */
+    for (size_t c = 0; c < ncell; ++c) {
+      ta77s_correct(s, li + cnt_i[c], (unsigned)(cnt_i[c + 1] - cnt_i[c]), m_ion, &tot[2 * c + 1]);
+      ta77s_correct(s, le + cnt_e[c], (unsigned)(cnt_e[c + 1] - cnt_e[c]), m_el, &tot[2 * c]);
+    }
+  free(tot);
   free(cnt_e); free(cnt_i); free(le); free(li);
   s->coll_pass++;
   return calls;
 }
+
+/* TA77S correct_velocities for one list of one cell: the list's momentum
+ * change is removed and its thermal velocities scaled by sqrt(alpha) so
+ * that momentum and kinetic energy return to the totals `t` collected
+ * before the pass.  The reference takes |alpha| when alpha < 0 and 1 when
+ * alpha == 0 (:494-498, :518-522); the fixed mode leaves such a list
+ * uncorrected. */
+static void ta77s_correct(orc_sim* s, pref* L, unsigned n, double mass, const coll_tot* t) {
+  double mr = 0, mp = 0, mz = 0, e_new = 0;
+  for (unsigned k = 0; k < n; ++k) {
+    const species_t* p = L[k].sp; size_t q = L[k].j;
+    double vr = p->vr[q], vphi = p->vphi[q], vz = p->vz[q];
+    double v_sq = vr * vr + vphi * vphi + vz * vz;
+    double mass_m = mass * p->w[q];
+    mr += mass_m * vr;
+    mp += mass_m * vphi;
+    mz += mass_m * vz;
+    e_new += mass_m * v_sq / 2;
+  }
+  const double mass_tot = t->amount * mass;
+  const double dvr = (mr - t->mom[0]) / mass_tot, dvp = (mp - t->mom[1]) / mass_tot,
+               dvz = (mz - t->mom[2]) / mass_tot;
+  const double v0r = t->mom[0] / mass_tot, v0p = t->mom[1] / mass_tot, v0z = t->mom[2] / mass_tot;
+  const double d_e = e_new - t->energy;
+  const double v0_sq = v0r * v0r + v0p * v0p + v0z * v0z;
+  double alpha = (t->energy - mass_tot * v0_sq / 2) /
+                 (t->energy + d_e -
+                  mass_tot * ((v0r + dvr) * (v0r + dvr) + (v0p + dvp) * (v0p + dvp) + (v0z + dvz) * (v0z + dvz)) / 2);
+  if (!isnormal(alpha)) return;
+  if (s->quirks == ORC_QUIRKS_FIXED) {
+    if (alpha < 0) return;
+  } else {
+    if (alpha < 0) alpha = -alpha;
+    if (alpha == 0) alpha = 1;
+  }
+  alpha = sqrt(alpha);
+  for (unsigned k = 0; k < n; ++k) {
+    species_t* p = L[k].sp; size_t q = L[k].j;
+    const double vr = p->vr[q], vphi = p->vphi[q], vz = p->vz[q];
+    p->vr[q] = v0r + alpha * (vr - v0r - dvr);
+    p->vphi[q] = v0p + alpha * (vphi - v0p - dvp);
+    p->vz[q] = v0z + alpha * (vz - v0z - dvz);
+  }
+}
+
+long orc_collide(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 0); }
+long orc_collide_ta77s(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 1); }

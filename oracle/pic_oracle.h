@@ -72,6 +72,9 @@ void orc_destroy(orc_sim* s);
  * cells from the last binding.  shuffle: Philox shuffle of the cell lists
  * (ORC_RNG_PHILOX).  Returns the number of pair calls or a negative status. */
 long orc_collide(orc_sim* s, int shuffle);
+/* One CollisionsTA77S pass (collisionsTA77S.cpp:568-576 without its
+ * random_sort): Takizuka-Abe pairs, then the per-cell velocity correction. */
+long orc_collide_ta77s(orc_sim* s, int shuffle);
 
 /* Building blocks exported for known-answer tests. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

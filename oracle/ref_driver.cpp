@@ -27,6 +27,7 @@
 
 #include "domain.hpp"
 #include "collisions/collisionsP12.hpp"
+#include "collisions/collisionsTA77S.hpp"
 
 namespace math::random {
 extern std::mt19937 gen;  // rand.cpp:25, a non-static global
@@ -67,6 +68,20 @@ class P12Pass : public CollisionsP12 {
     sort_to_cells();
     collect_weighted_params_tot_grid();
     collide();
+  }
+};
+
+// CollisionsTA77S::operator() (collisionsTA77S.cpp:568-576) without its
+// random_sort, which reseeds std::srand from time(0).
+class TA77SPass : public CollisionsTA77S {
+ public:
+  TA77SPass(Geometry* g, TimeSim* t, std::vector<SpecieP*> sp) : CollisionsTA77S(g, t, sp) {}
+  void run_unshuffled() {
+    clear();
+    sort_to_cells();
+    collect_weighted_params_tot_grid();
+    collide();
+    correct_velocities();
   }
 };
 
@@ -269,6 +284,14 @@ long ref_collide(void* h) {
   P12Pass c(s->geometry, &s->time, s->species);
   c.run_unshuffled();
   return pcg_ref_log::g_fatal ? -10 : (long)c.ncol;
+}
+
+long ref_collide_ta77s(void* h) {
+  RefSim* s = (RefSim*)h;
+  pcg_ref_log::g_fatal = false;
+  TA77SPass c(s->geometry, &s->time, s->species);
+  c.run_unshuffled();
+  return pcg_ref_log::g_fatal ? -10 : 0;
 }
 
 double ref_time(void* h) { return ((RefSim*)h)->time.current; }

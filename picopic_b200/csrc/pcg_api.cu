@@ -74,6 +74,7 @@ struct pcg_handle {
   LearnedWork learned;            // the learned collision step: model and scratch
   uint32_t coll_pass = 0;         // collision passes so far (their Philox counter)
   int collisions = PCG_COLLISIONS_NONE;  // collision operator of every pcg_step
+  int coll_scheme = PCG_COLLIDE_P12;     // binary operator of pcg_collide and binary steps
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -485,6 +486,7 @@ int run_collide(pcg_handle* h, unsigned long long* pair_calls) {
   if (!collision_species(h, v, p))
     return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
   p.pass = h->coll_pass++;
+  p.scheme = h->coll_scheme;
   unsigned long long calls = 0;
   if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
     return fail(h, PCG_ERR_CUDA, "collision pass");
@@ -953,6 +955,12 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (rc != PCG_OK) return rc;
   if ((rc = run_collide_learned(h, learned_cells, fallback_cells)) != PCG_OK) return rc;
   return check_status(h);
+}
+
+int pcg_set_collision_scheme(pcg_handle* h, int scheme) {
+  if (!h || (scheme != PCG_COLLIDE_P12 && scheme != PCG_COLLIDE_TA77S)) return PCG_ERR_ARG;
+  h->coll_scheme = scheme;
+  return PCG_OK;
 }
 
 int pcg_set_collisions(pcg_handle* h, int mode) {

@@ -206,15 +206,17 @@ __global__ void unstage_kernel(SpeciesTable tab, const unsigned long long* refs,
 __global__ void moments_kernel(GridGeom g, SpeciesTable tab, CollParams p, const unsigned* st_e,
                                const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                const unsigned* n_i, const unsigned long long* li, double* mom,
-                               int* row_stop) {
+                               int* row_stop, double* totals) {
   const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (c >= (size_t)g.nr * g.nz) return;
   const int i = (int)(c / g.nz), k = (int)(c - (size_t)i * g.nz);
   double e_tot_e = 0, amount_e = 0, e_tot_i = 0, amount_i = 0, v[3], w;
+  double pm_e[3] = {0, 0, 0}, pm_i[3] = {0, 0, 0};  // sum w m v (TA77S)
   for (unsigned q = 0; q < n_i[c]; ++q) {
     load_v(tab, li[st_i[c] + q], v, &w);
     const double v_sq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     const double wm = w * p.m_ion;
+    for (int d = 0; d < 3; ++d) pm_i[d] += wm * v[d];
     amount_i += w;
     e_tot_i += wm * v_sq / 2;
   }
@@ -222,8 +224,14 @@ __global__ void moments_kernel(GridGeom g, SpeciesTable tab, CollParams p, const
     load_v(tab, le[st_e[c] + q], v, &w);
     const double v_sq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
     const double wm = w * p.m_el;
+    for (int d = 0; d < 3; ++d) pm_e[d] += wm * v[d];
     amount_e += w;
     e_tot_e += wm * v_sq / 2;
+  }
+  if (totals) {
+    double* t = totals + 10 * c;
+    t[0] = amount_e; t[1] = pm_e[0]; t[2] = pm_e[1]; t[3] = pm_e[2]; t[4] = e_tot_e;
+    t[5] = amount_i; t[6] = pm_i[0]; t[7] = pm_i[1]; t[8] = pm_i[2]; t[9] = e_tot_i;
   }
   const double vol = kPi * g.dz * g.dr * g.dr * (2.0 * i + 1);  // CELL_VOLUME(i)
   const double T_el = e_tot_e / amount_e * (1. / kElCharge);
@@ -487,6 +495,127 @@ __device__ void p12_single(PairCtx& x, double m_real_a, double m_real_b, double 
 }
 
 // ---------------------------------------------------------------------------
+// 5'. the Takizuka-Abe pair collision (collisionsTA77S.cpp:33-208): a normal
+// delta of variance q_a^2 q_b^2 n L dt / (8 pi eps0^2 m_ab^2 u^3) (Box-Muller
+// on draws 0 and 1 of the collision's two Philox blocks), the angle Phi
+// (draw 2) and dzeta (draw 3) of the weighted second angle.  The reference
+// adds m_ab/m_b du2 to b (:191-193) where the scheme subtracts it; the
+// fixed mode subtracts.
+
+__device__ void ta77s_single(PairCtx& x, double m_real_a, double m_real_b, double q_real_a,
+                             double q_real_b, unsigned long long ra, unsigned long long rb,
+                             double density_a_in, double density_b_in, double debye) {
+  const CollParams& P = *x.p;
+  double va[3], vb[3], wa, wb;
+  load_v(*x.tab, ra, va, &wa);
+  load_v(*x.tab, rb, vb, &wb);
+  double w_ratio = wa / wb;
+  const bool swap = !(w_ratio <= 1);
+  if (swap) w_ratio = 1 / w_ratio;
+  const double charge_a = swap ? q_real_b : q_real_a, mass_a = swap ? m_real_b : m_real_a;
+  const double charge_b = swap ? q_real_a : q_real_b, mass_b = swap ? m_real_a : m_real_b;
+  const double density_a = swap ? density_b_in : density_a_in;
+  const double density_b = swap ? density_a_in : density_b_in;
+  const double* v_a = swap ? vb : va;
+  const double* v_b = swap ? va : vb;
+  const double density_lowest = density_a < density_b ? density_a : density_b;
+  const double m_ab = mass_a * mass_b / (mass_a + mass_b);
+  const double ux = v_a[0] - v_b[0], uy = v_a[1] - v_b[1], uz = v_a[2] - v_b[2];
+  const double u = sqrt(ux * ux + uy * uy + uz * uz);
+  if (u == 0) return;
+  const double cl = log(debye * m_ab * u / kPlankBar);  // plasma.cpp:42-52
+  const double lambda = cl > 2. ? cl : 2.;
+  const double u_p = sqrt(ux * ux + uy * uy);
+  const double variance_d = charge_a * charge_a * (charge_b * charge_b) * density_lowest * lambda /
+                            (8 * kPi * (kEps0 * kEps0) * (m_ab * m_ab) * pow(u, 3.0)) * P.dt;
+  uint32_t o[4], o2[4];
+  philox4x32_10(x.cell, 2u * x.m, P.pass, kCollTag, (uint32_t)P.seed, (uint32_t)(P.seed >> 32), o);
+  philox4x32_10(x.cell, 2u * x.m + 1u, P.pass, kCollTag, (uint32_t)P.seed, (uint32_t)(P.seed >> 32), o2);
+  const double u0 = u53(o[0], o[1]), u1 = u53(o[2], o[3]);
+  const double delta = sqrt(-2.0 * log(1.0 - u0)) * cos(2.0 * kPi * u1) * sqrt(variance_d);
+  const double sin_T = 2 * delta / (1 + delta * delta);
+  const double cos_T = 1 - 2 * (delta * delta) / (1 + delta * delta);
+  double sin_T2 = sqrt(w_ratio * (sin_T * sin_T) + w_ratio * (1 - w_ratio) * ((1 - cos_T) * (1 - cos_T)));
+  const double cos_T2 = 1 - w_ratio * (1 - cos_T);
+  if (sin_T2 * sin_T < 0) sin_T2 = -sin_T2;
+  const double phi = u53(o2[0], o2[1]) * (2 * kPi) + 0.0;
+  const double dzeta = u53(o2[2], o2[3]);
+  const double phi2 = phi + 2 * kPi * (1 - sqrt(w_ratio)) * (1 - dzeta);
+  double sin_P, cos_P, sin_P2, cos_P2;
+  sincos(phi, &sin_P, &cos_P);
+  sincos(phi2, &sin_P2, &cos_P2);
+  double du[3], du2[3];
+  if (u_p == 0) {
+    du[0] = u * sin_T * cos_P; du[1] = u * sin_T * sin_P; du[2] = -u * (1 - cos_T);
+    du2[0] = u * sin_T2 * cos_P2; du2[1] = u * sin_T2 * sin_P2; du2[2] = -u * (1 - cos_T2);
+  } else {
+    du[0] = (ux / u_p) * uz * sin_T * cos_P - (uy / u_p) * u * sin_T * sin_P - ux * (1 - cos_T);
+    du[1] = (uy / u_p) * uz * sin_T * cos_P + (ux / u_p) * u * sin_T * sin_P - uy * (1 - cos_T);
+    du[2] = u_p * sin_T * cos_P - uz * (1 - cos_T);
+    du2[0] = (ux / u_p) * uz * sin_T2 * cos_P2 - (uy / u_p) * u * sin_T2 * sin_P2 - ux * (1 - cos_T2);
+    du2[1] = (uy / u_p) * uz * sin_T2 * cos_P2 + (ux / u_p) * u * sin_T2 * sin_P2 - uy * (1 - cos_T2);
+    du2[2] = u_p * sin_T2 * cos_P2 - uz * (1 - cos_T2);
+  }
+  const double ka = m_ab / mass_a, kb = P.fixed ? -(m_ab / mass_b) : m_ab / mass_b;
+  const double na[3] = {v_a[0] + ka * du[0], v_a[1] + ka * du[1], v_a[2] + ka * du[2]};
+  const double nb[3] = {v_b[0] + kb * du2[0], v_b[1] + kb * du2[1], v_b[2] + kb * du2[2]};
+  store_v(*x.tab, swap ? rb : ra, na);
+  store_v(*x.tab, swap ? ra : rb, nb);
+}
+
+// correct_velocities (collisionsTA77S.cpp:419-566) of one list of one cell:
+// remove the list's momentum change and scale its thermal velocities by
+// sqrt(alpha) so that momentum and kinetic energy return to the totals t
+// (sum w, sum w m v, sum w m v^2/2) collected before the pass.  The
+// reference takes |alpha| for alpha < 0 and 1 for alpha == 0; the fixed
+// mode leaves such a list as it is.
+__device__ void ta77s_correct(const SpeciesTable& tab, const unsigned long long* L, unsigned n, double mass,
+                              const double* t, int fixed) {
+  double m3[3] = {0, 0, 0}, e_new = 0, v[3], w;
+  for (unsigned q = 0; q < n; ++q) {
+    load_v(tab, L[q], v, &w);
+    const double v_sq = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const double mass_m = mass * w;
+    for (int d = 0; d < 3; ++d) m3[d] += mass_m * v[d];
+    e_new += mass_m * v_sq / 2;
+  }
+  const double mass_tot = t[0] * mass;
+  double dv[3], v0[3];
+  for (int d = 0; d < 3; ++d) {
+    dv[d] = (m3[d] - t[1 + d]) / mass_tot;
+    v0[d] = t[1 + d] / mass_tot;
+  }
+  const double d_e = e_new - t[4];
+  const double v0_sq = v0[0] * v0[0] + v0[1] * v0[1] + v0[2] * v0[2];
+  double alpha = (t[4] - mass_tot * v0_sq / 2) /
+                 (t[4] + d_e - mass_tot * ((v0[0] + dv[0]) * (v0[0] + dv[0]) + (v0[1] + dv[1]) * (v0[1] + dv[1]) +
+                                           (v0[2] + dv[2]) * (v0[2] + dv[2])) / 2);
+  if (!normal(alpha)) return;
+  if (fixed) {
+    if (alpha < 0) return;
+  } else {
+    if (alpha < 0) alpha = -alpha;
+  }
+  alpha = sqrt(alpha);
+  for (unsigned q = 0; q < n; ++q) {
+    load_v(tab, L[q], v, &w);
+    const double c[3] = {v0[0] + alpha * (v[0] - v0[0] - dv[0]), v0[1] + alpha * (v[1] - v0[1] - dv[1]),
+                         v0[2] + alpha * (v[2] - v0[2] - dv[2])};
+    store_v(tab, L[q], c);
+  }
+}
+
+__global__ void ta77s_correct_kernel(GridGeom g, SpeciesTable tab, CollParams p, const unsigned* st_e,
+                                     const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
+                                     const unsigned* n_i, const unsigned long long* li, const double* totals) {
+  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= (size_t)g.nr * g.nz) return;
+  if (p.only && p.only[c] != p.only_value) return;
+  ta77s_correct(tab, li + st_i[c], n_i[c], p.m_ion, totals + 10 * c + 5, p.fixed);
+  ta77s_correct(tab, le + st_e[c], n_e[c], p.m_el, totals + 10 * c, p.fixed);
+}
+
+// ---------------------------------------------------------------------------
 // 5. the per-cell pairing sequence (collisionsP12.cpp:338-548)
 
 __global__ void collide_kernel(GridGeom g, SpeciesTable tab, CollParams p, const unsigned* st_e,
@@ -510,8 +639,12 @@ __global__ void collide_kernel(GridGeom g, SpeciesTable tab, CollParams p, const
   const double me = p.m_el, mi = p.m_ion, qe = p.q_el, qi = p.q_ion;
   double expect[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   PairCtx x{&tab, &p, (uint32_t)c, 0u, p.expect ? expect : nullptr};
-#define COLL(MA, MB, QA, QB, A, B, NA, NB) \
-  do { p12_single(x, MA, MB, QA, QB, A, B, NA, NB, debye); ++x.m; } while (0)
+#define COLL(MA, MB, QA, QB, A, B, NA, NB)                                       \
+  do {                                                                           \
+    if (p.scheme == 1) ta77s_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);      \
+    else p12_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);                     \
+    ++x.m;                                                                       \
+  } while (0)
   if (ni % 2 == 0)
     for (unsigned q = 0; q < ni; q += 2) COLL(mi, mi, qi, qi, I[q], I[q + 1], n_ion, n_ion);
   if (ne % 2 == 0)
@@ -587,6 +720,7 @@ void collide_free(CollWork& w) {
     cudaFree(w.count[l]); cudaFree(w.start[l]); cudaFree(w.stage[l]);
   }
   cudaFree(w.moments); cudaFree(w.row_stop); cudaFree(w.calls); cudaFree(w.valid); cudaFree(w.tmp);
+  cudaFree(w.totals);
   w = CollWork();
 }
 
@@ -619,6 +753,10 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
     if (grow((char**)&w.tmp, w.tmp_bytes)) return -1;
     w.cap = need;
     w.cells = cells;
+  }
+  if (p.scheme == 1 && w.totals_cells != cells) {
+    if (grow(&w.totals, 10 * cells)) return -1;
+    w.totals_cells = cells;
   }
   cudaMemsetAsync(w.calls, 0, sizeof(unsigned long long), s);
   cudaMemsetAsync(w.valid, 0, 2 * sizeof(unsigned), s);
@@ -664,10 +802,15 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   cudaMemsetAsync(w.row_stop, 0x7f, (size_t)g.nr * sizeof(int), s);
   moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
                                                         w.start[1], w.count[1], w.keys2[1], w.moments,
-                                                        w.row_stop);
+                                                        w.row_stop, p.scheme == 1 ? w.totals : nullptr);
   collide_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
                                                         w.start[1], w.count[1], w.keys2[1], w.moments,
                                                         w.row_stop, w.calls);
+  if (p.scheme == 1) {
+    ta77s_correct_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
+                                                                w.start[1], w.count[1], w.keys2[1], w.totals);
+    ++w.launches;
+  }
   for (int l = 0; l < 2; ++l)
     if (valid[l])
       unstage_kernel<<<blocks_for(valid[l]), kThreads, 0, s>>>(tab, w.vals2[l], valid[l], w.stage[l]);

@@ -46,6 +46,7 @@ struct CollParams {
   // sum w v^2 (3) of the electron list, then of the ion list
   // (non-relativistic kinematics of the mean)
   double* expect = nullptr;
+  int scheme = 0;  // 0: Perez 2012 (CollisionsP12), 1: Takizuka-Abe with correction (CollisionsTA77S)
 };
 
 // Scratch of a collision pass, grown on demand and kept by the handle.
@@ -55,6 +56,8 @@ struct CollWork {
   unsigned *count[2] = {}, *start[2] = {};  // per cell
   double4* stage[2] = {};                   // per list entry: v (3), w, in list order
   double* moments = nullptr;                // per cell: T_el, T_ion, n_el, n_ion
+  double* totals = nullptr;                 // TA77S, per cell and list: sum w, sum w m v (3), sum w m v^2/2
+  size_t totals_cells = 0;
   int* row_stop = nullptr;                  // per row: first cell that stops the row
   unsigned long long* calls = nullptr;      // device counter of pair calls
   unsigned* valid = nullptr;                // device: entries appended to each list

@@ -207,6 +207,12 @@ class Domain:
         self._check(self.lib.pcg_set_collision_model(self.h, p.ctypes.data_as(pf), n.ctypes.data_as(pf)),
                     "pcg_set_collision_model")
 
+    def set_collision_scheme(self, scheme):
+        """Binary operator of collide() and "binary" steps: "p12" (CollisionsP12,
+        the default) or "ta77s" (CollisionsTA77S with its velocity correction)."""
+        code = {"p12": 0, "ta77s": 1}[scheme]
+        self._check(self.lib.pcg_set_collision_scheme(self.h, code), "pcg_set_collision_scheme")
+
     def set_collisions(self, mode):
         """Collisions inside step(): "none", "binary" or "learned" (one pass opens every step)."""
         code = {"none": 0, "binary": 1, "learned": 2}[mode]

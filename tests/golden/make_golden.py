@@ -60,8 +60,10 @@ def main():
         print("wrote", name)
 
 
-def collisions_fixture():
-    """One Perez-2012 collision pass of the reference (no shuffle, mt19937)."""
+def collisions_fixture(scheme="p12"):
+    """One collision pass of the reference (no shuffle, mt19937): scheme
+    "p12" (CollisionsP12) or "ta77s" (CollisionsTA77S with its velocity
+    correction)."""
     grid = small_grid(nr=8, nz=16, pml=False)
     n = grid.nr * grid.nz * 10
     sim = RefSim(grid)
@@ -76,14 +78,15 @@ def collisions_fixture():
     for sid in (0, 1):
         for k, v in sim.get_particles(sid).items():
             out[f"in/p{sid}/{k}"] = v
-    out["ncol"] = np.array(sim.collide())
+    out["ncol"] = np.array(sim.collide(scheme=scheme))
     for sid in (0, 1):
         for k, v in sim.get_particles(sid).items():
             out[f"out/p{sid}/{k}"] = v
-    np.savez_compressed(os.path.join(HERE, "collisions", "p12_pass.npz"), **out)
-    print("wrote collisions/p12_pass")
+    np.savez_compressed(os.path.join(HERE, "collisions", f"{scheme}_pass.npz"), **out)
+    print(f"wrote collisions/{scheme}_pass")
 
 
 if __name__ == "__main__":
     main()
-    collisions_fixture()
+    collisions_fixture("p12")
+    collisions_fixture("ta77s")

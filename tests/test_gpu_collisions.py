@@ -22,7 +22,7 @@ RTOL_CONS_PASS = 2e-11
 ME = 9.1e-31
 
 
-def _pair(precision, quirks, ppc=20, passes=1, extra_ions=13):
+def _pair(precision, quirks, ppc=20, passes=1, extra_ions=13, scheme="p12"):
     from picopic_b200 import Domain
     grid = small_grid(nr=8, nz=16, pml=False)
     n = grid.nr * grid.nz * ppc
@@ -40,9 +40,10 @@ def _pair(precision, quirks, ppc=20, passes=1, extra_ions=13):
                       for k, a in enumerate(p))
         orc.set_particles(sid, *p)
     orc.set_rng("philox", 77)
+    gpu.set_collision_scheme(scheme)
     calls = []
     for _ in range(passes):
-        calls.append((gpu.collide(), orc.collide(shuffle=True)))
+        calls.append((gpu.collide(), orc.collide(shuffle=True, scheme=scheme)))
     return gpu, orc, calls
 
 
@@ -126,3 +127,65 @@ def test_expectation_pass_conserves_mean_momentum(precision):
     scale = np.abs(pe).max()
     assert scale > 0
     assert np.abs(pe + pi).max() <= 1e-9 * scale
+
+
+def _compare(gpu, orc, rtol):
+    for sid in (0, 1):
+        pg, po = gpu.get_particles(sid), orc.get_particles(sid)
+        scale = max(np.abs(po[k]).max() for k in ("vr", "vphi", "vz"))
+        for k in ("vr", "vphi", "vz"):
+            assert np.abs(pg[k] - po[k]).max() <= rtol * scale, f"species {sid} {k}"
+
+
+@pytest.mark.parametrize("quirks", ["reference", "fixed"])
+def test_ta77s_f64_matches_oracle(quirks):
+    """Takizuka-Abe pairs and the velocity correction (collisionsTA77S.cpp)
+    with the oracle's Philox draws, two passes."""
+    gpu, orc, calls = _pair("f64", quirks, passes=2, scheme="ta77s")
+    assert all(c[0] == c[1] > 0 for c in calls)
+    _compare(gpu, orc, RTOL_F64)
+
+
+def test_ta77s_f32_matches_oracle():
+    gpu, orc, _ = _pair("f32", "fixed", scheme="ta77s")
+    _compare(gpu, orc, RTOL_F32)
+
+
+@pytest.mark.parametrize("quirks", ["reference", "fixed"])
+def test_ta77s_keeps_each_species_momentum_and_energy(quirks):
+    """correct_velocities gives every species of every cell back its
+    momentum and kinetic energy from before the pass (checked on the
+    species totals, to 1e-11 of the momentum scale and of the energy)."""
+    gpu, _, _ = _pair("f64", quirks, ppc=30, scheme="ta77s", passes=0)
+
+    def totals(sid, m):
+        p = gpu.get_particles(sid)
+        mw = m * p["w"]
+        return np.array([np.sum(mw * p["vr"]), np.sum(mw * p["vphi"]), np.sum(mw * p["vz"]),
+                         0.5 * np.sum(mw * (p["vr"] ** 2 + p["vphi"] ** 2 + p["vz"] ** 2))])
+
+    t0 = [totals(0, ME), totals(1, 1836 * ME)]
+    p0 = gpu.get_particles(0)["vz"].copy()
+    for _ in range(3):
+        gpu.collide()
+    assert np.abs(gpu.get_particles(0)["vz"] - p0).max() > 0
+    for sid, m in ((0, ME), (1, 1836 * ME)):
+        t1 = totals(sid, m)
+        p = gpu.get_particles(sid)
+        pscale = np.sum(m * p["w"] * np.sqrt(p["vr"] ** 2 + p["vphi"] ** 2 + p["vz"] ** 2))
+        assert np.abs(t1[:3] - t0[sid][:3]).max() <= 1e-11 * pscale
+        assert abs(t1[3] - t0[sid][3]) <= 1e-11 * t0[sid][3]
+
+
+def test_ta77s_relaxes_anisotropy():
+    """Electrons with T_par = 2 T_perp approach isotropy over passes."""
+    gpu, _, _ = _pair("f64", "fixed", ppc=50, scheme="ta77s", passes=0)
+
+    def aniso():
+        p = gpu.get_particles(0)
+        return np.mean(p["vz"] ** 2) / (0.5 * np.mean(p["vr"] ** 2 + p["vphi"] ** 2))
+
+    a0 = aniso()
+    for _ in range(40):
+        gpu.collide()
+    assert aniso() < a0 - 0.01

@@ -93,3 +93,31 @@ def test_p12_collisions_bit_exact(ppc):
         po, pr = o.get_particles(sid), r.get_particles(sid)
         for k in ("vr", "vphi", "vz"):
             np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
+
+
+@pytest.mark.parametrize("ppc", [3, 10])
+def test_ta77s_collisions_bit_exact(ppc):
+    """One Takizuka-Abe pass with the weighted correction (collisionsTA77S.cpp:
+    pairs, then correct_velocities; no shuffle, the reference's mt19937
+    draws: normal by the polar method, angle, dzeta): velocities
+    bit-identical, with unequal electron and ion weights."""
+    if not reference_available():
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    grid = small_grid(nr=8, nz=16, pml=False)
+    n = grid.nr * grid.nz * ppc
+    o, r = OracleSim(grid, quirks="reference"), RefSim(grid)
+    for sim in (o, r):
+        sim.add(ELECTRONS)
+        sim.add(IONS)
+        sim.set_particles(0, *thermal_plasma(grid, n, 1, 1.0, 1.0, 1e20, t_par_ratio=2.0))
+        sim.set_particles(1, *thermal_plasma(grid, n + 7, 2, 1836.0, 0.5, 1e20))
+    o.set_rng("mt19937", 321)
+    r.seed(321)
+    before = o.get_particles(0)["vz"].copy()
+    assert o.collide(scheme="ta77s") > 0
+    assert r.collide(scheme="ta77s") == 0
+    for sid in (0, 1):
+        po, pr = o.get_particles(sid), r.get_particles(sid)
+        for k in ("vr", "vphi", "vz"):
+            np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
+    assert np.abs(o.get_particles(0)["vz"] - before).max() > 0
