@@ -324,6 +324,24 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
 int pcg_cell_moments(pcg_handle* h, double* moments);
 int pcg_cell_features(pcg_handle* h, float* features, double* scale);
 
+/* SpecieP's diagnostic maps of species `slot` (specieP.cpp:665-839:
+ * calc_density, calc_temperature, calc_energy, calc_momentum) into host
+ * `out`: (nr+4) x (nz+4) doubles laid out as the fields, three such grids
+ * (r, phi, z) for PCG_MAP_MOMENTUM.  Values spread over the nodes as
+ * weight_cylindrical does (weighter.hpp:27-130); temperature and energy are
+ * in eV on the interior nodes, momentum is p / n there.  Under
+ * PCG_QUIRKS_REFERENCE gamma enters a particle's momentum only below
+ * REL_LIMIT = 5e7 m/s (specieP.cpp:729, 764) and the temperature reads the
+ * absolute-momentum map of this species' last PCG_MAP_ENERGY call (its
+ * calc_momentum_w does not make one; before any call the reference reads
+ * an uninitialised grid, here zeros); PCG_QUIRKS_FIXED applies gamma at
+ * every speed and makes the map afresh. */
+#define PCG_MAP_DENSITY 0
+#define PCG_MAP_TEMPERATURE 1
+#define PCG_MAP_ENERGY 2
+#define PCG_MAP_MOMENTUM 3
+int pcg_species_map(pcg_handle* h, int slot, int which, double* out);
+
 /* Collisions inside pcg_step: every step then opens with one pass of the
  * chosen operator on the velocities the previous step left.  The reference
  * collides between the push and the move (SMB.cpp:1289-1293); a caller

@@ -144,6 +144,9 @@ class _Sim:
             f = getattr(lib, p + name)
             f.argtypes = [ctypes.c_void_p, ctypes.c_int]
             f.restype = ctypes.c_int
+        f = getattr(lib, p + "species_map")
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _PD]
+        f.restype = ctypes.c_int
         f = getattr(lib, p + "time")
         f.argtypes = [ctypes.c_void_p]
         f.restype = _D
@@ -204,6 +207,17 @@ class _Sim:
 
     def fields(self) -> dict:
         return {name: self.get_field(name) for name in FIELDS}
+
+    MAPS = {"density": 0, "temperature": 1, "energy": 2, "momentum": 3}
+
+    def species_map(self, sid: int, which: str) -> np.ndarray:
+        """SpecieP::calc_<which> of species sid (specieP.cpp:665-839): a
+        (nr+4, nz+4) grid, or (3, nr+4, nz+4) for "momentum"."""
+        k = self.MAPS[which]
+        out = np.zeros((3 if k == 3 else 1,) + self.grid.shape)
+        rc = self._fn("species_map")(self.h, sid, k, _dp(out))
+        assert rc == 0, f"species_map rc {rc}"
+        return out if k == 3 else out[0]
 
     def stage(self, name) -> int:
         idx = STAGE[name] if isinstance(name, str) else name

@@ -39,6 +39,7 @@ typedef struct {
   size_t n, cap;
   double *r, *phi, *z, *r_old, *phi_old, *z_old, *vr, *vphi, *vz, *w, *sn;
   long long *cell_r, *cell_z;
+  double* abs_map; /* SpecieP::momentum_abs_map_w as the last energy map left it (NULL: zeros) */
   /* BeamP state (beamP.cpp:22-69) */
   unsigned macro_amount, bunches_amount, current_bunch;
   double start_time, radius, density, bunch_length, bunches_distance, velocity;
@@ -1449,7 +1450,7 @@ void orc_destroy(orc_sim* s) {
     species_t* p = &s->sp[t];
     free(p->r); free(p->phi); free(p->z); free(p->r_old); free(p->phi_old); free(p->z_old);
     free(p->vr); free(p->vphi); free(p->vz); free(p->w); free(p->sn);
-    free(p->cell_r); free(p->cell_z);
+    free(p->cell_r); free(p->cell_z); free(p->abs_map);
   }
   free(s);
 }
@@ -2036,3 +2037,167 @@ static void ta77s_correct(orc_sim* s, pref* L, unsigned n, double mass, const co
 
 long orc_collide(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 0); }
 long orc_collide_ta77s(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 1); }
+
+
+/* ------------------------------------------------------------------ */
+/* Species diagnostic maps: SpecieP::calc_density / calc_temperature /   */
+/* calc_energy / calc_momentum (specieP.cpp:665-839) over                */
+/* weight_cylindrical (weighter.hpp:27-130).                              */
+
+static void grid_inc(const orc_sim* s, double* g, unsigned i, unsigned k, double v) {
+  g[IDX(s, (int)i, (int)k)] += v;
+}
+
+/* weight_cylindrical: the cloud [r - dr/2, r + dr/2] x [z - dz/2, z + dz/2]
+ * split at (i + 1/2) dr and (k + 1/2) dz, each part's ring volume over the
+ * node's CELL_VOLUME (macro argument unparenthesised: 2i + 1 + 1 for i + 1),
+ * times value / cloud volume; on the axis the cloud is cut at r = 0. */
+static void weight_cyl(const orc_sim* s, double* g, double pos_r, double pos_z, double weight_value) {
+  const double dr = s->dr, dz = s->dz;
+  unsigned r_i = (unsigned)CELL_NUMBER(pos_r, dr);
+  const unsigned z_k = (unsigned)CELL_NUMBER(pos_z, dz);
+  const unsigned ri_s = r_i, zk_s = z_k;
+  double v_1 = K_PI * dz * dr * dr * (2.0 * r_i + 1);
+  double v_2 = K_PI * dz * dr * dr * (2.0 * r_i + 1 + 1);
+  double r1, r2, r3, dz1, dz2, v_0, rho, value;
+  if (pos_r > dr) {
+    r1 = pos_r - 0.5 * dr;
+    r2 = (r_i + 0.5) * dr;
+    r3 = pos_r + 0.5 * dr;
+    v_0 = 2. * K_PI * dz * dr * pos_r;
+    dz1 = (z_k + 0.5) * dz - (pos_z - 0.5 * dz);
+    dz2 = (pos_z + 0.5 * dz) - (z_k + 0.5) * dz;
+    rho = weight_value / v_0;
+    value = K_PI * dz1 * (r2 * r2 - r1 * r1) / v_1; grid_inc(s, g, ri_s, zk_s, rho * value);
+    value = K_PI * dz1 * (r3 * r3 - r2 * r2) / v_2; grid_inc(s, g, ri_s + 1, zk_s, rho * value);
+    value = K_PI * dz2 * (r2 * r2 - r1 * r1) / v_1; grid_inc(s, g, ri_s, zk_s + 1, rho * value);
+    value = K_PI * dz2 * (r3 * r3 - r2 * r2) / v_2; grid_inc(s, g, ri_s + 1, zk_s + 1, rho * value);
+  } else if (pos_r <= dr / 2.) {
+    r_i = 0;
+    r2 = (r_i + 0.5) * dr;
+    r3 = pos_r + 0.5 * dr;
+    dz1 = (z_k + 0.5) * dz - (pos_z - 0.5 * dz);
+    dz2 = (pos_z + 0.5 * dz) - (z_k + 0.5) * dz;
+    v_0 = K_PI * dz * (2. * pos_r * pos_r + dr * dr / 2.);
+    rho = weight_value / v_0;
+    value = K_PI * dz1 * (dr * dr / 2. - pos_r * dr + pos_r * pos_r) / v_1; grid_inc(s, g, ri_s, zk_s, rho * value);
+    value = K_PI * dz1 * (r3 * r3 - r2 * r2) / v_2; grid_inc(s, g, ri_s + 1, zk_s, rho * value);
+    value = K_PI * dz2 * (dr * dr / 2. - pos_r * dr + pos_r * pos_r) / v_1; grid_inc(s, g, ri_s, zk_s + 1, rho * value);
+    value = K_PI * dz2 * (r3 * r3 - r2 * r2) / v_2; grid_inc(s, g, ri_s + 1, zk_s + 1, rho * value);
+  } else {
+    r1 = pos_r - 0.5 * dr;
+    r2 = (r_i + 0.5) * dr;
+    r3 = pos_r + 0.5 * dr;
+    dz1 = (z_k + 0.5) * dz - (pos_z - 0.5 * dz);
+    dz2 = (pos_z + 0.5 * dz) - (z_k + 0.5) * dz;
+    v_0 = 2. * K_PI * dz * dr * pos_r;
+    v_1 = K_PI * dz * dr * dr; /* CYL_VOL(dz, dr) */
+    v_2 = K_PI * dz * dr * dr * (2.0 * r_i + 1 + 1);
+    rho = weight_value / v_0;
+    value = K_PI * dz1 * (r2 * r2 - r1 * r1) / v_1; grid_inc(s, g, ri_s, zk_s, rho * value);
+    value = K_PI * dz1 * (r3 * r3 - r2 * r2) / v_2; grid_inc(s, g, ri_s + 1, zk_s, rho * value);
+    value = K_PI * dz2 * (r2 * r2 - r1 * r1) / v_1; grid_inc(s, g, ri_s, zk_s + 1, rho * value);
+    value = K_PI * dz2 * (r3 * r3 - r2 * r2) / v_2; grid_inc(s, g, ri_s + 1, zk_s + 1, rho * value);
+  }
+}
+
+/* phys::rel::energy_m (rel.cpp:88-101) */
+static double energy_m(double mass, double momentum_2) {
+  if (momentum_2 > K_REL_LIMIT_POW_2 * mass * mass) {
+    double e_rest = mass * K_LIGHT_VEL_POW_2;
+    return sqrt(momentum_2 * K_LIGHT_VEL_POW_2 + e_rest * e_rest) - e_rest;
+  }
+  return 0.5 * momentum_2 / mass;
+}
+
+/* calc_momentum_w (:740-782) into m[3], calc_momentum_abs_w (:714-738) into
+ * a; gamma is applied below REL_LIMIT only (the reference's test), at every
+ * speed in the fixed mode.  Returns nonzero when a speed exceeds c. */
+static int momentum_maps(orc_sim* s, const species_t* p, double* m[3], double* a) {
+  const int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  for (size_t j = 0; j < p->n; ++j) {
+    if (!(p->r[j] >= 0.0)) continue;
+    const double v_r = p->vr[j], v_phi = p->vphi[j], v_z = p->vz[j];
+    if (m) {
+      const double m_weighted = p->mass * p->w[j];
+      double p_r = m_weighted * v_r, p_phi = m_weighted * v_phi, p_z = m_weighted * v_z;
+      const double v_abs_2 = v_r * v_r + v_phi * v_phi + v_z * v_z;
+      if (fixed || v_abs_2 < K_REL_LIMIT_POW_2) {
+        double gamma;
+        if (lorenz_factor(v_abs_2, &gamma) != ST_OK) return -1;
+        p_r *= gamma; p_phi *= gamma; p_z *= gamma;
+      }
+      weight_cyl(s, m[0], p->r[j], p->z[j], p_r);
+      weight_cyl(s, m[1], p->r[j], p->z[j], p_phi);
+      weight_cyl(s, m[2], p->r[j], p->z[j], p_z);
+    }
+    if (a) {
+      const double v_abs = sqrt(v_r * v_r + v_phi * v_phi + v_z * v_z);
+      double p_abs = p->mass * p->w[j] * v_abs;
+      if (fixed || v_abs < K_REL_LIMIT) {
+        double gamma;
+        if (lorenz_factor(v_abs * v_abs, &gamma) != ST_OK) return -1;
+        p_abs *= gamma;
+      }
+      weight_cyl(s, a, p->r[j], p->z[j], p_abs);
+    }
+  }
+  return 0;
+}
+
+/* One map of species sid into out ((nr+4) x (nz+4) doubles, 3 of them for
+ * ORC_MAP_MOMENTUM: r, phi, z).  which: 0 density, 1 temperature (eV),
+ * 2 energy (eV), 3 momentum.  The temperature of the reference reads the
+ * absolute-momentum map the last energy map left (calc_momentum_w does not
+ * fill it, :681-683); before any it reads a grid never initialised, where
+ * this takes zeros.  The fixed mode makes the map afresh. */
+int orc_species_map(orc_sim* s, int sid, int which, double* out) {
+  if (sid < 0 || sid >= s->nsp || which < 0 || which > 3) return ST_ARG;
+  species_t* p = &s->sp[sid];
+  const size_t nodes = (size_t)(s->nr + 4) * (size_t)(s->nz + 4);
+  double* dens = calloc(nodes, sizeof(double));
+  for (size_t j = 0; j < p->n; ++j)
+    if (p->r[j] >= 0.0) weight_cyl(s, dens, p->r[j], p->z[j], p->w[j]);
+  if (which == 0) {
+    memcpy(out, dens, nodes * sizeof(double));
+    free(dens);
+    return ST_OK;
+  }
+  if (!p->abs_map) p->abs_map = calloc(nodes, sizeof(double));
+  double* mw[3] = {NULL, NULL, NULL};
+  int rc = 0;
+  if (which == 1 || which == 3) {
+    for (int c = 0; c < 3; ++c) mw[c] = calloc(nodes, sizeof(double));
+    rc = momentum_maps(s, p, mw, NULL);
+  }
+  if (rc == 0 && (which == 2 || (which == 1 && s->quirks == ORC_QUIRKS_FIXED))) {
+    memset(p->abs_map, 0, nodes * sizeof(double));
+    rc = momentum_maps(s, p, NULL, p->abs_map);
+  }
+  if (rc == 0) {
+    const int ncomp = which == 3 ? 3 : 1;
+    memset(out, 0, ncomp * nodes * sizeof(double));
+    for (int r = 0; r < s->nr; ++r)
+      for (int z = 0; z < s->nz; ++z) {
+        const size_t q = IDX(s, r, z);
+        const double dl = dens[q];
+        if (dl == 0) continue;
+        if (which == 3) {
+          for (int c = 0; c < 3; ++c) out[c * nodes + q] = mw[c][q] / dl;
+        } else {
+          double p2;
+          if (which == 1) {
+            const double p_vec_sum_2 = mw[0][q] * mw[0][q] + mw[1][q] * mw[1][q] + mw[2][q] * mw[2][q];
+            p2 = p->abs_map[q] * p->abs_map[q] - p_vec_sum_2;
+          } else {
+            p2 = p->abs_map[q] * p->abs_map[q];
+          }
+          p2 /= dl * dl;
+          out[q] = energy_m(p->mass, p2) * (1. / K_EL_CHARGE);
+        }
+      }
+  }
+  for (int c = 0; c < 3; ++c) free(mw[c]);
+  free(dens);
+  return rc == 0 ? ST_OK : ST_FATAL;
+}

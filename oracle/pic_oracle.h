@@ -75,6 +75,10 @@ long orc_collide(orc_sim* s, int shuffle);
 /* One CollisionsTA77S pass (collisionsTA77S.cpp:568-576 without its
  * random_sort): Takizuka-Abe pairs, then the per-cell velocity correction. */
 long orc_collide_ta77s(orc_sim* s, int shuffle);
+/* SpecieP's diagnostic maps (specieP.cpp:665-839): which 0 density, 1
+ * temperature, 2 energy, 3 momentum (3 grids); out holds (nr+4) x (nz+4)
+ * doubles per grid. */
+int orc_species_map(orc_sim* s, int sid, int which, double* out);
 
 /* Building blocks exported for known-answer tests. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

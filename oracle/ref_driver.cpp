@@ -294,6 +294,34 @@ long ref_collide_ta77s(void* h) {
   return pcg_ref_log::g_fatal ? -10 : 0;
 }
 
+// SpecieP's diagnostic maps (specieP.cpp:665-839): which 0 density, 1
+// temperature, 2 energy, 3 momentum (3 grids r, phi, z).
+int ref_species_map(void* h, int sid, int which, double* dst) {
+  RefSim* s = (RefSim*)h;
+  if (sid < 0 || sid >= (int)s->species.size()) return -1;
+  SpecieP* sp = s->species[sid];
+  pcg_ref_log::g_fatal = false;
+  std::vector<Grid<double>*> grids;
+  switch (which) {
+    case 0: sp->calc_density(); grids.push_back(&sp->density_map); break;
+    case 1: sp->calc_temperature(); grids.push_back(&sp->temperature_map); break;
+    case 2: sp->calc_energy(); grids.push_back(&sp->energy_map); break;
+    case 3:
+      sp->calc_momentum();
+      for (int c = 0; c < 3; ++c) grids.push_back(&sp->momentum_map[c]);
+      break;
+    default: return -1;
+  }
+  size_t off = 0;
+  for (Grid<double>* g : grids) {
+    double** a = g->get_grid();
+    for (unsigned i = 0; i < g->x_real_size; ++i)
+      std::memcpy(dst + off + (size_t)i * g->y_real_size, a[i], sizeof(double) * g->y_real_size);
+    off += (size_t)g->x_real_size * g->y_real_size;
+  }
+  return pcg_ref_log::g_fatal ? -10 : 0;
+}
+
 double ref_time(void* h) { return ((RefSim*)h)->time.current; }
 long ref_removed(void* h) { return (long)((RefSim*)h)->removed; }
 void ref_seed(unsigned seed) { math::random::gen.seed(seed); }

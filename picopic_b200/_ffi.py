@@ -88,6 +88,7 @@ SIGNATURES = {
     "pcg_cell_moments": (ctypes.c_int, [_H, _PD]),
     "pcg_set_collisions": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_scheme": (ctypes.c_int, [_H, ctypes.c_int]),
+    "pcg_species_map": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _PD]),
     "pcg_collide_expectation": (ctypes.c_int, [_H, _PD]),
     "pcg_cell_features": (ctypes.c_int, [_H, _PF, _PD]),
     "pcg_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),

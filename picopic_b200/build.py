@@ -37,6 +37,7 @@ UNITS = {
     "pcg_collide.cu": ["--fmad=false"],
     "pcg_mlp.cu": [],
     "pcg_learned.cu": ["--fmad=false"],
+    "pcg_maps.cu": ["--fmad=false"],
 }
 
 

@@ -20,6 +20,7 @@
 #include "pcg_f32.h"
 #include "pcg_init.h"
 #include "pcg_learned.h"
+#include "pcg_maps.h"
 #include "pcg_kernels.h"
 #include "pcg_yee.cuh"
 
@@ -49,6 +50,7 @@ struct Species {
   int *cell_r = nullptr, *cell_z = nullptr;
   // float layout
   SpeciesF32Buffers f32;
+  double* abs_map = nullptr;  // momentum_abs_map_w as the last energy map left it (pcg_species_map)
 };
 
 const char* kFieldNames[12] = {"E_r", "E_phi", "E_z", "H_r", "H_phi", "H_z",
@@ -68,6 +70,7 @@ struct pcg_handle {
   size_t f32_plane = 0;
   float4* recip32 = nullptr;      // radial reciprocal table of the float step
   uint64_t dead_dropped = 0;      // dead slots the float tile sorts dropped since the last compaction
+  double* map_work = nullptr;     // pcg_species_map: 4 scratch grids and 3 output grids
   uint64_t launches = 0;          // kernels launched by steps and stages
   double* diag = nullptr;         // node-value scratch of the diagnostics
   CollWork coll;                  // scratch of the collision passes
@@ -691,7 +694,9 @@ int pcg_destroy(pcg_handle* h) {
                     s.cell_r, s.cell_z};
     for (void* a : arrs) cudaFree(a);
     f32_free_species(s.f32);
+    cudaFree(s.abs_map);
   }
+  cudaFree(h->map_work);
   cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -968,6 +973,38 @@ int pcg_set_collisions(pcg_handle* h, int mode) {
   if (mode == PCG_COLLISIONS_LEARNED && !h->learned.model)
     return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
   h->collisions = mode;
+  return PCG_OK;
+}
+
+int pcg_species_map(pcg_handle* h, int slot, int which, double* out) {
+  if (!h || !out || slot < 0 || slot >= (int)h->sp.size() || which < PCG_MAP_DENSITY || which > PCG_MAP_MOMENTUM)
+    return PCG_ERR_ARG;
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  Species& s = h->sp[slot];
+  const size_t plane = (size_t)(h->g.nr + 4) * h->g.ld;
+  if (!h->map_work && (rc = dalloc(h, &h->map_work, 7 * plane)) != PCG_OK) return rc;
+  if (!s.abs_map) {
+    if ((rc = dalloc(h, &s.abs_map, plane)) != PCG_OK) return rc;
+    CUDA_TRY(h, cudaMemsetAsync(s.abs_map, 0, plane * sizeof(double), h->stream));
+  }
+  MapSpecies m;
+  m.n = s.n;
+  m.mass = s.mass;
+  if (is_f64(h)) {
+    m.r = s.r; m.z = s.z; m.vr = s.vr; m.vphi = s.vphi; m.vz = s.vz; m.w = s.w;
+  } else {
+    m.cell = s.f32.cell; m.off_r = s.f32.off_r; m.off_z = s.f32.off_z;
+    m.vr32 = s.f32.vr; m.vphi32 = s.f32.vphi; m.vz32 = s.f32.vz; m.w32 = s.f32.w;
+  }
+  double* dev_out = h->map_work + 4 * plane;
+  if (species_map(h->g, m, which, h->cfg.quirks == PCG_QUIRKS_FIXED, s.abs_map, h->map_work, dev_out,
+                  h->stream) != 0)
+    return fail(h, PCG_ERR_CUDA, "species map");
+  h->launches += 2;
+  const size_t count = (which == PCG_MAP_MOMENTUM ? 3 : 1) * plane;
+  CUDA_TRY(h, cudaMemcpyAsync(out, dev_out, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return PCG_OK;
 }
 

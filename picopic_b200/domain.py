@@ -207,6 +207,17 @@ class Domain:
         self._check(self.lib.pcg_set_collision_model(self.h, p.ctypes.data_as(pf), n.ctypes.data_as(pf)),
                     "pcg_set_collision_model")
 
+    MAPS = {"density": 0, "temperature": 1, "energy": 2, "momentum": 3}
+
+    def species_map(self, slot, which) -> np.ndarray:
+        """SpecieP::calc_<which> of species `slot` ("density", "temperature",
+        "energy" or "momentum"): a grid shaped like the fields, (3, ...) for
+        the momentum's r, phi, z."""
+        k = self.MAPS[which]
+        out = np.zeros((3 if k == 3 else 1,) + self.grid.shape)
+        self._check(self.lib.pcg_species_map(self.h, int(slot), k, _dp(out)), "pcg_species_map")
+        return out if k == 3 else out[0]
+
     def set_collision_scheme(self, scheme):
         """Binary operator of collide() and "binary" steps: "p12" (CollisionsP12,
         the default) or "ta77s" (CollisionsTA77S with its velocity correction)."""

@@ -90,6 +90,23 @@ def plasma_frequency(density, mass=1.0):
     return np.sqrt(density * 1.6e-19 ** 2 / (8.85e-12 * 9.1e-31 * mass))
 
 
+def map_particles(grid, n, seed, mass=1.0):
+    """Particles for the diagnostic maps: a quarter inside r <= dr/2, a
+    quarter in dr/2 < r <= dr (the three radial branches of the
+    reference's weighting), thermal speeds with a tenth above 5e7 m/s."""
+    rng = np.random.default_rng(seed)
+    r = grid.dr / 2 + rng.random(n) * (grid.radius - grid.dr)
+    q = n // 4
+    r[:q] = rng.random(q) * grid.dr / 2
+    r[q:2 * q] = grid.dr / 2 + rng.random(q) * grid.dr / 2
+    z = grid.dz / 2 + rng.random(n) * (grid.longitude - grid.dz)
+    v = rng.normal(size=(3, n)) * np.sqrt(1.6e-19 * 2.0 / (9.1e-31 * mass))
+    fast = rng.random(n) < 0.1
+    v[2, fast] = np.sign(rng.random(fast.sum()) - 0.5) * (6e7 + rng.random(fast.sum()) * 1e8)
+    w = rng.random(n) * 1e6 + 1e5
+    return (r, z, v[0], v[1], v[2], w)
+
+
 def random_fields(grid, seed, scale=1e3):
     rng = np.random.default_rng(seed + 7919)
     return {f: rng.normal(size=grid.shape) * scale for f in FIELDS}

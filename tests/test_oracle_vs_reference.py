@@ -121,3 +121,25 @@ def test_ta77s_collisions_bit_exact(ppc):
         for k in ("vr", "vphi", "vz"):
             np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
     assert np.abs(o.get_particles(0)["vz"] - before).max() > 0
+
+
+def test_species_maps_bit_exact():
+    """SpecieP::calc_density / calc_energy / calc_temperature / calc_momentum
+    over weight_cylindrical: bit-identical grids.  The temperature reads the
+    absolute-momentum map the last energy map left; before any, the
+    reference reads a grid it never initialised (undefined, not compared)."""
+    if not reference_available():
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    from tests.cases import map_particles
+    grid = small_grid(nr=12, nz=24, pml=False)
+    o, r = OracleSim(grid, quirks="reference"), RefSim(grid)
+    for sim in (o, r):
+        sim.add(ELECTRONS)
+        sim.add(IONS)
+        sim.set_particles(0, *map_particles(grid, 4000, 3))
+        sim.set_particles(1, *map_particles(grid, 3000, 4, mass=1836.0))
+    for which in ("density", "energy", "temperature", "momentum"):
+        for sid in (0, 1):
+            a, b = o.species_map(sid, which), r.species_map(sid, which)
+            assert np.abs(a).max() > 0, which
+            np.testing.assert_array_equal(a, b, err_msg=f"{which} species {sid}")
