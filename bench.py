@@ -273,6 +273,9 @@ def run_gpu(args):
     large = None
     if not args.no_large:
         large = run_large(args, local, barrier, allmax, allsum)
+    ensemble = None
+    if not args.no_ensemble and world == 1:
+        ensemble = run_ensemble(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w)
     if rank == 0:
@@ -295,6 +298,7 @@ def run_gpu(args):
             "e2e": e2e,
             "collisions": coll,
             "large": large,
+            "ensemble": ensemble,
             "accuracy": acc,
             "cpu_baseline": cpu,
             "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
@@ -379,6 +383,64 @@ def run_large(args, local, barrier, allmax, allsum):
                                       "learned_cell_fraction": learned / cells,
                                       "fallback_cell_fraction": fallback / cells}
     del d
+    torch.cuda.empty_cache()
+    return out
+
+
+# The batched configuration: 64 independent runs, nr ~ U{64..256}, nz ~
+# U{256..2048}, n = 1e17 m^-3, 20-50 macroparticles per cell per species,
+# each with the wakefield's 5 MeV Gaussian bunch at a density log-uniform in
+# 1e15..1e17 m^-3 (cells of 1e-4 m, dt 0.5 Courant, float path).
+ENSEMBLE = dict(name="ensemble of 64 runs: nr U{64..256}, nz U{256..2048}, n 1e17, 20-50 ppc/species e+p, "
+                     "5 MeV Gaussian bunch n_b log-uniform 1e15..1e17", runs=64, seed=99)
+
+
+def run_ensemble(args, local):
+    """The batched configuration through pcg_ensemble: particle-steps/s of K
+    steps of all runs issued from one host thread with the default tiling,
+    from 8 threads with the default tiling, and from 8 threads after the
+    autotuner's tiling, chosen on the whole ensemble (the device time of
+    each batch)."""
+    import torch
+    from picopic_b200.ensemble import Ensemble
+    rng = np.random.default_rng(ENSEMBLE["seed"])
+    nruns = 8 if args.small else ENSEMBLE["runs"]
+    runs, sizes = [], []
+    for k in range(nruns):
+        nr, nz, ppc = int(rng.integers(64, 257)), int(rng.integers(256, 2049)), int(rng.integers(20, 51))
+        nb = float(np.exp(rng.uniform(np.log(1e15), np.log(1e17))))
+        w = dict(WORKLOAD, nr=nr, nz=nz, ppc=ppc, beam_density=nb)
+        d, _, _, _ = make_domain(w, "f32", seed=5000 + k, device=local)
+        runs.append(d)
+        sizes.append((nr, nz, ppc))
+    k_steps = 5 if args.small else 20
+
+    def timed(ens):
+        p0 = sum(d.diag().particle_steps for d in runs)
+        ms = ens.step(k_steps)
+        p1 = sum(d.diag().particle_steps for d in runs)
+        return (p1 - p0) / (ms * 1e-3), ms / k_steps
+
+    one = Ensemble(runs, threads=1)
+    one.step(3)
+    v1, ms1 = timed(one)
+    one.close()
+    many = Ensemble(runs, threads=8)
+    many.step(2)
+    v8, ms8 = timed(many)
+    choices = many.autotune(trial_steps=3)
+    many.step(2)
+    vt, mst = timed(many)
+    many.close()
+    particles = sum(d.diag().particles for d in runs)
+    out = {"workload": ENSEMBLE["name"], "runs": nruns, "particles": int(particles),
+           "cells": int(sum(a * b for a, b, _ in sizes)), "steps": k_steps, "unit": UNIT,
+           "one_thread_default_tiling": {"value": v1, "ms_per_step": ms1},
+           "threads8_default_tiling": {"value": v8, "ms_per_step": ms8},
+           "threads8_autotuned": {"value": vt, "ms_per_step": mst},
+           "autotune_choice": {"target_blocks": choices[0], "times_particle_share": choices[1],
+                               "min_particles_per_block": choices[2]}}
+    del runs
     torch.cuda.empty_cache()
     return out
 
@@ -598,6 +660,7 @@ def main():
     ap.add_argument("--no-collisions", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -324,6 +324,38 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
 int pcg_cell_moments(pcg_handle* h, double* moments);
 int pcg_cell_features(pcg_handle* h, float* features, double* scale);
 
+/* Tiling of the float step (no reference counterpart: its particles are not
+ * tiled).  Species are re-sorted into 8 x 64-cell tiles at most every
+ * sort_interval steps (default 64; sooner when particles drift out of their
+ * tile's windows), and a sort spreads each occupied tile over enough blocks
+ * that about target_blocks blocks run (default 148 x 8), each with at least
+ * min_split particles (default 1024).  0 keeps a value; the next step
+ * re-sorts.  pcg_ensemble_autotune picks these per run. */
+int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_split);
+
+/* An ensemble: independent runs (handles, each with its own grid, species
+ * and stream; the batched configuration of many small runs) advanced
+ * together.  No reference counterpart: the reference runs one simulation
+ * per process.  pcg_ensemble_create groups handles it does not own (all on
+ * one device); pcg_ensemble_step advances every run by nsteps, the runs
+ * spread over `threads` host threads that each issue their runs' steps in
+ * turn, so that the GPU overlaps the runs' kernels and a run's tile sort
+ * (which waits for its own stream) holds up no other run; *device_ms (may
+ * be NULL) receives the device time from the first to the last of the
+ * batch's kernels (events on the runs' streams, joined on one stream).
+ * pcg_ensemble_autotune times trial_steps ensemble steps under each of six
+ * candidate tilings applied to every run (target blocks 1184, 148, 592 or
+ * 2368 per run, or 1184 or 4736 times the run's share of the ensemble's
+ * particles; 512 to 2048 particles per block at least), in context, with
+ * all runs on the GPU together, and keeps the fastest; *choice (may be
+ * NULL) receives its index.  It advances every run by 6 x (trial_steps + 1)
+ * steps. */
+typedef struct pcg_ensemble pcg_ensemble;
+int pcg_ensemble_create(pcg_handle* const* runs, int n, int threads, pcg_ensemble** out);
+int pcg_ensemble_step(pcg_ensemble* e, int nsteps, float* device_ms);
+int pcg_ensemble_autotune(pcg_ensemble* e, int trial_steps, int* choice);
+int pcg_ensemble_destroy(pcg_ensemble* e);
+
 /* SpecieP's diagnostic maps of species `slot` (specieP.cpp:665-839:
  * calc_density, calc_temperature, calc_energy, calc_momentum) into host
  * `out`: (nr+4) x (nz+4) doubles laid out as the fields, three such grids

@@ -89,6 +89,12 @@ SIGNATURES = {
     "pcg_set_collisions": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_scheme": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_species_map": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _PD]),
+    "pcg_set_tiling": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "pcg_ensemble_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "pcg_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    "pcg_ensemble_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "pcg_ensemble_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "pcg_collide_expectation": (ctypes.c_int, [_H, _PD]),
     "pcg_cell_features": (ctypes.c_int, [_H, _PF, _PD]),
     "pcg_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),

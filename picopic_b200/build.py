@@ -38,6 +38,7 @@ UNITS = {
     "pcg_mlp.cu": [],
     "pcg_learned.cu": ["--fmad=false"],
     "pcg_maps.cu": ["--fmad=false"],
+    "pcg_ensemble.cu": [],
 }
 
 

@@ -93,6 +93,7 @@ struct pcg_handle {
   // kernel timers: event pairs per class, recycled after each query
   TileGrid tiles{};       // float path: tile sort geometry
   int sort_interval = 64;  // float path: most steps between tile sorts
+  unsigned target_blocks = 148 * 8, min_split = 1024;  // float path: blocks per tile (pcg_set_tiling)
   bool timers = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
@@ -574,6 +575,8 @@ int fused_step(pcg_handle* h) {
     st.status = h->d_status;
     st.tiles = h->tiles;
     st.sort_interval = h->sort_interval;
+    st.target_blocks = h->target_blocks;
+    st.min_split = h->min_split;
     for (size_t t = 0; t < h->sp.size(); ++t) {
       Species& s = h->sp[t];
       const size_t n0 = s.n;
@@ -973,6 +976,15 @@ int pcg_set_collisions(pcg_handle* h, int mode) {
   if (mode == PCG_COLLISIONS_LEARNED && !h->learned.model)
     return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
   h->collisions = mode;
+  return PCG_OK;
+}
+
+int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_split) {
+  if (!h || sort_interval < 0 || target_blocks < 0 || min_split < 0) return PCG_ERR_ARG;
+  if (sort_interval) h->sort_interval = sort_interval;
+  if (target_blocks) h->target_blocks = (unsigned)target_blocks;
+  if (min_split) h->min_split = (unsigned)min_split;
+  for (Species& s : h->sp) s.f32.steps_since_sort = 1 << 30;  // the next step sorts with these
   return PCG_OK;
 }
 

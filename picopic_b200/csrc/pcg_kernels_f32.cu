@@ -253,11 +253,12 @@ void swap_buffers(SpeciesF32Buffers& b) {
   std::swap(b.id, b.id2);
 }
 
-// Blocks per tile for the step: enough to fill the GPU when few tiles are
-// occupied (a narrow beam), each with at least kMinSplitParticles particles.
-constexpr unsigned kTargetBlocks = 148 * 8, kMinSplitParticles = 4 * kThreads;
+// Blocks per tile for the step: enough that about target_blocks blocks run
+// when few tiles are occupied (a narrow beam), each with at least min_split
+// particles (F32Step; the defaults 148 x 8 and 1024 suit one run on the GPU).
 
-int tile_sort(const TileGrid& tg, SpeciesF32Buffers& b, size_t* n, cudaStream_t s) {
+int tile_sort(const TileGrid& tg, unsigned target_blocks, unsigned min_split, SpeciesF32Buffers& b,
+              size_t* n, cudaStream_t s) {
   const size_t nt = (size_t)tg.ntiles;
   unsigned* counts = b.tile_cursor;
   cudaMemsetAsync(b.cell_count, 0, nt * kTileCells * sizeof(unsigned), s);
@@ -276,8 +277,8 @@ int tile_sort(const TileGrid& tg, SpeciesF32Buffers& b, size_t* n, cudaStream_t 
   const unsigned kept = b.host_info[0], largest = b.host_info[1], occupied = b.host_info[2];
   unsigned splits = 1;
   if (occupied) {
-    splits = std::max(1u, std::min((kTargetBlocks + occupied - 1) / occupied,
-                                   (largest + kMinSplitParticles - 1) / kMinSplitParticles));
+    splits = std::max(1u, std::min((target_blocks + occupied - 1) / occupied,
+                                   (largest + min_split - 1) / min_split));
     splits = std::min(splits, 65535u);
   }
   b.splits = (int)splits;
@@ -433,7 +434,8 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   const size_t drifted = *(volatile unsigned*)b.drift_host;  // a recent step's count (a hint)
   if (b.sorted_n == 0 || b.steps_since_sort >= st.sort_interval || (*n - b.sorted_n) * 4 > *n ||
       drifted * 100 > b.sorted_n) {
-    if (tile_sort(st.tiles, b, n, s) != 0) return -1;  // synchronises: no copy of drift is pending
+    // synchronises: no copy of drift is pending
+    if (tile_sort(st.tiles, st.target_blocks, st.min_split, b, n, s) != 0) return -1;
     *b.drift_host = 0;
   }
   cudaMemsetAsync(b.drift, 0, sizeof(unsigned), s);
