@@ -328,7 +328,7 @@ int pcg_cell_features(pcg_handle* h, float* features, double* scale);
  * tiled).  Species are re-sorted into 8 x 64-cell tiles at most every
  * sort_interval steps (default 64; sooner when particles drift out of their
  * tile's windows), and a sort spreads each occupied tile over enough blocks
- * that about target_blocks blocks run (default 148 x 8), each with at least
+ * that about target_blocks blocks run (default 148 x 16), each with at least
  * min_split particles (default 1024).  0 keeps a value; the next step
  * re-sorts.  pcg_ensemble_autotune picks these per run. */
 int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_split);

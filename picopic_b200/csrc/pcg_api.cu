@@ -93,7 +93,11 @@ struct pcg_handle {
   // kernel timers: event pairs per class, recycled after each query
   TileGrid tiles{};       // float path: tile sort geometry
   int sort_interval = 64;  // float path: most steps between tile sorts
-  unsigned target_blocks = 148 * 8, min_split = 1024;  // float path: blocks per tile (pcg_set_tiling)
+  // float path: blocks per tile (pcg_set_tiling).  148 x 16 blocks: with
+  // 4 resident blocks per SM one block per occupied tile of a 256 x 4096
+  // grid (2048 tiles) runs 3.5 waves and leaves the last half empty; two
+  // per tile run 6.9
+  unsigned target_blocks = 148 * 16, min_split = 1024;
   bool timers = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;

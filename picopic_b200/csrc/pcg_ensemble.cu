@@ -30,8 +30,8 @@ namespace {
 
 // The autotuner's candidates: target blocks and minimum particles per block
 // of each run, from the run's share f of the ensemble's particles.  A run
-// alone fills the GPU with about 148 x 8 blocks; in an ensemble that many
-// per run oversubscribe it, so some candidates scale the target by f.
+// alone fills the GPU with one to two thousand blocks; in an ensemble that
+// many per run oversubscribe it, so some candidates scale the target by f.
 struct Tiling {
   double blocks;  // target blocks (absolute, or times f when shared)
   bool shared;

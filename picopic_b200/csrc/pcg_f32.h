@@ -77,7 +77,7 @@ struct F32Step {
   int sort_interval;  // most steps between tile sorts
   // a sort splits each occupied tile over enough blocks that about
   // target_blocks run, each with at least min_split particles
-  unsigned target_blocks = 148 * 8, min_split = 1024;
+  unsigned target_blocks = 148 * 16, min_split = 1024;
 };
 
 __host__ __device__ __forceinline__ int pack_cell(int ci, int ck) {

@@ -255,7 +255,7 @@ void swap_buffers(SpeciesF32Buffers& b) {
 
 // Blocks per tile for the step: enough that about target_blocks blocks run
 // when few tiles are occupied (a narrow beam), each with at least min_split
-// particles (F32Step; the defaults 148 x 8 and 1024 suit one run on the GPU).
+// particles (F32Step; the defaults 148 x 16 and 1024 suit one run on the GPU).
 
 int tile_sort(const TileGrid& tg, unsigned target_blocks, unsigned min_split, SpeciesF32Buffers& b,
               size_t* n, cudaStream_t s) {

@@ -207,6 +207,11 @@ class Domain:
         self._check(self.lib.pcg_set_collision_model(self.h, p.ctypes.data_as(pf), n.ctypes.data_as(pf)),
                     "pcg_set_collision_model")
 
+    def set_tiling(self, sort_interval=0, target_blocks=0, min_split=0):
+        """Tiling of the float step (pcg_set_tiling; 0 keeps a value)."""
+        self._check(self.lib.pcg_set_tiling(self.h, int(sort_interval), int(target_blocks), int(min_split)),
+                    "pcg_set_tiling")
+
     MAPS = {"density": 0, "temperature": 1, "energy": 2, "momentum": 3}
 
     def species_map(self, slot, which) -> np.ndarray:
