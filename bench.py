@@ -180,38 +180,16 @@ def timed_steps(d, K, stream_ptr):
 
 def run_gpu(args):
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    from picopic_b200.replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def allmax(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def allsum(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    rep = Replicas("nccl")
+    rank, world = rep.rank, rep.world
+    barrier, allmax, allsum = rep.barrier, rep.allmax, rep.allsum
 
     w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
     w = scaled(w, nz=args.nz, ppc=args.ppc)
-    d, slots, g, vb = make_domain(w, "f32", seed=1234 + 7919 * rank, device=local)
+    d, slots, g, vb = make_domain(w, "f32", seed=rep.seed(1234), device=local)
     d.step(args.warmup)
     d.synchronize()
     diag0 = d.diag()
@@ -249,7 +227,7 @@ def run_gpu(args):
     if not args.no_f64:
         del d
         torch.cuda.empty_cache()
-        d64, _, _, _ = make_domain(w, "f64", seed=1234 + 7919 * rank, device=local)
+        d64, _, _, _ = make_domain(w, "f64", seed=rep.seed(1234), device=local)
         d64.step(max(2, args.warmup // 2))
         d64.synchronize()
         q0 = d64.diag().particle_steps
@@ -304,8 +282,7 @@ def run_gpu(args):
             "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
         }
         print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def run_accuracy(w, args, local):

@@ -333,6 +333,16 @@ int pcg_cell_features(pcg_handle* h, float* features, double* scale);
  * re-sorts.  pcg_ensemble_autotune picks these per run. */
 int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_split);
 
+/* Sort species `slot` of a float-layout handle into its tiles now (as a
+ * step does when its particles have drifted; dead slots are dropped) and
+ * report the result: counts[c] (host, nr x nz, cell c = i * nz + k) the
+ * particles the sorted tiles hold in cell c, *misplaced those whose cell is
+ * outside their tile (0 unless the sort is wrong).  The reference groups
+ * particles per cell only for collisions (Collisions::sort_to_cells,
+ * collisions.cpp:87-108); this is the float step's replacement, exposed
+ * for checking.  PCG_ERR_UNSUPPORTED for the double layout. */
+int pcg_tile_sort(pcg_handle* h, int slot, unsigned* counts, unsigned long long* misplaced);
+
 /* An ensemble: independent runs (handles, each with its own grid, species
  * and stream; the batched configuration of many small runs) advanced
  * together.  No reference counterpart: the reference runs one simulation

@@ -90,6 +90,8 @@ SIGNATURES = {
     "pcg_set_collision_scheme": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_species_map": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _PD]),
     "pcg_set_tiling": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "pcg_tile_sort": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(ctypes.c_uint),
+                                     ctypes.POINTER(ctypes.c_ulonglong)]),
     "pcg_ensemble_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "pcg_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),

@@ -992,6 +992,34 @@ int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_
   return PCG_OK;
 }
 
+int pcg_tile_sort(pcg_handle* h, int slot, unsigned* counts, unsigned long long* misplaced) {
+  if (!h || !counts || !misplaced || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  if (is_f64(h)) return fail(h, PCG_ERR_UNSUPPORTED, "the tile sort belongs to the float layout");
+  int rc = check_status(h);
+  if (rc != PCG_OK) return rc;
+  Species& s = h->sp[slot];
+  const size_t cells = (size_t)h->g.nr * h->g.nz;
+  unsigned* dc = nullptr;
+  unsigned long long* dm = nullptr;
+  if ((rc = dalloc(h, &dc, cells)) != PCG_OK) return rc;
+  if ((rc = dalloc(h, &dm, 1)) != PCG_OK) { cudaFree(dc); return rc; }
+  const size_t n0 = s.n;
+  const uint64_t k0 = s.f32.launches;
+  if (f32_tile_check(h->tiles, h->target_blocks, h->min_split, h->g.nr, h->g.nz, s.f32, &s.n, dc, dm,
+                     h->stream) == 0) {
+    h->dead_dropped += n0 - s.n;
+    h->launches += s.f32.launches - k0;
+    cudaMemcpyAsync(counts, dc, cells * sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(misplaced, dm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream);
+    rc = cudaStreamSynchronize(h->stream) == cudaSuccess ? PCG_OK : fail(h, PCG_ERR_CUDA, "tile sort");
+  } else {
+    rc = fail(h, PCG_ERR_CUDA, "tile sort");
+  }
+  cudaFree(dc);
+  cudaFree(dm);
+  return rc;
+}
+
 int pcg_species_map(pcg_handle* h, int slot, int which, double* out) {
   if (!h || !out || slot < 0 || slot >= (int)h->sp.size() || which < PCG_MAP_DENSITY || which > PCG_MAP_MOMENTUM)
     return PCG_ERR_ARG;

@@ -88,6 +88,12 @@ __host__ __device__ __forceinline__ int cell_z_of(int cell) { return cell >> 16;
 constexpr int kDeadCell = (int)0x80000000u;
 
 TileGrid f32_tile_grid(const GridGeom& g);
+// A tile sort of the species now, then per cell (nr x nz, device) the
+// particles the sorted tiles hold and, in *misplaced (device), those whose
+// cell is outside their tile.
+int f32_tile_check(const TileGrid& tg, unsigned target_blocks, unsigned min_split, int nr, int nz,
+                   SpeciesF32Buffers& b, size_t* n, unsigned* counts, unsigned long long* misplaced,
+                   cudaStream_t s);
 int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg);
 void f32_free_species(SpeciesF32Buffers& b);
 void f32_launch_yee_e(const YeeArgs<float>& a, cudaStream_t s);

@@ -346,6 +346,40 @@ __global__ void kinetic_kernel(SpeciesF32Buffers b, size_t n, double mass, doubl
 
 }  // namespace
 
+namespace {
+
+// Per tile t, the particles [tile_start[t], tile_start[t+1]): each counted
+// in its cell, and counted as misplaced when its cell is not in tile t (or
+// not in the grid, or the slot is dead).
+__global__ void tile_check_kernel(TileGrid tg, SpeciesF32Buffers b, int nr, int nz, unsigned* counts,
+                                  unsigned long long* misplaced) {
+  const int t = blockIdx.x;
+  for (unsigned p = b.tile_start[t] + threadIdx.x; p < b.tile_start[t + 1]; p += blockDim.x) {
+    const int c = b.cell[p];
+    const int ci = cell_r_of(c), ck = cell_z_of(c);
+    if (c < 0 || ci < 0 || ck < 0 || ci >= nr || ck >= nz) {
+      atomicAdd(misplaced, 1ull);
+      continue;
+    }
+    if ((ci / tg.tr) * tg.ntz + ck / tg.tz != t) atomicAdd(misplaced, 1ull);
+    atomicAdd(counts + (size_t)ci * nz + ck, 1u);
+  }
+}
+
+}  // namespace
+
+int f32_tile_check(const TileGrid& tg, unsigned target_blocks, unsigned min_split, int nr, int nz,
+                   SpeciesF32Buffers& b, size_t* n, unsigned* counts, unsigned long long* misplaced,
+                   cudaStream_t s) {
+  if (tile_sort(tg, target_blocks, min_split, b, n, s) != 0) return -1;
+  *b.drift_host = 0;
+  cudaMemsetAsync(counts, 0, (size_t)nr * nz * sizeof(unsigned), s);
+  cudaMemsetAsync(misplaced, 0, sizeof(unsigned long long), s);
+  tile_check_kernel<<<(unsigned)tg.ntiles, kThreads, 0, s>>>(tg, b, nr, nz, counts, misplaced);
+  b.launches += 1;
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 TileGrid f32_tile_grid(const GridGeom& g) {
   TileGrid t;
   t.tr = kTileR;  // grids smaller than a tile get one partly empty tile

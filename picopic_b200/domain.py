@@ -207,6 +207,16 @@ class Domain:
         self._check(self.lib.pcg_set_collision_model(self.h, p.ctypes.data_as(pf), n.ctypes.data_as(pf)),
                     "pcg_set_collision_model")
 
+    def tile_sort(self, slot):
+        """Sort species `slot` into its tiles now (float layout); returns the
+        per-cell counts the sorted tiles hold (nr, nz) and how many
+        particles sit outside their tile."""
+        counts = np.zeros((self.grid.nr, self.grid.nz), dtype=np.uint32)
+        mis = ctypes.c_ulonglong(0)
+        self._check(self.lib.pcg_tile_sort(self.h, int(slot), counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)),
+                                           ctypes.byref(mis)), "pcg_tile_sort")
+        return counts, int(mis.value)
+
     def set_tiling(self, sort_interval=0, target_blocks=0, min_split=0):
         """Tiling of the float step (pcg_set_tiling; 0 keeps a value)."""
         self._check(self.lib.pcg_set_tiling(self.h, int(sort_interval), int(target_blocks), int(min_split)),
