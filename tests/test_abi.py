@@ -42,3 +42,23 @@ def test_missing_library_fails_loudly(tmp_path):
             _ffi.load(str(tmp_path / "libpcg.so"))
     finally:
         _ffi._lib = saved
+
+
+def test_null_handles_are_rejected_without_a_device():
+    """Every entry point checks its handle and pointers before any device
+    call: a null handle returns PCG_ERR_ARG (-1), also here without a GPU."""
+    lib = _ffi.load()
+    null = None
+    calls = [
+        ("pcg_step", (null, 1)), ("pcg_collide", (null, null)), ("pcg_diag", (null, null)),
+        ("pcg_set_tiling", (null, 0, 0, 0)), ("pcg_tile_sort", (null, 0, null, null)),
+        ("pcg_species_map", (null, 0, 0, null)), ("pcg_set_collision_scheme", (null, 0)),
+        ("pcg_set_collisions", (null, 0)), ("pcg_collide_learned", (null, null, null)),
+        ("pcg_count", (null, 0, null)), ("pcg_node_charge", (null, null)), ("pcg_stage", (null, 0)),
+        ("pcg_synchronize", (null,)), ("pcg_get_stream", (null, null)), ("pcg_set_field", (null, 0, null)),
+        ("pcg_export_field", (null, 0, null)), ("pcg_ensemble_create", (null, 0, 1, null)),
+        ("pcg_ensemble_step", (null, 1, null)), ("pcg_ensemble_autotune", (null, 1, null)),
+        ("pcg_ensemble_destroy", (null,)),
+    ]
+    for name, args in calls:
+        assert getattr(lib, name)(*args) == -1, name
