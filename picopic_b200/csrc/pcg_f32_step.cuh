@@ -787,9 +787,16 @@ static_assert((6 * kFWR * kFWZ + 3 * kJWR * kJWZ) % 4 == 0, "the table rows need
 // the fields around the tile and deposit into a shared current window that
 // is added to the global grid once at the end.  Particles that drifted
 // beyond the windows use the global grid.
-template <int CUR>
-__global__ void __launch_bounds__(kThreads, 4) step_tiled_kernel(StepArgs a, SpeciesF32Buffers b,
+// PUSH, BEAM, FIX >= 0 fix a.pusher, a.is_beam, a.fixed at compile time
+// (the local copy's constant fields fold every test of them away); -1
+// leaves them to the arguments.
+template <int CUR, int PUSH = -1, int BEAM = -1, int FIX = -1>
+__global__ void __launch_bounds__(kThreads, 4) step_tiled_kernel(StepArgs args, SpeciesF32Buffers b,
                                                                  TileGrid tg) {
+  StepArgs a = args;
+  if (PUSH >= 0) a.pusher = PUSH;
+  if (BEAM >= 0) a.is_beam = BEAM;
+  if (FIX >= 0) a.fixed = FIX;
   extern __shared__ float smem[];
   const int t = blockIdx.x;
   // blockIdx.y of gridDim.y blocks sharing the tile takes every gridDim.y-th run of blockDim.x

@@ -477,10 +477,15 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   const TileGrid& tg = st.tiles;
   if (b.sorted_n) {
     const size_t smem = f32::kTileSmemBytes;
+    const dim3 grid(tg.ntiles, b.splits);
     if (st.current == PCG_CURRENT_ZIGZAG)
-      f32::step_tiled_kernel<1><<<dim3(tg.ntiles, b.splits), f32::kThreads, smem, s>>>(a, b, tg);
+      f32::step_tiled_kernel<1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam && st.fixed)  // the plasma of the
+      f32::step_tiled_kernel<0, PCG_PUSHER_BORIS_RELATIVISTIC, 0, 1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam)               // common runs
+      f32::step_tiled_kernel<0, PCG_PUSHER_BORIS_RELATIVISTIC, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else
-      f32::step_tiled_kernel<0><<<dim3(tg.ntiles, b.splits), f32::kThreads, smem, s>>>(a, b, tg);
+      f32::step_tiled_kernel<0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
   }
   if (*n > b.sorted_n) {
     const unsigned nb = blocks_for(*n - b.sorted_n);
