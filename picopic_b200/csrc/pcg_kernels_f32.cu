@@ -478,7 +478,9 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   if (b.sorted_n) {
     const size_t smem = f32::kTileSmemBytes;
     const dim3 grid(tg.ntiles, b.splits);
-    if (st.current == PCG_CURRENT_ZIGZAG)
+    if (st.current == PCG_CURRENT_ZIGZAG && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed)
+      f32::step_tiled_kernel<1, PCG_PUSHER_VAY, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.current == PCG_CURRENT_ZIGZAG)
       f32::step_tiled_kernel<1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam && st.fixed)  // the plasma of the
       f32::step_tiled_kernel<0, PCG_PUSHER_BORIS_RELATIVISTIC, 0, 1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
