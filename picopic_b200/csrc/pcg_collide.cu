@@ -53,11 +53,17 @@ inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kT
 struct SpeciesTable {
   CollSpecies s[kCollMaxSpecies];
   int n;
-  double4* stage[2];  // the staged lists (entries referenced as kStaged | list << 40 | position)
 };
 
 constexpr unsigned long long kStaged = 1ull << 63;
 constexpr unsigned long long kRefMask = (1ull << 40) - 1;
+
+// The staged lists alone: what the moments, pair and correction kernels
+// read and write (their references are all staged), so that they index no
+// species table at run time.
+struct Staged {
+  double4* stage[2];
+};
 
 // std::isnormal: neither zero, subnormal, infinite nor NaN
 __device__ __forceinline__ bool normal(double x) {
@@ -131,16 +137,11 @@ __global__ void shuffle_kernel(size_t cells, const unsigned* start, const unsign
 // ---------------------------------------------------------------------------
 // accessors
 
+// A particle of the lists before staging (reference = species << 40 | slot).
 __device__ __forceinline__ void load_v(const SpeciesTable& tab, unsigned long long ref, double v[3],
                                        double* w) {
-  if (ref & kStaged) {
-    const double4 e = tab.stage[(ref >> 40) & 1][ref & kRefMask];
-    v[0] = e.x; v[1] = e.y; v[2] = e.z;
-    *w = e.w;
-    return;
-  }
   const CollSpecies& sp = tab.s[ref >> 40];
-  const size_t j = ref & ((1ull << 40) - 1);
+  const size_t j = ref & kRefMask;
   if (sp.vr64) {
     v[0] = sp.vr64[j]; v[1] = sp.vphi64[j]; v[2] = sp.vz64[j];
     *w = sp.w64[j];
@@ -150,32 +151,30 @@ __device__ __forceinline__ void load_v(const SpeciesTable& tab, unsigned long lo
   }
 }
 
-// 0 for the electron list, 1 for the ion list
-__device__ __forceinline__ int list_of(const SpeciesTable& tab, unsigned long long ref) {
-  return (ref & kStaged) ? (int)((ref >> 40) & 1) : tab.s[ref >> 40].is_ion;
-}
-
-__device__ __forceinline__ double load_w(const SpeciesTable& tab, unsigned long long ref) {
-  if (ref & kStaged) return tab.stage[(ref >> 40) & 1][ref & kRefMask].w;
-  const CollSpecies& sp = tab.s[ref >> 40];
-  const size_t j = ref & ((1ull << 40) - 1);
-  return sp.w64 ? sp.w64[j] : (double)sp.w32[j];
-}
-
 __device__ __forceinline__ void store_v(const SpeciesTable& tab, unsigned long long ref, const double v[3]) {
-  if (ref & kStaged) {
-    double4* e = tab.stage[(ref >> 40) & 1] + (ref & kRefMask);
-    e->x = v[0]; e->y = v[1]; e->z = v[2];
-    return;
-  }
   const CollSpecies& sp = tab.s[ref >> 40];
-  const size_t j = ref & ((1ull << 40) - 1);
+  const size_t j = ref & kRefMask;
   if (sp.vr64) {
     sp.vr64[j] = v[0]; sp.vphi64[j] = v[1]; sp.vz64[j] = v[2];
   } else {
     sp.vr32[j] = (float)v[0]; sp.vphi32[j] = (float)v[1]; sp.vz32[j] = (float)v[2];
   }
 }
+
+// A staged entry (reference = kStaged | list << 40 | position; list 1 = ions).
+__device__ __forceinline__ void load_v(const Staged& L, unsigned long long ref, double v[3], double* w) {
+  const double4 e = L.stage[(ref >> 40) & 1][ref & kRefMask];
+  v[0] = e.x; v[1] = e.y; v[2] = e.z;
+  *w = e.w;
+}
+__device__ __forceinline__ double load_w(const Staged& L, unsigned long long ref) {
+  return L.stage[(ref >> 40) & 1][ref & kRefMask].w;
+}
+__device__ __forceinline__ void store_v(const Staged& L, unsigned long long ref, const double v[3]) {
+  double4* e = L.stage[(ref >> 40) & 1] + (ref & kRefMask);
+  e->x = v[0]; e->y = v[1]; e->z = v[2];
+}
+__device__ __forceinline__ int list_of(const Staged&, unsigned long long ref) { return (int)((ref >> 40) & 1); }
 
 // 3b. staging: entry q of list `list` is copied to stage[q] and referenced
 // by staged[q]; the write-back stores the (possibly scattered) velocities
@@ -203,7 +202,7 @@ __global__ void unstage_kernel(SpeciesTable tab, const unsigned long long* refs,
 // ---------------------------------------------------------------------------
 // 4. per-cell moments (collisions.cpp:169-221, 123-156)
 
-__global__ void moments_kernel(GridGeom g, SpeciesTable tab, CollParams p, const unsigned* st_e,
+__global__ void moments_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
                                const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                const unsigned* n_i, const unsigned long long* li, double* mom,
                                int* row_stop, double* totals) {
@@ -270,7 +269,7 @@ __device__ __forceinline__ bool lorenz(double v2, double* g) {
 }
 
 struct PairCtx {
-  const SpeciesTable* tab;
+  const Staged* tab;
   const CollParams* p;
   uint32_t cell;
   uint32_t m;      // collision number in the cell
@@ -569,7 +568,7 @@ __device__ void ta77s_single(PairCtx& x, double m_real_a, double m_real_b, doubl
 // (sum w, sum w m v, sum w m v^2/2) collected before the pass.  The
 // reference takes |alpha| for alpha < 0 and 1 for alpha == 0; the fixed
 // mode leaves such a list as it is.
-__device__ void ta77s_correct(const SpeciesTable& tab, const unsigned long long* L, unsigned n, double mass,
+__device__ void ta77s_correct(const Staged& tab, const unsigned long long* L, unsigned n, double mass,
                               const double* t, int fixed) {
   double m3[3] = {0, 0, 0}, e_new = 0, v[3], w;
   for (unsigned q = 0; q < n; ++q) {
@@ -605,7 +604,7 @@ __device__ void ta77s_correct(const SpeciesTable& tab, const unsigned long long*
   }
 }
 
-__global__ void ta77s_correct_kernel(GridGeom g, SpeciesTable tab, CollParams p, const unsigned* st_e,
+__global__ void ta77s_correct_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
                                      const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                      const unsigned* n_i, const unsigned long long* li, const double* totals) {
   const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -618,7 +617,7 @@ __global__ void ta77s_correct_kernel(GridGeom g, SpeciesTable tab, CollParams p,
 // ---------------------------------------------------------------------------
 // 5. the per-cell pairing sequence (collisionsP12.cpp:338-548)
 
-__global__ void collide_kernel(GridGeom g, SpeciesTable tab, CollParams p, const unsigned* st_e,
+__global__ void collide_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
                                const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                const unsigned* n_i, const unsigned long long* li, const double* mom,
                                const int* row_stop, unsigned long long* calls) {
@@ -796,18 +795,17 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
       w.launches += 2;  // and its write-back
     }
   }
-  tab.stage[0] = w.stage[0];
-  tab.stage[1] = w.stage[1];
+  const Staged staged{{w.stage[0], w.stage[1]}};
   // 0x7f7f7f7f in every row: no stop unless a non-normal cell sets one
   cudaMemsetAsync(w.row_stop, 0x7f, (size_t)g.nr * sizeof(int), s);
-  moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
+  moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                         w.start[1], w.count[1], w.keys2[1], w.moments,
                                                         w.row_stop, p.scheme == 1 ? w.totals : nullptr);
-  collide_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
+  collide_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                         w.start[1], w.count[1], w.keys2[1], w.moments,
                                                         w.row_stop, w.calls);
   if (p.scheme == 1) {
-    ta77s_correct_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, tab, p, w.start[0], w.count[0], w.keys2[0],
+    ta77s_correct_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                                 w.start[1], w.count[1], w.keys2[1], w.totals);
     ++w.launches;
   }
