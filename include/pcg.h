@@ -287,6 +287,14 @@ int pcg_mlp_destroy(pcg_mlp* m);
 int pcg_mlp_get_params(pcg_mlp* m, float* params);
 int pcg_mlp_set_params(pcg_mlp* m, const float* params);
 int pcg_mlp_forward(pcg_mlp* m, const float* x, size_t rows, float* y);
+/* The same forward pass on the fifth-generation tensor cores (tcgen05.mma,
+ * accumulators in tensor memory, 128 rows per CTA; no reference
+ * counterpart): the same BF16 operands and FP32 accumulation, so outputs
+ * agree with pcg_mlp_forward to the order of the FP32 sums.  *device_ms
+ * (may be NULL) receives the kernel's device time.  PCG_ERR_TIMEOUT if a
+ * wait for the tensor cores timed out (the kernel then stops and frees its
+ * tensor memory). */
+int pcg_mlp_forward_tc(pcg_mlp* m, const float* x, size_t rows, float* y, float* device_ms);
 int pcg_mlp_gradient(pcg_mlp* m, const float* x, const float* t, size_t rows, float* grad, float* loss);
 int pcg_mlp_set_data(pcg_mlp* m, const float* x, const float* t, size_t rows);
 int pcg_mlp_train(pcg_mlp* m, int steps, int batch, float lr, float* last_loss);

@@ -104,6 +104,7 @@ SIGNATURES = {
     "pcg_mlp_get_params": (ctypes.c_int, [_H, _PF]),
     "pcg_mlp_set_params": (ctypes.c_int, [_H, _PF]),
     "pcg_mlp_forward": (ctypes.c_int, [_H, _PF, ctypes.c_size_t, _PF]),
+    "pcg_mlp_forward_tc": (ctypes.c_int, [_H, _PF, ctypes.c_size_t, _PF, _PF]),
     "pcg_mlp_gradient": (ctypes.c_int, [_H, _PF, _PF, ctypes.c_size_t, _PF, _PF]),
     "pcg_mlp_set_data": (ctypes.c_int, [_H, _PF, _PF, ctypes.c_size_t]),
     "pcg_mlp_train": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_float, _PF]),

@@ -21,6 +21,8 @@
 // cell's thermal energy sum_s W_s sum_a T_s,a is unchanged, and every
 // particle of the cell moves to v_a' = u_a + (v_a - u_a) sqrt(T'_a / T_a):
 // the species' momentum and the new second moments hold exactly in FP64.
+// The network itself runs on tcgen05 (pcg_mlp_tc.cuh) inside the per-cell
+// kernel; training keeps the mma.sync kernels of pcg_mlp.cu.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -31,6 +33,7 @@
 #include "pcg_f32.h"
 #include "pcg_learned.h"
 #include "pcg_mlp.cuh"
+#include "pcg_mlp_tc.cuh"
 
 namespace pcg {
 
@@ -166,92 +169,88 @@ __global__ void features_kernel(GridGeom g, LearnedPhys ph, const double* mom, f
 }
 
 struct LearnSmem {
-  double st[mlp::kRowsPerBlock][kStateWords];
-  float y[mlp::kRowsPerBlock][mlp::kOutPad];
-  mlp::FwdSmem f;
-  unsigned char state[mlp::kRowsPerBlock];  // 0 none, 1 learned, 2 fallback
+  mlp::tc::Smem t;  // weights, operand tiles, mbarrier and TMEM address of the tcgen05 MLP
+  double st[mlp::tc::kRows][kStateWords];
   unsigned long long n_learned, n_fallback;
 };
 
-// Blocks take tiles of 64 cells in turn (the weights are staged in shared
-// memory once per block): features (one thread per cell), the MLP on the
-// tensor cores (a warp per 16 cells), then the new temperatures and the
-// transform of each cell.
-__global__ void __launch_bounds__(mlp::kMlpThreads) learned_cells_kernel(GridGeom g, LearnedPhys ph,
-                                                                         const double* mom, const float* P,
-                                                                         LearnedNorm nm, double* xform,
-                                                                         unsigned char* flag,
-                                                                         unsigned long long* count) {
+// Blocks take tiles of 128 cells in turn (the weights are staged in shared
+// memory once per block), thread r the tile's cell r: its features, the MLP
+// on the fifth-generation tensor cores (tcgen05.mma into tensor memory,
+// pcg_mlp_tc.cuh), then the cell's new temperatures and transform.  A wait
+// for the tensor cores that times out sets count[2] and ends the block.
+__global__ void __launch_bounds__(mlp::tc::kThreads) learned_cells_kernel(GridGeom g, LearnedPhys ph,
+                                                                          const double* mom, const float* P,
+                                                                          LearnedNorm nm, double* xform,
+                                                                          unsigned char* flag,
+                                                                          unsigned long long* count) {
   extern __shared__ __align__(16) unsigned char raw[];
-  LearnSmem& sm = *reinterpret_cast<LearnSmem*>(raw);
+  LearnSmem& sm = *reinterpret_cast<LearnSmem*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
   const size_t cells = (size_t)g.nr * g.nz;
-  const size_t tiles = (cells + mlp::kRowsPerBlock - 1) / mlp::kRowsPerBlock;
-  mlp::load_forward_weights(sm.f.W1t, sm.f.W2t, sm.f.W3t, P);
-  mlp::load_biases(sm.f, P);
-  if (threadIdx.x == 0) { sm.n_learned = 0; sm.n_fallback = 0; }
+  const size_t tiles = (cells + mlp::tc::kRows - 1) / mlp::tc::kRows;
+  const int r = threadIdx.x;
+  mlp::tc::load_weights(sm.t, P);
+  if (r == 0) { sm.n_learned = 0; sm.n_fallback = 0; }
+  mlp::tc::begin(sm.t);
+  uint32_t phase = 0;
+  unsigned char* a1 = reinterpret_cast<unsigned char*>(sm.t.A1);
   for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const size_t c0 = tile * mlp::kRowsPerBlock;
-    __syncthreads();  // the previous tile is done with X, y and the state
-    if (threadIdx.x < mlp::kRowsPerBlock) {
-      const int r = threadIdx.x;
-      const size_t c = c0 + r;
-      float x[kFeatures];
-      unsigned char stt = 0;
-      if (c < cells && cell_features(g, ph, mom + c * kMomWords, (int)(c / g.nz), sm.st[r], x)) {
-        stt = 1;
-        for (int k = 0; k < kFeatures; ++k) {
-          const float span = nm.x_hi[k] - nm.x_lo[k];
-          if (!(x[k] >= nm.x_lo[k] - kBoxMargin * span && x[k] <= nm.x_hi[k] + kBoxMargin * span)) stt = 2;
-        }
+    const size_t c = tile * mlp::tc::kRows + r;
+    float x[kFeatures];
+    unsigned char stt = 0;
+    if (c < cells && cell_features(g, ph, mom + c * kMomWords, (int)(c / g.nz), sm.st[r], x)) {
+      stt = 1;
+      for (int k = 0; k < kFeatures; ++k) {
+        const float span = nm.x_hi[k] - nm.x_lo[k];
+        if (!(x[k] >= nm.x_lo[k] - kBoxMargin * span && x[k] <= nm.x_hi[k] + kBoxMargin * span)) stt = 2;
       }
-      sm.state[r] = stt;
-      for (int k = 0; k < mlp::kInPad; ++k)
-        sm.f.X[r * mlp::kInPad + k] =
-            __float2bfloat16_rn(stt == 1 && k < kFeatures ? (x[k] - nm.x_mean[k]) / nm.x_std[k] : 0.f);
     }
-    __syncthreads();
-    {
-      const int lane = threadIdx.x & 31, wr = (threadIdx.x >> 5) * 16, gq = lane >> 2, t = lane & 3;
-      float out[1][4];
-      mlp::forward_rows(sm.f, wr, lane, out);
-      for (int h = 0; h < 2; ++h)
-        for (int q = 0; q < 2; ++q) sm.y[wr + gq + 8 * h][2 * t + q] = out[0][2 * h + q];
-    }
-    __syncthreads();
-    if (threadIdx.x < mlp::kRowsPerBlock) {
-      const int r = threadIdx.x;
-      const size_t c = c0 + r;
-      if (c < cells) {
-        const unsigned char stt = sm.state[r];
-        double xf[12] = {0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1};
-        if (stt == 1) {
-          const double* st = sm.st[r];
-          double Tn[2][3], e0 = 0.0, e1 = 0.0;
-          for (int l = 0; l < 2; ++l)
-            for (int a = 0; a < 3; ++a) {
-              const double y = (double)sm.y[r][3 * l + a] * nm.y_std[3 * l + a] + nm.y_mean[3 * l + a];
-              Tn[l][a] = st[3 * l + a] + st[6 + l] * st[16] * y;
-              e0 += st[8 + l] * st[3 * l + a];
-              e1 += st[8 + l] * Tn[l][a];
-            }
-          const double f = e1 > 0.0 ? e0 / e1 : 1.0;  // the cell's thermal energy is kept
-          for (int l = 0; l < 2; ++l)
-            for (int a = 0; a < 3; ++a) {
-              const double T = st[3 * l + a], T1 = fmax(Tn[l][a] * f, 1e-6 * st[6 + l]);
-              xf[6 * l + a] = st[10 + 3 * l + a];
-              xf[6 * l + 3 + a] = T > 0.0 ? sqrt(T1 / T) : 1.0;
-            }
-          atomicAdd(&sm.n_learned, 1ull);
-        } else if (stt == 2) {
-          atomicAdd(&sm.n_fallback, 1ull);
-        }
-        for (int q = 0; q < 12; ++q) xform[c * 12 + q] = xf[q];
-        flag[c] = stt;
+    uint32_t pk[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      float v[2];
+      for (int h = 0; h < 2; ++h) {
+        const int k = 2 * q + h;
+        v[h] = stt == 1 && k < kFeatures ? (x[k] - nm.x_mean[k]) / nm.x_std[k] : 0.f;
       }
+      pk[q] = mlp::pack2(__float2bfloat16_rn(v[0]), __float2bfloat16_rn(v[1]));
+    }
+    *reinterpret_cast<uint4*>(a1 + mlp::tc::canon(r, 0, mlp::kInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    *reinterpret_cast<uint4*>(a1 + mlp::tc::canon(r, 8, mlp::kInPad)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    float y[mlp::kOut];
+    if (!mlp::tc::forward_tile(sm.t, phase, y)) {
+      if (r == 0) atomicAdd(count + 2, 1ull);
+      break;
+    }
+    if (c < cells) {
+      double xf[12] = {0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1};
+      if (stt == 1) {
+        const double* st = sm.st[r];
+        double Tn[2][3], e0 = 0.0, e1 = 0.0;
+        for (int l = 0; l < 2; ++l)
+          for (int a = 0; a < 3; ++a) {
+            const double yv = (double)y[3 * l + a] * nm.y_std[3 * l + a] + nm.y_mean[3 * l + a];
+            Tn[l][a] = st[3 * l + a] + st[6 + l] * st[16] * yv;
+            e0 += st[8 + l] * st[3 * l + a];
+            e1 += st[8 + l] * Tn[l][a];
+          }
+        const double f = e1 > 0.0 ? e0 / e1 : 1.0;  // the cell's thermal energy is kept
+        for (int l = 0; l < 2; ++l)
+          for (int a = 0; a < 3; ++a) {
+            const double T = st[3 * l + a], T1 = fmax(Tn[l][a] * f, 1e-6 * st[6 + l]);
+            xf[6 * l + a] = st[10 + 3 * l + a];
+            xf[6 * l + 3 + a] = T > 0.0 ? sqrt(T1 / T) : 1.0;
+          }
+        atomicAdd(&sm.n_learned, 1ull);
+      } else if (stt == 2) {
+        atomicAdd(&sm.n_fallback, 1ull);
+      }
+      for (int q = 0; q < 12; ++q) xform[c * 12 + q] = xf[q];
+      flag[c] = stt;
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  mlp::tc::end(sm.t);
+  if (r == 0) {
     if (sm.n_learned) atomicAdd(count, sm.n_learned);
     if (sm.n_fallback) atomicAdd(count + 1, sm.n_fallback);
   }
@@ -283,7 +282,7 @@ int ensure(const GridGeom& g, LearnedWork& w) {
   const size_t cells = (size_t)g.nr * g.nz;
   if (w.cells == cells && w.mom) return 0;
   if (grow(&w.mom, cells * kMomWords) || grow(&w.xform, cells * 12) || grow(&w.flag, cells) ||
-      grow(&w.count, 2))
+      grow(&w.count, 3))
     return -1;
   w.cells = cells;
   return 0;
@@ -310,22 +309,26 @@ int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const Learne
                  unsigned long long counts[2], cudaStream_t s) {
   if (!w.model) return -1;
   if (learned_moments(g, sp, nsp, w, s)) return -1;
+  const size_t smem = sizeof(LearnSmem) + 1024;
   static const bool attr = cudaFuncSetAttribute(learned_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)sizeof(LearnSmem)) == cudaSuccess;
+                                                (int)smem) == cudaSuccess;
   if (!attr) return -1;
-  cudaMemsetAsync(w.count, 0, 2 * sizeof(unsigned long long), s);
-  const size_t tiles = (w.cells + mlp::kRowsPerBlock - 1) / mlp::kRowsPerBlock;
+  cudaMemsetAsync(w.count, 0, 3 * sizeof(unsigned long long), s);
+  const size_t tiles = (w.cells + mlp::tc::kRows - 1) / mlp::tc::kRows;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const unsigned blocks = (unsigned)std::min<size_t>(tiles, (size_t)sms * 2);
-  learned_cells_kernel<<<blocks, mlp::kMlpThreads, sizeof(LearnSmem), s>>>(g, ph, w.mom, w.params, w.norm,
-                                                                           w.xform, w.flag, w.count);
+  learned_cells_kernel<<<blocks, mlp::tc::kThreads, smem, s>>>(g, ph, w.mom, w.params, w.norm, w.xform, w.flag,
+                                                                w.count);
   for (int t = 0; t < nsp; ++t)
     if (sp[t].n) transform_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.xform, w.flag);
-  if (cudaMemcpyAsync(counts, w.count, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
+  unsigned long long c3[3] = {0, 0, 0};
+  if (cudaMemcpyAsync(c3, w.count, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess || c3[2])  // c3[2]: a wait for the tensor cores timed out
     return -1;
+  counts[0] = c3[0];
+  counts[1] = c3[1];
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

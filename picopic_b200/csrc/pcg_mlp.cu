@@ -16,6 +16,7 @@
 
 #include "pcg.h"
 #include "pcg_mlp.cuh"
+#include "pcg_mlp_tc.cuh"
 #include "pcg_philox.cuh"
 
 static_assert(pcg::mlp::kParams == PCG_MLP_PARAMS, "parameter count of the C ABI");
@@ -244,6 +245,40 @@ __global__ void adam_kernel(float* P, float* G, float* M, float* V, float lr, fl
   G[q] = 0.f;
 }
 
+// The forward pass on tcgen05 (pcg_mlp_tc.cuh): persistent CTAs of 128
+// threads, 128 rows per tile; *err is set when a wait timed out.
+__global__ void __launch_bounds__(tc::kThreads, 1) forward_tc_kernel(const float* P, const float* x, size_t rows,
+                                                                      float* y, int* err) {
+  extern __shared__ __align__(16) unsigned char raw_tc[];
+  tc::Smem& sm = *reinterpret_cast<tc::Smem*>((reinterpret_cast<uintptr_t>(raw_tc) + 1023) & ~uintptr_t(1023));
+  tc::load_weights(sm, P);
+  tc::begin(sm);
+  uint32_t phase = 0;
+  unsigned char* a1 = reinterpret_cast<unsigned char*>(sm.A1);
+  const size_t tiles = (rows + tc::kRows - 1) / tc::kRows;
+  for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const size_t row = tile * tc::kRows + threadIdx.x;
+    uint32_t pk[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = 2 * q;
+      const float lo = row < rows && k < kIn ? x[row * kIn + k] : 0.f;
+      const float hi = row < rows && k + 1 < kIn ? x[row * kIn + k + 1] : 0.f;
+      pk[q] = pack2(__float2bfloat16_rn(lo), __float2bfloat16_rn(hi));
+    }
+    *reinterpret_cast<uint4*>(a1 + tc::canon(threadIdx.x, 0, kInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    *reinterpret_cast<uint4*>(a1 + tc::canon(threadIdx.x, 8, kInPad)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    float out[kOut];
+    if (!tc::forward_tile(sm, phase, out)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      break;
+    }
+    if (row < rows)
+      for (int q = 0; q < kOut; ++q) y[row * kOut + q] = out[q];
+  }
+  tc::end(sm);
+}
+
 }  // namespace
 }  // namespace mlp
 }  // namespace pcg
@@ -352,6 +387,48 @@ int pcg_mlp_forward(pcg_mlp* m, const float* x, size_t rows, float* y) {
   cudaFree(dx);
   cudaFree(dy);
   return ok ? PCG_OK : PCG_ERR_CUDA;
+}
+
+int pcg_mlp_forward_tc(pcg_mlp* m, const float* x, size_t rows, float* y, float* device_ms) {
+  if (!m || (!x && rows) || (!y && rows)) return PCG_ERR_ARG;
+  if (device_ms) *device_ms = 0.f;
+  if (rows == 0) return PCG_OK;
+  const size_t smem = sizeof(tc::Smem) + 1024;
+  static const bool attr = cudaFuncSetAttribute(forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem) == cudaSuccess;
+  if (!attr) return PCG_ERR_CUDA;
+  float *dx = nullptr, *dy = nullptr;
+  int* derr = nullptr;
+  if (upload(&dx, x, rows * kIn, m->stream) != 0 || cudaMalloc((void**)&dy, rows * kOut * sizeof(float)) != cudaSuccess ||
+      cudaMalloc((void**)&derr, sizeof(int)) != cudaSuccess) {
+    cudaFree(dx);
+    cudaFree(dy);
+    return PCG_ERR_NOMEM;
+  }
+  cudaMemsetAsync(derr, 0, sizeof(int), m->stream);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  const size_t tiles = (rows + tc::kRows - 1) / tc::kRows;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, m->stream);
+  forward_tc_kernel<<<(unsigned)std::min<size_t>(tiles, (size_t)sms), tc::kThreads, smem, m->stream>>>(
+      m->params, dx, rows, dy, derr);
+  cudaEventRecord(e1, m->stream);
+  int herr = 0;
+  bool ok = cudaGetLastError() == cudaSuccess &&
+            cudaMemcpyAsync(y, dy, rows * kOut * sizeof(float), cudaMemcpyDeviceToHost, m->stream) == cudaSuccess &&
+            cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, m->stream) == cudaSuccess &&
+            cudaStreamSynchronize(m->stream) == cudaSuccess;
+  if (ok && device_ms) cudaEventElapsedTime(device_ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dx);
+  cudaFree(dy);
+  cudaFree(derr);
+  if (!ok) return PCG_ERR_CUDA;
+  return herr ? PCG_ERR_TIMEOUT : PCG_OK;
 }
 
 int pcg_mlp_gradient(pcg_mlp* m, const float* x, const float* t, size_t rows, float* grad_out, float* loss_out) {

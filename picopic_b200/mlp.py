@@ -74,6 +74,15 @@ class Mlp:
         self._check(self.lib.pcg_mlp_forward(self.h, _fp(x), x.shape[0], _fp(y)), "pcg_mlp_forward")
         return y
 
+    def forward_tc(self, x):
+        """The forward pass on tcgen05 (pcg_mlp_forward_tc); returns (y, device ms)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], OUTPUTS), dtype=np.float32)
+        ms = ctypes.c_float(0.0)
+        self._check(self.lib.pcg_mlp_forward_tc(self.h, _fp(x), x.shape[0], _fp(y), ctypes.byref(ms)),
+                    "pcg_mlp_forward_tc")
+        return y, float(ms.value)
+
     def gradient(self, x, t):
         """Full-batch gradient and value of mean((y - t)^2)."""
         x = np.ascontiguousarray(x, dtype=np.float32)

@@ -56,3 +56,24 @@ def test_training_reduces_loss():
     m.train(600, batch=1024, lr=2e-3)
     _, l1 = m.gradient(x, t)
     assert l1 < 0.3 * l0
+
+
+@pytest.mark.parametrize("rows", [1000, 20000])
+def test_forward_on_tcgen05_matches(rows):
+    """The tcgen05 forward pass (pcg_mlp_forward_tc: UMMA from shared-memory
+    descriptors, FP32 accumulators in tensor memory) against the mma.sync one
+    on the same BF16 operands: within RTOL_TC = 5e-3 of the output scale
+    (FP32 sum order, and the rare hidden activation whose BF16 rounding it
+    flips), and against the restatement within RTOL_FWD; a partial last tile
+    and several tiles per CTA."""
+    from picopic_b200.mlp import Mlp
+    m = Mlp(seed=5)
+    x, t = _data(rows, 7)
+    y = m.forward(x)
+    y_tc, ms = m.forward_tc(x)
+    assert ms > 0
+    scale = np.abs(y).max()
+    assert np.abs(y_tc - y).max() <= 5e-3 * scale
+    assert np.median(np.abs(y_tc - y)) <= 1e-5 * scale
+    _, _, yo = forward_backward(m.params, x, t)
+    assert np.abs(y_tc - yo).max() <= RTOL_FWD * np.abs(yo).max()
