@@ -789,9 +789,12 @@ static_assert((6 * kFWR * kFWZ + 3 * kJWR * kJWZ) % 4 == 0, "the table rows need
 // beyond the windows use the global grid.
 // PUSH, BEAM, FIX >= 0 fix a.pusher, a.is_beam, a.fixed at compile time
 // (the local copy's constant fields fold every test of them away); -1
-// leaves them to the arguments.
+// leaves them to the arguments.  The specialised ZigZag instance fits 48
+// registers without spilling and runs 5 blocks per SM (shared memory allows
+// 5); the others keep 64 registers and 4 blocks.
 template <int CUR, int PUSH = -1, int BEAM = -1, int FIX = -1>
-__global__ void __launch_bounds__(kThreads, 4) step_tiled_kernel(StepArgs args, SpeciesF32Buffers b,
+__global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
+    step_tiled_kernel(StepArgs args, SpeciesF32Buffers b,
                                                                  TileGrid tg) {
   StepArgs a = args;
   if (PUSH >= 0) a.pusher = PUSH;
