@@ -20,15 +20,18 @@ RTOL_TEMP = 1e-8
 ORDER = ("density", "energy", "temperature", "momentum")
 
 
-@pytest.mark.parametrize("precision,quirks", [("f64", "reference"), ("f64", "fixed"), ("f32", "reference")])
-def test_species_maps_match_oracle(precision, quirks):
+@pytest.mark.parametrize("precision,quirks,counts", [
+    ("f64", "reference", (4000, 3000)), ("f64", "fixed", (4000, 3000)), ("f32", "reference", (4000, 3000)),
+    ("f64", "reference", (60, 25)), ("f32", "fixed", (60, 25))])
+def test_species_maps_match_oracle(precision, quirks, counts):
+    """Dense, and with most nodes empty (their maps hold zeros)."""
     from picopic_b200 import Domain
     grid = small_grid(nr=12, nz=24, pml=False)
     d = Domain(grid, precision=precision, quirks=quirks, seed=5)
     d.add(ELECTRONS, capacity=5000)
     d.add(IONS, capacity=5000)
-    d.set_particles(0, *map_particles(grid, 4000, 3))
-    d.set_particles(1, *map_particles(grid, 3000, 4, mass=1836.0))
+    d.set_particles(0, *map_particles(grid, counts[0], 3))
+    d.set_particles(1, *map_particles(grid, counts[1], 4, mass=1836.0))
     o = OracleSim(grid, quirks=quirks)
     o.add(ELECTRONS)
     o.add(IONS)

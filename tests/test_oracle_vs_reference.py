@@ -71,7 +71,7 @@ def test_long_run_removal_and_reflection():
     _assert_same(o, r, 2, "after 20 steps")
 
 
-@pytest.mark.parametrize("ppc", [3, 10])
+@pytest.mark.parametrize("ppc", [1, 2, 3, 10])
 def test_p12_collisions_bit_exact(ppc):
     """One Perez-2012 collision pass (cells from the binding, no shuffle,
     the reference's mt19937 draws): velocities bit-identical."""
@@ -87,15 +87,20 @@ def test_p12_collisions_bit_exact(ppc):
         sim.set_particles(1, *thermal_plasma(grid, n + 7, 2, 1836.0, 0.5, 1e20))
     o.set_rng("mt19937", 123)
     r.seed(123)
-    assert o.collide() > 0
-    assert r.collide() > 0
+    before = o.get_particles(0)["vz"].copy()
+    # the oracle counts pair calls, the reference (collisionsP12.cpp:287)
+    # only those that passed the early returns
+    assert o.collide() >= r.collide() > 0 or ppc == 1
     for sid in (0, 1):
         po, pr = o.get_particles(sid), r.get_particles(sid)
         for k in ("vr", "vphi", "vz"):
             np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
+    # one per cell: a row stops at its first cell without both species
+    # (collisionsP12.cpp:351-354), so the pass may change nothing there
+    assert ppc == 1 or np.abs(o.get_particles(0)["vz"] - before).max() > 0
 
 
-@pytest.mark.parametrize("ppc", [3, 10])
+@pytest.mark.parametrize("ppc", [1, 2, 3, 10])
 def test_ta77s_collisions_bit_exact(ppc):
     """One Takizuka-Abe pass with the weighted correction (collisionsTA77S.cpp:
     pairs, then correct_velocities; no shuffle, the reference's mt19937
@@ -114,19 +119,21 @@ def test_ta77s_collisions_bit_exact(ppc):
     o.set_rng("mt19937", 321)
     r.seed(321)
     before = o.get_particles(0)["vz"].copy()
-    assert o.collide(scheme="ta77s") > 0
+    assert o.collide(scheme="ta77s") >= 0
     assert r.collide(scheme="ta77s") == 0
     for sid in (0, 1):
         po, pr = o.get_particles(sid), r.get_particles(sid)
         for k in ("vr", "vphi", "vz"):
             np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
-    assert np.abs(o.get_particles(0)["vz"] - before).max() > 0
+    assert ppc == 1 or np.abs(o.get_particles(0)["vz"] - before).max() > 0
 
 
-def test_species_maps_bit_exact():
+@pytest.mark.parametrize("counts", [(4000, 3000), (60, 25)])
+def test_species_maps_bit_exact(counts):
     """SpecieP::calc_density / calc_energy / calc_temperature / calc_momentum
-    over weight_cylindrical: bit-identical grids.  The temperature reads the
-    absolute-momentum map the last energy map left; before any, the
+    over weight_cylindrical: bit-identical grids, dense and with most cells
+    empty (0/0 temperatures compare as NaN == NaN).  The temperature reads
+    the absolute-momentum map the last energy map left; before any, the
     reference reads a grid it never initialised (undefined, not compared)."""
     if not reference_available():
         pytest.skip("compiled reference not built (oracle/Makefile.ref)")
@@ -136,8 +143,8 @@ def test_species_maps_bit_exact():
     for sim in (o, r):
         sim.add(ELECTRONS)
         sim.add(IONS)
-        sim.set_particles(0, *map_particles(grid, 4000, 3))
-        sim.set_particles(1, *map_particles(grid, 3000, 4, mass=1836.0))
+        sim.set_particles(0, *map_particles(grid, counts[0], 3))
+        sim.set_particles(1, *map_particles(grid, counts[1], 4, mass=1836.0))
     for which in ("density", "energy", "temperature", "momentum"):
         for sid in (0, 1):
             a, b = o.species_map(sid, which), r.species_map(sid, which)
