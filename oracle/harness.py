@@ -316,6 +316,9 @@ class RefSim(_Sim):
             lib.ref_collide.restype = ctypes.c_long
             lib.ref_collide_ta77s.argtypes = [ctypes.c_void_p]
             lib.ref_collide_ta77s.restype = ctypes.c_long
+            lib.ref_add_plasma.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, _D, _D,
+                                           ctypes.c_uint, _D, _D]
+            lib.ref_distribute.argtypes = [ctypes.c_void_p]
             self._bind(lib)
             RefSim._libs[path] = lib
         self.lib = RefSim._libs[path]
@@ -329,6 +332,17 @@ class RefSim(_Sim):
     def seed(self, s: int):
         """Seed the reference's global std::mt19937 (rand.cpp:25)."""
         self.lib.ref_seed(s)
+
+    def add_plasma(self, sp: SpeciesSpec, macro_amount: int, density: float, temperature: float) -> int:
+        """A species the reference fills itself at distribute()."""
+        return self.lib.ref_add_plasma(self.h, sp.id, sp.name.encode(), sp.charge, sp.mass,
+                                       int(macro_amount), density, temperature)
+
+    def distribute(self):
+        """Domain::distribute (domain.cpp:86-94): the reference's own flat
+        placement, weights and thermal velocities for every plasma species."""
+        rc = self.lib.ref_distribute(self.h)
+        assert rc == 0, rc
 
     def collide(self, scheme: str = "p12") -> int:
         """One CollisionsP12 pass without its time-seeded shuffle (returns ncol),

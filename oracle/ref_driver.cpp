@@ -179,6 +179,30 @@ int ref_add_species(void* h, int id, const char* name, double charge_e, double m
   return (int)s->species.size() - 1;
 }
 
+// A plasma species that the reference initialises itself: SpecieP with its
+// macroparticle count, density and temperature (SMB.cpp:129-146 for one
+// domain); its particles appear at ref_distribute.
+int ref_add_plasma(void* h, int id, const char* name, double charge_e, double mass_e,
+                   unsigned macro_amount, double density, double temperature) {
+  RefSim* s = (RefSim*)h;
+  if (s->domain) return -3;
+  s->species.push_back(new SpecieP((unsigned)id, name, charge_e, mass_e, macro_amount, density,
+                                   density, temperature, s->geometry, &s->time));
+  return (int)s->species.size() - 1;
+}
+
+// Domain::distribute (domain.cpp:86-94): every species' own spatial
+// placement (flat: the radical-inverse sequences of specieP.cpp:127-189 and
+// the weights of :280-331), cell binding, then its thermal velocities
+// (Maxwell-Juettner energies and uniform2 directions, :346-384) drawn from
+// math::random::gen.  Beams place nothing here (beamP.hpp:63-64).
+int ref_distribute(void* h) {
+  RefSim* s = (RefSim*)h;
+  pcg_ref_log::g_fatal = false;
+  domain_of(s)->distribute();
+  return pcg_ref_log::g_fatal ? -10 : 0;
+}
+
 int ref_add_beam(void* h, int id, const char* name, double charge_e, double mass_e,
                  unsigned macro_amount, double start_time, double b_radius, double density,
                  double amount, double length, double distance, double velocity) {

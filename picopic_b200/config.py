@@ -177,9 +177,17 @@ def _id(name: str) -> int:
 
 
 def build_domain(cfg: RunConfig, pusher="borisrel", current="vb", precision="f32", quirks="reference",
-                 seed=0, device=0, use_external_fields=False):
+                 seed=0, device=0, use_external_fields=False, plasma="maxwellian"):
     """A Domain with the configuration's species (seeded) and beams.  Returns
-    (domain, {name: slot})."""
+    (domain, {name: slot}).
+
+    plasma: "maxwellian" seeds each species on the device (r = R sqrt(U),
+    equal weights, a Maxwellian at the configured temperature);
+    "reference" builds on the host the particles the reference's own
+    Domain::distribute makes (picopic_b200.initial: flat placement and
+    weights bit for bit, its thermal velocity distribution)."""
+    if plasma not in ("maxwellian", "reference"):
+        raise ValueError(f"plasma initialiser {plasma!r}: 'maxwellian' or 'reference'")
     for kind in ("electric", "magnetic"):
         ff = cfg.external_fields.get(kind, {}).get("formfactor", "none")
         if ff != "none" and use_external_fields:
@@ -199,8 +207,15 @@ def build_domain(cfg: RunConfig, pusher="borisrel", current="vb", precision="f32
                     velocity=b["velocity"])
         slots[b["name"]] = d.add(_Spec(b["name"], b["charge"], b["mass"], _id(b["name"]), beam=beam),
                                  capacity=b["macro_amount"] + 4096)
+    g = cfg.geometry
     for k, s in enumerate(cfg.species):
-        d.seed_plasma(slots[s["name"]], s["macro_amount"], s["density"], s["temperature"], seed + k)
+        if plasma == "reference":
+            from . import initial
+            d.set_particles(slots[s["name"]], *initial.reference_plasma(
+                s["macro_amount"], g.nr, g.nz, g.dr, g.dz, s["density"], s["temperature"], s["mass"],
+                seed=seed * 1000 + k))
+        else:
+            d.seed_plasma(slots[s["name"]], s["macro_amount"], s["density"], s["temperature"], seed + k)
     return d, slots
 
 
@@ -232,14 +247,24 @@ def _frame(d, slots, p: Probe):
 def run(cfg: RunConfig, d, slots, steps=None, out_dir=None, log=print):
     """Step the domain `steps` times (default: to the configured end time),
     recording every probe on its schedule; writes <out_dir>/<probe path>.npy
-    (frames x probe shape) and returns {path: array}."""
+    (frames x probe shape) and returns {path: array}.
+
+    The schedule is the reference's: its main loop (PiCoPiC.cpp:326-347)
+    runs a step and then the writers while the clock still reads the step's
+    start time t, and a probe writes when ceil(t / dt) is a multiple of its
+    schedule (outController.cpp:341-351), t accumulated by repeated
+    additions of dt.  So frame j is the state after schedule * j + 1 steps."""
     n = cfg.steps if steps is None else int(steps)
+    g = cfg.geometry
     frames = {p.path: [] for p in cfg.probes}
-    for k in range(1, n + 1):
+    t = g.t_start
+    for _ in range(n):
         d.step(1)
+        ts = int(np.ceil(t / g.dt))
         for p in cfg.probes:
-            if k % p.schedule == 0:
+            if ts % p.schedule == 0:
                 frames[p.path].append(np.array(_frame(d, slots, p)))
+        t += g.dt
     d.synchronize()
     out = {path: np.stack(f) if f else np.zeros((0,)) for path, f in frames.items()}
     if out_dir:
@@ -261,9 +286,11 @@ def main(argv=None):
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--quirks", default="reference", choices=["reference", "fixed"])
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--plasma", default="maxwellian", choices=["maxwellian", "reference"],
+                    help="plasma initial condition: device Maxwellian, or the reference's own")
     a = ap.parse_args(argv)
     cfg = load(a.config)
-    d, slots = build_domain(cfg, a.pusher, a.current, a.precision, a.quirks, a.seed)
+    d, slots = build_domain(cfg, a.pusher, a.current, a.precision, a.quirks, a.seed, plasma=a.plasma)
     run(cfg, d, slots, a.steps, a.out or cfg.data_root)
 
 

@@ -1,0 +1,117 @@
+"""The reference's own functional test as a pin (test/functional/test.py).
+
+Its known answers (tests/golden/functional/step80.json, made by
+tests/golden/make_functional.py) are the mean, standard deviation and
+variance of nine probes (E, H_at_et and J; r, phi, z; nodes r 0-32, z 0-128)
+in frame 4, the state after 81 steps, of its configuration
+(tests/golden/functional/PiCoPiC.json: 128 x 256 cells with PML, an electron
+and an ion plasma of 103964 macroparticles each from the reference's own
+initialiser, an electron bunch entering at z = 0).  The reference's test
+accepts a run when the standard deviation and the variance are within
+rtol 0.15 (test.py:169-200, 614-622) and retries up to four times, because
+the initial velocities are random.  Compiled here and run on one domain, the
+reference gives standard deviations 0.945-1.169 times the known answers over
+eight seeds; a single run is therefore held to 0.2 (three seeds averaged,
+on the GPU, to 0.15).
+
+The first test runs the compiled reference with its own initialiser and
+the oracle from the same particles in lockstep: identical bit for bit after
+81 steps, and both within the bound.  The second starts the oracle from the
+restated initial condition (picopic_b200.initial), the one the GPU tests use.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.harness import FIELDS, GridSpec, OracleSim, RefSim, SpeciesSpec, reference_available
+from picopic_b200 import config, initial
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FUNCTIONAL = os.path.join(HERE, "golden", "functional", "PiCoPiC.json")
+ANSWERS = os.path.join(HERE, "golden", "functional", "step80.json")
+STEPS = 81          # frame 4 of a schedule of 20: iterations 0..80
+RTOL_ONE_RUN = 0.2
+PREFIX = {"E": "e", "H": "hat", "J": "j"}
+
+
+def known_answers():
+    with open(ANSWERS) as f:
+        return json.load(f)["components"]
+
+
+def probe_std(sim) -> dict:
+    """Standard deviation of each probed window (nodes r 0-32, z 0-128)."""
+    out = {}
+    for comp in known_answers():
+        f, a = comp.split("/")
+        out[comp] = float(sim.get_field(f"{PREFIX[f]}_{a}")[2:34, 2:130].std())
+    return out
+
+
+def check(std: dict, rtol: float, who: str):
+    answers = known_answers()
+    bad = {c: round(s / answers[c]["std"], 3) for c, s in std.items() if abs(s / answers[c]["std"] - 1) > rtol}
+    assert not bad, f"{who}: std / known answer outside 1 +- {rtol}: {bad}"
+
+
+def functional_grid(cfg):
+    g = cfg.geometry
+    return GridSpec(g.nr, g.nz, g.radius, g.longitude, g.dt, pml_size=g.pml_size, pml_sigma=g.pml_sigma)
+
+
+def specs(cfg):
+    plasma = [SpeciesSpec(s["name"], s["charge"], s["mass"], id=k) for k, s in enumerate(cfg.species)]
+    beams = [SpeciesSpec(b["name"], b["charge"], b["mass"], id=100 + k, beam=dict(b))
+             for k, b in enumerate(cfg.beams)]
+    return plasma, beams
+
+
+def test_reference_run_meets_its_known_answers_and_the_oracle_follows_it():
+    if not reference_available():
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    cfg = config.load(FUNCTIONAL)
+    grid = functional_grid(cfg)
+    plasma, beams = specs(cfg)
+    ref = RefSim(grid)
+    ref.seed(2)
+    for sp, s in zip(plasma, cfg.species):
+        ref.add_plasma(sp, s["macro_amount"], s["density"], s["temperature"])
+    for sp in beams:
+        ref.add(sp)
+    ref.distribute()
+    orc = OracleSim(grid, quirks="reference")
+    for sp in plasma + beams:
+        orc.add(sp)
+    for k in range(len(plasma)):
+        p = ref.get_particles(k)
+        orc.set_particles(k, p["r"], p["z"], p["vr"], p["vphi"], p["vz"], p["w"])
+    ref.seed(7)
+    orc.set_rng("mt19937", 7)
+    assert ref.step(STEPS) == 0
+    assert orc.step(STEPS) == 0
+    for name in FIELDS:
+        np.testing.assert_array_equal(orc.get_field(name), ref.get_field(name), err_msg=name)
+    for k in range(len(plasma) + len(beams)):
+        po, pr = orc.get_particles(k), ref.get_particles(k)
+        assert po["r"].size == pr["r"].size
+        for key in ("r", "z", "vr", "vphi", "vz", "w", "cell_r", "cell_z"):
+            np.testing.assert_array_equal(po[key], pr[key], err_msg=f"species {k} {key}")
+    assert orc.count(len(plasma)) > 400  # the bunch entered
+    check(probe_std(ref), RTOL_ONE_RUN, "compiled reference")
+
+
+def test_oracle_from_the_restated_initial_condition_meets_the_known_answers():
+    cfg = config.load(FUNCTIONAL)
+    g = cfg.geometry
+    plasma, beams = specs(cfg)
+    orc = OracleSim(functional_grid(cfg), quirks="reference")
+    for sp in plasma + beams:
+        orc.add(sp)
+    for k, s in enumerate(cfg.species):
+        orc.set_particles(k, *initial.reference_plasma(s["macro_amount"], g.nr, g.nz, g.dr, g.dz,
+                                                       s["density"], s["temperature"], s["mass"], seed=k))
+    orc.set_rng("mt19937", 1)
+    assert orc.step(STEPS) == 0
+    check(probe_std(orc), RTOL_ONE_RUN, "oracle")
