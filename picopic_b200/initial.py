@@ -72,10 +72,12 @@ def flat_positions(n: int, nr: int, nz: int, dr: float, dz: float):
 def flat_weights(r: np.ndarray, nr: int, nz: int, dr: float, dz: float, density: float) -> np.ndarray:
     """SpecieP::set_weight (specieP.cpp:280-331) for a uniform density."""
     n = r.size
+    if n == 0:
+        return np.zeros(0)
     z_size = nz * dz - dz
     inner = r > dr / 2
     vol = np.where(inner, 2 * PI * r * dr * dz, PI * r * r * dz)
-    v_sum = float(np.add.accumulate(vol)[-1]) if n else 0.0   # in particle order
+    v_sum = float(np.add.accumulate(vol)[-1])   # in particle order
     v_avg = v_sum / n
     top = float(nr - 1)
     n_total = (density + density) / 2 * PI * dr * dr * (top * top - 0.0 * 0.0) * z_size

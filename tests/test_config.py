@@ -45,6 +45,42 @@ def test_refusals():
         config.load(bad)
 
 
+class _CountingDomain:
+    """Stands in for a Domain: every grid holds the number of steps taken."""
+    def __init__(self, shape):
+        self.shape, self.steps = shape, 0
+
+    def step(self, n):
+        self.steps += n
+
+    def get_field(self, which):
+        return np.full(self.shape, float(self.steps))
+
+    def species_map(self, slot, which):
+        return np.full((3,) + self.shape if which == "momentum" else self.shape, float(self.steps))
+
+    def synchronize(self):
+        pass
+
+
+def test_probe_schedule_is_the_references():
+    """Frame j of a probe of schedule s is the state after s j + 1 steps: the
+    reference's writers run after the step of iteration k, while the clock
+    still reads k dt (PiCoPiC.cpp:326-347, outController.cpp:341-351)."""
+    c = config.load(CFG)
+    g = c.geometry
+    d = _CountingDomain((g.nr + 4, g.nz + 4))
+    slots = {"electrons": 0, "ions": 1}
+    out = config.run(c, d, slots, steps=31, log=lambda *a: None)
+    assert d.steps == 31
+    frames = {p.path: p.schedule for p in c.probes}
+    for path, a in out.items():
+        s = frames[path]
+        want = [s * j + 1 for j in range((31 - 1) // s + 1)]
+        got = [float(np.asarray(f).flat[0]) for f in a]
+        assert got == want, (path, got, want)
+
+
 @pytest.mark.gpu
 def test_run_writes_probes(tmp_path):
     c = config.load(CFG)
