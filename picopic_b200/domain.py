@@ -119,7 +119,9 @@ class Domain:
         return slot.value
 
     def set_particles(self, slot, r, z, vr, vphi, vz, w, append=False):
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (r, z, vr, vphi, vz, w)]
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (r, z, vr, vphi, vz, w)]
+        if len({a.size for a in arrs}) != 1:
+            raise ValueError(f"particle arrays differ in length: {[a.size for a in arrs]}")
         fn = self.lib.pcg_append_species if append else self.lib.pcg_import_species
         self._check(fn(self.h, slot, arrs[0].size, *[_dp(a) for a in arrs]), "pcg_import_species")
 
@@ -178,7 +180,8 @@ class Domain:
     def set_field(self, which, arr):
         idx = FIELD[which] if isinstance(which, str) else int(which)
         a = np.ascontiguousarray(arr, dtype=np.float64)
-        assert a.shape == tuple(self.grid.shape)
+        if a.shape != tuple(self.grid.shape):
+            raise ValueError(f"field {which!r}: shape {a.shape}, the grid is {tuple(self.grid.shape)}")
         self._check(self.lib.pcg_set_field(self.h, idx, _dp(a)), "pcg_set_field")
 
     def get_field(self, which) -> np.ndarray:

@@ -227,7 +227,9 @@ def save_model(path, params, norm, meta: dict):
 
 def load_model(path=MODEL_PATH):
     d = np.load(path)
-    assert d["params"].size == PARAMS and d["norm"].size == 64
+    if d["params"].size != PARAMS or d["norm"].size != 64:
+        raise ValueError(f"{path}: {d['params'].size} parameters and {d['norm'].size} normalisation "
+                         f"values, the network has {PARAMS} and 64")
     return d["params"], d["norm"]
 
 

@@ -65,7 +65,8 @@ class Mlp:
     @params.setter
     def params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
-        assert p.size == PARAMS
+        if p.size != PARAMS:
+            raise ValueError(f"{p.size} parameters, the network has {PARAMS}")
         self._check(self.lib.pcg_mlp_set_params(self.h, _fp(p)), "pcg_mlp_set_params")
 
     def forward(self, x) -> np.ndarray:
