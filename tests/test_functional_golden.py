@@ -14,6 +14,12 @@ reference gives standard deviations 0.945-1.169 times the known answers over
 eight seeds; a single run is therefore held to 0.2 (three seeds averaged,
 on the GPU, to 0.15).
 
+The reference's test builds with its default switches: adaptive Boris and
+Villasenor-Buneman (configure.ac:96-110).  Adaptive Boris reads an
+uninitialised flag below REL_LIMIT (pusherBoris.cpp:38), so these runs use
+relativistic Boris, which differs from it by gamma - 1 < 1e-5 for this
+plasma (the bunch is above REL_LIMIT, where both are relativistic).
+
 The first test runs the compiled reference with its own initialiser and
 the oracle from the same particles in lockstep: identical bit for bit after
 81 steps, and both within the bound.  The second starts the oracle from the
