@@ -17,7 +17,7 @@ on the GPU, to 0.15).
 The reference's test builds with its default switches: adaptive Boris and
 Villasenor-Buneman (configure.ac:96-110).  Adaptive Boris reads an
 uninitialised flag below REL_LIMIT (pusherBoris.cpp:38), so these runs use
-relativistic Boris, which differs from it by gamma - 1 < 1e-5 for this
+relativistic Boris, which differs from it by gamma - 1 < 3e-5 for this
 plasma (the bunch is above REL_LIMIT, where both are relativistic).
 
 The first test runs the compiled reference with its own initialiser and
