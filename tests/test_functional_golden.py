@@ -108,6 +108,39 @@ def test_reference_run_meets_its_known_answers_and_the_oracle_follows_it():
     check(probe_std(ref), RTOL_ONE_RUN, "compiled reference")
 
 
+def test_vay_zigzag_oracle_follows_the_reference_on_the_functional_run():
+    """The large configuration's switches (Vay, ZigZag) over 41 steps of the
+    same run: oracle and compiled reference identical bit for bit."""
+    if not reference_available("vay", "zigzag"):
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    cfg = config.load(FUNCTIONAL)
+    grid = functional_grid(cfg)
+    plasma, beams = specs(cfg)
+    ref = RefSim(grid, "vay", "zigzag")
+    ref.seed(5)
+    for sp, s in zip(plasma, cfg.species):
+        ref.add_plasma(sp, s["macro_amount"], s["density"], s["temperature"])
+    for sp in beams:
+        ref.add(sp)
+    ref.distribute()
+    orc = OracleSim(grid, "vay", "zigzag", quirks="reference")
+    for sp in plasma + beams:
+        orc.add(sp)
+    for k in range(len(plasma)):
+        p = ref.get_particles(k)
+        orc.set_particles(k, p["r"], p["z"], p["vr"], p["vphi"], p["vz"], p["w"])
+    ref.seed(9)
+    orc.set_rng("mt19937", 9)
+    assert ref.step(41) == 0
+    assert orc.step(41) == 0
+    for name in FIELDS:
+        np.testing.assert_array_equal(orc.get_field(name), ref.get_field(name), err_msg=name)
+    for k in range(len(plasma) + len(beams)):
+        po, pr = orc.get_particles(k), ref.get_particles(k)
+        for key in ("r", "z", "vr", "vphi", "vz", "cell_r", "cell_z"):
+            np.testing.assert_array_equal(po[key], pr[key], err_msg=f"species {k} {key}")
+
+
 def test_oracle_from_the_restated_initial_condition_meets_the_known_answers():
     cfg = config.load(FUNCTIONAL)
     g = cfg.geometry
