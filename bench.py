@@ -582,11 +582,57 @@ def cpu_baseline(w, nz=256, steps=2):
                       "reference hot path compiled with its release flags"}
 
 
+def _smb_reference(w, steps):
+    """The reference's own scheduler (src/SMB.cpp, unmodified, release flags,
+    OpenMP over domains, its overlays): the workload's radial extent cut into
+    square 64 x 64-cell domains (its overlays need square domains, and each
+    axis 1 or an even number of them), with enough z-domains that every host
+    thread has one.  Plasma from the reference's own initialiser at the
+    workload's density, temperatures and macroparticles per cell."""
+    from oracle.harness import GridSpec, SmbSim, SpeciesSpec
+    cells = 64
+    threads = len(os.sched_getaffinity(0))
+    r_dom = max(1, w["nr"] // cells)
+    if r_dom > 1 and r_dom % 2:
+        r_dom -= 1
+    z_dom = max(2, 2 * -(-threads // (2 * r_dom)))
+    nr, nz = r_dom * cells, z_dom * cells
+    grid = GridSpec(nr, nz, nr * w["dr"], nz * w["dz"], dt_courant(w["dr"]))
+    smb = SmbSim(grid, r_dom, z_dom)
+    smb.seed(7)
+    for sid, (name, q, m, T) in enumerate((("electrons", -1, 1, w["te"]), ("ions", 1, 1836, w["ti"]))):
+        smb.add_species(SpeciesSpec(name, q, m, id=sid), nr * nz * w["ppc"], w["density"], T)
+    smb.build()
+    smb.distribute()
+    n = smb.particles()
+    assert smb.step(1) == 0  # warm-up
+    t0 = time.perf_counter()
+    assert smb.step(steps) == 0
+    el = time.perf_counter() - t0
+    sample = (f"reference SMB scheduler, {r_dom} x {z_dom} domains of {cells} x {cells} cells "
+              f"({nr} x {nz}, {n} particles), {smb.threads()} OpenMP threads, {steps} steps")
+    return n, el, smb.threads(), sample
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
+    steps = max(1, args.steps // 25)
+    from oracle.harness import smb_available
+    if smb_available():
+        n, el, threads, sample = _smb_reference(w, steps)
+        value = n * steps / el
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+                "steps": steps, "warmup": 1, "ms_per_step": el * 1e3 / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": w["name"], "sample": sample},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
     threads = os.cpu_count() or 1
     nz = 64 if not args.small else 32
     sims = []
@@ -596,7 +642,6 @@ def run_reference(args):
         sims.append((s, n))
     for s, _ in sims:  # one warm-up step per domain
         s.step(1)
-    steps = max(1, args.steps // 25)
 
     def work(s):
         s.step(steps)

@@ -354,3 +354,79 @@ class RefSim(_Sim):
     @property
     def errors(self) -> int:
         return int(self.lib.ref_error_count())
+
+
+SMB_LIB = os.path.join(REF_DIR, "libpicopic_ref_smb_borisrel_vb.so")
+
+
+def smb_available() -> bool:
+    return os.path.exists(SMB_LIB)
+
+
+class SmbSim:
+    """The reference's own scheduler (src/SMB.cpp, unmodified, release flags,
+    OpenMP over its domains) driven by oracle/ref_smb.cpp: relativistic
+    Boris and Villasenor-Buneman.  Species and beams are added before
+    build(); distribute() places every domain's plasma with the reference's
+    own initialiser."""
+    _lib = None
+    FIELDS = ["e_r", "e_phi", "e_z", "hat_r", "hat_phi", "hat_z", "j_r", "j_phi", "j_z"]
+
+    def __init__(self, grid: GridSpec, r_domains: int, z_domains: int):
+        if SmbSim._lib is None:
+            lib = ctypes.CDLL(SMB_LIB)
+            lib.smb_new.restype = ctypes.c_void_p
+            lib.smb_new.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, ctypes.c_int, ctypes.c_int, _PI, _PD]
+            lib.smb_add_species.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_char_p, ctypes.c_int,
+                                            ctypes.c_uint, _D, _D, _D]
+            lib.smb_add_beam.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_char_p, ctypes.c_int,
+                                         ctypes.c_uint, _D, _D, _D, _D, ctypes.c_int, _D, _D, _D]
+            lib.smb_build.argtypes = [ctypes.c_void_p]
+            lib.smb_distribute.argtypes = [ctypes.c_void_p]
+            lib.smb_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.smb_particles.argtypes = [ctypes.c_void_p]
+            lib.smb_particles.restype = ctypes.c_long
+            lib.smb_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _PD]
+            lib.smb_threads.restype = ctypes.c_int
+            lib.smb_seed.argtypes = [ctypes.c_uint]
+            SmbSim._lib = lib
+        self.lib = SmbSim._lib
+        self.grid = grid
+        pml, sig = _make_arrays(grid)
+        h = self.lib.smb_new(grid.nr, grid.nz, grid.radius, grid.longitude, grid.dt, r_domains, z_domains, pml, sig)
+        assert h, "smb_new refused the decomposition (domains 1 or even per axis)"
+        self.h = ctypes.c_void_p(h)
+
+    def seed(self, s: int):
+        """Seed the reference's global std::mt19937 (rand.cpp:25)."""
+        self.lib.smb_seed(s)
+
+    def add_species(self, sp: SpeciesSpec, macro_amount: float, density: float, temperature: float):
+        assert self.lib.smb_add_species(self.h, sp.id, sp.name.encode(), int(sp.charge), int(sp.mass),
+                                        float(macro_amount), density, temperature) == 0
+
+    def add_beam(self, sp: SpeciesSpec):
+        b = sp.beam
+        assert self.lib.smb_add_beam(self.h, sp.id, sp.name.encode(), int(sp.charge), int(sp.mass),
+                                     float(b["macro_amount"]), b["start_time"], b["radius"], b["density"],
+                                     int(b["amount"]), b["length"], b["distance"], b["velocity"]) == 0
+
+    def build(self):
+        assert self.lib.smb_build(self.h) == 0
+
+    def distribute(self):
+        assert self.lib.smb_distribute(self.h) == 0
+
+    def step(self, n: int = 1) -> int:
+        return self.lib.smb_step(self.h, n)
+
+    def particles(self) -> int:
+        return int(self.lib.smb_particles(self.h))
+
+    def threads(self) -> int:
+        return int(self.lib.smb_threads())
+
+    def get_field(self, which) -> np.ndarray:
+        a = np.zeros(self.grid.shape)
+        assert self.lib.smb_get_field(self.h, self.FIELDS.index(which), _dp(a)) == 0
+        return a

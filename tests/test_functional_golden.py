@@ -22,16 +22,20 @@ plasma (the bunch is above REL_LIMIT, where both are relativistic).
 
 The first test runs the compiled reference with its own initialiser and
 the oracle from the same particles in lockstep: identical bit for bit after
-81 steps, and both within the bound.  The second starts the oracle from the
-restated initial condition (picopic_b200.initial), the one the GPU tests use.
+81 steps, and both within the bound.  Another runs the reference's own
+scheduler with the test's 2 x 4 domains.  The last starts the oracle from
+the restated initial condition (picopic_b200.initial), the one the GPU
+tests use.
 """
 import json
+import multiprocessing as mp
 import os
 
 import numpy as np
 import pytest
 
-from oracle.harness import FIELDS, GridSpec, OracleSim, RefSim, SpeciesSpec, reference_available
+from oracle.harness import (FIELDS, GridSpec, OracleSim, RefSim, SmbSim, SpeciesSpec, reference_available,
+                            smb_available)
 from picopic_b200 import config, initial
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -139,6 +143,45 @@ def test_vay_zigzag_oracle_follows_the_reference_on_the_functional_run():
         po, pr = orc.get_particles(k), ref.get_particles(k)
         for key in ("r", "z", "vr", "vphi", "vz", "cell_r", "cell_z"):
             np.testing.assert_array_equal(po[key], pr[key], err_msg=f"species {k} {key}")
+
+
+def _smb_probe_std(seed, queue):
+    """Child process: the reference's SMB with the known answers' own 2 x 4
+    domains, pinned to one core so that its OpenMP loops (which share the
+    reference's one generator while distributing) run in a fixed order."""
+    os.sched_setaffinity(0, {min(os.sched_getaffinity(0))})
+    cfg = config.load(FUNCTIONAL)
+    plasma, beams = specs(cfg)
+    smb = SmbSim(functional_grid(cfg), 2, 4)
+    smb.seed(seed)
+    for sp, s in zip(plasma, cfg.species):
+        smb.add_species(sp, s["macro_amount"], s["density"], s["temperature"])
+    for sp in beams:
+        smb.add_beam(sp)
+    smb.build()
+    smb.distribute()
+    n0 = smb.particles()
+    rc = smb.step(STEPS)
+    queue.put((rc, smb.threads(), n0, smb.particles(), probe_std(smb)))
+
+
+def test_reference_smb_meets_its_known_answers():
+    """The reference's own scheduler (src/SMB.cpp: domains, overlays, OpenMP)
+    on the configuration as its test runs it: within 0.2 of every known
+    standard deviation."""
+    if not smb_available():
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_smb_probe_std, args=(3, q))
+    p.start()
+    try:
+        rc, threads, n0, n1, std = q.get(timeout=600)
+    finally:
+        p.join(timeout=60)
+    assert rc == 0 and threads == 1
+    assert n1 > n0 + 400  # the bunch entered; the plasma stays
+    check(std, RTOL_ONE_RUN, "reference SMB, 2 x 4 domains")
 
 
 def test_oracle_from_the_restated_initial_condition_meets_the_known_answers():
