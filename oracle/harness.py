@@ -274,6 +274,8 @@ class OracleSim(_Sim):
             lib.orc_collide.restype = ctypes.c_long
             lib.orc_collide_ta77s.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.orc_collide_ta77s.restype = ctypes.c_long
+            lib.orc_collide_sk98.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.orc_collide_sk98.restype = ctypes.c_long
             self._bind(lib)
             OracleSim._lib = lib
         self.lib = OracleSim._lib
@@ -290,8 +292,10 @@ class OracleSim(_Sim):
 
     def collide(self, shuffle: bool = False, scheme: str = "p12") -> int:
         """One binary-collision pass (scheme "p12": Perez 2012, "ta77s":
-        Takizuka-Abe with the weighted correction); returns the pair calls."""
-        f = self.lib.orc_collide_ta77s if scheme == "ta77s" else self.lib.orc_collide
+        Takizuka-Abe with the weighted correction, "sk98": the relativistic
+        CM-frame scheme); returns the pair calls."""
+        f = {"p12": self.lib.orc_collide, "ta77s": self.lib.orc_collide_ta77s,
+             "sk98": self.lib.orc_collide_sk98}[scheme]
         return int(f(self.h, int(shuffle)))
 
     @property
@@ -316,6 +320,8 @@ class RefSim(_Sim):
             lib.ref_collide.restype = ctypes.c_long
             lib.ref_collide_ta77s.argtypes = [ctypes.c_void_p]
             lib.ref_collide_ta77s.restype = ctypes.c_long
+            lib.ref_collide_sk98.argtypes = [ctypes.c_void_p]
+            lib.ref_collide_sk98.restype = ctypes.c_long
             lib.ref_add_plasma.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, _D, _D,
                                            ctypes.c_uint, _D, _D]
             lib.ref_distribute.argtypes = [ctypes.c_void_p]
@@ -346,9 +352,12 @@ class RefSim(_Sim):
 
     def collide(self, scheme: str = "p12") -> int:
         """One CollisionsP12 pass without its time-seeded shuffle (returns ncol),
-        or one CollisionsTA77S pass likewise (returns 0: it keeps no count)."""
+        or one CollisionsTA77S / CollisionsSK98 pass likewise (returns 0: they
+        keep no count)."""
         if scheme == "ta77s":
             return int(self.lib.ref_collide_ta77s(self.h))
+        if scheme == "sk98":
+            return int(self.lib.ref_collide_sk98(self.h))
         return int(self.lib.ref_collide(self.h))
 
     @property

@@ -1801,6 +1801,133 @@ static void ta77s_single(orc_sim* s, coll_rng* g, double m_real_a, double m_real
   B.sp->vz[B.j] = vz_b + kb * du2[2];
 }
 
+/* CollisionsSK98::collide_single (collisionsSK98.cpp:29-244): relativistic
+ * scattering in the centre-of-mass frame by a normal delta whose variance is
+ * the collision frequency (plasma.cpp:54-63) times dt; the CM deflection
+ * angle follows from tan theta_cm = sin theta / (gamma_cm (cos theta -
+ * v_cm / v_rel)), the azimuth is uniform.  Both particles always take the
+ * new velocities (no weight rejection, no correction pass).  Draws: delta
+ * (normal), Phi (uniform angle).  The reference's relative speed subtracts
+ * the CM speeds of two particles moving apart (:131-132); the fixed mode
+ * adds them, as for P12. */
+static void sk98_single(orc_sim* s, coll_rng* g, double m_real_a, double m_real_b, double q_real_a,
+                        double q_real_b, pref pa, pref pb, double density_a_in, double density_b_in,
+                        double debye) {
+  const int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  double charge_a, mass_a, charge_b, mass_b, density_a, density_b;
+  int swap = 0;
+  const double w_ratio = pa.sp->w[pa.j] / pb.sp->w[pb.j];
+  pref A = pa, B = pb;
+  if (w_ratio <= 1) {
+    charge_a = q_real_a; mass_a = m_real_a; density_a = density_a_in;
+    charge_b = q_real_b; mass_b = m_real_b; density_b = density_b_in;
+  } else {
+    A = pb; B = pa;
+    charge_a = q_real_b; mass_a = m_real_b; density_a = density_b_in;
+    charge_b = q_real_a; mass_b = m_real_a; density_b = density_a_in;
+    swap = 1;
+  }
+  double v_a[3], v_b[3];
+  v_a[0] = A.sp->vr[A.j]; v_a[1] = A.sp->vphi[A.j]; v_a[2] = A.sp->vz[A.j];
+  v_b[0] = B.sp->vr[B.j]; v_b[1] = B.sp->vphi[B.j]; v_b[2] = B.sp->vz[B.j];
+  if (v_a[0] == v_b[0] && v_a[1] == v_b[1] && v_a[2] == v_b[2]) return;
+
+  double gamma_a, gamma_b;
+  if (!lorenz_or_flag(s, len2(v_a), &gamma_a) || !lorenz_or_flag(s, len2(v_b), &gamma_b)) return;
+  const double p0_a = gamma_a * mass_a * K_LIGHT_VEL, p0_b = gamma_b * mass_b * K_LIGHT_VEL; /* rel.cpp:57-64 */
+  double p_a[3], p_b[3], beta_cm[3];
+  for (int c = 0; c < 3; ++c) { p_a[c] = v_a[c] * gamma_a; p_a[c] *= mass_a; } /* rel.cpp:66-72 */
+  for (int c = 0; c < 3; ++c) { p_b[c] = v_b[c] * gamma_b; p_b[c] *= mass_b; }
+  for (int c = 0; c < 3; ++c) beta_cm[c] = p_a[c] + p_b[c];
+  const double p0_sum = p0_a + p0_b;
+  for (int c = 0; c < 3; ++c) beta_cm[c] /= p0_sum;
+
+  double gamma_cm;
+  const double v_cm_2 = len2(beta_cm) * K_LIGHT_VEL_POW_2;
+  if (!lorenz_or_flag(s, v_cm_2, &gamma_cm)) return;
+  const double p0_a_cm = gamma_cm * (p0_a - dot3(beta_cm, p_a));
+  const double p0_b_cm = gamma_cm * (p0_b - dot3(beta_cm, p_b));
+
+  /* Lorentz boost of a 3-momentum: p + beta (beta.p)(gamma - 1)/beta^2 + sign beta gamma p0 */
+  double p_a_cm[3], p_b_cm[3], t[3];
+  const double l2 = len2(beta_cm);
+  {
+    const double d = dot3(beta_cm, p_a);
+    for (int c = 0; c < 3; ++c) p_a_cm[c] = p_a[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2; }
+    for (int c = 0; c < 3; ++c) p_a_cm[c] += t[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0_a; }
+    for (int c = 0; c < 3; ++c) p_a_cm[c] -= t[c];
+  }
+  for (int c = 0; c < 3; ++c) p_b_cm[c] = -p_a_cm[c];
+
+  const double gamma_a_cm = p0_a_cm / mass_a / K_LIGHT_VEL;
+  const double gamma_b_cm = p0_b_cm / mass_b / K_LIGHT_VEL;
+  double v_a_cm[3], v_b_cm[3];
+  const double da = mass_a * gamma_a_cm, db = mass_b * gamma_b_cm;
+  for (int c = 0; c < 3; ++c) { v_a_cm[c] = p_a_cm[c] / da; v_b_cm[c] = p_b_cm[c] / db; }
+  double p_cm[3];
+  for (int c = 0; c < 3; ++c) p_cm[c] = p_a_cm[c];
+
+  const double la = sqrt(len2(v_a_cm)), lb = sqrt(len2(v_b_cm));
+  const double v_rel_abs = (fixed ? la + lb : la - lb) / (1 - dot3(v_a_cm, v_b_cm) / K_LIGHT_VEL_POW_2);
+  double gamma_rel;
+  if (!lorenz_or_flag(s, v_rel_abs * v_rel_abs, &gamma_rel)) return;
+  const double p_rel_abs = gamma_rel * mass_b * v_rel_abs;
+  const double density_lowest = density_b < density_a ? density_b : density_a; /* std::min */
+  if (p_rel_abs == 0) return;
+  if (v_rel_abs < K_MNZL) return;
+  const double L_coulomb = coulomb_log(mass_a, mass_b, debye, v_rel_abs);
+  if (L_coulomb <= 0) return;
+  /* phys::plasma::collision_freqency (plasma.cpp:54-63) */
+  const double coll_freq = pow(charge_a * charge_b, 2) * density_lowest * L_coulomb /
+                           (8 * K_PI * pow(K_EPSILON0, 2) * pow(p_rel_abs, 2) * v_rel_abs);
+  const double variance_d = coll_freq * s->dt;
+  const double std_dev_d = sqrt(variance_d);
+  const double delta = coll_normal(g, std_dev_d);
+  const double sin_theta = 2 * delta / (1 + pow(delta, 2));
+  const double cos_theta = 1 - 2 * pow(delta, 2) / (1 + pow(delta, 2));
+  const double tg_theta_cm = sin_theta / (gamma_cm * (cos_theta - sqrt(v_cm_2) / v_rel_abs));
+  const double sin_theta_cm = sin(atan(tg_theta_cm));
+  const double cos_theta_cm = cos(atan(tg_theta_cm));
+  const double phi_angle = (s->rng_kind == ORC_RNG_PHILOX ? coll_draw(g, 2) : mt_uniform(&s->mt)) * (2 * K_PI) + 0.0;
+  const double sin_phi = sin(phi_angle), cos_phi = cos(phi_angle);
+
+  const double p_cm_abs = sqrt(len2(p_cm));
+  const double p_cm_prp = sqrt(p_cm[0] * p_cm[0] + p_cm[1] * p_cm[1]);
+  double d_p[3];
+  d_p[0] = p_cm[0] * p_cm[2] / p_cm_prp * sin_theta_cm * cos_phi
+         - p_cm[1] * p_cm_abs / p_cm_prp * sin_theta_cm * sin_phi
+         - p_cm[0] * (1 - cos_theta_cm);
+  d_p[1] = p_cm[1] * p_cm[2] / p_cm_prp * sin_theta_cm * cos_phi
+         + p_cm[0] * p_cm_abs / p_cm_prp * sin_theta_cm * sin_phi
+         - p_cm[1] * (1 - cos_theta_cm);
+  d_p[2] = -p_cm_prp * sin_theta_cm * cos_phi - p_cm[2] * (1 - cos_theta_cm);
+
+  double pa_prime[3], pb_prime[3];
+  for (int c = 0; c < 3; ++c) { pa_prime[c] = p_a_cm[c] + d_p[c]; pb_prime[c] = p_b_cm[c] - d_p[c]; }
+  /* back to the LAB frame: + beta (beta.p')(gamma - 1)/beta^2 + beta gamma p0_cm */
+  double* outs[2] = {pa_prime, pb_prime};
+  const double p0s[2] = {p0_a_cm, p0_b_cm};
+  for (int k = 0; k < 2; ++k) {
+    double* q = outs[k];
+    const double d = dot3(beta_cm, q);
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2; }
+    for (int c = 0; c < 3; ++c) q[c] += t[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0s[k]; }
+    for (int c = 0; c < 3; ++c) q[c] += t[c];
+  }
+  double v_a_prime[3], v_b_prime[3];
+  for (int c = 0; c < 3; ++c) { v_a_prime[c] = pa_prime[c] / mass_a; v_b_prime[c] = pb_prime[c] / mass_b; }
+  const double gia = pow(1.0 + len2(v_a_prime) / K_LIGHT_VEL_POW_2, -0.5); /* lorenz_factor_inv */
+  const double gib = pow(1.0 + len2(v_b_prime) / K_LIGHT_VEL_POW_2, -0.5);
+  for (int c = 0; c < 3; ++c) { v_a_prime[c] *= gia; v_b_prime[c] *= gib; }
+  const double* to_pa = swap ? v_b_prime : v_a_prime;
+  const double* to_pb = swap ? v_a_prime : v_b_prime;
+  pa.sp->vr[pa.j] = to_pa[0]; pa.sp->vphi[pa.j] = to_pa[1]; pa.sp->vz[pa.j] = to_pa[2];
+  pb.sp->vr[pb.j] = to_pb[0]; pb.sp->vphi[pb.j] = to_pb[1]; pb.sp->vz[pb.j] = to_pb[2];
+}
+
 static int name_is(const char* n, const char* lower, const char* cap) {
   return strcmp(n, lower) == 0 || strcmp(n, cap) == 0;
 }
@@ -1814,7 +1941,8 @@ typedef struct {
 static void ta77s_correct(orc_sim* s, pref* L, unsigned n, double mass, const coll_tot* t);
 
 /* One collision pass over all cells (scheme 0: CollisionsP12, 1:
- * CollisionsTA77S with its correct_velocities).  shuffle: Philox
+ * CollisionsTA77S with its correct_velocities, 2: CollisionsSK98, whose
+ * collide() pairs as P12's does, collisionsSK98.cpp:246-440).  shuffle: Philox
  * Fisher-Yates of the cell lists (ORC_RNG_PHILOX only).  Returns the number
  * of collide_single calls, or a negative status. */
 static long collide_pass(orc_sim* s, int shuffle, int scheme) {
@@ -1919,6 +2047,7 @@ static long collide_pass(orc_sim* s, int shuffle, int scheme) {
 #define COLL(MA, MB, QA, QB, PA, PB, NA, NB) \
       do {                                                                          \
         if (scheme == 1) ta77s_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye);    \
+        else if (scheme == 2) sk98_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye);\
         else p12_single(s, &g, MA, MB, QA, QB, PA, PB, NA, NB, debye);                  \
         g.m++;                                                                      \
         calls++;                                                                    \
@@ -2037,6 +2166,7 @@ static void ta77s_correct(orc_sim* s, pref* L, unsigned n, double mass, const co
 
 long orc_collide(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 0); }
 long orc_collide_ta77s(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 1); }
+long orc_collide_sk98(orc_sim* s, int shuffle) { return collide_pass(s, shuffle, 2); }
 
 
 /* ------------------------------------------------------------------ */

@@ -75,6 +75,7 @@ long orc_collide(orc_sim* s, int shuffle);
 /* One CollisionsTA77S pass (collisionsTA77S.cpp:568-576 without its
  * random_sort): Takizuka-Abe pairs, then the per-cell velocity correction. */
 long orc_collide_ta77s(orc_sim* s, int shuffle);
+long orc_collide_sk98(orc_sim* s, int shuffle);
 /* SpecieP's diagnostic maps (specieP.cpp:665-839): which 0 density, 1
  * temperature, 2 energy, 3 momentum (3 grids); out holds (nr+4) x (nz+4)
  * doubles per grid. */

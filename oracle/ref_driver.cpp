@@ -28,6 +28,7 @@
 #include "domain.hpp"
 #include "collisions/collisionsP12.hpp"
 #include "collisions/collisionsTA77S.hpp"
+#include "collisions/collisionsSK98.hpp"
 
 namespace math::random {
 extern std::mt19937 gen;  // rand.cpp:25, a non-static global
@@ -82,6 +83,19 @@ class TA77SPass : public CollisionsTA77S {
     collect_weighted_params_tot_grid();
     collide();
     correct_velocities();
+  }
+};
+
+// CollisionsSK98::operator() (collisionsSK98.cpp:442-450) without its
+// random_sort; it has no correction pass.
+class SK98Pass : public CollisionsSK98 {
+ public:
+  SK98Pass(Geometry* g, TimeSim* t, std::vector<SpecieP*> sp) : CollisionsSK98(g, t, sp) {}
+  void run_unshuffled() {
+    clear();
+    sort_to_cells();
+    collect_weighted_params_tot_grid();
+    collide();
   }
 };
 
@@ -314,6 +328,14 @@ long ref_collide_ta77s(void* h) {
   RefSim* s = (RefSim*)h;
   pcg_ref_log::g_fatal = false;
   TA77SPass c(s->geometry, &s->time, s->species);
+  c.run_unshuffled();
+  return pcg_ref_log::g_fatal ? -10 : 0;
+}
+
+long ref_collide_sk98(void* h) {
+  RefSim* s = (RefSim*)h;
+  pcg_ref_log::g_fatal = false;
+  SK98Pass c(s->geometry, &s->time, s->species);
   c.run_unshuffled();
   return pcg_ref_log::g_fatal ? -10 : 0;
 }

@@ -62,8 +62,8 @@ def main():
 
 def collisions_fixture(scheme="p12"):
     """One collision pass of the reference (no shuffle, mt19937): scheme
-    "p12" (CollisionsP12) or "ta77s" (CollisionsTA77S with its velocity
-    correction)."""
+    "p12" (CollisionsP12), "ta77s" (CollisionsTA77S with its velocity
+    correction) or "sk98" (CollisionsSK98)."""
     grid = small_grid(nr=8, nz=16, pml=False)
     n = grid.nr * grid.nz * 10
     sim = RefSim(grid)
@@ -90,3 +90,4 @@ if __name__ == "__main__":
     main()
     collisions_fixture("p12")
     collisions_fixture("ta77s")
+    collisions_fixture("sk98")

@@ -87,3 +87,21 @@ def test_oracle_ta77s_matches_reference_fixture():
         p = o.get_particles(sid)
         for k in ("vr", "vphi", "vz"):
             np.testing.assert_array_equal(p[k], d[f"out/p{sid}/{k}"], err_msg=f"species {sid} {k}")
+
+
+def test_oracle_sk98_matches_reference_fixture():
+    """tests/golden/collisions/sk98_pass.npz: one CollisionsSK98 pass of the
+    reference (no shuffle, mt19937 seeded) reproduced bit for bit."""
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "collisions", "sk98_pass.npz"))
+    grid = _grid(d["grid"])
+    o = OracleSim(grid, quirks="reference")
+    o.add(ELECTRONS)
+    o.add(IONS)
+    for sid in (0, 1):
+        o.set_particles(sid, *[d[f"in/p{sid}/{k}"] for k in ("r", "z", "vr", "vphi", "vz", "w")])
+    o.set_rng("mt19937", int(d["seed"]))
+    assert o.collide(scheme="sk98") > 0
+    for sid in (0, 1):
+        p = o.get_particles(sid)
+        for k in ("vr", "vphi", "vz"):
+            np.testing.assert_array_equal(p[k], d[f"out/p{sid}/{k}"], err_msg=f"species {sid} {k}")

@@ -128,6 +128,34 @@ def test_ta77s_collisions_bit_exact(ppc):
     assert ppc == 1 or np.abs(o.get_particles(0)["vz"] - before).max() > 0
 
 
+@pytest.mark.parametrize("ppc", [1, 2, 3, 10])
+def test_sk98_collisions_bit_exact(ppc):
+    """One CollisionsSK98 pass (collisionsSK98.cpp: relativistic CM-frame
+    scattering, no rejection, no correction; no shuffle, the reference's
+    mt19937 draws: normal by the polar method, uniform angle): velocities
+    bit-identical, with unequal electron and ion weights."""
+    if not reference_available():
+        pytest.skip("compiled reference not built (oracle/Makefile.ref)")
+    grid = small_grid(nr=8, nz=16, pml=False)
+    n = grid.nr * grid.nz * ppc
+    o, r = OracleSim(grid, quirks="reference"), RefSim(grid)
+    for sim in (o, r):
+        sim.add(ELECTRONS)
+        sim.add(IONS)
+        sim.set_particles(0, *thermal_plasma(grid, n, 1, 1.0, 1.0, 1e20, t_par_ratio=2.0))
+        sim.set_particles(1, *thermal_plasma(grid, n + 7, 2, 1836.0, 0.5, 1e20))
+    o.set_rng("mt19937", 99)
+    r.seed(99)
+    before = o.get_particles(0)["vz"].copy()
+    assert o.collide(scheme="sk98") >= 0
+    assert r.collide(scheme="sk98") == 0
+    for sid in (0, 1):
+        po, pr = o.get_particles(sid), r.get_particles(sid)
+        for k in ("vr", "vphi", "vz"):
+            np.testing.assert_array_equal(po[k], pr[k], err_msg=f"species {sid} {k}")
+    assert ppc == 1 or np.abs(o.get_particles(0)["vz"] - before).max() > 0
+
+
 @pytest.mark.parametrize("counts", [(4000, 3000), (60, 25)])
 def test_species_maps_bit_exact(counts):
     """SpecieP::calc_density / calc_energy / calc_temperature / calc_momentum
@@ -150,3 +178,40 @@ def test_species_maps_bit_exact(counts):
             a, b = o.species_map(sid, which), r.species_map(sid, which)
             assert np.abs(a).max() > 0, which
             np.testing.assert_array_equal(a, b, err_msg=f"{which} species {sid}")
+
+
+def test_sk98_conserves_momentum_and_energy_at_equal_weights():
+    """Each SK98 pair rotates its CM-frame momentum and boosts back, so at
+    equal weights the relativistic momentum sum(gamma m v) and energy
+    sum(gamma m c^2) of the whole plasma are kept to rounding."""
+    grid = small_grid(nr=8, nz=16, pml=False)
+    n = grid.nr * grid.nz * 10
+    o = OracleSim(grid, quirks="reference")
+    o.add(ELECTRONS)
+    o.add(IONS)
+    masses = (9.1e-31, 1836 * 9.1e-31)
+    for sid, (m, seed, T) in enumerate(((1.0, 1, 1.0), (1836.0, 2, 0.5))):
+        r, z, vr, vphi, vz, w = thermal_plasma(grid, n, seed, m, T, 1e20)
+        o.set_particles(sid, r, z, vr * 30, vphi * 30, vz * 30, np.full_like(w, 1e6))
+
+    def totals():
+        p_sum, e_sum = np.zeros(3), 0.0
+        for sid, m in enumerate(masses):
+            p = o.get_particles(sid)
+            v = np.stack([p["vr"], p["vphi"], p["vz"]])
+            g = 1 / np.sqrt(1 - (v ** 2).sum(0) / 9e16)
+            p_sum += (g * m * v).sum(1)
+            e_sum += (g * m * 9e16).sum()
+        return p_sum, e_sum
+
+    p0, e0 = totals()
+    before = o.get_particles(0)["vz"].copy()
+    o.set_rng("mt19937", 5)
+    assert o.collide(scheme="sk98") > 0
+    p1, e1 = totals()
+    assert np.abs(o.get_particles(0)["vz"] - before).max() > 0
+    # rounding against the sum of the momenta's magnitudes
+    scale = sum(m * np.abs(np.stack([o.get_particles(sid)[k] for k in ("vr", "vphi", "vz")])).sum()
+                for sid, m in enumerate(masses))
+    assert np.abs(p1 - p0).max() <= 1e-13 * scale
+    assert abs(e1 / e0 - 1) < 1e-14
