@@ -254,17 +254,24 @@ int pcg_collide(pcg_handle* h, unsigned long long* pair_calls);
 
 /* The binary operator of pcg_collide and of PCG_COLLISIONS_BINARY steps;
  * replaces the compile-time choice of collisions scheme
- * (Domain::Domain domain.cpp:55-60, CollisionsP12 or CollisionsTA77S).
+ * (Domain::Domain domain.cpp:55-60: CollisionsP12, CollisionsTA77S or
+ * CollisionsSK98).
  * PCG_COLLIDE_TA77S is collisionsTA77S.cpp: Takizuka-Abe pairs with the
  * weighted second angle (:33-208) in the same pairing sequence, then
  * correct_velocities (:419-566), which gives each species of each cell back
  * its momentum and kinetic energy from before the pass.
  * PCG_QUIRKS_REFERENCE keeps its sign of b's velocity change (+m_ab/m_b du2,
  * :191-193) and its |alpha| for a negative correction factor; the fixed mode
- * subtracts and leaves such a species uncorrected.  The learned step's
+ * subtracts and leaves such a species uncorrected.  PCG_COLLIDE_SK98 is
+ * collisionsSK98.cpp:29-244: the CM momentum of each pair rotated by a
+ * normal delta of variance (collision frequency) x dt and both particles
+ * boosted back, no weight rejection, no correction; the reference subtracts
+ * the CM speeds in the relative velocity (:131-132), the fixed mode adds
+ * them.  The learned step's
  * fallback is always P12, the operator its model was trained on. */
 #define PCG_COLLIDE_P12 0
 #define PCG_COLLIDE_TA77S 1
+#define PCG_COLLIDE_SK98 2
 int pcg_set_collision_scheme(pcg_handle* h, int scheme);
 
 /* The per-cell collision MLP of the learned collision step (no counterpart

@@ -970,7 +970,8 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
 }
 
 int pcg_set_collision_scheme(pcg_handle* h, int scheme) {
-  if (!h || (scheme != PCG_COLLIDE_P12 && scheme != PCG_COLLIDE_TA77S)) return PCG_ERR_ARG;
+  if (!h || (scheme != PCG_COLLIDE_P12 && scheme != PCG_COLLIDE_TA77S && scheme != PCG_COLLIDE_SK98))
+    return PCG_ERR_ARG;
   h->coll_scheme = scheme;
   return PCG_OK;
 }

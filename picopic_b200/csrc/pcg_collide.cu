@@ -562,6 +562,123 @@ __device__ void ta77s_single(PairCtx& x, double m_real_a, double m_real_b, doubl
   store_v(*x.tab, swap ? ra : rb, nb);
 }
 
+// ---------------------------------------------------------------------------
+// 5''. the relativistic centre-of-mass scheme of CollisionsSK98
+// (collisionsSK98.cpp:29-244): a normal delta whose variance is the
+// collision frequency (plasma.cpp:54-63) times dt (Box-Muller on draws 0 and
+// 1), the CM deflection tan theta_cm = sin theta / (gamma_cm (cos theta -
+// v_cm / v_rel)), the azimuth Phi (draw 2); the CM momentum is rotated and
+// both particles boosted back, with no weight rejection and no correction
+// pass.  The reference subtracts the CM speeds of two particles moving apart
+// (:131-132); the fixed mode adds them, as for P12.
+
+__device__ void sk98_single(PairCtx& x, double m_real_a, double m_real_b, double q_real_a,
+                            double q_real_b, unsigned long long ra, unsigned long long rb,
+                            double density_a_in, double density_b_in, double debye) {
+  const CollParams& P = *x.p;
+  double va0[3], vb0[3], wa0, wb0;
+  load_v(*x.tab, ra, va0, &wa0);
+  load_v(*x.tab, rb, vb0, &wb0);
+  const bool swap = !(wa0 / wb0 <= 1);
+  const double charge_a = swap ? q_real_b : q_real_a, mass_a = swap ? m_real_b : m_real_a;
+  const double charge_b = swap ? q_real_a : q_real_b, mass_b = swap ? m_real_a : m_real_b;
+  const double density_a = swap ? density_b_in : density_a_in;
+  const double density_b = swap ? density_a_in : density_b_in;
+  const double* v_a = swap ? vb0 : va0;
+  const double* v_b = swap ? va0 : vb0;
+  if (v_a[0] == v_b[0] && v_a[1] == v_b[1] && v_a[2] == v_b[2]) return;
+
+  double gamma_a, gamma_b;
+  if (!lorenz(len2(v_a), &gamma_a) || !lorenz(len2(v_b), &gamma_b)) { raise_error(P.status, kErrSuperluminal); return; }
+  const double p0_a = gamma_a * mass_a * kC, p0_b = gamma_b * mass_b * kC;
+  double p_a[3], p_b[3], beta_cm[3], t[3];
+  for (int c = 0; c < 3; ++c) { p_a[c] = v_a[c] * gamma_a; p_a[c] *= mass_a; }
+  for (int c = 0; c < 3; ++c) { p_b[c] = v_b[c] * gamma_b; p_b[c] *= mass_b; }
+  for (int c = 0; c < 3; ++c) beta_cm[c] = p_a[c] + p_b[c];
+  const double p0_sum = p0_a + p0_b;
+  for (int c = 0; c < 3; ++c) beta_cm[c] /= p0_sum;
+  double gamma_cm;
+  const double v_cm_2 = len2(beta_cm) * kC2;
+  if (!lorenz(v_cm_2, &gamma_cm)) { raise_error(P.status, kErrSuperluminal); return; }
+  const double p0_a_cm = gamma_cm * (p0_a - dot3(beta_cm, p_a));
+  const double p0_b_cm = gamma_cm * (p0_b - dot3(beta_cm, p_b));
+  const double l2 = len2(beta_cm);
+
+  double p_a_cm[3], p_b_cm[3];
+  {
+    const double d = dot3(beta_cm, p_a);
+    for (int c = 0; c < 3; ++c) p_a_cm[c] = p_a[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2; }
+    for (int c = 0; c < 3; ++c) p_a_cm[c] += t[c];
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0_a; }
+    for (int c = 0; c < 3; ++c) p_a_cm[c] -= t[c];
+  }
+  for (int c = 0; c < 3; ++c) p_b_cm[c] = -p_a_cm[c];
+  const double gamma_a_cm = p0_a_cm / mass_a / kC;
+  const double gamma_b_cm = p0_b_cm / mass_b / kC;
+  double v_a_cm[3], v_b_cm[3];
+  const double da = mass_a * gamma_a_cm, db = mass_b * gamma_b_cm;
+  for (int c = 0; c < 3; ++c) { v_a_cm[c] = p_a_cm[c] / da; v_b_cm[c] = p_b_cm[c] / db; }
+  const double la = sqrt(len2(v_a_cm)), lb = sqrt(len2(v_b_cm));
+  const double v_rel_abs = (P.fixed ? la + lb : la - lb) / (1 - dot3(v_a_cm, v_b_cm) / kC2);
+  double gamma_rel;
+  if (!lorenz(v_rel_abs * v_rel_abs, &gamma_rel)) { raise_error(P.status, kErrSuperluminal); return; }
+  const double p_rel_abs = gamma_rel * mass_b * v_rel_abs;
+  const double density_lowest = density_b < density_a ? density_b : density_a;
+  if (p_rel_abs == 0) return;
+  if (v_rel_abs < kMnzl) return;
+  const double m_red = mass_a * mass_b / (mass_a + mass_b);
+  const double cl = log(debye * m_red * v_rel_abs / kPlankBar);  // plasma.cpp:42-52
+  const double L_coulomb = cl > 2. ? cl : 2.;
+  const double qq = charge_a * charge_b;
+  const double coll_freq = (qq * qq) * density_lowest * L_coulomb /
+                           (8 * kPi * (kEps0 * kEps0) * (p_rel_abs * p_rel_abs) * v_rel_abs);
+  const double std_dev_d = sqrt(coll_freq * P.dt);
+  uint32_t o[4], o2[4];
+  philox4x32_10(x.cell, 2u * x.m, P.pass, kCollTag, (uint32_t)P.seed, (uint32_t)(P.seed >> 32), o);
+  philox4x32_10(x.cell, 2u * x.m + 1u, P.pass, kCollTag, (uint32_t)P.seed, (uint32_t)(P.seed >> 32), o2);
+  const double u0 = u53(o[0], o[1]), u1 = u53(o[2], o[3]);
+  const double delta = sqrt(-2.0 * log(1.0 - u0)) * cos(2.0 * kPi * u1) * std_dev_d;
+  const double sin_theta = 2 * delta / (1 + delta * delta);
+  const double cos_theta = 1 - 2 * (delta * delta) / (1 + delta * delta);
+  const double tg_theta_cm = sin_theta / (gamma_cm * (cos_theta - sqrt(v_cm_2) / v_rel_abs));
+  double sin_theta_cm, cos_theta_cm;
+  sincos(atan(tg_theta_cm), &sin_theta_cm, &cos_theta_cm);
+  const double phi_angle = u53(o2[0], o2[1]) * (2 * kPi) + 0.0;
+  double sin_phi, cos_phi;
+  sincos(phi_angle, &sin_phi, &cos_phi);
+
+  const double* p_cm = p_a_cm;
+  const double p_cm_abs = sqrt(len2(p_cm));
+  const double p_cm_prp = sqrt(p_cm[0] * p_cm[0] + p_cm[1] * p_cm[1]);
+  double d_p[3];
+  d_p[0] = p_cm[0] * p_cm[2] / p_cm_prp * sin_theta_cm * cos_phi -
+           p_cm[1] * p_cm_abs / p_cm_prp * sin_theta_cm * sin_phi - p_cm[0] * (1 - cos_theta_cm);
+  d_p[1] = p_cm[1] * p_cm[2] / p_cm_prp * sin_theta_cm * cos_phi +
+           p_cm[0] * p_cm_abs / p_cm_prp * sin_theta_cm * sin_phi - p_cm[1] * (1 - cos_theta_cm);
+  d_p[2] = -p_cm_prp * sin_theta_cm * cos_phi - p_cm[2] * (1 - cos_theta_cm);
+
+  // back to the LAB frame: p' + beta (beta.p')(gamma_cm - 1)/beta^2 + beta gamma_cm p0_cm
+  double v_new[2][3];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    double q[3];
+    for (int c = 0; c < 3; ++c) q[c] = k == 0 ? p_a_cm[c] + d_p[c] : p_b_cm[c] - d_p[c];
+    const double d = dot3(beta_cm, q);
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * d; t[c] *= (gamma_cm - 1); t[c] /= l2; }
+    for (int c = 0; c < 3; ++c) q[c] += t[c];
+    const double p0k = k == 0 ? p0_a_cm : p0_b_cm;
+    for (int c = 0; c < 3; ++c) { t[c] = beta_cm[c] * gamma_cm; t[c] *= p0k; }
+    for (int c = 0; c < 3; ++c) q[c] += t[c];
+    const double mk = k == 0 ? mass_a : mass_b;
+    for (int c = 0; c < 3; ++c) v_new[k][c] = q[c] / mk;
+    const double gi = pow(1.0 + len2(v_new[k]) / kC2, -0.5);  // rel.cpp:47-55
+    for (int c = 0; c < 3; ++c) v_new[k][c] *= gi;
+  }
+  store_v(*x.tab, swap ? rb : ra, v_new[0]);
+  store_v(*x.tab, swap ? ra : rb, v_new[1]);
+}
+
 // correct_velocities (collisionsTA77S.cpp:419-566) of one list of one cell:
 // remove the list's momentum change and scale its thermal velocities by
 // sqrt(alpha) so that momentum and kinetic energy return to the totals t
@@ -615,8 +732,11 @@ __global__ void ta77s_correct_kernel(GridGeom g, Staged tab, CollParams p, const
 }
 
 // ---------------------------------------------------------------------------
-// 5. the per-cell pairing sequence (collisionsP12.cpp:338-548)
+// 5. the per-cell pairing sequence (collisionsP12.cpp:338-548), one kernel
+// instance per scheme (SCHEME = CollParams::scheme: 0 P12, 1 TA77S, 2 SK98)
+// so that each is compiled, and given registers, for its own pair function.
 
+template <int SCHEME>
 __global__ void collide_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
                                const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                const unsigned* n_i, const unsigned long long* li, const double* mom,
@@ -640,7 +760,8 @@ __global__ void collide_kernel(GridGeom g, Staged tab, CollParams p, const unsig
   PairCtx x{&tab, &p, (uint32_t)c, 0u, p.expect ? expect : nullptr};
 #define COLL(MA, MB, QA, QB, A, B, NA, NB)                                       \
   do {                                                                           \
-    if (p.scheme == 1) ta77s_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);      \
+    if (SCHEME == 1) ta77s_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);        \
+    else if (SCHEME == 2) sk98_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);    \
     else p12_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);                     \
     ++x.m;                                                                       \
   } while (0)
@@ -801,9 +922,9 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                         w.start[1], w.count[1], w.keys2[1], w.moments,
                                                         w.row_stop, p.scheme == 1 ? w.totals : nullptr);
-  collide_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
-                                                        w.start[1], w.count[1], w.keys2[1], w.moments,
-                                                        w.row_stop, w.calls);
+  auto collide = p.scheme == 1 ? collide_kernel<1> : p.scheme == 2 ? collide_kernel<2> : collide_kernel<0>;
+  collide<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0], w.start[1],
+                                                 w.count[1], w.keys2[1], w.moments, w.row_stop, w.calls);
   if (p.scheme == 1) {
     ta77s_correct_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                                 w.start[1], w.count[1], w.keys2[1], w.totals);

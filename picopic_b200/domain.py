@@ -238,8 +238,9 @@ class Domain:
 
     def set_collision_scheme(self, scheme):
         """Binary operator of collide() and "binary" steps: "p12" (CollisionsP12,
-        the default) or "ta77s" (CollisionsTA77S with its velocity correction)."""
-        code = {"p12": 0, "ta77s": 1}[scheme]
+        the default), "ta77s" (CollisionsTA77S with its velocity correction) or
+        "sk98" (CollisionsSK98)."""
+        code = {"p12": 0, "ta77s": 1, "sk98": 2}[scheme]
         self._check(self.lib.pcg_set_collision_scheme(self.h, code), "pcg_set_collision_scheme")
 
     def set_collisions(self, mode):

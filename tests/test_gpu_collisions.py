@@ -189,3 +189,49 @@ def test_ta77s_relaxes_anisotropy():
     for _ in range(40):
         gpu.collide()
     assert aniso() < a0 - 0.01
+
+
+@pytest.mark.parametrize("quirks", ["reference", "fixed"])
+def test_sk98_f64_matches_oracle(quirks):
+    """CollisionsSK98 pairs (collisionsSK98.cpp:29-244) with the oracle's
+    Philox draws, two passes."""
+    gpu, orc, calls = _pair("f64", quirks, passes=2, scheme="sk98")
+    assert all(c[0] == c[1] > 0 for c in calls)
+    _compare(gpu, orc, RTOL_F64)
+
+
+def test_sk98_f32_matches_oracle():
+    gpu, orc, _ = _pair("f32", "fixed", scheme="sk98")
+    _compare(gpu, orc, RTOL_F32)
+
+
+@pytest.mark.parametrize("quirks", ["reference", "fixed"])
+def test_sk98_conserves_momentum_and_energy_at_equal_weights(quirks):
+    """Each SK98 pair rotates its CM momentum and boosts back; with equal
+    weights the relativistic momentum and kinetic energy sums drift only by
+    the rounding of the transforms (RTOL_CONS_PASS per pass), in both modes
+    (the reference's relative speed only sets the scattering strength)."""
+    gpu, _, _ = _pair("f64", quirks, ppc=30, extra_ions=0, scheme="sk98")
+    c2 = 9e16
+
+    def totals():
+        out = np.zeros(4)
+        for sid, m in ((0, ME), (1, 1836 * ME)):
+            p = gpu.get_particles(sid)
+            v2 = p["vr"] ** 2 + p["vphi"] ** 2 + p["vz"] ** 2
+            g = 1 / np.sqrt(1 - v2 / c2)
+            mw = m * p["w"]
+            out += [np.sum(mw * g * p["vr"]), np.sum(mw * g * p["vphi"]), np.sum(mw * g * p["vz"]),
+                    np.sum(mw * v2 * g * g / (g + 1))]
+        return out
+
+    t0 = totals()
+    before = gpu.get_particles(0)["vz"].copy()
+    for _ in range(3):
+        assert gpu.collide() > 0
+    t1 = totals()
+    assert np.abs(gpu.get_particles(0)["vz"] - before).max() > 0
+    p0 = gpu.get_particles(0)
+    pscale = np.sum(ME * p0["w"] * np.sqrt(p0["vr"] ** 2 + p0["vphi"] ** 2 + p0["vz"] ** 2))
+    assert np.abs(t1[:3] - t0[:3]).max() <= 3 * RTOL_CONS_PASS * pscale
+    assert abs(t1[3] - t0[3]) <= 3 * RTOL_CONS_PASS * t0[3]
