@@ -45,6 +45,11 @@ def test_refusals():
         config.load(bad)
 
 
+def test_unknown_plasma_initialiser_is_refused():
+    with pytest.raises(ValueError):
+        config.build_domain(config.load(CFG), plasma="uniform")
+
+
 class _CountingDomain:
     """Stands in for a Domain: every grid holds the number of steps taken."""
     def __init__(self, shape):
