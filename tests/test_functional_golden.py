@@ -22,7 +22,8 @@ plasma (the bunch is above REL_LIMIT, where both are relativistic).
 
 The first test runs the compiled reference with its own initialiser and
 the oracle from the same particles in lockstep: identical bit for bit after
-81 steps, and both within the bound.  Another runs the reference's own
+81 steps, and both within the bound; on that state the species maps and a
+pass of each collision scheme are identical too.  Another runs the reference's own
 scheduler with the test's 2 x 4 domains.  The last starts the oracle from
 the restated initial condition (picopic_b200.initial), the one the GPU
 tests use.
@@ -110,6 +111,21 @@ def test_reference_run_meets_its_known_answers_and_the_oracle_follows_it():
             np.testing.assert_array_equal(po[key], pr[key], err_msg=f"species {k} {key}")
     assert orc.count(len(plasma)) > 400  # the bunch entered
     check(probe_std(ref), RTOL_ONE_RUN, "compiled reference")
+    # on this evolved state: the species maps, then one pass of each binary
+    # collision scheme (the bunch counts as electrons, collisions.cpp:28-48)
+    for which in ("density", "energy", "temperature", "momentum"):
+        for k in range(len(plasma) + len(beams)):
+            np.testing.assert_array_equal(orc.species_map(k, which), ref.species_map(k, which),
+                                          err_msg=f"{which} species {k}")
+    for scheme, seed in (("p12", 11), ("ta77s", 12), ("sk98", 13)):
+        ref.seed(seed)
+        orc.set_rng("mt19937", seed)
+        ref.collide(scheme=scheme)
+        assert orc.collide(scheme=scheme) > 0
+        for k in range(len(plasma) + len(beams)):
+            po, pr = orc.get_particles(k), ref.get_particles(k)
+            for key in ("vr", "vphi", "vz"):
+                np.testing.assert_array_equal(po[key], pr[key], err_msg=f"{scheme} species {k} {key}")
 
 
 def test_vay_zigzag_oracle_follows_the_reference_on_the_functional_run():
