@@ -242,6 +242,9 @@ def run_gpu(args):
         torch.cuda.empty_cache()
     if not args.no_e2e:
         e2e = run_e2e(w, args, rank, local, barrier, allmax, allsum)
+    cfg0 = None
+    if not args.no_config0:
+        cfg0 = run_config0(args, local, barrier, allmax, allsum, rank, world)
     acc = None
     if not args.no_accuracy and world == 1:
         acc = run_accuracy(w, args, local)
@@ -273,6 +276,7 @@ def run_gpu(args):
             "kernel_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in kt.items() if v[1]},
             "clocks": clocks,
             "f64": f64,
+            "config0": cfg0,
             "e2e": e2e,
             "collisions": coll,
             "large": large,
@@ -533,6 +537,58 @@ def run_e2e(w, args, rank, local, barrier, allmax, allsum):
             "path": "pcg_append_species (pinned host, bunch slice) + pcg_step(1) + pcg_synchronize"}
 
 
+# The plain FP64 configuration: 128 x 512 cells of 1e-4 m, electrons and
+# protons at 1e17 m^-3, 20 macroparticles per cell per species (r = R sqrt(U),
+# z uniform), Maxwellian at Te = 1 eV, Ti = 0.1 eV, relativistic Boris, VB,
+# Yee, dt 0.5 Courant, no bunch, no collisions.
+CONFIG0 = dict(name="plain FP64 plasma 128x512, 20 ppc/species e+p, Te 1 eV, Ti 0.1 eV",
+               nr=128, nz=512, dr=DR, dz=DR, density=1e17, ppc=20, te=1.0, ti=0.1,
+               pusher="borisrel", current="vb")
+
+
+def run_config0(args, local, barrier, allmax, allsum, rank, world):
+    """The plain configuration in FP64 on the GPU (particle-steps/s over K
+    steps) and, on rank 0 of a one-GPU run, the reference's own hot path on
+    one host core over the whole configuration with host-generated particles
+    of the same distribution (2 steps after one warm-up), so that the FP64
+    speed-up is stated without a precision change."""
+    import torch
+    from picopic_b200 import Domain, Geometry
+    w = CONFIG0
+    g = Geometry(w["nr"], w["nz"], w["nr"] * w["dr"], w["nz"] * w["dz"], dt_courant(w["dr"]))
+    d = Domain(g, pusher=w["pusher"], current=w["current"], precision="f64", seed=1234, device=local)
+    n = w["nr"] * w["nz"] * w["ppc"]
+    e = d.add(_spec("electrons", -1, 1, 1), capacity=n)
+    i = d.add(_spec("ions", 1, 1836, 2), capacity=n)
+    d.seed_plasma(e, n, w["density"], w["te"], 1234)
+    d.seed_plasma(i, n, w["density"], w["ti"], 1235)
+    d.step(args.warmup)
+    d.synchronize()
+    p0 = d.diag().particle_steps
+    k = max(10, args.steps)
+    barrier()
+    ms = allmax(timed_steps(d, k, d.stream))
+    p1 = d.diag().particle_steps
+    out = {"workload": w["name"], "grid": [w["nr"], w["nz"]], "particles": int(d.diag().particles),
+           "precision": "f64", "pusher": w["pusher"], "current": w["current"],
+           "value": allsum(float(p1 - p0)) / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+           "bytes_per_particle_step": BYTES_PER_PARTICLE_F64}
+    del d
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sim, kind, npart = _ref_domain(w, w["nz"], 11)
+        sim.step(1)
+        t0 = time.perf_counter()
+        steps = 2
+        sim.step(steps)
+        el = time.perf_counter() - t0
+        out["cpu_reference_1core"] = {"value": npart * steps / el, "unit": UNIT, "cores": 1, "kind": kind,
+                                      "sample": f"the whole configuration, {npart} particles, {steps} steps "
+                                                "after 1, reference hot path compiled with its release flags"}
+        out["gpu_over_cpu_1core"] = out["value"] / out["cpu_reference_1core"]["value"]
+    return out
+
+
 # ---------------------------------------------------------------------------
 # CPU arms (the reference's own sources, compiled by oracle/Makefile.ref)
 
@@ -582,7 +638,7 @@ def cpu_baseline(w, nz=256, steps=2):
                       "reference hot path compiled with its release flags"}
 
 
-def _smb_reference(w, steps):
+def _smb_reference(w, steps, warmup=1):
     """The reference's own scheduler (src/SMB.cpp, unmodified, release flags,
     OpenMP over domains, its overlays): the workload's radial extent cut into
     square 64 x 64-cell domains (its overlays need square domains, and each
@@ -605,7 +661,7 @@ def _smb_reference(w, steps):
     smb.build()
     smb.distribute()
     n = smb.particles()
-    assert smb.step(1) == 0  # warm-up
+    assert smb.step(warmup) == 0
     t0 = time.perf_counter()
     assert smb.step(steps) == 0
     el = time.perf_counter() - t0
@@ -619,13 +675,15 @@ def run_reference(args):
     if rank != 0:
         return
     w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
-    steps = max(1, args.steps // 25)
+    # the same K and W as the GPU arm (a slab step takes ~0.2 s on 16 threads),
+    # bounded so that the arm ends within a few minutes on small hosts
+    steps, warmup = min(args.steps, 60), min(args.warmup, 10)
     from oracle.harness import smb_available
     if smb_available():
-        n, el, threads, sample = _smb_reference(w, steps)
+        n, el, threads, sample = _smb_reference(w, steps, warmup)
         value = n * steps / el
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-                "steps": steps, "warmup": 1, "ms_per_step": el * 1e3 / steps, "higher_is_better": True,
+                "steps": steps, "warmup": warmup, "ms_per_step": el * 1e3 / steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": w["name"], "sample": sample},
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
@@ -640,8 +698,8 @@ def run_reference(args):
     for t in range(threads):
         s, kind, n = _ref_domain(w, nz, 100 + t)
         sims.append((s, n))
-    for s, _ in sims:  # one warm-up step per domain
-        s.step(1)
+    for s, _ in sims:  # warm-up steps per domain
+        s.step(warmup)
 
     def work(s):
         s.step(steps)
@@ -656,7 +714,7 @@ def run_reference(args):
     total = sum(n for _, n in sims) * steps
     value = total / el
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-            "steps": steps, "warmup": 1, "ms_per_step": el * 1e3 / steps, "higher_is_better": True,
+            "steps": steps, "warmup": warmup, "ms_per_step": el * 1e3 / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": w["name"], "sample": f"{threads} domains of {w['nr']}x{nz} cells, "
                                                         f"one per host thread"},
@@ -683,6 +741,7 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-config0", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -426,8 +426,14 @@ int pcg_set_collisions(pcg_handle* h, int mode);
  * grids with (nr+4)*(nz+4) > PCG_NOALLOC_MAX_NODES return PCG_ERR_CAPACITY;
  * each call clears the scratch first, so calls that overlap on the GPU
  * (different streams, no ordering) race.  The first call on each device
- * looks up the scratch address; make that first call before any stream
- * capture on that device. */
+ * (and the first after a cudaDeviceReset) looks up the scratch address;
+ * under lazy module loading (the CUDA default) that lookup also loads the
+ * library's device code, which reserves the 2 MiB array and may
+ * synchronise.  So make one warm-up call on each device before the region
+ * that must not allocate, and before any stream capture on that device, or
+ * run with CUDA_MODULE_LOADING=EAGER.  A non-NULL move_errors while
+ * `stream` is being captured returns PCG_ERR_STATE: its read-back would
+ * synchronise the stream. */
 #define PCG_NOALLOC_MAX_NODES 262144
 int pcg_current_vb_f64_noalloc(int nr, int nz, double radius, double longitude, double dt,
                                size_t n, double charge_e, const double* r, const double* z,

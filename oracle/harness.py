@@ -25,7 +25,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF_SRC = os.environ.get("PICOPIC_REFERENCE", "/root/reference")
+REF_ROOT_FILE = os.path.join(HERE, "_ref", "reference_root")
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
@@ -58,12 +58,28 @@ def build_oracle(force: bool = False) -> str:
     return ORACLE_SO
 
 
-def build_reference(jobs: int = 8) -> bool:
-    """Compile the reference hot path (oracle/Makefile.ref) when its sources are present."""
-    if not os.path.isdir(os.path.join(REF_SRC, "src")):
+def reference_root() -> str | None:
+    """The reference checkout: $PICOPIC_REFERENCE, else the checkout the last
+    build_reference compiled (recorded in oracle/_ref/reference_root); None
+    when neither names a directory with the reference's sources."""
+    root = os.environ.get("PICOPIC_REFERENCE")
+    if not root and os.path.exists(REF_ROOT_FILE):
+        with open(REF_ROOT_FILE) as f:
+            root = f.read().strip()
+    return root if root and os.path.isdir(os.path.join(root, "src")) else None
+
+
+def build_reference(root: str | None = None, jobs: int = 8) -> bool:
+    """Compile the reference hot path (oracle/Makefile.ref) from the checkout
+    `root` (default: reference_root()); False when there is none."""
+    root = root or reference_root()
+    if not root or not os.path.isdir(os.path.join(root, "src")):
         return False
     subprocess.check_call(["make", "-s", "-f", os.path.join("oracle", "Makefile.ref"),
-                           f"REF={REF_SRC}", f"-j{jobs}"], cwd=REPO)
+                           f"REF={root}", f"-j{jobs}"], cwd=REPO)
+    os.makedirs(REF_DIR, exist_ok=True)
+    with open(REF_ROOT_FILE, "w") as f:
+        f.write(os.path.abspath(root) + "\n")
     return True
 
 

@@ -99,6 +99,9 @@ struct pcg_handle {
   // per tile run 6.9
   unsigned target_blocks = 148 * 16, min_split = 1024;
   bool timers = false;
+  // set when a tensor-core wait timed out: the kernel's TMEM may still be in
+  // use, so the handle refuses further steps and collisions
+  bool halted = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
   std::string err;
@@ -512,8 +515,12 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (!collision_species(h, v, p))
     return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
   unsigned long long counts[2] = {0, 0};
-  if (learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream) != 0)
-    return fail(h, PCG_ERR_CUDA, "learned collision step");
+  const int lr = learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream);
+  if (lr == kLearnedTimeout) {
+    h->halted = true;
+    return fail(h, PCG_ERR_TIMEOUT, "learned collision step: a tensor-core wait timed out; the handle is halted");
+  }
+  if (lr != 0) return fail(h, PCG_ERR_CUDA, "learned collision step");
   h->launches += 1 + 2 * v.size();
   if (counts[1]) {  // the binary operator on the cells outside the training box
     p.pass = h->coll_pass++;
@@ -963,6 +970,7 @@ int pcg_set_collision_model(pcg_handle* h, const float* params, const float* nor
 
 int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells) {
   if (!h) return PCG_ERR_ARG;
+  if (h->halted) return fail(h, PCG_ERR_TIMEOUT, "halted after a tensor-core time-out");
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
   if ((rc = run_collide_learned(h, learned_cells, fallback_cells)) != PCG_OK) return rc;
@@ -1108,6 +1116,7 @@ int pcg_stage(pcg_handle* h, int stage) {
 
 int pcg_step(pcg_handle* h, int nsteps) {
   if (!h || nsteps < 0) return PCG_ERR_ARG;
+  if (h->halted) return fail(h, PCG_ERR_TIMEOUT, "halted after a tensor-core time-out");
   h->started = true;
   for (int n = 0; n < nsteps; ++n) {
     int rc = fused_step(h);

@@ -249,16 +249,19 @@ __global__ void __launch_bounds__(mlp::tc::kThreads) learned_cells_kernel(GridGe
       flag[c] = stt;
     }
   }
-  mlp::tc::end(sm.t);
+  mlp::tc::end(sm.t, phase);
   if (r == 0) {
     if (sm.n_learned) atomicAdd(count, sm.n_learned);
     if (sm.n_fallback) atomicAdd(count + 1, sm.n_fallback);
   }
 }
 
-__global__ void transform_kernel(GridGeom g, CollSpecies sp, const double* xform, const unsigned char* flag) {
+// Applies the per-cell transforms; after a tensor-core time-out (count[2])
+// the transforms are incomplete and nothing is applied.
+__global__ void transform_kernel(GridGeom g, CollSpecies sp, const double* xform, const unsigned char* flag,
+                                 const unsigned long long* count) {
   const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (j >= sp.n) return;
+  if (j >= sp.n || count[2]) return;
   size_t c;
   double v[3];
   if (!slot_of(g, sp, j, &c, v) || flag[c] != 1) return;
@@ -322,11 +325,12 @@ int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const Learne
   learned_cells_kernel<<<blocks, mlp::tc::kThreads, smem, s>>>(g, ph, w.mom, w.params, w.norm, w.xform, w.flag,
                                                                 w.count);
   for (int t = 0; t < nsp; ++t)
-    if (sp[t].n) transform_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.xform, w.flag);
+    if (sp[t].n) transform_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.xform, w.flag, w.count);
   unsigned long long c3[3] = {0, 0, 0};
   if (cudaMemcpyAsync(c3, w.count, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess || c3[2])  // c3[2]: a wait for the tensor cores timed out
+      cudaStreamSynchronize(s) != cudaSuccess)
     return -1;
+  if (c3[2]) return kLearnedTimeout;  // a wait for the tensor cores timed out; no velocity was changed
   counts[0] = c3[0];
   counts[1] = c3[1];
   return cudaGetLastError() == cudaSuccess ? 0 : -1;

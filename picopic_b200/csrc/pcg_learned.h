@@ -51,6 +51,10 @@ int learned_features(const GridGeom& g, const CollSpecies* sp, int nsp, const Le
 // One learned collision step: moments, features, MLP, transform.  Cells
 // outside the training box are flagged 2 in w.flag (the caller runs the
 // binary operator on them); counts[0] learned cells, counts[1] fallback.
+// Returns 0, -1 on a CUDA error, or kLearnedTimeout when a wait for the
+// tensor cores timed out (no velocity changed; the kernel's TMEM may still
+// be held, so the caller stops using the device work of this handle).
+constexpr int kLearnedTimeout = 1;
 int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const LearnedPhys& ph, LearnedWork& w,
                  unsigned long long counts[2], cudaStream_t s);
 int learned_set_model(LearnedWork& w, const float* params_host, const float* norm_host, cudaStream_t s);

@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) forward_tc_kernel(const float
     if (row < rows)
       for (int q = 0; q < kOut; ++q) y[row * kOut + q] = out[q];
   }
-  tc::end(sm);
+  tc::end(sm, phase);
 }
 
 }  // namespace

@@ -160,13 +160,21 @@ __device__ __forceinline__ void begin(Smem& sm) {
   fence_after();
 }
 
-__device__ __forceinline__ void end(Smem& sm) {
+// Release of the TMEM columns.  After a timed-out wait (sm.stop) the last
+// committed MMA may still be writing them, so warp 0 first waits again,
+// bounded, for that commit (phase counts the committed phases); if it has
+// still not arrived the columns stay allocated rather than be handed to
+// another CTA under a running MMA.  The caller has reported the time-out,
+// and the host treats the kernel's results as invalid.
+__device__ __forceinline__ void end(Smem& sm, uint32_t phase) {
   fence_before();
   __syncthreads();
   if (threadIdx.x < 32) {
+    const bool drained = !sm.stop || phase == 0 || __all_sync(0xffffffffu, wait(&sm.mbar, (phase - 1) & 1));
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTmemCols)
-                 : "memory");
+    if (drained)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem), "r"(kTmemCols)
+                   : "memory");
   }
 }
 

@@ -36,24 +36,62 @@ struct Scratch {
 };
 
 // Host code must not use g_reset's name as a device address; the address is
-// looked up once per device, with that device current.
+// looked up with the device current, once per device and context.  The
+// context's id is part of the key: after a cudaDeviceReset the runtime loads
+// the module again, possibly elsewhere, in a new primary context, and a
+// cached address from the old one would point at freed memory.
 constexpr int kMaxDevices = 64;
-Scratch g_scratch[kMaxDevices];
-bool g_ready[kMaxDevices] = {};
+struct Cached {
+  unsigned long long ctx_id = 0;
+  bool ready = false;
+  Scratch s;
+};
+Cached g_cache[kMaxDevices];
 std::mutex g_lock;
+
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+// The current context's id through the driver's entry points (the runtime
+// has no call for it); 0 when the driver cannot say.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 int scratch_for_current_device(Scratch* out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PCG_ERR_CUDA;
   std::lock_guard<std::mutex> guard(g_lock);
-  if (!g_ready[dev]) {
+  Cached& c = g_cache[dev];
+  // once looked up, the context exists; a reset context reads as another id
+  // (or none), and a driver without context ids makes every call look up again
+  const unsigned long long ctx = c.ready ? current_context_id() : 0;
+  if (!c.ready || ctx == 0 || ctx != c.ctx_id) {
     Scratch s;
+    c.ready = false;
     if (cudaGetSymbolAddress((void**)&s.reset, g_reset) != cudaSuccess) return PCG_ERR_CUDA;
     if (cudaGetSymbolAddress((void**)&s.move_errors, g_move_errors) != cudaSuccess) return PCG_ERR_CUDA;
-    g_scratch[dev] = s;
-    g_ready[dev] = true;
+    c.s = s;
+    c.ctx_id = current_context_id();  // the lookup made the device's primary context current
+    c.ready = true;
   }
-  *out = g_scratch[dev];
+  *out = c.s;
   return PCG_OK;
 }
 
@@ -123,10 +161,15 @@ extern "C" int pcg_current_vb_f64_noalloc(int nr, int nz, double radius, double 
   if (!j_r || !j_phi || !j_z || (n && !(r && z && r_old && z_old && vphi && w))) return PCG_ERR_ARG;
   const long long nodes = (long long)(nr + 4) * (long long)(nz + 4);
   if (nodes > kNoallocMaxNodes) return PCG_ERR_CAPACITY;  // (nr+4)*(nz+4) above the fixed scratch
+  cudaStream_t s = (cudaStream_t)stream;
+  if (move_errors) {  // the count's read-back synchronises the stream, which a capture forbids
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return PCG_ERR_CUDA;
+    if (cs != cudaStreamCaptureStatusNone) return PCG_ERR_STATE;
+  }
   Scratch sc;
   int rc = scratch_for_current_device(&sc);
   if (rc != PCG_OK) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
   GridGeom g{};
   g.nr = nr; g.nz = nz; g.ld = nz + 4;
   g.R = radius; g.L = longitude;

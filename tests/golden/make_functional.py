@@ -20,7 +20,7 @@ COMPONENTS = [f"{f}/{a}" for f in ("E", "H", "J") for a in ("r", "phi", "z")]
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference checkout")
     args = ap.parse_args()
     src = os.path.join(args.ref, "test", "functional")
     out = os.path.join(HERE, "functional")

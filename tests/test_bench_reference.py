@@ -31,7 +31,8 @@ def test_reference_arm_line():
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
                 "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert key in line, key
-    assert line["value"] > 0 and line["higher_is_better"] is True and line["steps"] >= 1
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["steps"] == 25 and line["warmup"] == 5  # the K and W it was given
     assert line["unit"] == "particle-steps/s" and line["config"]["workload"]
     cb = line["cpu_baseline"]
     assert cb["value"] == line["value"] and cb["cores"] >= 1 and cb["kind"] == "reference" and cb["sample"]

@@ -6,7 +6,8 @@ oracle/ref_shim, so that the GpuDomain / GpuSpecieP bindings name members
 the reference's classes really have.  Fragments are wrapped in a function
 that has a handle `h` (and a `slot`); the GpuSpecieP method gets a class
 declaration around it.  Skipped where the reference's headers are absent
-(the REF variable of oracle/Makefile.ref) or no compiler is installed.
+($PICOPIC_REFERENCE, or the checkout the last
+oracle build compiled) or no compiler is installed.
 """
 import os
 import re
@@ -15,9 +16,11 @@ import subprocess
 
 import pytest
 
+from oracle.harness import reference_root
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF = os.environ.get("REF", "/root/reference")
+REF = reference_root()
 
 
 def blocks():
@@ -40,7 +43,7 @@ def wrap(lang: str, body: str) -> str:
 
 
 def test_integration_snippets_compile(tmp_path):
-    if not os.path.isdir(os.path.join(REF, "include")):
+    if not REF or not os.path.isdir(os.path.join(REF, "include")):
         pytest.skip("the reference's headers are not here")
     if not shutil.which("g++") or not shutil.which("gcc"):
         pytest.skip("no host compiler")
