@@ -244,6 +244,7 @@ int check_status(pcg_handle* h) {
   if (e & kErrOutOfGrid) return fail(h, PCG_ERR_STATE, "particle outside the grid");
   if (e & kErrCapacity) return fail(h, PCG_ERR_CAPACITY, "species capacity exceeded");
   if (e & kErrUnsupported) return fail(h, PCG_ERR_UNSUPPORTED, "switch combination not implemented");
+  if (e & kErrTimeout) return fail(h, PCG_ERR_TIMEOUT, "a bounded wait in a kernel ran out");
   return PCG_OK;
 }
 

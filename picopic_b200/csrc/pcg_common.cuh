@@ -28,6 +28,7 @@ enum ErrBits : unsigned {
   kErrCapacity = 1u << 4,      // species buffer full
   kErrOutOfGrid = 1u << 5,     // a particle outside the grid and its halo
   kErrUnsupported = 1u << 6,   // a switch combination this path does not implement
+  kErrTimeout = 1u << 7,       // a bounded wait in a kernel ran out (its results are invalid)
 };
 
 // Device-side counters and the error word, one block per handle.

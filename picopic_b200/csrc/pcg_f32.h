@@ -19,10 +19,13 @@ template <typename Real>
 struct YeeArgs;
 
 // Tiles of tr x tz cells; a block's shared window adds `halo` cells per side.
-constexpr int kTileR = 8, kTileZ = 64, kHalo = 3;  // every tile is kTileR x kTileZ cells
+// every tile is kTileR x kTileZ cells: 256 cells, one per thread of a step
+// block in a full layer, and 32 along z so that a warp's 32 cells share a row
+constexpr int kTileR = 8, kTileZ = 32, kHalo = 3;
 constexpr int kTileCells = kTileR * kTileZ;
 constexpr int kTileWords = kTileCells / 32;  // 32-cell words of a tile's layer mask
 constexpr int kLayerCap = 128;              // layers kept in order; deeper ranks go to an overflow run
+constexpr int kSlotPad = 4;                 // spare elements after each slot array (16 bytes)
 struct TileGrid {
   int tr, tz, ntr, ntz, ntiles, halo;
 };

@@ -50,6 +50,11 @@ struct StepArgs {
 // tile plus kHalo nodes per side.
 constexpr int kFWR = kTileR + 2 * kHalo + 2, kFWZ = kTileZ + 2 * kHalo + 2;
 constexpr int kJWR = kTileR + 2 * kHalo, kJWZ = kTileZ + 2 * kHalo;
+// Row stride of the field window in shared memory: a multiple of the 32
+// banks, so that lanes whose half-cell staggered reads land in adjacent rows
+// (rows ci-1 and ci) still hit distinct banks.
+constexpr int kFWS = 64;
+static_assert(kFWS >= kFWZ && kFWS % 32 == 0, "field window rows are whole multiples of the bank count");
 
 // Grids are far below 2^31 nodes, so node indices are 32-bit.
 __device__ __forceinline__ int node(const StepArgs& a, int i, int k) {
@@ -94,7 +99,7 @@ struct GlobalFields {
 };
 
 struct SharedFields {
-  static constexpr int kLd = kFWZ, kPlane = kFWR * kFWZ;
+  static constexpr int kLd = kFWS, kPlane = kFWR * kFWS;
   const float* base;
   int i0, k0;
   const float4* rt;  // the window's rows of the table, row i at rt[2 * (i - i0)]
@@ -779,8 +784,8 @@ __device__ __forceinline__ void tile_particle(const StepArgs& a, const SpeciesF3
 }
 
 // Shared memory of a tile block: the field window, then the current window.
-constexpr size_t kTileSmemBytes = sizeof(float) * (6 * kFWR * kFWZ + 3 * kJWR * kJWZ) + sizeof(float4) * 2 * kFWR;
-static_assert((6 * kFWR * kFWZ + 3 * kJWR * kJWZ) % 4 == 0, "the table rows need 16-byte alignment");
+constexpr size_t kTileSmemBytes = sizeof(float) * (6 * kFWR * kFWS + 3 * kJWR * kJWZ) + sizeof(float4) * 2 * kFWR;
+static_assert((6 * kFWR * kFWS + 3 * kJWR * kJWZ) % 4 == 0, "the table rows need 16-byte alignment");
 
 // One block per tile (or gridDim.y blocks sharing a crowded tile): the
 // tile's particles (grouped by the last sort) gather from a shared copy of
@@ -810,7 +815,7 @@ __global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
   const int fi0 = r0 - kHalo - 1, fk0 = z0 - kHalo - 1;  // field window origin (node)
   const int ji0 = r0 - kHalo, jk0 = z0 - kHalo;          // current window origin (node)
   float* sF = smem;
-  float* sJ = smem + 6 * kFWR * kFWZ;
+  float* sJ = smem + 6 * kFWR * kFWS;
   // load the field window, one row of one component per warp pass (nodes
   // outside the halo-padded grid read as 0)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -820,7 +825,7 @@ __global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
     const float* src = a.Er + c * a.plane + (i + 2) * a.ld + 2;
     for (int q = lane; q < kFWZ; q += 32) {
       const int k = fk0 + q;
-      sF[row * kFWZ + q] = (row_ok && k >= -2 && k < a.nz + 2) ? __ldg(src + k) : 0.f;
+      sF[row * kFWS + q] = (row_ok && k >= -2 && k < a.nz + 2) ? __ldg(src + k) : 0.f;
     }
   }
   for (int q = threadIdx.x; q < 3 * kJWR * kJWZ; q += kThreads) sJ[q] = 0.f;

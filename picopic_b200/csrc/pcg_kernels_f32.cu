@@ -11,6 +11,7 @@
 
 #include "pcg.h"
 #include "pcg_f32.h"
+#include "pcg_f32_pair.cuh"
 #include "pcg_f32_step.cuh"
 #include "pcg_philox.cuh"
 #include "pcg_yee.cuh"
@@ -394,13 +395,15 @@ TileGrid f32_tile_grid(const GridGeom& g) {
 int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg) {
   if (cap == 0) cap = 1;
   b.cap = cap;
+  // the slot arrays have kSlotPad spare elements: the step's bulk copies
+  // round the end of a range up to 16 bytes
   int** ints[] = {&b.cell, &b.cell2};
   for (int** a : ints)
-    if (cudaMalloc((void**)a, cap * sizeof(int)) != cudaSuccess) return -1;
+    if (cudaMalloc((void**)a, (cap + kSlotPad) * sizeof(int)) != cudaSuccess) return -1;
   float** arrs[] = {&b.off_r, &b.off_z, &b.vr, &b.vphi, &b.vz, &b.w,
                     &b.off_r2, &b.off_z2, &b.vr2, &b.vphi2, &b.vz2, &b.w2};
   for (float** a : arrs)
-    if (cudaMalloc((void**)a, cap * sizeof(float)) != cudaSuccess) return -1;
+    if (cudaMalloc((void**)a, (cap + kSlotPad) * sizeof(float)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.id, cap * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.id2, cap * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.tile_start, (tg.ntiles + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
@@ -482,10 +485,13 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
       f32::step_tiled_kernel<1, PCG_PUSHER_VAY, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.current == PCG_CURRENT_ZIGZAG)
       f32::step_tiled_kernel<1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
-    else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam && st.fixed)  // the plasma of the
-      f32::step_tiled_kernel<0, PCG_PUSHER_BORIS_RELATIVISTIC, 0, 1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
-    else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam)               // common runs
-      f32::step_tiled_kernel<0, PCG_PUSHER_BORIS_RELATIVISTIC, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam) {  // the plasma of the common runs
+      auto kern = st.fixed ? f32::step_pair_kernel<1> : f32::step_pair_kernel<0>;
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f32::kPairSmemBytes) !=
+          cudaSuccess)
+        return -1;
+      kern<<<grid, f32::kThreads, f32::kPairSmemBytes, s>>>(a, b, tg);
+    }
     else
       f32::step_tiled_kernel<0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
   }
