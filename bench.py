@@ -190,6 +190,8 @@ def run_gpu(args):
     w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
     w = scaled(w, nz=args.nz, ppc=args.ppc)
     d, slots, g, vb = make_domain(w, "f32", seed=rep.seed(1234), device=local)
+    if args.target_blocks:
+        d.set_tiling(target_blocks=args.target_blocks)
     d.step(args.warmup)
     d.synchronize()
     diag0 = d.diag()
@@ -742,6 +744,8 @@ def main():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-config0", action="store_true")
+    ap.add_argument("--target-blocks", type=int, default=0,
+                    help="float step: blocks the tile sort aims for (0 keeps the default)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
