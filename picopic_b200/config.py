@@ -59,6 +59,7 @@ class RunConfig:
     probes: list
     data_root: str
     external_fields: dict
+    raw: dict = dataclasses.field(default_factory=dict)  # the configuration as read, for the output metadata
 
     @property
     def steps(self) -> int:
@@ -159,7 +160,7 @@ def load(src) -> RunConfig:
     probes = [_probe(o, nr, nz) for o in data.get("probes", [])]
     ext = src.get("external_fields", {})
     return RunConfig(geom, float(t["end"]), macro, ratio, species, beams, probes,
-                     data.get("data_root", "./"), ext)
+                     data.get("data_root", "./"), ext, raw=src)
 
 
 class _Spec:
@@ -244,10 +245,13 @@ def _frame(d, slots, p: Probe):
     return g[r1, z1]
 
 
-def run(cfg: RunConfig, d, slots, steps=None, out_dir=None, log=print):
+def run(cfg: RunConfig, d, slots, steps=None, out_dir=None, log=print, attrs=None):
     """Step the domain `steps` times (default: to the configured end time),
     recording every probe on its schedule; writes <out_dir>/<probe path>.npy
-    (frames x probe shape) and returns {path: array}.
+    (frames x probe shape) with the layout of the reference's data.h5 in
+    <out_dir>/data.h5.json (h5layout: the root attributes `attrs`, by
+    default those of the relativistic Boris / VB float build) and returns
+    {path: array}.
 
     The schedule is the reference's: its main loop (PiCoPiC.cpp:326-347)
     runs a step and then the writers while the clock still reads the step's
@@ -268,10 +272,8 @@ def run(cfg: RunConfig, d, slots, steps=None, out_dir=None, log=print):
     d.synchronize()
     out = {path: np.stack(f) if f else np.zeros((0,)) for path, f in frames.items()}
     if out_dir:
-        for path, a in out.items():
-            dst = os.path.join(out_dir, path + ".npy")
-            os.makedirs(os.path.dirname(dst), exist_ok=True)
-            np.save(dst, a)
+        from . import h5layout
+        h5layout.write_tree(out_dir, out, attrs if attrs is not None else h5layout.root_attributes(cfg.raw))
         log(f"{n} steps, {len(out)} probes written under {out_dir}")
     return out
 
@@ -291,7 +293,9 @@ def main(argv=None):
     a = ap.parse_args(argv)
     cfg = load(a.config)
     d, slots = build_domain(cfg, a.pusher, a.current, a.precision, a.quirks, a.seed, plasma=a.plasma)
-    run(cfg, d, slots, a.steps, a.out or cfg.data_root)
+    from . import h5layout
+    attrs = h5layout.root_attributes(cfg.raw, a.pusher, a.current, a.precision, a.quirks, a.plasma)
+    run(cfg, d, slots, a.steps, a.out or cfg.data_root, attrs=attrs)
 
 
 if __name__ == "__main__":
