@@ -274,6 +274,14 @@ int pcg_collide(pcg_handle* h, unsigned long long* pair_calls);
 #define PCG_COLLIDE_SK98 2
 int pcg_set_collision_scheme(pcg_handle* h, int scheme);
 
+/* Work split of the binary pass (no counterpart in the reference, which
+ * runs every cell's pairing sequence in turn): cells holding more than
+ * `threshold` particles (256 by default) run their sequence on a warp, the
+ * collisions touching disjoint particles on different lanes in the
+ * reference's order and with the same draws; the others on one thread
+ * each.  The result does not depend on the threshold. */
+int pcg_set_collision_crowding(pcg_handle* h, unsigned threshold);
+
 /* The per-cell collision MLP of the learned collision step (no counterpart
  * in the reference): 13 inputs -> 128 -> 128 -> 6 outputs, ReLU, BF16
  * operands on the tensor cores with FP32 accumulation.  Parameters are FP32,
@@ -399,11 +407,12 @@ int pcg_ensemble_destroy(pcg_ensemble* e);
 #define PCG_MAP_MOMENTUM 3
 int pcg_species_map(pcg_handle* h, int slot, int which, double* out);
 
-/* Collisions inside pcg_step: every step then opens with one pass of the
- * chosen operator on the velocities the previous step left.  The reference
- * collides between the push and the move (SMB.cpp:1289-1293); a caller
- * that needs exactly that order drives the step with pcg_stage and calls
- * pcg_collide or pcg_collide_learned after PCG_STAGE_PUSH. */
+/* Collisions inside pcg_step: every step then runs one pass of the chosen
+ * operator between the push and the move, as SMB::advance_particles does
+ * (SMB.cpp:1289-1293, Domain::collide): the step pushes every species,
+ * collides, then moves, reflects, binds and deposits.  The same order by
+ * stages: PCG_STAGE_PUSH, pcg_collide (or pcg_collide_learned), then
+ * PCG_STAGE_DUMP_OLD onwards. */
 #define PCG_COLLISIONS_NONE 0
 #define PCG_COLLISIONS_BINARY 1
 #define PCG_COLLISIONS_LEARNED 2

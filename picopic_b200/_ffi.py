@@ -88,6 +88,7 @@ SIGNATURES = {
     "pcg_cell_moments": (ctypes.c_int, [_H, _PD]),
     "pcg_set_collisions": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_scheme": (ctypes.c_int, [_H, ctypes.c_int]),
+    "pcg_set_collision_crowding": (ctypes.c_int, [_H, ctypes.c_uint]),
     "pcg_species_map": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _PD]),
     "pcg_set_tiling": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "pcg_tile_sort": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(ctypes.c_uint),

@@ -35,6 +35,7 @@ UNITS = {
     "pcg_noalloc.cu": ["--fmad=false"],
     "pcg_diag.cu": ["--fmad=false"],
     "pcg_collide.cu": ["--fmad=false"],
+    "pcg_collide_crowded.cu": ["--fmad=false"],
     "pcg_mlp.cu": [],
     "pcg_learned.cu": ["--fmad=false"],
     "pcg_maps.cu": ["--fmad=false"],

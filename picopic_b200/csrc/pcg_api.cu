@@ -78,6 +78,7 @@ struct pcg_handle {
   uint32_t coll_pass = 0;         // collision passes so far (their Philox counter)
   int collisions = PCG_COLLISIONS_NONE;  // collision operator of every pcg_step
   int coll_scheme = PCG_COLLIDE_P12;     // binary operator of pcg_collide and binary steps
+  unsigned coll_crowded = 256;           // particles above which a cell's pairs take a warp
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -499,6 +500,7 @@ int run_collide(pcg_handle* h, unsigned long long* pair_calls) {
     return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
   p.pass = h->coll_pass++;
   p.scheme = h->coll_scheme;
+  p.crowded = h->coll_crowded;
   unsigned long long calls = 0;
   if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
     return fail(h, PCG_ERR_CUDA, "collision pass");
@@ -537,13 +539,23 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   return PCG_OK;
 }
 
+// The collision operator of pcg_step, between the push and the move.
+int step_collide(pcg_handle* h) {
+  if (h->collisions == PCG_COLLISIONS_BINARY) return run_collide(h, nullptr);
+  if (h->collisions == PCG_COLLISIONS_LEARNED) return run_collide_learned(h, nullptr, nullptr);
+  return PCG_OK;
+}
+
+// One step in the order of PiCoPiC's main loop (PiCoPiC.cpp:326-347 over
+// SMB.cpp:1231-1322): beam injection, E, H, then per species the push, the
+// collisions (SMB::advance_particles collides after the push and before the
+// move), the move with reflection and binding, and the current.  Without
+// collisions the push and the move are one kernel; with them the push runs
+// first for every species, then the collision operator, then the move.
 int fused_step(pcg_handle* h) {
   int rc;
   const int fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
-  // collisions open the step (on the velocities the last step left)
-  if (h->collisions == PCG_COLLISIONS_BINARY && (rc = run_collide(h, nullptr)) != PCG_OK) return rc;
-  if (h->collisions == PCG_COLLISIONS_LEARNED && (rc = run_collide_learned(h, nullptr, nullptr)) != PCG_OK)
-    return rc;
+  const bool collide = h->collisions != PCG_COLLISIONS_NONE;
   if ((rc = stage_inject(h)) != PCG_OK) return rc;
   uint64_t live = 0;
   for (Species& s : h->sp) live += s.n;
@@ -553,13 +565,24 @@ int fused_step(pcg_handle* h) {
     { TimerScope ts(h, PCG_TIMER_FIELD_H); launch_yee_h_f64(yee_args<double>(h, h->f64, h->sig64, 0), fixed, h->stream); }
     h->launches += 2;
     FieldsF64 f = fields64(h);
+    if (collide) {
+      {
+        TimerScope ts(h, PCG_TIMER_PARTICLES);
+        for (size_t t = 0; t < h->sp.size(); ++t) {
+          launch_stage_f64(PCG_STAGE_PUSH, h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
+                           h->d_status, h->stream);
+          h->launches += h->sp[t].n ? 1 : 0;
+        }
+      }
+      if ((rc = step_collide(h)) != PCG_OK) return rc;
+    }
     {
       TimerScope ts(h, PCG_TIMER_PARTICLES);
       if (h->cfg.current == PCG_CURRENT_VB)
         CUDA_TRY(h, cudaMemsetAsync(h->reset, 0, sizeof(unsigned long long) * h->nodes, h->stream));
       for (size_t t = 0; t < h->sp.size(); ++t) {
         launch_advance_f64(h->g, f, view64(h, h->sp[t]), (int)t, h->cfg.pusher, fixed,
-                           h->cfg.current, h->reset, h->d_status, h->stream);
+                           h->cfg.current, h->reset, h->d_status, h->stream, collide ? 0 : 1);
         h->launches += h->sp[t].n ? 1 : 0;
       }
     }
@@ -575,7 +598,6 @@ int fused_step(pcg_handle* h) {
     { TimerScope ts(h, PCG_TIMER_FIELD_E); f32_launch_yee_e(yee_args<float>(h, h->f32, h->sig32, 1), h->stream); }
     { TimerScope ts(h, PCG_TIMER_FIELD_H); f32_launch_yee_h(yee_args<float>(h, h->f32, h->sig32, 0), fixed, h->stream); }
     h->launches += 2;
-    TimerScope ts(h, PCG_TIMER_PARTICLES);
     F32Step st;
     st.g = h->g;
     for (int c = 0; c < 12; ++c) st.fld[c] = h->f32[c];
@@ -589,6 +611,20 @@ int fused_step(pcg_handle* h) {
     st.sort_interval = h->sort_interval;
     st.target_blocks = h->target_blocks;
     st.min_split = h->min_split;
+    if (collide) {
+      {
+        TimerScope ts(h, PCG_TIMER_PARTICLES);
+        for (size_t t = 0; t < h->sp.size(); ++t) {
+          Species& s = h->sp[t];
+          const uint64_t k0 = s.f32.launches;
+          f32_push_species(st, s.f32, s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream);
+          h->launches += s.f32.launches - k0;
+        }
+      }
+      if ((rc = step_collide(h)) != PCG_OK) return rc;
+      st.pushed = 1;
+    }
+    TimerScope ts(h, PCG_TIMER_PARTICLES);
     for (size_t t = 0; t < h->sp.size(); ++t) {
       Species& s = h->sp[t];
       const size_t n0 = s.n;
@@ -976,6 +1012,12 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (rc != PCG_OK) return rc;
   if ((rc = run_collide_learned(h, learned_cells, fallback_cells)) != PCG_OK) return rc;
   return check_status(h);
+}
+
+int pcg_set_collision_crowding(pcg_handle* h, unsigned threshold) {
+  if (!h) return PCG_ERR_ARG;
+  h->coll_crowded = threshold;
+  return PCG_OK;
 }
 
 int pcg_set_collision_scheme(pcg_handle* h, int scheme) {

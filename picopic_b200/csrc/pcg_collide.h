@@ -47,6 +47,9 @@ struct CollParams {
   // (non-relativistic kinematics of the mean)
   double* expect = nullptr;
   int scheme = 0;  // 0: Perez 2012 (CollisionsP12), 1: Takizuka-Abe with correction (CollisionsTA77S)
+  // cells of more than `crowded` particles take the warp-per-cell pair
+  // kernel (pcg_collide_crowded.cu), the others a thread each
+  unsigned crowded = 256;
 };
 
 // Scratch of a collision pass, grown on demand and kept by the handle.
@@ -72,5 +75,11 @@ struct CollWork {
 int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollParams& p,
                 CollWork& w, unsigned long long* pair_calls, cudaStream_t s);
 void collide_free(CollWork& w);
+// The pairs of the cells holding more than p.crowded particles, one warp per
+// cell (pcg_collide_crowded.cu); the per-cell kernel of collide_p12 skips them.
+void collide_crowded(const GridGeom& g, double4* const stage[2], const CollParams& p, const unsigned* st_e,
+                     const unsigned* n_e, const unsigned long long* le, const unsigned* st_i, const unsigned* n_i,
+                     const unsigned long long* li, const double* mom, const int* row_stop, unsigned long long* calls,
+                     cudaStream_t s);
 
 }  // namespace pcg

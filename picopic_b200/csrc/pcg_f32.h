@@ -81,6 +81,9 @@ struct F32Step {
   // a sort splits each occupied tile over enough blocks that about
   // target_blocks run, each with at least min_split particles
   unsigned target_blocks = 148 * 16, min_split = 1024;
+  // the velocities were pushed by f32_push_species already (collisions act
+  // between the push and the move): the step moves and deposits only
+  int pushed = 0;
 };
 
 __host__ __device__ __forceinline__ int pack_cell(int ci, int ck) {
@@ -111,6 +114,10 @@ void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_
 // left their tile's windows in a recent step, or after `sort_interval` steps.
 int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
                      double mass, int is_beam, cudaStream_t s);
+// The push alone of a species' particles (fields from the global grid),
+// for a step with collisions between the push and the move.
+void f32_push_species(const F32Step& st, SpeciesF32Buffers& b, size_t n, double charge, double mass,
+                      int is_beam, cudaStream_t s);
 void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s);
 int f32_compact(SpeciesF32Buffers& b, const unsigned* idx, size_t kept, cudaStream_t s);
 int f32_export(const GridGeom& g, SpeciesF32Buffers& b, size_t n, double* r, double* z,

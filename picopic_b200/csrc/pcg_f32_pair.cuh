@@ -220,7 +220,7 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   v0 = mul(v0, gm); v1 = mul(v1, gm); v2 = mul(v2, gm);
 
   // ---- move in the local Cartesian frame and back to r-z (specieP.cpp:482-491, 609-640) ----
-  const float2 dx = mul(v0, bc(a.dt_dr)), dyp = mul(v1, bc(a.dt_dr)), dY = mul(v2, bc(a.dt_dz));
+  const float2 dx = mul(v0, bc(a.dt_dr)), dyp = mul(v1, bc(a.dt_dr)), dYv = mul(v2, bc(a.dt_dz));
   const float2 x0 = add(fi, fr);
   const float2 X = add(x0, dx);
   const float2 dy2 = mul(dyp, dyp);
@@ -228,8 +228,12 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   const float2 rxn = rsq(xn2);                          // 1/x'
   const float2 xn = mul(xn2, rxn);                      // x' = sqrt(X^2 + dy^2)
   const float2 sn = mul(dyp, rxn);
-  const float2 dX = fma(dy2, rcp(add(X, xn)), dx);       // x' - x = dx + dy^2/(X + x')
-  const float2 frn = add(fr, dX), fzn = add(fz, dY);
+  const float2 dXv = fma(dy2, rcp(add(X, xn)), dx);      // x' - x = dx + dy^2/(X + x')
+  const float2 frn = add(fr, dXv), fzn = add(fz, dYv);
+  // the deposit's displacement: the move itself, or in the fixed mode the
+  // difference of the stored offsets (exact for close offsets), so that the
+  // current carries the charge the rounded new position holds
+  const float2 dX = FIX ? sub(frn, fr) : dXv, dY = FIX ? sub(fzn, fz) : dYv;
   const float2 ixo = rcp(x0);
   const float2 t = mul(dX, ixo);
   // the in-cell case with the logarithm's series valid (|t| < 0.02); motion

@@ -38,6 +38,7 @@ struct StepArgs {
   float dr_m, dz_m, dt_s;      // dr, dz, dt in SI (ZigZag keeps metre-valued weights)
   float zz_vol;                // 1/(PI dz dr^2)
   int pusher, current, fixed, is_beam;
+  int pushed;  // the velocities were pushed by push_flat_kernel (a step with collisions)
   // per radial node i (row i + 2): {1/(2i+1), 1/(2i+2), 1/(2i+3), 1/(2i+4)},
   // {1/i, 1/(i+1), 1/(i+1/2), 0}; a zero where the denominator is zero
   const float4* rt;
@@ -609,7 +610,7 @@ __device__ __forceinline__ bool advance_one(const StepArgs& a, const SpeciesF32B
   const int ci0 = cell_r_of(p.cell), ck0 = cell_z_of(p.cell);
   const float fr0 = p.fr, fz0 = p.fz;
   float v[3] = {p.vr, p.vphi, p.vz};
-  if (!push(a, e, bb, v)) return false;
+  if (!a.pushed && !push(a, e, bb, v)) return false;
   // mover_cylindrical + back_position_to_rz: x' = sqrt((x+dx)^2 + dy^2),
   // taken as dx + dy^2/(X + x') to keep the displacement's precision.
   const float dx = v[0] * a.dt_dr, dyp = v[1] * a.dt_dr, dzz = v[2] * a.dt_dz;
@@ -635,7 +636,12 @@ __device__ __forceinline__ bool advance_one(const StepArgs& a, const SpeciesF32B
     if (!reflect(a, &ci, &fr, &ck, &fz, &v[0], &v[2])) raise_error(a.st, kErrReflectLoop);
     reflected = ci != c0 || ck != k0 || fr != f0 || fz != g0;
   }
-  if (reflected) {  // the deposit follows the straight line to the mirrored point
+  // After a reflection the deposit follows the straight line to the mirrored
+  // point.  In the fixed mode every deposit takes its displacement from the
+  // stored (rounded) offsets, so that the charge its current moves is the
+  // charge the new position holds (the difference of two close offsets is
+  // exact), not the unrounded move.
+  if (reflected || a.fixed) {
     dX = (float)(ci - ci0) + (fr - fr0);
     dY = (float)(ck - ck0) + (fz - fz0);
   }
@@ -740,10 +746,28 @@ __global__ void __launch_bounds__(kThreads) step_flat_kernel(StepArgs a, Species
   if (j >= j1) return;
   const Slot p = load_slot(b, j);
   if (p.cell < 0 || !cell_in_halo(a, p.cell)) return;
-  float e[3], bb[3];
-  gather(a, global_fields(a), cell_r_of(p.cell), p.fr, cell_z_of(p.cell), p.fz, e, bb);
+  float e[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};
+  if (!a.pushed) gather(a, global_fields(a), cell_r_of(p.cell), p.fr, cell_z_of(p.cell), p.fz, e, bb);
   Moved m;
   if (advance_one(a, b, j, p, e, bb, &m)) deposit<CUR>(a, global_dep(a), m);
+}
+
+// The push alone, one thread per slot of [0, n), fields from the global
+// grid: the first half of a step whose collisions act between the push and
+// the move (SMB::advance_particles, SMB.cpp:1289-1293); the step kernels
+// then run with StepArgs::pushed set.
+__global__ void __launch_bounds__(kThreads) push_flat_kernel(StepArgs a, SpeciesF32Buffers b, size_t n) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const Slot p = load_slot(b, j);
+  if (p.cell < 0 || !cell_in_halo(a, p.cell)) return;
+  float e[3], bb[3];
+  gather(a, global_fields(a), cell_r_of(p.cell), p.fr, cell_z_of(p.cell), p.fz, e, bb);
+  float v[3] = {p.vr, p.vphi, p.vz};
+  if (!push(a, e, bb, v)) return;
+  b.vr[j] = v[0];
+  b.vphi[j] = v[1];
+  b.vz[j] = v[2];
 }
 
 // One particle of a tile block: gather from the shared window (or the grid
@@ -760,9 +784,13 @@ __device__ __forceinline__ void tile_particle(const StepArgs& a, const SpeciesF3
                       ck0 + 2 < sv.k0 + kFWZ;
   if (!inside && !cell_in_halo(a, p.cell)) return;
   bool slow = !inside;
-  float ef[3], bf[3];
-  if (inside) gather(a, sv, ci0, p.fr, ck0, p.fz, ef, bf);
-  else gather(a, global_fields(a), ci0, p.fr, ck0, p.fz, ef, bf);
+  float ef[3] = {0.f, 0.f, 0.f}, bf[3] = {0.f, 0.f, 0.f};
+  if (a.pushed) {
+  } else if (inside) {
+    gather(a, sv, ci0, p.fr, ck0, p.fz, ef, bf);
+  } else {
+    gather(a, global_fields(a), ci0, p.fr, ck0, p.fz, ef, bf);
+  }
   Moved m;
   if (!advance_one(a, b, j, p, ef, bf, &m)) {
     if (slow) atomicAdd(b.drift, 1u);
@@ -890,6 +918,7 @@ inline f32::StepArgs f32_step_args(const F32Step& st, double charge, double mass
   // ZigZag: 1/(PI dz dr^2) with the species charge folded in
   a.zz_vol = (float)(charge / (kPi * g.dz * g.dr * g.dr));
   a.pusher = st.pusher; a.current = st.current; a.fixed = st.fixed; a.is_beam = is_beam;
+  a.pushed = st.pushed;
   a.rt = st.recip;
   a.st = st.status;
   return a;

@@ -80,7 +80,7 @@ void launch_current_stage_f64(const GridGeom& g, const FieldsF64& f, const Speci
                               DevStatus* st, cudaStream_t s);
 void launch_advance_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp, int slot,
                         int pusher, int fixed, int current, unsigned long long* reset,
-                        DevStatus* st, cudaStream_t s);
+                        DevStatus* st, cudaStream_t s, int do_push = 1);
 void launch_deposit_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp, int slot,
                         int fixed, int current, const unsigned long long* reset, DevStatus* st,
                         cudaStream_t s);

@@ -481,10 +481,12 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   if (b.sorted_n) {
     const size_t smem = f32::kTileSmemBytes;
     const dim3 grid(tg.ntiles, b.splits);
-    if (st.current == PCG_CURRENT_ZIGZAG && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed)
+    if (st.current == PCG_CURRENT_ZIGZAG && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed && !st.pushed)
       f32::step_tiled_kernel<1, PCG_PUSHER_VAY, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.current == PCG_CURRENT_ZIGZAG)
       f32::step_tiled_kernel<1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.pushed)
+      f32::step_tiled_kernel<0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.pusher == PCG_PUSHER_BORIS_RELATIVISTIC && !is_beam) {  // the plasma of the common runs
       auto kern = st.fixed ? f32::step_pair_kernel<1> : f32::step_pair_kernel<0>;
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f32::kPairSmemBytes) !=
@@ -506,6 +508,15 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   cudaMemcpyAsync(b.drift_host, b.drift, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   b.steps_since_sort += 1;
   return 0;
+}
+
+void f32_push_species(const F32Step& st, SpeciesF32Buffers& b, size_t n, double charge, double mass,
+                      int is_beam, cudaStream_t s) {
+  if (n == 0) return;
+  f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
+  a.pushed = 0;
+  f32::push_flat_kernel<<<blocks_for(n), f32::kThreads, 0, s>>>(a, b, n);
+  b.launches += 1;
 }
 
 void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s) {

@@ -169,11 +169,13 @@ __global__ void zigzag_kernel(GridGeom g, FieldsF64 fd, SpeciesF64 sp) {
 // ---------------------------------------------------------------------------
 // Fused step, kernel 1: push, move, rotate, reflect, rotate back, bind and
 // the runaway test in registers; stores new and old positions and marks the
-// strict-axial J_r overwrites.
+// strict-axial J_r overwrites.  Without do_push the velocities are taken as
+// pushed already (the step of a run with collisions, which act between the
+// push and the move).
 __global__ void __launch_bounds__(kThreads) advance_kernel(GridGeom g, FieldsF64 fd, SpeciesF64 sp,
                                                            int slot, int pusher, int fixed,
                                                            int current, unsigned long long* reset,
-                                                           DevStatus* st) {
+                                                           DevStatus* st, int do_push) {
   const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (j >= sp.n) return;
   double r = sp.r[j];
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) advance_kernel(GridGeom g, FieldsF64
   double z = sp.z[j];
   Fields f = make_fields(fd);
   double v[3] = {sp.vr[j], sp.vphi[j], sp.vz[j]};
-  if (!gather_push(g, f, pusher, fixed, sp.c2m, r, z, v, st)) return;
+  if (do_push && !gather_push(g, f, pusher, fixed, sp.c2m, r, z, v, st)) return;
   const double r_old = r, z_old = z;                 // dump_position_to_old (phi = 0)
   const double X = r + v[0] * g.dt;                  // mover_cylindrical
   const double Y = 0 + v[1] * g.dt;
@@ -338,9 +340,10 @@ void launch_current_stage_f64(const GridGeom& g, const FieldsF64& f, const Speci
 
 void launch_advance_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp, int slot,
                         int pusher, int fixed, int current, unsigned long long* reset,
-                        DevStatus* st, cudaStream_t s) {
+                        DevStatus* st, cudaStream_t s, int do_push) {
   if (sp.n == 0) return;
-  advance_kernel<<<blocks_for(sp.n), kThreads, 0, s>>>(g, f, sp, slot, pusher, fixed, current, reset, st);
+  advance_kernel<<<blocks_for(sp.n), kThreads, 0, s>>>(g, f, sp, slot, pusher, fixed, current, reset, st,
+                                                       do_push);
 }
 
 void launch_deposit_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64& sp, int slot,

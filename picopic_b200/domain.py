@@ -243,6 +243,11 @@ class Domain:
         code = {"p12": 0, "ta77s": 1, "sk98": 2}[scheme]
         self._check(self.lib.pcg_set_collision_scheme(self.h, code), "pcg_set_collision_scheme")
 
+    def set_collision_crowding(self, threshold):
+        """Cells of more than `threshold` particles run their collisions on a
+        warp each (pcg_set_collision_crowding; the result does not change)."""
+        self._check(self.lib.pcg_set_collision_crowding(self.h, int(threshold)), "pcg_set_collision_crowding")
+
     def set_collisions(self, mode):
         """Collisions inside step(): "none", "binary" or "learned" (one pass opens every step)."""
         code = {"none": 0, "binary": 1, "learned": 2}[mode]

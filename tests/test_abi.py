@@ -53,6 +53,7 @@ def test_null_handles_are_rejected_without_a_device():
         ("pcg_step", (null, 1)), ("pcg_collide", (null, null)), ("pcg_diag", (null, null)),
         ("pcg_set_tiling", (null, 0, 0, 0)), ("pcg_tile_sort", (null, 0, null, null)),
         ("pcg_species_map", (null, 0, 0, null)), ("pcg_set_collision_scheme", (null, 0)),
+        ("pcg_set_collision_crowding", (null, 0)),
         ("pcg_set_collisions", (null, 0)), ("pcg_collide_learned", (null, null, null)),
         ("pcg_count", (null, 0, null)), ("pcg_node_charge", (null, null)), ("pcg_stage", (null, 0)),
         ("pcg_synchronize", (null,)), ("pcg_get_stream", (null, null)), ("pcg_set_field", (null, 0, null)),
