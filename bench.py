@@ -678,8 +678,9 @@ def run_reference(args):
         return
     w = WORKLOAD if not args.small else scaled(WORKLOAD, nz=512, ppc=10)
     # the same K and W as the GPU arm (a slab step takes ~0.2 s on 16 threads),
-    # bounded so that the arm ends within a few minutes on small hosts
-    steps, warmup = min(args.steps, 60), min(args.warmup, 10)
+    # at least 8 steps after 1, at most 60 after 10 so that the arm ends
+    # within a few minutes on small hosts
+    steps, warmup = max(8, min(args.steps, 60)), max(1, min(args.warmup, 10))
     from oracle.harness import smb_available
     if smb_available():
         n, el, threads, sample = _smb_reference(w, steps, warmup)
