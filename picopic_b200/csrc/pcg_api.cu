@@ -474,6 +474,12 @@ bool collision_species(pcg_handle* h, std::vector<CollSpecies>& v, CollParams& p
     } else {
       c.cell = s.f32.cell; c.id = s.f32.id;
       c.vr32 = s.f32.vr; c.vphi32 = s.f32.vphi; c.vz32 = s.f32.vz; c.w32 = s.f32.w;
+      c.tile_start = s.f32.tile_start;
+      c.cell_count = s.f32.cell_count;
+      c.layer_mask = s.f32.layer_mask;
+      c.layer_prefix = s.f32.layer_prefix;
+      c.layer_start = s.f32.layer_start;
+      c.sorted = std::min(s.f32.sorted_n, s.n);
     }
   }
   if (el < 0 || ion < 0) return false;
@@ -524,7 +530,7 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
     return fail(h, PCG_ERR_TIMEOUT, "learned collision step: a tensor-core wait timed out; the handle is halted");
   }
   if (lr != 0) return fail(h, PCG_ERR_CUDA, "learned collision step");
-  h->launches += 1 + 2 * v.size();
+  h->launches += h->learned.launches;
   if (counts[1]) {  // the binary operator on the cells outside the training box
     p.pass = h->coll_pass++;
     p.only = h->learned.flag;

@@ -158,9 +158,13 @@ __global__ void unstage_kernel(SpeciesTable tab, const unsigned long long* refs,
 __global__ void moments_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
                                const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                const unsigned* n_i, const unsigned long long* li, double* mom,
-                               int* row_stop, double* totals) {
+                               int* row_stop, double* totals, unsigned* crowded, unsigned* active) {
   const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (c >= (size_t)g.nr * g.nz) return;
+  // a pass over chosen cells: the others are neither collided nor stop a row
+  if (p.only && p.only[c] != p.only_value) return;
+  if (n_e[c] + n_i[c] > p.crowded) crowded[1 + atomicAdd(crowded, 1u)] = (unsigned)c;
+  else if (p.only) active[1 + atomicAdd(active, 1u)] = (unsigned)c;
   const int i = (int)(c / g.nz), k = (int)(c - (size_t)i * g.nz);
   double e_tot_e = 0, amount_e = 0, e_tot_i = 0, amount_i = 0, v[3], w;
   double pm_e[3] = {0, 0, 0}, pm_i[3] = {0, 0, 0};  // sum w m v (TA77S)
@@ -266,13 +270,107 @@ __global__ void ta77s_correct_kernel(GridGeom g, Staged tab, CollParams p, const
 // sequence no longer sets the pass's duration.  Both give the same result.
 // (The threshold is a CollParams field, 256 by default.)
 
+// The pairing sequence of a cell (collisionsP12.cpp:359-529; TA77S and SK98
+// repeat it), as the collision numbers m = 0, 1, ... of the reference's
+// order: like pairs of an even list of ions, of an even list of electrons,
+// then of an odd ion list (the triangle (0,1), (1,2), (2,0), then (3,4),
+// (5,6), ...) and of an odd electron list, then electron-ion pairs, where
+// with unequal counts one particle of the less numerous list meets several
+// of the other in turn, in two groups (the split the reference computes in
+// float).
+struct PairPlan {
+  unsigned seg[3];  // collisions of the first like list, the second, then electron-ion
+  int first_ion;    // the first like list is the ions'
+  unsigned total;
+  // electron-ion groups (unequal counts)
+  unsigned g1, g2, off_few, off_many;  // group sizes; index offsets of the second group
+  float d1, d2;                        // partners per particle of each group, as floats
+};
+
+__device__ __forceinline__ unsigned like_count(unsigned n) { return n % 2 == 0 ? n / 2 : (n >= 3 ? 3 + (n - 3) / 2 : 0); }
+
+__device__ __forceinline__ PairPlan pair_plan(unsigned ne, unsigned ni) {
+  PairPlan q{};
+  // even lists first, ions before electrons in each parity
+  q.first_ion = (ni % 2 == 0) || (ne % 2 != 0);
+  q.seg[0] = like_count(q.first_ion ? ni : ne);
+  q.seg[1] = like_count(q.first_ion ? ne : ni);
+  if (ni == ne) {
+    q.seg[2] = ne;
+  } else if (ne > 0 && ni > 0 && ni > ne) {
+    const unsigned c_i = (unsigned)floorf((float)ni / (float)ne);
+    const double c_r = (double)((float)ni / (float)ne - (float)c_i);
+    q.g1 = (unsigned)((double)(c_i + 1) * c_r * ne);  // ions of the first group
+    q.off_few = (unsigned)(c_r * ne);                  // electrons of the first group
+    q.g2 = (unsigned)((double)c_i * (1 - c_r) * ne);
+    q.off_many = q.g1;
+    q.d1 = (float)(c_i + 1);
+    q.d2 = (float)c_i;
+    q.seg[2] = q.g1 + q.g2;
+  } else if (ne > 0 && ni > 0 && ni < ne) {
+    const double c_i = (double)floorf((float)ne / (float)ni);
+    const double c_r = (double)((float)ne / (float)ni) - c_i;
+    q.g1 = (unsigned)((c_i + 1) * c_r * ni);  // electrons of the first group
+    q.off_few = (unsigned)(c_r * ni);         // ions of the first group
+    q.g2 = (unsigned)(c_i * (1 - c_r) * ni);
+    q.off_many = q.g1;
+    q.d1 = (float)(c_i + 1);
+    q.d2 = (float)c_i;
+    q.seg[2] = q.g1 + q.g2;
+  }
+  q.total = q.seg[0] + q.seg[1] + q.seg[2];
+  return q;
+}
+
+struct PairRef {
+  int kind;  // 0: ion-ion, 1: electron-electron, 2: electron (a) - ion (b)
+  unsigned a, b;
+};
+
+__device__ __forceinline__ void like_pair(unsigned n, unsigned k, unsigned* a, unsigned* b) {
+  if (n % 2 == 0) { *a = 2 * k; *b = 2 * k + 1; return; }
+  if (k < 3) { *a = k; *b = k == 2 ? 0 : k + 1; return; }
+  *a = 3 + 2 * (k - 3);
+  *b = *a + 1;
+}
+
+__device__ __forceinline__ PairRef pair_of(const PairPlan& q, unsigned m, unsigned ne, unsigned ni) {
+  PairRef r;
+  if (m < q.seg[0] + q.seg[1]) {
+    const bool first = m < q.seg[0];
+    const bool ion = first ? q.first_ion : !q.first_ion;
+    r.kind = ion ? 0 : 1;
+    like_pair(ion ? ni : ne, first ? m : m - q.seg[0], &r.a, &r.b);
+    return r;
+  }
+  const unsigned k = m - q.seg[0] - q.seg[1];
+  r.kind = 2;
+  if (ni == ne) { r.a = k; r.b = k; return r; }
+  // the many-list index s, the few-list owner floor(s / d) (float, as in the reference)
+  unsigned few, many;
+  if (k < q.g1) {
+    many = k;
+    few = (unsigned)(int)floorf((float)k / q.d1);
+  } else {
+    const unsigned s2 = k - q.g1;
+    many = s2 + q.off_many;
+    few = (unsigned)(int)floorf((float)s2 / q.d2) + q.off_few;
+  }
+  if (ni > ne) { r.a = few; r.b = many; } else { r.a = many; r.b = few; }
+  return r;
+}
+
 // One cell's pairing sequence (collisionsP12.cpp:359-529) on one thread.
 template <int SCHEME>
-__global__ void collide_cells_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
+__global__ void __launch_bounds__(kThreads, 2) collide_cells_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
                                const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
                                const unsigned* n_i, const unsigned long long* li, const double* mom,
-                               const int* row_stop, unsigned long long* calls) {
-  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+                               const int* row_stop, unsigned long long* calls, const unsigned* list) {
+  // a pass over chosen cells takes them from the list the moments pass
+  // made (the chosen cells packed into whole warps), else thread c, cell c
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (list && tid >= list[0]) return;
+  const size_t c = list ? list[1 + tid] : tid;
   if (c >= (size_t)g.nr * g.nz) return;
   if (p.only && p.only[c] != p.only_value) return;
   if (n_e[c] + n_i[c] > p.crowded) return;  // collide_kernel takes the crowded cells
@@ -290,68 +388,23 @@ __global__ void collide_cells_kernel(GridGeom g, Staged tab, CollParams p, const
   const double me = p.m_el, mi = p.m_ion, qe = p.q_el, qi = p.q_ion;
   double expect[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   PairCtx x{&tab, &p, (uint32_t)c, 0u, p.expect ? expect : nullptr};
-#define COLL(MA, MB, QA, QB, A, B, NA, NB)                                       \
-  do {                                                                           \
-    if (SCHEME == 1) ta77s_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);        \
-    else if (SCHEME == 2) sk98_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);    \
-    else p12_single(x, MA, MB, QA, QB, A, B, NA, NB, debye);                     \
-    ++x.m;                                                                       \
-  } while (0)
-  if (ni % 2 == 0)
-    for (unsigned q = 0; q < ni; q += 2) COLL(mi, mi, qi, qi, I[q], I[q + 1], n_ion, n_ion);
-  if (ne % 2 == 0)
-    for (unsigned q = 0; q < ne; q += 2) COLL(me, me, qe, qe, E[q], E[q + 1], n_el, n_el);
-  if (ni % 2 != 0) {
-    if (ni >= 3) {
-      COLL(mi, mi, qi, qi, I[0], I[1], n_ion, n_ion);
-      COLL(mi, mi, qi, qi, I[1], I[2], n_ion, n_ion);
-      COLL(mi, mi, qi, qi, I[2], I[0], n_ion, n_ion);
-    }
-    if (ni >= 5)
-      for (unsigned q = 3; q < ni; q += 2) COLL(mi, mi, qi, qi, I[q], I[q + 1], n_ion, n_ion);
+  // The sequence as one loop over the collision number m with a single
+  // call of the pair function: cells of different counts in a warp then
+  // run the same code and diverge only in their trip counts.
+  const PairPlan plan = pair_plan(ne, ni);
+  for (unsigned m = 0; m < plan.total; ++m) {
+    const PairRef r = pair_of(plan, m, ne, ni);
+    const bool ion_a = r.kind == 0, el_b = r.kind == 1;
+    const unsigned long long A = ion_a ? I[r.a] : E[r.a];
+    const unsigned long long B = el_b ? E[r.b] : I[r.b];
+    const double ma = ion_a ? mi : me, qa = ion_a ? qi : qe, na = ion_a ? n_ion : n_el;
+    const double mb = el_b ? me : mi, qb = el_b ? qe : qi, nb = el_b ? n_el : n_ion;
+    x.m = m;
+    if (SCHEME == 1) ta77s_single(x, ma, mb, qa, qb, A, B, na, nb, debye);
+    else if (SCHEME == 2) sk98_single(x, ma, mb, qa, qb, A, B, na, nb, debye);
+    else p12_single(x, ma, mb, qa, qb, A, B, na, nb, debye);
   }
-  if (ne % 2 != 0) {
-    if (ne >= 3) {
-      COLL(me, me, qe, qe, E[0], E[1], n_el, n_el);
-      COLL(me, me, qe, qe, E[1], E[2], n_el, n_el);
-      COLL(me, me, qe, qe, E[2], E[0], n_el, n_el);
-    }
-    if (ne >= 5)
-      for (unsigned q = 3; q < ne; q += 2) COLL(me, me, qe, qe, E[q], E[q + 1], n_el, n_el);
-  }
-  if (ni == ne)
-    for (unsigned q = 0; q < ne; ++q) COLL(me, mi, qe, qi, E[q], I[q], n_el, n_ion);
-  if (ni > ne && ne > 0 && ni > 0) {
-    const unsigned c_i = (unsigned)floorf((float)ni / (float)ne);
-    const double c_r = (double)((float)ni / (float)ne - (float)c_i);
-    const unsigned ions_1st = (unsigned)((double)(c_i + 1) * c_r * ne);
-    const unsigned els_1st = (unsigned)(c_r * ne);
-    const unsigned ions_2nd = (unsigned)((double)c_i * (1 - c_r) * ne);
-    for (unsigned fgi = 0; fgi < ions_1st; ++fgi) {
-      const int fge = (int)floorf((float)fgi / (float)(c_i + 1));
-      COLL(me, mi, qe, qi, E[fge], I[fgi], n_el, n_ion);
-    }
-    for (unsigned fgi = 0; fgi < ions_2nd; ++fgi) {
-      const int fge = (int)floorf((float)fgi / (float)c_i);
-      COLL(me, mi, qe, qi, E[fge + els_1st], I[fgi + ions_1st], n_el, n_ion);
-    }
-  }
-  if (ni < ne && ne > 0 && ni > 0) {
-    const double c_i = (double)floorf((float)ne / (float)ni);
-    const double c_r = (double)((float)ne / (float)ni) - c_i;
-    const unsigned els_1st = (unsigned)((c_i + 1) * c_r * ni);
-    const unsigned ions_1st = (unsigned)(c_r * ni);
-    const unsigned els_2nd = (unsigned)(c_i * (1 - c_r) * ni);
-    for (unsigned fge = 0; fge < els_1st; ++fge) {
-      const int fgi = (int)floorf((float)fge / (float)(c_i + 1));
-      COLL(me, mi, qe, qi, E[fge], I[fgi], n_el, n_ion);
-    }
-    for (unsigned fge = 0; fge < els_2nd; ++fge) {
-      const int fgi = (int)floorf((float)fge / (float)c_i);
-      COLL(me, mi, qe, qi, E[fge + els_1st], I[fgi + ions_1st], n_el, n_ion);
-    }
-  }
-#undef COLL
+  x.m = plan.total;
   if (x.m) atomicAdd(calls, (unsigned long long)x.m);
   if (p.expect)
     for (int q = 0; q < 12; ++q) p.expect[c * 12 + q] = expect[q];
@@ -372,6 +425,7 @@ void collide_free(CollWork& w) {
     cudaFree(w.count[l]); cudaFree(w.start[l]); cudaFree(w.stage[l]);
   }
   cudaFree(w.moments); cudaFree(w.row_stop); cudaFree(w.calls); cudaFree(w.valid); cudaFree(w.tmp);
+  cudaFree(w.crowded); cudaFree(w.active);
   cudaFree(w.totals);
   w = CollWork();
 }
@@ -387,8 +441,9 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
     total[sp[t].is_ion ? 1 : 0] += sp[t].n;
   }
   const size_t cells = (size_t)g.nr * g.nz;
-  const size_t need = std::max(total[0], total[1]);
+  size_t need = std::max(total[0], total[1]);
   if (w.cap < need || w.cells != cells) {
+    need += need / 4 + 4096;  // headroom: an injected beam grows the lists every step
     for (int l = 0; l < 2; ++l) {
       if (grow(&w.keys[l], need) || grow(&w.keys2[l], need) || grow(&w.vals[l], need) ||
           grow(&w.vals2[l], need) || grow(&w.count[l], cells + 1) || grow(&w.start[l], cells + 1) ||
@@ -396,7 +451,7 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
         return -1;
     }
     if (grow(&w.moments, 4 * cells) || grow(&w.row_stop, (size_t)g.nr) || grow(&w.calls, 1) ||
-        grow(&w.valid, 2))
+        grow(&w.valid, 2) || grow(&w.crowded, cells + 1) || grow(&w.active, cells + 1))
       return -1;
     size_t b1 = 0, b2 = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b1, w.keys[0], w.keys2[0], w.vals[0], w.vals2[0], (int)need);
@@ -412,6 +467,8 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   }
   cudaMemsetAsync(w.calls, 0, sizeof(unsigned long long), s);
   cudaMemsetAsync(w.valid, 0, 2 * sizeof(unsigned), s);
+  cudaMemsetAsync(w.crowded, 0, sizeof(unsigned), s);
+  cudaMemsetAsync(w.active, 0, sizeof(unsigned), s);
   w.launches = 3;  // moments and the pairs of ordinary and of crowded cells
   for (int l = 0; l < 2; ++l) {
     cudaMemsetAsync(w.count[l], 0, (cells + 1) * sizeof(unsigned), s);
@@ -453,13 +510,15 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   cudaMemsetAsync(w.row_stop, 0x7f, (size_t)g.nr * sizeof(int), s);
   moments_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                         w.start[1], w.count[1], w.keys2[1], w.moments,
-                                                        w.row_stop, p.scheme == 1 ? w.totals : nullptr);
+                                                        w.row_stop, p.scheme == 1 ? w.totals : nullptr,
+                                                        w.crowded, w.active);
   auto cells_k = p.scheme == 1 ? collide_cells_kernel<1>
                  : p.scheme == 2 ? collide_cells_kernel<2> : collide_cells_kernel<0>;
   cells_k<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0], w.start[1],
-                                                 w.count[1], w.keys2[1], w.moments, w.row_stop, w.calls);
+                                                 w.count[1], w.keys2[1], w.moments, w.row_stop, w.calls,
+                                                 p.only ? w.active : nullptr);
   collide_crowded(g, staged.stage, p, w.start[0], w.count[0], w.keys2[0], w.start[1], w.count[1], w.keys2[1],
-                  w.moments, w.row_stop, w.calls, s);
+                  w.moments, w.row_stop, w.calls, w.crowded, s);
   if (p.scheme == 1) {
     ta77s_correct_kernel<<<blocks_for(cells), kThreads, 0, s>>>(g, staged, p, w.start[0], w.count[0], w.keys2[0],
                                                                 w.start[1], w.count[1], w.keys2[1], w.totals);

@@ -28,6 +28,18 @@ struct CollSpecies {
   const unsigned* id = nullptr;
   float *vr32 = nullptr, *vphi32 = nullptr, *vz32 = nullptr;
   const float* w32 = nullptr;
+  // float layout: slots [0, sorted) are grouped by tile, tile t holding
+  // [tile_start[t], tile_start[t+1]) (the step's tile sort; sorted = 0 when
+  // not), in layers: layer q holds, in cell order, the q-th particle of each
+  // tile cell whose count at the sort (cell_count) exceeds q, from
+  // layer_start[t][q] with the cell's place given by layer_mask and
+  // layer_prefix; the particles beyond kLayerCap layers follow in a run
+  const unsigned* tile_start = nullptr;
+  const unsigned* cell_count = nullptr;
+  const unsigned* layer_mask = nullptr;
+  const unsigned short* layer_prefix = nullptr;
+  const unsigned* layer_start = nullptr;
+  size_t sorted = 0;
 };
 
 struct CollParams {
@@ -64,6 +76,8 @@ struct CollWork {
   int* row_stop = nullptr;                  // per row: first cell that stops the row
   unsigned long long* calls = nullptr;      // device counter of pair calls
   unsigned* valid = nullptr;                // device: entries appended to each list
+  unsigned* crowded = nullptr;              // device: [0] crowded cells listed in [1..]
+  unsigned* active = nullptr;               // device: [0] other chosen cells (CollParams::only) in [1..]
   void* tmp = nullptr;
   size_t tmp_bytes = 0;
   size_t cells = 0;
@@ -77,9 +91,10 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
 void collide_free(CollWork& w);
 // The pairs of the cells holding more than p.crowded particles, one warp per
 // cell (pcg_collide_crowded.cu); the per-cell kernel of collide_p12 skips them.
+// list[0] is the number of such cells, list[1..] the cells (device memory).
 void collide_crowded(const GridGeom& g, double4* const stage[2], const CollParams& p, const unsigned* st_e,
                      const unsigned* n_e, const unsigned long long* le, const unsigned* st_i, const unsigned* n_i,
                      const unsigned long long* li, const double* mom, const int* row_stop, unsigned long long* calls,
-                     cudaStream_t s);
+                     const unsigned* list, cudaStream_t s);
 
 }  // namespace pcg

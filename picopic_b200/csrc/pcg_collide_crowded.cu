@@ -3,6 +3,8 @@
 // pcg_collide.cu.  Built with --fmad=false like the other FP64 kernels.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "pcg_collide_pair.cuh"
 
 namespace pcg {
@@ -31,12 +33,10 @@ __device__ __forceinline__ void collide_pair(PairCtx& x, double ma, double mb, d
 // collision therefore sees the velocities it sees in the reference order
 // and the results are the same.
 template <int SCHEME>
-__global__ void collide_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
-                               const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
-                               const unsigned* n_i, const unsigned long long* li, const double* mom,
-                               const int* row_stop, unsigned long long* calls) {
-  const size_t c = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;  // one warp per cell
-  const unsigned lane = threadIdx.x & 31;
+__device__ void crowded_cell(size_t c, unsigned lane, const GridGeom& g, const Staged& tab, const CollParams& p,
+                             const unsigned* st_e, const unsigned* n_e, const unsigned long long* le,
+                             const unsigned* st_i, const unsigned* n_i, const unsigned long long* li,
+                             const double* mom, const int* row_stop, unsigned long long* calls) {
   if (c >= (size_t)g.nr * g.nz) return;
   if (p.only && p.only[c] != p.only_value) return;
   if (n_e[c] + n_i[c] <= p.crowded) return;  // collide_cells_kernel takes the others
@@ -145,16 +145,36 @@ __global__ void collide_kernel(GridGeom g, Staged tab, CollParams p, const unsig
   }
 }
 
+// The crowded cells listed by the moments pass (list[0] cells in list[1..]),
+// a warp per cell over a grid of fixed size: with no crowded cell the
+// launch costs nothing in proportion to the grid.
+template <int SCHEME>
+__global__ void collide_kernel(GridGeom g, Staged tab, CollParams p, const unsigned* st_e,
+                               const unsigned* n_e, const unsigned long long* le, const unsigned* st_i,
+                               const unsigned* n_i, const unsigned long long* li, const double* mom,
+                               const int* row_stop, unsigned long long* calls, const unsigned* list) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned warps = (gridDim.x * blockDim.x) >> 5;
+  const unsigned n = list[0];
+  for (unsigned q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += warps)
+    crowded_cell<SCHEME>(list[1 + q], lane, g, tab, p, st_e, n_e, le, st_i, n_i, li, mom, row_stop, calls);
+}
+
 }  // namespace
 
 void collide_crowded(const GridGeom& g, double4* const stage[2], const CollParams& p, const unsigned* st_e,
                      const unsigned* n_e, const unsigned long long* le, const unsigned* st_i, const unsigned* n_i,
                      const unsigned long long* li, const double* mom, const int* row_stop, unsigned long long* calls,
-                     cudaStream_t s) {
+                     const unsigned* list, cudaStream_t s) {
   const size_t cells = (size_t)g.nr * g.nz;
   const Staged tab{{stage[0], stage[1]}};
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // up to 8 blocks of kThreads / 32 warps per SM, no more warps than cells
+  const size_t blocks = std::min<size_t>(blocks_for(32 * cells), (size_t)sms * 8);
   auto k = p.scheme == 1 ? collide_kernel<1> : p.scheme == 2 ? collide_kernel<2> : collide_kernel<0>;
-  k<<<blocks_for(32 * cells), kThreads, 0, s>>>(g, tab, p, st_e, n_e, le, st_i, n_i, li, mom, row_stop, calls);
+  k<<<(unsigned)blocks, kThreads, 0, s>>>(g, tab, p, st_e, n_e, le, st_i, n_i, li, mom, row_stop, calls, list);
 }
 
 }  // namespace pcg

@@ -73,8 +73,8 @@ __device__ __forceinline__ bool slot_of(const GridGeom& g, const CollSpecies& sp
 // their values with a warp reduction first (whole-warp groups, the usual
 // case for particles stored cell by cell) or one after another through the
 // group's leader, so that one atomic per word and group reaches memory.
-__global__ void moments_kernel(GridGeom g, CollSpecies sp, double* mom) {
-  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+__global__ void moments_kernel(GridGeom g, CollSpecies sp, double* mom, size_t j0) {
+  const size_t j = j0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   size_t c = 0;
   double v[3] = {0, 0, 0}, w = 0;
   const bool valid = j < sp.n && slot_of(g, sp, j, &c, v);
@@ -102,6 +102,84 @@ __global__ void moments_kernel(GridGeom g, CollSpecies sp, double* mom) {
   if (!valid || lane != leader) return;
   double* m = mom + c * kMomWords + (sp.is_ion ? 8 : 0);
   for (int q = 0; q < 8; ++q) atomicAdd(m + q, val[q]);
+}
+
+constexpr int kWalk = 4;  // layers a tile walk loads at once
+
+// Slot of the q-th particle (q < kLayerCap) that the last tile sort put in
+// cell lc of tile t (tile-relative: the tile's first slot is 0).
+__device__ __forceinline__ unsigned layer_slot(const CollSpecies& sp, const unsigned* ls, int t, unsigned q, int lc) {
+  const size_t at = ((size_t)t * kLayerCap + q) * kTileWords + (lc >> 5);
+  return ls[q] + sp.layer_prefix[at] + __popc(sp.layer_mask[at] & ((1u << (lc & 31)) - 1u));
+}
+
+// The same sums for the tile-sorted slots [0, sp.sorted) of a float species.
+// A block of kTileCells threads takes a tile at a time and thread lc the
+// tile's cell lc: it walks the particles the sort put in its cell, layer by
+// layer (a layer's particles are contiguous and in cell order, so the
+// block's loads coalesce), sums in registers and adds the sums to the grid
+// with one atomic per word.  A particle that has left its cell since the
+// sort, and the run of particles beyond kLayerCap layers, add to the grid
+// directly.  The sums equal moments_kernel's up to the order of the FP64
+// additions.
+__global__ void __launch_bounds__(kTileCells) tile_moments_kernel(GridGeom g, TileGrid tg, CollSpecies sp,
+                                                                  double* mom) {
+  __shared__ unsigned ls[kLayerCap + 1];
+  const int off = sp.is_ion ? 8 : 0, lc = threadIdx.x;
+  for (int t = blockIdx.x; t < tg.ntiles; t += gridDim.x) {
+    const size_t base = sp.tile_start[t], end = sp.tile_start[t + 1];
+    if (base >= end) continue;  // the same for every thread of the block
+    __syncthreads();            // the previous tile's layer starts are read
+    for (int q = threadIdx.x; q <= kLayerCap; q += blockDim.x) ls[q] = sp.layer_start[(size_t)t * (kLayerCap + 1) + q];
+    __syncthreads();
+    const int ti = t / tg.ntz, tk = t - ti * tg.ntz;
+    const int ci = ti * tg.tr + lc / tg.tz, ck = tk * tg.tz + lc % tg.tz;
+    const size_t mine = (size_t)ci * g.nz + ck;
+    const unsigned nq = min(sp.cell_count[(size_t)t * kTileCells + lc], (unsigned)kLayerCap);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // kWalk layers at a time: their loads are independent and overlap
+    for (unsigned q0 = 0; q0 < nq; q0 += kWalk) {
+      size_t j[kWalk];
+      int cell[kWalk];
+      float vr[kWalk], vp[kWalk], vz[kWalk], ww[kWalk];
+#pragma unroll
+      for (int u = 0; u < kWalk; ++u) j[u] = q0 + u < nq ? base + layer_slot(sp, ls, t, q0 + u, lc) : ~(size_t)0;
+#pragma unroll
+      for (int u = 0; u < kWalk; ++u) {
+        cell[u] = j[u] != ~(size_t)0 ? sp.cell[j[u]] : kDeadCell;
+        if (cell[u] >= 0) { vr[u] = sp.vr32[j[u]]; vp[u] = sp.vphi32[j[u]]; vz[u] = sp.vz32[j[u]]; ww[u] = sp.w32[j[u]]; }
+      }
+#pragma unroll
+      for (int u = 0; u < kWalk; ++u) {
+        if (cell[u] < 0) continue;
+        const int pi = cell_r_of(cell[u]), pk = cell_z_of(cell[u]);
+        if (pi < 0 || pi >= g.nr || pk >= g.nz) continue;
+        const size_t c = (size_t)pi * g.nz + pk;
+        const double w = ww[u], v0 = vr[u], v1 = vp[u], v2 = vz[u];
+        const double val[8] = {1.0, w, w * v0, w * v1, w * v2, w * v0 * v0, w * v1 * v1, w * v2 * v2};
+        if (c == mine) {
+          for (int k = 0; k < 8; ++k) acc[k] += val[k];
+        } else {
+          double* m = mom + c * kMomWords + off;
+          for (int k = 0; k < 8; ++k) atomicAdd(m + k, val[k]);
+        }
+      }
+    }
+    for (size_t j = base + ls[kLayerCap] + threadIdx.x; j < end; j += blockDim.x) {
+      size_t c;
+      double v[3];
+      if (!slot_of(g, sp, j, &c, v)) continue;
+      const double w = sp.w32[j];
+      const double val[8] = {1.0, w, w * v[0], w * v[1], w * v[2], w * v[0] * v[0], w * v[1] * v[1],
+                             w * v[2] * v[2]};
+      double* m = mom + c * kMomWords + off;
+      for (int k = 0; k < 8; ++k) atomicAdd(m + k, val[k]);
+    }
+    if (acc[0] != 0.0) {
+      double* m = mom + mine * kMomWords + off;
+      for (int k = 0; k < 8; ++k) atomicAdd(m + k, acc[k]);
+    }
+  }
 }
 
 // The state and raw features of cell c (row i); false when the cell has
@@ -259,8 +337,8 @@ __global__ void __launch_bounds__(mlp::tc::kThreads) learned_cells_kernel(GridGe
 // Applies the per-cell transforms; after a tensor-core time-out (count[2])
 // the transforms are incomplete and nothing is applied.
 __global__ void transform_kernel(GridGeom g, CollSpecies sp, const double* xform, const unsigned char* flag,
-                                 const unsigned long long* count) {
-  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+                                 const unsigned long long* count, size_t j0) {
+  const size_t j = j0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (j >= sp.n || count[2]) return;
   size_t c;
   double v[3];
@@ -274,11 +352,92 @@ __global__ void transform_kernel(GridGeom g, CollSpecies sp, const double* xform
   }
 }
 
+// transform_kernel over the tile-sorted slots of a float species, walked
+// as tile_moments_kernel walks them: thread lc reads its cell's transform
+// once; a particle that has left its cell since the sort, and the run
+// beyond kLayerCap layers, read their cell's from the grid.
+__device__ __forceinline__ void apply_transform(const CollSpecies& sp, size_t j, double v[3], const double tr[6]) {
+  for (int a = 0; a < 3; ++a) v[a] = tr[a] + (v[a] - tr[a]) * tr[3 + a];
+  sp.vr32[j] = (float)v[0]; sp.vphi32[j] = (float)v[1]; sp.vz32[j] = (float)v[2];
+}
+
+__global__ void __launch_bounds__(kTileCells) tile_transform_kernel(GridGeom g, TileGrid tg, CollSpecies sp,
+                                                                    const double* xform,
+                                                                    const unsigned char* flag,
+                                                                    const unsigned long long* count) {
+  __shared__ unsigned ls[kLayerCap + 1];
+  if (count[2]) return;
+  const int off = sp.is_ion ? 6 : 0, lc = threadIdx.x;
+  for (int t = blockIdx.x; t < tg.ntiles; t += gridDim.x) {
+    const size_t base = sp.tile_start[t], end = sp.tile_start[t + 1];
+    if (base >= end) continue;  // the same for every thread of the block
+    __syncthreads();
+    for (int q = threadIdx.x; q <= kLayerCap; q += blockDim.x) ls[q] = sp.layer_start[(size_t)t * (kLayerCap + 1) + q];
+    __syncthreads();
+    const int ti = t / tg.ntz, tk = t - ti * tg.ntz;
+    const int ci = ti * tg.tr + lc / tg.tz, ck = tk * tg.tz + lc % tg.tz;
+    const size_t mine = (size_t)ci * g.nz + ck;
+    const unsigned nq = min(sp.cell_count[(size_t)t * kTileCells + lc], (unsigned)kLayerCap);
+    double my_tr[6];
+    const bool my_on = nq > 0 && flag[mine] == 1;
+    if (my_on)
+      for (int k = 0; k < 6; ++k) my_tr[k] = xform[mine * 12 + off + k];
+    for (unsigned q0 = 0; q0 < nq; q0 += kWalk) {
+      size_t j[kWalk];
+      int cell[kWalk];
+      float vr[kWalk], vp[kWalk], vz[kWalk];
+#pragma unroll
+      for (int u = 0; u < kWalk; ++u) j[u] = q0 + u < nq ? base + layer_slot(sp, ls, t, q0 + u, lc) : ~(size_t)0;
+#pragma unroll
+      for (int u = 0; u < kWalk; ++u) {
+        cell[u] = j[u] != ~(size_t)0 ? sp.cell[j[u]] : kDeadCell;
+        if (cell[u] >= 0) { vr[u] = sp.vr32[j[u]]; vp[u] = sp.vphi32[j[u]]; vz[u] = sp.vz32[j[u]]; }
+      }
+#pragma unroll
+      for (int u = 0; u < kWalk; ++u) {
+        if (cell[u] < 0) continue;
+        const int pi = cell_r_of(cell[u]), pk = cell_z_of(cell[u]);
+        if (pi < 0 || pi >= g.nr || pk >= g.nz) continue;
+        const size_t c = (size_t)pi * g.nz + pk;
+        double v[3] = {vr[u], vp[u], vz[u]};
+        if (c == mine) {
+          if (my_on) apply_transform(sp, j[u], v, my_tr);
+        } else if (flag[c] == 1) {
+          double tr[6];
+          for (int k = 0; k < 6; ++k) tr[k] = xform[c * 12 + off + k];
+          apply_transform(sp, j[u], v, tr);
+        }
+      }
+    }
+    for (size_t j = base + ls[kLayerCap] + threadIdx.x; j < end; j += blockDim.x) {
+      size_t c;
+      double v[3];
+      if (!slot_of(g, sp, j, &c, v) || flag[c] != 1) continue;
+      double tr[6];
+      for (int k = 0; k < 6; ++k) tr[k] = xform[c * 12 + off + k];
+      apply_transform(sp, j, v, tr);
+    }
+  }
+}
+
 template <typename T>
 int grow(T** p, size_t n) {
   cudaFree(*p);
   *p = nullptr;
   return cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess ? 0 : -1;
+}
+
+// a float species whose first slots are grouped by tile (the tile kernels' input)
+bool tiled(const CollSpecies& sp) {
+  return sp.cell && sp.tile_start && sp.cell_count && sp.layer_mask && sp.layer_prefix && sp.layer_start &&
+         sp.sorted > 0 && sp.sorted <= sp.n;
+}
+
+unsigned tile_grid_blocks(const TileGrid& tg) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (unsigned)std::max(1, std::min(tg.ntiles, sms * 8));
 }
 
 int ensure(const GridGeom& g, LearnedWork& w) {
@@ -296,8 +455,15 @@ int ensure(const GridGeom& g, LearnedWork& w) {
 int learned_moments(const GridGeom& g, const CollSpecies* sp, int nsp, LearnedWork& w, cudaStream_t s) {
   if (ensure(g, w)) return -1;
   cudaMemsetAsync(w.mom, 0, w.cells * kMomWords * sizeof(double), s);
-  for (int t = 0; t < nsp; ++t)
-    if (sp[t].n) moments_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.mom);
+  const TileGrid tg = f32_tile_grid(g);
+  const unsigned tile_blocks = tile_grid_blocks(tg);
+  w.launches = 0;
+  for (int t = 0; t < nsp; ++t) {
+    const size_t j0 = tiled(sp[t]) ? sp[t].sorted : 0;
+    if (j0) tile_moments_kernel<<<tile_blocks, kTileCells, 0, s>>>(g, tg, sp[t], w.mom);
+    if (sp[t].n > j0) moments_kernel<<<blocks_for(sp[t].n - j0), kThreads, 0, s>>>(g, sp[t], w.mom, j0);
+    w.launches += (j0 ? 1 : 0) + (sp[t].n > j0 ? 1 : 0);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -324,8 +490,16 @@ int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const Learne
   const unsigned blocks = (unsigned)std::min<size_t>(tiles, (size_t)sms * 2);
   learned_cells_kernel<<<blocks, mlp::tc::kThreads, smem, s>>>(g, ph, w.mom, w.params, w.norm, w.xform, w.flag,
                                                                 w.count);
-  for (int t = 0; t < nsp; ++t)
-    if (sp[t].n) transform_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], w.xform, w.flag, w.count);
+  ++w.launches;
+  const TileGrid tg = f32_tile_grid(g);
+  const unsigned tile_blocks = tile_grid_blocks(tg);
+  for (int t = 0; t < nsp; ++t) {
+    const size_t j0 = tiled(sp[t]) ? sp[t].sorted : 0;
+    if (j0) tile_transform_kernel<<<tile_blocks, kTileCells, 0, s>>>(g, tg, sp[t], w.xform, w.flag, w.count);
+    if (sp[t].n > j0)
+      transform_kernel<<<blocks_for(sp[t].n - j0), kThreads, 0, s>>>(g, sp[t], w.xform, w.flag, w.count, j0);
+    w.launches += (j0 ? 1 : 0) + (sp[t].n > j0 ? 1 : 0);
+  }
   unsigned long long c3[3] = {0, 0, 0};
   if (cudaMemcpyAsync(c3, w.count, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)

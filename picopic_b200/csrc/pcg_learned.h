@@ -39,6 +39,7 @@ struct LearnedWork {
   float* params = nullptr;        // the model's FP32 parameters
   LearnedNorm norm{};
   bool model = false;
+  unsigned launches = 0;  // kernels launched by the last learned_moments / learned_step
 };
 
 // Per-cell moment sums of the species (electron list: every species not

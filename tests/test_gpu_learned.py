@@ -46,15 +46,18 @@ def _grid(nr=32, nz=64, dt=1e-13):
     return Geometry(nr, nz, nr * dr, nz * dr, dt)
 
 
-def _random_domain(grid, seed=3):
+def _random_domain(grid, seed=3, precision="f64"):
     from picopic_b200 import learned as L
     rng = np.random.default_rng(seed)
     te, ti, dens, drift, ppc = L.cell_states(grid, rng, L.Sampling())
     pe = L.cell_particles(grid, rng, te, dens[0], drift, ppc[0], 1.0)
     pi = L.cell_particles(grid, rng, ti, dens[1], np.zeros_like(drift), ppc[1], L.MASS_ION)
-    d = L._domain(grid, 0, seed, capacity=max(pe[0].size, pi[0].size) + 16)
+    d = L._domain(grid, 0, seed, capacity=max(pe[0].size, pi[0].size) + 16, precision=precision)
     d.set_particles(0, *pe)
     d.set_particles(1, *pi)
+    if precision == "f32":  # group the slots by tile, as steps keep them
+        d.tile_sort(0)
+        d.tile_sort(1)
     return d
 
 
@@ -69,11 +72,12 @@ def test_features_match_restatement():
     assert np.abs(S - So).max() <= 1e-12 * So.max()
 
 
-def test_learned_step_conserves_and_matches_transform():
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_learned_step_conserves_and_matches_transform(precision):
     from picopic_b200 import learned as L
     from picopic_b200.mlp import Mlp
     g = _grid()
-    d = _random_domain(g, seed=4)
+    d = _random_domain(g, seed=4, precision=precision)
     params, norm = L.load_model()
     d.set_collision_model(params, norm)
     m0 = d.cell_moments()
@@ -94,13 +98,15 @@ def test_learned_step_conserves_and_matches_transform():
     on = np.isfinite(rel) & (rel <= 1e-4)  # BF16 network: outputs agree to ~1e-3 of y, y S ~ 1e-4
     assert on.sum() >= learned
     # per cell: each species' momentum and the total kinetic energy unchanged
+    # (to FP64 rounding; the float layout stores the new velocities in FP32)
+    rtol = RTOL_CONS if precision == "f64" else 1e-6
     for l in (0, 1):
         dp = np.abs(m1[on, 8 * l + 2:8 * l + 5] - m0[on, 8 * l + 2:8 * l + 5]).max(1)
         scale = np.sqrt(m0[on, 8 * l + 1] * m0[on, 8 * l + 5:8 * l + 8].sum(1))
-        assert (dp <= RTOL_CONS * scale).all()
+        assert (dp <= rtol * scale).all()
     e0 = ME * m0[on, 5:8].sum(1) + 1836 * ME * m0[on, 13:16].sum(1)
     e1 = ME * m1[on, 5:8].sum(1) + 1836 * ME * m1[on, 13:16].sum(1)
-    assert (np.abs(e1 - e0) <= RTOL_CONS * e0).all()
+    assert (np.abs(e1 - e0) <= rtol * e0).all()
 
 
 # (density, electron T_par/T_perp eV, ion T eV)
@@ -182,6 +188,81 @@ def test_out_of_box_cells_take_the_binary_operator():
     d.set_collision_model(*L.load_model())
     learned, fallback = d.collide_learned()
     assert learned == 0 and fallback == cells
+
+
+def _host_moments(d, g, slots=(0, 1)):
+    """Domain.cell_moments restated from the exported particles."""
+    m = np.zeros((g.nr * g.nz, 16))
+    for l, slot in enumerate(slots):
+        p = d.get_particles(slot)
+        c = p["cell_r"] * g.nz + p["cell_z"]
+        ok = (p["cell_r"] >= 0) & (p["cell_r"] < g.nr) & (p["cell_z"] >= 0) & (p["cell_z"] < g.nz)
+        w = p["w"]
+        cols = [np.ones_like(w), w, w * p["vr"], w * p["vphi"], w * p["vz"],
+                w * p["vr"] * p["vr"], w * p["vphi"] * p["vphi"], w * p["vz"] * p["vz"]]
+        for q, v in enumerate(cols):
+            np.add.at(m[:, 8 * l + q], c[ok], v[ok])
+    return m
+
+
+def test_float_layout_moments_by_tile():
+    """Cell moments of tile-sorted float species (a block per tile, the
+    tile's cells summed in shared memory), with particles that left their
+    tile since the sort and slots appended after it, equal the sums over
+    the exported particles."""
+    from picopic_b200 import learned as L
+    g = _grid(40, 96, dt=2e-14)  # 5 x 3 tiles, the last row of tiles partly outside the grid
+    rng = np.random.default_rng(7)
+    cells = g.nr * g.nz
+    te = np.full((cells, 3), 2.0)
+    drift = np.zeros((cells, 3))
+    drift[:, 2] = 1e8  # 0.2 cells per step along z: particles cross tile borders
+    pp = rng.integers(10, 30, cells)
+    d = L._domain(g, 0, 5, capacity=cells * 80, precision="f32")
+    d.set_particles(0, *L.cell_particles(g, rng, te, np.full(cells, 1e20), drift, pp, 1.0))
+    d.set_particles(1, *L.cell_particles(g, rng, te / 4, np.full(cells, 1e20), np.zeros((cells, 3)), pp,
+                                         L.MASS_ION))
+    d.step(2)
+    d.tile_sort(0)
+    d.tile_sort(1)
+    d.step(1)
+    extra = L.cell_particles(g, rng, te, np.full(cells, 1e20), drift, np.full(cells, 2), 1.0)
+    d.set_particles(0, *extra, append=True)
+    m = d.cell_moments()
+    h = _host_moments(d, g)
+    scale = np.abs(h).max(0) + 1e-300
+    assert (np.abs(m - h) <= 1e-12 * scale).all()
+
+
+def test_fallback_collides_every_fallback_cell():
+    """Reference quirks: the binary pass stops a row at its first empty
+    cell (collisionsP12.cpp:351-354).  The fallback pass of a learned step
+    runs over the fallback cells only, and a cell left to the learned path
+    is not an empty cell of that pass: every fallback cell collides, also
+    behind learned cells in its row."""
+    from picopic_b200 import Domain
+    from picopic_b200 import learned as L
+    g = _grid(16, 32)
+    rng = np.random.default_rng(2)
+    cells = g.nr * g.nz
+    te = np.full((cells, 3), 1.0)
+    drift = np.zeros((cells, 3))
+    odd = np.arange(cells) % 2 == 1
+    drift[odd, 2] = 4 * np.sqrt(1.6e-19 / ME)  # outside the training box
+    d = Domain(g, precision="f64", quirks="reference", seed=1)
+    d.add(L.ELECTRONS, capacity=cells * 100 + 16)
+    d.add(L.IONS, capacity=cells * 100 + 16)
+    pp = np.full(cells, 100)
+    d.set_particles(0, *L.cell_particles(g, rng, te, np.full(cells, 1e20), drift, pp, 1.0))
+    d.set_particles(1, *L.cell_particles(g, rng, te / 2, np.full(cells, 1e20), np.zeros((cells, 3)), pp,
+                                         L.MASS_ION))
+    d.set_collision_model(*L.load_model())
+    m0 = d.cell_moments()
+    learned, fallback = d.collide_learned()
+    m1 = d.cell_moments()
+    assert fallback == odd.sum() and learned == cells - odd.sum()
+    changed = np.any(m1[:, 5:8] != m0[:, 5:8], axis=1)
+    assert changed[odd].all()
 
 
 @pytest.mark.parametrize("mode", ["binary", "learned"])
