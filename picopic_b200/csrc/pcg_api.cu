@@ -329,6 +329,8 @@ struct TimerScope {
   }
 };
 
+int compact(pcg_handle* h);
+
 int stage_inject(pcg_handle* h) {
   TimerScope ts(h, PCG_TIMER_INJECT);
   for (size_t t = 0; t < h->sp.size(); ++t) {
@@ -337,6 +339,13 @@ int stage_inject(pcg_handle* h) {
     BeamInject b{};
     unsigned count = beam_count(h, s, &b, (int)t);
     if (count == 0) continue;
+    if (s.n + count > s.cap && !is_f64(h)) {
+      // the dead slots that the float sorts left behind still count in n:
+      // remove them (this waits for the stream) before giving up
+      int rc = check_status(h);
+      if (rc != PCG_OK) return rc;
+      if (h->h_status->dead_slots > h->dead_dropped && (rc = compact(h)) != PCG_OK) return rc;
+    }
     if (s.n + count > s.cap) return fail(h, PCG_ERR_CAPACITY, "beam '" + s.name + "' capacity exceeded");
     if (is_f64(h)) {
       launch_inject_f64(h->g, view64(h, s), s.n, count, b, h->stream);

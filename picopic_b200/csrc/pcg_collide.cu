@@ -45,11 +45,12 @@ namespace {
 // ---------------------------------------------------------------------------
 // 1. keys
 
-__global__ void key_kernel(GridGeom g, SpeciesTable tab, int t, unsigned long long* keys,
+// (the species comes by value: a run-time index into the by-value species
+// table would copy the whole table to each thread's local memory)
+__global__ void key_kernel(GridGeom g, CollSpecies sp, int t, unsigned long long* keys,
                            unsigned long long* vals, unsigned* count, unsigned* n_valid,
                            const unsigned char* only, unsigned char only_value) {
   const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const CollSpecies& sp = tab.s[t];
   int ci = -1, ck = -1;
   unsigned id = 0;
   if (j < sp.n) {
@@ -474,7 +475,7 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
     cudaMemsetAsync(w.count[l], 0, (cells + 1) * sizeof(unsigned), s);
     for (int t = 0; t < nsp; ++t) {
       if ((sp[t].is_ion ? 1 : 0) != l || !sp[t].n) continue;
-      key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, tab, t, w.keys[l], w.vals[l], w.count[l],
+      key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], t, w.keys[l], w.vals[l], w.count[l],
                                                           w.valid + l, p.only, p.only_value);
       ++w.launches;
     }

@@ -52,14 +52,18 @@ struct SpeciesF32Buffers {
   unsigned short* layer_prefix = nullptr;  // same shape: set bits in the words before
   unsigned* layer_start = nullptr;     // ntiles * (kLayerCap + 1); entry kLayerCap: overflow run
   unsigned* overflow = nullptr;        // ntiles, cursors of the overflow runs
-  unsigned* sort_info = nullptr;       // device: largest tile, occupied tiles
-  unsigned* host_info = nullptr;       // pinned: live count, largest tile, occupied tiles
+  // device: largest tile, occupied tiles, blocks per tile, live slots of
+  // the last sort (the step kernels read the blocks per tile here)
+  unsigned* sort_info = nullptr;
+  unsigned* host_info = nullptr;       // pinned: the same, copied after each sort (a hint)
   void* scan_tmp = nullptr;            // the tile-count scan's workspace
   size_t scan_tmp_bytes = 0;
-  int splits = 1;                      // blocks per tile in the step (the largest tile's share)
+  int splits = 1;                      // blocks per tile launched (the largest tile's share)
+  int sorts = 0;                       // sorts issued
   // particles of a step that left their tile's shared windows (and took the
-  // slow global path): counted on the device, copied to pinned memory after
-  // every step and read by the host, possibly a step late, to decide a sort
+  // slow global path): counted on the device in drift[0], copied with the
+  // device's count of sorts (drift[1]) to pinned memory after every step
+  // and read by the host, possibly steps late, to decide a sort
   unsigned* drift = nullptr;
   unsigned* drift_host = nullptr;
   uint64_t launches = 0;  // kernels launched for this species (sorts and steps)

@@ -407,8 +407,8 @@ constexpr size_t kPairFixedBytes = sizeof(float) * (6 * kFWR * kFWS + 3 * kJWR *
                                    sizeof(float4) * 2 * kFWR + sizeof(unsigned) * kQueue * (kThreads / 32);
 constexpr size_t kPairSmemBytes = kPairFixedBytes + 1024 + (size_t)kStages * kStageBytes + 2 * kStages * 8;
 
-// One block per part of a tile (gridDim.y blocks share a crowded tile, each
-// a contiguous part of its slots), for a plasma species under the
+// One block per part of a tile (up to gridDim.y blocks share a crowded tile,
+// each a contiguous part of its slots), for a plasma species under the
 // relativistic Boris pusher and the Villasenor-Buneman current.  The slots
 // arrive through the staged chunks above; each thread takes two per chunk
 // (i and i + kThreads) through pair_particles.  Live particles the pair path
@@ -428,8 +428,12 @@ __global__ void __launch_bounds__(kThreads, 4)
   a.fixed = FIX;
   extern __shared__ __align__(16) float smem[];
   const int t = blockIdx.x;
+  // the tile's parts: the blocks per tile of the last sort (on the device),
+  // up to the gridDim.y launched
+  const unsigned np = max(1u, min(b.sort_info[2], gridDim.y));
+  if (blockIdx.y >= np) return;
   const unsigned ts = b.tile_start[t], te = b.tile_start[t + 1];
-  const unsigned part = (te - ts + gridDim.y - 1) / gridDim.y;
+  const unsigned part = (te - ts + np - 1) / np;
   const unsigned bs = ts + blockIdx.y * part, be = min(bs + part, te);
   if (bs >= be) return;
   const unsigned nchunks = (be - bs + kChunk - 1) / kChunk;

@@ -836,7 +836,11 @@ __global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
   if (FIX >= 0) a.fixed = FIX;
   extern __shared__ float smem[];
   const int t = blockIdx.x;
-  // blockIdx.y of gridDim.y blocks sharing the tile takes every gridDim.y-th run of blockDim.x
+  // blockIdx.y of the np blocks sharing the tile (the blocks per tile of the
+  // last sort, on the device, up to the gridDim.y launched) takes every
+  // np-th run of blockDim.x
+  const unsigned np = max(1u, min(b.sort_info[2], gridDim.y));
+  if (blockIdx.y >= np) return;
   const unsigned s = b.tile_start[t] + blockIdx.y * blockDim.x, e = b.tile_start[t + 1];
   if (s >= e) return;
   const int tr = t / tg.ntz, tz = t - tr * tg.ntz;
@@ -869,7 +873,7 @@ __global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
   const SharedFields sv{sF, fi0, fk0, sR};
   const SharedDep sd{sJ, ji0, jk0};
   // each thread walks its slots with the next slot's loads in flight
-  const unsigned stride = gridDim.y * blockDim.x;
+  const unsigned stride = np * blockDim.x;
   unsigned j = s + threadIdx.x;
   Slot cur{};
   if (j < e) cur = load_slot(b, j);

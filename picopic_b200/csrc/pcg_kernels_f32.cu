@@ -257,34 +257,61 @@ void swap_buffers(SpeciesF32Buffers& b) {
 // Blocks per tile for the step: enough that about target_blocks blocks run
 // when few tiles are occupied (a narrow beam), each with at least min_split
 // particles (F32Step; the defaults 148 x 16 and 1024 suit one run on the GPU).
+// Computed on the device after a sort into info[2] (info[0] the largest
+// tile, info[1] the occupied tiles), with info[3] the live slots.
+__global__ void sort_finish_kernel(unsigned* info, const unsigned* live, unsigned target_blocks, unsigned min_split,
+                                   unsigned* epoch) {
+  *epoch += 1;  // drift[1]: the sorts so far, copied to the host with each step's drift count
+  const unsigned largest = info[0], occupied = info[1];
+  unsigned splits = 1;
+  if (occupied) {
+    splits = max(1u, min((target_blocks + occupied - 1) / occupied, (largest + min_split - 1) / min_split));
+    splits = min(splits, 65535u);
+  }
+  info[2] = splits;
+  info[3] = *live;
+}
 
+// The slots from the live count on (the dead slots the sort dropped) read
+// as dead in the sorted buffer.
+__global__ void fill_dead_kernel(int* cell, const unsigned* live, size_t n) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j < n && j >= *live) cell[j] = kDeadCell;
+}
+
+// A tile sort of the species' n slots.  With `wait` the host reads the
+// outcome (the live count becomes n, the blocks per tile exact); without,
+// nothing waits for the stream: n stays, the dropped dead slots remain as
+// dead slots after the tiles, and the step's launch takes the blocks per
+// tile of the last sort the host has seen (the kernels use the device's
+// value, up to that many).
 int tile_sort(const TileGrid& tg, unsigned target_blocks, unsigned min_split, SpeciesF32Buffers& b,
-              size_t* n, cudaStream_t s) {
+              size_t* n, cudaStream_t s, bool wait) {
   const size_t nt = (size_t)tg.ntiles;
   unsigned* counts = b.tile_cursor;
   cudaMemsetAsync(b.cell_count, 0, nt * kTileCells * sizeof(unsigned), s);
   cudaMemsetAsync(counts + nt, 0, sizeof(unsigned), s);
-  cudaMemsetAsync(b.sort_info, 0, 2 * sizeof(unsigned), s);
+  cudaMemsetAsync(b.sort_info, 0, 4 * sizeof(unsigned), s);
   if (*n) cell_rank_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b.cell, *n, tg, b.cell_count, b.rank);
   tile_layers_kernel<<<(unsigned)nt, kThreads, 0, s>>>(tg, b, counts);
   size_t tmp = b.scan_tmp_bytes;
   cub::DeviceScan::ExclusiveSum(b.scan_tmp, tmp, counts, b.tile_start, (int)(nt + 1), s);
   if (*n) tile_scatter_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b, *n, tg);
-  b.launches += (*n ? 2 : 0) + 1 + 2;  // rank, scatter; layers; the scan's two kernels
-  cudaMemcpyAsync(b.host_info, b.tile_start + nt, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(b.host_info + 1, b.sort_info, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+  sort_finish_kernel<<<1, 1, 0, s>>>(b.sort_info, b.tile_start + nt, target_blocks, min_split, b.drift + 1);
+  if (*n) fill_dead_kernel<<<blocks_for(*n), kThreads, 0, s>>>(b.cell2, b.tile_start + nt, *n);
+  b.launches += (*n ? 4 : 0) + 2 + 2;  // rank, scatter, dead fill; layers, finish; the scan's two kernels
+  const unsigned hint = b.host_info[2];  // the blocks per tile of an earlier sort
+  cudaMemcpyAsync(b.host_info, b.sort_info, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   swap_buffers(b);
-  const unsigned kept = b.host_info[0], largest = b.host_info[1], occupied = b.host_info[2];
-  unsigned splits = 1;
-  if (occupied) {
-    splits = std::max(1u, std::min((target_blocks + occupied - 1) / occupied,
-                                   (largest + min_split - 1) / min_split));
-    splits = std::min(splits, 65535u);
+  if (wait || b.sorts == 0) {
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+    if (wait) *n = b.host_info[3];
+    b.splits = (int)std::max(1u, b.host_info[2]);
+  } else {
+    b.splits = (int)std::max(1u, std::min(hint, 65535u));
   }
-  b.splits = (int)splits;
-  *n = kept;
-  b.sorted_n = kept;
+  b.sorts += 1;
+  b.sorted_n = *n;
   b.steps_since_sort = 0;
   return 0;
 }
@@ -372,8 +399,7 @@ __global__ void tile_check_kernel(TileGrid tg, SpeciesF32Buffers b, int nr, int 
 int f32_tile_check(const TileGrid& tg, unsigned target_blocks, unsigned min_split, int nr, int nz,
                    SpeciesF32Buffers& b, size_t* n, unsigned* counts, unsigned long long* misplaced,
                    cudaStream_t s) {
-  if (tile_sort(tg, target_blocks, min_split, b, n, s) != 0) return -1;
-  *b.drift_host = 0;
+  if (tile_sort(tg, target_blocks, min_split, b, n, s, true) != 0) return -1;
   cudaMemsetAsync(counts, 0, (size_t)nr * nz * sizeof(unsigned), s);
   cudaMemsetAsync(misplaced, 0, sizeof(unsigned long long), s);
   tile_check_kernel<<<(unsigned)tg.ntiles, kThreads, 0, s>>>(tg, b, nr, nz, counts, misplaced);
@@ -416,11 +442,14 @@ int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg) {
     return -1;
   if (cudaMalloc((void**)&b.layer_start, nt * (kLayerCap + 1) * sizeof(unsigned)) != cudaSuccess) return -1;
   if (cudaMalloc((void**)&b.overflow, nt * sizeof(unsigned)) != cudaSuccess) return -1;
-  if (cudaMalloc((void**)&b.sort_info, 2 * sizeof(unsigned)) != cudaSuccess) return -1;
-  if (cudaMallocHost((void**)&b.host_info, 3 * sizeof(unsigned)) != cudaSuccess) return -1;
-  if (cudaMalloc((void**)&b.drift, sizeof(unsigned)) != cudaSuccess) return -1;
-  if (cudaMallocHost((void**)&b.drift_host, sizeof(unsigned)) != cudaSuccess) return -1;
-  *b.drift_host = 0;
+  if (cudaMalloc((void**)&b.sort_info, 4 * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMallocHost((void**)&b.host_info, 4 * sizeof(unsigned)) != cudaSuccess) return -1;
+  b.host_info[0] = b.host_info[1] = b.host_info[3] = 0;
+  b.host_info[2] = 1;
+  if (cudaMalloc((void**)&b.drift, 2 * sizeof(unsigned)) != cudaSuccess) return -1;
+  if (cudaMallocHost((void**)&b.drift_host, 2 * sizeof(unsigned)) != cudaSuccess) return -1;
+  cudaMemset(b.drift, 0, 2 * sizeof(unsigned));
+  b.drift_host[0] = b.drift_host[1] = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, b.scan_tmp_bytes, b.tile_cursor, b.tile_start, (int)(nt + 1));
   if (cudaMalloc(&b.scan_tmp, std::max<size_t>(b.scan_tmp_bytes, 16)) != cudaSuccess) return -1;
   return 0;
@@ -468,12 +497,13 @@ void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_
 int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
                      double mass, int is_beam, cudaStream_t s) {
   if (*n == 0) return 0;
-  const size_t drifted = *(volatile unsigned*)b.drift_host;  // a recent step's count (a hint)
+  // a recent step's count (a hint), if that step came after the last sort
+  const volatile unsigned* dh = b.drift_host;
+  const size_t drifted = dh[1] == (unsigned)b.sorts ? dh[0] : 0;
   if (b.sorted_n == 0 || b.steps_since_sort >= st.sort_interval || (*n - b.sorted_n) * 4 > *n ||
       drifted * 100 > b.sorted_n) {
-    // synchronises: no copy of drift is pending
-    if (tile_sort(st.tiles, st.target_blocks, st.min_split, b, n, s) != 0) return -1;
-    *b.drift_host = 0;
+    // waits for nothing (the first sort of a species excepted)
+    if (tile_sort(st.tiles, st.target_blocks, st.min_split, b, n, s, false) != 0) return -1;
   }
   cudaMemsetAsync(b.drift, 0, sizeof(unsigned), s);
   const f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
@@ -505,7 +535,7 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
       f32::step_flat_kernel<0><<<nb, f32::kThreads, 0, s>>>(a, b, b.sorted_n, *n);
   }
   b.launches += (b.sorted_n ? 1 : 0) + (*n > b.sorted_n ? 1 : 0);
-  cudaMemcpyAsync(b.drift_host, b.drift, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(b.drift_host, b.drift, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   b.steps_since_sort += 1;
   return 0;
 }

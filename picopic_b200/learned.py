@@ -56,12 +56,12 @@ class Sampling:
 
     @classmethod
     def wide(cls):
-        """The states of the wide model: down to 8 macroparticles per cell
+        """The states of the wide model: down to 2 macroparticles per cell
         and 1e16 m^-3 (collision numbers down to ~1e-7 per step), with the
         drift, anisotropy and density-ratio spread that few particles per
         cell show."""
         return cls(ti=(0.05, 2.0), density=(1e16, 1e21), e_aniso=0.8, i_aniso=0.6, drift=0.6,
-                   ppc=(8, 200), ion_density=1.0)
+                   ppc=(2, 200), ion_density=1.0)
 
 
 class _Spec:
