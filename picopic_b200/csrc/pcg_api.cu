@@ -465,6 +465,10 @@ int run_stage(pcg_handle* h, int stage) {
 }
 
 // One fused step (PiCoPiC.cpp:326-347).
+// The collision list of a species: ions ("ions" or "Ions"), electrons every
+// other species (collisions.cpp:87-108).
+bool is_ion_list(const Species& s) { return s.name == "ions" || s.name == "Ions"; }
+
 // The species as the collision passes see them, and the masses and charges
 // of the species named electrons and ions (collisions.cpp:28-48: the last
 // match wins).  False when either is missing.
@@ -477,7 +481,7 @@ bool collision_species(pcg_handle* h, std::vector<CollSpecies>& v, CollParams& p
     if (s.name == "ions" || s.name == "Ions") ion = (int)t;
     CollSpecies& c = v[t];
     c.n = s.n;
-    c.is_ion = s.name == "ions" || s.name == "Ions";
+    c.is_ion = is_ion_list(s);
     if (is_f64(h)) {
       c.r = s.r; c.z = s.z; c.vr64 = s.vr; c.vphi64 = s.vphi; c.vz64 = s.vz; c.w64 = s.w;
     } else {
@@ -525,7 +529,9 @@ int run_collide(pcg_handle* h, unsigned long long* pair_calls) {
 }
 
 // One learned collision step with the binary fallback (no status check).
-int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells) {
+// In a fused float step (in_step) the move applies the transforms.
+int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells,
+                        bool in_step = false) {
   if (!h->learned.model) return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
   if (h->sp.size() > (size_t)kCollMaxSpecies) return fail(h, PCG_ERR_UNSUPPORTED, "too many species for collisions");
   CollParams p{};
@@ -533,7 +539,8 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (!collision_species(h, v, p))
     return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
   unsigned long long counts[2] = {0, 0};
-  const int lr = learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream);
+  const int lr = learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream,
+                              !in_step);
   if (lr == kLearnedTimeout) {
     h->halted = true;
     return fail(h, PCG_ERR_TIMEOUT, "learned collision step: a tensor-core wait timed out; the handle is halted");
@@ -557,7 +564,7 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
 // The collision operator of pcg_step, between the push and the move.
 int step_collide(pcg_handle* h) {
   if (h->collisions == PCG_COLLISIONS_BINARY) return run_collide(h, nullptr);
-  if (h->collisions == PCG_COLLISIONS_LEARNED) return run_collide_learned(h, nullptr, nullptr);
+  if (h->collisions == PCG_COLLISIONS_LEARNED) return run_collide_learned(h, nullptr, nullptr, !is_f64(h));
   return PCG_OK;
 }
 
@@ -626,6 +633,7 @@ int fused_step(pcg_handle* h) {
     st.sort_interval = h->sort_interval;
     st.target_blocks = h->target_blocks;
     st.min_split = h->min_split;
+    const bool learned = h->collisions == PCG_COLLISIONS_LEARNED;
     if (collide) {
       {
         TimerScope ts(h, PCG_TIMER_PARTICLES);
@@ -638,13 +646,18 @@ int fused_step(pcg_handle* h) {
       }
       if ((rc = step_collide(h)) != PCG_OK) return rc;
       st.pushed = 1;
+      if (learned) {  // the move applies the learned transforms
+        st.xform = h->learned.xform;
+        st.xflag = h->learned.flag;
+      }
     }
     TimerScope ts(h, PCG_TIMER_PARTICLES);
     for (size_t t = 0; t < h->sp.size(); ++t) {
       Species& s = h->sp[t];
       const size_t n0 = s.n;
       const uint64_t k0 = s.f32.launches;
-      if (f32_step_species(st, s.f32, &s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream) != 0)
+      if (f32_step_species(st, s.f32, &s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream,
+                           is_ion_list(s) ? 6 : 0) != 0)
         return fail(h, PCG_ERR_CUDA, "tile sort of species '" + s.name + "' failed");
       h->dead_dropped += n0 - s.n;  // a sort drops the species' dead slots
       h->launches += s.f32.launches - k0;

@@ -88,6 +88,10 @@ struct F32Step {
   // the velocities were pushed by f32_push_species already (collisions act
   // between the push and the move): the step moves and deposits only
   int pushed = 0;
+  // with pushed, the learned collision transforms to apply before the move
+  // (12 doubles and a flag per cell; see f32_step_species)
+  const double* xform = nullptr;
+  const unsigned char* xflag = nullptr;
 };
 
 __host__ __device__ __forceinline__ int pack_cell(int ci, int ck) {
@@ -116,8 +120,9 @@ void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_
 // particles).  Sorts when the species has no tile grouping, when appended
 // particles exceed 1/4 of the slots, when more than 1 % of the particles
 // left their tile's windows in a recent step, or after `sort_interval` steps.
+// xoff: the species' half of the learned transforms (0 electron list, 6 ions).
 int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
-                     double mass, int is_beam, cudaStream_t s);
+                     double mass, int is_beam, cudaStream_t s, int xoff = 0);
 // The push alone of a species' particles (fields from the global grid),
 // for a step with collisions between the push and the move.
 void f32_push_species(const F32Step& st, SpeciesF32Buffers& b, size_t n, double charge, double mass,

@@ -39,6 +39,12 @@ struct StepArgs {
   float zz_vol;                // 1/(PI dz dr^2)
   int pusher, current, fixed, is_beam;
   int pushed;  // the velocities were pushed by push_flat_kernel (a step with collisions)
+  // with pushed: the learned collision step's per-cell transforms, applied
+  // to a particle before its move when its cell's flag is 1 (v' = u + (v -
+  // u) s per axis, u = xform[12 c + xoff ..], s = xform[12 c + xoff + 3 ..])
+  const double* xform;
+  const unsigned char* xflag;
+  int xoff;
   // per radial node i (row i + 2): {1/(2i+1), 1/(2i+2), 1/(2i+3), 1/(2i+4)},
   // {1/i, 1/(i+1), 1/(i+1/2), 0}; a zero where the denominator is zero
   const float4* rt;
@@ -611,6 +617,13 @@ __device__ __forceinline__ bool advance_one(const StepArgs& a, const SpeciesF32B
   const float fr0 = p.fr, fz0 = p.fz;
   float v[3] = {p.vr, p.vphi, p.vz};
   if (!a.pushed && !push(a, e, bb, v)) return false;
+  if (a.pushed && a.xform && ci0 >= 0 && ck0 >= 0 && ci0 < a.nr && ck0 < a.nz) {
+    const size_t c = (size_t)ci0 * a.nz + ck0;
+    if (a.xflag[c] == 1) {  // the learned collision step's transform of the cell
+      const double* t = a.xform + c * 12 + a.xoff;
+      for (int q = 0; q < 3; ++q) v[q] = (float)(t[q] + ((double)v[q] - t[q]) * t[3 + q]);
+    }
+  }
   // mover_cylindrical + back_position_to_rz: x' = sqrt((x+dx)^2 + dy^2),
   // taken as dx + dy^2/(X + x') to keep the displacement's precision.
   const float dx = v[0] * a.dt_dr, dyp = v[1] * a.dt_dr, dzz = v[2] * a.dt_dz;
@@ -923,6 +936,9 @@ inline f32::StepArgs f32_step_args(const F32Step& st, double charge, double mass
   a.zz_vol = (float)(charge / (kPi * g.dz * g.dr * g.dr));
   a.pusher = st.pusher; a.current = st.current; a.fixed = st.fixed; a.is_beam = is_beam;
   a.pushed = st.pushed;
+  a.xform = st.pushed ? st.xform : nullptr;
+  a.xflag = st.xflag;
+  a.xoff = 0;
   a.rt = st.recip;
   a.st = st.status;
   return a;

@@ -495,7 +495,7 @@ void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_
 }
 
 int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double charge,
-                     double mass, int is_beam, cudaStream_t s) {
+                     double mass, int is_beam, cudaStream_t s, int xoff) {
   if (*n == 0) return 0;
   // a recent step's count (a hint), if that step came after the last sort
   const volatile unsigned* dh = b.drift_host;
@@ -506,7 +506,8 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
     if (tile_sort(st.tiles, st.target_blocks, st.min_split, b, n, s, false) != 0) return -1;
   }
   cudaMemsetAsync(b.drift, 0, sizeof(unsigned), s);
-  const f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
+  f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
+  a.xoff = xoff;
   const TileGrid& tg = st.tiles;
   if (b.sorted_n) {
     const size_t smem = f32::kTileSmemBytes;

@@ -34,6 +34,7 @@
 #include "pcg_learned.h"
 #include "pcg_mlp.cuh"
 #include "pcg_mlp_tc.cuh"
+#include "pcg_tile_walk.cuh"
 
 namespace pcg {
 
@@ -106,44 +107,36 @@ __global__ void moments_kernel(GridGeom g, CollSpecies sp, double* mom, size_t j
 
 constexpr int kWalk = 4;  // layers a tile walk loads at once
 
-// Slot of the q-th particle (q < kLayerCap) that the last tile sort put in
-// cell lc of tile t (tile-relative: the tile's first slot is 0).
-__device__ __forceinline__ unsigned layer_slot(const CollSpecies& sp, const unsigned* ls, int t, unsigned q, int lc) {
-  const size_t at = ((size_t)t * kLayerCap + q) * kTileWords + (lc >> 5);
-  return ls[q] + sp.layer_prefix[at] + __popc(sp.layer_mask[at] & ((1u << (lc & 31)) - 1u));
-}
-
-// The same sums for the tile-sorted slots [0, sp.sorted) of a float species.
-// A block of kTileCells threads takes a tile at a time and thread lc the
-// tile's cell lc: it walks the particles the sort put in its cell, layer by
-// layer (a layer's particles are contiguous and in cell order, so the
-// block's loads coalesce), sums in registers and adds the sums to the grid
-// with one atomic per word.  A particle that has left its cell since the
-// sort, and the run of particles beyond kLayerCap layers, add to the grid
-// directly.  The sums equal moments_kernel's up to the order of the FP64
-// additions.
+// The same sums for the tile-sorted slots of a float species, a block per
+// tile and a thread per tile cell (pcg_tile_walk.cuh): thread lc walks the
+// particles the last sort put in its cell, kWalk layers at a time, sums in
+// registers and adds the sums to the grid with one atomic per word.  A
+// particle that has left its cell since the sort, and the run beyond
+// kLayerCap layers, add to the grid directly.  The sums equal
+// moments_kernel's up to the order of the FP64 additions.
 __global__ void __launch_bounds__(kTileCells) tile_moments_kernel(GridGeom g, TileGrid tg, CollSpecies sp,
                                                                   double* mom) {
-  __shared__ unsigned ls[kLayerCap + 1];
+  __shared__ TileWalk tw;
   const int off = sp.is_ion ? 8 : 0, lc = threadIdx.x;
   for (int t = blockIdx.x; t < tg.ntiles; t += gridDim.x) {
     const size_t base = sp.tile_start[t], end = sp.tile_start[t + 1];
     if (base >= end) continue;  // the same for every thread of the block
-    __syncthreads();            // the previous tile's layer starts are read
-    for (int q = threadIdx.x; q <= kLayerCap; q += blockDim.x) ls[q] = sp.layer_start[(size_t)t * (kLayerCap + 1) + q];
-    __syncthreads();
+    const unsigned cnt = sp.cell_count[(size_t)t * kTileCells + lc];
+    tile_walk_begin(tw, sp.layer_start, sp.layer_prefix, t, cnt);
     const int ti = t / tg.ntz, tk = t - ti * tg.ntz;
     const int ci = ti * tg.tr + lc / tg.tz, ck = tk * tg.tz + lc % tg.tz;
     const size_t mine = (size_t)ci * g.nz + ck;
-    const unsigned nq = min(sp.cell_count[(size_t)t * kTileCells + lc], (unsigned)kLayerCap);
+    const unsigned my_n = min(cnt, (unsigned)kLayerCap), wn = tile_walk_layers(cnt);
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    // kWalk layers at a time: their loads are independent and overlap
-    for (unsigned q0 = 0; q0 < nq; q0 += kWalk) {
+    for (unsigned q0 = 0; q0 < wn; q0 += kWalk) {
       size_t j[kWalk];
       int cell[kWalk];
       float vr[kWalk], vp[kWalk], vz[kWalk], ww[kWalk];
 #pragma unroll
-      for (int u = 0; u < kWalk; ++u) j[u] = q0 + u < nq ? base + layer_slot(sp, ls, t, q0 + u, lc) : ~(size_t)0;
+      for (int u = 0; u < kWalk; ++u) {
+        const unsigned bal = __ballot_sync(0xffffffffu, my_n > q0 + u);
+        j[u] = my_n > q0 + u ? base + tile_walk_slot(tw, q0 + u, bal) : ~(size_t)0;
+      }
 #pragma unroll
       for (int u = 0; u < kWalk; ++u) {
         cell[u] = j[u] != ~(size_t)0 ? sp.cell[j[u]] : kDeadCell;
@@ -165,7 +158,7 @@ __global__ void __launch_bounds__(kTileCells) tile_moments_kernel(GridGeom g, Ti
         }
       }
     }
-    for (size_t j = base + ls[kLayerCap] + threadIdx.x; j < end; j += blockDim.x) {
+    for (size_t j = base + tw.ls[kLayerCap] + threadIdx.x; j < end; j += blockDim.x) {
       size_t c;
       double v[3];
       if (!slot_of(g, sp, j, &c, v)) continue;
@@ -365,29 +358,31 @@ __global__ void __launch_bounds__(kTileCells) tile_transform_kernel(GridGeom g, 
                                                                     const double* xform,
                                                                     const unsigned char* flag,
                                                                     const unsigned long long* count) {
-  __shared__ unsigned ls[kLayerCap + 1];
+  __shared__ TileWalk tw;
   if (count[2]) return;
   const int off = sp.is_ion ? 6 : 0, lc = threadIdx.x;
   for (int t = blockIdx.x; t < tg.ntiles; t += gridDim.x) {
     const size_t base = sp.tile_start[t], end = sp.tile_start[t + 1];
     if (base >= end) continue;  // the same for every thread of the block
-    __syncthreads();
-    for (int q = threadIdx.x; q <= kLayerCap; q += blockDim.x) ls[q] = sp.layer_start[(size_t)t * (kLayerCap + 1) + q];
-    __syncthreads();
+    const unsigned cnt = sp.cell_count[(size_t)t * kTileCells + lc];
+    tile_walk_begin(tw, sp.layer_start, sp.layer_prefix, t, cnt);
     const int ti = t / tg.ntz, tk = t - ti * tg.ntz;
     const int ci = ti * tg.tr + lc / tg.tz, ck = tk * tg.tz + lc % tg.tz;
     const size_t mine = (size_t)ci * g.nz + ck;
-    const unsigned nq = min(sp.cell_count[(size_t)t * kTileCells + lc], (unsigned)kLayerCap);
+    const unsigned my_n = min(cnt, (unsigned)kLayerCap), wn = tile_walk_layers(cnt);
     double my_tr[6];
-    const bool my_on = nq > 0 && flag[mine] == 1;
+    const bool my_on = my_n > 0 && flag[mine] == 1;
     if (my_on)
       for (int k = 0; k < 6; ++k) my_tr[k] = xform[mine * 12 + off + k];
-    for (unsigned q0 = 0; q0 < nq; q0 += kWalk) {
+    for (unsigned q0 = 0; q0 < wn; q0 += kWalk) {
       size_t j[kWalk];
       int cell[kWalk];
       float vr[kWalk], vp[kWalk], vz[kWalk];
 #pragma unroll
-      for (int u = 0; u < kWalk; ++u) j[u] = q0 + u < nq ? base + layer_slot(sp, ls, t, q0 + u, lc) : ~(size_t)0;
+      for (int u = 0; u < kWalk; ++u) {
+        const unsigned bal = __ballot_sync(0xffffffffu, my_n > q0 + u);
+        j[u] = my_n > q0 + u ? base + tile_walk_slot(tw, q0 + u, bal) : ~(size_t)0;
+      }
 #pragma unroll
       for (int u = 0; u < kWalk; ++u) {
         cell[u] = j[u] != ~(size_t)0 ? sp.cell[j[u]] : kDeadCell;
@@ -409,7 +404,7 @@ __global__ void __launch_bounds__(kTileCells) tile_transform_kernel(GridGeom g, 
         }
       }
     }
-    for (size_t j = base + ls[kLayerCap] + threadIdx.x; j < end; j += blockDim.x) {
+    for (size_t j = base + tw.ls[kLayerCap] + threadIdx.x; j < end; j += blockDim.x) {
       size_t c;
       double v[3];
       if (!slot_of(g, sp, j, &c, v) || flag[c] != 1) continue;
@@ -475,7 +470,7 @@ int learned_features(const GridGeom& g, const CollSpecies* sp, int nsp, const Le
 }
 
 int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const LearnedPhys& ph, LearnedWork& w,
-                 unsigned long long counts[2], cudaStream_t s) {
+                 unsigned long long counts[2], cudaStream_t s, bool apply) {
   if (!w.model) return -1;
   if (learned_moments(g, sp, nsp, w, s)) return -1;
   const size_t smem = sizeof(LearnSmem) + 1024;
@@ -493,7 +488,7 @@ int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const Learne
   ++w.launches;
   const TileGrid tg = f32_tile_grid(g);
   const unsigned tile_blocks = tile_grid_blocks(tg);
-  for (int t = 0; t < nsp; ++t) {
+  for (int t = 0; apply && t < nsp; ++t) {
     const size_t j0 = tiled(sp[t]) ? sp[t].sorted : 0;
     if (j0) tile_transform_kernel<<<tile_blocks, kTileCells, 0, s>>>(g, tg, sp[t], w.xform, w.flag, w.count);
     if (sp[t].n > j0)

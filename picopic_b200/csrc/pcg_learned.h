@@ -55,9 +55,11 @@ int learned_features(const GridGeom& g, const CollSpecies* sp, int nsp, const Le
 // Returns 0, -1 on a CUDA error, or kLearnedTimeout when a wait for the
 // tensor cores timed out (no velocity changed; the kernel's TMEM may still
 // be held, so the caller stops using the device work of this handle).
+// Without apply the transforms stay in w.xform and w.flag for the caller
+// to apply (the float step applies them in its move).
 constexpr int kLearnedTimeout = 1;
 int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const LearnedPhys& ph, LearnedWork& w,
-                 unsigned long long counts[2], cudaStream_t s);
+                 unsigned long long counts[2], cudaStream_t s, bool apply = true);
 int learned_set_model(LearnedWork& w, const float* params_host, const float* norm_host, cudaStream_t s);
 void learned_free(LearnedWork& w);
 

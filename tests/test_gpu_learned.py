@@ -234,6 +234,31 @@ def test_float_layout_moments_by_tile():
     assert (np.abs(m - h) <= 1e-12 * scale).all()
 
 
+def test_fused_learned_step_matches_collide_then_step():
+    """A float step with learned collisions sums the cell moments in its push
+    and applies the transforms in its move.  In the first step of a fresh
+    domain the fields are zero and the push only rounds, so the step equals
+    a learned collision pass (moments, network, transform in their own
+    kernels) followed by a collisionless step, to float rounding."""
+    from picopic_b200 import learned as L
+    g = _grid()
+    out = []
+    for fused in (True, False):
+        d = _random_domain(g, seed=6, precision="f32")
+        d.set_collision_model(*L.load_model())
+        if fused:
+            d.set_collisions("learned")
+        else:
+            learned, _ = d.collide_learned()
+            assert learned > 0.9 * g.nr * g.nz
+        d.step(1)
+        out.append([d.get_particles(s) for s in (0, 1)])
+    for a, b in zip(*out):
+        for k in ("r", "z", "vr", "vphi", "vz", "w"):
+            scale = np.abs(b[k]).max()
+            assert np.abs(a[k] - b[k]).max() <= 1e-5 * scale, k
+
+
 def test_fallback_collides_every_fallback_cell():
     """Reference quirks: the binary pass stops a row at its first empty
     cell (collisionsP12.cpp:351-354).  The fallback pass of a learned step
