@@ -333,14 +333,11 @@ LARGE = dict(
     beam_ppc=100, pusher="vay", current="zigzag")
 
 
-def run_large(args, local, barrier, allmax, allsum):
-    """The large configuration in the float path: particle-steps/s of the
-    collisionless step, then the step with the learned collision operator
-    (the wide model; binary fallback for cells outside its training box,
-    the bunch's among them) opening it."""
-    import torch
+def _large_leg(w, args, local, barrier, allmax, allsum):
+    """One large-grid leg: particle-steps/s of the collisionless step, then
+    the step with the learned collision operator (the wide model; binary
+    fallback for cells outside its training box) between push and move."""
     from picopic_b200 import learned as L
-    w = LARGE if not args.small else scaled(LARGE, nz=2048)
     d, _, _, _ = make_domain(w, "f32", seed=4321, device=local)
     d.step(3)
     d.synchronize()
@@ -353,19 +350,30 @@ def run_large(args, local, barrier, allmax, allsum):
            "pusher": w["pusher"], "current": w["current"], "precision": "f32",
            "value": allsum(float(dg.particle_steps - p0)) / (ms * 1e-3), "unit": UNIT,
            "ms_per_step": ms / k, "steps": k}
-    d.set_collision_model(*L.load_model(L.WIDE_MODEL_PATH))  # 12 ppc, n 1e18: the wide model's states
+    d.set_collision_model(*L.load_model(L.WIDE_MODEL_PATH))  # few per cell, n 1e18: the wide model's states
     learned, fallback = d.collide_learned()
     d.set_collisions("learned")
     d.step(1)
     d.synchronize()
-    kc = 3
+    kc = 10
     barrier()
     ms_c = allmax(timed_steps(d, kc, d.stream))
     cells = w["nr"] * w["nz"]
     out["with_learned_collisions"] = {"ms_per_step": ms_c / kc, "steps": kc,
                                       "learned_cell_fraction": learned / cells,
                                       "fallback_cell_fraction": fallback / cells}
-    del d
+    d.close()
+    return out
+
+
+def run_large(args, local, barrier, allmax, allsum):
+    """The large configuration in the float path at 12 macroparticles per
+    cell per species (4e8 particles), and at 6 (2e8)."""
+    import torch
+    w = LARGE if not args.small else scaled(LARGE, nz=2048)
+    out = _large_leg(w, args, local, barrier, allmax, allsum)
+    w6 = dict(w, ppc=6, name=w["name"].replace("12 ppc", "6 ppc"))
+    out["ppc6"] = _large_leg(w6, args, local, barrier, allmax, allsum)
     torch.cuda.empty_cache()
     return out
 

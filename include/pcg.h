@@ -274,6 +274,29 @@ int pcg_collide(pcg_handle* h, unsigned long long* pair_calls);
 #define PCG_COLLIDE_SK98 2
 int pcg_set_collision_scheme(pcg_handle* h, int scheme);
 
+/* External fields: ExternalFields (src/maxwellSolver/externalFields.cpp),
+ * whose E and H the pushers gather at each particle and add to the field
+ * solver's (pusherBoris.cpp:62-65, pusherVay.cpp:48-50, pusherHC.cpp:51-54), set
+ * after the H update of every step (SMB.cpp:1253-1262) and constant in time.
+ * The reference builds it only with ENABLE_EXTERNAL_FIELDS (configure.ac:
+ * 215-222, a development option); without this call there are none.
+ * `electric` and `magnetic` are the formfactor names of PiCoPiC.json's
+ * external_fields section (cfg.cpp:454-487): "none", "const_r",
+ * "const_phi", "const_z", "linerad_r", "linerad_z"; params[0] is the
+ * amplitude (V/m, A/m).  The fields live on the cells 1 <= i < nr-1,
+ * 1 <= k < nz-1 (the wall rows and the halo stay 0, externalFields.cpp:
+ * 298-348).  PCG_QUIRKS_REFERENCE: the electric name test
+ * (externalFields.cpp:51-62) maps every name but "none" to "none" and
+ * "none" to "const_r", and neither sets a field, so no electric field
+ * applies; of the magnetic names only "const_z" sets one, H_z = params[0];
+ * an unknown magnetic name is PCG_ERR_ARG (the reference's FATAL).
+ * PCG_QUIRKS_FIXED: "const_r", "const_phi" and "const_z" of either field
+ * set that component to params[0]; "linerad_*", whose parameters the
+ * reference leaves undefined, is PCG_ERR_UNSUPPORTED.  NULL or "none" for
+ * both removes the fields. */
+int pcg_set_external_fields(pcg_handle* h, const char* electric, const double* e_params, int n_e,
+                            const char* magnetic, const double* m_params, int n_m);
+
 /* Work split of the binary pass (no counterpart in the reference, which
  * runs every cell's pairing sequence in turn): cells holding more than
  * `threshold` particles (256 by default) run their sequence on a warp, the
@@ -348,7 +371,7 @@ int pcg_cell_moments(pcg_handle* h, double* moments);
 int pcg_cell_features(pcg_handle* h, float* features, double* scale);
 
 /* Tiling of the float step (no reference counterpart: its particles are not
- * tiled).  Species are re-sorted into 8 x 64-cell tiles at most every
+ * tiled).  Species are re-sorted into 8 x 32-cell tiles at most every
  * sort_interval steps (default 64; sooner when particles drift out of their
  * tile's windows), and a sort spreads each occupied tile over enough blocks
  * that about target_blocks blocks run (default 148 x 16), each with at least

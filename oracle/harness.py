@@ -83,12 +83,13 @@ def build_reference(root: str | None = None, jobs: int = 8) -> bool:
     return True
 
 
-def reference_available(pusher: str = "borisrel", current: str = "vb", perf: bool = False) -> bool:
-    return os.path.exists(_ref_path(pusher, current, perf))
+def reference_available(pusher: str = "borisrel", current: str = "vb", perf: bool = False,
+                        extf: bool = False) -> bool:
+    return os.path.exists(_ref_path(pusher, current, perf, extf))
 
 
-def _ref_path(pusher: str, current: str, perf: bool = False) -> str:
-    tag = "perf_" if perf else ""
+def _ref_path(pusher: str, current: str, perf: bool = False, extf: bool = False) -> str:
+    tag = "perf_" if perf else "extf_" if extf else ""
     return os.path.join(REF_DIR, f"libpicopic_ref_{tag}{pusher}_{current}.so")
 
 
@@ -235,6 +236,17 @@ class _Sim:
         assert rc == 0, f"species_map rc {rc}"
         return out if k == 3 else out[0]
 
+    def set_external_fields(self, electric="none", e_params=(), magnetic="none", m_params=()) -> int:
+        """ExternalFields' formfactors and params (externalFields.cpp); the
+        reference library must be the ENABLE_EXTERNAL_FIELDS build (extf)."""
+        f = self._fn("set_external_fields")
+        f.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _PD, ctypes.c_int, ctypes.c_char_p, _PD, ctypes.c_int]
+        f.restype = ctypes.c_int
+        ep = np.ascontiguousarray(e_params, dtype=np.float64).reshape(-1)
+        mp = np.ascontiguousarray(m_params, dtype=np.float64).reshape(-1)
+        return int(f(self.h, electric.encode(), _dp(ep) if ep.size else None, ep.size,
+                     magnetic.encode(), _dp(mp) if mp.size else None, mp.size))
+
     def stage(self, name) -> int:
         idx = STAGE[name] if isinstance(name, str) else name
         return self._fn("stage")(self.h, idx)
@@ -324,8 +336,8 @@ class RefSim(_Sim):
     prefix = "ref_"
     _libs: dict = {}
 
-    def __init__(self, grid: GridSpec, pusher="borisrel", current="vb", perf=False):
-        path = _ref_path(pusher, current, perf)
+    def __init__(self, grid: GridSpec, pusher="borisrel", current="vb", perf=False, extf=False):
+        path = _ref_path(pusher, current, perf, extf)
         if path not in RefSim._libs:
             lib = ctypes.CDLL(path)
             lib.ref_create.restype = ctypes.c_void_p

@@ -59,6 +59,7 @@ struct orc_sim {
   size_t gcr, gcz; /* Geometry::global_cell_amount (geometry.hpp:70-71) */
   int pusher, current, quirks;
   double *E[3], *H[3], *Hat[3], *J[3], *sigma;
+  double *Eext[3], *Hext[3]; /* ExternalFields' field_e, field_h (NULL: none) */
   int nsp;
   species_t sp[MAX_SPECIES];
   int rng_kind;
@@ -315,9 +316,9 @@ static inline double term(double f, double dzz, double ra, double rb, double vol
     if ((s)->quirks == ORC_QUIRKS_FIXED) (a) = (b) = cloud;                \
   } while (0)
 
-static void gather_h(const orc_sim* s, double radius, double longitude, double cmp[3]) {
+static void gather_h(const orc_sim* s, double* const H[3], double radius, double longitude, double cmp[3]) {
   const double dr = s->dr, dz = s->dz;
-  const double *Hr = s->H[0], *Hp = s->H[1], *Hz = s->H[2];
+  const double *Hr = H[0], *Hp = H[1], *Hz = H[2];
   double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr, r2, dz1, dz2, v1, v2;
   const double cloud = K_PI * dz * (r3 * r3 - r1 * r1);
   int i, k;
@@ -363,9 +364,9 @@ static void gather_h(const orc_sim* s, double radius, double longitude, double c
   cmp[1] += term(Hp[IDX(s, i + 1, k + 1)], dz2, r2, r3, v2);
 }
 
-static void gather_e(const orc_sim* s, double radius, double longitude, double cmp[3]) {
+static void gather_e(const orc_sim* s, double* const E[3], double radius, double longitude, double cmp[3]) {
   const double dr = s->dr, dz = s->dz;
-  const double *Er = s->E[0], *Ep = s->E[1], *Ez = s->E[2];
+  const double *Er = E[0], *Ep = E[1], *Ez = E[2];
   double r1 = radius - 0.5 * dr, r3 = radius + 0.5 * dr, r2, dz1, dz2, v1, v2;
   const double cloud = K_PI * dz * (r3 * r3 - r1 * r1);
   int i, k;
@@ -1378,8 +1379,17 @@ int orc_stage(orc_sim* s, int stage) {
           double pr = p->r[j], pz = p->z[j], e[3], b[3];
           double v[3] = {p->vr[j], p->vphi[j], p->vz[j]};
           if (isnan(pr) || isinf(pr) || isnan(pz) || isinf(pz)) return ST_FATAL; /* :51-57 */
-          gather_e(s, pr, pz, e);
-          gather_h(s, pr, pz, b);
+          gather_e(s, s->E, pr, pz, e);
+          gather_h(s, s->H, pr, pz, b);
+          if (s->Eext[0]) { /* e += external_fields->get_field_e(pos_r, pos_z), pusherBoris.cpp:62-65 */
+            double ex[3], bx[3];
+            gather_e(s, s->Eext, pr, pz, ex);
+            gather_h(s, s->Hext, pr, pz, bx);
+            for (int c = 0; c < 3; ++c) {
+              e[c] += ex[c];
+              b[c] += bx[c];
+            }
+          }
           int fixed = s->quirks == ORC_QUIRKS_FIXED;
           if (s->pusher == ORC_PUSHER_VAY) st = push_vay(fixed, p->charge, p->mass, s->dt, e, b, v);
           else if (s->pusher == ORC_PUSHER_HC) st = push_hc(fixed, p->charge, p->mass, s->dt, e, b, v);
@@ -1440,10 +1450,59 @@ double orc_time(orc_sim* s) { return s->t; }
 long orc_removed(orc_sim* s) { return s->removed; }
 long orc_error_count(orc_sim* s) { return s->errors; }
 
+/* ExternalFields (externalFields.cpp): the profile named by each formfactor
+ * (:51-79), applied after every H update (operator(), :351-436; SMB.cpp:
+ * 1253-1262) and constant, so set here once.  The reference's electric name
+ * test maps every name but "none" to code 0 and "none" to 1 (const_r), and
+ * neither sets a field; of the magnetic codes only 3 (const_z) sets one,
+ * set_magn_field_homogenous_z (:298-348): H_z = params[0] on the cells
+ * r_begin <= i < r_end, z_begin <= k < z_end, which for one domain with its
+ * four walls are 1 <= i < nr-1, 1 <= k < nz-1 (:29-47), zero elsewhere.  The
+ * fixed mode applies const_r, const_phi and const_z of both fields to the
+ * named component on the same cells; linerad_* has no defined parameters. */
+static int extf_code(const char* name) {
+  static const char* names[6] = {"none", "const_r", "const_phi", "const_z", "linerad_r", "linerad_z"};
+  if (!name) return 0;
+  for (int c = 0; c < 6; ++c)
+    if (!strcmp(name, names[c])) return c;
+  return -1;
+}
+
+int orc_set_external_fields(orc_sim* s, const char* electric, const double* e_params, int n_e,
+                            const char* magnetic, const double* m_params, int n_m) {
+  const int fixed = s->quirks == ORC_QUIRKS_FIXED;
+  int ec = extf_code(electric), mc = extf_code(magnetic);
+  if (mc < 0 || (fixed && ec < 0)) return ST_ARG;
+  if (!fixed) {
+    ec = 0;
+    if (mc != 3) mc = 0;
+  }
+  if (ec >= 4 || mc >= 4) return -13; /* PCG_ERR_UNSUPPORTED */
+  if ((ec && (!e_params || n_e < 1)) || (mc && (!m_params || n_m < 1))) return ST_ARG;
+  size_t ng = (size_t)(s->nr + 4) * (size_t)(s->nz + 4);
+  for (int c = 0; c < 3; ++c) {
+    free(s->Eext[c]); free(s->Hext[c]);
+    s->Eext[c] = s->Hext[c] = NULL;
+  }
+  if (!ec && !mc) return ST_OK;
+  for (int c = 0; c < 3; ++c) {
+    s->Eext[c] = (double*)calloc(ng, sizeof(double));
+    s->Hext[c] = (double*)calloc(ng, sizeof(double));
+  }
+  if (ec)
+    for (int i = 1; i < s->nr - 1; ++i)
+      for (int k = 1; k < s->nz - 1; ++k) s->Eext[ec - 1][IDX(s, i, k)] = e_params[0];
+  if (mc)
+    for (int i = 1; i < s->nr - 1; ++i)
+      for (int k = 1; k < s->nz - 1; ++k) s->Hext[mc - 1][IDX(s, i, k)] = m_params[0];
+  return ST_OK;
+}
+
 void orc_destroy(orc_sim* s) {
   if (!s) return;
   for (int c = 0; c < 3; ++c) {
     free(s->E[c]); free(s->H[c]); free(s->Hat[c]); free(s->J[c]);
+    free(s->Eext[c]); free(s->Hext[c]);
   }
   free(s->sigma);
   for (int t = 0; t < s->nsp; ++t) {

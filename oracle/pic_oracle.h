@@ -60,6 +60,10 @@ int orc_get_particles(orc_sim* s, int sid, size_t cap, double* r, double* z, dou
 /* which: 0-2 E(r,phi,z), 3-5 H, 6-8 H_at_et, 9-11 J, 12 sigma (read only) */
 int orc_set_field(orc_sim* s, int which, const double* src);
 int orc_get_field(orc_sim* s, int which, double* dst);
+/* ExternalFields (externalFields.cpp): formfactor names and params as
+ * pcg_set_external_fields takes them. */
+int orc_set_external_fields(orc_sim* s, const char* electric, const double* e_params, int n_e,
+                            const char* magnetic, const double* m_params, int n_m);
 int orc_stage(orc_sim* s, int stage);
 int orc_step(orc_sim* s, int nsteps);
 double orc_time(orc_sim* s);

@@ -55,6 +55,9 @@ struct RefSim {
   std::vector<SpecieP*> species;
   Domain* domain = nullptr;
   size_t removed = 0;
+  // ExternalFields' formfactors and params (the ENABLE_EXTERNAL_FIELDS build)
+  std::string e_form = "none", m_form = "none";
+  std::vector<double> e_params, m_params;
 };
 
 // CollisionsP12 with its protected steps reachable: the pass without
@@ -100,7 +103,13 @@ class SK98Pass : public CollisionsSK98 {
 };
 
 Domain* domain_of(RefSim* s) {
+#ifdef ENABLE_EXTERNAL_FIELDS
+  // SMB.cpp:164-171 passes the configuration's formfactors and params
+  if (!s->domain)
+    s->domain = new Domain(*s->geometry, s->species, &s->time, s->e_form, s->m_form, s->e_params, s->m_params);
+#else
   if (!s->domain) s->domain = new Domain(*s->geometry, s->species, &s->time);
+#endif
   return s->domain;
 }
 
@@ -143,7 +152,12 @@ int run_stage(RefSim* s, int stage) {
   switch (stage) {
     case 0: d->manage_beam(); break;                      // inject
     case 1: d->weight_field_e(); break;                   // E
-    case 2: d->weight_field_h(); break;                   // H
+    case 2:                                               // H
+      d->weight_field_h();
+#ifdef ENABLE_EXTERNAL_FIELDS
+      d->apply_external_fields();  // after the H update, SMB.cpp:1253-1262
+#endif
+      break;
     case 3: d->push_particles(); break;                   // gather + push
     case 4: d->dump_particle_positions_to_old(); break;
     case 5: d->update_particles_coords(); break;          // mover_cylindrical
@@ -183,6 +197,18 @@ void* ref_create(int nr, int nz, double radius, double longitude, double dt, dou
   s->time.end = 1e300;
   s->time.step = dt;
   return s;
+}
+
+// ExternalFields of the domain (before it is built: its constructor takes them).
+int ref_set_external_fields(void* h, const char* electric, const double* e_params, int n_e,
+                            const char* magnetic, const double* m_params, int n_m) {
+  RefSim* s = (RefSim*)h;
+  if (s->domain) return -3;
+  s->e_form = electric ? electric : "none";
+  s->m_form = magnetic ? magnetic : "none";
+  s->e_params.assign(e_params, e_params + (e_params ? n_e : 0));
+  s->m_params.assign(m_params, m_params + (m_params ? n_m : 0));
+  return 0;
 }
 
 int ref_add_species(void* h, int id, const char* name, double charge_e, double mass_e) {

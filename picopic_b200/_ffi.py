@@ -89,6 +89,8 @@ SIGNATURES = {
     "pcg_set_collisions": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_scheme": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_crowding": (ctypes.c_int, [_H, ctypes.c_uint]),
+    "pcg_set_external_fields": (ctypes.c_int, [_H, ctypes.c_char_p, _PD, ctypes.c_int, ctypes.c_char_p, _PD,
+                                               ctypes.c_int]),
     "pcg_species_map": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _PD]),
     "pcg_set_tiling": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "pcg_tile_sort": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(ctypes.c_uint),

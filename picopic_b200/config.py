@@ -21,9 +21,10 @@ reference, by design:
   <component>/[<specie>/]<shape>/<r0>-<r1>_<z0>-<z1>), frames stacked on
   the first axis, since no HDF5 library is available;
 * external fields (`external_fields`) are read and ignored, as the
-  reference's default build ignores them (configure.ac:84-85, 214-220:
-  a development-only switch); with use_external_fields=True a form factor
-  other than "none" is refused (the engine has no external fields).
+  reference's default build ignores them (configure.ac:84-85, 214-222:
+  a development-only switch); with use_external_fields=True (the
+  --external-fields switch) they are applied as the ENABLE_EXTERNAL_FIELDS
+  build applies them (Domain.set_external_fields, pcg_set_external_fields).
 """
 from __future__ import annotations
 
@@ -189,12 +190,13 @@ def build_domain(cfg: RunConfig, pusher="borisrel", current="vb", precision="f32
     weights bit for bit, its thermal velocity distribution)."""
     if plasma not in ("maxwellian", "reference"):
         raise ValueError(f"plasma initialiser {plasma!r}: 'maxwellian' or 'reference'")
-    for kind in ("electric", "magnetic"):
-        ff = cfg.external_fields.get(kind, {}).get("formfactor", "none")
-        if ff != "none" and use_external_fields:
-            raise NotImplementedError(f"external {kind} field {ff!r}: the engine has none")
     d = Domain(cfg.geometry, pusher=pusher, current=current, precision=precision, quirks=quirks, seed=seed,
                device=device)
+    if use_external_fields:  # the reference's ENABLE_EXTERNAL_FIELDS build (cfg.cpp:454-487)
+        ef = cfg.external_fields
+        e, m = ef.get("electric", {}), ef.get("magnetic", {})
+        d.set_external_fields(e.get("formfactor", "none"), e.get("params", []),
+                              m.get("formfactor", "none"), m.get("params", []))
     slots = {}
     for s in cfg.species:
         slots[s["name"]] = d.add(_Spec(s["name"], s["charge"], s["mass"], _id(s["name"])),
@@ -290,9 +292,12 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--plasma", default="maxwellian", choices=["maxwellian", "reference"],
                     help="plasma initial condition: device Maxwellian, or the reference's own")
+    ap.add_argument("--external-fields", action="store_true",
+                    help="apply the configuration's external_fields (the reference's ENABLE_EXTERNAL_FIELDS build)")
     a = ap.parse_args(argv)
     cfg = load(a.config)
-    d, slots = build_domain(cfg, a.pusher, a.current, a.precision, a.quirks, a.seed, plasma=a.plasma)
+    d, slots = build_domain(cfg, a.pusher, a.current, a.precision, a.quirks, a.seed,
+                            use_external_fields=a.external_fields, plasma=a.plasma)
     from . import h5layout
     attrs = h5layout.root_attributes(cfg.raw, a.pusher, a.current, a.precision, a.quirks, a.plasma)
     run(cfg, d, slots, a.steps, a.out or cfg.data_root, attrs=attrs)

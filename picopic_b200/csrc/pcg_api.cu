@@ -79,6 +79,12 @@ struct pcg_handle {
   int collisions = PCG_COLLISIONS_NONE;  // collision operator of every pcg_step
   int coll_scheme = PCG_COLLIDE_P12;     // binary operator of pcg_collide and binary steps
   unsigned coll_crowded = 256;           // particles above which a cell's pairs take a warp
+  // external fields (pcg_set_external_fields): E_r, E_phi, E_z, H_r, H_phi,
+  // H_z planes of nodes doubles (double path) and floats (float path), and
+  // the float step's gather planes E + E_ext, H + H_ext, f32_plane apart
+  double* ext64 = nullptr;
+  float* ext32 = nullptr;
+  float* push32 = nullptr;
   double* sig64[3] = {};          // r, z0, zl profiles
   float* sig32[3] = {};
   unsigned long long* reset = nullptr;
@@ -170,6 +176,7 @@ FieldsF64 fields64(pcg_handle* h) {
     f.E[c] = h->f64[c]; f.H[c] = h->f64[3 + c]; f.Hat[c] = h->f64[6 + c]; f.J[c] = h->f64[9 + c];
   }
   f.sig_r = h->sig64[0]; f.sig_z0 = h->sig64[1]; f.sig_zl = h->sig64[2];
+  f.ext = h->ext64;
   return f;
 }
 
@@ -623,6 +630,11 @@ int fused_step(pcg_handle* h) {
     F32Step st;
     st.g = h->g;
     for (int c = 0; c < 12; ++c) st.fld[c] = h->f32[c];
+    if (h->ext32) {  // the step gathers E + E_ext and H + H_ext
+      f32_add_planes(h->push32, h->f32[0], h->ext32, 6 * h->f32_plane, h->stream);
+      h->launches += 1;
+      for (int c = 0; c < 6; ++c) st.fld[c] = h->push32 + c * h->f32_plane;
+    }
     st.plane = (int)h->f32_plane;
     st.recip = h->recip32;
     st.pusher = h->cfg.pusher;
@@ -763,6 +775,9 @@ int pcg_destroy(pcg_handle* h) {
   collide_free(h->coll);
   learned_free(h->learned);
   for (int c = 0; c < 3; ++c) { cudaFree(h->sig64[c]); cudaFree(h->sig32[c]); }
+  cudaFree(h->ext64);
+  cudaFree(h->ext32);
+  cudaFree(h->push32);
   cudaFree(h->reset);
   cudaFree(h->scratch);
   cudaFree(h->staging);
@@ -1040,6 +1055,63 @@ int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (rc != PCG_OK) return rc;
   if ((rc = run_collide_learned(h, learned_cells, fallback_cells)) != PCG_OK) return rc;
   return check_status(h);
+}
+
+// ExternalFields (externalFields.cpp:22-95, 298-348, 351-436): the profile
+// codes 0 none, 1 const_r, 2 const_phi, 3 const_z, 4 linerad_r, 5 linerad_z.
+int extf_code(const char* name) {
+  static const char* names[6] = {"none", "const_r", "const_phi", "const_z", "linerad_r", "linerad_z"};
+  if (!name) return 0;
+  for (int c = 0; c < 6; ++c)
+    if (!strcmp(name, names[c])) return c;
+  return -1;
+}
+
+int pcg_set_external_fields(pcg_handle* h, const char* electric, const double* e_params, int n_e,
+                            const char* magnetic, const double* m_params, int n_m) {
+  if (!h) return PCG_ERR_ARG;
+  const bool fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
+  int ec = extf_code(electric), mc = extf_code(magnetic);
+  if (mc < 0) return fail(h, PCG_ERR_ARG, std::string("unknown magnetic field profile ") + magnetic);
+  if (fixed && ec < 0) return fail(h, PCG_ERR_ARG, std::string("unknown electric field profile ") + electric);
+  if (!fixed) ec = 0;  // the reference's electric name test never selects a profile that sets a field
+  if (!fixed && mc != 3) mc = 0;  // of the magnetic profiles only const_z sets one
+  if (ec >= 4 || mc >= 4) return fail(h, PCG_ERR_UNSUPPORTED, "linerad external field profiles are not defined");
+  if ((ec && (!e_params || n_e < 1)) || (mc && (!m_params || n_m < 1)))
+    return fail(h, PCG_ERR_ARG, "an external field profile needs its amplitude in params[0]");
+  int rc;
+  if (!ec && !mc) {  // no external fields
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->ext64); cudaFree(h->ext32); cudaFree(h->push32);
+    h->ext64 = nullptr; h->ext32 = nullptr; h->push32 = nullptr;
+    return PCG_OK;
+  }
+  // component c of E (0..2) or H (3..5) = amplitude on 1 <= i < nr-1, 1 <= k < nz-1
+  const size_t nodes = h->nodes;
+  std::vector<double> host(6 * nodes, 0.0);
+  const int comp[2] = {ec ? ec - 1 : -1, mc ? 3 + mc - 1 : -1};
+  const double amp[2] = {ec ? e_params[0] : 0.0, mc ? m_params[0] : 0.0};
+  for (int f = 0; f < 2; ++f) {
+    if (comp[f] < 0) continue;
+    double* plane = host.data() + (size_t)comp[f] * nodes;
+    for (int i = 1; i < h->g.nr - 1; ++i)
+      for (int k = 1; k < h->g.nz - 1; ++k) plane[(size_t)(i + 2) * h->g.ld + (k + 2)] = amp[f];
+  }
+  if (is_f64(h)) {
+    if (!h->ext64 && (rc = dalloc(h, &h->ext64, 6 * nodes)) != PCG_OK) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->ext64, host.data(), 6 * nodes * sizeof(double), cudaMemcpyHostToDevice,
+                                h->stream));
+  } else {
+    std::vector<float> hf(6 * h->f32_plane, 0.f);
+    for (int c = 0; c < 6; ++c)
+      for (size_t q = 0; q < nodes; ++q) hf[c * h->f32_plane + q] = (float)host[c * nodes + q];
+    if (!h->ext32 && (rc = dalloc(h, &h->ext32, 6 * h->f32_plane)) != PCG_OK) return rc;
+    if (!h->push32 && (rc = dalloc(h, &h->push32, 6 * h->f32_plane)) != PCG_OK) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->ext32, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));  // the host arrays go out of scope
+  return PCG_OK;
 }
 
 int pcg_set_collision_crowding(pcg_handle* h, unsigned threshold) {

@@ -111,6 +111,8 @@ int f32_tile_check(const TileGrid& tg, unsigned target_blocks, unsigned min_spli
 int f32_alloc_species(SpeciesF32Buffers& b, size_t cap, const TileGrid& tg);
 void f32_free_species(SpeciesF32Buffers& b);
 void f32_launch_yee_e(const YeeArgs<float>& a, cudaStream_t s);
+// dst[q] = a[q] + b[q], q < n (the external fields added to the step's gather planes)
+void f32_add_planes(float* dst, const float* a, const float* b, size_t n, cudaStream_t s);
 void f32_launch_yee_h(const YeeArgs<float>& a, int fixed, cudaStream_t s);
 void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsigned count,
                        const BeamInject& bi, cudaStream_t s);

@@ -426,6 +426,8 @@ __global__ void __launch_bounds__(kThreads, 4)
   a.pusher = PCG_PUSHER_BORIS_RELATIVISTIC;
   a.is_beam = 0;
   a.fixed = FIX;
+  a.pushed = 0;  // launched for whole steps only
+  a.xform = nullptr;
   extern __shared__ __align__(16) float smem[];
   const int t = blockIdx.x;
   // the tile's parts: the blocks per tile of the last sort (on the device),

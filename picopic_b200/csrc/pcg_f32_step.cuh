@@ -844,7 +844,11 @@ __global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
     step_tiled_kernel(StepArgs args, SpeciesF32Buffers b,
                                                                  TileGrid tg) {
   StepArgs a = args;
-  if (PUSH >= 0) a.pusher = PUSH;
+  if (PUSH >= 0) {  // the specialised instances run whole steps only
+    a.pusher = PUSH;
+    a.pushed = 0;
+    a.xform = nullptr;
+  }
   if (BEAM >= 0) a.is_beam = BEAM;
   if (FIX >= 0) a.fixed = FIX;
   extern __shared__ float smem[];

@@ -19,6 +19,7 @@ struct Fields {
   const double* sig_r;   // PML sigma contribution of the r=R wall, per radial cell
   const double* sig_z0;  // of the z=0 wall, per axial cell
   const double* sig_zl;  // of the z=L wall, per axial cell
+  const double* ext;     // external E (3 planes) then H (3 planes), or null
 };
 
 __device__ __forceinline__ int cell_number(double pos, double dx) {  // geometry.hpp:198
@@ -301,7 +302,29 @@ __device__ __forceinline__ bool push_hc(bool fixed, double c2m, const double e_i
   return true;
 }
 
-// Gather at (r, z) and push one particle; pusher numbering as pcg.h.
+// e += external_fields->get_field_e(pos_r, pos_z), b += ...get_field_h
+// (pusherBoris.cpp:62-65): the external planes gathered as the fields are.
+__device__ __forceinline__ void add_external(const GridGeom& g, const Fields& f, bool fixed, double r, double z,
+                                          double e[3], double b[3]) {
+  const size_t pl = (size_t)(g.nr + 4) * g.ld;
+  Fields x = f;
+  for (int c = 0; c < 3; ++c) {
+    x.E[c] = const_cast<double*>(f.ext) + c * pl;
+    x.H[c] = const_cast<double*>(f.ext) + (3 + c) * pl;
+  }
+  double ex[3], bx[3];
+  gather_e(g, x, fixed, r, z, ex);
+  gather_h(g, x, fixed, r, z, bx);
+  for (int c = 0; c < 3; ++c) {
+    e[c] += ex[c];
+    b[c] += bx[c];
+  }
+}
+
+// Gather at (r, z) and push one particle; pusher numbering as pcg.h.  EXT:
+// add the external fields (f.ext); the kernels are instantiated with and
+// without, so that runs without keep the push's registers.
+template <bool EXT = false>
 __device__ __forceinline__ bool gather_push(const GridGeom& g, const Fields& f, int pusher,
                                             bool fixed, double c2m, double r, double z,
                                             double v[3], DevStatus* st) {
@@ -318,6 +341,7 @@ __device__ __forceinline__ bool gather_push(const GridGeom& g, const Fields& f, 
   double e[3], b[3];
   gather_e(g, f, fixed, r, z, e);
   gather_h(g, f, fixed, r, z, b);
+  if (EXT) add_external(g, f, fixed, r, z, e, b);
   if (pusher == 3) return push_vay(fixed, c2m, e, b, v, st);
   if (pusher == 4) return push_hc(fixed, c2m, e, b, v, st);
   return push_boris(pusher, c2m, e, b, v, st);

@@ -22,6 +22,9 @@ struct FieldsF64 {
   const double* sig_r;
   const double* sig_z0;
   const double* sig_zl;
+  // external fields: E_r, E_phi, E_z, H_r, H_phi, H_z planes of (nr+4)(nz+4)
+  // nodes, gathered and added to E and H by the push; null when none
+  const double* ext = nullptr;
 };
 
 // One species in the double-precision layout (structure of arrays).

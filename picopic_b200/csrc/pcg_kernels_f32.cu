@@ -466,6 +466,15 @@ void f32_free_species(SpeciesF32Buffers& b) {
   b = SpeciesF32Buffers();
 }
 
+__global__ void add_planes_kernel(float* dst, const float* a, const float* b, size_t n) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    dst[q] = a[q] + b[q];
+}
+
+void f32_add_planes(float* dst, const float* a, const float* b, size_t n, cudaStream_t s) {
+  add_planes_kernel<<<(unsigned)std::min<size_t>(blocks_for(n), 148 * 16), kThreads, 0, s>>>(dst, a, b, n);
+}
+
 void f32_launch_yee_e(const YeeArgs<float>& a, cudaStream_t s) {
   dim3 grid((a.g.nz + 4 + kThreads - 1) / kThreads, a.g.nr + 4);
   yee_e_kernel<float><<<grid, kThreads, 0, s>>>(a);

@@ -23,6 +23,7 @@ __host__ __device__ inline Fields make_fields(const FieldsF64& d) {
     f.E[c] = d.E[c]; f.H[c] = d.H[c]; f.Hat[c] = d.Hat[c]; f.J[c] = d.J[c];
   }
   f.sig_r = d.sig_r; f.sig_z0 = d.sig_z0; f.sig_zl = d.sig_zl;
+  f.ext = d.ext;
   return f;
 }
 
@@ -31,6 +32,7 @@ inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kT
 // ---------------------------------------------------------------------------
 // Stage kernels (one per Domain method)
 
+template <bool EXT>
 __global__ void push_kernel(GridGeom g, FieldsF64 fd, SpeciesF64 sp, int pusher, int fixed,
                             DevStatus* st) {
   size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -38,7 +40,7 @@ __global__ void push_kernel(GridGeom g, FieldsF64 fd, SpeciesF64 sp, int pusher,
   if (sp.r[j] < 0) return;  // dead slot
   Fields f = make_fields(fd);
   double v[3] = {sp.vr[j], sp.vphi[j], sp.vz[j]};
-  if (!gather_push(g, f, pusher, fixed, sp.c2m, sp.r[j], sp.z[j], v, st)) return;
+  if (!gather_push<EXT>(g, f, pusher, fixed, sp.c2m, sp.r[j], sp.z[j], v, st)) return;
   sp.vr[j] = v[0]; sp.vphi[j] = v[1]; sp.vz[j] = v[2];
 }
 
@@ -172,6 +174,7 @@ __global__ void zigzag_kernel(GridGeom g, FieldsF64 fd, SpeciesF64 sp) {
 // strict-axial J_r overwrites.  Without do_push the velocities are taken as
 // pushed already (the step of a run with collisions, which act between the
 // push and the move).
+template <bool EXT>
 __global__ void __launch_bounds__(kThreads) advance_kernel(GridGeom g, FieldsF64 fd, SpeciesF64 sp,
                                                            int slot, int pusher, int fixed,
                                                            int current, unsigned long long* reset,
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) advance_kernel(GridGeom g, FieldsF64
   double z = sp.z[j];
   Fields f = make_fields(fd);
   double v[3] = {sp.vr[j], sp.vphi[j], sp.vz[j]};
-  if (do_push && !gather_push(g, f, pusher, fixed, sp.c2m, r, z, v, st)) return;
+  if (do_push && !gather_push<EXT>(g, f, pusher, fixed, sp.c2m, r, z, v, st)) return;
   const double r_old = r, z_old = z;                 // dump_position_to_old (phi = 0)
   const double X = r + v[0] * g.dt;                  // mover_cylindrical
   const double Y = 0 + v[1] * g.dt;
@@ -300,7 +303,10 @@ void launch_stage_f64(int stage, const GridGeom& g, const FieldsF64& f, const Sp
   if (sp.n == 0) return;
   unsigned nb = blocks_for(sp.n);
   switch (stage) {
-    case 3: push_kernel<<<nb, kThreads, 0, s>>>(g, f, sp, pusher, fixed, st); break;
+    case 3:
+      if (f.ext) push_kernel<true><<<nb, kThreads, 0, s>>>(g, f, sp, pusher, fixed, st);
+      else push_kernel<false><<<nb, kThreads, 0, s>>>(g, f, sp, pusher, fixed, st);
+      break;
     case 4: dump_old_kernel<<<nb, kThreads, 0, s>>>(sp); break;
     case 5: move_kernel<<<nb, kThreads, 0, s>>>(sp, g.dt); break;
     case 6: pos_rz_kernel<<<nb, kThreads, 0, s>>>(sp); break;
@@ -342,7 +348,8 @@ void launch_advance_f64(const GridGeom& g, const FieldsF64& f, const SpeciesF64&
                         int pusher, int fixed, int current, unsigned long long* reset,
                         DevStatus* st, cudaStream_t s, int do_push) {
   if (sp.n == 0) return;
-  advance_kernel<<<blocks_for(sp.n), kThreads, 0, s>>>(g, f, sp, slot, pusher, fixed, current, reset, st,
+  auto k = f.ext ? advance_kernel<true> : advance_kernel<false>;
+  k<<<blocks_for(sp.n), kThreads, 0, s>>>(g, f, sp, slot, pusher, fixed, current, reset, st,
                                                        do_push);
 }
 

@@ -243,6 +243,17 @@ class Domain:
         code = {"p12": 0, "ta77s": 1, "sk98": 2}[scheme]
         self._check(self.lib.pcg_set_collision_scheme(self.h, code), "pcg_set_collision_scheme")
 
+    def set_external_fields(self, electric="none", e_params=(), magnetic="none", m_params=()):
+        """External E and H fields (ExternalFields, externalFields.cpp), by the
+        formfactor names of PiCoPiC.json's external_fields section; params[0]
+        is the amplitude.  See pcg_set_external_fields for what applies in
+        each quirk mode."""
+        ep = np.ascontiguousarray(e_params, dtype=np.float64).reshape(-1)
+        mp = np.ascontiguousarray(m_params, dtype=np.float64).reshape(-1)
+        self._check(self.lib.pcg_set_external_fields(self.h, electric.encode(), _dp(ep) if ep.size else None,
+                                                     ep.size, magnetic.encode(), _dp(mp) if mp.size else None,
+                                                     mp.size), "pcg_set_external_fields")
+
     def set_collision_crowding(self, threshold):
         """Cells of more than `threshold` particles run their collisions on a
         warp each (pcg_set_collision_crowding; the result does not change)."""
