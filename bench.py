@@ -456,6 +456,8 @@ def run_collisions(args, local, barrier, allmax):
     c = COLLISIONS
     if args.small:
         c = dict(c, nr=128, nz=256)
+    if args.coll_nz:
+        c = dict(c, nz=args.coll_nz)
     g = Geometry(c["nr"], c["nz"], c["nr"] * c["dr"], c["nz"] * c["dr"], dt_courant(c["dr"]))
     n = c["nr"] * c["nz"] * c["ppc"]
     d = Domain(g, precision="f32", quirks="fixed", seed=11, device=local)
@@ -482,15 +484,19 @@ def run_collisions(args, local, barrier, allmax):
     lrn_ms, counts = timed(d.collide_learned, 10)
     del d
     torch.cuda.empty_cache()
+    cells = c["nr"] * c["nz"]
+    out = {"workload": c["name"] if not args.coll_nz else f"{c['name']} at {c['nr']}x{c['nz']}",
+           "particles": 2 * n, "precision": "f32 particles, FP64 collision arithmetic",
+           "binary_ms_per_step": bin_ms, "learned_ms_per_step": lrn_ms, "speedup": bin_ms / lrn_ms,
+           "learned_cell_fraction": counts[-1][0] / cells, "fallback_cell_fraction": counts[-1][1] / cells}
+    if args.no_relax:
+        return out
     gs = Geometry(64, 128, 64 * c["dr"], 128 * c["dr"], 1e-13)
     tb, eb, _ = L.initial_relaxation_time(gs, "binary", passes=60, density=3e20, device=local)
     tl, _, _ = L.initial_relaxation_time(gs, "learned", passes=1, density=3e20, device=local)
-    cells = c["nr"] * c["nz"]
-    return {"workload": c["name"], "particles": 2 * n, "precision": "f32 particles, FP64 collision arithmetic",
-            "binary_ms_per_step": bin_ms, "learned_ms_per_step": lrn_ms, "speedup": bin_ms / lrn_ms,
-            "learned_cell_fraction": counts[-1][0] / cells, "fallback_cell_fraction": counts[-1][1] / cells,
-            "relaxation_time_steps": {"slab": "64x128 cells, 100 ppc, n 3e20, dt 1e-13, Te 2/1 eV, Ti 0.5 eV",
-                                      "binary": tb, "binary_stderr": eb, "learned": tl, "ratio": tl / tb}}
+    out["relaxation_time_steps"] = {"slab": "64x128 cells, 100 ppc, n 3e20, dt 1e-13, Te 2/1 eV, Ti 0.5 eV",
+                                    "binary": tb, "binary_stderr": eb, "learned": tl, "ratio": tl / tb}
+    return out
 
 
 def run_e2e(w, args, rank, local, barrier, allmax, allsum):
@@ -753,6 +759,8 @@ def main():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-config0", action="store_true")
+    ap.add_argument("--coll-nz", type=int, default=0, help="axial cells of the collisional workload (profiling)")
+    ap.add_argument("--no-relax", action="store_true", help="skip the relaxation-time measurement")
     ap.add_argument("--target-blocks", type=int, default=0,
                     help="float step: blocks the tile sort aims for (0 keeps the default)")
     args = ap.parse_args()
