@@ -466,6 +466,10 @@ def run_collisions(args, local, barrier, allmax):
     d.seed_plasma_cells(0, c["ppc"], c["density"], c["te_par"], c["te_perp"], seed=1)
     d.seed_plasma_cells(1, c["ppc"], c["density"], c["ti"], seed=2)
     d.set_collision_model(*L.load_model())
+    # the slots grouped by tile, as every step keeps them (the collision
+    # passes of a running simulation see that layout)
+    d.tile_sort(0)
+    d.tile_sort(1)
     d.collide()
     d.collide_learned()
     d.synchronize()

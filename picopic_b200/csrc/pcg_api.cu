@@ -62,6 +62,8 @@ struct pcg_handle {
   pcg_config cfg{};
   GridGeom g{};
   cudaStream_t stream = nullptr;
+  cudaStream_t aux = nullptr;     // float steps: the second stream of the species' step kernels
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DevStatus* d_status = nullptr;
   DevStatus* h_status = nullptr;  // pinned mirror
   size_t nodes = 0;               // (nr+4)*(nz+4)
@@ -664,15 +666,29 @@ int fused_step(pcg_handle* h) {
       }
     }
     TimerScope ts(h, PCG_TIMER_PARTICLES);
+    // Species are independent until their currents meet in J (atomics), so
+    // without collisions the odd-numbered ones run on a second stream: one
+    // species' last blocks overlap the next one's first instead of the GPU
+    // draining between them.
+    const bool fork = !collide && h->sp.size() >= 2 && h->aux;
+    if (fork) {
+      CUDA_TRY(h, cudaEventRecord(h->ev_fork, h->stream));
+      CUDA_TRY(h, cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
+    }
     for (size_t t = 0; t < h->sp.size(); ++t) {
       Species& s = h->sp[t];
       const size_t n0 = s.n;
       const uint64_t k0 = s.f32.launches;
-      if (f32_step_species(st, s.f32, &s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream,
+      cudaStream_t stream = fork && (t & 1) ? h->aux : h->stream;
+      if (f32_step_species(st, s.f32, &s.n, s.charge, s.mass, s.beam ? 1 : 0, stream,
                            is_ion_list(s) ? 6 : 0) != 0)
         return fail(h, PCG_ERR_CUDA, "tile sort of species '" + s.name + "' failed");
       h->dead_dropped += n0 - s.n;  // a sort drops the species' dead slots
       h->launches += s.f32.launches - k0;
+    }
+    if (fork) {
+      CUDA_TRY(h, cudaEventRecord(h->ev_join, h->aux));
+      CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     }
   }
   h->t += h->cfg.dt;
@@ -715,6 +731,11 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
   int rc = PCG_OK;
   auto bail = [&](int code) { pcg_destroy(h); return code; };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PCG_ERR_CUDA);
+  if (cfg->precision == PCG_PRECISION_F32 &&
+      (cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess))
+    return bail(PCG_ERR_CUDA);
   if ((rc = dalloc(h, &h->d_status, 1)) != PCG_OK) return bail(rc);
   if (cudaMallocHost((void**)&h->h_status, sizeof(DevStatus)) != cudaSuccess) return bail(PCG_ERR_NOMEM);
   cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), h->stream);
@@ -793,7 +814,11 @@ int pcg_destroy(pcg_handle* h) {
   cudaFree(h->map_work);
   cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);
+  if (h->aux) cudaStreamSynchronize(h->aux);
   if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->aux) cudaStreamDestroy(h->aux);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   delete h;
   return PCG_OK;
 }
