@@ -651,11 +651,20 @@ int fused_step(pcg_handle* h) {
     if (collide) {
       {
         TimerScope ts(h, PCG_TIMER_PARTICLES);
+        const bool fork = h->sp.size() >= 2 && h->aux;
+        if (fork) {
+          CUDA_TRY(h, cudaEventRecord(h->ev_fork, h->stream));
+          CUDA_TRY(h, cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
+        }
         for (size_t t = 0; t < h->sp.size(); ++t) {
           Species& s = h->sp[t];
           const uint64_t k0 = s.f32.launches;
-          f32_push_species(st, s.f32, s.n, s.charge, s.mass, s.beam ? 1 : 0, h->stream);
+          f32_push_species(st, s.f32, s.n, s.charge, s.mass, s.beam ? 1 : 0, fork && (t & 1) ? h->aux : h->stream);
           h->launches += s.f32.launches - k0;
+        }
+        if (fork) {
+          CUDA_TRY(h, cudaEventRecord(h->ev_join, h->aux));
+          CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_join, 0));
         }
       }
       if ((rc = step_collide(h)) != PCG_OK) return rc;
@@ -667,10 +676,10 @@ int fused_step(pcg_handle* h) {
     }
     TimerScope ts(h, PCG_TIMER_PARTICLES);
     // Species are independent until their currents meet in J (atomics), so
-    // without collisions the odd-numbered ones run on a second stream: one
-    // species' last blocks overlap the next one's first instead of the GPU
-    // draining between them.
-    const bool fork = !collide && h->sp.size() >= 2 && h->aux;
+    // the odd-numbered ones run on a second stream: one species' last blocks
+    // overlap the next one's first instead of the GPU draining between them
+    // (the push of a step with collisions is split the same way).
+    const bool fork = h->sp.size() >= 2 && h->aux;
     if (fork) {
       CUDA_TRY(h, cudaEventRecord(h->ev_fork, h->stream));
       CUDA_TRY(h, cudaStreamWaitEvent(h->aux, h->ev_fork, 0));

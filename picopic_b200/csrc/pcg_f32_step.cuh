@@ -839,8 +839,11 @@ static_assert((6 * kFWR * kFWS + 3 * kJWR * kJWZ) % 4 == 0, "the table rows need
 // leaves them to the arguments.  The specialised ZigZag instance fits 48
 // registers without spilling and runs 5 blocks per SM (shared memory allows
 // 5); the others keep 64 registers and 4 blocks.
+// PUSH = kMoveOnly: the instance for steps whose push ran already (with
+// collisions), the pusher's code left out.
+constexpr int kMoveOnly = -2;
 template <int CUR, int PUSH = -1, int BEAM = -1, int FIX = -1>
-__global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
+__global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH != -1) ? 5 : 4)
     step_tiled_kernel(StepArgs args, SpeciesF32Buffers b,
                                                                  TileGrid tg) {
   StepArgs a = args;
@@ -849,6 +852,7 @@ __global__ void __launch_bounds__(kThreads, (CUR == 1 && PUSH >= 0) ? 5 : 4)
     a.pushed = 0;
     a.xform = nullptr;
   }
+  if (PUSH == kMoveOnly) a.pushed = 1;
   if (BEAM >= 0) a.is_beam = BEAM;
   if (FIX >= 0) a.fixed = FIX;
   extern __shared__ float smem[];

@@ -523,6 +523,8 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
     const dim3 grid(tg.ntiles, b.splits);
     if (st.current == PCG_CURRENT_ZIGZAG && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed && !st.pushed)
       f32::step_tiled_kernel<1, PCG_PUSHER_VAY, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.current == PCG_CURRENT_ZIGZAG && st.pushed && !is_beam && !st.fixed)
+      f32::step_tiled_kernel<1, f32::kMoveOnly, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.current == PCG_CURRENT_ZIGZAG)
       f32::step_tiled_kernel<1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.pushed)
