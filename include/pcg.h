@@ -479,6 +479,16 @@ int pcg_export_field(pcg_handle* h, int which, double* dst);
 int pcg_stage(pcg_handle* h, int stage);
 int pcg_step(pcg_handle* h, int nsteps);
 int pcg_synchronize(pcg_handle* h);
+/* The status of the steps queued before the last call of pcg_step_status,
+ * read without waiting for the steps queued since (no reference counterpart:
+ * the reference aborts inside the step).  Each call queues a copy of the
+ * device status block to pinned host memory and returns the block the
+ * previous call queued, waiting for that copy only; a loop of pcg_step +
+ * pcg_step_status therefore reads every step's status, one step late, while
+ * the GPU keeps a step queued.  pcg_synchronize reads the current one.
+ * pcg_import_species and pcg_append_species likewise wait for their own
+ * host-to-device copies, not for the steps queued before them. */
+int pcg_step_status(pcg_handle* h);
 int pcg_diag(pcg_handle* h, pcg_diagnostics* out);
 /* The handle's cudaStream_t, for callers that time or order work on it. */
 int pcg_get_stream(pcg_handle* h, void** stream);

@@ -89,6 +89,7 @@ SIGNATURES = {
     "pcg_set_collisions": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_scheme": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_set_collision_crowding": (ctypes.c_int, [_H, ctypes.c_uint]),
+    "pcg_step_status": (ctypes.c_int, [_H]),
     "pcg_set_external_fields": (ctypes.c_int, [_H, ctypes.c_char_p, _PD, ctypes.c_int, ctypes.c_char_p, _PD,
                                                ctypes.c_int]),
     "pcg_species_map": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, _PD]),

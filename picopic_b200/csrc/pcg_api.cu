@@ -64,6 +64,14 @@ struct pcg_handle {
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;     // float steps: the second stream of the species' step kernels
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // host particle uploads: copies on their own stream, so that the caller
+  // waits for its copies only, not for the steps queued before them
+  cudaStream_t copy = nullptr;
+  cudaEvent_t ev_copied = nullptr, ev_staging_free = nullptr;
+  // pcg_step_status: the status block of the last step, copied without waiting
+  DevStatus* h_status_lag = nullptr;
+  cudaEvent_t ev_status = nullptr;
+  bool status_pending = false;
   DevStatus* d_status = nullptr;
   DevStatus* h_status = nullptr;  // pinned mirror
   size_t nodes = 0;               // (nr+4)*(nz+4)
@@ -241,12 +249,19 @@ int ensure_staged(pcg_handle* h) {
   return PCG_OK;
 }
 
+int status_code(pcg_handle* h, const DevStatus* st);
+
 int check_status(pcg_handle* h) {
   CUDA_TRY(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
                               h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   CUDA_TRY(h, cudaGetLastError());
-  unsigned e = h->h_status->error;
+  return status_code(h, h->h_status);
+}
+
+// The error word of a status block as a PCG_ERR_* code.
+int status_code(pcg_handle* h, const DevStatus* st) {
+  unsigned e = st->error;
   if (e & kErrNanPosition) return fail(h, PCG_ERR_NAN, "particle position is not a finite number");
   if (e & kErrNanField) return fail(h, PCG_ERR_NAN, "electric field became NaN");
   if (e & kErrSuperluminal) return fail(h, PCG_ERR_SUPERLUMINAL, "particle speed above c");
@@ -740,6 +755,12 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
   int rc = PCG_OK;
   auto bail = [&](int code) { pcg_destroy(h); return code; };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(PCG_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_copied, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_staging_free, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_status, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost((void**)&h->h_status_lag, sizeof(DevStatus)) != cudaSuccess)
+    return bail(PCG_ERR_CUDA);
   if (cfg->precision == PCG_PRECISION_F32 &&
       (cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) != cudaSuccess ||
        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
@@ -824,6 +845,12 @@ int pcg_destroy(pcg_handle* h) {
   cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->aux) cudaStreamSynchronize(h->aux);
+  if (h->copy) cudaStreamSynchronize(h->copy);
+  if (h->copy) cudaStreamDestroy(h->copy);
+  if (h->ev_copied) cudaEventDestroy(h->ev_copied);
+  if (h->ev_staging_free) cudaEventDestroy(h->ev_staging_free);
+  if (h->ev_status) cudaEventDestroy(h->ev_status);
+  if (h->h_status_lag) cudaFreeHost(h->h_status_lag);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->aux) cudaStreamDestroy(h->aux);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -908,12 +935,18 @@ static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, con
     }
     double* stage = h->staging;
     const double* src[6] = {r, z, vr, vphi, vz, w};
+    // the copies wait for the last import's read of the staging buffer only,
+    // and the import for the copies; the steps queued before run on
+    CUDA_TRY(h, cudaStreamWaitEvent(h->copy, h->ev_staging_free, 0));
     for (int a = 0; a < 6; ++a)
-      CUDA_TRY(h, cudaMemcpyAsync(stage + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+      CUDA_TRY(h, cudaMemcpyAsync(stage + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->copy));
+    CUDA_TRY(h, cudaEventRecord(h->ev_copied, h->copy));
+    CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_copied, 0));
     if (is_f64(h)) launch_import_f64(h->g, view64(h, s), n0, n, stage, h->stream);
     else f32_launch_import(h->g, s.f32, n0, n, stage, h->stream);
+    CUDA_TRY(h, cudaEventRecord(h->ev_staging_free, h->stream));
     // the caller may reuse its host arrays once this call returns
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    CUDA_TRY(h, cudaEventSynchronize(h->ev_copied));
   }
   s.n = n0 + n;
   return PCG_OK;
@@ -1307,6 +1340,21 @@ int pcg_step(pcg_handle* h, int nsteps) {
 int pcg_synchronize(pcg_handle* h) {
   if (!h) return PCG_ERR_ARG;
   return check_status(h);
+}
+
+int pcg_step_status(pcg_handle* h) {
+  if (!h) return PCG_ERR_ARG;
+  int rc = PCG_OK;
+  if (h->status_pending) {  // the block copied after the step before: that step has ended
+    CUDA_TRY(h, cudaEventSynchronize(h->ev_status));
+    h->status_pending = false;
+    rc = status_code(h, h->h_status_lag);
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_status_lag, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                              h->stream));
+  CUDA_TRY(h, cudaEventRecord(h->ev_status, h->stream));
+  h->status_pending = true;
+  return rc;
 }
 
 int pcg_seed_plasma_cells(pcg_handle* h, int slot, unsigned per_cell, double density, double t_par_ev,

@@ -341,6 +341,11 @@ class Domain:
         self._check(self.lib.pcg_step(self.h, int(n)), "pcg_step")
         return 0
 
+    def step_status(self):
+        """Check the status of the steps before the previous call without
+        waiting for the later ones (pcg_step_status); raises on an error."""
+        self._check(self.lib.pcg_step_status(self.h), "pcg_step_status")
+
     def synchronize(self):
         self._check(self.lib.pcg_synchronize(self.h), "pcg_synchronize")
 

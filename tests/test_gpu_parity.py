@@ -174,6 +174,30 @@ def test_nan_position_is_an_error():
     assert e.value.code == -10
 
 
+def test_step_status_reports_each_step_a_step_late():
+    """pcg_step_status returns the status queued by the previous call: a
+    NaN position raised in step 1 shows at the status read after step 2,
+    and a clean run reads clean throughout."""
+    from picopic_b200 import PcgError
+    grid = small_grid(pml=False)
+    clean = _gpu(grid, "borisrel", "vb")
+    clean.add(ELECTRONS)
+    clean.set_particles(0, [5e-4, 6e-4], [5e-4, 5e-4], [0, 0], [0, 0], [0, 0], [1, 1])
+    for _ in range(3):
+        clean.step(1)
+        clean.step_status()
+    clean.synchronize()
+    gpu = _gpu(grid, "borisrel", "vb")
+    gpu.add(ELECTRONS)
+    gpu.set_particles(0, [np.nan, 5e-4], [5e-4, 5e-4], [0, 0], [0, 0], [0, 0], [1, 1])
+    gpu.step(1)
+    gpu.step_status()  # nothing queued before: clean
+    gpu.step(1)
+    with pytest.raises(PcgError) as e:
+        gpu.step_status()  # the block copied after step 1
+    assert e.value.code == -10
+
+
 def load_pairs(gpu, orc, grid, species, n, seed):
     from tests.cases import particles, random_fields
     for i, sp in enumerate(species):
