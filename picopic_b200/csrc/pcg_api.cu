@@ -509,7 +509,7 @@ bool collision_species(pcg_handle* h, std::vector<CollSpecies>& v, CollParams& p
     if (is_f64(h)) {
       c.r = s.r; c.z = s.z; c.vr64 = s.vr; c.vphi64 = s.vphi; c.vz64 = s.vz; c.w64 = s.w;
     } else {
-      c.cell = s.f32.cell; c.id = s.f32.id;
+      c.cell = s.f32.cell; c.id = s.f32.id; c.id_bound = s.f32.next_id;
       c.vr32 = s.f32.vr; c.vphi32 = s.f32.vphi; c.vz32 = s.f32.vz; c.w32 = s.f32.w;
       c.tile_start = s.f32.tile_start;
       c.cell_count = s.f32.cell_count;

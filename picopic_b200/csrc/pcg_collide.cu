@@ -47,9 +47,11 @@ namespace {
 
 // (the species comes by value: a run-time index into the by-value species
 // table would copy the whole table to each thread's local memory)
+// The key cell << cs | species << ts | id orders a list by cell, then
+// species, then id (insertion order), in as few bits as the list needs.
 __global__ void key_kernel(GridGeom g, CollSpecies sp, int t, unsigned long long* keys,
-                           unsigned long long* vals, unsigned* count, unsigned* n_valid,
-                           const unsigned char* only, unsigned char only_value) {
+                           unsigned long long* vals, unsigned* n_valid,
+                           const unsigned char* only, unsigned char only_value, int cs, int ts) {
   const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   int ci = -1, ck = -1;
   unsigned id = 0;
@@ -58,7 +60,6 @@ __global__ void key_kernel(GridGeom g, CollSpecies sp, int t, unsigned long long
       const int c = sp.cell[j];
       ci = c < 0 ? -1 : cell_r_of(c);
       ck = c < 0 ? -1 : cell_z_of(c);
-      id = sp.id[j];
     } else {
       const double r = sp.r[j];
       ci = r >= 0.0 ? (int)floor(r / g.dr) : -1;  // CELL_NUMBER geometry.hpp:198; dead slots have r < 0
@@ -69,36 +70,102 @@ __global__ void key_kernel(GridGeom g, CollSpecies sp, int t, unsigned long long
   bool valid = ci >= 0 && ck >= 0 && ci < g.nr && ck < g.nz;
   const unsigned long long c = valid ? (unsigned long long)ci * g.nz + ck : 0ull;
   if (valid && only && only[c] != only_value) valid = false;
-  // valid entries are appended (keys are unique, so the sort fixes the order)
+  // valid entries are appended (keys are unique, so the sort fixes the
+  // order), one counter increment per block: per warp, the counter is one
+  // address that every warp of the grid would wait on in turn
+  __shared__ unsigned warp_n[kThreads / 32], block_base;
   const unsigned mask = __ballot_sync(0xffffffffu, valid);
-  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
-  unsigned base = 0;
-  if (mask && lane == leader) base = atomicAdd(n_valid, (unsigned)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) warp_n[wid] = __popc(mask);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned tot = 0;
+    for (int q = 0; q < kThreads / 32; ++q) {
+      const unsigned v = warp_n[q];
+      warp_n[q] = tot;
+      tot += v;
+    }
+    block_base = tot ? atomicAdd(n_valid, tot) : 0u;
+  }
+  __syncthreads();
+  const unsigned base = block_base + warp_n[wid];
   if (!valid) return;
+  if (sp.cell) id = sp.id[j];
   const unsigned pos = base + __popc(mask & ((1u << lane) - 1u));
-  keys[pos] = (c << 36) | ((unsigned long long)t << 32) | id;
+  keys[pos] = (c << cs) | ((unsigned long long)t << ts) | id;
   vals[pos] = ((unsigned long long)t << 40) | j;
-  atomicAdd(count + c, 1u);
+}
+
+// Each cell's run in the sorted keys: start[c] its first entry, end[c] one
+// past its last (both 0 for a cell without entries, cleared before).
+__global__ void bounds_kernel(const unsigned long long* keys, unsigned n, int cs, unsigned* start, unsigned* end) {
+  const size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const unsigned long long c = keys[e] >> cs;
+  if (e == 0 || (keys[e - 1] >> cs) != c) start[c] = (unsigned)e;
+  if (e + 1 == n || (keys[e + 1] >> cs) != c) end[c] = (unsigned)e + 1;
+}
+
+// count[c] = end[c] - start[c], in place of end
+__global__ void run_count_kernel(size_t cells, const unsigned* start, unsigned* count) {
+  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c < cells) count[c] -= start[c];
 }
 
 // ---------------------------------------------------------------------------
 // 3. shuffle
 
+// The partner of position i in the Fisher-Yates pass of cell c.
+__device__ __forceinline__ unsigned shuffle_partner(size_t c, unsigned i, uint64_t seed, uint32_t pass,
+                                                    uint32_t list) {
+  uint32_t o[4];
+  philox4x32_10((uint32_t)c, i, pass, kShufTag + list, (uint32_t)seed, (uint32_t)(seed >> 32), o);
+  const unsigned j = (unsigned)(u53(o[0], o[1]) * (double)(i + 1));
+  return j > i ? i : j;
+}
+
+// A warp per cell: the lanes draw every position's partner at once and
+// stage the list in shared memory, one lane makes the swaps in order (the
+// same permutation as one thread drawing and swapping in turn), and the
+// lanes write the list back.  A list longer than kShufCap is shuffled by
+// one lane in place.
+constexpr unsigned kShufCap = 256;
 __global__ void shuffle_kernel(size_t cells, const unsigned* start, const unsigned* count,
                                unsigned long long* vals, uint64_t seed, uint32_t pass, uint32_t list) {
-  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (c >= cells) return;
-  unsigned long long* L = vals + start[c];
-  const unsigned n = count[c];
-  for (unsigned i = 1; i < n; ++i) {
-    uint32_t o[4];
-    philox4x32_10((uint32_t)c, i, pass, kShufTag + list, (uint32_t)seed, (uint32_t)(seed >> 32), o);
-    unsigned j = (unsigned)(u53(o[0], o[1]) * (double)(i + 1));
-    if (j > i) j = i;
-    const unsigned long long tmp = L[i];
-    L[i] = L[j];
-    L[j] = tmp;
+  __shared__ unsigned long long buf[kThreads / 32][kShufCap];
+  __shared__ unsigned short part[kThreads / 32][kShufCap];
+  const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const size_t stride = (size_t)gridDim.x * (kThreads / 32);
+  for (size_t c = blockIdx.x * (size_t)(kThreads / 32) + w; c < cells; c += stride) {
+    const unsigned n = count[c];
+    if (n < 2) continue;
+    unsigned long long* L = vals + start[c];
+    if (n > kShufCap) {
+      if (lane == 0)
+        for (unsigned i = 1; i < n; ++i) {
+          const unsigned j = shuffle_partner(c, i, seed, pass, list);
+          const unsigned long long tmp = L[i];
+          L[i] = L[j];
+          L[j] = tmp;
+        }
+      __syncwarp();
+      continue;
+    }
+    for (unsigned i = lane; i < n; i += 32) {
+      buf[w][i] = L[i];
+      part[w][i] = i ? (unsigned short)shuffle_partner(c, i, seed, pass, list) : 0;
+    }
+    __syncwarp();
+    if (lane == 0)
+      for (unsigned i = 1; i < n; ++i) {
+        const unsigned j = part[w][i];
+        const unsigned long long tmp = buf[w][i];
+        buf[w][i] = buf[w][j];
+        buf[w][j] = tmp;
+      }
+    __syncwarp();
+    for (unsigned i = lane; i < n; i += 32) L[i] = buf[w][i];
+    __syncwarp();
   }
 }
 
@@ -471,12 +538,19 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   cudaMemsetAsync(w.crowded, 0, sizeof(unsigned), s);
   cudaMemsetAsync(w.active, 0, sizeof(unsigned), s);
   w.launches = 3;  // moments and the pairs of ordinary and of crowded cells
+  // bits of the sort keys: id (below the largest id bound of a species), species, cell
+  auto width = [](unsigned long long v) { int b = 0; while (b < 64 && (v >> b) != 0) ++b; return b; };
+  unsigned long long max_id = 0;
+  for (int t = 0; t < nsp; ++t)
+    max_id = std::max<unsigned long long>(max_id, sp[t].cell ? sp[t].id_bound : sp[t].n);
+  const int id_bits = std::max(1, width(max_id)), sp_bits = std::max(1, width((unsigned long long)(nsp - 1)));
+  const int key_ts = id_bits, key_cs = id_bits + sp_bits, key_bits = key_cs + std::max(1, width(cells - 1));
+  if (key_bits > 64) return -1;
   for (int l = 0; l < 2; ++l) {
-    cudaMemsetAsync(w.count[l], 0, (cells + 1) * sizeof(unsigned), s);
     for (int t = 0; t < nsp; ++t) {
       if ((sp[t].is_ion ? 1 : 0) != l || !sp[t].n) continue;
-      key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], t, w.keys[l], w.vals[l], w.count[l],
-                                                          w.valid + l, p.only, p.only_value);
+      key_kernel<<<blocks_for(sp[t].n), kThreads, 0, s>>>(g, sp[t], t, w.keys[l], w.vals[l], w.valid + l, p.only,
+                                                          p.only_value, key_cs, key_ts);
       ++w.launches;
     }
   }
@@ -487,16 +561,24 @@ int collide_p12(const GridGeom& g, const CollSpecies* sp, int nsp, const CollPar
   for (int l = 0; l < 2; ++l) {
     if (valid[l]) {
       size_t b = w.tmp_bytes;
-      int bits = 36;  // the key is cell << 36 | species << 32 | id, cell < 2^28
-      while (bits < 64 && (1ull << (bits - 36)) < cells) ++bits;
       cub::DeviceRadixSort::SortPairs(w.tmp, b, w.keys[l], w.keys2[l], w.vals[l], w.vals2[l],
-                                      (int)valid[l], 0, std::min(bits + 1, 64), s);
+                                      (int)valid[l], 0, key_bits, s);
     }
-    size_t b = w.tmp_bytes;
-    cub::DeviceScan::ExclusiveSum(w.tmp, b, w.count[l], w.start[l], (int)(cells + 1), s);
+    // per cell the run of its entries in the sorted list (count = end - start)
+    cudaMemsetAsync(w.start[l], 0, (cells + 1) * sizeof(unsigned), s);
+    cudaMemsetAsync(w.count[l], 0, (cells + 1) * sizeof(unsigned), s);
+    if (valid[l]) {
+      bounds_kernel<<<blocks_for(valid[l]), kThreads, 0, s>>>(w.keys2[l], valid[l], key_cs, w.start[l], w.count[l]);
+      run_count_kernel<<<blocks_for(cells), kThreads, 0, s>>>(cells, w.start[l], w.count[l]);
+      w.launches += 2;
+    }
     if (p.shuffle && valid[l]) {
-      shuffle_kernel<<<blocks_for(cells), kThreads, 0, s>>>(cells, w.start[l], w.count[l], w.vals2[l],
-                                                             p.seed, p.pass, (uint32_t)l);
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const size_t blocks = std::min<size_t>((cells + kThreads / 32 - 1) / (kThreads / 32), (size_t)sms * 16);
+      shuffle_kernel<<<(unsigned)blocks, kThreads, 0, s>>>(cells, w.start[l], w.count[l], w.vals2[l], p.seed,
+                                                          p.pass, (uint32_t)l);
       ++w.launches;
     }
     // the sorted keys are spent: keys2 now holds the staged references

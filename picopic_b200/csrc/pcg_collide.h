@@ -26,6 +26,7 @@ struct CollSpecies {
   const double* w64 = nullptr;
   const int* cell = nullptr;
   const unsigned* id = nullptr;
+  unsigned long long id_bound = 0;  // float layout: every id is below it
   float *vr32 = nullptr, *vphi32 = nullptr, *vz32 = nullptr;
   const float* w32 = nullptr;
   // float layout: slots [0, sorted) are grouped by tile, tile t holding

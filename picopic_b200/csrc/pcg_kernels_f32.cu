@@ -25,11 +25,14 @@ constexpr int kThreads = 256;
 inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 // Position in metres -> (cell, offset) with 0 <= offset < 1.
+// The cell is the reference's CELL_NUMBER (floor(pos / cell size) in
+// double, geometry.hpp:198); an offset that rounds up to 1 in float stays
+// the largest float below 1, so that the cell never differs from it.
 __device__ __forceinline__ void split_position(double x_m, double d, int* cell, float* off) {
   const double x = x_m / d;
-  double c = floor(x);
+  const double c = floor(x);
   float f = (float)(x - c);
-  if (f >= 1.0f) { f = 0.0f; c += 1.0; }
+  if (f >= 1.0f) f = 0x1.fffffep-1f;
   *cell = (int)c;
   *off = f;
 }

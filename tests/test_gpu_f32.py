@@ -102,13 +102,38 @@ def test_f32_removal_counts_and_launches():
     assert gpu.diag().kernel_launches - d0.kernel_launches >= 3 * 240
 
 
+def test_import_binds_cells_as_the_reference():
+    """The float layout's cell of an imported particle is the reference's
+    CELL_NUMBER (floor(pos / cell size) in double, geometry.hpp:198) of the
+    same double position, also exactly on cell boundaries and one ulp below
+    them."""
+    from picopic_b200 import Domain
+    grid = small_grid(nr=24, nz=160, pml=False)
+    d = Domain(grid, precision="f32", seed=7)
+    d.add(ELECTRONS, capacity=40000)
+    rng = np.random.default_rng(12)
+    n = 30000
+    r = rng.uniform(0.5, grid.nr - 0.5, n) * grid.dr
+    z = rng.uniform(0.5, grid.nz - 0.5, n) * grid.dz
+    kr = rng.integers(1, grid.nr - 1, 2000)
+    kz = rng.integers(1, grid.nz - 1, 2000)
+    r[:1000], z[:1000] = kr[:1000] * grid.dr, kz[:1000] * grid.dz
+    r[1000:2000] = np.nextafter(kr[1000:] * grid.dr, 0.0)
+    z[1000:2000] = np.nextafter(kz[1000:] * grid.dz, 0.0)
+    zero = np.zeros(n)
+    d.set_particles(0, r, z, zero, zero, zero, np.ones(n))
+    p = d.get_particles(0)
+    np.testing.assert_array_equal(p["cell_r"], np.floor(r / grid.dr).astype(np.int64))
+    np.testing.assert_array_equal(p["cell_z"], np.floor(z / grid.dz).astype(np.int64))
+
+
 def test_tile_sort_groups_cells_exactly():
     """The float step's tile sort (pcg_tile_sort, the sort a step runs when
     particles drift): no particle outside its tile, and the per-cell counts
     the sorted tiles hold equal, bit for bit, those of the particles' cells
     and those the FP64 oracle binds (floor(r / dr), floor(z / dz)) from the
-    same positions.  3 x 3 tiles of 8 x 64 cells, the last column partly
-    empty; after 3 steps of moving particles."""
+    same positions.  3 x 5 tiles of 8 x 32 cells; after 3 steps of moving
+    particles."""
     from picopic_b200 import Domain
     grid = small_grid(nr=24, nz=160, pml=False)
     d = Domain(grid, precision="f32", seed=7)
