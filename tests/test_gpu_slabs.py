@@ -1,0 +1,77 @@
+"""A run split along z into slabs of GPU domains (picopic_b200/slabs.py,
+several domains on one GPU in one process) against the undivided run on the
+same GPU: the FP64 layout within 1e-9 of each field array's largest value
+and of each particle quantity after 10 steps (the deposit adds the same
+currents in another order), the float layout within 1e-4 (fields) and 1e-5
+(particles), as the float path is checked against the oracle."""
+import numpy as np
+import pytest
+
+from oracle.harness import SpeciesSpec
+from picopic_b200 import slabs as S
+from tests.cases import ELECTRONS, IONS, beam_spec, particles, random_fields, small_grid
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 10
+
+
+def _species(grid):
+    return [ELECTRONS, IONS, beam_spec(grid)]
+
+
+def _domain(geometry, precision, quirks, species):
+    from picopic_b200 import Domain
+    d = Domain(geometry, pusher="borisrel", current="vb", precision=precision, quirks=quirks, seed=7)
+    for sp in species:
+        d.add(sp, capacity=40000)
+    return d
+
+
+def _inputs(grid):
+    parts = {}
+    for i, sp in enumerate(_species(grid)):
+        if sp.beam is None:
+            parts[i] = particles(grid, 3000, 30 + i, mass=sp.mass, boost=30.0 if sp.mass == 1 else 150.0)
+    return parts, random_fields(grid, 5)
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _sorted(p):
+    order = np.lexsort((p["r"], p["z"]))
+    return {k: np.asarray(p[k])[order] for k in S.PARTICLE_KEYS}
+
+
+@pytest.mark.parametrize("precision,quirks,count", [("f64", "reference", 2), ("f64", "fixed", 3), ("f32", "fixed", 2)])
+def test_gpu_slabs_equal_the_undivided_run(precision, quirks, count):
+    grid = small_grid(nr=16, nz=96)
+    species = _species(grid)
+
+    def make(geometry, slab):
+        sp = [s if (slab.first or s.beam is None) else SpeciesSpec(s.name, s.charge, s.mass, id=s.id)
+              for s in species]
+        return _domain(geometry, precision, quirks, sp)
+
+    g = S.SlabGroup(grid, count, make, len(species))
+    whole = _domain(grid, precision, quirks, species)
+    parts, fields = _inputs(grid)
+    for i, p in parts.items():
+        g.set_particles(i, *p)
+        whole.set_particles(i, *p)
+    for k, a in fields.items():
+        g.set_field(k, a)
+        whole.set_field(k, a)
+    g.step(STEPS)
+    whole.step(STEPS)
+    tol_f, tol_p = (1e-9, 1e-9) if precision == "f64" else (1e-4, 1e-5)
+    for k in S.FIELDS:
+        assert _rel(g.get_field(k), whole.get_field(k)) <= tol_f, k
+    for t in range(len(species)):
+        a, b = _sorted(g.get_particles(t)), _sorted(whole.get_particles(t))
+        assert a["r"].size == b["r"].size, t
+        for k in S.PARTICLE_KEYS:
+            assert _rel(a[k], b[k]) <= tol_p, (t, k)
+    assert g.get_particles(2)["r"].size > 0, "the beam was injected"
