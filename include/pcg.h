@@ -168,7 +168,9 @@ int pcg_add_beam(pcg_handle* h, int id, const char* name, double charge_e, doubl
                  double density, double bunches_amount, double bunch_length,
                  double bunches_distance, double velocity, int* slot);
 
-/* Replace (import) or extend (append) a species' particles from host SoA. */
+/* Replace (import) or extend (append) a species' particles from host SoA.
+ * An append that would exceed the capacity first reclaims the species'
+ * dead slots (a compaction, which waits for the stream). */
 int pcg_import_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
                        const double* vr, const double* vphi, const double* vz, const double* w);
 int pcg_append_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
@@ -475,6 +477,31 @@ int pcg_current_vb_f64_noalloc(int nr, int nz, double radius, double longitude, 
 
 int pcg_set_field(pcg_handle* h, int which, const double* src);
 int pcg_export_field(pcg_handle* h, int which, double* dst);
+
+/* Array columns [c0, c1) of a field grid, 0 <= c0 < c1 <= nz+4 (column
+ * c holds the nodes of cell k = c - 2 along z): (nr+4) x (c1-c0) doubles,
+ * row-major, copied from or to the device without touching the other
+ * columns.  These replace whole-array copies in an exchange of ghost
+ * columns between domains split along z, the counterpart of the
+ * reference's overlap copies (SMB::field_e_overlay, field_h_overlay,
+ * current_overlay, SMB.cpp:566-1229). */
+int pcg_get_field_columns(pcg_handle* h, int which, int c0, int c1, double* dst);
+int pcg_set_field_columns(pcg_handle* h, int which, int c0, int c1, const double* src);
+
+/* The live particles of a species with lo <= z < hi (z in m, the domain's
+ * coordinates; -inf and +inf are allowed), in slot order:
+ * pcg_export_species_range writes their r, z, v_r, v_phi, v_z, w (a null
+ * array is skipped) and *n = their count; with cap < count it writes
+ * nothing else and returns PCG_ERR_CAPACITY.  pcg_keep_species_range
+ * removes every live particle outside [lo, hi); its slots become dead and
+ * are reclaimed by the next compaction.  The two use the same z of a
+ * particle (the float layout's cell and offset in double), so one band's
+ * export and the complementary keep split the particles exactly.  With
+ * pcg_append_species they hand particles between domains split along z,
+ * the counterpart of SMB::particles_runaway_collector (SMB.cpp:194-564). */
+int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size_t cap, double* r,
+                             double* z, double* vr, double* vphi, double* vz, double* w, size_t* n);
+int pcg_keep_species_range(pcg_handle* h, int slot, double lo, double hi);
 
 int pcg_stage(pcg_handle* h, int stage);
 int pcg_step(pcg_handle* h, int nsteps);

@@ -65,6 +65,11 @@ SIGNATURES = {
                            [_PI32, _PI32, ctypes.POINTER(ctypes.c_size_t)]),
     "pcg_set_field": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
     "pcg_export_field": (ctypes.c_int, [_H, ctypes.c_int, _PD]),
+    "pcg_get_field_columns": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PD]),
+    "pcg_set_field_columns": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PD]),
+    "pcg_export_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D, ctypes.c_size_t] + [_PD] * 6 +
+                                 [ctypes.POINTER(ctypes.c_size_t)]),
+    "pcg_keep_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D]),
     "pcg_stage": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_step": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_synchronize": (ctypes.c_int, [_H]),

@@ -40,6 +40,7 @@ UNITS = {
     "pcg_learned.cu": ["--fmad=false"],
     "pcg_maps.cu": ["--fmad=false"],
     "pcg_ensemble.cu": [],
+    "pcg_region.cu": ["--fmad=false"],
 }
 
 

@@ -22,6 +22,7 @@
 #include "pcg_learned.h"
 #include "pcg_maps.h"
 #include "pcg_kernels.h"
+#include "pcg_region.h"
 #include "pcg_yee.cuh"
 
 using namespace pcg;
@@ -105,6 +106,11 @@ struct pcg_handle {
   bool started = false;  // particles imported or stepped: species list frozen
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  // pcg_export_species_range: selection scratch and the gathered particles
+  unsigned char* region = nullptr;
+  size_t region_bytes = 0;
+  double* region_out = nullptr;
+  size_t region_out_n = 0;
   double* staging = nullptr;  // host-to-device particle staging, reused
   size_t staging_n = 0;
   // kernel timers: event pairs per class, recycled after each query
@@ -831,6 +837,8 @@ int pcg_destroy(pcg_handle* h) {
   cudaFree(h->push32);
   cudaFree(h->reset);
   cudaFree(h->scratch);
+  cudaFree(h->region);
+  cudaFree(h->region_out);
   cudaFree(h->staging);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   for (auto& u : h->ev_used) { cudaEventDestroy(u.second.first); cudaEventDestroy(u.second.second); }
@@ -920,6 +928,11 @@ static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, con
   if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   if (n && !(r && z && vr && vphi && vz && w)) return fail(h, PCG_ERR_ARG, "null particle array");
   Species& s = h->sp[slot];
+  if (append && s.n + n > s.cap) {  // reclaim the dead slots first
+    int rc = check_status(h);
+    if (rc != PCG_OK) return rc;
+    if (h->h_status->dead_slots > h->dead_dropped && (rc = compact(h)) != PCG_OK) return rc;
+  }
   size_t n0 = append ? s.n : 0;
   if (n0 + n > s.cap) return fail(h, PCG_ERR_CAPACITY, "species '" + s.name + "' capacity exceeded");
   h->started = true;
@@ -1029,6 +1042,142 @@ int pcg_export_field(pcg_handle* h, int which, double* dst) {
     for (size_t p = 0; p < h->nodes; ++p) dst[p] = tmp[p];
   }
   (void)kFieldNames;
+  return PCG_OK;
+}
+
+namespace {
+
+// Columns [c0, c1) of every row of a field grid to or from the host.
+int field_columns(pcg_handle* h, int which, int c0, int c1, double* host, bool set) {
+  if (!h || !host || which < 0 || which >= 12) return PCG_ERR_ARG;
+  const int ld = h->g.ld, rows = h->g.nr + 4;
+  if (c0 < 0 || c1 > ld || c0 >= c1) return fail(h, PCG_ERR_ARG, "field columns out of range");
+  const size_t w = (size_t)(c1 - c0);
+  if (!set) {
+    int rc = check_status(h);
+    if (rc != PCG_OK) return rc;
+  }
+  if (is_f64(h)) {
+    double* dev = h->f64[which] + c0;
+    if (set)
+      CUDA_TRY(h, cudaMemcpy2DAsync(dev, sizeof(double) * ld, host, sizeof(double) * w, sizeof(double) * w, rows,
+                                    cudaMemcpyHostToDevice, h->stream));
+    else
+      CUDA_TRY(h, cudaMemcpy2DAsync(host, sizeof(double) * w, dev, sizeof(double) * ld, sizeof(double) * w, rows,
+                                    cudaMemcpyDeviceToHost, h->stream));
+    if (!set) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  } else {
+    float* dev = h->f32[which] + c0;
+    std::vector<float> tmp(w * rows);
+    if (set) {
+      for (size_t p = 0; p < tmp.size(); ++p) tmp[p] = (float)host[p];
+      CUDA_TRY(h, cudaMemcpy2DAsync(dev, sizeof(float) * ld, tmp.data(), sizeof(float) * w, sizeof(float) * w, rows,
+                                    cudaMemcpyHostToDevice, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    } else {
+      CUDA_TRY(h, cudaMemcpy2DAsync(tmp.data(), sizeof(float) * w, dev, sizeof(float) * ld, sizeof(float) * w, rows,
+                                    cudaMemcpyDeviceToHost, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+      for (size_t p = 0; p < tmp.size(); ++p) host[p] = tmp[p];
+    }
+  }
+  return PCG_OK;
+}
+
+// The species' layout view for the band kernels (one of the two is set).
+void region_views(pcg_handle* h, Species& s, SpeciesF64* v64, const SpeciesF32Buffers** b32,
+                  const SpeciesF64** s64) {
+  if (is_f64(h)) {
+    *v64 = view64(h, s);
+    *s64 = v64;
+    *b32 = nullptr;
+  } else {
+    *s64 = nullptr;
+    *b32 = &s.f32;
+  }
+}
+
+}  // namespace
+
+int pcg_get_field_columns(pcg_handle* h, int which, int c0, int c1, double* dst) {
+  return field_columns(h, which, c0, c1, dst, false);
+}
+
+int pcg_set_field_columns(pcg_handle* h, int which, int c0, int c1, const double* src) {
+  return field_columns(h, which, c0, c1, const_cast<double*>(src), true);
+}
+
+int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size_t cap, double* r,
+                             double* z, double* vr, double* vphi, double* vz, double* w, size_t* n) {
+  if (!h || !n || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  if (std::isnan(lo) || std::isnan(hi)) return fail(h, PCG_ERR_ARG, "NaN band limit");
+  *n = 0;
+  int rc = check_status(h);  // the steps queued before are done
+  if (rc != PCG_OK) return rc;
+  Species& s = h->sp[slot];
+  const size_t ns = s.n;
+  if (ns == 0) return PCG_OK;
+  if (ns > 0x7fffffffu) return fail(h, PCG_ERR_UNSUPPORTED, "a band selection of more than 2^31 slots");
+  // scratch: slot indices, selected indices, their count, flags, select temp
+  size_t tmp = 0;
+  cub::DeviceSelect::Flagged(nullptr, tmp, (const unsigned*)nullptr, (const unsigned char*)nullptr,
+                             (unsigned*)nullptr, (unsigned*)nullptr, (int)ns, h->stream);
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t o_sel = up(4 * ns), o_cnt = o_sel + up(4 * ns), o_flags = o_cnt + 256,
+               o_tmp = o_flags + up(ns), bytes = o_tmp + tmp;
+  if (bytes > h->region_bytes) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->region);
+    h->region = nullptr;
+    h->region_bytes = 0;
+    if ((rc = dalloc(h, &h->region, bytes)) != PCG_OK) return rc;
+    h->region_bytes = bytes;
+  }
+  unsigned* iota = (unsigned*)h->region;
+  unsigned* sel = (unsigned*)(h->region + o_sel);
+  unsigned* cnt = (unsigned*)(h->region + o_cnt);
+  unsigned char* flags = h->region + o_flags;
+  SpeciesF64 v64{};
+  const SpeciesF32Buffers* b32;
+  const SpeciesF64* s64;
+  region_views(h, s, &v64, &b32, &s64);
+  region_flags(h->g, b32, s64, ns, lo, hi, flags, h->stream);
+  iota_u32(iota, ns, h->stream);
+  cub::DeviceSelect::Flagged(h->region + o_tmp, tmp, iota, flags, sel, cnt, (int)ns, h->stream);
+  unsigned m = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&m, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  CUDA_TRY(h, cudaGetLastError());
+  *n = m;
+  if (cap < m) return fail(h, PCG_ERR_CAPACITY, "export buffer too small");
+  if (m == 0) return PCG_OK;
+  if (h->region_out_n < m) {
+    cudaFree(h->region_out);
+    h->region_out = nullptr;
+    h->region_out_n = 0;
+    if ((rc = dalloc(h, &h->region_out, 6 * (size_t)m)) != PCG_OK) return rc;
+    h->region_out_n = m;
+  }
+  region_gather(h->g, b32, s64, sel, m, h->region_out, h->stream);
+  double* dst[6] = {r, z, vr, vphi, vz, w};
+  for (int a = 0; a < 6; ++a)
+    if (dst[a])
+      CUDA_TRY(h, cudaMemcpyAsync(dst[a], h->region_out + (size_t)a * m, sizeof(double) * m, cudaMemcpyDeviceToHost,
+                                  h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return PCG_OK;
+}
+
+int pcg_keep_species_range(pcg_handle* h, int slot, double lo, double hi) {
+  if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  if (std::isnan(lo) || std::isnan(hi)) return fail(h, PCG_ERR_ARG, "NaN band limit");
+  Species& s = h->sp[slot];
+  SpeciesF64 v64{};
+  const SpeciesF32Buffers* b32;
+  const SpeciesF64* s64;
+  region_views(h, s, &v64, &b32, &s64);
+  region_keep(h->g, b32, s64, s.n, lo, hi, h->d_status, h->stream);
+  CUDA_TRY(h, cudaGetLastError());
   return PCG_OK;
 }
 

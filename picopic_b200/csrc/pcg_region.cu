@@ -1,0 +1,103 @@
+// pcg_region.cu — particles of a species within a band of z: selected,
+// copied out, or all others removed.  The exchange of a run split into
+// z-slabs (picopic_b200/slabs.py) moves only the particles near a slab's
+// ends this way, in place of the reference's particle hand-over between
+// domains (SMB::particles_runaway_collector, SMB.cpp:194-564).
+#include <cuda_runtime.h>
+
+#include "pcg_f32.h"
+#include "pcg_kernels.h"
+#include "pcg_region.h"
+
+namespace pcg {
+namespace {
+
+constexpr int kThreads = 256;
+inline unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+// z of slot j (float layout: cell and offset, as an export computes it)
+__device__ __forceinline__ bool slot_z(const GridGeom& g, const SpeciesF32Buffers* b, const SpeciesF64* s,
+                                       size_t j, double* z) {
+  if (b) {
+    const int c = b->cell[j];
+    if (c < 0) return false;
+    *z = ((double)cell_z_of(c) + (double)b->off_z[j]) * g.dz;
+    return true;
+  }
+  if (!(s->r[j] >= 0.0)) return false;
+  *z = s->z[j];
+  return true;
+}
+
+__global__ void flags_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, int f32, size_t n, double lo,
+                             double hi, unsigned char* flags) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double z;
+  const bool live = slot_z(g, f32 ? &b32 : nullptr, &s64, j, &z);
+  flags[j] = live && z >= lo && z < hi ? 1 : 0;
+}
+
+// out: 6 x m doubles (r, z, v_r, v_phi, v_z, w) of the slots idx[0..m)
+__global__ void gather_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, int f32, const unsigned* idx,
+                              size_t m, double* out) {
+  const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (q >= m) return;
+  const size_t j = idx[q];
+  if (f32) {
+    const int c = b32.cell[j];
+    out[q] = ((double)cell_r_of(c) + (double)b32.off_r[j]) * g.dr;
+    out[m + q] = ((double)cell_z_of(c) + (double)b32.off_z[j]) * g.dz;
+    out[2 * m + q] = b32.vr[j];
+    out[3 * m + q] = b32.vphi[j];
+    out[4 * m + q] = b32.vz[j];
+    out[5 * m + q] = b32.w[j];
+  } else {
+    out[q] = s64.r[j];
+    out[m + q] = s64.z[j];
+    out[2 * m + q] = s64.vr[j];
+    out[3 * m + q] = s64.vphi[j];
+    out[4 * m + q] = s64.vz[j];
+    out[5 * m + q] = s64.w[j];
+  }
+}
+
+// Live slots outside [lo, hi) become dead slots (counted as dead, not as
+// removed by the runaway collector).
+__global__ void keep_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, int f32, size_t n, double lo,
+                            double hi, DevStatus* st) {
+  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  double z;
+  const bool drop = j < n && slot_z(g, f32 ? &b32 : nullptr, &s64, j, &z) && !(z >= lo && z < hi);
+  if (drop) {
+    if (f32) b32.cell[j] = kDeadCell;
+    else s64.r[j] = -1.0;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, drop);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(&st->dead_slots, (unsigned long long)__popc(m));
+}
+
+}  // namespace
+
+void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
+                  double hi, unsigned char* flags, cudaStream_t s) {
+  if (!n) return;
+  flags_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b32 ? *b32 : SpeciesF32Buffers{}, s64 ? *s64 : SpeciesF64{},
+                                                   b32 ? 1 : 0, n, lo, hi, flags);
+}
+
+void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, const unsigned* idx,
+                   size_t m, double* out, cudaStream_t s) {
+  if (!m) return;
+  gather_kernel<<<blocks_for(m), kThreads, 0, s>>>(g, b32 ? *b32 : SpeciesF32Buffers{}, s64 ? *s64 : SpeciesF64{},
+                                                    b32 ? 1 : 0, idx, m, out);
+}
+
+void region_keep(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
+                 double hi, DevStatus* st, cudaStream_t s) {
+  if (!n) return;
+  keep_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b32 ? *b32 : SpeciesF32Buffers{}, s64 ? *s64 : SpeciesF64{},
+                                                  b32 ? 1 : 0, n, lo, hi, st);
+}
+
+}  // namespace pcg

@@ -1,0 +1,26 @@
+// pcg_region.h — band-of-z particle selection (pcg_region.cu), shared by
+// pcg_export_species_range and pcg_keep_species_range.  Exactly one of b32
+// (float layout) and s64 (double layout) is non-null.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "pcg_common.cuh"
+#include "pcg_f32.h"
+#include "pcg_kernels.h"
+
+namespace pcg {
+
+// flags[j] = 1 for the live slots j < n with lo <= z < hi
+void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
+                  double hi, unsigned char* flags, cudaStream_t s);
+// out: r, z, v_r, v_phi, v_z, w of the slots idx[0..m), m doubles apart
+void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, const unsigned* idx,
+                   size_t m, double* out, cudaStream_t s);
+// marks the live slots outside [lo, hi) dead and counts them in st->dead_slots
+void region_keep(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
+                 double hi, DevStatus* st, cudaStream_t s);
+
+}  // namespace pcg

@@ -193,6 +193,46 @@ class Domain:
     def fields(self) -> dict:
         return {n: self.get_field(n) for n in FIELDS}
 
+    def get_field_columns(self, which, c0, c1) -> np.ndarray:
+        """Array columns [c0, c1) of a field: (nr+4) x (c1-c0)."""
+        idx = FIELD[which] if isinstance(which, str) else int(which)
+        a = np.zeros((self.grid.shape[0], max(c1 - c0, 0)))
+        self._check(self.lib.pcg_get_field_columns(self.h, idx, int(c0), int(c1), _dp(a)),
+                    "pcg_get_field_columns")
+        return a
+
+    def set_field_columns(self, which, c0, arr):
+        """Array columns [c0, c0 + arr.shape[1]) of a field from arr."""
+        idx = FIELD[which] if isinstance(which, str) else int(which)
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.ndim != 2 or a.shape[0] != self.grid.shape[0]:
+            raise ValueError(f"field {which!r}: columns of shape {a.shape}, rows must be {self.grid.shape[0]}")
+        self._check(self.lib.pcg_set_field_columns(self.h, idx, int(c0), int(c0) + a.shape[1], _dp(a)),
+                    "pcg_set_field_columns")
+
+    # -- particles in a band of z (hand-over between domains split along z) --------
+    def export_range(self, slot, lo, hi) -> dict:
+        """The live particles with lo <= z < hi, in slot order."""
+        keys = ("r", "z", "vr", "vphi", "vz", "w")
+        n = ctypes.c_size_t()
+        null = [None] * 6
+        rc = self.lib.pcg_export_species_range(self.h, slot, float(lo), float(hi), 0, *null, ctypes.byref(n))
+        if rc == 0:
+            return {k: np.zeros(0) for k in keys}
+        if rc != -5:  # PCG_ERR_CAPACITY: the count is set
+            self._check(rc, "pcg_export_species_range")
+        m = n.value
+        out = {k: np.zeros(m) for k in keys}
+        self._check(self.lib.pcg_export_species_range(self.h, slot, float(lo), float(hi), m,
+                                                      *[_dp(out[k]) for k in keys], ctypes.byref(n)),
+                    "pcg_export_species_range")
+        return {k: v[:n.value] for k, v in out.items()}
+
+    def keep_range(self, slot, lo, hi):
+        """Remove the live particles outside lo <= z < hi."""
+        self._check(self.lib.pcg_keep_species_range(self.h, slot, float(lo), float(hi)),
+                    "pcg_keep_species_range")
+
     def collide(self) -> int:
         """One binary-collision pass (Perez 2012, CollisionsP12::operator());
         returns the number of pair collisions attempted."""

@@ -17,18 +17,20 @@ with ghost >= 4 the slab's own cells come out as the undivided run's do
 (to the order of floating-point sums).  After every step the ghost cells
 are overwritten from the slabs that own them: the twelve field arrays (E,
 the time-centred H, H at integer time, J) column by column, and the
-particles: a slab keeps the particles whose z lies in its own cells and
-takes copies of its neighbours' particles in its ghost cells.  A particle
-moves less than a cell per step, so a particle that crosses into a
-neighbour was already there as a copy, pushed with the same fields; the
-slab that owns its new position keeps it.
+particles.  Each species has two slots in a slab's domain: the particles
+the slab owns and the ghost copies of its neighbours' particles, pushed
+alongside (with the same fields, so they deposit the same currents into
+the own cells near the boundary).  After a step the owner hands the own
+particles that left its cells to the neighbour (a particle moves less than
+a cell per step, so only to a neighbour) and then sends copies of the own
+particles in the neighbours' ghost cells, which replace their ghost slots.
 
 Only the end slabs keep the run's PML at their outer ends and only the
 first injects beams (at z = 0).  :class:`SlabGroup` holds every slab in
 one process (several domains on one GPU, or one per GPU); :class:`SlabRank`
-holds one slab per process and exchanges the ghost strips with its
-neighbours through ``torch.distributed`` point-to-point messages of host
-tensors (a gloo group).
+holds one slab per process and exchanges the strips with its neighbours
+through ``torch.distributed`` point-to-point messages of host tensors (a
+gloo group).
 """
 from __future__ import annotations
 
@@ -95,6 +97,18 @@ def slab_geometry(grid, slab: Slab):
     return dataclasses.replace(grid, nz=slab.nz, longitude=slab.nz * grid.dz, pml_size=tuple(pml))
 
 
+@dataclasses.dataclass(frozen=True)
+class GhostSpecies:
+    """The ghost copies of a species in a slab's domain: the species'
+    charge and mass, no injection (what ``add`` of a domain reads)."""
+    name: str
+    charge: float
+    mass: float
+    id: int = 0
+    capacity: int | None = None
+    beam: None = None
+
+
 def _owned(z, slab: Slab, dz):
     lo = -np.inf if slab.first else slab.k0 * dz
     hi = np.inf if slab.last else slab.k1 * dz
@@ -108,32 +122,158 @@ def _strip(p, lo, hi):
 
 
 def _cat(parts):
+    parts = [p for p in parts if p is not None]
+    if not parts:
+        return {k: np.zeros(0) for k in PARTICLE_KEYS}
     return {k: np.concatenate([p[k] for p in parts]) for k in PARTICLE_KEYS}
 
 
+def _empty():
+    return {k: np.zeros(0) for k in PARTICLE_KEYS}
+
+
 class _SlabEngine:
-    """A slab's domain with global coordinates on the outside."""
+    """A slab's domain with global coordinates on the outside.
+
+    Species slot t < nsp holds the particles the slab owns (z in its own
+    cells, as this domain computes z); slot nsp + t holds the copies of the
+    neighbours' particles of species t in the ghost cells, replaced at every
+    exchange.  A particle's owner alone decides where it goes after a step,
+    with one computation of its z for both the hand-over and the keep, so
+    no particle is lost or doubled at a slab boundary, however close to it.
+    Band selections and column copies go through the domain's own
+    ``export_range``/``keep_range``/``get_field_columns``/
+    ``set_field_columns`` where it has them (a GPU domain: only the strips
+    cross to the host), else through whole-array copies."""
 
     def __init__(self, grid, slab: Slab, engine, species_count):
         self.grid, self.slab, self.engine, self.nsp = grid, slab, engine, species_count
-        self.z0 = slab.e0 * grid.dz  # global z of the domain's z = 0
+        dz = grid.dz
+        self.z0 = slab.e0 * dz  # global z of the domain's z = 0
+        # own cells in the domain's coordinates
+        self.lo = -np.inf if slab.first else (slab.k0 - slab.e0) * dz
+        self.hi = np.inf if slab.last else (slab.k1 - slab.e0) * dz
 
-    # particles in global z
-    def particles(self, slot):
-        p = self.engine.get_particles(slot)
+    # -- band selections, in the domain's coordinates --------------------------------
+    def _export(self, slot, lo, hi):
+        e = self.engine
+        if hasattr(e, "export_range"):
+            p = e.export_range(slot, lo, hi)
+        else:
+            q = e.get_particles(slot)
+            z = np.asarray(q["z"], dtype=np.float64)
+            m = (z >= lo) & (z < hi)
+            p = {k: np.asarray(q[k], dtype=np.float64)[m] for k in PARTICLE_KEYS}
         out = {k: np.asarray(p[k], dtype=np.float64) for k in PARTICLE_KEYS}
         out["z"] = out["z"] + self.z0
         return out
 
-    def set_particles(self, slot, p):
-        self.engine.set_particles(slot, p["r"], p["z"] - self.z0, p["vr"], p["vphi"], p["vz"], p["w"])
+    def _keep(self, slot, lo, hi):
+        e = self.engine
+        if hasattr(e, "keep_range"):
+            e.keep_range(slot, lo, hi)
+            return
+        q = e.get_particles(slot)
+        z = np.asarray(q["z"], dtype=np.float64)
+        m = (z >= lo) & (z < hi)
+        e.set_particles(slot, *[np.asarray(q[k], dtype=np.float64)[m] for k in PARTICLE_KEYS])
 
-    # field columns: global node k is local column k - e0 + 2
-    def local(self, name):
-        return self.engine.get_field(name)
+    def _put(self, slot, p, append):
+        arrs = [p[k] for k in PARTICLE_KEYS]
+        arrs[1] = p["z"] - self.z0
+        e = self.engine
+        if not append:
+            e.set_particles(slot, *arrs)
+        elif arrs[0].size:
+            if hasattr(e, "export_range"):  # a domain with pcg_append_species
+                e.set_particles(slot, *arrs, append=True)
+            else:
+                q = e.get_particles(slot)
+                e.set_particles(slot, *[np.concatenate([np.asarray(q[k], dtype=np.float64), a])
+                                        for k, a in zip(PARTICLE_KEYS, arrs)])
 
+    # -- the particle hand-over ---------------------------------------------------------
+    def migrants(self, t):
+        """Own particles that left the own cells (to the left, to the right),
+        global z; they are removed here."""
+        s = self.slab
+        left = None if s.first else self._export(t, -np.inf, self.lo)
+        right = None if s.last else self._export(t, self.hi, np.inf)
+        if not (s.first and s.last):
+            self._keep(t, self.lo, self.hi)
+        return left, right
+
+    def take(self, t, parts):
+        """Append the migrants that neighbours handed over."""
+        self._put(t, _cat(parts), append=True)
+
+    def strips(self, t, nl, nr):
+        """Copies of the own particles in the neighbours' ghost cells: the
+        first nl own cells (and anything further left) and the last nr."""
+        s, dz = self.slab, self.grid.dz
+        left = None if s.first else self._export(t, -np.inf, (s.k0 + nl - s.e0) * dz)
+        right = None if s.last else self._export(t, (s.k1 - nr - s.e0) * dz, np.inf)
+        return left, right
+
+    def set_ghosts(self, t, parts):
+        self._put(self.nsp + t, _cat(parts), append=False)
+
+    def own(self, t):
+        return self._export(t, -np.inf, np.inf)
+
+    # -- field columns: global node k is local column k - e0 + 2 -----------------------
     def col(self, k):
         return k - self.slab.e0 + 2
+
+    def columns(self, name, k0, k1):
+        e = self.engine
+        if hasattr(e, "get_field_columns"):
+            return e.get_field_columns(name, self.col(k0), self.col(k1))
+        return np.asarray(e.get_field(name))[:, self.col(k0):self.col(k1)].copy()
+
+    def set_columns(self, name, k0, a):
+        e = self.engine
+        if hasattr(e, "set_field_columns"):
+            e.set_field_columns(name, self.col(k0), a)
+            return
+        full = np.array(e.get_field(name), dtype=np.float64)
+        full[:, self.col(k0):self.col(k0) + a.shape[1]] = a
+        e.set_field(name, full)
+
+    def field_strips(self, nl, nr):
+        """The own columns of every field that the neighbours hold as ghosts."""
+        s = self.slab
+        left = None if s.first else {f: self.columns(f, s.k0, s.k0 + nl) for f in FIELDS}
+        right = None if s.last else {f: self.columns(f, s.k1 - nr, s.k1) for f in FIELDS}
+        return left, right
+
+    def set_ghost_fields(self, left, right):
+        s = self.slab
+        for f in FIELDS:
+            if left is not None:
+                self.set_columns(f, s.e0, left[f])
+            if right is not None:
+                self.set_columns(f, s.k1, right[f])
+
+    # -- set-up from global data ----------------------------------------------------------
+    def set_particles(self, t, p):
+        """Global particles: the own ones and the ghost copies."""
+        s, dz = self.slab, self.grid.dz
+        m = _owned(p["z"], s, dz)
+        g = ~m & (p["z"] >= s.e0 * dz) & (p["z"] < s.e1 * dz)
+        self._put(t, {k: p[k][m] for k in PARTICLE_KEYS}, append=False)
+        self._put(self.nsp + t, {k: p[k][g] for k in PARTICLE_KEYS}, append=False)
+
+    def set_field(self, name, a):
+        """The domain's columns of a global (nr+4) x (nz+4) array (its halo
+        columns where the global array has them, zeros beyond)."""
+        s = self.slab
+        loc = np.zeros((a.shape[0], s.nz + 4))
+        for lc in range(s.nz + 4):
+            gk = lc + s.e0  # global array column
+            if 0 <= gk < a.shape[1]:
+                loc[:, lc] = a[:, gk]
+        self.engine.set_field(name, loc)
 
 
 def _ghost_widths(slabs):
@@ -141,44 +281,42 @@ def _ghost_widths(slabs):
     return [(s.k0 - s.e0, s.e1 - s.k1) for s in slabs]
 
 
+def _add_ghosts(engine, species, capacity):
+    for sp in species:
+        engine.add(GhostSpecies(sp.name + ".ghost", sp.charge, sp.mass, getattr(sp, "id", 0), capacity))
+
+
 class SlabGroup:
     """Every slab of the run in this process.
 
     make_engine(geometry, slab) returns a domain for the slab's geometry
-    with the run's species added in the same order (a beam with its
-    injection in the first slab only, plain in the others); the group sets
-    its particles and fields from global arrays and steps all slabs."""
+    with the run's species added in the given order (a beam with its
+    injection in the first slab only, plain in the others); the group adds
+    the ghost species after them, sets the slabs' particles and fields from
+    global arrays and steps all slabs."""
 
-    def __init__(self, grid, count, make_engine, species_count, ghost=6):
+    def __init__(self, grid, count, make_engine, species, ghost=6, ghost_capacity=None):
         self.grid = grid
         self.slabs = plan(grid.nz, count, ghost)
         self.widths = _ghost_widths(self.slabs)
-        self.nsp = species_count
-        self.parts = [_SlabEngine(grid, s, make_engine(slab_geometry(grid, s), s), species_count)
-                      for s in self.slabs]
+        self.nsp = len(species)
+        self.parts = []
+        for s in self.slabs:
+            e = make_engine(slab_geometry(grid, s), s)
+            _add_ghosts(e, species, ghost_capacity)
+            self.parts.append(_SlabEngine(grid, s, e, self.nsp))
 
     # -- set-up from global data ------------------------------------------------------
     def set_particles(self, slot, r, z, vr, vphi, vz, w):
         p = {"r": np.asarray(r, float), "z": np.asarray(z, float), "vr": np.asarray(vr, float),
              "vphi": np.asarray(vphi, float), "vz": np.asarray(vz, float), "w": np.asarray(w, float)}
         for se in self.parts:
-            s, dz = se.slab, self.grid.dz
-            lo = -np.inf if s.first else s.e0 * dz
-            hi = np.inf if s.last else s.e1 * dz
-            se.set_particles(slot, _strip(p, lo, hi))
+            se.set_particles(slot, p)
 
     def set_field(self, name, a):
-        """A global (nr+4) x (nz+4) array: each domain gets its columns, with
-        the halo columns the global array has (zeros beyond it)."""
         a = np.asarray(a, dtype=np.float64)
         for se in self.parts:
-            s = se.slab
-            loc = np.zeros((a.shape[0], s.nz + 4))
-            for lc in range(s.nz + 4):
-                gk = lc - 2 + s.e0 + 2  # global array column
-                if 0 <= gk < a.shape[1]:
-                    loc[:, lc] = a[:, gk]
-            se.engine.set_field(name, loc)
+            se.set_field(name, a)
 
     # -- stepping ------------------------------------------------------------------------
     def step(self, n=1):
@@ -187,38 +325,29 @@ class SlabGroup:
                 se.engine.step(1)
             self.exchange()
 
+    def _neighbour_widths(self, i):
+        s = self.slabs[i]
+        nl = 0 if s.first else self.widths[i - 1][1]  # the left slab's right ghost width
+        nr = 0 if s.last else self.widths[i + 1][0]   # the right slab's left ghost width
+        return nl, nr
+
     def exchange(self):
-        dz = self.grid.dz
-        fields = [{f: se.local(f) for f in FIELDS} for se in self.parts]
-        owned = []
-        for se in self.parts:
-            slots = []
-            for t in range(self.nsp):
-                p = se.particles(t)
-                m = _owned(p["z"], se.slab, dz)
-                slots.append({k: p[k][m] for k in PARTICLE_KEYS})
-            owned.append(slots)
+        last = len(self.parts) - 1
+        # 1. owners hand over the particles that left their cells
+        mig = [[se.migrants(t) for t in range(self.nsp)] for se in self.parts]
         for i, se in enumerate(self.parts):
-            s = se.slab
-            lw, rw = self.widths[i]
-            # fields: ghost columns from the owners
-            for f in FIELDS:
-                a = fields[i][f]
-                if lw:
-                    src = self.parts[i - 1]
-                    a[:, se.col(s.e0):se.col(s.k0)] = fields[i - 1][f][:, src.col(s.e0):src.col(s.k0)]
-                if rw:
-                    src = self.parts[i + 1]
-                    a[:, se.col(s.k1):se.col(s.e1)] = fields[i + 1][f][:, src.col(s.k1):src.col(s.e1)]
-                se.engine.set_field(f, a)
-            # particles: own ones, then copies of the neighbours' in the ghost cells
             for t in range(self.nsp):
-                parts = [owned[i][t]]
-                if lw:
-                    parts.append(_strip(owned[i - 1][t], s.e0 * dz, s.k0 * dz))
-                if rw:
-                    parts.append(_strip(owned[i + 1][t], s.k1 * dz, s.e1 * dz))
-                se.set_particles(t, _cat(parts))
+                se.take(t, [mig[i - 1][t][1] if i > 0 else None, mig[i + 1][t][0] if i < last else None])
+        # 2. ghost columns and ghost particles from the owners
+        fs, ps = [], []
+        for i, se in enumerate(self.parts):
+            nl, nr = self._neighbour_widths(i)
+            fs.append(se.field_strips(nl, nr))
+            ps.append([se.strips(t, nl, nr) for t in range(self.nsp)])
+        for i, se in enumerate(self.parts):
+            se.set_ghost_fields(fs[i - 1][1] if i > 0 else None, fs[i + 1][0] if i < last else None)
+            for t in range(self.nsp):
+                se.set_ghosts(t, [ps[i - 1][t][1] if i > 0 else None, ps[i + 1][t][0] if i < last else None])
 
     # -- global views ------------------------------------------------------------------
     def get_field(self, name):
@@ -227,29 +356,23 @@ class SlabGroup:
         out = np.zeros((self.grid.nr + 4, self.grid.nz + 4))
         for se in self.parts:
             s = se.slab
-            a = se.local(name)
             lo = s.k0 - (2 if s.first else 0)
             hi = s.k1 + (2 if s.last else 0)
-            out[:, lo + 2:hi + 2] = a[:, se.col(lo):se.col(hi)]
+            out[:, lo + 2:hi + 2] = se.columns(name, lo, hi)
         return out
 
     def get_particles(self, slot):
         """The run's particles of a species: each slab's own (global z)."""
-        parts = []
-        for se in self.parts:
-            p = se.particles(slot)
-            m = _owned(p["z"], se.slab, self.grid.dz)
-            parts.append({k: p[k][m] for k in PARTICLE_KEYS})
-        return _cat(parts)
+        return _cat([se.own(slot) for se in self.parts])
 
 
 class SlabRank:
     """One slab per process: rank r of a torch.distributed group (host
-    tensors: a gloo group) holds slab r and exchanges the ghost strips
-    with ranks r - 1 and r + 1 after every step.  Every rank calls the same
-    methods in the same order."""
+    tensors: a gloo group) holds slab r and exchanges the migrants and the
+    ghost strips with ranks r - 1 and r + 1 after every step.  Every rank
+    calls the same methods in the same order."""
 
-    def __init__(self, grid, make_engine, species_count, group=None, ghost=6):
+    def __init__(self, grid, make_engine, species, group=None, ghost=6, ghost_capacity=None):
         import torch.distributed as dist
         self.dist, self.group = dist, group
         self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
@@ -257,9 +380,10 @@ class SlabRank:
         self.slabs = plan(grid.nz, self.size, ghost)
         self.widths = _ghost_widths(self.slabs)
         self.slab = self.slabs[self.rank]
-        self.nsp = species_count
-        self.se = _SlabEngine(grid, self.slab, make_engine(slab_geometry(grid, self.slab), self.slab),
-                              species_count)
+        self.nsp = len(species)
+        e = make_engine(slab_geometry(grid, self.slab), self.slab)
+        _add_ghosts(e, species, ghost_capacity)
+        self.se = _SlabEngine(grid, self.slab, e, self.nsp)
 
     # point-to-point of numpy arrays (shape known to both sides)
     def _send(self, a, peer):
@@ -280,27 +404,44 @@ class SlabRank:
     def _recv_particles(self, peer):
         n = int(self._recv((1,), peer)[0])
         if n == 0:
-            return {k: np.zeros(0) for k in PARTICLE_KEYS}
+            return _empty()
         a = self._recv((len(PARTICLE_KEYS), n), peer)
         return {k: a[q] for q, k in enumerate(PARTICLE_KEYS)}
 
+    def _swap(self, send_left, send_right, recv_left, recv_right):
+        """One exchange with both neighbours: even ranks send first, odd
+        ranks receive first, so no two ranks wait on each other."""
+        s = self.slab
+        left, right = self.rank - 1, self.rank + 1
+        got_l = got_r = None
+        if self.rank % 2 == 0:
+            if not s.last:
+                send_right(right)
+            if not s.first:
+                got_l = recv_left(left)
+            if not s.first:
+                send_left(left)
+            if not s.last:
+                got_r = recv_right(right)
+        else:
+            if not s.first:
+                got_l = recv_left(left)
+            if not s.last:
+                send_right(right)
+            if not s.last:
+                got_r = recv_right(right)
+            if not s.first:
+                send_left(left)
+        return got_l, got_r
+
     def set_particles(self, slot, r, z, vr, vphi, vz, w):
         """Global arrays (the same on every rank): the slab keeps its own and ghost ones."""
-        s, dz = self.slab, self.grid.dz
         p = {"r": np.asarray(r, float), "z": np.asarray(z, float), "vr": np.asarray(vr, float),
              "vphi": np.asarray(vphi, float), "vz": np.asarray(vz, float), "w": np.asarray(w, float)}
-        lo = -np.inf if s.first else s.e0 * dz
-        hi = np.inf if s.last else s.e1 * dz
-        self.se.set_particles(slot, _strip(p, lo, hi))
+        self.se.set_particles(slot, p)
 
     def set_field(self, name, a):
-        s = self.slab
-        loc = np.zeros((a.shape[0], s.nz + 4))
-        for lc in range(s.nz + 4):
-            gk = lc + s.e0
-            if 0 <= gk < a.shape[1]:
-                loc[:, lc] = a[:, gk]
-        self.se.engine.set_field(name, loc)
+        self.se.set_field(name, np.asarray(a, dtype=np.float64))
 
     def step(self, n=1):
         for _ in range(n):
@@ -308,85 +449,50 @@ class SlabRank:
             self.exchange()
 
     def exchange(self):
-        s, se, dz = self.slab, self.se, self.grid.dz
+        s, se, nsp = self.slab, self.se, self.nsp
         lw, rw = self.widths[self.rank]
-        fields = {f: se.local(f) for f in FIELDS}
-        owned = []
-        for t in range(self.nsp):
-            p = se.particles(t)
-            m = _owned(p["z"], s, dz)
-            owned.append({k: p[k][m] for k in PARTICLE_KEYS})
-        # the strips each neighbour needs: its ghost columns are these own columns
-        left, right = self.rank - 1, self.rank + 1
-        nl = self.widths[left][1] if not s.first else 0    # the left slab's right ghost width
-        nr = self.widths[right][0] if not s.last else 0    # the right slab's left ghost width
         rows = self.grid.nr + 4
-        # even ranks send first, odd ranks receive first: no two ranks wait on each other
-        def to_left():
-            for f in FIELDS:
-                self._send(fields[f][:, se.col(s.k0):se.col(s.k0 + nl)], left)
-            for t in range(self.nsp):
-                self._send_particles(_strip(owned[t], s.k0 * dz, (s.k0 + nl) * dz), left)
+        # 1. migrants
+        mig = [se.migrants(t) for t in range(nsp)]
+        got_l, got_r = self._swap(
+            lambda peer: [self._send_particles(mig[t][0], peer) for t in range(nsp)],
+            lambda peer: [self._send_particles(mig[t][1], peer) for t in range(nsp)],
+            lambda peer: [self._recv_particles(peer) for _ in range(nsp)],
+            lambda peer: [self._recv_particles(peer) for _ in range(nsp)])
+        for t in range(nsp):
+            se.take(t, [got_l[t] if got_l else None, got_r[t] if got_r else None])
+        # 2. ghost columns and ghost particles
+        nl = 0 if s.first else self.widths[self.rank - 1][1]
+        nr = 0 if s.last else self.widths[self.rank + 1][0]
+        fl, fr = se.field_strips(nl, nr)
+        ps = [se.strips(t, nl, nr) for t in range(nsp)]
 
-        def to_right():
-            for f in FIELDS:
-                self._send(fields[f][:, se.col(s.k1 - nr):se.col(s.k1)], right)
-            for t in range(self.nsp):
-                self._send_particles(_strip(owned[t], (s.k1 - nr) * dz, s.k1 * dz), right)
+        def send(fields, side):
+            def go(peer):
+                for f in FIELDS:
+                    self._send(fields[f], peer)
+                for t in range(nsp):
+                    self._send_particles(ps[t][side], peer)
+            return go
 
-        got_left = got_right = None
+        def recv(width):
+            def go(peer):
+                f_ = {f: self._recv((rows, width), peer) for f in FIELDS}
+                return f_, [self._recv_particles(peer) for _ in range(nsp)]
+            return go
 
-        def from_left():
-            f_ = {f: self._recv((rows, lw), left) for f in FIELDS}
-            return f_, [self._recv_particles(left) for _ in range(self.nsp)]
-
-        def from_right():
-            f_ = {f: self._recv((rows, rw), right) for f in FIELDS}
-            return f_, [self._recv_particles(right) for _ in range(self.nsp)]
-
-        # phase 1: left-to-right along the chain; phase 2: right-to-left
-        if self.rank % 2 == 0:
-            if not s.last:
-                to_right()
-            if not s.first:
-                got_left = from_left()
-            if not s.first:
-                to_left()
-            if not s.last:
-                got_right = from_right()
-        else:
-            if not s.first:
-                got_left = from_left()
-            if not s.last:
-                to_right()
-            if not s.last:
-                got_right = from_right()
-            if not s.first:
-                to_left()
-        for f in FIELDS:
-            a = fields[f]
-            if got_left is not None:
-                a[:, se.col(s.e0):se.col(s.k0)] = got_left[0][f]
-            if got_right is not None:
-                a[:, se.col(s.k1):se.col(s.e1)] = got_right[0][f]
-            se.engine.set_field(f, a)
-        for t in range(self.nsp):
-            parts = [owned[t]]
-            if got_left is not None:
-                parts.append(got_left[1][t])
-            if got_right is not None:
-                parts.append(got_right[1][t])
-            se.set_particles(t, _cat(parts))
+        got_l, got_r = self._swap(send(fl, 0), send(fr, 1), recv(lw), recv(rw))
+        se.set_ghost_fields(got_l[0] if got_l else None, got_r[0] if got_r else None)
+        for t in range(nsp):
+            se.set_ghosts(t, [got_l[1][t] if got_l else None, got_r[1][t] if got_r else None])
 
     def own_field_columns(self, name):
         """This slab's own columns of a field (the end slabs with their outer halo):
         (first global node, array)."""
-        s, se = self.slab, self.se
+        s = self.slab
         lo = s.k0 - (2 if s.first else 0)
         hi = s.k1 + (2 if s.last else 0)
-        return lo, se.local(name)[:, se.col(lo):se.col(hi)]
+        return lo, self.se.columns(name, lo, hi)
 
     def own_particles(self, slot):
-        p = self.se.particles(slot)
-        m = _owned(p["z"], self.slab, self.grid.dz)
-        return {k: p[k][m] for k in PARTICLE_KEYS}
+        return self.se.own(slot)

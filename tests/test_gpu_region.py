@@ -1,0 +1,110 @@
+"""Band-of-z particle selection and field column copies (pcg_export_species_range,
+pcg_keep_species_range, pcg_get_field_columns, pcg_set_field_columns) on
+both particle layouts, against the whole-array exports of the same domain.
+
+The band export must return exactly the particles of the whole export with
+lo <= z < hi (the same z: bit-equal), the keep must leave exactly those
+(the complement of the two side bands, so a hand-over neither loses nor
+doubles a particle), and an append beyond the capacity must succeed once
+the dead slots of a keep are reclaimed.
+"""
+import numpy as np
+import pytest
+
+from tests.cases import ELECTRONS, particles, random_fields, small_grid
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("r", "z", "vr", "vphi", "vz", "w")
+
+
+def _domain(grid, precision, cap=20000):
+    from picopic_b200 import Domain
+    d = Domain(grid, pusher="borisrel", current="vb", precision=precision, seed=7)
+    d.add(ELECTRONS, capacity=cap)
+    return d
+
+
+def _sorted(p):
+    order = np.lexsort((p["vz"], p["r"], p["z"]))
+    return {k: np.asarray(p[k])[order] for k in KEYS}
+
+
+def _equal(a, b):
+    a, b = _sorted(a), _sorted(b)
+    assert a["r"].size == b["r"].size
+    for k in KEYS:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_band_export_and_keep_split_the_particles(precision):
+    grid = small_grid(nr=16, nz=96)
+    d = _domain(grid, precision)
+    p = particles(grid, 12000, 11)
+    d.set_particles(0, *p)
+    for name, a in random_fields(grid, 2).items():
+        d.set_field(name, a)
+    d.step(3)  # float layout: tile-sorted, with dead slots of the runaways
+    whole = d.get_particles(0)
+    z = whole["z"]
+    lo, hi = 31 * grid.dz, 64.5 * grid.dz
+    band = d.export_range(0, lo, hi)
+    m = (z >= lo) & (z < hi)
+    _equal(band, {k: whole[k][m] for k in KEYS})
+    left, right = d.export_range(0, -np.inf, lo), d.export_range(0, hi, np.inf)
+    assert left["r"].size + band["r"].size + right["r"].size == z.size
+    assert d.export_range(0, hi, lo)["r"].size == 0
+    d.keep_range(0, lo, hi)
+    assert d.count(0) == m.sum()
+    _equal(d.get_particles(0), {k: whole[k][m] for k in KEYS})
+    # the kept particles step on: the same as a domain given only them
+    ref = _domain(grid, precision)
+    ref.set_particles(0, *[whole[k][m] for k in KEYS])
+    for name in random_fields(grid, 2):
+        ref.set_field(name, d.get_field(name))
+    d.step(2)
+    ref.step(2)
+    a, b = _sorted(d.get_particles(0)), _sorted(ref.get_particles(0))
+    assert a["r"].size == b["r"].size
+    tol = 1e-12 if precision == "f64" else 1e-6  # the deposit adds in another order
+    for k in KEYS:
+        np.testing.assert_allclose(a[k], b[k], rtol=0, atol=tol * np.abs(b[k]).max(), err_msg=k)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_append_reclaims_dead_slots_before_giving_up(precision):
+    grid = small_grid(nr=16, nz=96)
+    d = _domain(grid, precision, cap=4000)
+    p = particles(grid, 4000, 5)
+    d.set_particles(0, *p)
+    d.keep_range(0, 0.0, grid.longitude / 2)
+    live = int((p[1] < grid.longitude / 2).sum())  # no count(): it would compact
+    extra = particles(grid, 4000 - live, 6)
+    d.set_particles(0, *extra, append=True)
+    assert d.count(0) == 4000
+    from picopic_b200._ffi import PcgError
+    with pytest.raises(PcgError):
+        d.set_particles(0, *particles(grid, 1, 7), append=True)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_field_columns(precision):
+    grid = small_grid(nr=16, nz=96)
+    d = _domain(grid, precision)
+    fields = random_fields(grid, 4)
+    for name, a in fields.items():
+        d.set_field(name, a)
+    rng = np.random.default_rng(1)
+    for name, a in fields.items():
+        whole = d.get_field(name)
+        for c0, c1 in ((0, 5), (40, 52), (grid.nz - 2, grid.nz + 4)):
+            np.testing.assert_array_equal(d.get_field_columns(name, c0, c1), whole[:, c0:c1])
+        new = rng.normal(size=(grid.nr + 4, 7))
+        d.set_field_columns(name, 20, new)
+        expect = whole.copy()
+        expect[:, 20:27] = new if precision == "f64" else new.astype(np.float32)
+        np.testing.assert_array_equal(d.get_field(name), expect)
+    from picopic_b200._ffi import PcgError
+    with pytest.raises(PcgError):
+        d.get_field_columns("e_r", 90, grid.nz + 5)

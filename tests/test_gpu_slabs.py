@@ -55,7 +55,7 @@ def test_gpu_slabs_equal_the_undivided_run(precision, quirks, count):
               for s in species]
         return _domain(geometry, precision, quirks, sp)
 
-    g = S.SlabGroup(grid, count, make, len(species))
+    g = S.SlabGroup(grid, count, make, species)
     whole = _domain(grid, precision, quirks, species)
     parts, fields = _inputs(grid)
     for i, p in parts.items():

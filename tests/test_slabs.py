@@ -2,8 +2,8 @@
 run undivided, on the CPU oracle as the slabs' engine.
 
 Every slab is an ordinary domain over its cells plus ghost cells; after each
-step the ghost cells' fields and particles come from the slabs that own
-them.  The slabs' own cells must then hold what the undivided run holds:
+step the owners hand over the particles that left their cells, and the
+ghost cells' fields and particles come from the slabs that own them.  The slabs' own cells must then hold what the undivided run holds:
 the twelve field arrays within 1e-10 of each array's largest value (the
 deposit sums the same currents in another particle order) and the same
 particles.  With one slab per process the strips go through
@@ -43,7 +43,7 @@ def _engine_factory(grid, quirks):
             o.add(sp if (slab.first or sp.beam is None) else _plain(sp))
         o.set_rng("philox", 7)
         return o
-    return make, len(species)
+    return make, species
 
 
 def _inputs(grid):
@@ -103,8 +103,9 @@ def test_plan_covers_the_grid():
 @pytest.mark.parametrize("count,quirks", [(2, "fixed"), (3, "reference")])
 def test_slabs_equal_the_undivided_run(count, quirks):
     grid = small_grid(nr=16, nz=96)
-    make, nsp = _engine_factory(grid, quirks)
-    g = S.SlabGroup(grid, count, make, nsp)
+    make, species = _engine_factory(grid, quirks)
+    nsp = len(species)
+    g = S.SlabGroup(grid, count, make, species)
     parts, fields = _inputs(grid)
     for i, p in parts.items():
         g.set_particles(i, *p)
@@ -123,8 +124,9 @@ def _rank_main(rank, world, port, out_dir, quirks):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         grid = small_grid(nr=16, nz=96)
-        make, nsp = _engine_factory(grid, quirks)
-        r = S.SlabRank(grid, make, nsp)
+        make, species = _engine_factory(grid, quirks)
+        nsp = len(species)
+        r = S.SlabRank(grid, make, species)
         parts, fields = _inputs(grid)
         for i, p in parts.items():
             r.set_particles(i, *p)
@@ -165,3 +167,41 @@ def test_one_slab_per_gloo_rank(world, tmp_path):
             parts[t].append({k: d[f"p{t}_{k}"] for k in S.PARTICLE_KEYS})
     merged = [{k: np.concatenate([p[k] for p in parts[t]]) for k in S.PARTICLE_KEYS} for t in range(nsp)]
     _compare(fields, merged, _whole(grid, quirks), nsp)
+
+
+def test_particles_at_slab_boundaries_are_handed_over_once():
+    """Particles on and within a few ulp of the slab boundaries, crossing them
+    both ways: after every step each is owned by exactly one slab, and the
+    run ends as the undivided one does."""
+    grid = small_grid(nr=16, nz=96)
+    species = [ELECTRONS]
+    make = lambda geometry, slab: _single(geometry)
+    g = S.SlabGroup(grid, 3, make, species)
+    rng = np.random.default_rng(3)
+    faces = np.array([sl.k0 for sl in g.slabs[1:]], dtype=float) * grid.dz
+    z = np.concatenate([[np.nextafter(f, -np.inf), f, np.nextafter(f, np.inf)] for f in faces] +
+                       [f + grid.dz * np.array([-1e-9, 1e-9, -0.3, 0.3]) for f in faces])
+    n = z.size * 20
+    z = np.repeat(z, 20)
+    r = grid.dr * (1.5 + rng.random(n) * (grid.nr - 3))
+    vz = rng.choice([-1.0, 1.0], size=n) * (0.02 + 0.9 * rng.random(n)) * grid.dz / grid.dt
+    p = (r, z, rng.normal(size=n) * 1e5, rng.normal(size=n) * 1e5, vz, np.full(n, 1e5))
+    g.set_particles(0, *p)
+    whole = _single(grid)
+    whole.set_particles(0, *p)
+    for _ in range(STEPS):
+        g.step(1)
+        whole.step(1)
+        own = g.get_particles(0)
+        assert own["r"].size == whole.count(0) == n
+    b = _sorted(whole.get_particles(0))
+    a = _sorted(g.get_particles(0))
+    for k in S.PARTICLE_KEYS:
+        assert _rel(a[k], b[k]) <= RTOL, k
+
+
+def _single(geometry):
+    o = OracleSim(geometry, "borisrel", "vb", quirks="fixed")
+    o.add(ELECTRONS)
+    o.set_rng("philox", 7)
+    return o
