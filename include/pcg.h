@@ -503,6 +503,26 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
                              double* z, double* vr, double* vphi, double* vz, double* w, size_t* n);
 int pcg_keep_species_range(pcg_handle* h, int slot, double lo, double hi);
 
+/* The same hand-over from one handle to another on the device, with only
+ * counts crossing to the host; the handles may be on one GPU or on two (a
+ * peer copy, over NVLink where the GPUs reach each other).
+ * pcg_transfer_species_range selects src's live particles of `slot` with
+ * lo <= z < hi as pcg_export_species_range does, subtracts `shift` from
+ * their z (dst's coordinates), and appends them to dst's species dst_slot
+ * (append = 1; dead slots are reclaimed first as pcg_append_species does)
+ * or replaces that species' particles with them (append = 0); *n = their
+ * count.  It waits for src's queued work (the selection's count), not for
+ * dst's.  pcg_copy_field_columns copies the array columns [c0, c1) of
+ * src's field `which` (PCG_FIELD_ALL: all twelve) into dst's columns
+ * [g0, g0 + c1 - c0); both handles need the same precision and nr.  In
+ * both, the copy runs after the work queued on both handles before the
+ * call, and the work queued on either after the call runs after the copy;
+ * the host does not wait for it. */
+#define PCG_FIELD_ALL (-1)
+int pcg_transfer_species_range(pcg_handle* src, int slot, double lo, double hi, double shift,
+                               pcg_handle* dst, int dst_slot, int append, size_t* n);
+int pcg_copy_field_columns(pcg_handle* src, int which, int c0, int c1, pcg_handle* dst, int g0);
+
 int pcg_stage(pcg_handle* h, int stage);
 int pcg_step(pcg_handle* h, int nsteps);
 int pcg_synchronize(pcg_handle* h);
@@ -519,6 +539,10 @@ int pcg_step_status(pcg_handle* h);
 int pcg_diag(pcg_handle* h, pcg_diagnostics* out);
 /* The handle's cudaStream_t, for callers that time or order work on it. */
 int pcg_get_stream(pcg_handle* h, void** stream);
+/* The handle's GPU (pcg_config.device).  Every call on a handle runs with
+ * that GPU current and restores the caller's current device on return, so
+ * one host thread may drive handles on several GPUs. */
+int pcg_get_device(pcg_handle* h, int* device);
 
 #ifdef __cplusplus
 }

@@ -70,6 +70,10 @@ SIGNATURES = {
     "pcg_export_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D, ctypes.c_size_t] + [_PD] * 6 +
                                  [ctypes.POINTER(ctypes.c_size_t)]),
     "pcg_keep_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D]),
+    "pcg_transfer_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D, _D, _H, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(ctypes.c_size_t)]),
+    "pcg_copy_field_columns": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, _H, ctypes.c_int]),
+    "pcg_get_device": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),
     "pcg_stage": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_step": (ctypes.c_int, [_H, ctypes.c_int]),
     "pcg_synchronize": (ctypes.c_int, [_H]),

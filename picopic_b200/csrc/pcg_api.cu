@@ -16,6 +16,7 @@
 
 #include "pcg.h"
 #include "pcg_collide.h"
+#include "pcg_device.h"
 #include "pcg_diag.h"
 #include "pcg_f32.h"
 #include "pcg_init.h"
@@ -72,6 +73,8 @@ struct pcg_handle {
   // pcg_step_status: the status block of the last step, copied without waiting
   DevStatus* h_status_lag = nullptr;
   cudaEvent_t ev_status = nullptr;
+  // device-to-device hand-over between handles: orders the two streams
+  cudaEvent_t ev_region = nullptr;
   bool status_pending = false;
   DevStatus* d_status = nullptr;
   DevStatus* h_status = nullptr;  // pinned mirror
@@ -153,6 +156,7 @@ int dalloc(pcg_handle* h, T** p, size_t count) {
 }
 
 bool is_f64(const pcg_handle* h) { return h->cfg.precision == PCG_PRECISION_F64; }
+
 
 // PML profiles of MaxwellSolverYee::set_pml (maxwellSolverYee.cpp:57-109):
 // each wall adds a quadratic ramp that depends on i alone (r=R) or k alone
@@ -745,7 +749,13 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PCG_ERR_CUDA;
   if (cfg->device < 0 || cfg->device >= ndev) return PCG_ERR_ARG;
+  int prev_device = 0;
+  if (cudaGetDevice(&prev_device) != cudaSuccess) return PCG_ERR_CUDA;
   if (cudaSetDevice(cfg->device) != cudaSuccess) return PCG_ERR_CUDA;
+  struct Restore {  // the caller's device is current again on return
+    int d;
+    ~Restore() { cudaSetDevice(d); }
+  } restore{prev_device};
   pcg_handle* h = new pcg_handle();
   h->cfg = *cfg;
   GridGeom& g = h->g;
@@ -765,6 +775,7 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
       cudaEventCreateWithFlags(&h->ev_copied, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_staging_free, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_status, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_region, cudaEventDisableTiming) != cudaSuccess ||
       cudaMallocHost((void**)&h->h_status_lag, sizeof(DevStatus)) != cudaSuccess)
     return bail(PCG_ERR_CUDA);
   if (cfg->precision == PCG_PRECISION_F32 &&
@@ -823,6 +834,7 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
 }
 
 int pcg_destroy(pcg_handle* h) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (int c = 0; c < 12; ++c) cudaFree(h->f64[c]);
@@ -858,6 +870,7 @@ int pcg_destroy(pcg_handle* h) {
   if (h->ev_copied) cudaEventDestroy(h->ev_copied);
   if (h->ev_staging_free) cudaEventDestroy(h->ev_staging_free);
   if (h->ev_status) cudaEventDestroy(h->ev_status);
+  if (h->ev_region) cudaEventDestroy(h->ev_region);
   if (h->h_status_lag) cudaFreeHost(h->h_status_lag);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->aux) cudaStreamDestroy(h->aux);
@@ -892,6 +905,7 @@ static int add_common(pcg_handle* h, int id, const char* name, double charge_e, 
 
 int pcg_add_species(pcg_handle* h, int id, const char* name, double charge_e, double mass_e,
                     size_t capacity, int* slot) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   Species* s = nullptr;
   return add_common(h, id, name, charge_e, mass_e, capacity, slot, &s);
 }
@@ -900,6 +914,7 @@ int pcg_add_beam(pcg_handle* h, int id, const char* name, double charge_e, doubl
                  size_t capacity, unsigned macro_amount, double start_time, double bunch_radius,
                  double density, double bunches_amount, double bunch_length,
                  double bunches_distance, double velocity, int* slot) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!(velocity > 0) || !(bunch_length > 0) || !(bunch_radius > 0) || bunches_amount < 1)
     return fail(h, PCG_ERR_ARG, "beam velocity, length, radius and bunch count must be positive");
   Species* s = nullptr;
@@ -967,15 +982,18 @@ static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, con
 
 int pcg_import_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
                        const double* vr, const double* vphi, const double* vz, const double* w) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   return put_particles(h, slot, n, r, z, vr, vphi, vz, w, false);
 }
 
 int pcg_append_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
                        const double* vr, const double* vphi, const double* vz, const double* w) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   return put_particles(h, slot, n, r, z, vr, vphi, vz, w, true);
 }
 
 int pcg_count(pcg_handle* h, int slot, size_t* n) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !n || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -987,6 +1005,7 @@ int pcg_count(pcg_handle* h, int slot, size_t* n) {
 int pcg_export_species(pcg_handle* h, int slot, size_t cap, double* r, double* z, double* vr,
                        double* vphi, double* vz, double* w, int32_t* cell_r, int32_t* cell_z,
                        size_t* n) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   size_t cnt = 0;
   int rc = pcg_count(h, slot, &cnt);
   if (rc != PCG_OK) return rc;
@@ -1017,6 +1036,7 @@ int pcg_export_species(pcg_handle* h, int slot, size_t cap, double* r, double* z
 }
 
 int pcg_set_field(pcg_handle* h, int which, const double* src) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !src || which < 0 || which >= 12) return PCG_ERR_ARG;
   if (is_f64(h)) {
     CUDA_TRY(h, cudaMemcpyAsync(h->f64[which], src, sizeof(double) * h->nodes, cudaMemcpyHostToDevice, h->stream));
@@ -1029,6 +1049,7 @@ int pcg_set_field(pcg_handle* h, int which, const double* src) {
 }
 
 int pcg_export_field(pcg_handle* h, int which, double* dst) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !dst || which < 0 || which >= 12) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1100,21 +1121,24 @@ void region_views(pcg_handle* h, Species& s, SpeciesF64* v64, const SpeciesF32Bu
 }  // namespace
 
 int pcg_get_field_columns(pcg_handle* h, int which, int c0, int c1, double* dst) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   return field_columns(h, which, c0, c1, dst, false);
 }
 
 int pcg_set_field_columns(pcg_handle* h, int which, int c0, int c1, const double* src) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   return field_columns(h, which, c0, c1, const_cast<double*>(src), true);
 }
 
-int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size_t cap, double* r,
-                             double* z, double* vr, double* vphi, double* vz, double* w, size_t* n) {
-  if (!h || !n || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
-  if (std::isnan(lo) || std::isnan(hi)) return fail(h, PCG_ERR_ARG, "NaN band limit");
-  *n = 0;
+namespace {
+
+// The live slots of species s with lo <= z < hi: their count in *m and
+// their indices in *sel (the handle's selection scratch).  Waits for the
+// handle's stream.
+int select_band(pcg_handle* h, Species& s, double lo, double hi, unsigned* m, const unsigned** sel) {
+  *m = 0;
   int rc = check_status(h);  // the steps queued before are done
   if (rc != PCG_OK) return rc;
-  Species& s = h->sp[slot];
   const size_t ns = s.n;
   if (ns == 0) return PCG_OK;
   if (ns > 0x7fffffffu) return fail(h, PCG_ERR_UNSUPPORTED, "a band selection of more than 2^31 slots");
@@ -1134,7 +1158,7 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
     h->region_bytes = bytes;
   }
   unsigned* iota = (unsigned*)h->region;
-  unsigned* sel = (unsigned*)(h->region + o_sel);
+  unsigned* out = (unsigned*)(h->region + o_sel);
   unsigned* cnt = (unsigned*)(h->region + o_cnt);
   unsigned char* flags = h->region + o_flags;
   SpeciesF64 v64{};
@@ -1143,22 +1167,54 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
   region_views(h, s, &v64, &b32, &s64);
   region_flags(h->g, b32, s64, ns, lo, hi, flags, h->stream);
   iota_u32(iota, ns, h->stream);
-  cub::DeviceSelect::Flagged(h->region + o_tmp, tmp, iota, flags, sel, cnt, (int)ns, h->stream);
-  unsigned m = 0;
-  CUDA_TRY(h, cudaMemcpyAsync(&m, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  cub::DeviceSelect::Flagged(h->region + o_tmp, tmp, iota, flags, out, cnt, (int)ns, h->stream);
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_status, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   CUDA_TRY(h, cudaGetLastError());
-  *n = m;
-  if (cap < m) return fail(h, PCG_ERR_CAPACITY, "export buffer too small");
+  std::memcpy(m, h->h_status, sizeof(unsigned));
+  *sel = out;
+  return PCG_OK;
+}
+
+// The m selected particles as 6 x m doubles (r, z - zshift, v_r, v_phi,
+// v_z, w) in the handle's region_out, queued on its stream.
+int gather_band(pcg_handle* h, Species& s, const unsigned* sel, unsigned m, double zshift) {
   if (m == 0) return PCG_OK;
   if (h->region_out_n < m) {
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     cudaFree(h->region_out);
     h->region_out = nullptr;
     h->region_out_n = 0;
-    if ((rc = dalloc(h, &h->region_out, 6 * (size_t)m)) != PCG_OK) return rc;
+    int rc = dalloc(h, &h->region_out, 6 * (size_t)m);
+    if (rc != PCG_OK) return rc;
     h->region_out_n = m;
   }
-  region_gather(h->g, b32, s64, sel, m, h->region_out, h->stream);
+  SpeciesF64 v64{};
+  const SpeciesF32Buffers* b32;
+  const SpeciesF64* s64;
+  region_views(h, s, &v64, &b32, &s64);
+  region_gather(h->g, b32, s64, sel, m, zshift, h->region_out, h->stream);
+  CUDA_TRY(h, cudaGetLastError());
+  return PCG_OK;
+}
+
+}  // namespace
+
+int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size_t cap, double* r,
+                             double* z, double* vr, double* vphi, double* vz, double* w, size_t* n) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
+  if (!h || !n || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
+  if (std::isnan(lo) || std::isnan(hi)) return fail(h, PCG_ERR_ARG, "NaN band limit");
+  *n = 0;
+  Species& s = h->sp[slot];
+  unsigned m = 0;
+  const unsigned* sel = nullptr;
+  int rc = select_band(h, s, lo, hi, &m, &sel);
+  if (rc != PCG_OK) return rc;
+  *n = m;
+  if (cap < m) return fail(h, PCG_ERR_CAPACITY, "export buffer too small");
+  if (m == 0) return PCG_OK;
+  if ((rc = gather_band(h, s, sel, m, 0.0)) != PCG_OK) return rc;
   double* dst[6] = {r, z, vr, vphi, vz, w};
   for (int a = 0; a < 6; ++a)
     if (dst[a])
@@ -1168,7 +1224,113 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
   return PCG_OK;
 }
 
+int pcg_transfer_species_range(pcg_handle* src, int slot, double lo, double hi, double shift, pcg_handle* dst,
+                               int dst_slot, int append, size_t* n) {
+  if (!src || !dst || !n || slot < 0 || slot >= (int)src->sp.size() || dst_slot < 0 ||
+      dst_slot >= (int)dst->sp.size())
+    return PCG_ERR_ARG;
+  if (std::isnan(lo) || std::isnan(hi) || !std::isfinite(shift)) return fail(src, PCG_ERR_ARG, "bad band or shift");
+  *n = 0;
+  unsigned m = 0;
+  int rc;
+  {  // select and gather on the source's GPU
+    DeviceScope on_src(src->cfg.device);
+    Species& s = src->sp[slot];
+    const unsigned* sel = nullptr;
+    if ((rc = select_band(src, s, lo, hi, &m, &sel)) != PCG_OK) return rc;
+    if ((rc = gather_band(src, s, sel, m, shift)) != PCG_OK) return rc;
+    CUDA_TRY(src, cudaEventRecord(src->ev_region, src->stream));
+  }
+  {  // copy and import on the destination's GPU, after the gather
+    DeviceScope on_dst(dst->cfg.device);
+    Species& d = dst->sp[dst_slot];
+    if (append && d.n + m > d.cap) {  // reclaim the dead slots first
+      if ((rc = check_status(dst)) != PCG_OK) return rc;
+      if (dst->h_status->dead_slots > dst->dead_dropped && (rc = compact(dst)) != PCG_OK) return rc;
+    }
+    const size_t n0 = append ? d.n : 0;
+    if (n0 + m > d.cap) return fail(dst, PCG_ERR_CAPACITY, "species '" + d.name + "' capacity exceeded");
+    dst->started = true;
+    if (m) {
+      if (dst->staging_n < m) {
+        CUDA_TRY(dst, cudaStreamSynchronize(dst->stream));
+        CUDA_TRY(dst, cudaStreamSynchronize(dst->copy));
+        cudaFree(dst->staging);
+        dst->staging = nullptr;
+        dst->staging_n = 0;
+        if ((rc = dalloc(dst, &dst->staging, 6 * (size_t)m)) != PCG_OK) return rc;
+        dst->staging_n = m;
+      }
+      CUDA_TRY(dst, cudaStreamWaitEvent(dst->stream, src->ev_region, 0));
+      // the staging buffer's last host upload has landed (put_particles waits for it)
+      const size_t bytes = sizeof(double) * 6 * (size_t)m;
+      if (src->cfg.device == dst->cfg.device)
+        CUDA_TRY(dst, cudaMemcpyAsync(dst->staging, src->region_out, bytes, cudaMemcpyDeviceToDevice, dst->stream));
+      else
+        CUDA_TRY(dst, cudaMemcpyPeerAsync(dst->staging, dst->cfg.device, src->region_out, src->cfg.device, bytes,
+                                          dst->stream));
+    }
+    // a replacement with no particles still resets the species (ids, tile grouping)
+    if (m || !append) {
+      if (is_f64(dst)) launch_import_f64(dst->g, view64(dst, d), n0, m, dst->staging, dst->stream);
+      else f32_launch_import(dst->g, d.f32, n0, m, dst->staging, dst->stream);
+    }
+    d.n = n0 + m;
+    CUDA_TRY(dst, cudaEventRecord(dst->ev_staging_free, dst->stream));
+    CUDA_TRY(dst, cudaEventRecord(dst->ev_region, dst->stream));
+    CUDA_TRY(dst, cudaGetLastError());
+  }
+  {  // the source's later gathers wait for the copy out of region_out
+    DeviceScope on_src(src->cfg.device);
+    CUDA_TRY(src, cudaStreamWaitEvent(src->stream, dst->ev_region, 0));
+  }
+  *n = m;
+  return PCG_OK;
+}
+
+int pcg_copy_field_columns(pcg_handle* src, int which, int c0, int c1, pcg_handle* dst, int g0) {
+  if (!src || !dst || which < PCG_FIELD_ALL || which >= 12) return PCG_ERR_ARG;
+  if (src->cfg.precision != dst->cfg.precision || src->g.nr != dst->g.nr)
+    return fail(dst, PCG_ERR_ARG, "field columns between handles of another precision or radial size");
+  if (c0 < 0 || c1 > src->g.ld || c0 >= c1 || g0 < 0 || g0 + (c1 - c0) > dst->g.ld)
+    return fail(dst, PCG_ERR_ARG, "field columns out of range");
+  {
+    DeviceScope on_src(src->cfg.device);
+    CUDA_TRY(src, cudaEventRecord(src->ev_region, src->stream));
+  }
+  {
+    DeviceScope on_dst(dst->cfg.device);
+    CUDA_TRY(dst, cudaStreamWaitEvent(dst->stream, src->ev_region, 0));
+    const size_t es = is_f64(dst) ? sizeof(double) : sizeof(float);
+    const size_t w = (size_t)(c1 - c0), rows = (size_t)dst->g.nr + 4;
+    const int f0 = which == PCG_FIELD_ALL ? 0 : which, f1 = which == PCG_FIELD_ALL ? 12 : which + 1;
+    for (int f = f0; f < f1; ++f) {
+      char* d = is_f64(dst) ? (char*)(dst->f64[f] + g0) : (char*)(dst->f32[f] + g0);
+      const char* s = is_f64(src) ? (const char*)(src->f64[f] + c0) : (const char*)(src->f32[f] + c0);
+      if (src->cfg.device == dst->cfg.device) {
+        CUDA_TRY(dst, cudaMemcpy2DAsync(d, es * dst->g.ld, s, es * src->g.ld, es * w, rows, cudaMemcpyDeviceToDevice,
+                                        dst->stream));
+      } else {
+        cudaMemcpy3DPeerParms p{};
+        p.srcPtr = make_cudaPitchedPtr(const_cast<char*>(s), es * src->g.ld, es * w, rows);
+        p.srcDevice = src->cfg.device;
+        p.dstPtr = make_cudaPitchedPtr(d, es * dst->g.ld, es * w, rows);
+        p.dstDevice = dst->cfg.device;
+        p.extent = make_cudaExtent(es * w, rows, 1);
+        CUDA_TRY(dst, cudaMemcpy3DPeerAsync(&p, dst->stream));
+      }
+    }
+    CUDA_TRY(dst, cudaEventRecord(dst->ev_region, dst->stream));
+  }
+  {
+    DeviceScope on_src(src->cfg.device);
+    CUDA_TRY(src, cudaStreamWaitEvent(src->stream, dst->ev_region, 0));
+  }
+  return PCG_OK;
+}
+
 int pcg_keep_species_range(pcg_handle* h, int slot, double lo, double hi) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   if (std::isnan(lo) || std::isnan(hi)) return fail(h, PCG_ERR_ARG, "NaN band limit");
   Species& s = h->sp[slot];
@@ -1194,6 +1356,7 @@ int diag_buffer(pcg_handle* h, double** out) {
 }  // namespace
 
 int pcg_node_charge(pcg_handle* h, double* q) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !q) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1211,6 +1374,7 @@ int pcg_node_charge(pcg_handle* h, double* q) {
 }
 
 int pcg_divergence(pcg_handle* h, int which, double* out) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !out || (which != PCG_FIELD_E_R && which != PCG_FIELD_J_R)) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1227,6 +1391,7 @@ int pcg_divergence(pcg_handle* h, int which, double* out) {
 
 
 int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1235,6 +1400,7 @@ int pcg_collide(pcg_handle* h, unsigned long long* pair_calls) {
 }
 
 int pcg_collide_expectation(pcg_handle* h, double* out) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !out) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1259,12 +1425,14 @@ int pcg_collide_expectation(pcg_handle* h, double* out) {
 }
 
 int pcg_set_collision_model(pcg_handle* h, const float* params, const float* norm) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !params || !norm) return PCG_ERR_ARG;
   if (learned_set_model(h->learned, params, norm, h->stream) != 0) return fail(h, PCG_ERR_NOMEM, "collision model");
   return PCG_OK;
 }
 
 int pcg_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsigned long long* fallback_cells) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   if (h->halted) return fail(h, PCG_ERR_TIMEOUT, "halted after a tensor-core time-out");
   int rc = check_status(h);
@@ -1285,6 +1453,7 @@ int extf_code(const char* name) {
 
 int pcg_set_external_fields(pcg_handle* h, const char* electric, const double* e_params, int n_e,
                             const char* magnetic, const double* m_params, int n_m) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   const bool fixed = h->cfg.quirks == PCG_QUIRKS_FIXED;
   int ec = extf_code(electric), mc = extf_code(magnetic);
@@ -1331,12 +1500,14 @@ int pcg_set_external_fields(pcg_handle* h, const char* electric, const double* e
 }
 
 int pcg_set_collision_crowding(pcg_handle* h, unsigned threshold) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   h->coll_crowded = threshold;
   return PCG_OK;
 }
 
 int pcg_set_collision_scheme(pcg_handle* h, int scheme) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || (scheme != PCG_COLLIDE_P12 && scheme != PCG_COLLIDE_TA77S && scheme != PCG_COLLIDE_SK98))
     return PCG_ERR_ARG;
   h->coll_scheme = scheme;
@@ -1344,6 +1515,7 @@ int pcg_set_collision_scheme(pcg_handle* h, int scheme) {
 }
 
 int pcg_set_collisions(pcg_handle* h, int mode) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || mode < PCG_COLLISIONS_NONE || mode > PCG_COLLISIONS_LEARNED) return PCG_ERR_ARG;
   if (mode == PCG_COLLISIONS_LEARNED && !h->learned.model)
     return fail(h, PCG_ERR_STATE, "no collision model: call pcg_set_collision_model");
@@ -1352,6 +1524,7 @@ int pcg_set_collisions(pcg_handle* h, int mode) {
 }
 
 int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_split) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || sort_interval < 0 || target_blocks < 0 || min_split < 0) return PCG_ERR_ARG;
   if (sort_interval) h->sort_interval = sort_interval;
   if (target_blocks) h->target_blocks = (unsigned)target_blocks;
@@ -1361,6 +1534,7 @@ int pcg_set_tiling(pcg_handle* h, int sort_interval, int target_blocks, int min_
 }
 
 int pcg_tile_sort(pcg_handle* h, int slot, unsigned* counts, unsigned long long* misplaced) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !counts || !misplaced || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   if (is_f64(h)) return fail(h, PCG_ERR_UNSUPPORTED, "the tile sort belongs to the float layout");
   int rc = check_status(h);
@@ -1389,6 +1563,7 @@ int pcg_tile_sort(pcg_handle* h, int slot, unsigned* counts, unsigned long long*
 }
 
 int pcg_species_map(pcg_handle* h, int slot, int which, double* out) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !out || slot < 0 || slot >= (int)h->sp.size() || which < PCG_MAP_DENSITY || which > PCG_MAP_MOMENTUM)
     return PCG_ERR_ARG;
   int rc = check_status(h);
@@ -1421,6 +1596,7 @@ int pcg_species_map(pcg_handle* h, int slot, int which, double* out) {
 }
 
 int pcg_cell_moments(pcg_handle* h, double* out) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !out) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1436,6 +1612,7 @@ int pcg_cell_moments(pcg_handle* h, double* out) {
 }
 
 int pcg_cell_features(pcg_handle* h, float* x, double* scale) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !x || !scale) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;
@@ -1464,6 +1641,7 @@ int pcg_cell_features(pcg_handle* h, float* x, double* scale) {
 }
 
 int pcg_stage(pcg_handle* h, int stage) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   if (stage < 0 || stage > PCG_STAGE_ADVANCE_TIME) return fail(h, PCG_ERR_ARG, "unknown stage");
   h->started = true;
@@ -1474,6 +1652,7 @@ int pcg_stage(pcg_handle* h, int stage) {
 }
 
 int pcg_step(pcg_handle* h, int nsteps) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || nsteps < 0) return PCG_ERR_ARG;
   if (h->halted) return fail(h, PCG_ERR_TIMEOUT, "halted after a tensor-core time-out");
   h->started = true;
@@ -1487,11 +1666,13 @@ int pcg_step(pcg_handle* h, int nsteps) {
 }
 
 int pcg_synchronize(pcg_handle* h) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   return check_status(h);
 }
 
 int pcg_step_status(pcg_handle* h) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   int rc = PCG_OK;
   if (h->status_pending) {  // the block copied after the step before: that step has ended
@@ -1508,6 +1689,7 @@ int pcg_step_status(pcg_handle* h) {
 
 int pcg_seed_plasma_cells(pcg_handle* h, int slot, unsigned per_cell, double density, double t_par_ev,
                           double t_perp_ev, uint64_t seed) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || slot < 0 || slot >= (int)h->sp.size() || per_cell == 0) return PCG_ERR_ARG;
   if (!(density >= 0) || !(t_par_ev >= 0) || !(t_perp_ev >= 0))
     return fail(h, PCG_ERR_ARG, "negative density or temperature");
@@ -1536,6 +1718,7 @@ int pcg_seed_plasma_cells(pcg_handle* h, int slot, unsigned per_cell, double den
 
 int pcg_seed_plasma(pcg_handle* h, int slot, size_t n, double density, double temperature_ev,
                     uint64_t seed) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   if (!(density >= 0) || !(temperature_ev >= 0)) return fail(h, PCG_ERR_ARG, "negative density or temperature");
   Species& s = h->sp[slot];
@@ -1562,6 +1745,7 @@ int pcg_seed_plasma(pcg_handle* h, int slot, size_t n, double density, double te
 
 int pcg_set_beam_profile(pcg_handle* h, int slot, int profile, double sigma_z,
                          double macro_per_cell) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || slot < 0 || slot >= (int)h->sp.size()) return PCG_ERR_ARG;
   Species& s = h->sp[slot];
   if (!s.beam) return fail(h, PCG_ERR_ARG, "not a beam");
@@ -1580,12 +1764,14 @@ int pcg_set_beam_profile(pcg_handle* h, int slot, int profile, double sigma_z,
 }
 
 int pcg_enable_timers(pcg_handle* h, int on) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h) return PCG_ERR_ARG;
   h->timers = on != 0;
   return PCG_OK;
 }
 
 int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !ms || n < 0) return PCG_ERR_ARG;
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   for (int c = 0; c < n; ++c) { ms[c] = 0; if (launches) launches[c] = 0; }
@@ -1604,12 +1790,20 @@ int pcg_kernel_times(pcg_handle* h, double* ms, int* launches, int n) {
 }
 
 int pcg_get_stream(pcg_handle* h, void** stream) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !stream) return PCG_ERR_ARG;
   *stream = (void*)h->stream;
   return PCG_OK;
 }
 
+int pcg_get_device(pcg_handle* h, int* device) {
+  if (!h || !device) return PCG_ERR_ARG;
+  *device = h->cfg.device;
+  return PCG_OK;
+}
+
 int pcg_diag(pcg_handle* h, pcg_diagnostics* out) {
+  DeviceScope device_scope(h ? h->cfg.device : -1);
   if (!h || !out) return PCG_ERR_ARG;
   int rc = check_status(h);
   if (rc != PCG_OK) return rc;

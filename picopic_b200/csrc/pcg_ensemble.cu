@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pcg.h"
+#include "pcg_device.h"
 
 struct pcg_ensemble {
   std::vector<pcg_handle*> runs;
@@ -57,8 +58,13 @@ extern "C" {
 int pcg_ensemble_create(pcg_handle* const* runs, int n, int threads, pcg_ensemble** out) {
   if (!runs || n <= 0 || !out) return PCG_ERR_ARG;
   *out = nullptr;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return PCG_ERR_CUDA;
+  int dev = -1;
+  for (int i = 0; i < n; ++i) {  // the runs share one GPU
+    int d = -1;
+    if (!runs[i] || pcg_get_device(runs[i], &d) != PCG_OK || (i > 0 && d != dev)) return PCG_ERR_ARG;
+    dev = d;
+  }
+  pcg::DeviceScope device_scope(dev);
   pcg_ensemble* e = new pcg_ensemble();
   e->device = dev;
   e->threads = std::max(1, std::min(threads > 0 ? threads : 8, n));
@@ -84,6 +90,7 @@ int pcg_ensemble_create(pcg_handle* const* runs, int n, int threads, pcg_ensembl
 }
 
 int pcg_ensemble_step(pcg_ensemble* e, int nsteps, float* device_ms) {
+  pcg::DeviceScope device_scope(e ? e->device : -1);
   if (!e || nsteps < 0) return PCG_ERR_ARG;
   const int n = (int)e->runs.size();
   if (cudaEventRecord(e->start, e->join) != cudaSuccess) return PCG_ERR_CUDA;
@@ -123,6 +130,7 @@ int pcg_ensemble_step(pcg_ensemble* e, int nsteps, float* device_ms) {
 }
 
 int pcg_ensemble_autotune(pcg_ensemble* e, int trial_steps, int* choice) {
+  pcg::DeviceScope device_scope(e ? e->device : -1);
   if (!e || trial_steps <= 0) return PCG_ERR_ARG;
   std::vector<double> share;
   double total = 0;
@@ -149,6 +157,7 @@ int pcg_ensemble_autotune(pcg_ensemble* e, int trial_steps, int* choice) {
 }
 
 int pcg_ensemble_destroy(pcg_ensemble* e) {
+  pcg::DeviceScope device_scope(e ? e->device : -1);
   if (!e) return PCG_ERR_ARG;
   for (cudaEvent_t ev : e->done)
     if (ev) cudaEventDestroy(ev);

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pcg.h"
+#include "pcg_device.h"
 #include "pcg_mlp.cuh"
 #include "pcg_mlp_tc.cuh"
 #include "pcg_philox.cuh"
@@ -284,6 +285,7 @@ __global__ void __launch_bounds__(tc::kThreads, 1) forward_tc_kernel(const float
 }  // namespace pcg
 
 using namespace pcg::mlp;
+using pcg::DeviceScope;
 
 namespace {
 
@@ -311,7 +313,9 @@ extern "C" {
 int pcg_mlp_create(int device, uint64_t seed, pcg_mlp** out) {
   if (!out) return PCG_ERR_ARG;
   *out = nullptr;
-  if (cudaSetDevice(device) != cudaSuccess) return PCG_ERR_CUDA;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return PCG_ERR_ARG;
+  DeviceScope device_scope(device);
   pcg_mlp* m = new pcg_mlp();
   m->device = device;
   m->seed = seed;
@@ -344,6 +348,7 @@ int pcg_mlp_create(int device, uint64_t seed, pcg_mlp** out) {
 }
 
 int pcg_mlp_destroy(pcg_mlp* m) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m) return PCG_OK;
   if (m->stream) cudaStreamSynchronize(m->stream);
   cudaFree(m->params); cudaFree(m->grad); cudaFree(m->adam_m); cudaFree(m->adam_v); cudaFree(m->loss);
@@ -354,6 +359,7 @@ int pcg_mlp_destroy(pcg_mlp* m) {
 }
 
 int pcg_mlp_get_params(pcg_mlp* m, float* out) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || !out) return PCG_ERR_ARG;
   if (cudaMemcpyAsync(out, m->params, kParams * sizeof(float), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
       cudaStreamSynchronize(m->stream) != cudaSuccess)
@@ -362,6 +368,7 @@ int pcg_mlp_get_params(pcg_mlp* m, float* out) {
 }
 
 int pcg_mlp_set_params(pcg_mlp* m, const float* in) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || !in) return PCG_ERR_ARG;
   if (cudaMemcpyAsync(m->params, in, kParams * sizeof(float), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
       cudaMemsetAsync(m->adam_m, 0, kParams * sizeof(float), m->stream) != cudaSuccess ||
@@ -373,6 +380,7 @@ int pcg_mlp_set_params(pcg_mlp* m, const float* in) {
 }
 
 int pcg_mlp_forward(pcg_mlp* m, const float* x, size_t rows, float* y) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || (!x && rows) || (!y && rows)) return PCG_ERR_ARG;
   if (rows == 0) return PCG_OK;
   float *dx = nullptr, *dy = nullptr;
@@ -390,6 +398,7 @@ int pcg_mlp_forward(pcg_mlp* m, const float* x, size_t rows, float* y) {
 }
 
 int pcg_mlp_forward_tc(pcg_mlp* m, const float* x, size_t rows, float* y, float* device_ms) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || (!x && rows) || (!y && rows)) return PCG_ERR_ARG;
   if (device_ms) *device_ms = 0.f;
   if (rows == 0) return PCG_OK;
@@ -432,6 +441,7 @@ int pcg_mlp_forward_tc(pcg_mlp* m, const float* x, size_t rows, float* y, float*
 }
 
 int pcg_mlp_gradient(pcg_mlp* m, const float* x, const float* t, size_t rows, float* grad_out, float* loss_out) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || !x || !t || !grad_out || rows == 0) return PCG_ERR_ARG;
   float *dx = nullptr, *dt = nullptr;
   if (upload(&dx, x, rows * kIn, m->stream) != 0 || upload(&dt, t, rows * kOut, m->stream) != 0) {
@@ -454,6 +464,7 @@ int pcg_mlp_gradient(pcg_mlp* m, const float* x, const float* t, size_t rows, fl
 }
 
 int pcg_mlp_set_data(pcg_mlp* m, const float* x, const float* t, size_t rows) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || !x || !t || rows == 0) return PCG_ERR_ARG;
   if (upload(&m->x, x, rows * kIn, m->stream) != 0 || upload(&m->t, t, rows * kOut, m->stream) != 0)
     return PCG_ERR_NOMEM;
@@ -462,6 +473,7 @@ int pcg_mlp_set_data(pcg_mlp* m, const float* x, const float* t, size_t rows) {
 }
 
 int pcg_mlp_train(pcg_mlp* m, int steps, int batch, float lr, float* last_loss) {
+  DeviceScope device_scope(m ? m->device : -1);
   if (!m || steps < 0 || batch <= 0 || !m->rows) return PCG_ERR_ARG;
   const unsigned blocks = (unsigned)((batch + kRowsPerBlock - 1) / kRowsPerBlock);
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;

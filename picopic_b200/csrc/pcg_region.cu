@@ -38,23 +38,23 @@ __global__ void flags_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, 
   flags[j] = live && z >= lo && z < hi ? 1 : 0;
 }
 
-// out: 6 x m doubles (r, z, v_r, v_phi, v_z, w) of the slots idx[0..m)
+// out: 6 x m doubles (r, z - zshift, v_r, v_phi, v_z, w) of the slots idx[0..m)
 __global__ void gather_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, int f32, const unsigned* idx,
-                              size_t m, double* out) {
+                              size_t m, double zshift, double* out) {
   const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (q >= m) return;
   const size_t j = idx[q];
   if (f32) {
     const int c = b32.cell[j];
     out[q] = ((double)cell_r_of(c) + (double)b32.off_r[j]) * g.dr;
-    out[m + q] = ((double)cell_z_of(c) + (double)b32.off_z[j]) * g.dz;
+    out[m + q] = ((double)cell_z_of(c) + (double)b32.off_z[j]) * g.dz - zshift;
     out[2 * m + q] = b32.vr[j];
     out[3 * m + q] = b32.vphi[j];
     out[4 * m + q] = b32.vz[j];
     out[5 * m + q] = b32.w[j];
   } else {
     out[q] = s64.r[j];
-    out[m + q] = s64.z[j];
+    out[m + q] = s64.z[j] - zshift;
     out[2 * m + q] = s64.vr[j];
     out[3 * m + q] = s64.vphi[j];
     out[4 * m + q] = s64.vz[j];
@@ -87,10 +87,10 @@ void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const Species
 }
 
 void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, const unsigned* idx,
-                   size_t m, double* out, cudaStream_t s) {
+                   size_t m, double zshift, double* out, cudaStream_t s) {
   if (!m) return;
   gather_kernel<<<blocks_for(m), kThreads, 0, s>>>(g, b32 ? *b32 : SpeciesF32Buffers{}, s64 ? *s64 : SpeciesF64{},
-                                                    b32 ? 1 : 0, idx, m, out);
+                                                    b32 ? 1 : 0, idx, m, zshift, out);
 }
 
 void region_keep(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,

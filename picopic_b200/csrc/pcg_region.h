@@ -16,9 +16,9 @@ namespace pcg {
 // flags[j] = 1 for the live slots j < n with lo <= z < hi
 void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
                   double hi, unsigned char* flags, cudaStream_t s);
-// out: r, z, v_r, v_phi, v_z, w of the slots idx[0..m), m doubles apart
+// out: r, z - zshift, v_r, v_phi, v_z, w of the slots idx[0..m), m doubles apart
 void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, const unsigned* idx,
-                   size_t m, double* out, cudaStream_t s);
+                   size_t m, double zshift, double* out, cudaStream_t s);
 // marks the live slots outside [lo, hi) dead and counts them in st->dead_slots
 void region_keep(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
                  double hi, DevStatus* st, cudaStream_t s);

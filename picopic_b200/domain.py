@@ -228,6 +228,30 @@ class Domain:
                     "pcg_export_species_range")
         return {k: v[:n.value] for k, v in out.items()}
 
+    def transfer_range(self, slot, lo, hi, shift, dst, dst_slot, append=True) -> int:
+        """Device to device: this domain's live particles with lo <= z < hi,
+        z - shift, appended to (or replacing) dst's species dst_slot; returns
+        their count."""
+        n = ctypes.c_size_t()
+        rc = self.lib.pcg_transfer_species_range(self.h, slot, float(lo), float(hi), float(shift), dst.h,
+                                                 int(dst_slot), 1 if append else 0, ctypes.byref(n))
+        if rc != 0:
+            self._raise_pair(rc, "pcg_transfer_species_range", dst)
+        return n.value
+
+    def _raise_pair(self, rc, where, dst):
+        """An error of a call on two handles: the last message of each."""
+        msgs = [(self.lib.pcg_last_error(d.h) or b"").decode() for d in (self, dst)]
+        raise PcgError(rc, where, f"source: {msgs[0]!r}; destination: {msgs[1]!r}")
+
+    def copy_field_columns(self, c0, c1, dst, g0, which=None):
+        """Device to device: array columns [c0, c1) of a field (all twelve
+        when which is None) into dst's columns from g0."""
+        idx = -1 if which is None else (FIELD[which] if isinstance(which, str) else int(which))
+        rc = self.lib.pcg_copy_field_columns(self.h, idx, int(c0), int(c1), dst.h, int(g0))
+        if rc != 0:
+            self._raise_pair(rc, "pcg_copy_field_columns", dst)
+
     def keep_range(self, slot, lo, hi):
         """Remove the live particles outside lo <= z < hi."""
         self._check(self.lib.pcg_keep_species_range(self.h, slot, float(lo), float(hi)),

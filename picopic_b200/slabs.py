@@ -295,7 +295,7 @@ class SlabGroup:
     the ghost species after them, sets the slabs' particles and fields from
     global arrays and steps all slabs."""
 
-    def __init__(self, grid, count, make_engine, species, ghost=6, ghost_capacity=None):
+    def __init__(self, grid, count, make_engine, species, ghost=6, ghost_capacity=None, on_device=None):
         self.grid = grid
         self.slabs = plan(grid.nz, count, ghost)
         self.widths = _ghost_widths(self.slabs)
@@ -305,6 +305,13 @@ class SlabGroup:
             e = make_engine(slab_geometry(grid, s), s)
             _add_ghosts(e, species, ghost_capacity)
             self.parts.append(_SlabEngine(grid, s, e, self.nsp))
+        # device to device (GPU domains: pcg_transfer_species_range and
+        # pcg_copy_field_columns, a peer copy between GPUs), else through the host
+        can = all(hasattr(se.engine, "transfer_range") and hasattr(se.engine, "copy_field_columns")
+                  for se in self.parts)
+        if on_device and not can:
+            raise ValueError("the slabs' engines have no device-to-device exchange")
+        self.on_device = can if on_device is None else bool(on_device)
 
     # -- set-up from global data ------------------------------------------------------
     def set_particles(self, slot, r, z, vr, vphi, vz, w):
@@ -332,6 +339,9 @@ class SlabGroup:
         return nl, nr
 
     def exchange(self):
+        if self.on_device:
+            self._exchange_on_device()
+            return
         last = len(self.parts) - 1
         # 1. owners hand over the particles that left their cells
         mig = [[se.migrants(t) for t in range(self.nsp)] for se in self.parts]
@@ -348,6 +358,45 @@ class SlabGroup:
             se.set_ghost_fields(fs[i - 1][1] if i > 0 else None, fs[i + 1][0] if i < last else None)
             for t in range(self.nsp):
                 se.set_ghosts(t, [ps[i - 1][t][1] if i > 0 else None, ps[i + 1][t][0] if i < last else None])
+
+    def _exchange_on_device(self):
+        """The same exchange with the strips moved between the domains on the
+        device; only the particle counts reach the host.  The slabs go in
+        order: a slab's hand-over sees the migrants its left neighbour has
+        just appended and passes on any that lie outside its own cells."""
+        last, dz, inf = len(self.parts) - 1, self.grid.dz, np.inf
+        for i, se in enumerate(self.parts):
+            s = se.slab
+            for t in range(self.nsp):
+                if not s.first:
+                    nb = self.parts[i - 1]
+                    se.engine.transfer_range(t, -inf, se.lo, nb.z0 - se.z0, nb.engine, t, append=True)
+                if not s.last:
+                    nb = self.parts[i + 1]
+                    se.engine.transfer_range(t, se.hi, inf, nb.z0 - se.z0, nb.engine, t, append=True)
+                if not (s.first and s.last):
+                    se.engine.keep_range(t, se.lo, se.hi)
+        for i, se in enumerate(self.parts):
+            s = se.slab
+            lw, rw = self.widths[i]
+            if i > 0:  # left ghost columns: global nodes [e0, k0) of the left slab
+                src = self.parts[i - 1]
+                src.engine.copy_field_columns(src.col(s.e0), src.col(s.k0), se.engine, se.col(s.e0))
+            if i < last:
+                src = self.parts[i + 1]
+                src.engine.copy_field_columns(src.col(s.k1), src.col(s.e1), se.engine, se.col(s.k1))
+            for t in range(self.nsp):
+                replace = True
+                if i > 0:  # the left slab's own particles from lw cells before its end
+                    src = self.parts[i - 1]
+                    lo = (src.slab.k1 - lw - src.slab.e0) * dz
+                    src.engine.transfer_range(t, lo, inf, se.z0 - src.z0, se.engine, self.nsp + t, append=False)
+                    replace = False
+                if i < last:  # the right slab's own particles up to rw cells after its start
+                    src = self.parts[i + 1]
+                    hi = (src.slab.k0 + rw - src.slab.e0) * dz
+                    src.engine.transfer_range(t, -inf, hi, se.z0 - src.z0, se.engine, self.nsp + t,
+                                              append=not replace)
 
     # -- global views ------------------------------------------------------------------
     def get_field(self, name):

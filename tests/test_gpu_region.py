@@ -108,3 +108,61 @@ def test_field_columns(precision):
     from picopic_b200._ffi import PcgError
     with pytest.raises(PcgError):
         d.get_field_columns("e_r", 90, grid.nz + 5)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_transfer_between_domains_on_the_device(precision):
+    """A band of one domain appended to (or replacing) another domain's species
+    with z shifted, device to device: the same particles as the band's host
+    export, shifted; and the source keeps all of its own."""
+    grid = small_grid(nr=16, nz=96)
+    src, dst = _domain(grid, precision), _domain(grid, precision)
+    src.set_particles(0, *particles(grid, 6000, 21))
+    dst.set_particles(0, *particles(grid, 500, 22))
+    for name, a in random_fields(grid, 3).items():
+        src.set_field(name, a)
+    src.step(2)
+    before = dst.get_particles(0)
+    lo, hi, shift = 60 * grid.dz, np.inf, 50 * grid.dz
+    band = src.export_range(0, lo, hi)
+    n_src = src.count(0)
+    assert src.transfer_range(0, lo, hi, shift, dst, 0, append=True) == band["r"].size > 0
+    assert src.count(0) == n_src
+    got = dst.get_particles(0)
+    expect = {k: np.concatenate([before[k], band[k] - (shift if k == "z" else 0.0)]) for k in KEYS}
+    a, b = _sorted(got), _sorted(expect)
+    assert a["r"].size == b["r"].size
+    for k in KEYS:  # the float layout re-splits z into cell and offset: within its rounding
+        np.testing.assert_allclose(a[k], b[k], rtol=0, atol=(0 if precision == "f64" else 1e-7) * np.abs(b[k]).max(),
+                                   err_msg=k)
+    assert src.transfer_range(0, -np.inf, 10 * grid.dz, 0.0, dst, 0, append=False) == dst.count(0)
+    if precision == "f64":  # a replacement: exactly the band
+        _equal(dst.get_particles(0), src.export_range(0, -np.inf, 10 * grid.dz))
+    # the destination steps on with what it received
+    dst.step(1)
+    assert dst.count(0) > 0
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_field_columns_between_domains_on_the_device(precision):
+    grid = small_grid(nr=16, nz=96)
+    src, dst = _domain(grid, precision), _domain(grid, precision)
+    fa, fb = random_fields(grid, 8), random_fields(grid, 9)
+    for name in fa:
+        src.set_field(name, fa[name])
+        dst.set_field(name, fb[name])
+    src.copy_field_columns(10, 17, dst, 60)
+    src.copy_field_columns(30, 32, dst, 0, which="j_z")
+    for name in fa:
+        a, b = src.get_field(name), _get_expected(fb[name], precision)
+        b[:, 60:67] = a[:, 10:17]
+        if name == "j_z":
+            b[:, 0:2] = a[:, 30:32]
+        np.testing.assert_array_equal(dst.get_field(name), b, err_msg=name)
+    from picopic_b200._ffi import PcgError
+    with pytest.raises(PcgError):
+        src.copy_field_columns(90, grid.nz + 4, dst, 95)
+
+
+def _get_expected(a, precision):
+    return a.copy() if precision == "f64" else a.astype(np.float32).astype(np.float64)

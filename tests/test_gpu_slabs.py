@@ -1,6 +1,7 @@
 """A run split along z into slabs of GPU domains (picopic_b200/slabs.py,
 several domains on one GPU in one process) against the undivided run on the
-same GPU: the FP64 layout within 1e-9 of each field array's largest value
+same GPU, with the strips exchanged through the host and device to device
+(pcg_transfer_species_range, pcg_copy_field_columns): the FP64 layout within 1e-9 of each field array's largest value
 and of each particle quantity after 10 steps (the deposit adds the same
 currents in another order), the float layout within 1e-4 (fields) and 1e-5
 (particles), as the float path is checked against the oracle."""
@@ -45,8 +46,10 @@ def _sorted(p):
     return {k: np.asarray(p[k])[order] for k in S.PARTICLE_KEYS}
 
 
-@pytest.mark.parametrize("precision,quirks,count", [("f64", "reference", 2), ("f64", "fixed", 3), ("f32", "fixed", 2)])
-def test_gpu_slabs_equal_the_undivided_run(precision, quirks, count):
+@pytest.mark.parametrize("precision,quirks,count,on_device", [
+    ("f64", "reference", 2, False), ("f64", "reference", 2, True), ("f64", "fixed", 3, True),
+    ("f32", "fixed", 2, False), ("f32", "fixed", 3, True)])
+def test_gpu_slabs_equal_the_undivided_run(precision, quirks, count, on_device):
     grid = small_grid(nr=16, nz=96)
     species = _species(grid)
 
@@ -55,7 +58,8 @@ def test_gpu_slabs_equal_the_undivided_run(precision, quirks, count):
               for s in species]
         return _domain(geometry, precision, quirks, sp)
 
-    g = S.SlabGroup(grid, count, make, species)
+    g = S.SlabGroup(grid, count, make, species, on_device=on_device)
+    assert g.on_device == on_device
     whole = _domain(grid, precision, quirks, species)
     parts, fields = _inputs(grid)
     for i, p in parts.items():
