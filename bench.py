@@ -259,6 +259,9 @@ def run_gpu(args):
     ensemble = None
     if not args.no_ensemble and world == 1:
         ensemble = run_ensemble(args, local)
+    slab_leg = None
+    if not args.no_slabs and world == 1:
+        slab_leg = run_slabs(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(w)
     if rank == 0:
@@ -283,12 +286,77 @@ def run_gpu(args):
             "collisions": coll,
             "large": large,
             "ensemble": ensemble,
+            "slabs": slab_leg,
             "accuracy": acc,
             "cpu_baseline": cpu,
             "gpu_launches": int(diag.kernel_launches - diag0.kernel_launches),
         }
         print(json.dumps(line))
     rep.close()
+
+
+def run_slabs(args, local, counts=(2, 4), steps=20, warmup=3):
+    """The wakefield workload at nz = 1024 split along z into slabs of one
+    GPU (picopic_b200.slabs, device-to-device exchange after every step)
+    against the same workload undivided; wall clock, as the exchange waits
+    for each slab's step on the host (a band's particle count)."""
+    import time
+    import torch
+    from picopic_b200 import Domain, Geometry, slabs
+    w = scaled(WORKLOAD, nz=1024)
+    dt = dt_courant(w["dr"])
+    g = Geometry(w["nr"], w["nz"], w["nr"] * w["dr"], w["nz"] * w["dz"], dt)
+    vb = beam_velocity(w["beam_energy_mev"])
+    cells_b = (w["beam_radius"] / w["dr"]) * (6 * w["beam_sigma_z"] / w["dz"])
+    nb = int(w["beam_ppc"] * cells_b * 1.05) + 4096
+    beam = dict(macro_amount=max(1, int(w["beam_ppc"] * cells_b)), start_time=0.0, radius=w["beam_radius"],
+                density=w["beam_density"], amount=1, length=6 * w["beam_sigma_z"], distance=0.0, velocity=vb)
+    species = [_spec("electrons", -1, 1, 1), _spec("ions", 1, 1836, 2), _spec("beam_electrons", -1, 1, 1000)]
+
+    def wall(fn, k):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(k)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / k
+
+    whole, _, _, _ = make_domain(w, "f32", device=local)
+    whole.step(warmup)
+    ms_whole = wall(whole.step, steps)
+    n_whole = whole.diag().particles
+    del whole
+    torch.cuda.empty_cache()
+    out = {"workload": w["name"].replace("4096", "1024"), "precision": "f32", "steps": steps,
+           "timing": "wall clock", "undivided_ms_per_step": ms_whole, "particles": int(n_whole)}
+    for count in counts:
+        def make(geometry, slab):
+            d = Domain(geometry, pusher=w["pusher"], current=w["current"], precision="f32", seed=1234,
+                       device=local)
+            n = geometry.nr * geometry.nz * w["ppc"]
+            d.add(species[0], capacity=int(n * 1.1))
+            d.add(species[1], capacity=int(n * 1.1))
+            d.add(_spec("beam_electrons", -1, 1, 1000, beam=beam if slab.first else None), capacity=nb)
+            return d
+        ghost = 2 * 6 * w["nr"] * w["ppc"] * 2
+        grp = slabs.SlabGroup(g, count, make, species, ghost_capacity=ghost, on_device=True)
+        for se in grp.parts:
+            d, geo = se.engine, slabs.slab_geometry(g, se.slab)
+            n = geo.nr * geo.nz * w["ppc"]
+            d.seed_plasma(0, n, w["density"], w["te"], 1234 + 2 * se.slab.index)
+            d.seed_plasma(1, n, w["density"], w["ti"], 1235 + 2 * se.slab.index)
+            if se.slab.first:
+                d.set_beam_profile(2, "gaussian", w["beam_sigma_z"], w["beam_ppc"])
+            for t in range(2):  # the seeded ghost cells belong to the neighbours
+                d.keep_range(t, se.lo, se.hi)
+        grp.exchange()
+        grp.step(warmup)
+        ms = wall(grp.step, steps)
+        live = sum(se.engine.count(t) for se in grp.parts for t in range(3))
+        out[f"slabs{count}"] = {"ms_per_step": ms, "over_undivided": ms / ms_whole,
+                                "particles_with_ghosts": int(live)}
+        del grp
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_accuracy(w, args, local):
@@ -766,6 +834,7 @@ def main():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-config0", action="store_true")
+    ap.add_argument("--no-slabs", action="store_true")
     ap.add_argument("--coll-nz", type=int, default=0, help="axial cells of the collisional workload (profiling)")
     ap.add_argument("--no-relax", action="store_true", help="skip the relaxation-time measurement")
     ap.add_argument("--target-blocks", type=int, default=0,

@@ -486,6 +486,11 @@ int pcg_export_field(pcg_handle* h, int which, double* dst);
  * reference's overlap copies (SMB::field_e_overlay, field_h_overlay,
  * current_overlay, SMB.cpp:566-1229). */
 int pcg_get_field_columns(pcg_handle* h, int which, int c0, int c1, double* dst);
+/* (dst and src, and the particle arrays of pcg_import_species,
+ * pcg_append_species and pcg_export_species_range, may also be device
+ * memory on the handle's GPU: the copies then stay on the device.  Device
+ * arrays must be complete when the call is made, and are free for reuse
+ * when it returns.) */
 int pcg_set_field_columns(pcg_handle* h, int which, int c0, int c1, const double* src);
 
 /* The live particles of a species with lo <= z < hi (z in m, the domain's

@@ -114,6 +114,7 @@ struct pcg_handle {
   size_t region_bytes = 0;
   double* region_out = nullptr;
   size_t region_out_n = 0;
+  unsigned* h_count = nullptr;  // pinned: a band's particle count
   double* staging = nullptr;  // host-to-device particle staging, reused
   size_t staging_n = 0;
   // kernel timers: event pairs per class, recycled after each query
@@ -156,6 +157,17 @@ int dalloc(pcg_handle* h, T** p, size_t count) {
 }
 
 bool is_f64(const pcg_handle* h) { return h->cfg.precision == PCG_PRECISION_F64; }
+
+// True for memory the GPU addresses directly (a device or managed
+// allocation): the particle and column calls then copy device to device.
+bool device_memory(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // plain host memory on older drivers
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
 
 
 // PML profiles of MaxwellSolverYee::set_pml (maxwellSolverYee.cpp:57-109):
@@ -776,7 +788,8 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
       cudaEventCreateWithFlags(&h->ev_staging_free, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_status, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_region, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost((void**)&h->h_status_lag, sizeof(DevStatus)) != cudaSuccess)
+      cudaMallocHost((void**)&h->h_status_lag, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMallocHost((void**)&h->h_count, sizeof(unsigned)) != cudaSuccess)
     return bail(PCG_ERR_CUDA);
   if (cfg->precision == PCG_PRECISION_F32 &&
       (cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) != cudaSuccess ||
@@ -872,6 +885,7 @@ int pcg_destroy(pcg_handle* h) {
   if (h->ev_status) cudaEventDestroy(h->ev_status);
   if (h->ev_region) cudaEventDestroy(h->ev_region);
   if (h->h_status_lag) cudaFreeHost(h->h_status_lag);
+  if (h->h_count) cudaFreeHost(h->h_count);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->aux) cudaStreamDestroy(h->aux);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -967,7 +981,7 @@ static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, con
     // and the import for the copies; the steps queued before run on
     CUDA_TRY(h, cudaStreamWaitEvent(h->copy, h->ev_staging_free, 0));
     for (int a = 0; a < 6; ++a)
-      CUDA_TRY(h, cudaMemcpyAsync(stage + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->copy));
+      CUDA_TRY(h, cudaMemcpyAsync(stage + a * n, src[a], sizeof(double) * n, cudaMemcpyDefault, h->copy));
     CUDA_TRY(h, cudaEventRecord(h->ev_copied, h->copy));
     CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_copied, 0));
     if (is_f64(h)) launch_import_f64(h->g, view64(h, s), n0, n, stage, h->stream);
@@ -1082,11 +1096,16 @@ int field_columns(pcg_handle* h, int which, int c0, int c1, double* host, bool s
     double* dev = h->f64[which] + c0;
     if (set)
       CUDA_TRY(h, cudaMemcpy2DAsync(dev, sizeof(double) * ld, host, sizeof(double) * w, sizeof(double) * w, rows,
-                                    cudaMemcpyHostToDevice, h->stream));
+                                    cudaMemcpyDefault, h->stream));
     else
       CUDA_TRY(h, cudaMemcpy2DAsync(host, sizeof(double) * w, dev, sizeof(double) * ld, sizeof(double) * w, rows,
-                                    cudaMemcpyDeviceToHost, h->stream));
-    if (!set) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+                                    cudaMemcpyDefault, h->stream));
+    // a read, or a write from device memory the caller may reuse on return
+    if (!set || device_memory(host)) CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  } else if (device_memory(host)) {  // doubles in device memory: converted by a kernel
+    region_columns_f32(h->f32[which], ld, c0, (int)w, rows, host, set, h->stream);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   } else {
     float* dev = h->f32[which] + c0;
     std::vector<float> tmp(w * rows);
@@ -1137,10 +1156,9 @@ namespace {
 // handle's stream.
 int select_band(pcg_handle* h, Species& s, double lo, double hi, unsigned* m, const unsigned** sel) {
   *m = 0;
-  int rc = check_status(h);  // the steps queued before are done
-  if (rc != PCG_OK) return rc;
+  int rc;
   const size_t ns = s.n;
-  if (ns == 0) return PCG_OK;
+  if (ns == 0) return check_status(h);
   if (ns > 0x7fffffffu) return fail(h, PCG_ERR_UNSUPPORTED, "a band selection of more than 2^31 slots");
   // scratch: slot indices, selected indices, their count, flags, select temp
   size_t tmp = 0;
@@ -1168,10 +1186,13 @@ int select_band(pcg_handle* h, Species& s, double lo, double hi, unsigned* m, co
   region_flags(h->g, b32, s64, ns, lo, hi, flags, h->stream);
   iota_u32(iota, ns, h->stream);
   cub::DeviceSelect::Flagged(h->region + o_tmp, tmp, iota, flags, out, cnt, (int)ns, h->stream);
-  CUDA_TRY(h, cudaMemcpyAsync(h->h_status, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  // the count and the status of the steps queued before, in one wait
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   CUDA_TRY(h, cudaGetLastError());
-  std::memcpy(m, h->h_status, sizeof(unsigned));
+  if ((rc = status_code(h, h->h_status)) != PCG_OK) return rc;
+  *m = *h->h_count;
   *sel = out;
   return PCG_OK;
 }
@@ -1218,7 +1239,7 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
   double* dst[6] = {r, z, vr, vphi, vz, w};
   for (int a = 0; a < 6; ++a)
     if (dst[a])
-      CUDA_TRY(h, cudaMemcpyAsync(dst[a], h->region_out + (size_t)a * m, sizeof(double) * m, cudaMemcpyDeviceToHost,
+      CUDA_TRY(h, cudaMemcpyAsync(dst[a], h->region_out + (size_t)a * m, sizeof(double) * m, cudaMemcpyDefault,
                                   h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return PCG_OK;

@@ -77,7 +77,23 @@ __global__ void keep_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, i
   if ((threadIdx.x & 31) == 0 && m) atomicAdd(&st->dead_slots, (unsigned long long)__popc(m));
 }
 
+// rows x w block of a float plane (row length ld, from column c0) to or
+// from doubles in buf (row-major, w per row)
+__global__ void columns_f32_kernel(float* plane, int ld, int c0, int w, int rows, double* buf, int set) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= w * rows) return;
+  const int row = q / w, col = q - row * w;
+  float* f = plane + (size_t)row * ld + c0 + col;
+  if (set) *f = (float)buf[q];
+  else buf[q] = *f;
+}
+
 }  // namespace
+
+void region_columns_f32(float* plane, int ld, int c0, int w, int rows, double* buf, bool set, cudaStream_t s) {
+  const int n = w * rows;
+  if (n > 0) columns_f32_kernel<<<blocks_for((size_t)n), kThreads, 0, s>>>(plane, ld, c0, w, rows, buf, set ? 1 : 0);
+}
 
 void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
                   double hi, unsigned char* flags, cudaStream_t s) {

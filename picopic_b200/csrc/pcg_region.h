@@ -23,4 +23,8 @@ void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const Specie
 void region_keep(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
                  double hi, DevStatus* st, cudaStream_t s);
 
+// rows x w values of a float plane (row length ld, columns from c0) from
+// (set) or to device doubles, row-major
+void region_columns_f32(float* plane, int ld, int c0, int w, int rows, double* buf, bool set, cudaStream_t s);
+
 }  // namespace pcg

@@ -89,6 +89,7 @@ class Domain:
             raise PcgError(rc, "pcg_create", "invalid configuration or no CUDA device")
         self.h = h
         self.precision = precision
+        self.device = int(device)
         self.species = []
 
     # -- error handling ------------------------------------------------------
@@ -251,6 +252,65 @@ class Domain:
         rc = self.lib.pcg_copy_field_columns(self.h, idx, int(c0), int(c1), dst.h, int(g0))
         if rc != 0:
             self._raise_pair(rc, "pcg_copy_field_columns", dst)
+
+    # -- device buffers: torch CUDA tensors on this domain's GPU ------------------------
+    @property
+    def torch_device(self):
+        return f"cuda:{self.device}"
+
+    def _ready(self):
+        """Work queued on torch's current stream of this GPU (the tensors'
+        producers) is complete."""
+        import torch
+        torch.cuda.current_stream(self.device).synchronize()
+
+    def export_range_device(self, slot, lo, hi):
+        """The live particles with lo <= z < hi as a (6, n) float64 CUDA tensor
+        (rows r, z, v_r, v_phi, v_z, w), copied device to device."""
+        import torch
+        n = ctypes.c_size_t()
+        rc = self.lib.pcg_export_species_range(self.h, slot, float(lo), float(hi), 0, *[None] * 6, ctypes.byref(n))
+        if rc == 0:
+            return torch.zeros((6, 0), dtype=torch.float64, device=self.torch_device)
+        if rc != -5:  # PCG_ERR_CAPACITY: the count is set
+            self._check(rc, "pcg_export_species_range")
+        m = n.value
+        t = torch.empty((6, m), dtype=torch.float64, device=self.torch_device)
+        self._ready()
+        ptrs = [ctypes.cast(t[k].data_ptr(), _PD) for k in range(6)]
+        self._check(self.lib.pcg_export_species_range(self.h, slot, float(lo), float(hi), m, *ptrs, ctypes.byref(n)),
+                    "pcg_export_species_range")
+        return t
+
+    def set_particles_device(self, slot, t, append=False):
+        """Particles from a (6, n) float64 CUDA tensor on this GPU."""
+        import torch
+        t = t.to(dtype=torch.float64).contiguous()
+        if t.dim() != 2 or t.shape[0] != 6:
+            raise ValueError(f"particles as a (6, n) tensor, not {tuple(t.shape)}")
+        self._ready()
+        ptrs = [ctypes.cast(t[k].data_ptr(), _PD) for k in range(6)]
+        fn = self.lib.pcg_append_species if append else self.lib.pcg_import_species
+        self._check(fn(self.h, slot, int(t.shape[1]), *ptrs), "pcg_import_species")
+
+    def get_field_columns_device(self, which, c0, c1):
+        """Array columns [c0, c1) of a field as a (nr+4, c1-c0) float64 CUDA tensor."""
+        import torch
+        idx = FIELD[which] if isinstance(which, str) else int(which)
+        t = torch.empty((self.grid.shape[0], c1 - c0), dtype=torch.float64, device=self.torch_device)
+        self._ready()
+        self._check(self.lib.pcg_get_field_columns(self.h, idx, int(c0), int(c1), ctypes.cast(t.data_ptr(), _PD)),
+                    "pcg_get_field_columns")
+        return t
+
+    def set_field_columns_device(self, which, c0, t):
+        """Array columns [c0, c0 + t.shape[1]) of a field from a float64 CUDA tensor."""
+        import torch
+        idx = FIELD[which] if isinstance(which, str) else int(which)
+        t = t.to(dtype=torch.float64).contiguous()
+        self._ready()
+        self._check(self.lib.pcg_set_field_columns(self.h, idx, int(c0), int(c0) + int(t.shape[1]),
+                                                   ctypes.cast(t.data_ptr(), _PD)), "pcg_set_field_columns")
 
     def keep_range(self, slot, lo, hi):
         """Remove the live particles outside lo <= z < hi."""

@@ -416,10 +416,14 @@ class SlabGroup:
 
 
 class SlabRank:
-    """One slab per process: rank r of a torch.distributed group (host
-    tensors: a gloo group) holds slab r and exchanges the migrants and the
-    ghost strips with ranks r - 1 and r + 1 after every step.  Every rank
-    calls the same methods in the same order."""
+    """One slab per process: rank r of a torch.distributed group holds slab
+    r and exchanges the migrants and the ghost strips with ranks r - 1 and
+    r + 1 after every step.  Every rank calls the same methods in the same
+    order.  Over a gloo group the strips travel as host tensors; over an
+    NCCL group, with GPU domains (``export_range_device`` and the other
+    device-buffer methods of :class:`picopic_b200.Domain`), they stay on
+    the GPUs: band exports and column copies into CUDA tensors, NCCL
+    point-to-point sends between the ranks' GPUs."""
 
     def __init__(self, grid, make_engine, species, group=None, ghost=6, ghost_capacity=None):
         import torch.distributed as dist
@@ -433,25 +437,36 @@ class SlabRank:
         e = make_engine(slab_geometry(grid, self.slab), self.slab)
         _add_ghosts(e, species, ghost_capacity)
         self.se = _SlabEngine(grid, self.slab, e, self.nsp)
+        on_gpu = dist.get_backend(group) == "nccl" and hasattr(e, "export_range_device")
+        self.device = e.torch_device if on_gpu else None
 
-    # point-to-point of numpy arrays (shape known to both sides)
+    # point-to-point of float64 arrays (shape known to both sides): numpy
+    # arrays through host tensors, or CUDA tensors in place
     def _send(self, a, peer):
         import torch
-        self.dist.send(torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)), dst=peer, group=self.group)
+        if self.device is not None:
+            t = a if torch.is_tensor(a) else torch.as_tensor(np.asarray(a, dtype=np.float64), device=self.device)
+            self.dist.send(t.contiguous(), dst=peer, group=self.group)
+        else:
+            self.dist.send(torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)), dst=peer, group=self.group)
 
     def _recv(self, shape, peer):
         import torch
-        t = torch.empty(shape, dtype=torch.float64)
+        t = torch.empty(shape, dtype=torch.float64, device=self.device or "cpu")
         self.dist.recv(t, src=peer, group=self.group)
-        return t.numpy()
+        return t if self.device is not None else t.numpy()
 
     def _send_particles(self, p, peer):
-        self._send(np.array([p["r"].size], dtype=np.float64), peer)
-        if p["r"].size:
-            self._send(np.stack([p[k] for k in PARTICLE_KEYS]), peer)
+        """A particle set: a dict of arrays, or a (6, n) CUDA tensor."""
+        n = p.shape[1] if self.device is not None else p["r"].size
+        self._send(np.array([n], dtype=np.float64), peer)
+        if n:
+            self._send(p if self.device is not None else np.stack([p[k] for k in PARTICLE_KEYS]), peer)
 
     def _recv_particles(self, peer):
         n = int(self._recv((1,), peer)[0])
+        if self.device is not None:
+            return self._recv((len(PARTICLE_KEYS), n), peer) if n else None
         if n == 0:
             return _empty()
         a = self._recv((len(PARTICLE_KEYS), n), peer)
@@ -498,6 +513,9 @@ class SlabRank:
             self.exchange()
 
     def exchange(self):
+        if self.device is not None:
+            self._exchange_on_device()
+            return
         s, se, nsp = self.slab, self.se, self.nsp
         lw, rw = self.widths[self.rank]
         rows = self.grid.nr + 4
@@ -534,6 +552,71 @@ class SlabRank:
         se.set_ghost_fields(got_l[0] if got_l else None, got_r[0] if got_r else None)
         for t in range(nsp):
             se.set_ghosts(t, [got_l[1][t] if got_l else None, got_r[1][t] if got_r else None])
+
+    def _exchange_on_device(self):
+        """The exchange with CUDA tensors: the same two rounds (migrants, then
+        ghost columns and ghost particles), z shifted on the GPU."""
+        import torch
+        s, se, nsp, e = self.slab, self.se, self.nsp, self.se.engine
+        lw, rw = self.widths[self.rank]
+        rows, dz, inf = self.grid.nr + 4, self.grid.dz, np.inf
+
+        def out(t):  # domain z to global z
+            if t is not None and t.shape[1]:
+                t[1] += se.z0
+            return t
+
+        def into(parts, slot, append):  # global z to domain z, then import
+            parts = [q for q in parts if q is not None and q.shape[1]]
+            t = torch.cat(parts, dim=1) if parts else torch.zeros((6, 0), dtype=torch.float64, device=self.device)
+            t[1] -= se.z0
+            if t.shape[1] or not append:
+                e.set_particles_device(slot, t, append=append)
+
+        mig = []
+        for t in range(nsp):
+            left = None if s.first else out(e.export_range_device(t, -inf, se.lo))
+            right = None if s.last else out(e.export_range_device(t, se.hi, inf))
+            if not (s.first and s.last):
+                e.keep_range(t, se.lo, se.hi)
+            mig.append((left, right))
+        got_l, got_r = self._swap(
+            lambda peer: [self._send_particles(mig[t][0], peer) for t in range(nsp)],
+            lambda peer: [self._send_particles(mig[t][1], peer) for t in range(nsp)],
+            lambda peer: [self._recv_particles(peer) for _ in range(nsp)],
+            lambda peer: [self._recv_particles(peer) for _ in range(nsp)])
+        for t in range(nsp):
+            into([got_l[t] if got_l else None, got_r[t] if got_r else None], t, append=True)
+        nl = 0 if s.first else self.widths[self.rank - 1][1]
+        nr = 0 if s.last else self.widths[self.rank + 1][0]
+        fl = None if s.first else {f: e.get_field_columns_device(f, se.col(s.k0), se.col(s.k0 + nl)) for f in FIELDS}
+        fr = None if s.last else {f: e.get_field_columns_device(f, se.col(s.k1 - nr), se.col(s.k1)) for f in FIELDS}
+        ps = [(None if s.first else out(e.export_range_device(t, -inf, (s.k0 + nl - s.e0) * dz)),
+               None if s.last else out(e.export_range_device(t, (s.k1 - nr - s.e0) * dz, inf)))
+              for t in range(nsp)]
+
+        def send(fields, side):
+            def go(peer):
+                for f in FIELDS:
+                    self._send(fields[f], peer)
+                for t in range(nsp):
+                    self._send_particles(ps[t][side], peer)
+            return go
+
+        def recv(width):
+            def go(peer):
+                f_ = {f: self._recv((rows, width), peer) for f in FIELDS}
+                return f_, [self._recv_particles(peer) for _ in range(nsp)]
+            return go
+
+        got_l, got_r = self._swap(send(fl, 0), send(fr, 1), recv(lw), recv(rw))
+        for f in FIELDS:
+            if got_l is not None:
+                e.set_field_columns_device(f, se.col(s.e0), got_l[0][f])
+            if got_r is not None:
+                e.set_field_columns_device(f, se.col(s.k1), got_r[0][f])
+        for t in range(nsp):
+            into([got_l[1][t] if got_l else None, got_r[1][t] if got_r else None], nsp + t, append=False)
 
     def own_field_columns(self, name):
         """This slab's own columns of a field (the end slabs with their outer halo):

@@ -166,3 +166,33 @@ def test_field_columns_between_domains_on_the_device(precision):
 
 def _get_expected(a, precision):
     return a.copy() if precision == "f64" else a.astype(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_device_buffers(precision):
+    """The particle and column calls with CUDA tensors in place of host arrays
+    (what an NCCL exchange sends) give what the host arrays give."""
+    import torch
+    grid = small_grid(nr=16, nz=96)
+    src, dst = _domain(grid, precision), _domain(grid, precision)
+    src.set_particles(0, *particles(grid, 5000, 31))
+    for name, a in random_fields(grid, 5).items():
+        src.set_field(name, a)
+    src.step(2)
+    lo, hi = 20 * grid.dz, 41 * grid.dz
+    t = src.export_range_device(0, lo, hi)
+    assert t.is_cuda and t.shape[0] == 6
+    band = src.export_range(0, lo, hi)
+    _equal({k: t[q].cpu().numpy() for q, k in enumerate(KEYS)}, band)
+    dst.set_particles_device(0, t)
+    _equal(dst.export_range(0, -np.inf, np.inf), dst.get_particles(0))
+    assert dst.count(0) == band["r"].size
+    dst.set_particles_device(0, t[:, :7], append=True)
+    assert dst.count(0) == band["r"].size + 7
+    c = src.get_field_columns_device("e_z", 30, 45)
+    np.testing.assert_array_equal(c.cpu().numpy(), src.get_field_columns("e_z", 30, 45))
+    dst.set_field_columns_device("h_phi", 3, c)
+    np.testing.assert_array_equal(dst.get_field_columns("h_phi", 3, 18), c.cpu().numpy())
+    empty = src.export_range_device(0, hi, lo)
+    assert empty.shape == (6, 0)
+    torch.cuda.synchronize()
