@@ -79,3 +79,35 @@ def test_gpu_slabs_equal_the_undivided_run(precision, quirks, count, on_device):
         for k in S.PARTICLE_KEYS:
             assert _rel(a[k], b[k]) <= tol_p, (t, k)
     assert g.get_particles(2)["r"].size > 0, "the beam was injected"
+
+
+def test_gpu_beam_crosses_slab_boundaries():
+    """The bunch injected in the first slab runs into the second (120 steps,
+    48 cells, 2 slabs, device exchange, FP64) as in the undivided run."""
+    grid = small_grid(nr=16, nz=48)
+    species = _species(grid)
+
+    def make(geometry, slab):
+        sp = [s if (slab.first or s.beam is None) else SpeciesSpec(s.name, s.charge, s.mass, id=s.id)
+              for s in species]
+        return _domain(geometry, "f64", "fixed", sp)
+
+    g = S.SlabGroup(grid, 2, make, species, on_device=True)
+    whole = _domain(grid, "f64", "fixed", species)
+    parts, fields = _inputs(grid)
+    for i, p in parts.items():
+        g.set_particles(i, *p)
+        whole.set_particles(i, *p)
+    for k, a in fields.items():
+        g.set_field(k, a)
+        whole.set_field(k, a)
+    g.step(120)
+    whole.step(120)
+    assert g.parts[1].own(2)["r"].size > 0, "the bunch reached the second slab"
+    for k in S.FIELDS:
+        assert _rel(g.get_field(k), whole.get_field(k)) <= 1e-8, k
+    for t in range(len(species)):
+        a, b = _sorted(g.get_particles(t)), _sorted(whole.get_particles(t))
+        assert a["r"].size == b["r"].size, t
+        for k in S.PARTICLE_KEYS:
+            assert _rel(a[k], b[k]) <= 1e-8, (t, k)

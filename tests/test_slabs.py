@@ -205,3 +205,40 @@ def _single(geometry):
     o.add(ELECTRONS)
     o.set_rng("philox", 7)
     return o
+
+
+def test_beam_crosses_slab_boundaries():
+    """The injected bunch runs from the first slab through a boundary into the
+    next (as plain particles there): 120 steps on a 48-cell grid in 2 slabs,
+    against the undivided run (fields within 1e-8 of each array's largest
+    value: rounding differences grow over the longer run)."""
+    grid = small_grid(nr=16, nz=48)
+    make, species = _engine_factory(grid, "fixed")
+    g = S.SlabGroup(grid, 2, make, species)
+    parts, fields = _inputs(grid)
+    for i, p in parts.items():
+        g.set_particles(i, *p)
+    for k, a in fields.items():
+        g.set_field(k, a)
+    whole = OracleSim(grid, "borisrel", "vb", quirks="fixed")
+    for sp in species:
+        whole.add(sp)
+    whole.set_rng("philox", 7)
+    for i, p in parts.items():
+        whole.set_particles(i, *p)
+    for k, a in fields.items():
+        whole.set_field(k, a)
+    steps = 120
+    g.step(steps)
+    assert whole.step(steps) == 0
+    beam = g.get_particles(2)
+    boundary = g.slabs[1].k0 * grid.dz
+    assert (beam["z"] >= boundary).sum() > 0, "the bunch reached the second slab"
+    assert g.parts[1].own(2)["r"].size > 0
+    for k in S.FIELDS:
+        assert _rel(g.get_field(k), whole.get_field(k)) <= 1e-8, k
+    for t in range(len(species)):
+        a, b = _sorted(g.get_particles(t)), _sorted(whole.get_particles(t))
+        assert a["r"].size == b["r"].size, t
+        for k in S.PARTICLE_KEYS:
+            assert _rel(a[k], b[k]) <= 1e-8, (t, k)
