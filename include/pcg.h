@@ -526,6 +526,21 @@ int pcg_keep_species_range(pcg_handle* h, int slot, double lo, double hi);
 #define PCG_FIELD_ALL (-1)
 int pcg_transfer_species_range(pcg_handle* src, int slot, double lo, double hi, double shift,
                                pcg_handle* dst, int dst_slot, int append, size_t* n);
+/* Several bands of src at once, with one wait for all their counts: every
+ * band is selected from src's particles as they are at the call, then the
+ * bands are appended or imported in order (a destination slot that gets
+ * two bands takes the first with append = 0 to replace, the second with
+ * append = 1).  counts (may be NULL) receives each band's count.  A band's
+ * destination must not be src itself. */
+typedef struct pcg_band {
+  int slot;           /* src species */
+  double lo, hi;      /* lo <= z < hi, src coordinates */
+  double shift;       /* subtracted from z: dst coordinates */
+  pcg_handle* dst;
+  int dst_slot;
+  int append;
+} pcg_band;
+int pcg_transfer_species_bands(pcg_handle* src, int nbands, const pcg_band* bands, size_t* counts);
 int pcg_copy_field_columns(pcg_handle* src, int which, int c0, int c1, pcg_handle* dst, int g0);
 
 int pcg_stage(pcg_handle* h, int stage);

@@ -41,6 +41,13 @@ class Diagnostics(ctypes.Structure):
                 ("kinetic_energy", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
 
 
+class Band(ctypes.Structure):
+    """pcg_band: one band of a device-to-device transfer."""
+    _fields_ = [("slot", ctypes.c_int), ("lo", ctypes.c_double), ("hi", ctypes.c_double),
+                ("shift", ctypes.c_double), ("dst", ctypes.c_void_p), ("dst_slot", ctypes.c_int),
+                ("append", ctypes.c_int)]
+
+
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
 _PF = ctypes.POINTER(ctypes.c_float)
@@ -71,6 +78,8 @@ SIGNATURES = {
                                  [ctypes.POINTER(ctypes.c_size_t)]),
     "pcg_keep_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D]),
     "pcg_transfer_species_range": (ctypes.c_int, [_H, ctypes.c_int, _D, _D, _D, _H, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(ctypes.c_size_t)]),
+    "pcg_transfer_species_bands": (ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(Band),
                                                   ctypes.POINTER(ctypes.c_size_t)]),
     "pcg_copy_field_columns": (ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, _H, ctypes.c_int]),
     "pcg_get_device": (ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int)]),

@@ -114,7 +114,8 @@ struct pcg_handle {
   size_t region_bytes = 0;
   double* region_out = nullptr;
   size_t region_out_n = 0;
-  unsigned* h_count = nullptr;  // pinned: a band's particle count
+  unsigned* h_count = nullptr;  // pinned: the band counts of a selection
+  int h_count_n = 0;
   double* staging = nullptr;  // host-to-device particle staging, reused
   size_t staging_n = 0;
   // kernel timers: event pairs per class, recycled after each query
@@ -788,8 +789,7 @@ int pcg_create(const pcg_config* cfg, pcg_handle** out) {
       cudaEventCreateWithFlags(&h->ev_staging_free, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_status, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_region, cudaEventDisableTiming) != cudaSuccess ||
-      cudaMallocHost((void**)&h->h_status_lag, sizeof(DevStatus)) != cudaSuccess ||
-      cudaMallocHost((void**)&h->h_count, sizeof(unsigned)) != cudaSuccess)
+      cudaMallocHost((void**)&h->h_status_lag, sizeof(DevStatus)) != cudaSuccess)
     return bail(PCG_ERR_CUDA);
   if (cfg->precision == PCG_PRECISION_F32 &&
       (cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1151,22 +1151,27 @@ int pcg_set_field_columns(pcg_handle* h, int which, int c0, int c1, const double
 
 namespace {
 
-// The live slots of species s with lo <= z < hi: their count in *m and
-// their indices in *sel (the handle's selection scratch).  Waits for the
-// handle's stream.
-int select_band(pcg_handle* h, Species& s, double lo, double hi, unsigned* m, const unsigned** sel) {
-  *m = 0;
+// One band of a selection: the live slots of species `slot` with lo <= z < hi.
+struct Band {
+  int slot;
+  double lo, hi;
+};
+
+// Selects every band (one pass over its species' slots each), then waits
+// once for the counts and the status of the work queued before: m[b] and
+// the indices sel[b] (the handle's selection scratch, valid until the next
+// selection).
+int select_bands(pcg_handle* h, const Band* bands, int nb, unsigned* m, const unsigned** sel) {
+  size_t tmp = 0, idx = 0;
+  for (int b = 0; b < nb; ++b) {
+    const size_t ns = h->sp[bands[b].slot].n;
+    if (ns > 0x7fffffffu) return fail(h, PCG_ERR_UNSUPPORTED, "a band selection of more than 2^31 slots");
+    tmp = std::max(tmp, region_select_bytes(ns));
+    idx += (ns + 63) & ~(size_t)63;
+  }
+  const size_t o_cnt = 0, o_idx = 256 + (((size_t)nb * sizeof(unsigned) + 255) & ~(size_t)255),
+               o_tmp = o_idx + ((4 * idx + 255) & ~(size_t)255), bytes = o_tmp + tmp;
   int rc;
-  const size_t ns = s.n;
-  if (ns == 0) return check_status(h);
-  if (ns > 0x7fffffffu) return fail(h, PCG_ERR_UNSUPPORTED, "a band selection of more than 2^31 slots");
-  // scratch: slot indices, selected indices, their count, flags, select temp
-  size_t tmp = 0;
-  cub::DeviceSelect::Flagged(nullptr, tmp, (const unsigned*)nullptr, (const unsigned char*)nullptr,
-                             (unsigned*)nullptr, (unsigned*)nullptr, (int)ns, h->stream);
-  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t o_sel = up(4 * ns), o_cnt = o_sel + up(4 * ns), o_flags = o_cnt + 256,
-               o_tmp = o_flags + up(ns), bytes = o_tmp + tmp;
   if (bytes > h->region_bytes) {
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     cudaFree(h->region);
@@ -1175,47 +1180,105 @@ int select_band(pcg_handle* h, Species& s, double lo, double hi, unsigned* m, co
     if ((rc = dalloc(h, &h->region, bytes)) != PCG_OK) return rc;
     h->region_bytes = bytes;
   }
-  unsigned* iota = (unsigned*)h->region;
-  unsigned* out = (unsigned*)(h->region + o_sel);
+  if (nb > h->h_count_n) {
+    if (h->h_count) cudaFreeHost(h->h_count);
+    h->h_count = nullptr;
+    h->h_count_n = 0;
+    if (cudaMallocHost((void**)&h->h_count, sizeof(unsigned) * nb) != cudaSuccess)
+      return fail(h, PCG_ERR_NOMEM, "pinned band counts");
+    h->h_count_n = nb;
+  }
   unsigned* cnt = (unsigned*)(h->region + o_cnt);
-  unsigned char* flags = h->region + o_flags;
-  SpeciesF64 v64{};
-  const SpeciesF32Buffers* b32;
-  const SpeciesF64* s64;
-  region_views(h, s, &v64, &b32, &s64);
-  region_flags(h->g, b32, s64, ns, lo, hi, flags, h->stream);
-  iota_u32(iota, ns, h->stream);
-  cub::DeviceSelect::Flagged(h->region + o_tmp, tmp, iota, flags, out, cnt, (int)ns, h->stream);
-  // the count and the status of the steps queued before, in one wait
-  CUDA_TRY(h, cudaMemcpyAsync(h->h_count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  unsigned* out = (unsigned*)(h->region + o_idx);
+  for (int b = 0; b < nb; ++b) {
+    Species& s = h->sp[bands[b].slot];
+    SpeciesF64 v64{};
+    const SpeciesF32Buffers* b32;
+    const SpeciesF64* s64;
+    region_views(h, s, &v64, &b32, &s64);
+    if (region_select(h->g, b32, s64, s.n, bands[b].lo, bands[b].hi, h->region + o_tmp, tmp, out, cnt + b,
+                      h->stream) != 0)
+      return fail(h, PCG_ERR_CUDA, "band selection");
+    sel[b] = out;
+    out += (s.n + 63) & ~(size_t)63;
+  }
+  // the counts and the status of the steps queued before, in one wait
+  CUDA_TRY(h, cudaMemcpyAsync(h->h_count, cnt, sizeof(unsigned) * nb, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   CUDA_TRY(h, cudaGetLastError());
   if ((rc = status_code(h, h->h_status)) != PCG_OK) return rc;
-  *m = *h->h_count;
-  *sel = out;
+  for (int b = 0; b < nb; ++b) m[b] = h->h_count[b];
+  return PCG_OK;
+}
+
+// Room for `total` gathered particles (6 doubles each) in region_out.
+int region_room(pcg_handle* h, size_t total) {
+  if (h->region_out_n >= total) return PCG_OK;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  cudaFree(h->region_out);
+  h->region_out = nullptr;
+  h->region_out_n = 0;
+  int rc = dalloc(h, &h->region_out, 6 * total);
+  if (rc != PCG_OK) return rc;
+  h->region_out_n = total;
   return PCG_OK;
 }
 
 // The m selected particles as 6 x m doubles (r, z - zshift, v_r, v_phi,
-// v_z, w) in the handle's region_out, queued on its stream.
-int gather_band(pcg_handle* h, Species& s, const unsigned* sel, unsigned m, double zshift) {
-  if (m == 0) return PCG_OK;
-  if (h->region_out_n < m) {
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    cudaFree(h->region_out);
-    h->region_out = nullptr;
-    h->region_out_n = 0;
-    int rc = dalloc(h, &h->region_out, 6 * (size_t)m);
-    if (rc != PCG_OK) return rc;
-    h->region_out_n = m;
-  }
+// v_z, w) at out, queued on the handle's stream.
+void gather_band(pcg_handle* h, Species& s, const unsigned* sel, unsigned m, double zshift, double* out) {
+  if (m == 0) return;
   SpeciesF64 v64{};
   const SpeciesF32Buffers* b32;
   const SpeciesF64* s64;
   region_views(h, s, &v64, &b32, &s64);
-  region_gather(h->g, b32, s64, sel, m, zshift, h->region_out, h->stream);
-  CUDA_TRY(h, cudaGetLastError());
+  region_gather(h->g, b32, s64, sel, m, zshift, out, h->stream);
+}
+
+// Appends (or, append = 0, imports in place of the species' particles) m
+// particles that lie as 6 x m doubles in src's device memory at data, on
+// dst's stream after src's ev_region; src's later work waits for the copy.
+int import_band(pcg_handle* src, const double* data, unsigned m, pcg_handle* dst, int dst_slot, int append) {
+  DeviceScope on_dst(dst->cfg.device);
+  Species& d = dst->sp[dst_slot];
+  int rc;
+  if (append && d.n + m > d.cap) {  // reclaim the dead slots first
+    if ((rc = check_status(dst)) != PCG_OK) return rc;
+    if (dst->h_status->dead_slots > dst->dead_dropped && (rc = compact(dst)) != PCG_OK) return rc;
+  }
+  const size_t n0 = append ? d.n : 0;
+  if (n0 + m > d.cap) return fail(dst, PCG_ERR_CAPACITY, "species '" + d.name + "' capacity exceeded");
+  dst->started = true;
+  if (m) {
+    if (dst->staging_n < m) {
+      CUDA_TRY(dst, cudaStreamSynchronize(dst->stream));
+      CUDA_TRY(dst, cudaStreamSynchronize(dst->copy));
+      cudaFree(dst->staging);
+      dst->staging = nullptr;
+      dst->staging_n = 0;
+      if ((rc = dalloc(dst, &dst->staging, 6 * (size_t)m)) != PCG_OK) return rc;
+      dst->staging_n = m;
+    }
+    CUDA_TRY(dst, cudaStreamWaitEvent(dst->stream, src->ev_region, 0));
+    // the staging buffer's last host upload has landed (put_particles waits for it)
+    const size_t bytes = sizeof(double) * 6 * (size_t)m;
+    if (src->cfg.device == dst->cfg.device)
+      CUDA_TRY(dst, cudaMemcpyAsync(dst->staging, data, bytes, cudaMemcpyDeviceToDevice, dst->stream));
+    else
+      CUDA_TRY(dst, cudaMemcpyPeerAsync(dst->staging, dst->cfg.device, data, src->cfg.device, bytes, dst->stream));
+  }
+  // a replacement with no particles still resets the species (ids, tile grouping)
+  if (m || !append) {
+    if (is_f64(dst)) launch_import_f64(dst->g, view64(dst, d), n0, m, dst->staging, dst->stream);
+    else f32_launch_import(dst->g, d.f32, n0, m, dst->staging, dst->stream);
+  }
+  d.n = n0 + m;
+  CUDA_TRY(dst, cudaEventRecord(dst->ev_staging_free, dst->stream));
+  CUDA_TRY(dst, cudaEventRecord(dst->ev_region, dst->stream));
+  CUDA_TRY(dst, cudaGetLastError());
+  DeviceScope on_src(src->cfg.device);
+  CUDA_TRY(src, cudaStreamWaitEvent(src->stream, dst->ev_region, 0));  // region_out is read
   return PCG_OK;
 }
 
@@ -1228,14 +1291,17 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
   if (std::isnan(lo) || std::isnan(hi)) return fail(h, PCG_ERR_ARG, "NaN band limit");
   *n = 0;
   Species& s = h->sp[slot];
+  const Band band{slot, lo, hi};
   unsigned m = 0;
   const unsigned* sel = nullptr;
-  int rc = select_band(h, s, lo, hi, &m, &sel);
+  int rc = select_bands(h, &band, 1, &m, &sel);
   if (rc != PCG_OK) return rc;
   *n = m;
   if (cap < m) return fail(h, PCG_ERR_CAPACITY, "export buffer too small");
   if (m == 0) return PCG_OK;
-  if ((rc = gather_band(h, s, sel, m, 0.0)) != PCG_OK) return rc;
+  if ((rc = region_room(h, m)) != PCG_OK) return rc;
+  gather_band(h, s, sel, m, 0.0, h->region_out);
+  CUDA_TRY(h, cudaGetLastError());
   double* dst[6] = {r, z, vr, vphi, vz, w};
   for (int a = 0; a < 6; ++a)
     if (dst[a])
@@ -1245,68 +1311,48 @@ int pcg_export_species_range(pcg_handle* h, int slot, double lo, double hi, size
   return PCG_OK;
 }
 
-int pcg_transfer_species_range(pcg_handle* src, int slot, double lo, double hi, double shift, pcg_handle* dst,
-                               int dst_slot, int append, size_t* n) {
-  if (!src || !dst || !n || slot < 0 || slot >= (int)src->sp.size() || dst_slot < 0 ||
-      dst_slot >= (int)dst->sp.size())
-    return PCG_ERR_ARG;
-  if (std::isnan(lo) || std::isnan(hi) || !std::isfinite(shift)) return fail(src, PCG_ERR_ARG, "bad band or shift");
-  *n = 0;
-  unsigned m = 0;
+int pcg_transfer_species_bands(pcg_handle* src, int nbands, const pcg_band* bands, size_t* counts) {
+  if (!src || nbands < 0 || (nbands && !bands)) return PCG_ERR_ARG;
+  for (int b = 0; b < nbands; ++b) {
+    const pcg_band& q = bands[b];
+    if (q.slot < 0 || q.slot >= (int)src->sp.size() || !q.dst || q.dst == src || q.dst_slot < 0 ||
+        q.dst_slot >= (int)q.dst->sp.size())
+      return fail(src, PCG_ERR_ARG, "band " + std::to_string(b) + ": bad species slot or destination");
+    if (std::isnan(q.lo) || std::isnan(q.hi) || !std::isfinite(q.shift))
+      return fail(src, PCG_ERR_ARG, "band " + std::to_string(b) + ": bad limits or shift");
+  }
+  if (nbands == 0) return PCG_OK;
+  std::vector<Band> sb(nbands);
+  for (int b = 0; b < nbands; ++b) sb[b] = Band{bands[b].slot, bands[b].lo, bands[b].hi};
+  std::vector<unsigned> m(nbands);
+  std::vector<const unsigned*> sel(nbands);
+  std::vector<size_t> off(nbands + 1, 0);
   int rc;
-  {  // select and gather on the source's GPU
+  {  // select all bands (one wait) and gather them on the source's GPU
     DeviceScope on_src(src->cfg.device);
-    Species& s = src->sp[slot];
-    const unsigned* sel = nullptr;
-    if ((rc = select_band(src, s, lo, hi, &m, &sel)) != PCG_OK) return rc;
-    if ((rc = gather_band(src, s, sel, m, shift)) != PCG_OK) return rc;
+    if ((rc = select_bands(src, sb.data(), nbands, m.data(), sel.data())) != PCG_OK) return rc;
+    for (int b = 0; b < nbands; ++b) off[b + 1] = off[b] + m[b];
+    if ((rc = region_room(src, off[nbands])) != PCG_OK) return rc;
+    for (int b = 0; b < nbands; ++b)
+      gather_band(src, src->sp[bands[b].slot], sel[b], m[b], bands[b].shift, src->region_out + 6 * off[b]);
+    CUDA_TRY(src, cudaGetLastError());
     CUDA_TRY(src, cudaEventRecord(src->ev_region, src->stream));
   }
-  {  // copy and import on the destination's GPU, after the gather
-    DeviceScope on_dst(dst->cfg.device);
-    Species& d = dst->sp[dst_slot];
-    if (append && d.n + m > d.cap) {  // reclaim the dead slots first
-      if ((rc = check_status(dst)) != PCG_OK) return rc;
-      if (dst->h_status->dead_slots > dst->dead_dropped && (rc = compact(dst)) != PCG_OK) return rc;
-    }
-    const size_t n0 = append ? d.n : 0;
-    if (n0 + m > d.cap) return fail(dst, PCG_ERR_CAPACITY, "species '" + d.name + "' capacity exceeded");
-    dst->started = true;
-    if (m) {
-      if (dst->staging_n < m) {
-        CUDA_TRY(dst, cudaStreamSynchronize(dst->stream));
-        CUDA_TRY(dst, cudaStreamSynchronize(dst->copy));
-        cudaFree(dst->staging);
-        dst->staging = nullptr;
-        dst->staging_n = 0;
-        if ((rc = dalloc(dst, &dst->staging, 6 * (size_t)m)) != PCG_OK) return rc;
-        dst->staging_n = m;
-      }
-      CUDA_TRY(dst, cudaStreamWaitEvent(dst->stream, src->ev_region, 0));
-      // the staging buffer's last host upload has landed (put_particles waits for it)
-      const size_t bytes = sizeof(double) * 6 * (size_t)m;
-      if (src->cfg.device == dst->cfg.device)
-        CUDA_TRY(dst, cudaMemcpyAsync(dst->staging, src->region_out, bytes, cudaMemcpyDeviceToDevice, dst->stream));
-      else
-        CUDA_TRY(dst, cudaMemcpyPeerAsync(dst->staging, dst->cfg.device, src->region_out, src->cfg.device, bytes,
-                                          dst->stream));
-    }
-    // a replacement with no particles still resets the species (ids, tile grouping)
-    if (m || !append) {
-      if (is_f64(dst)) launch_import_f64(dst->g, view64(dst, d), n0, m, dst->staging, dst->stream);
-      else f32_launch_import(dst->g, d.f32, n0, m, dst->staging, dst->stream);
-    }
-    d.n = n0 + m;
-    CUDA_TRY(dst, cudaEventRecord(dst->ev_staging_free, dst->stream));
-    CUDA_TRY(dst, cudaEventRecord(dst->ev_region, dst->stream));
-    CUDA_TRY(dst, cudaGetLastError());
+  for (int b = 0; b < nbands; ++b) {  // copy and import on each destination's GPU, in band order
+    if ((rc = import_band(src, src->region_out + 6 * off[b], m[b], bands[b].dst, bands[b].dst_slot,
+                          bands[b].append)) != PCG_OK)
+      return rc;
+    if (counts) counts[b] = m[b];
   }
-  {  // the source's later gathers wait for the copy out of region_out
-    DeviceScope on_src(src->cfg.device);
-    CUDA_TRY(src, cudaStreamWaitEvent(src->stream, dst->ev_region, 0));
-  }
-  *n = m;
   return PCG_OK;
+}
+
+int pcg_transfer_species_range(pcg_handle* src, int slot, double lo, double hi, double shift, pcg_handle* dst,
+                               int dst_slot, int append, size_t* n) {
+  if (!n) return PCG_ERR_ARG;
+  *n = 0;
+  const pcg_band band{slot, lo, hi, shift, dst, dst_slot, append};
+  return pcg_transfer_species_bands(src, 1, &band, n);
 }
 
 int pcg_copy_field_columns(pcg_handle* src, int which, int c0, int c1, pcg_handle* dst, int g0) {

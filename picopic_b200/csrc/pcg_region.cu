@@ -4,6 +4,8 @@
 // ends this way, in place of the reference's particle hand-over between
 // domains (SMB::particles_runaway_collector, SMB.cpp:194-564).
 #include <cuda_runtime.h>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "pcg_f32.h"
 #include "pcg_kernels.h"
@@ -29,13 +31,44 @@ __device__ __forceinline__ bool slot_z(const GridGeom& g, const SpeciesF32Buffer
   return true;
 }
 
-__global__ void flags_kernel(GridGeom g, SpeciesF32Buffers b32, SpeciesF64 s64, int f32, size_t n, double lo,
-                             double hi, unsigned char* flags) {
-  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  double z;
-  const bool live = slot_z(g, f32 ? &b32 : nullptr, &s64, j, &z);
-  flags[j] = live && z >= lo && z < hi ? 1 : 0;
+// lo <= z < hi for a live slot j, z as slot_z computes it (the selection
+// predicate of a band; keep_kernel's complement)
+struct BandTest {
+  GridGeom g;
+  const int* cell;
+  const float* off_z;
+  const double* r;
+  const double* z;
+  int f32;
+  double lo, hi;
+  __device__ __forceinline__ bool operator()(const unsigned& j) const {
+    double zz;
+    if (f32) {
+      const int c = cell[j];
+      if (c < 0) return false;
+      zz = ((double)cell_z_of(c) + (double)off_z[j]) * g.dz;
+    } else {
+      if (!(r[j] >= 0.0)) return false;
+      zz = z[j];
+    }
+    return zz >= lo && zz < hi;
+  }
+};
+
+BandTest band_test(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, double lo, double hi) {
+  BandTest t{};
+  t.g = g;
+  t.f32 = b32 ? 1 : 0;
+  if (b32) {
+    t.cell = b32->cell;
+    t.off_z = b32->off_z;
+  } else {
+    t.r = s64->r;
+    t.z = s64->z;
+  }
+  t.lo = lo;
+  t.hi = hi;
+  return t;
 }
 
 // out: 6 x m doubles (r, z - zshift, v_r, v_phi, v_z, w) of the slots idx[0..m)
@@ -90,16 +123,26 @@ __global__ void columns_f32_kernel(float* plane, int ld, int c0, int w, int rows
 
 }  // namespace
 
+size_t region_select_bytes(size_t n) {
+  size_t bytes = 0;
+  BandTest t{};
+  cub::DeviceSelect::If(nullptr, bytes, thrust::counting_iterator<unsigned>(0u), (unsigned*)nullptr,
+                        (unsigned*)nullptr, (int)n, t, (cudaStream_t)0);
+  return bytes;
+}
+
+int region_select(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
+                  double hi, void* temp, size_t temp_bytes, unsigned* out, unsigned* count, cudaStream_t s) {
+  if (n == 0) return cudaMemsetAsync(count, 0, sizeof(unsigned), s) == cudaSuccess ? 0 : -1;
+  return cub::DeviceSelect::If(temp, temp_bytes, thrust::counting_iterator<unsigned>(0u), out, count, (int)n,
+                               band_test(g, b32, s64, lo, hi), s) == cudaSuccess
+             ? 0
+             : -1;
+}
+
 void region_columns_f32(float* plane, int ld, int c0, int w, int rows, double* buf, bool set, cudaStream_t s) {
   const int n = w * rows;
   if (n > 0) columns_f32_kernel<<<blocks_for((size_t)n), kThreads, 0, s>>>(plane, ld, c0, w, rows, buf, set ? 1 : 0);
-}
-
-void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
-                  double hi, unsigned char* flags, cudaStream_t s) {
-  if (!n) return;
-  flags_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b32 ? *b32 : SpeciesF32Buffers{}, s64 ? *s64 : SpeciesF64{},
-                                                   b32 ? 1 : 0, n, lo, hi, flags);
 }
 
 void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, const unsigned* idx,

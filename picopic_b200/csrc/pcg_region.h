@@ -13,9 +13,13 @@
 
 namespace pcg {
 
-// flags[j] = 1 for the live slots j < n with lo <= z < hi
-void region_flags(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
-                  double hi, unsigned char* flags, cudaStream_t s);
+// Scratch bytes of region_select over n slots (at least those of any smaller n).
+size_t region_select_bytes(size_t n);
+// The indices of the live slots j < n with lo <= z < hi, in slot order, into
+// out and their count into *count (device memory); one pass over the
+// slots' positions.  Nonzero on a CUDA error.
+int region_select(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, size_t n, double lo,
+                  double hi, void* temp, size_t temp_bytes, unsigned* out, unsigned* count, cudaStream_t s);
 // out: r, z - zshift, v_r, v_phi, v_z, w of the slots idx[0..m), m doubles apart
 void region_gather(const GridGeom& g, const SpeciesF32Buffers* b32, const SpeciesF64* s64, const unsigned* idx,
                    size_t m, double zshift, double* out, cudaStream_t s);

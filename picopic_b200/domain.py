@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._ffi import Config, Diagnostics, PcgError, load
+from ._ffi import Band, Config, Diagnostics, PcgError, load
 
 PUSHERS = {"boris": 0, "borisadaptive": 1, "borisrel": 2, "vay": 3, "hc": 4}
 CURRENTS = {"vb": 0, "zigzag": 1}
@@ -239,6 +239,23 @@ class Domain:
         if rc != 0:
             self._raise_pair(rc, "pcg_transfer_species_range", dst)
         return n.value
+
+    def transfer_bands(self, bands) -> list:
+        """Several bands at once, one wait for all counts: bands of
+        (slot, lo, hi, shift, dst, dst_slot, append), selected from this
+        domain's particles as they are now, then imported in order; returns
+        each band's count."""
+        n = len(bands)
+        arr = (Band * max(n, 1))()
+        for q, (slot, lo, hi, shift, dst, dst_slot, append) in enumerate(bands):
+            arr[q] = Band(int(slot), float(lo), float(hi), float(shift), dst.h.value, int(dst_slot),
+                          1 if append else 0)
+        counts = (ctypes.c_size_t * max(n, 1))()
+        rc = self.lib.pcg_transfer_species_bands(self.h, n, arr, counts)
+        if rc != 0:
+            dst = bands[0][4] if bands else self
+            self._raise_pair(rc, "pcg_transfer_species_bands", dst)
+        return [counts[q] for q in range(n)]
 
     def _raise_pair(self, rc, where, dst):
         """An error of a call on two handles: the last message of each."""

@@ -307,7 +307,7 @@ class SlabGroup:
             self.parts.append(_SlabEngine(grid, s, e, self.nsp))
         # device to device (GPU domains: pcg_transfer_species_range and
         # pcg_copy_field_columns, a peer copy between GPUs), else through the host
-        can = all(hasattr(se.engine, "transfer_range") and hasattr(se.engine, "copy_field_columns")
+        can = all(hasattr(se.engine, "transfer_bands") and hasattr(se.engine, "copy_field_columns")
                   for se in self.parts)
         if on_device and not can:
             raise ValueError("the slabs' engines have no device-to-device exchange")
@@ -361,20 +361,24 @@ class SlabGroup:
 
     def _exchange_on_device(self):
         """The same exchange with the strips moved between the domains on the
-        device; only the particle counts reach the host.  The slabs go in
-        order: a slab's hand-over sees the migrants its left neighbour has
-        just appended and passes on any that lie outside its own cells."""
+        device (one band transfer call, one host wait, per slab and phase);
+        only the particle counts reach the host.  The slabs go in order: a
+        slab's hand-over sees the migrants its left neighbour has just
+        appended and passes on any that lie outside its own cells."""
         last, dz, inf = len(self.parts) - 1, self.grid.dz, np.inf
         for i, se in enumerate(self.parts):
             s = se.slab
+            bands = []
             for t in range(self.nsp):
                 if not s.first:
                     nb = self.parts[i - 1]
-                    se.engine.transfer_range(t, -inf, se.lo, nb.z0 - se.z0, nb.engine, t, append=True)
+                    bands.append((t, -inf, se.lo, nb.z0 - se.z0, nb.engine, t, True))
                 if not s.last:
                     nb = self.parts[i + 1]
-                    se.engine.transfer_range(t, se.hi, inf, nb.z0 - se.z0, nb.engine, t, append=True)
-                if not (s.first and s.last):
+                    bands.append((t, se.hi, inf, nb.z0 - se.z0, nb.engine, t, True))
+            se.engine.transfer_bands(bands)
+            if not (s.first and s.last):
+                for t in range(self.nsp):
                     se.engine.keep_range(t, se.lo, se.hi)
         for i, se in enumerate(self.parts):
             s = se.slab
@@ -385,18 +389,21 @@ class SlabGroup:
             if i < last:
                 src = self.parts[i + 1]
                 src.engine.copy_field_columns(src.col(s.k1), src.col(s.e1), se.engine, se.col(s.k1))
+        # ghost particles: slab i sends to i - 1 (after i - 2 has replaced that
+        # slab's ghosts: append) and to i + 1 (the first to reach it: replace)
+        for i, se in enumerate(self.parts):
+            s = se.slab
+            bands = []
             for t in range(self.nsp):
-                replace = True
-                if i > 0:  # the left slab's own particles from lw cells before its end
-                    src = self.parts[i - 1]
-                    lo = (src.slab.k1 - lw - src.slab.e0) * dz
-                    src.engine.transfer_range(t, lo, inf, se.z0 - src.z0, se.engine, self.nsp + t, append=False)
-                    replace = False
-                if i < last:  # the right slab's own particles up to rw cells after its start
-                    src = self.parts[i + 1]
-                    hi = (src.slab.k0 + rw - src.slab.e0) * dz
-                    src.engine.transfer_range(t, -inf, hi, se.z0 - src.z0, se.engine, self.nsp + t,
-                                              append=not replace)
+                if i > 0:  # the left slab's right ghost cells: our first cells
+                    dst = self.parts[i - 1]
+                    hi = (s.k0 + self.widths[i - 1][1] - s.e0) * dz
+                    bands.append((t, -inf, hi, dst.z0 - se.z0, dst.engine, self.nsp + t, i - 1 > 0))
+                if i < last:  # the right slab's left ghost cells: our last cells
+                    dst = self.parts[i + 1]
+                    lo = (s.k1 - self.widths[i + 1][0] - s.e0) * dz
+                    bands.append((t, lo, inf, dst.z0 - se.z0, dst.engine, self.nsp + t, False))
+            se.engine.transfer_bands(bands)
 
     # -- global views ------------------------------------------------------------------
     def get_field(self, name):

@@ -196,3 +196,36 @@ def test_device_buffers(precision):
     empty = src.export_range_device(0, hi, lo)
     assert empty.shape == (6, 0)
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_transfer_bands_in_one_call(precision):
+    """Several bands of one source to two destinations in one call: each band
+    selected from the source as it was at the call, imported in band order
+    (the first band to a slot replaces, the next appends)."""
+    grid = small_grid(nr=16, nz=96)
+    src, a, b = (_domain(grid, precision) for _ in range(3))
+    src.set_particles(0, *particles(grid, 6000, 41))
+    a.set_particles(0, *particles(grid, 300, 42))
+    b.set_particles(0, *particles(grid, 300, 43))
+    src.step(1)
+    dz = grid.dz
+    bands = [(0, -np.inf, 20 * dz, 0.0, a, 0, False),
+             (0, 70 * dz, np.inf, 10 * dz, b, 0, True),
+             (0, 20 * dz, 40 * dz, -5 * dz, a, 0, True)]
+    expect_a = [src.export_range(0, -np.inf, 20 * dz), src.export_range(0, 20 * dz, 40 * dz)]
+    expect_a[1]["z"] = expect_a[1]["z"] + 5 * dz
+    before_b = b.get_particles(0)
+    band_b = src.export_range(0, 70 * dz, np.inf)
+    band_b["z"] = band_b["z"] - 10 * dz
+    counts = src.transfer_bands(bands)
+    assert counts == [expect_a[0]["r"].size, band_b["r"].size, expect_a[1]["r"].size]
+    tol = 0 if precision == "f64" else 1e-7
+    for got, parts in ((a.get_particles(0), expect_a), (b.get_particles(0), [before_b, band_b])):
+        x, y = _sorted(got), _sorted({k: np.concatenate([p[k] for p in parts]) for k in KEYS})
+        assert x["r"].size == y["r"].size
+        for k in KEYS:
+            np.testing.assert_allclose(x[k], y[k], rtol=0, atol=tol * np.abs(y[k]).max(), err_msg=k)
+    from picopic_b200._ffi import PcgError
+    with pytest.raises(PcgError):  # a band into the source itself
+        src.transfer_bands([(0, 0.0, dz, 0.0, src, 0, True)])
