@@ -1172,13 +1172,14 @@ int select_bands(pcg_handle* h, const Band* bands, int nb, unsigned* m, const un
   const size_t o_cnt = 0, o_idx = 256 + (((size_t)nb * sizeof(unsigned) + 255) & ~(size_t)255),
                o_tmp = o_idx + ((4 * idx + 255) & ~(size_t)255), bytes = o_tmp + tmp;
   int rc;
-  if (bytes > h->region_bytes) {
+  if (bytes > h->region_bytes) {  // grown with headroom: species counts creep up between exchanges
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     cudaFree(h->region);
     h->region = nullptr;
     h->region_bytes = 0;
-    if ((rc = dalloc(h, &h->region, bytes)) != PCG_OK) return rc;
-    h->region_bytes = bytes;
+    const size_t grown = bytes + bytes / 4;
+    if ((rc = dalloc(h, &h->region, grown)) != PCG_OK) return rc;
+    h->region_bytes = grown;
   }
   if (nb > h->h_count_n) {
     if (h->h_count) cudaFreeHost(h->h_count);
@@ -1219,9 +1220,10 @@ int region_room(pcg_handle* h, size_t total) {
   cudaFree(h->region_out);
   h->region_out = nullptr;
   h->region_out_n = 0;
-  int rc = dalloc(h, &h->region_out, 6 * total);
+  const size_t grown = total + total / 4 + 1024;
+  int rc = dalloc(h, &h->region_out, 6 * grown);
   if (rc != PCG_OK) return rc;
-  h->region_out_n = total;
+  h->region_out_n = grown;
   return PCG_OK;
 }
 
@@ -1257,8 +1259,9 @@ int import_band(pcg_handle* src, const double* data, unsigned m, pcg_handle* dst
       cudaFree(dst->staging);
       dst->staging = nullptr;
       dst->staging_n = 0;
-      if ((rc = dalloc(dst, &dst->staging, 6 * (size_t)m)) != PCG_OK) return rc;
-      dst->staging_n = m;
+      const size_t grown = (size_t)m + m / 4 + 1024;
+      if ((rc = dalloc(dst, &dst->staging, 6 * grown)) != PCG_OK) return rc;
+      dst->staging_n = grown;
     }
     CUDA_TRY(dst, cudaStreamWaitEvent(dst->stream, src->ev_region, 0));
     // the staging buffer's last host upload has landed (put_particles waits for it)
