@@ -397,7 +397,7 @@ int stage_inject(pcg_handle* h) {
     if (is_f64(h)) {
       launch_inject_f64(h->g, view64(h, s), s.n, count, b, h->stream);
     } else {
-      f32_launch_inject(h->g, s.f32, s.n, count, b, h->stream);
+      f32_launch_inject(h->g, s.f32, s.n, count, b, h->d_status, h->stream);
     }
     s.n += count;
     h->launches += 1;
@@ -985,7 +985,7 @@ static int put_particles(pcg_handle* h, int slot, size_t n, const double* r, con
     CUDA_TRY(h, cudaEventRecord(h->ev_copied, h->copy));
     CUDA_TRY(h, cudaStreamWaitEvent(h->stream, h->ev_copied, 0));
     if (is_f64(h)) launch_import_f64(h->g, view64(h, s), n0, n, stage, h->stream);
-    else f32_launch_import(h->g, s.f32, n0, n, stage, h->stream);
+    else f32_launch_import(h->g, s.f32, n0, n, stage, h->d_status, h->stream);
     CUDA_TRY(h, cudaEventRecord(h->ev_staging_free, h->stream));
     // the caller may reuse its host arrays once this call returns
     CUDA_TRY(h, cudaEventSynchronize(h->ev_copied));
@@ -1274,7 +1274,7 @@ int import_band(pcg_handle* src, const double* data, unsigned m, pcg_handle* dst
   // a replacement with no particles still resets the species (ids, tile grouping)
   if (m || !append) {
     if (is_f64(dst)) launch_import_f64(dst->g, view64(dst, d), n0, m, dst->staging, dst->stream);
-    else f32_launch_import(dst->g, d.f32, n0, m, dst->staging, dst->stream);
+    else f32_launch_import(dst->g, d.f32, n0, m, dst->staging, dst->d_status, dst->stream);
   }
   d.n = n0 + m;
   CUDA_TRY(dst, cudaEventRecord(dst->ev_staging_free, dst->stream));

@@ -114,10 +114,12 @@ void f32_launch_yee_e(const YeeArgs<float>& a, cudaStream_t s);
 // dst[q] = a[q] + b[q], q < n (the external fields added to the step's gather planes)
 void f32_add_planes(float* dst, const float* a, const float* b, size_t n, cudaStream_t s);
 void f32_launch_yee_h(const YeeArgs<float>& a, int fixed, cudaStream_t s);
+// Positions outside the grid (or not finite: kErrNanPosition) become dead
+// slots counted in st->removed and st->dead_slots.
 void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsigned count,
-                       const BeamInject& bi, cudaStream_t s);
+                       const BeamInject& bi, DevStatus* st, cudaStream_t s);
 void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_t n,
-                       const double* src, cudaStream_t s);
+                       const double* src, DevStatus* st, cudaStream_t s);
 // One step of a species; returns the new slot count (a tile sort drops dead
 // particles).  Sorts when the species has no tile grouping, when appended
 // particles exceed 1/4 of the slots, when more than 1 % of the particles

@@ -37,16 +37,46 @@ __device__ __forceinline__ void split_position(double x_m, double d, int* cell, 
   *off = f;
 }
 
+// The float layout's cell word of a position.  A position outside the
+// grid becomes a dead slot, counted as removed, as the runaway collector
+// removes such particles (SMB.cpp:252-337: r < 0, z < 0, r >= R, z >= L):
+// the cell of such a position has no tile to be sorted into.  The double
+// layout stops a step at positions more than a cell beyond the grid
+// (kErrOutOfGrid) and at positions that are not finite numbers
+// (kErrNanPosition, the reference's fatal error, pusherBoris.cpp:51-57);
+// both are raised here too, and the particle dropped.
+__device__ __forceinline__ int place(const GridGeom& g, double r, double z, float* fr, float* fz, DevStatus* st) {
+  bool dead = false;
+  if (!(isfinite(r) && isfinite(z))) {
+    raise_error(st, kErrNanPosition);
+    dead = true;
+  } else if (!(r >= 0.0 && z >= 0.0 && r / g.dr < (double)g.nr && z / g.dz < (double)g.nz)) {
+    if (!(r >= -1.5 * g.dr && r < (g.nr + 1) * g.dr && z >= -1.5 * g.dz && z < (g.nz + 1) * g.dz))
+      raise_error(st, kErrOutOfGrid);
+    dead = true;
+  }
+  int ci = 0, ck = 0;
+  if (!dead) {
+    split_position(r, g.dr, &ci, fr);
+    split_position(z, g.dz, &ck, fz);
+    dead = ci < 0 || ck < 0 || ci >= g.nr || ck >= g.nz;
+  }
+  if (dead) {
+    *fr = *fz = 0.f;
+    atomicAdd(&st->removed, 1ull);
+    atomicAdd(&st->dead_slots, 1ull);
+    return kDeadCell;
+  }
+  return pack_cell(ci, ck);
+}
+
 __global__ void import_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, size_t n,
-                              const double* src) {
+                              const double* src, DevStatus* st) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   size_t j = n0 + i;
-  int ci, ck;
   float fr, fz;
-  split_position(src[i], g.dr, &ci, &fr);
-  split_position(src[n + i], g.dz, &ck, &fz);
-  b.cell[j] = pack_cell(ci, ck);
+  b.cell[j] = place(g, src[i], src[n + i], &fr, &fz, st);
   b.off_r[j] = fr;
   b.off_z[j] = fz;
   b.vr[j] = (float)src[2 * n + i];
@@ -59,7 +89,7 @@ __global__ void import_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, size_t
 // BeamP::inject (beamP.cpp:100-145), or the Gaussian bunch, with the same
 // Philox stream as the double path; positions are computed in double.
 __global__ void inject_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, unsigned count,
-                              BeamInject bi) {
+                              BeamInject bi, DevStatus* st) {
   unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const double dr = g.dr, dz = g.dz;
@@ -68,11 +98,8 @@ __global__ void inject_kernel(GridGeom g, SpeciesF32Buffers b, size_t n0, unsign
   double pos_r, pos_z, wgt;
   beam_particle(bi, dr, dz, u, &pos_r, &pos_z, &wgt);
   const size_t j = n0 + i;
-  int ci, ck;
   float fr, fz;
-  split_position(pos_r, dr, &ci, &fr);
-  split_position(pos_z, dz, &ck, &fz);
-  b.cell[j] = pack_cell(ci, ck);
+  b.cell[j] = place(g, pos_r, pos_z, &fr, &fz, st);  // a bunch wider than the domain loses its edge
   b.off_r[j] = fr;
   b.off_z[j] = fz;
   b.vr[j] = 0.f;
@@ -489,20 +516,20 @@ void f32_launch_yee_h(const YeeArgs<float>& a, int fixed, cudaStream_t s) {
 }
 
 void f32_launch_inject(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, unsigned count,
-                       const BeamInject& bi, cudaStream_t s) {
+                       const BeamInject& bi, DevStatus* st, cudaStream_t s) {
   if (!count) return;
-  inject_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, b, n0, count, bi);
+  inject_kernel<<<(count + kThreads - 1) / kThreads, kThreads, 0, s>>>(g, b, n0, count, bi, st);
   b.next_id += count;
 }
 
 void f32_launch_import(const GridGeom& g, SpeciesF32Buffers& b, size_t n0, size_t n,
-                       const double* src, cudaStream_t s) {
+                       const double* src, DevStatus* st, cudaStream_t s) {
   if (n0 == 0) {  // a replacement: ids restart, no tile grouping yet
     b.next_id = 0;
     b.sorted_n = 0;
     b.steps_since_sort = 1 << 30;
   }
-  if (n) import_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b, n0, n, src);
+  if (n) import_kernel<<<blocks_for(n), kThreads, 0, s>>>(g, b, n0, n, src, st);
   b.next_id += (unsigned)n;
 }
 

@@ -9,12 +9,12 @@ from tests.cases import ELECTRONS, IONS, particles, small_grid, thermal_plasma
 pytestmark = pytest.mark.gpu
 
 
-def _domain(precision, n=0, seed=3):
+def _domain(precision, n=0, seed=3, cap=0):
     from picopic_b200 import Domain
     grid = small_grid(nr=16, nz=64, pml=False)
     d = Domain(grid, precision=precision, quirks="fixed", seed=seed)
-    d.add(ELECTRONS, capacity=max(n, 1) + 16)
-    d.add(IONS, capacity=max(n, 1) + 16)
+    d.add(ELECTRONS, capacity=max(n, cap, 1) + 16)
+    d.add(IONS, capacity=max(n, cap, 1) + 16)
     if n:
         for i, sp in enumerate((ELECTRONS, IONS)):
             d.set_particles(i, *particles(grid, n, seed + i, mass=sp.mass))
@@ -76,3 +76,48 @@ def test_errors_for_bad_arguments():
         d.tile_sort(0)                       # the double layout has no tiles
     with pytest.raises(PcgError):
         d.set_particles(0, *particles(grid, 500, 9))  # capacity 116
+
+
+def _with(grid, p, extra):
+    """Particle arrays p with the particles of `extra` (r, z, vr, vphi, vz, w tuples) appended."""
+    return [np.concatenate([np.asarray(a, float), np.array([e[q] for e in extra], float)])
+            for q, a in enumerate(p)]
+
+
+def test_float_import_drops_positions_outside_the_grid():
+    """The float layout has no cell for a position outside the grid: such a
+    particle is dropped at import and counted as removed, as the runaway
+    collector removes it (a position within a cell of the grid raises no
+    error; one farther out raises the out-of-grid error the double path
+    raises, a position that is not a number the NaN error)."""
+    from picopic_b200._ffi import PcgError
+    d, grid = _domain("f32", cap=200)
+    p = particles(grid, 100, 5)
+    R, L = grid.radius, grid.longitude
+    near = [(R + 0.5 * grid.dr, L / 2, 0, 0, 0, 1e5), (R / 2, -0.5 * grid.dz, 0, 0, 0, 1e5),
+            (R / 2, L, 0, 0, 0, 1e5)]
+    d.set_particles(0, *_with(grid, p, near))
+    assert d.count(0) == 100
+    assert d.diag().removed == 3
+    d.step(2)
+    d.synchronize()
+    for bad, code in (((5 * R, L / 2, 0, 0, 0, 1e5), -4), ((float("nan"), L / 2, 0, 0, 0, 1e5), -10)):
+        e, _ = _domain("f32", cap=200)
+        e.set_particles(0, *_with(grid, p, [bad]))
+        with pytest.raises(PcgError) as err:
+            e.synchronize()
+        assert err.value.code == code
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_superluminal_particle_stops_the_step(precision):
+    """A particle faster than light ends the step with PCG_ERR_SUPERLUMINAL,
+    the reference's fatal error (rel.cpp:33-34)."""
+    from picopic_b200._ffi import PcgError
+    d, grid = _domain(precision, cap=300)
+    p = particles(grid, 200, 6)
+    d.set_particles(0, *_with(grid, p, [(grid.radius / 2, grid.longitude / 2, 0, 0, 3.2e8, 1e5)]))
+    d.step(1)
+    with pytest.raises(PcgError) as err:
+        d.synchronize()
+    assert err.value.code == -11
