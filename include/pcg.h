@@ -170,7 +170,12 @@ int pcg_add_beam(pcg_handle* h, int id, const char* name, double charge_e, doubl
 
 /* Replace (import) or extend (append) a species' particles from host SoA.
  * An append that would exceed the capacity first reclaims the species'
- * dead slots (a compaction, which waits for the stream). */
+ * dead slots (a compaction, which waits for the stream).  The float layout
+ * drops a position outside the grid at once (counted in
+ * pcg_diagnostics.removed, as the runaway collector counts it); one more
+ * than a cell beyond the grid, or not a number, also makes the next call
+ * that reads the status return PCG_ERR_STATE or PCG_ERR_NAN, which the
+ * double layout returns from the step that meets such a particle. */
 int pcg_import_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
                        const double* vr, const double* vphi, const double* vz, const double* w);
 int pcg_append_species(pcg_handle* h, int slot, size_t n, const double* r, const double* z,
