@@ -1,6 +1,9 @@
 // pcg_f32_pair.cuh — the plasma step of the single-precision path, two
 // macroparticles per thread in Blackwell's packed FP32 pairs.
 //
+// Two instances: the relativistic Boris pusher with the Villasenor-Buneman
+// current, and the Vay pusher with the ZigZag current.
+//
 // The common case of a sorted plasma tile is a particle that stays in an
 // interior cell during the step: no wall, no cell crossing, a single
 // Villasenor-Buneman segment.  For that case each thread takes two slots of
@@ -111,7 +114,7 @@ struct PairWindow {
 // it did not complete is left untouched for the scalar path.  A particle in
 // a cell outside [rlo, rhi] x [zlo, zhi], or a dead slot, never enters: its
 // lane computes on the other particle's cell and is discarded.
-template <int FIX>
+template <int FIX, int KIND>
 __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF32Buffers& b, unsigned ja,
                                                unsigned jb, const Slot& A, const Slot& B, bool hasA, bool hasB,
                                                const PairWindow& W, bool& okA, bool& okB) {
@@ -193,12 +196,41 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
     if (FIX) E1 = add(E1, t11); else E2 = add(E2, t11);  // maxwellSolver.hpp:313
   }
 
-  // ---- relativistic Boris push (pusherBoris.cpp:33-149) ----
   float2 v0 = make_float2(A.vr, B.vr), v1 = make_float2(A.vphi, B.vphi), v2 = make_float2(A.vz, B.vz);
-  const float2 ck = bc(a.c2m), ic2 = bc(1.f / kC2);
-  E0 = mul(E0, ck); E1 = mul(E1, ck); E2 = mul(E2, ck);
+  const float2 ic2 = bc(1.f / kC2);
   const float2 beta = mul(fma(v2, v2, fma(v1, v1, mul(v0, v0))), ic2);
   const bool subA = beta.x < 1.f, subB = beta.y < 1.f;  // superluminal or NaN: the scalar path reports it
+  if constexpr (KIND == 1) {
+    // ---- Vay push (pusherVay.cpp:22-114), as the scalar push computes it: u =
+    // gamma v, in units of c in the fixed mode and in m/s as the reference has it ----
+    const float cn = FIX ? 1.f / 3.0e8f : 1.f;
+    const float2 g0 = rsq(one_minus(beta));
+    const float2 gc = FIX ? mul(g0, bc(cn)) : g0;
+    const float2 u0 = mul(v0, gc), u1 = mul(v1, gc), u2 = mul(v2, gc);
+    const float2 ek = bc(2.f * a.c2m * cn), bk = bc(a.bk);
+    B0 = mul(B0, bk); B1 = mul(B1, bk); B2 = mul(B2, bk);
+    const float2 uu = fma(u2, u2, fma(u1, u1, mul(u0, u0)));
+    const float2 gi = FIX ? rsq(add(bc(1.f), uu)) : rsq(fma(uu, ic2, bc(1.f)));
+    const float2 up0 = fma(gi, fma(u1, B2, mul(mul(u2, B1), bc(-1.f))), fma(E0, ek, u0));
+    const float2 up1 = fma(gi, fma(u2, B0, mul(mul(u0, B2), bc(-1.f))), fma(E1, ek, u1));
+    const float2 up2 = fma(gi, fma(u0, B1, mul(mul(u1, B0), bc(-1.f))), fma(E2, ek, u2));
+    const float2 Bsq = fma(B2, B2, fma(B1, B1, mul(B0, B0)));
+    const float2 s0 = sub(fma(up2, up2, fma(up1, up1, fma(up0, up0, bc(1.f)))), Bsq);
+    const float2 ub = fma(up2, B2, fma(up1, B1, mul(up0, B0)));
+    const float2 al = rsq(mul(bc(0.5f), add(s0, sqr(fma(s0, s0, mul(bc(4.f), fma(ub, ub, Bsq)))))));
+    B0 = mul(B0, al); B1 = mul(B1, al); B2 = mul(B2, al);
+    const float2 sc = rcp(fma(B2, B2, fma(B1, B1, fma(B0, B0, bc(1.f)))));
+    const float2 ab = fma(up2, B2, fma(up1, B1, mul(up0, B0)));
+    const float2 p0 = mul(sc, fma(ab, B0, fma(B2, up1, fma(mul(B1, up2), bc(-1.f), up0))));
+    const float2 p1 = mul(sc, fma(ab, B1, fma(B0, up2, fma(mul(B2, up0), bc(-1.f), up1))));
+    const float2 p2 = mul(sc, fma(ab, B2, fma(B1, up0, fma(mul(B0, up1), bc(-1.f), up2))));
+    const float2 pp = fma(p2, p2, fma(p1, p1, mul(p0, p0)));
+    const float2 go = FIX ? mul(rsq(add(bc(1.f), pp)), bc(3.0e8f)) : rsq(fma(pp, ic2, bc(1.f)));
+    v0 = mul(p0, go); v1 = mul(p1, go); v2 = mul(p2, go);
+  } else {
+  // ---- relativistic Boris push (pusherBoris.cpp:33-149) ----
+  const float2 ck = bc(a.c2m);
+  E0 = mul(E0, ck); E1 = mul(E1, ck); E2 = mul(E2, ck);
   float2 gm = rsq(one_minus(beta));
   v0 = fma(v0, gm, E0); v1 = fma(v1, gm, E1); v2 = fma(v2, gm, E2);
   gm = mul(rsq(fma(fma(v2, v2, fma(v1, v1, mul(v0, v0))), ic2, bc(1.f))), bc(a.bk));
@@ -218,6 +250,7 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   }
   gm = rsq(fma(fma(v2, v2, fma(v1, v1, mul(v0, v0))), ic2, bc(1.f)));
   v0 = mul(v0, gm); v1 = mul(v1, gm); v2 = mul(v2, gm);
+  }
 
   // ---- move in the local Cartesian frame and back to r-z (specieP.cpp:482-491, 609-640) ----
   const float2 dx = mul(v0, bc(a.dt_dr)), dyp = mul(v1, bc(a.dt_dr)), dYv = mul(v2, bc(a.dt_dz));
@@ -236,19 +269,52 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   const float2 dX = FIX ? sub(frn, fr) : dXv, dY = FIX ? sub(fzn, fz) : dYv;
   const float2 ixo = rcp(x0);
   const float2 t = mul(dX, ixo);
-  // the in-cell case with the logarithm's series valid (|t| < 0.02); motion
-  // below 1e-15 m on an axis takes the strict-motion branch (currentVB.cpp:500-729)
-  okA = preA && subA && frn.x >= 0.f && frn.x < 1.f && fzn.x >= 0.f && fzn.x < 1.f && X.x > 0.5f &&
-        fabsf(t.x) < 0.02f && fabsf(dX.x) >= a.mnzl_r && fabsf(dY.x) >= a.mnzl_z;
-  okB = preB && subB && frn.y >= 0.f && frn.y < 1.f && fzn.y >= 0.f && fzn.y < 1.f && X.y > 0.5f &&
-        fabsf(t.y) < 0.02f && fabsf(dX.y) >= a.mnzl_r && fabsf(dY.y) >= a.mnzl_z;
+  if constexpr (KIND == 1) {  // the in-cell case
+    okA = preA && subA && frn.x >= 0.f && frn.x < 1.f && fzn.x >= 0.f && fzn.x < 1.f && X.x > 0.5f;
+    okB = preB && subB && frn.y >= 0.f && frn.y < 1.f && fzn.y >= 0.f && fzn.y < 1.f && X.y > 0.5f;
+  } else {
+    // the in-cell case with the logarithm's series valid (|t| < 0.02); motion
+    // below 1e-15 m on an axis takes the strict-motion branch (currentVB.cpp:500-729)
+    okA = preA && subA && frn.x >= 0.f && frn.x < 1.f && fzn.x >= 0.f && fzn.x < 1.f && X.x > 0.5f &&
+          fabsf(t.x) < 0.02f && fabsf(dX.x) >= a.mnzl_r && fabsf(dY.x) >= a.mnzl_z;
+    okB = preB && subB && frn.y >= 0.f && frn.y < 1.f && fzn.y >= 0.f && fzn.y < 1.f && X.y > 0.5f &&
+          fabsf(t.y) < 0.02f && fabsf(dX.y) >= a.mnzl_r && fabsf(dY.y) >= a.mnzl_z;
+  }
   if (!okA && !okB) return;
   const float2 cs = sqr(fma(sn, mul(sn, bc(-1.f)), bc(1.f)));
   const float2 vr2 = fma(cs, v0, mul(mul(sn, v1), bc(-1.f)));
   const float2 vp2 = fma(sn, v0, mul(cs, v1));
-
-  // ---- in-cell Villasenor-Buneman deposit (currentVB.cpp:22-173, 398-498) ----
   const float2 w = make_float2(A.w, B.w);
+  // the eight node currents of each particle: J_phi at (i, k), (i+1, k),
+  // (i, k+1), (i+1, k+1); J_z at (i, k), (i+1, k); J_r at (i, k), (i, k+1)
+  float2 J[8];
+  if constexpr (KIND == 1) {
+    // ---- in-cell ZigZag deposit (currentZigZag.cpp:22-136) as the scalar
+    // zigzag computes it: relay point at the mid-point, weights in metres ----
+    const float2 oov = mul(bc(a.zz_vol), rcp(fma(bc(2.f), fi, bc(1.f))));
+    const float2 ro = mul(x0, bc(a.dr_m)), rn = mul(add(fi, frn), bc(a.dr_m));
+    const float2 Fp = mul(w, vp2);
+    const float2 Wp = mul(mul(vp2, bc(a.dt_s)), rcp(mul(bc(2.f * 3.14159265f), add(ro, rn))));
+    const float2 xr = mul(bc(0.5f), add(fr, frn)), yr = mul(bc(0.5f), add(fz, fzn));
+    const float2 cod = mul(w, bc(1.f / a.dt_s));
+    const float2 cr = mul(cod, bc(a.dr_m)), cz = mul(cod, bc(a.dz_m));
+    const float2 Fr1 = mul(cr, sub(xr, fr)), Fr2 = mul(cr, sub(frn, xr));
+    const float2 Fz1 = mul(cz, sub(yr, fz)), Fz2 = mul(cz, sub(fzn, yr));
+    const float2 Wr1 = mul(bc(a.dr_m), mul(bc(0.5f), add(fr, xr))), Wr2 = mul(bc(a.dr_m), mul(bc(0.5f), add(frn, xr)));
+    const float2 Wz1 = mul(bc(a.dz_m), mul(bc(0.5f), add(fz, yr))), Wz2 = mul(bc(a.dz_m), mul(bc(0.5f), add(fzn, yr)));
+    const float2 mWr1 = one_minus(Wr1), mWr2 = one_minus(Wr2), mWz1 = one_minus(Wz1), mWz2 = one_minus(Wz2);
+    const float2 op = mul(oov, add(one_minus(Wp), Wp));  // the reference's (1 - W_phi) + W_phi split
+    const float2 of = mul(oov, Fp);
+    J[0] = mul(of, mul(mWr2, mWz2));
+    J[1] = mul(of, mul(Wr2, mWz2));
+    J[2] = mul(of, mul(mWr2, Wz1));  // W_z1, as the reference has it (currentZigZag.cpp:104)
+    J[3] = mul(of, mul(Wr2, Wz2));
+    J[4] = mul(op, fma(Fz2, mWr2, mul(Fz1, mWr1)));
+    J[5] = mul(op, fma(Fz2, Wr2, mul(Fz1, Wr1)));
+    J[6] = mul(op, fma(Fr2, mWz2, mul(Fr1, mWz1)));
+    J[7] = mul(op, fma(Fr2, Wz2, mul(Fr1, Wz1)));
+  } else {
+  // ---- in-cell Villasenor-Buneman deposit (currentVB.cpp:22-173, 398-498) ----
   const float2 inv_i = make_float2(NA.z, NB.z), inv_i1 = make_float2(NA.w, NB.w);
   // J_phi from the mid-point
   const float2 Xm = fma(bc(0.5f), dX, fr), Ym = fma(bc(0.5f), dY, fz);
@@ -278,7 +344,6 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   const float2 dXi = mul(dX, ixn);
   const float2 jr0 = mul(qr, fma(dX, sub(mul(bc(0.5f), bb), q4v), mul(cx, fma(dXi, bb, dm))));
   const float2 jr1 = mul(qr, fma(dX, fma(bc(0.5f), fz, q4v), mul(cx, sub(mul(dXi, fz), dm))));
-  constexpr int JP = kJWR * kJWZ;
   if (okA) {
     b.off_r[ja] = frn.x; b.off_z[ja] = fzn.x;
     b.vr[ja] = vr2.x; b.vphi[ja] = vp2.x; b.vz[ja] = v2.x;
@@ -287,10 +352,23 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
     b.off_r[jb] = frn.y; b.off_z[jb] = fzn.y;
     b.vr[jb] = vr2.y; b.vphi[jb] = vp2.y; b.vz[jb] = v2.y;
   }
-  // the eight node currents of each particle; two particles of one cell (the
-  // common case: in a full layer a thread's slots i and i + kThreads are
-  // the same cell's) add theirs first and reduce once
-  float2 J[8] = {mul(a0, oYm), mul(a1, oYm), mul(a0, Ym), mul(a1, Ym), jz0, jz1, jr0, jr1};
+  J[0] = mul(a0, oYm); J[1] = mul(a1, oYm); J[2] = mul(a0, Ym); J[3] = mul(a1, Ym);
+  J[4] = jz0; J[5] = jz1; J[6] = jr0; J[7] = jr1;
+  }
+  if constexpr (KIND == 1) {
+    if (okA) {
+      b.off_r[ja] = frn.x; b.off_z[ja] = fzn.x;
+      b.vr[ja] = vr2.x; b.vphi[ja] = vp2.x; b.vz[ja] = v2.x;
+    }
+    if (okB) {
+      b.off_r[jb] = frn.y; b.off_z[jb] = fzn.y;
+      b.vr[jb] = vr2.y; b.vphi[jb] = vp2.y; b.vz[jb] = v2.y;
+    }
+  }
+  constexpr int JP = kJWR * kJWZ;
+  // two particles of one cell (the common case: in a full layer a thread's
+  // slots i and i + kThreads are the same cell's) add theirs first and
+  // reduce once
   const bool same = okA && okB && ciA == ciB && ckA == ckB;
   if (same) {
 #pragma unroll
@@ -417,13 +495,15 @@ constexpr size_t kPairSmemBytes = kPairFixedBytes + 1024 + (size_t)kStages * kSt
 // one per lane (reading them from global memory), so that the rare cases do
 // not stall the warp's other lanes.  A wait for a chunk that runs out sets
 // kErrTimeout, waits (bounded) for the copies in flight and ends the block.
-template <int FIX>
+// KIND 0: the relativistic Boris pusher and the Villasenor-Buneman current;
+// KIND 1: the Vay pusher and the ZigZag current.
+template <int FIX, int KIND = 0>
 // Four resident blocks per SM (64 registers) measured faster than three
 // with 80 registers and no spill.
 __global__ void __launch_bounds__(kThreads, 4)
     step_pair_kernel(StepArgs args, SpeciesF32Buffers b, TileGrid tg) {
   StepArgs a = args;
-  a.pusher = PCG_PUSHER_BORIS_RELATIVISTIC;
+  a.pusher = KIND == 1 ? PCG_PUSHER_VAY : PCG_PUSHER_BORIS_RELATIVISTIC;
   a.is_beam = 0;
   a.fixed = FIX;
   a.pushed = 0;  // launched for whole steps only
@@ -538,7 +618,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       __syncwarp();
       if (lane == 0) tma::mbar_arrive(empty0 + 8 * st);  // this warp is done reading the buffer
       bool okA, okB;
-      pair_particles<FIX>(a, b, ja, jb, A, B, hasA, hasB, W, okA, okB);
+      pair_particles<FIX, KIND>(a, b, ja, jb, A, B, hasA, hasB, W, okA, okB);
       const bool needA = hasA && A.cell >= 0 && !okA, needB = hasB && B.cell >= 0 && !okB;
       const unsigned mA = __ballot_sync(0xffffffffu, needA), mB = __ballot_sync(0xffffffffu, needB);
       if (needA) myq[(qtail + __popc(mA & below)) & (kQueue - 1)] = ja;
@@ -556,7 +636,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       const unsigned n = min(32u, qtail - qhead);
       const unsigned jj = myq[(qhead + lane) & (kQueue - 1)];
       qhead += n;
-      if ((unsigned)lane < n) tile_particle<0>(a, b, jj, load_slot(b, jj), sv, sd);
+      if ((unsigned)lane < n) tile_particle<KIND>(a, b, jj, load_slot(b, jj), sv, sd);
       __syncwarp();
     }
   }

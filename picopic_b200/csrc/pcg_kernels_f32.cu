@@ -551,8 +551,13 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
   if (b.sorted_n) {
     const size_t smem = f32::kTileSmemBytes;
     const dim3 grid(tg.ntiles, b.splits);
-    if (st.current == PCG_CURRENT_ZIGZAG && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed && !st.pushed)
-      f32::step_tiled_kernel<1, PCG_PUSHER_VAY, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    if (st.current == PCG_CURRENT_ZIGZAG && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed && !st.pushed) {
+      auto kern = f32::step_pair_kernel<0, 1>;  // the plasma of the large Vay + ZigZag runs
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f32::kPairSmemBytes) !=
+          cudaSuccess)
+        return -1;
+      kern<<<grid, f32::kThreads, f32::kPairSmemBytes, s>>>(a, b, tg);
+    }
     else if (st.current == PCG_CURRENT_ZIGZAG && st.pushed && !is_beam && !st.fixed)
       f32::step_tiled_kernel<1, f32::kMoveOnly, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.current == PCG_CURRENT_ZIGZAG)
