@@ -109,6 +109,80 @@ struct PairWindow {
   int rlo, rhi, zlo, zhi;  // the cells whose particles may take the pair path
 };
 
+// The in-cell ZigZag currents of a pair (currentZigZag.cpp:22-136) as the
+// scalar zigzag computes them: relay point at the mid-point, weights in
+// metres.  J: J_phi at (i, k), (i+1, k), (i, k+1), (i+1, k+1); J_z at (i, k),
+// (i+1, k); J_r at (i, k), (i, k+1).
+__device__ __forceinline__ void zigzag_pair(const StepArgs& a, float2 fi, float2 fr, float2 fz, float2 frn,
+                                            float2 fzn, float2 w, float2 vp2, float2 J[8]) {
+  using namespace pk;
+  const float2 x0 = add(fi, fr);
+  const float2 oov = mul(bc(a.zz_vol), rcp(fma(bc(2.f), fi, bc(1.f))));
+  const float2 ro = mul(x0, bc(a.dr_m)), rn = mul(add(fi, frn), bc(a.dr_m));
+  const float2 Fp = mul(w, vp2);
+  const float2 Wp = mul(mul(vp2, bc(a.dt_s)), rcp(mul(bc(2.f * 3.14159265f), add(ro, rn))));
+  const float2 xr = mul(bc(0.5f), add(fr, frn)), yr = mul(bc(0.5f), add(fz, fzn));
+  const float2 cod = mul(w, bc(1.f / a.dt_s));
+  const float2 cr = mul(cod, bc(a.dr_m)), cz = mul(cod, bc(a.dz_m));
+  const float2 Fr1 = mul(cr, sub(xr, fr)), Fr2 = mul(cr, sub(frn, xr));
+  const float2 Fz1 = mul(cz, sub(yr, fz)), Fz2 = mul(cz, sub(fzn, yr));
+  const float2 Wr1 = mul(bc(a.dr_m), mul(bc(0.5f), add(fr, xr))), Wr2 = mul(bc(a.dr_m), mul(bc(0.5f), add(frn, xr)));
+  const float2 Wz1 = mul(bc(a.dz_m), mul(bc(0.5f), add(fz, yr))), Wz2 = mul(bc(a.dz_m), mul(bc(0.5f), add(fzn, yr)));
+  const float2 mWr1 = one_minus(Wr1), mWr2 = one_minus(Wr2), mWz1 = one_minus(Wz1), mWz2 = one_minus(Wz2);
+  const float2 op = mul(oov, add(one_minus(Wp), Wp));  // the reference's (1 - W_phi) + W_phi split
+  const float2 of = mul(oov, Fp);
+  J[0] = mul(of, mul(mWr2, mWz2));
+  J[1] = mul(of, mul(Wr2, mWz2));
+  J[2] = mul(of, mul(mWr2, Wz1));  // W_z1, as the reference has it (currentZigZag.cpp:104)
+  J[3] = mul(of, mul(Wr2, Wz2));
+  J[4] = mul(op, fma(Fz2, mWr2, mul(Fz1, mWr1)));
+  J[5] = mul(op, fma(Fz2, Wr2, mul(Fz1, Wr1)));
+  J[6] = mul(op, fma(Fr2, mWz2, mul(Fr1, mWz1)));
+  J[7] = mul(op, fma(Fr2, Wz2, mul(Fr1, Wz1)));
+}
+
+// The completed particles of a pair written back.
+__device__ __forceinline__ void pair_store(const SpeciesF32Buffers& b, unsigned ja, unsigned jb, bool okA, bool okB,
+                                           float2 frn, float2 fzn, float2 vr2, float2 vp2, float2 v2) {
+  if (okA) {
+    b.off_r[ja] = frn.x; b.off_z[ja] = fzn.x;
+    b.vr[ja] = vr2.x; b.vphi[ja] = vp2.x; b.vz[ja] = v2.x;
+  }
+  if (okB) {
+    b.off_r[jb] = frn.y; b.off_z[jb] = fzn.y;
+    b.vr[jb] = vr2.y; b.vphi[jb] = vp2.y; b.vz[jb] = v2.y;
+  }
+}
+
+// The currents of a pair added to the block's window (two particles of one
+// cell add theirs first and reduce once).
+__device__ __forceinline__ void pair_reduce(const PairWindow& W, bool okA, bool okB, int rowA, int rowB, int ckA,
+                                            int ckB, bool same_cell, float2 J[8]) {
+  using namespace pk;
+  constexpr int JP = kJWR * kJWZ;
+  const bool same = okA && okB && same_cell;
+  if (same) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) J[q].x += J[q].y;
+  }
+  // J_r of the cell's node in the current window, which starts one node
+  // after the field window on each axis
+  if (okA) {
+    const unsigned p = W.J + 4u * (unsigned)((rowA - 1) * kJWZ + (ckA - W.fk0 - 1));
+    red<4 * JP>(p, J[0].x);                   red<4 * (JP + kJWZ)>(p, J[1].x);
+    red<4 * (JP + 1)>(p, J[2].x);             red<4 * (JP + kJWZ + 1)>(p, J[3].x);
+    red<4 * (2 * JP)>(p, J[4].x);             red<4 * (2 * JP + kJWZ)>(p, J[5].x);
+    red<0>(p, J[6].x);                        red<4>(p, J[7].x);
+  }
+  if (okB && !same) {
+    const unsigned p = W.J + 4u * (unsigned)((rowB - 1) * kJWZ + (ckB - W.fk0 - 1));
+    red<4 * JP>(p, J[0].y);                   red<4 * (JP + kJWZ)>(p, J[1].y);
+    red<4 * (JP + 1)>(p, J[2].y);             red<4 * (JP + kJWZ + 1)>(p, J[3].y);
+    red<4 * (2 * JP)>(p, J[4].y);             red<4 * (2 * JP + kJWZ)>(p, J[5].y);
+    red<0>(p, J[6].y);                        red<4>(p, J[7].y);
+  }
+}
+
 // The fast path of one pair of slots.  okA / okB come back true for each
 // particle it completed (slot written, current deposited); a live particle
 // it did not complete is left untouched for the scalar path.  A particle in
@@ -289,30 +363,7 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   // (i, k+1), (i+1, k+1); J_z at (i, k), (i+1, k); J_r at (i, k), (i, k+1)
   float2 J[8];
   if constexpr (KIND == 1) {
-    // ---- in-cell ZigZag deposit (currentZigZag.cpp:22-136) as the scalar
-    // zigzag computes it: relay point at the mid-point, weights in metres ----
-    const float2 oov = mul(bc(a.zz_vol), rcp(fma(bc(2.f), fi, bc(1.f))));
-    const float2 ro = mul(x0, bc(a.dr_m)), rn = mul(add(fi, frn), bc(a.dr_m));
-    const float2 Fp = mul(w, vp2);
-    const float2 Wp = mul(mul(vp2, bc(a.dt_s)), rcp(mul(bc(2.f * 3.14159265f), add(ro, rn))));
-    const float2 xr = mul(bc(0.5f), add(fr, frn)), yr = mul(bc(0.5f), add(fz, fzn));
-    const float2 cod = mul(w, bc(1.f / a.dt_s));
-    const float2 cr = mul(cod, bc(a.dr_m)), cz = mul(cod, bc(a.dz_m));
-    const float2 Fr1 = mul(cr, sub(xr, fr)), Fr2 = mul(cr, sub(frn, xr));
-    const float2 Fz1 = mul(cz, sub(yr, fz)), Fz2 = mul(cz, sub(fzn, yr));
-    const float2 Wr1 = mul(bc(a.dr_m), mul(bc(0.5f), add(fr, xr))), Wr2 = mul(bc(a.dr_m), mul(bc(0.5f), add(frn, xr)));
-    const float2 Wz1 = mul(bc(a.dz_m), mul(bc(0.5f), add(fz, yr))), Wz2 = mul(bc(a.dz_m), mul(bc(0.5f), add(fzn, yr)));
-    const float2 mWr1 = one_minus(Wr1), mWr2 = one_minus(Wr2), mWz1 = one_minus(Wz1), mWz2 = one_minus(Wz2);
-    const float2 op = mul(oov, add(one_minus(Wp), Wp));  // the reference's (1 - W_phi) + W_phi split
-    const float2 of = mul(oov, Fp);
-    J[0] = mul(of, mul(mWr2, mWz2));
-    J[1] = mul(of, mul(Wr2, mWz2));
-    J[2] = mul(of, mul(mWr2, Wz1));  // W_z1, as the reference has it (currentZigZag.cpp:104)
-    J[3] = mul(of, mul(Wr2, Wz2));
-    J[4] = mul(op, fma(Fz2, mWr2, mul(Fz1, mWr1)));
-    J[5] = mul(op, fma(Fz2, Wr2, mul(Fz1, Wr1)));
-    J[6] = mul(op, fma(Fr2, mWz2, mul(Fr1, mWz1)));
-    J[7] = mul(op, fma(Fr2, Wz2, mul(Fr1, Wz1)));
+    zigzag_pair(a, fi, fr, fz, frn, fzn, w, vp2, J);
   } else {
   // ---- in-cell Villasenor-Buneman deposit (currentVB.cpp:22-173, 398-498) ----
   const float2 inv_i = make_float2(NA.z, NB.z), inv_i1 = make_float2(NA.w, NB.w);
@@ -344,52 +395,69 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   const float2 dXi = mul(dX, ixn);
   const float2 jr0 = mul(qr, fma(dX, sub(mul(bc(0.5f), bb), q4v), mul(cx, fma(dXi, bb, dm))));
   const float2 jr1 = mul(qr, fma(dX, fma(bc(0.5f), fz, q4v), mul(cx, sub(mul(dXi, fz), dm))));
-  if (okA) {
-    b.off_r[ja] = frn.x; b.off_z[ja] = fzn.x;
-    b.vr[ja] = vr2.x; b.vphi[ja] = vp2.x; b.vz[ja] = v2.x;
-  }
-  if (okB) {
-    b.off_r[jb] = frn.y; b.off_z[jb] = fzn.y;
-    b.vr[jb] = vr2.y; b.vphi[jb] = vp2.y; b.vz[jb] = v2.y;
-  }
+  pair_store(b, ja, jb, okA, okB, frn, fzn, vr2, vp2, v2);
   J[0] = mul(a0, oYm); J[1] = mul(a1, oYm); J[2] = mul(a0, Ym); J[3] = mul(a1, Ym);
   J[4] = jz0; J[5] = jz1; J[6] = jr0; J[7] = jr1;
   }
-  if constexpr (KIND == 1) {
-    if (okA) {
-      b.off_r[ja] = frn.x; b.off_z[ja] = fzn.x;
-      b.vr[ja] = vr2.x; b.vphi[ja] = vp2.x; b.vz[ja] = v2.x;
+  if constexpr (KIND != 0) pair_store(b, ja, jb, okA, okB, frn, fzn, vr2, vp2, v2);
+  pair_reduce(W, okA, okB, rowA, rowB, ckA, ckB, ciA == ciB && ckA == ckB, J);
+}
+
+
+// The fast path of a pair in the move half of a collisional step (the
+// velocities were pushed before the collisions): the learned collision
+// step's transform of the particle's cell where its flag is set, then the
+// move and the in-cell ZigZag currents of pair_particles.
+template <int FIX>
+__device__ __forceinline__ void pair_move_particles(const StepArgs& a, const SpeciesF32Buffers& b, unsigned ja,
+                                                    unsigned jb, const Slot& A, const Slot& B, bool hasA, bool hasB,
+                                                    const PairWindow& W, bool& okA, bool& okB) {
+  using namespace pk;
+  okA = okB = false;
+  int ciA = cell_r_of(A.cell), ckA = cell_z_of(A.cell);
+  int ciB = cell_r_of(B.cell), ckB = cell_z_of(B.cell);
+  const bool preA = hasA && A.cell >= 0 && (unsigned)(ciA - W.rlo) <= (unsigned)(W.rhi - W.rlo) &&
+                    (unsigned)(ckA - W.zlo) <= (unsigned)(W.zhi - W.zlo);
+  const bool preB = hasB && B.cell >= 0 && (unsigned)(ciB - W.rlo) <= (unsigned)(W.rhi - W.rlo) &&
+                    (unsigned)(ckB - W.zlo) <= (unsigned)(W.zhi - W.zlo);
+  if (!preA && !preB) return;
+  if (!preA) { ciA = ciB; ckA = ckB; }
+  if (!preB) { ciB = ciA; ckB = ckA; }
+  float vA[3] = {A.vr, A.vphi, A.vz}, vB[3] = {B.vr, B.vphi, B.vz};
+  if (a.xform) {  // v' = u + (v - u) s per axis, in FP64 (the transform's arithmetic)
+    const size_t cA = (size_t)ciA * a.nz + ckA, cB = (size_t)ciB * a.nz + ckB;
+    if (preA && a.xflag[cA] == 1) {
+      const double* t = a.xform + cA * 12 + a.xoff;
+      for (int q = 0; q < 3; ++q) vA[q] = (float)(t[q] + ((double)vA[q] - t[q]) * t[3 + q]);
     }
-    if (okB) {
-      b.off_r[jb] = frn.y; b.off_z[jb] = fzn.y;
-      b.vr[jb] = vr2.y; b.vphi[jb] = vp2.y; b.vz[jb] = v2.y;
+    if (preB && a.xflag[cB] == 1) {
+      const double* t = a.xform + cB * 12 + a.xoff;
+      for (int q = 0; q < 3; ++q) vB[q] = (float)(t[q] + ((double)vB[q] - t[q]) * t[3 + q]);
     }
   }
-  constexpr int JP = kJWR * kJWZ;
-  // two particles of one cell (the common case: in a full layer a thread's
-  // slots i and i + kThreads are the same cell's) add theirs first and
-  // reduce once
-  const bool same = okA && okB && ciA == ciB && ckA == ckB;
-  if (same) {
-#pragma unroll
-    for (int q = 0; q < 8; ++q) J[q].x += J[q].y;
-  }
-  // J_r of the cell's node in the current window, which starts one node
-  // after the field window on each axis
-  if (okA) {
-    const unsigned p = W.J + 4u * (unsigned)((rowA - 1) * kJWZ + (ckA - W.fk0 - 1));
-    red<4 * JP>(p, J[0].x);                   red<4 * (JP + kJWZ)>(p, J[1].x);
-    red<4 * (JP + 1)>(p, J[2].x);             red<4 * (JP + kJWZ + 1)>(p, J[3].x);
-    red<4 * (2 * JP)>(p, J[4].x);             red<4 * (2 * JP + kJWZ)>(p, J[5].x);
-    red<0>(p, J[6].x);                        red<4>(p, J[7].x);
-  }
-  if (okB && !same) {
-    const unsigned p = W.J + 4u * (unsigned)((rowB - 1) * kJWZ + (ckB - W.fk0 - 1));
-    red<4 * JP>(p, J[0].y);                   red<4 * (JP + kJWZ)>(p, J[1].y);
-    red<4 * (JP + 1)>(p, J[2].y);             red<4 * (JP + kJWZ + 1)>(p, J[3].y);
-    red<4 * (2 * JP)>(p, J[4].y);             red<4 * (2 * JP + kJWZ)>(p, J[5].y);
-    red<0>(p, J[6].y);                        red<4>(p, J[7].y);
-  }
+  const float2 fr = make_float2(A.fr, B.fr), fz = make_float2(A.fz, B.fz);
+  const float2 fi = make_float2((float)ciA, (float)ciB);
+  const float2 v0 = make_float2(vA[0], vB[0]), v1 = make_float2(vA[1], vB[1]), v2 = make_float2(vA[2], vB[2]);
+  // the move of pair_particles (specieP.cpp:482-491, 609-640)
+  const float2 dx = mul(v0, bc(a.dt_dr)), dyp = mul(v1, bc(a.dt_dr)), dYv = mul(v2, bc(a.dt_dz));
+  const float2 x0 = add(fi, fr);
+  const float2 X = add(x0, dx);
+  const float2 dy2 = mul(dyp, dyp);
+  const float2 xn2 = fma(X, X, dy2);
+  const float2 rxn = rsq(xn2);
+  const float2 sn = mul(dyp, rxn);
+  const float2 dXv = fma(dy2, rcp(add(X, mul(xn2, rxn))), dx);
+  const float2 frn = add(fr, dXv), fzn = add(fz, dYv);
+  okA = preA && frn.x >= 0.f && frn.x < 1.f && fzn.x >= 0.f && fzn.x < 1.f && X.x > 0.5f;
+  okB = preB && frn.y >= 0.f && frn.y < 1.f && fzn.y >= 0.f && fzn.y < 1.f && X.y > 0.5f;
+  if (!okA && !okB) return;
+  const float2 cs = sqr(fma(sn, mul(sn, bc(-1.f)), bc(1.f)));
+  const float2 vr2 = fma(cs, v0, mul(mul(sn, v1), bc(-1.f)));
+  const float2 vp2 = fma(sn, v0, mul(cs, v1));
+  float2 J[8];
+  zigzag_pair(a, fi, fr, fz, frn, fzn, make_float2(A.w, B.w), vp2, J);
+  pair_store(b, ja, jb, okA, okB, frn, fzn, vr2, vp2, v2);
+  pair_reduce(W, okA, okB, ciA - W.fi0, ciB - W.fi0, ckA, ckB, ciA == ciB && ckA == ckB, J);
 }
 
 
@@ -496,18 +564,19 @@ constexpr size_t kPairSmemBytes = kPairFixedBytes + 1024 + (size_t)kStages * kSt
 // not stall the warp's other lanes.  A wait for a chunk that runs out sets
 // kErrTimeout, waits (bounded) for the copies in flight and ends the block.
 // KIND 0: the relativistic Boris pusher and the Villasenor-Buneman current;
-// KIND 1: the Vay pusher and the ZigZag current.
+// KIND 1: the Vay pusher and the ZigZag current; KIND 2: the move half of
+// a collisional step with the ZigZag current (no field window).
 template <int FIX, int KIND = 0>
 // Four resident blocks per SM (64 registers) measured faster than three
 // with 80 registers and no spill.
 __global__ void __launch_bounds__(kThreads, 4)
     step_pair_kernel(StepArgs args, SpeciesF32Buffers b, TileGrid tg) {
   StepArgs a = args;
-  a.pusher = KIND == 1 ? PCG_PUSHER_VAY : PCG_PUSHER_BORIS_RELATIVISTIC;
+  a.pusher = KIND == 0 ? PCG_PUSHER_BORIS_RELATIVISTIC : PCG_PUSHER_VAY;
   a.is_beam = 0;
   a.fixed = FIX;
-  a.pushed = 0;  // launched for whole steps only
-  a.xform = nullptr;
+  a.pushed = KIND == 2 ? 1 : 0;  // whole steps, or the move half of one
+  if (KIND != 2) a.xform = nullptr;
   extern __shared__ __align__(16) float smem[];
   const int t = blockIdx.x;
   // the tile's parts: the blocks per tile of the last sort (on the device),
@@ -542,7 +611,8 @@ __global__ void __launch_bounds__(kThreads, 4)
       stage_chunk(b, bs, be, k, stage0 + k * kStageBytes, full0 + 8 * k);
   }
   // the field window, each thread's loads issued before its shared stores
-  {
+  // (the move half of a collisional step gathers nothing)
+  if constexpr (KIND != 2) {
     constexpr int kRows = 6 * kFWR, kPer = (kRows + kThreads / 32 - 1) / (kThreads / 32);
     constexpr int kCols = (kFWZ + 31) / 32;
     float v[kPer][kCols];
@@ -569,13 +639,13 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
   }
   for (int q = threadIdx.x; q < 3 * kJWR * kJWZ; q += kThreads) sJ[q] = 0.f;
-  if (threadIdx.x < 2 * kFWR) {
+  if (KIND != 2 && threadIdx.x < 2 * kFWR) {
     const int i = fi0 + (int)(threadIdx.x >> 1);
     sR[threadIdx.x] = (i >= -2 && i <= a.nr + 2) ? __ldg(a.rt + 2 * (i + 2) + (threadIdx.x & 1))
                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
-  if (threadIdx.x < kFWR) {
+  if (KIND != 2 && threadIdx.x < kFWR) {
     const float4 p = sR[2 * threadIdx.x], q = sR[2 * threadIdx.x + 1];
     tb->N[threadIdx.x] = make_float4(p.x, p.z, q.x, q.y);
     tb->H[threadIdx.x] = make_float2(p.y, p.w);
@@ -618,7 +688,8 @@ __global__ void __launch_bounds__(kThreads, 4)
       __syncwarp();
       if (lane == 0) tma::mbar_arrive(empty0 + 8 * st);  // this warp is done reading the buffer
       bool okA, okB;
-      pair_particles<FIX, KIND>(a, b, ja, jb, A, B, hasA, hasB, W, okA, okB);
+      if constexpr (KIND == 2) pair_move_particles<FIX>(a, b, ja, jb, A, B, hasA, hasB, W, okA, okB);
+      else pair_particles<FIX, KIND>(a, b, ja, jb, A, B, hasA, hasB, W, okA, okB);
       const bool needA = hasA && A.cell >= 0 && !okA, needB = hasB && B.cell >= 0 && !okB;
       const unsigned mA = __ballot_sync(0xffffffffu, needA), mB = __ballot_sync(0xffffffffu, needB);
       if (needA) myq[(qtail + __popc(mA & below)) & (kQueue - 1)] = ja;
@@ -636,7 +707,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       const unsigned n = min(32u, qtail - qhead);
       const unsigned jj = myq[(qhead + lane) & (kQueue - 1)];
       qhead += n;
-      if ((unsigned)lane < n) tile_particle<KIND>(a, b, jj, load_slot(b, jj), sv, sd);
+      if ((unsigned)lane < n) tile_particle<KIND == 0 ? 0 : 1>(a, b, jj, load_slot(b, jj), sv, sd);
       __syncwarp();
     }
   }

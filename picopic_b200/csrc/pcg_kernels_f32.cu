@@ -558,8 +558,13 @@ int f32_step_species(const F32Step& st, SpeciesF32Buffers& b, size_t* n, double 
         return -1;
       kern<<<grid, f32::kThreads, f32::kPairSmemBytes, s>>>(a, b, tg);
     }
-    else if (st.current == PCG_CURRENT_ZIGZAG && st.pushed && !is_beam && !st.fixed)
-      f32::step_tiled_kernel<1, f32::kMoveOnly, 0, 0><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
+    else if (st.current == PCG_CURRENT_ZIGZAG && st.pushed && !is_beam && !st.fixed) {
+      auto kern = f32::step_pair_kernel<0, 2>;  // the move half of a collisional step
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f32::kPairSmemBytes) !=
+          cudaSuccess)
+        return -1;
+      kern<<<grid, f32::kThreads, f32::kPairSmemBytes, s>>>(a, b, tg);
+    }
     else if (st.current == PCG_CURRENT_ZIGZAG)
       f32::step_tiled_kernel<1><<<grid, f32::kThreads, smem, s>>>(a, b, tg);
     else if (st.pushed)

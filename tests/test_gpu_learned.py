@@ -46,13 +46,22 @@ def _grid(nr=32, nz=64, dt=1e-13):
     return Geometry(nr, nz, nr * dr, nz * dr, dt)
 
 
-def _random_domain(grid, seed=3, precision="f64"):
+def _random_domain(grid, seed=3, precision="f64", scheme=None):
+    """Random learned-box cell states; scheme (pusher, current, quirks) in
+    place of the default relativistic Boris, VB, fixed quirks."""
     from picopic_b200 import learned as L
+    from picopic_b200 import Domain
     rng = np.random.default_rng(seed)
     te, ti, dens, drift, ppc = L.cell_states(grid, rng, L.Sampling())
     pe = L.cell_particles(grid, rng, te, dens[0], drift, ppc[0], 1.0)
     pi = L.cell_particles(grid, rng, ti, dens[1], np.zeros_like(drift), ppc[1], L.MASS_ION)
-    d = L._domain(grid, 0, seed, capacity=max(pe[0].size, pi[0].size) + 16, precision=precision)
+    cap = max(pe[0].size, pi[0].size) + 16
+    if scheme is None:
+        d = L._domain(grid, 0, seed, capacity=cap, precision=precision)
+    else:
+        d = Domain(grid, pusher=scheme[0], current=scheme[1], precision=precision, quirks=scheme[2], seed=seed)
+        d.add(L.ELECTRONS, capacity=cap)
+        d.add(L.IONS, capacity=cap)
     d.set_particles(0, *pe)
     d.set_particles(1, *pi)
     if precision == "f32":  # group the slots by tile, as steps keep them
@@ -234,17 +243,20 @@ def test_float_layout_moments_by_tile():
     assert (np.abs(m - h) <= 1e-12 * scale).all()
 
 
-def test_fused_learned_step_matches_collide_then_step():
+@pytest.mark.parametrize("scheme", [None, ("vay", "zigzag", "reference")])
+def test_fused_learned_step_matches_collide_then_step(scheme):
     """A float step with learned collisions sums the cell moments in its push
     and applies the transforms in its move.  In the first step of a fresh
     domain the fields are zero and the push only rounds, so the step equals
     a learned collision pass (moments, network, transform in their own
-    kernels) followed by a collisionless step, to float rounding."""
+    kernels) followed by a collisionless step, to float rounding.  With the
+    Vay pusher and the ZigZag current (reference quirks) the move half and
+    the collisionless step both run the pair kernel's fast paths."""
     from picopic_b200 import learned as L
     g = _grid()
     out = []
     for fused in (True, False):
-        d = _random_domain(g, seed=6, precision="f32")
+        d = _random_domain(g, seed=6, precision="f32", scheme=scheme)
         d.set_collision_model(*L.load_model())
         if fused:
             d.set_collisions("learned")
