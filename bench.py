@@ -457,9 +457,9 @@ ENSEMBLE = dict(name="ensemble of 64 runs: nr U{64..256}, nz U{256..2048}, n 1e1
 def run_ensemble(args, local):
     """The batched configuration through pcg_ensemble: particle-steps/s of K
     steps of all runs issued from one host thread with the default tiling,
-    from 8 threads with the default tiling, and from 8 threads after the
-    autotuner's tiling, chosen on the whole ensemble (the device time of
-    each batch)."""
+    from 8 threads with the default tiling, from 8 threads after the
+    autotuner's tiling, chosen on the whole ensemble, and, with that tiling,
+    as one CUDA graph launch per batch (the device time of each batch)."""
     import torch
     from picopic_b200.ensemble import Ensemble
     rng = np.random.default_rng(ENSEMBLE["seed"])
@@ -490,6 +490,10 @@ def run_ensemble(args, local):
     choices = many.autotune(trial_steps=3)
     many.step(2)
     vt, mst = timed(many)
+    many.set_graph(True)
+    many.step(k_steps)  # the first captured batch: instantiates the graph
+    vg, msg = timed(many)
+    nodes, capture_ms = many.graph_info()
     many.close()
     particles = sum(d.diag().particles for d in runs)
     out = {"workload": ENSEMBLE["name"], "runs": nruns, "particles": int(particles),
@@ -497,6 +501,10 @@ def run_ensemble(args, local):
            "one_thread_default_tiling": {"value": v1, "ms_per_step": ms1},
            "threads8_default_tiling": {"value": v8, "ms_per_step": ms8},
            "threads8_autotuned": {"value": vt, "ms_per_step": mst},
+           "graph_autotuned": {"value": vg, "ms_per_step": msg, "graph_nodes": nodes,
+                               "steps_per_graph": k_steps, "host_capture_ms_per_step": capture_ms / k_steps,
+                               "note": "each batch of steps of all runs captured into one CUDA graph, "
+                                       "one graph launch (device time of the launch)"},
            "autotune_choice": {"target_blocks": choices[0], "times_particle_share": choices[1],
                                "min_particles_per_block": choices[2]}}
     del runs

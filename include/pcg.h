@@ -402,8 +402,7 @@ int pcg_tile_sort(pcg_handle* h, int slot, unsigned* counts, unsigned long long*
  * per process.  pcg_ensemble_create groups handles it does not own (all on
  * one device); pcg_ensemble_step advances every run by nsteps, the runs
  * spread over `threads` host threads that each issue their runs' steps in
- * turn, so that the GPU overlaps the runs' kernels and a run's tile sort
- * (which waits for its own stream) holds up no other run; *device_ms (may
+ * turn, so that the GPU overlaps the runs' kernels; *device_ms (may
  * be NULL) receives the device time from the first to the last of the
  * batch's kernels (events on the runs' streams, joined on one stream).
  * pcg_ensemble_autotune times trial_steps ensemble steps under each of six
@@ -418,6 +417,26 @@ int pcg_ensemble_create(pcg_handle* const* runs, int n, int threads, pcg_ensembl
 int pcg_ensemble_step(pcg_ensemble* e, int nsteps, float* device_ms);
 int pcg_ensemble_autotune(pcg_ensemble* e, int trial_steps, int* choice);
 int pcg_ensemble_destroy(pcg_ensemble* e);
+
+/* Graph mode of an ensemble (no reference counterpart).  With on != 0, each
+ * later pcg_ensemble_step(e, nsteps, ...) captures nsteps steps of every run
+ * from the calling thread into one CUDA graph, the runs as parallel
+ * branches forked from and joined to the ensemble's own stream, and issues
+ * it as one graph launch; *device_ms is then the device time of that
+ * launch.  A call before the ensemble's first batch steps directly (the
+ * first tile sort of a float species waits for its stream, which a capture
+ * cannot).  Each step's host decisions (beam particle counts, re-sorts) are
+ * taken at capture as a direct step takes them; the graph of the previous
+ * batch is updated in place when the new one has the same nodes, and
+ * instantiated anew otherwise.  A step that would wait for the device
+ * inside the capture (a species at its capacity, dropping dead slots) fails
+ * the capture: the call returns its error, the runs' host state has moved
+ * on without their kernels, and every later call returns PCG_ERR_STATE.
+ * pcg_ensemble_graph_info reports the last graph's node count and the host
+ * time (ms) of its capture and instantiation or update; either pointer may
+ * be NULL. */
+int pcg_ensemble_set_graph(pcg_ensemble* e, int on);
+int pcg_ensemble_graph_info(pcg_ensemble* e, unsigned long long* nodes, float* capture_ms);
 
 /* SpecieP's diagnostic maps of species `slot` (specieP.cpp:665-839:
  * calc_density, calc_temperature, calc_energy, calc_momentum) into host

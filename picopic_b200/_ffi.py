@@ -119,6 +119,9 @@ SIGNATURES = {
     "pcg_ensemble_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
     "pcg_ensemble_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "pcg_ensemble_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "pcg_ensemble_set_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "pcg_ensemble_graph_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong),
+                                               ctypes.POINTER(ctypes.c_float)]),
     "pcg_collide_expectation": (ctypes.c_int, [_H, _PD]),
     "pcg_cell_features": (ctypes.c_int, [_H, _PF, _PD]),
     "pcg_mlp_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),

@@ -3,14 +3,23 @@
 //
 // Each run is a pcg_handle with its own stream.  A step of the ensemble
 // spreads the runs over a few host threads; each thread issues one step of
-// each of its runs in turn, so the GPU overlaps all runs' kernels, and the
-// tile sort of one run (the only part of a step that waits for its stream)
-// holds up only its own thread.  The device time of a batch runs from an
-// event all run streams wait on to an event that waits on all of them.
+// each of its runs in turn, so the GPU overlaps all runs' kernels.  The
+// device time of a batch runs from an event all run streams wait on to an
+// event that waits on all of them.
+//
+// In graph mode (pcg_ensemble_set_graph) a batch of steps of all runs is
+// captured from one host thread into one CUDA graph (the runs' streams
+// forked from and joined to the ensemble's stream, so the graph holds every
+// run's kernels for every step of the batch as parallel branches) and
+// issued as one graph launch.  The host decisions of a step (beam particle
+// counts, when to re-sort) are taken at capture, as a direct step takes
+// them; the graph of the previous batch is updated in place when the new
+// one has the same shape, and instantiated anew otherwise.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <thread>
 #include <vector>
 
@@ -25,6 +34,14 @@ struct pcg_ensemble {
   cudaStream_t join = nullptr;  // the batch's timing stream
   cudaEvent_t start = nullptr, stop = nullptr;
   std::vector<cudaEvent_t> done;
+  // graph mode
+  bool graph = false;
+  bool stepped = false;   // a batch has run: every species with particles has had its first sort
+  bool broken = false;    // a capture failed after some runs had advanced their host state
+  cudaGraphExec_t exec = nullptr;
+  size_t graph_nodes = 0;
+  float capture_ms = 0;   // host time of the last capture and instantiation or update
+  cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -78,7 +95,8 @@ int pcg_ensemble_create(pcg_handle* const* runs, int n, int threads, pcg_ensembl
     e->streams.push_back((cudaStream_t)st);
   }
   bool ok = cudaStreamCreateWithFlags(&e->join, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreate(&e->start) == cudaSuccess && cudaEventCreate(&e->stop) == cudaSuccess;
+            cudaEventCreate(&e->start) == cudaSuccess && cudaEventCreate(&e->stop) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
   e->done.assign(n, nullptr);
   for (int i = 0; ok && i < n; ++i) ok = cudaEventCreateWithFlags(&e->done[i], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
@@ -89,9 +107,89 @@ int pcg_ensemble_create(pcg_handle* const* runs, int n, int threads, pcg_ensembl
   return PCG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// nsteps steps of every run captured into one graph and launched once on
+// the ensemble's stream.
+int graph_step(pcg_ensemble* e, int nsteps, float* device_ms) {
+  const int n = (int)e->runs.size();
+  const auto t0 = std::chrono::steady_clock::now();
+  if (cudaStreamBeginCapture(e->join, cudaStreamCaptureModeRelaxed) != cudaSuccess) return PCG_ERR_CUDA;
+  int rc = PCG_OK;
+  if (cudaEventRecord(e->fork, e->join) != cudaSuccess) rc = PCG_ERR_CUDA;
+  for (int i = 0; rc == PCG_OK && i < n; ++i)
+    if (cudaStreamWaitEvent(e->streams[i], e->fork, 0) != cudaSuccess) rc = PCG_ERR_CUDA;
+  for (int step = 0; rc == PCG_OK && step < nsteps; ++step)
+    for (int i = 0; rc == PCG_OK && i < n; ++i) {
+      rc = pcg_step(e->runs[i], 1);
+      if (rc != PCG_OK) e->broken = true;  // earlier runs advanced their host state without their kernels
+    }
+  for (int i = 0; rc == PCG_OK && i < n; ++i)
+    if (cudaEventRecord(e->done[i], e->streams[i]) != cudaSuccess ||
+        cudaStreamWaitEvent(e->join, e->done[i], 0) != cudaSuccess)
+      rc = PCG_ERR_CUDA;
+  cudaGraph_t g = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(e->join, &g);
+  if (rc != PCG_OK || end != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    e->broken = true;
+    return rc != PCG_OK ? rc : PCG_ERR_CUDA;
+  }
+  if (e->exec) {  // same shape as the last batch: update its executable graph in place
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(e->exec, g, &info) != cudaSuccess) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(e->exec);
+      e->exec = nullptr;
+    }
+  }
+  if (!e->exec && cudaGraphInstantiate(&e->exec, g, 0) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    e->exec = nullptr;
+    e->broken = true;
+    return PCG_ERR_CUDA;
+  }
+  size_t nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nodes);
+  cudaGraphDestroy(g);
+  e->graph_nodes = nodes;
+  e->capture_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (cudaEventRecord(e->start, e->join) != cudaSuccess || cudaGraphLaunch(e->exec, e->join) != cudaSuccess ||
+      cudaEventRecord(e->stop, e->join) != cudaSuccess || cudaEventSynchronize(e->stop) != cudaSuccess)
+    return PCG_ERR_CUDA;
+  if (device_ms && cudaEventElapsedTime(device_ms, e->start, e->stop) != cudaSuccess) return PCG_ERR_CUDA;
+  for (pcg_handle* h : e->runs) {  // device-side errors (NaN, capacity, ...) of any run
+    const int rs = pcg_synchronize(h);
+    if (rs != PCG_OK) return rs;
+  }
+  return PCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pcg_ensemble_set_graph(pcg_ensemble* e, int on) {
+  if (!e) return PCG_ERR_ARG;
+  e->graph = on != 0;
+  return PCG_OK;
+}
+
+int pcg_ensemble_graph_info(pcg_ensemble* e, unsigned long long* nodes, float* capture_ms) {
+  if (!e) return PCG_ERR_ARG;
+  if (nodes) *nodes = e->graph_nodes;
+  if (capture_ms) *capture_ms = e->capture_ms;
+  return PCG_OK;
+}
+
 int pcg_ensemble_step(pcg_ensemble* e, int nsteps, float* device_ms) {
   pcg::DeviceScope device_scope(e ? e->device : -1);
   if (!e || nsteps < 0) return PCG_ERR_ARG;
+  if (e->broken) return PCG_ERR_STATE;
+  if (e->graph && e->stepped && nsteps > 0) return graph_step(e, nsteps, device_ms);
   const int n = (int)e->runs.size();
   if (cudaEventRecord(e->start, e->join) != cudaSuccess) return PCG_ERR_CUDA;
   for (int i = 0; i < n; ++i)
@@ -126,6 +224,7 @@ int pcg_ensemble_step(pcg_ensemble* e, int nsteps, float* device_ms) {
     const int rc = pcg_synchronize(h);
     if (rc != PCG_OK) return rc;
   }
+  if (nsteps > 0) e->stepped = true;
   return PCG_OK;
 }
 
@@ -161,6 +260,8 @@ int pcg_ensemble_destroy(pcg_ensemble* e) {
   if (!e) return PCG_ERR_ARG;
   for (cudaEvent_t ev : e->done)
     if (ev) cudaEventDestroy(ev);
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->fork) cudaEventDestroy(e->fork);
   if (e->start) cudaEventDestroy(e->start);
   if (e->stop) cudaEventDestroy(e->stop);
   if (e->join) cudaStreamDestroy(e->join);

@@ -333,7 +333,13 @@ int tile_sort(const TileGrid& tg, unsigned target_blocks, unsigned min_split, Sp
   const unsigned hint = b.host_info[2];  // the blocks per tile of an earlier sort
   cudaMemcpyAsync(b.host_info, b.sort_info, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, s);
   swap_buffers(b);
-  if (wait || b.sorts == 0) {
+  // a sort inside a stream capture (an ensemble's graph) cannot wait: the
+  // first sort of a species then launches with the earlier hint (one block
+  // per tile unless an earlier sort said more; the kernels take what runs)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool capturing = cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+  if (wait && capturing) return -1;
+  if (wait || (b.sorts == 0 && !capturing)) {
     if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
     if (wait) *n = b.host_info[3];
     b.splits = (int)std::max(1u, b.host_info[2]);

@@ -4,6 +4,8 @@
     ens = Ensemble(runs, threads=8)
     ens.autotune(trial_steps=5)          # a tiling per run, timed run by run
     ms = ens.step(100)                   # device ms of the whole batch
+    ens.set_graph(True)
+    ms = ens.step(20)                    # 20 steps of all runs as one graph launch
 """
 from __future__ import annotations
 
@@ -46,6 +48,22 @@ class Ensemble:
         if rc != 0:
             raise PcgError(rc, "pcg_ensemble_autotune", "")
         return CANDIDATES[choice.value]
+
+    def set_graph(self, on: bool = True):
+        """Graph mode: each later step(n) captures the n steps of every run
+        into one CUDA graph and issues it as one launch (the first batch of
+        an ensemble steps directly)."""
+        rc = self.lib.pcg_ensemble_set_graph(self.e, 1 if on else 0)
+        if rc != 0:
+            raise PcgError(rc, "pcg_ensemble_set_graph", "")
+
+    def graph_info(self):
+        """(nodes of the last graph, host ms of its capture and instantiation or update)."""
+        nodes, ms = ctypes.c_ulonglong(0), ctypes.c_float(0.0)
+        rc = self.lib.pcg_ensemble_graph_info(self.e, ctypes.byref(nodes), ctypes.byref(ms))
+        if rc != 0:
+            raise PcgError(rc, "pcg_ensemble_graph_info", "")
+        return int(nodes.value), float(ms.value)
 
     def close(self):
         if getattr(self, "e", None):
