@@ -274,7 +274,7 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   const float2 ic2 = bc(1.f / kC2);
   const float2 beta = mul(fma(v2, v2, fma(v1, v1, mul(v0, v0))), ic2);
   const bool subA = beta.x < 1.f, subB = beta.y < 1.f;  // superluminal or NaN: the scalar path reports it
-  if constexpr (KIND == 1) {
+  if constexpr (KIND == 1 || KIND == 3) {
     // ---- Vay push (pusherVay.cpp:22-114), as the scalar push computes it: u =
     // gamma v, in units of c in the fixed mode and in m/s as the reference has it ----
     const float cn = FIX ? 1.f / 3.0e8f : 1.f;
@@ -324,6 +324,13 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
   }
   gm = rsq(fma(fma(v2, v2, fma(v1, v1, mul(v0, v0))), ic2, bc(1.f)));
   v0 = mul(v0, gm); v1 = mul(v1, gm); v2 = mul(v2, gm);
+  }
+  if constexpr (KIND == 3) {  // the push half of a collisional step: the velocities alone
+    okA = preA && subA;
+    okB = preB && subB;
+    if (okA) { b.vr[ja] = v0.x; b.vphi[ja] = v1.x; b.vz[ja] = v2.x; }
+    if (okB) { b.vr[jb] = v0.y; b.vphi[jb] = v1.y; b.vz[jb] = v2.y; }
+    return;
   }
 
   // ---- move in the local Cartesian frame and back to r-z (specieP.cpp:482-491, 609-640) ----
@@ -565,7 +572,9 @@ constexpr size_t kPairSmemBytes = kPairFixedBytes + 1024 + (size_t)kStages * kSt
 // kErrTimeout, waits (bounded) for the copies in flight and ends the block.
 // KIND 0: the relativistic Boris pusher and the Villasenor-Buneman current;
 // KIND 1: the Vay pusher and the ZigZag current; KIND 2: the move half of
-// a collisional step with the ZigZag current (no field window).
+// a collisional step with the ZigZag current (no field window); KIND 3:
+// the push half of a collisional step with the Vay pusher (gather and push
+// from the field window, velocities stored, no current).
 template <int FIX, int KIND = 0>
 // Four resident blocks per SM (64 registers) measured faster than three
 // with 80 registers and no spill.
@@ -707,7 +716,10 @@ __global__ void __launch_bounds__(kThreads, 4)
       const unsigned n = min(32u, qtail - qhead);
       const unsigned jj = myq[(qhead + lane) & (kQueue - 1)];
       qhead += n;
-      if ((unsigned)lane < n) tile_particle<KIND == 0 ? 0 : 1>(a, b, jj, load_slot(b, jj), sv, sd);
+      if ((unsigned)lane < n) {
+        if constexpr (KIND == 3) push_slot(a, b, jj, load_slot(b, jj));
+        else tile_particle<KIND == 0 ? 0 : 1>(a, b, jj, load_slot(b, jj), sv, sd);
+      }
       __syncwarp();
     }
   }
@@ -720,6 +732,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (lane == 0) raise_error(a.st, kErrTimeout);
   }
   __syncthreads();
+  if constexpr (KIND == 3) return;  // a push deposits nothing
   for (int row = warp; row < 3 * kJWR; row += kThreads / 32) {
     const int c = row / kJWR, i = ji0 + (row - c * kJWR);
     float* dst = a.Jr + c * a.plane + (i + 2) * a.ld + 2;

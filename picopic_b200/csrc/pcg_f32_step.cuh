@@ -765,14 +765,10 @@ __global__ void __launch_bounds__(kThreads) step_flat_kernel(StepArgs a, Species
   if (advance_one(a, b, j, p, e, bb, &m)) deposit<CUR>(a, global_dep(a), m);
 }
 
-// The push alone, one thread per slot of [0, n), fields from the global
-// grid: the first half of a step whose collisions act between the push and
+// The push alone, one thread per slot, fields from the global grid: the first half of a step whose collisions act between the push and
 // the move (SMB::advance_particles, SMB.cpp:1289-1293); the step kernels
 // then run with StepArgs::pushed set.
-__global__ void __launch_bounds__(kThreads) push_flat_kernel(StepArgs a, SpeciesF32Buffers b, size_t n) {
-  const size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const Slot p = load_slot(b, j);
+__device__ __forceinline__ void push_slot(const StepArgs& a, const SpeciesF32Buffers& b, size_t j, const Slot& p) {
   if (p.cell < 0 || !cell_in_halo(a, p.cell)) return;
   float e[3], bb[3];
   gather(a, global_fields(a), cell_r_of(p.cell), p.fr, cell_z_of(p.cell), p.fz, e, bb);
@@ -781,6 +777,13 @@ __global__ void __launch_bounds__(kThreads) push_flat_kernel(StepArgs a, Species
   b.vr[j] = v[0];
   b.vphi[j] = v[1];
   b.vz[j] = v[2];
+}
+
+// Slots [j0, n).
+__global__ void __launch_bounds__(kThreads) push_flat_kernel(StepArgs a, SpeciesF32Buffers b, size_t j0, size_t n) {
+  const size_t j = j0 + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  push_slot(a, b, j, load_slot(b, j));
 }
 
 // One particle of a tile block: gather from the shared window (or the grid

@@ -603,8 +603,21 @@ void f32_push_species(const F32Step& st, SpeciesF32Buffers& b, size_t n, double 
   if (n == 0) return;
   f32::StepArgs a = f32_step_args(st, charge, mass, is_beam);
   a.pushed = 0;
-  f32::push_flat_kernel<<<blocks_for(n), f32::kThreads, 0, s>>>(a, b, n);
-  b.launches += 1;
+  size_t j0 = 0;
+  if (b.sorted_n && st.pusher == PCG_PUSHER_VAY && !is_beam && !st.fixed) {
+    // the tile-sorted slots through the pair kernel's push (field window, two per thread)
+    auto kern = f32::step_pair_kernel<0, 3>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f32::kPairSmemBytes) !=
+        cudaSuccess)
+      return;
+    kern<<<dim3(st.tiles.ntiles, b.splits), f32::kThreads, f32::kPairSmemBytes, s>>>(a, b, st.tiles);
+    b.launches += 1;
+    j0 = std::min(n, b.sorted_n);
+  }
+  if (n > j0) {
+    f32::push_flat_kernel<<<blocks_for(n - j0), f32::kThreads, 0, s>>>(a, b, j0, n);
+    b.launches += 1;
+  }
 }
 
 void f32_alive_flags(const SpeciesF32Buffers& b, unsigned char* flags, size_t n, cudaStream_t s) {

@@ -341,3 +341,45 @@ def test_warp_pairing_equals_thread_pairing(scheme, quirks, extra_ions):
     for sid in (0, 1):
         for k in ("vr", "vphi", "vz"):
             assert np.array_equal(pa[sid][k], pb[sid][k]), (sid, k)
+
+
+def test_collisional_vay_zigzag_step_at_zero_density_matches_collisionless():
+    """A float step with collisions pushes, collides, then moves.  With the
+    Vay pusher and the ZigZag current (reference quirks), its push of the
+    tile-sorted slots runs the pair kernel's push-only instance (field
+    window, two particles per thread) and its move the move-only instance;
+    a collisionless step runs the fused instance.  With zero-weight
+    particles every cell's density is zero, which stops the binary pass at
+    each row's first cell (collisionsP12.cpp:351-354), so three steps in
+    random fields give the same particles in both; from the second step on
+    the push sees sorted slots.  (With small but non-zero weights a few
+    close pairs still scatter at large angles.)"""
+    from picopic_b200 import Domain
+    from tests.cases import particles, random_fields
+    grid = small_grid(nr=16, nz=64, pml=False)
+    out = []
+    for collide in (False, True):
+        d = Domain(grid, pusher="vay", current="zigzag", precision="f32", quirks="reference", seed=5)
+        for sp in (ELECTRONS, IONS):
+            d.add(sp, capacity=40000)
+        for i, sp in enumerate((ELECTRONS, IONS)):
+            r, z, vr, vp, vz, w = particles(grid, 16000, 30 + i, mass=sp.mass, boost=3.0)
+            d.set_particles(i, r, z, vr, vp, vz, w * 0.0)
+        for name, a in random_fields(grid, 8, scale=1e3).items():
+            d.set_field(name, a)
+        if collide:
+            d.set_collisions("binary")
+        d.step(3)
+        out.append(d)
+    a, b = out
+    for sid in (0, 1):
+        pa, pb = a.get_particles(sid), b.get_particles(sid)
+        assert pa["r"].size == pb["r"].size
+        vscale = max(np.abs(pa[k]).max() for k in ("vr", "vphi", "vz"))
+        for k in ("vr", "vphi", "vz"):
+            assert np.abs(pa[k] - pb[k]).max() <= 1e-5 * vscale, (sid, k)
+        for k, L in (("r", grid.radius), ("z", grid.longitude)):
+            assert np.abs(pa[k] - pb[k]).max() <= 1e-6 * L, (sid, k)
+    for name in ("e_r", "e_z", "h_phi"):
+        fa, fb = a.get_field(name), b.get_field(name)
+        assert np.abs(fa - fb).max() <= 1e-6 * np.abs(fa).max(), name
