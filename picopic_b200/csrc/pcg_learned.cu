@@ -21,8 +21,9 @@
 // cell's thermal energy sum_s W_s sum_a T_s,a is unchanged, and every
 // particle of the cell moves to v_a' = u_a + (v_a - u_a) sqrt(T'_a / T_a):
 // the species' momentum and the new second moments hold exactly in FP64.
-// The network itself runs on tcgen05 (pcg_mlp_tc.cuh) inside the per-cell
-// kernel; training keeps the mma.sync kernels of pcg_mlp.cu.
+// The network itself runs on tcgen05 (pcg_mlp_tc.cuh) in a kernel of its
+// own between the per-cell input and transform kernels; training keeps the
+// mma.sync kernels of pcg_mlp.cu.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -175,13 +176,14 @@ __global__ void __launch_bounds__(kTileCells) tile_moments_kernel(GridGeom g, Ti
   }
 }
 
-// The state and raw features of cell c (row i); false when the cell has
+// The state of cell c (row i) from its moment sums (st: axis temperatures,
+// their means, weights, mean velocities, S), its list densities n, list
+// counts N and collision numbers s_ee, s_ei, s_ii; false when the cell has
 // fewer than two particles in a list or no positive temperature.
-__device__ bool cell_features(const GridGeom& g, const LearnedPhys& ph, const double* m, int i,
-                              double st[kStateWords], float x[kFeatures]) {
+__device__ bool cell_state(const GridGeom& g, const LearnedPhys& ph, const double* m, int i,
+                           double st[kStateWords], double n[2], double N[2], double s3[3]) {
   const double mass[2] = {ph.m_el, ph.m_ion}, q[2] = {ph.q_el, ph.q_ion};
   const double vol = kPi * g.dz * g.dr * g.dr * (2.0 * i + 1);
-  double n[2], N[2];
   for (int l = 0; l < 2; ++l) {
     const double* ml = m + 8 * l;
     N[l] = ml[0];
@@ -208,8 +210,19 @@ __device__ bool cell_features(const GridGeom& g, const LearnedPhys& ph, const do
     const double em = kEps0 * mab;
     return fmax(n[a], n[b]) * ph.dt * kLogL * (qq * qq) / (4.0 * kPi * em * em * v2 * sqrt(v2));
   };
-  const double see = s_of(0, 0), sei = s_of(0, 1), sii = s_of(1, 1);
-  st[16] = see + sei + sii;
+  s3[0] = s_of(0, 0);
+  s3[1] = s_of(0, 1);
+  s3[2] = s_of(1, 1);
+  st[16] = s3[0] + s3[1] + s3[2];
+  return true;
+}
+
+// The state and raw features of cell c (row i); false as cell_state.
+__device__ bool cell_features(const GridGeom& g, const LearnedPhys& ph, const double* m, int i,
+                              double st[kStateWords], float x[kFeatures]) {
+  double n[2], N[2], s3[3];
+  if (!cell_state(g, ph, m, i, st, n, N, s3)) return false;
+  const double see = s3[0], sei = s3[1], sii = s3[2];
   for (int a = 0; a < 3; ++a) {
     x[a] = (float)(st[a] / st[6] - 1.0);
     x[3 + a] = (float)(st[3 + a] / st[7] - 1.0);
@@ -223,7 +236,7 @@ __device__ bool cell_features(const GridGeom& g, const LearnedPhys& ph, const do
     const double d = st[10 + a] - st[13 + a];
     du2 += d * d;
   }
-  x[10] = (float)sqrt(du2 / (3.0 * kE * st[6] / mass[0]));
+  x[10] = (float)sqrt(du2 / (3.0 * kE * st[6] / ph.m_el));
   x[11] = (float)log(n[1] / n[0]);
   x[12] = (float)(1.0 / sqrt(N[0] + N[1]));
   return true;
@@ -239,37 +252,30 @@ __global__ void features_kernel(GridGeom g, LearnedPhys ph, const double* mom, f
   scale[c] = ok ? st[16] : 0.0;
 }
 
-struct LearnSmem {
-  mlp::tc::Smem t;  // weights, operand tiles, mbarrier and TMEM address of the tcgen05 MLP
-  double st[mlp::tc::kRows][kStateWords];
-  unsigned long long n_learned, n_fallback;
-};
+// The learned step's cells in three passes, so that the FP64 state and
+// feature arithmetic runs at full occupancy and the tensor-core pass only
+// moves operands:
+//   learned_input_kernel: a thread per cell: features, the training-box
+//     test (flag: 0 no collision, 1 learned, 2 binary fallback) and the
+//     normalised BF16 network input (16 values, 32 bytes per cell);
+//   learned_mlp_kernel: blocks take tiles of 128 cells in turn (weights
+//     staged once per block), thread r the tile's cell r: the MLP on the
+//     fifth-generation tensor cores (tcgen05.mma into tensor memory,
+//     pcg_mlp_tc.cuh) for tiles with a learned cell, the 6 outputs stored;
+//     a wait that times out sets count[2] and ends the block;
+//   learned_xform_kernel: a thread per cell: the state again from the
+//     moments, the new temperatures and the cell's transform.
 
-// Blocks take tiles of 128 cells in turn (the weights are staged in shared
-// memory once per block), thread r the tile's cell r: its features, the MLP
-// on the fifth-generation tensor cores (tcgen05.mma into tensor memory,
-// pcg_mlp_tc.cuh), then the cell's new temperatures and transform.  A wait
-// for the tensor cores that times out sets count[2] and ends the block.
-__global__ void __launch_bounds__(mlp::tc::kThreads) learned_cells_kernel(GridGeom g, LearnedPhys ph,
-                                                                          const double* mom, const float* P,
-                                                                          LearnedNorm nm, double* xform,
-                                                                          unsigned char* flag,
-                                                                          unsigned long long* count) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  LearnSmem& sm = *reinterpret_cast<LearnSmem*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
+__global__ void __launch_bounds__(kThreads) learned_input_kernel(GridGeom g, LearnedPhys ph, const double* mom,
+                                                                 LearnedNorm nm, uint4* xin, unsigned char* flag,
+                                                                 unsigned long long* count) {
   const size_t cells = (size_t)g.nr * g.nz;
-  const size_t tiles = (cells + mlp::tc::kRows - 1) / mlp::tc::kRows;
-  const int r = threadIdx.x;
-  mlp::tc::load_weights(sm.t, P);
-  if (r == 0) { sm.n_learned = 0; sm.n_fallback = 0; }
-  mlp::tc::begin(sm.t);
-  uint32_t phase = 0;
-  unsigned char* a1 = reinterpret_cast<unsigned char*>(sm.t.A1);
-  for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const size_t c = tile * mlp::tc::kRows + r;
-    float x[kFeatures];
-    unsigned char stt = 0;
-    if (c < cells && cell_features(g, ph, mom + c * kMomWords, (int)(c / g.nz), sm.st[r], x)) {
+  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  unsigned char stt = 0;
+  float x[kFeatures];
+  if (c < cells) {
+    double st[kStateWords];
+    if (cell_features(g, ph, mom + c * kMomWords, (int)(c / g.nz), st, x)) {
       stt = 1;
       for (int k = 0; k < kFeatures; ++k) {
         const float span = nm.x_hi[k] - nm.x_lo[k];
@@ -286,45 +292,75 @@ __global__ void __launch_bounds__(mlp::tc::kThreads) learned_cells_kernel(GridGe
       }
       pk[q] = mlp::pack2(__float2bfloat16_rn(v[0]), __float2bfloat16_rn(v[1]));
     }
-    *reinterpret_cast<uint4*>(a1 + mlp::tc::canon(r, 0, mlp::kInPad)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-    *reinterpret_cast<uint4*>(a1 + mlp::tc::canon(r, 8, mlp::kInPad)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    xin[2 * c] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    xin[2 * c + 1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    flag[c] = stt;
+  }
+  const int nl = __syncthreads_count(stt == 1), nf = __syncthreads_count(stt == 2);
+  if (threadIdx.x == 0) {
+    if (nl) atomicAdd(count, (unsigned long long)nl);
+    if (nf) atomicAdd(count + 1, (unsigned long long)nf);
+  }
+}
+
+__global__ void __launch_bounds__(mlp::tc::kThreads) learned_mlp_kernel(size_t cells, const float* P,
+                                                                        const uint4* xin,
+                                                                        const unsigned char* flag, float* yout,
+                                                                        unsigned long long* count) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  mlp::tc::Smem& sm = *reinterpret_cast<mlp::tc::Smem*>((reinterpret_cast<uintptr_t>(raw) + 1023) &
+                                                        ~uintptr_t(1023));
+  const size_t tiles = (cells + mlp::tc::kRows - 1) / mlp::tc::kRows;
+  const int r = threadIdx.x;
+  mlp::tc::load_weights(sm, P);
+  mlp::tc::begin(sm);
+  uint32_t phase = 0;
+  unsigned char* a1 = reinterpret_cast<unsigned char*>(sm.A1);
+  for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const size_t c = tile * mlp::tc::kRows + r;
+    const bool on = c < cells && flag[c] == 1;
+    if (!__syncthreads_or(on)) continue;  // no learned cell in the tile (the same in every thread)
+    const uint4 lo = on ? xin[2 * c] : make_uint4(0, 0, 0, 0), hi = on ? xin[2 * c + 1] : make_uint4(0, 0, 0, 0);
+    *reinterpret_cast<uint4*>(a1 + mlp::tc::canon(r, 0, mlp::kInPad)) = lo;
+    *reinterpret_cast<uint4*>(a1 + mlp::tc::canon(r, 8, mlp::kInPad)) = hi;
     float y[mlp::kOut];
-    if (!mlp::tc::forward_tile(sm.t, phase, y)) {
+    if (!mlp::tc::forward_tile(sm, phase, y)) {
       if (r == 0) atomicAdd(count + 2, 1ull);
       break;
     }
-    if (c < cells) {
-      double xf[12] = {0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1};
-      if (stt == 1) {
-        const double* st = sm.st[r];
-        double Tn[2][3], e0 = 0.0, e1 = 0.0;
-        for (int l = 0; l < 2; ++l)
-          for (int a = 0; a < 3; ++a) {
-            const double yv = (double)y[3 * l + a] * nm.y_std[3 * l + a] + nm.y_mean[3 * l + a];
-            Tn[l][a] = st[3 * l + a] + st[6 + l] * st[16] * yv;
-            e0 += st[8 + l] * st[3 * l + a];
-            e1 += st[8 + l] * Tn[l][a];
-          }
-        const double f = e1 > 0.0 ? e0 / e1 : 1.0;  // the cell's thermal energy is kept
-        for (int l = 0; l < 2; ++l)
-          for (int a = 0; a < 3; ++a) {
-            const double T = st[3 * l + a], T1 = fmax(Tn[l][a] * f, 1e-6 * st[6 + l]);
-            xf[6 * l + a] = st[10 + 3 * l + a];
-            xf[6 * l + 3 + a] = T > 0.0 ? sqrt(T1 / T) : 1.0;
-          }
-        atomicAdd(&sm.n_learned, 1ull);
-      } else if (stt == 2) {
-        atomicAdd(&sm.n_fallback, 1ull);
+    if (on)
+      for (int q = 0; q < mlp::kOut; ++q) yout[c * mlp::kOut + q] = y[q];
+  }
+  mlp::tc::end(sm, phase);
+}
+
+__global__ void __launch_bounds__(kThreads) learned_xform_kernel(GridGeom g, LearnedPhys ph, const double* mom,
+                                                                 LearnedNorm nm, const float* yout,
+                                                                 const unsigned char* flag, double* xform,
+                                                                 const unsigned long long* count) {
+  const size_t cells = (size_t)g.nr * g.nz;
+  const size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (c >= cells || count[2]) return;
+  double xf[12] = {0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1};
+  double st[kStateWords], n[2], N[2], s3[3];
+  if (flag[c] == 1 && cell_state(g, ph, mom + c * kMomWords, (int)(c / g.nz), st, n, N, s3)) {
+    double Tn[2][3], e0 = 0.0, e1 = 0.0;
+    for (int l = 0; l < 2; ++l)
+      for (int a = 0; a < 3; ++a) {
+        const double yv = (double)yout[c * kTargets + 3 * l + a] * nm.y_std[3 * l + a] + nm.y_mean[3 * l + a];
+        Tn[l][a] = st[3 * l + a] + st[6 + l] * st[16] * yv;
+        e0 += st[8 + l] * st[3 * l + a];
+        e1 += st[8 + l] * Tn[l][a];
       }
-      for (int q = 0; q < 12; ++q) xform[c * 12 + q] = xf[q];
-      flag[c] = stt;
-    }
+    const double f = e1 > 0.0 ? e0 / e1 : 1.0;  // the cell's thermal energy is kept
+    for (int l = 0; l < 2; ++l)
+      for (int a = 0; a < 3; ++a) {
+        const double T = st[3 * l + a], T1 = fmax(Tn[l][a] * f, 1e-6 * st[6 + l]);
+        xf[6 * l + a] = st[10 + 3 * l + a];
+        xf[6 * l + 3 + a] = T > 0.0 ? sqrt(T1 / T) : 1.0;
+      }
   }
-  mlp::tc::end(sm.t, phase);
-  if (r == 0) {
-    if (sm.n_learned) atomicAdd(count, sm.n_learned);
-    if (sm.n_fallback) atomicAdd(count + 1, sm.n_fallback);
-  }
+  for (int q = 0; q < 12; ++q) xform[c * 12 + q] = xf[q];
 }
 
 // Applies the per-cell transforms; after a tensor-core time-out (count[2])
@@ -439,7 +475,7 @@ int ensure(const GridGeom& g, LearnedWork& w) {
   const size_t cells = (size_t)g.nr * g.nz;
   if (w.cells == cells && w.mom) return 0;
   if (grow(&w.mom, cells * kMomWords) || grow(&w.xform, cells * 12) || grow(&w.flag, cells) ||
-      grow(&w.count, 3))
+      grow(&w.count, 3) || grow(&w.xin, 2 * cells) || grow(&w.yout, cells * kTargets))
     return -1;
   w.cells = cells;
   return 0;
@@ -473,19 +509,21 @@ int learned_step(const GridGeom& g, const CollSpecies* sp, int nsp, const Learne
                  unsigned long long counts[2], cudaStream_t s, bool apply) {
   if (!w.model) return -1;
   if (learned_moments(g, sp, nsp, w, s)) return -1;
-  const size_t smem = sizeof(LearnSmem) + 1024;
-  static const bool attr = cudaFuncSetAttribute(learned_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t smem = sizeof(mlp::tc::Smem) + 1024;
+  static const bool attr = cudaFuncSetAttribute(learned_mlp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)smem) == cudaSuccess;
   if (!attr) return -1;
   cudaMemsetAsync(w.count, 0, 3 * sizeof(unsigned long long), s);
+  learned_input_kernel<<<blocks_for(w.cells), kThreads, 0, s>>>(g, ph, w.mom, w.norm, w.xin, w.flag, w.count);
   const size_t tiles = (w.cells + mlp::tc::kRows - 1) / mlp::tc::kRows;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const unsigned blocks = (unsigned)std::min<size_t>(tiles, (size_t)sms * 2);
-  learned_cells_kernel<<<blocks, mlp::tc::kThreads, smem, s>>>(g, ph, w.mom, w.params, w.norm, w.xform, w.flag,
-                                                                w.count);
-  ++w.launches;
+  learned_mlp_kernel<<<blocks, mlp::tc::kThreads, smem, s>>>(w.cells, w.params, w.xin, w.flag, w.yout, w.count);
+  learned_xform_kernel<<<blocks_for(w.cells), kThreads, 0, s>>>(g, ph, w.mom, w.norm, w.yout, w.flag, w.xform,
+                                                                  w.count);
+  w.launches += 3;
   const TileGrid tg = f32_tile_grid(g);
   const unsigned tile_blocks = tile_grid_blocks(tg);
   for (int t = 0; apply && t < nsp; ++t) {
@@ -519,6 +557,7 @@ int learned_set_model(LearnedWork& w, const float* params_host, const float* nor
 
 void learned_free(LearnedWork& w) {
   cudaFree(w.mom); cudaFree(w.xform); cudaFree(w.flag); cudaFree(w.count); cudaFree(w.params);
+  cudaFree(w.xin); cudaFree(w.yout);
   w = LearnedWork();
 }
 

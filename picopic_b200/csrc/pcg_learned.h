@@ -35,7 +35,9 @@ struct LearnedWork {
   double* mom = nullptr;          // cells x kMomWords
   double* xform = nullptr;        // cells x 12: u_e (3), s_e (3), u_i (3), s_i (3)
   unsigned char* flag = nullptr;  // cells: 0 no collision, 1 learned, 2 binary fallback
-  unsigned long long* count = nullptr;  // learned cells, fallback cells
+  unsigned long long* count = nullptr;  // learned cells, fallback cells, tensor-core time-outs
+  uint4* xin = nullptr;           // cells x 2: the network's normalised BF16 inputs
+  float* yout = nullptr;          // cells x kTargets: its outputs
   float* params = nullptr;        // the model's FP32 parameters
   LearnedNorm norm{};
   bool model = false;
