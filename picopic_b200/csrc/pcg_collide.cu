@@ -135,10 +135,17 @@ __global__ void shuffle_kernel(size_t cells, const unsigned* start, const unsign
   __shared__ unsigned long long buf[kThreads / 32][kShufCap];
   __shared__ unsigned short part[kThreads / 32][kShufCap];
   const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const size_t stride = (size_t)gridDim.x * (kThreads / 32);
-  for (size_t c = blockIdx.x * (size_t)(kThreads / 32) + w; c < cells; c += stride) {
-    const unsigned n = count[c];
-    if (n < 2) continue;
+  // a warp reads the counts of 32 cells at once and takes the ones with a
+  // list of two or more in turn (a pass over chosen cells leaves most empty)
+  const size_t stride = (size_t)gridDim.x * (kThreads / 32) * 32;
+  for (size_t c0 = (blockIdx.x * (size_t)(kThreads / 32) + w) * 32; c0 < cells; c0 += stride) {
+    const unsigned nl = c0 + lane < cells ? count[c0 + lane] : 0u;
+    unsigned todo = __ballot_sync(0xffffffffu, nl >= 2);
+    while (todo) {
+    const int b = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const size_t c = c0 + b;
+    const unsigned n = __shfl_sync(0xffffffffu, nl, b);
     unsigned long long* L = vals + start[c];
     if (n > kShufCap) {
       if (lane == 0)
@@ -166,6 +173,7 @@ __global__ void shuffle_kernel(size_t cells, const unsigned* start, const unsign
     __syncwarp();
     for (unsigned i = lane; i < n; i += 32) L[i] = buf[w][i];
     __syncwarp();
+    }
   }
 }
 

@@ -413,8 +413,11 @@ __device__ __forceinline__ void pair_particles(const StepArgs& a, const SpeciesF
 
 // The fast path of a pair in the move half of a collisional step (the
 // velocities were pushed before the collisions): the learned collision
-// step's transform of the particle's cell where its flag is set, then the
-// move and the in-cell ZigZag currents of pair_particles.
+// step's transform of the particle's cell, v' = u + (v - u) s per axis in
+// FP32 from the block's table of its window cells (the identity where the
+// cell's flag is not 1; the float store rounds as the FP64 form of the
+// scalar path does, to within an ulp), then the move and the in-cell ZigZag
+// currents of pair_particles.
 template <int FIX>
 __device__ __forceinline__ void pair_move_particles(const StepArgs& a, const SpeciesF32Buffers& b, unsigned ja,
                                                     unsigned jb, const Slot& A, const Slot& B, bool hasA, bool hasB,
@@ -430,21 +433,20 @@ __device__ __forceinline__ void pair_move_particles(const StepArgs& a, const Spe
   if (!preA && !preB) return;
   if (!preA) { ciA = ciB; ckA = ckB; }
   if (!preB) { ciB = ciA; ckB = ckA; }
-  float vA[3] = {A.vr, A.vphi, A.vz}, vB[3] = {B.vr, B.vphi, B.vz};
-  if (a.xform) {  // v' = u + (v - u) s per axis, in FP64 (the transform's arithmetic)
-    const size_t cA = (size_t)ciA * a.nz + ckA, cB = (size_t)ciB * a.nz + ckB;
-    if (preA && a.xflag[cA] == 1) {
-      const double* t = a.xform + cA * 12 + a.xoff;
-      for (int q = 0; q < 3; ++q) vA[q] = (float)(t[q] + ((double)vA[q] - t[q]) * t[3 + q]);
-    }
-    if (preB && a.xflag[cB] == 1) {
-      const double* t = a.xform + cB * 12 + a.xoff;
-      for (int q = 0; q < 3; ++q) vB[q] = (float)(t[q] + ((double)vB[q] - t[q]) * t[3 + q]);
-    }
+  float2 v0 = make_float2(A.vr, B.vr), v1 = make_float2(A.vphi, B.vphi), v2 = make_float2(A.vz, B.vz);
+  if (a.xform) {  // the table: {u_r, u_phi, u_z, s_r} per window cell, then {s_phi, s_z}
+    constexpr unsigned kXS = 16u * kFWR * kFWS;
+    const unsigned qA = (unsigned)((ciA - W.fi0) * kFWS + (ckA - W.fk0));
+    const unsigned qB = (unsigned)((ciB - W.fi0) * kFWS + (ckB - W.fk0));
+    const float4 UA = lds4(W.F + 16u * qA), UB = lds4(W.F + 16u * qB);
+    const float2 SA = lds2(W.F + kXS + 8u * qA), SB = lds2(W.F + kXS + 8u * qB);
+    const float2 u0 = make_float2(UA.x, UB.x), u1 = make_float2(UA.y, UB.y), u2 = make_float2(UA.z, UB.z);
+    v0 = fma(sub(v0, u0), make_float2(UA.w, UB.w), u0);
+    v1 = fma(sub(v1, u1), make_float2(SA.x, SB.x), u1);
+    v2 = fma(sub(v2, u2), make_float2(SA.y, SB.y), u2);
   }
   const float2 fr = make_float2(A.fr, B.fr), fz = make_float2(A.fz, B.fz);
   const float2 fi = make_float2((float)ciA, (float)ciB);
-  const float2 v0 = make_float2(vA[0], vB[0]), v1 = make_float2(vA[1], vB[1]), v2 = make_float2(vA[2], vB[2]);
   // the move of pair_particles (specieP.cpp:482-491, 609-640)
   const float2 dx = mul(v0, bc(a.dt_dr)), dyp = mul(v1, bc(a.dt_dr)), dYv = mul(v2, bc(a.dt_dz));
   const float2 x0 = add(fi, fr);
@@ -644,6 +646,32 @@ __global__ void __launch_bounds__(kThreads, 4)
       for (int q = 0; q < kCols; ++q) {
         const int col = lane + 32 * q;
         if (row < kRows && col < kFWZ) sF[row * kFWS + col] = v[r][q];
+      }
+    }
+  }
+  if constexpr (KIND == 2) {
+    // the learned transforms of the window's cells, in the field window's
+    // place (the move gathers nothing): {u_r, u_phi, u_z, s_r}, then
+    // {s_phi, s_z}; the identity where a cell's flag is not 1
+    static_assert(6 * kFWR * kFWS * sizeof(float) == (sizeof(float4) + sizeof(float2)) * kFWR * kFWS,
+                  "the transform table fills the field window");
+    if (a.xform) {
+      float4* XU = reinterpret_cast<float4*>(sF);
+      float2* XS = reinterpret_cast<float2*>(XU + kFWR * kFWS);
+      for (int q = threadIdx.x; q < kFWR * kFWS; q += kThreads) {
+        const int i = fi0 + q / kFWS, k = fk0 + q % kFWS;
+        float4 u = make_float4(0.f, 0.f, 0.f, 1.f);
+        float2 v = make_float2(1.f, 1.f);
+        if (i >= 0 && i < a.nr && k >= 0 && k < a.nz) {
+          const size_t c = (size_t)i * a.nz + k;
+          if (a.xflag[c] == 1) {
+            const double* t = a.xform + c * 12 + a.xoff;
+            u = make_float4((float)t[0], (float)t[1], (float)t[2], (float)t[3]);
+            v = make_float2((float)t[4], (float)t[5]);
+          }
+        }
+        XU[q] = u;
+        XS[q] = v;
       }
     }
   }
