@@ -598,6 +598,9 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
     p.pass = h->coll_pass++;
     p.only = h->learned.flag;
     p.only_value = 2;
+    // few cells, often the fullest (a bunch's): a warp per cell from 32
+    // particles on (the same collisions and results as a thread per cell)
+    p.crowded = std::min(p.crowded, 32u);
     unsigned long long calls = 0;
     if (collide_p12(h->g, v.data(), (int)v.size(), p, h->coll, &calls, h->stream) != 0)
       return fail(h, PCG_ERR_CUDA, "collision fallback");
