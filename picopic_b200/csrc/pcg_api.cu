@@ -586,6 +586,9 @@ int run_collide_learned(pcg_handle* h, unsigned long long* learned_cells, unsign
   if (!collision_species(h, v, p))
     return fail(h, PCG_ERR_STATE, "collisions need species named 'electrons' and 'ions'");
   unsigned long long counts[2] = {0, 0};
+  h->learned.aux = h->aux;
+  h->learned.ev_fork = h->aux ? h->ev_fork : nullptr;
+  h->learned.ev_join = h->aux ? h->ev_join : nullptr;
   const int lr = learned_step(h->g, v.data(), (int)v.size(), learned_phys(p), h->learned, counts, h->stream,
                               !in_step);
   if (lr == kLearnedTimeout) {

@@ -489,12 +489,20 @@ int learned_moments(const GridGeom& g, const CollSpecies* sp, int nsp, LearnedWo
   const TileGrid tg = f32_tile_grid(g);
   const unsigned tile_blocks = tile_grid_blocks(tg);
   w.launches = 0;
+  // the passes are latency-bound walks that only add to the sums: the
+  // odd-numbered species' run on the second stream beside the others
+  const bool fork = nsp >= 2 && w.aux && w.ev_fork && w.ev_join;
+  if (fork && (cudaEventRecord(w.ev_fork, s) != cudaSuccess || cudaStreamWaitEvent(w.aux, w.ev_fork, 0) != cudaSuccess))
+    return -1;
   for (int t = 0; t < nsp; ++t) {
+    const cudaStream_t st = fork && (t & 1) ? w.aux : s;
     const size_t j0 = tiled(sp[t]) ? sp[t].sorted : 0;
-    if (j0) tile_moments_kernel<<<tile_blocks, kTileCells, 0, s>>>(g, tg, sp[t], w.mom);
-    if (sp[t].n > j0) moments_kernel<<<blocks_for(sp[t].n - j0), kThreads, 0, s>>>(g, sp[t], w.mom, j0);
+    if (j0) tile_moments_kernel<<<tile_blocks, kTileCells, 0, st>>>(g, tg, sp[t], w.mom);
+    if (sp[t].n > j0) moments_kernel<<<blocks_for(sp[t].n - j0), kThreads, 0, st>>>(g, sp[t], w.mom, j0);
     w.launches += (j0 ? 1 : 0) + (sp[t].n > j0 ? 1 : 0);
   }
+  if (fork && (cudaEventRecord(w.ev_join, w.aux) != cudaSuccess || cudaStreamWaitEvent(s, w.ev_join, 0) != cudaSuccess))
+    return -1;
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -42,6 +42,10 @@ struct LearnedWork {
   LearnedNorm norm{};
   bool model = false;
   unsigned launches = 0;  // kernels launched by the last learned_moments / learned_step
+  // a second stream and two events of the caller (all or none): the moment
+  // passes of odd-numbered species run there, concurrently with the others
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // Per-cell moment sums of the species (electron list: every species not
