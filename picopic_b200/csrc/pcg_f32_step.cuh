@@ -38,7 +38,7 @@ struct StepArgs {
   float dr_m, dz_m, dt_s;      // dr, dz, dt in SI (ZigZag keeps metre-valued weights)
   float zz_vol;                // 1/(PI dz dr^2)
   int pusher, current, fixed, is_beam;
-  int pushed;  // the velocities were pushed by push_flat_kernel (a step with collisions)
+  int pushed;  // the velocities were pushed already (the push half of a step with collisions)
   // with pushed: the learned collision step's per-cell transforms, applied
   // to a particle before its move when its cell's flag is 1 (v' = u + (v -
   // u) s per axis, u = xform[12 c + xoff ..], s = xform[12 c + xoff + 3 ..])
