@@ -59,7 +59,8 @@ def test_null_handles_are_rejected_without_a_device():
         ("pcg_synchronize", (null,)), ("pcg_get_stream", (null, null)), ("pcg_set_field", (null, 0, null)),
         ("pcg_export_field", (null, 0, null)), ("pcg_ensemble_create", (null, 0, 1, null)),
         ("pcg_ensemble_step", (null, 1, null)), ("pcg_ensemble_autotune", (null, 1, null)),
-        ("pcg_ensemble_destroy", (null,)),
+        ("pcg_ensemble_destroy", (null,)), ("pcg_ensemble_set_graph", (null, 1)),
+        ("pcg_ensemble_graph_info", (null, null, null)),
     ]
     for name, args in calls:
         assert getattr(lib, name)(*args) == -1, name
